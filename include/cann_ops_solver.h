@@ -1,0 +1,101 @@
+/*
+ * cann_ops_solver.h -- drop-in C ABI of the B200 (sm_100a) factor-and-solve library.
+ *
+ * Every declaration below keeps the name, argument order, argument meaning, status codes
+ * and info conventions of the reference entry point cited beside it (paths are relative
+ * to the reference project root).  Matrices are column major, A[i + j*lda]; matrices,
+ * pointer tables, pivots and info live in device memory unless stated otherwise.  All
+ * compute entries enqueue on the handle stream and return without synchronising, except
+ * where the reference contract itself synchronises (the finite/pivot checks of the real
+ * LU family and the host-buffer aclsolverSgetrs).
+ *
+ * Argument-error info values are -i, i the 1-based argument position excluding handle.
+ */
+#pragma once
+#include <stdint.h>
+
+#include "cann_ops_solver_common.h"
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+#ifdef __cplusplus
+extern "C"
+{
+#endif
+
+    /* ---- handle and stream; reference include/cann_ops_solver.h:50,61,70,80 ----------- */
+
+    /* Creates a handle bound to the current CUDA device.  *handle must be NULL on entry. */
+    aclsolverStatus_t aclsolverCreate(aclsolverHandle_t *handle);
+    /* Waits for the handle's scratch users, frees scratch, frees the handle. */
+    aclsolverStatus_t aclsolverDestroy(aclsolverHandle_t handle);
+    /* Binds a stream (NULL = legacy default stream) to the handle. */
+    aclsolverStatus_t aclsolverSetStream(aclsolverHandle_t handle, aclrtStream stream);
+    aclsolverStatus_t aclsolverGetStream(aclsolverHandle_t handle, aclrtStream *stream);
+
+    /* ---- real LU family; reference include/cann_ops_solver.h:100-110 -------------------- */
+
+    /* Lwork in float elements; replaces cann_ops_solver.h:100 (src/sgetrf/sgetrf_host.cpp:24). */
+    aclsolverStatus_t aclsolverSgetrf_bufferSize(aclsolverHandle_t handle, int m, int n, float *A, int lda, int *Lwork);
+    /* P*A = L*U in place, 1-based devIpiv (NULL = no pivoting), devInfo = first zero U(k,k);
+     * replaces cann_ops_solver.h:101 (src/sgetrf/sgetrf_host.cpp:96).  Non-finite input gives
+     * INVALID_VALUE with devInfo=-3 after a synchronous check, as in the reference. */
+    aclsolverStatus_t aclsolverSgetrf(aclsolverHandle_t handle, int m, int n, float *A, int lda, float *Workspace,
+                                      int *devIpiv, int *devInfo);
+    /* replaces cann_ops_solver.h:103 (src/sgetri/sgetri_host.cpp:59). */
+    aclsolverStatus_t aclsolverSgetri_bufferSize(aclsolverHandle_t handle, int n, float *A, int lda, int *Lwork);
+    /* In-place inverse from packed LU + pivots; replaces cann_ops_solver.h:104 (src/sgetri/sgetri_host.cpp:86). */
+    aclsolverStatus_t aclsolverSgetri(aclsolverHandle_t handle, int n, float *A, int lda, int *devIpiv,
+                                      float *Workspace, int Lwork, int *devInfo);
+    /* Out-of-place inverse of a batch of LU factors, PivotArray n*batchSize (NULL = none);
+     * replaces cann_ops_solver.h:106 (src/sgetri_batched/sgetri_batched_host.cpp:86). */
+    aclsolverStatus_t aclsolverSgetriBatched(aclsolverHandle_t handle, int n, const float *const Aarray[], int lda,
+                                             const int *PivotArray, float *const Carray[], int ldc, int *infoArray,
+                                             int batchSize);
+    /* Inverse of original matrices, 0 <= n <= 32; replaces cann_ops_solver.h:109
+     * (src/smatinv_batched/smatinv_batched_host.cpp:11). */
+    aclsolverStatus_t aclsolverSmatinvBatched(aclsolverHandle_t handle, int n, const float *const A[], int lda,
+                                              float *const Ainv[], int lda_inv, int *info, int batchSize);
+
+    /* ---- real Cholesky family; reference include/cann_ops_solver.h:433-547 -------------- */
+
+    /* replaces cann_ops_solver.h:433 (src/cholesky/arch35/cholesky_host.cpp:236). */
+    aclsolverStatus_t aclsolverSpotrf_bufferSize(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n, float *A,
+                                                 int lda, int *Lwork);
+    /* replaces cann_ops_solver.h:451 (src/cholesky/arch35/cholesky_host.cpp:246). */
+    aclsolverStatus_t aclsolverSpotrf(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n, float *A, int lda,
+                                      float *Workspace, int Lwork, int *devInfo);
+    /* 0 <= nrhs <= 128; replaces cann_ops_solver.h:470 (src/cholesky/arch35/cholesky_host.cpp:331). */
+    aclsolverStatus_t aclsolverSpotrs(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n, int nrhs,
+                                      const float *A, int lda, float *B, int ldb, int *devInfo);
+    /* replaces cann_ops_solver.h:484 (src/cholesky/arch35/cholesky_host.cpp:241). */
+    aclsolverStatus_t aclsolverSpotri_bufferSize(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n, float *A,
+                                                 int lda, int *Lwork);
+    /* Batched in-place Cholesky; a null slot sets only its info to -3; host argument errors
+     * fill every info entry; replaces cann_ops_solver.h:524 (cholesky_host.cpp:283). */
+    aclsolverStatus_t aclsolverSpotrfBatched(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n, float *Aarray[],
+                                             int lda, int *infoArray, int batchSize);
+    /* Batched solve, nrhs must be 1 for non-empty problems; info is a device scalar set to -4
+     * (null A slot) or -6 (null B slot); replaces cann_ops_solver.h:545 (cholesky_host.cpp:363). */
+    aclsolverStatus_t aclsolverSpotrsBatched(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n, int nrhs,
+                                             float *Aarray[], int lda, float *Barray[], int ldb, int *info,
+                                             int batchSize);
+
+    /* ---- host-buffer LU solve; reference include/cann_ops_solver.h:1011 ----------------- */
+
+    /* A (packed LU), ipiv, B and info are HOST buffers in ROW-major order: A(r,c) = A[r*lda+c],
+     * B(r,c) = B[r*ldb+c].  trans 0 solves A X = B, 1 solves A^T X = B.  Synchronous.  An ipiv
+     * entry outside [1,n] sets *info = -4.  Returns ACL_SUCCESS or ACL_ERROR_INVALID_PARAM;
+     * replaces cann_ops_solver.h:1011 (src/sgetrs/sgetrs_host.cpp:131). */
+    aclError aclsolverSgetrs(aclsolverHandle_t handle, const uint64_t trans, const int64_t n, const int64_t nrhs,
+                             float *A, const int64_t lda, int32_t *ipiv, float *B, const int64_t ldb, int32_t *info);
+
+#ifdef __cplusplus
+}
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#include "cann_ops_solver_b200.h"

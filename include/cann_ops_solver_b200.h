@@ -1,0 +1,60 @@
+/*
+ * cann_ops_solver_b200.h -- entry points this build adds beside the reference C ABI.
+ *
+ * None of these names exists in the reference; the existing entry points of
+ * cann_ops_solver.h keep their reference contracts unchanged.  Each addition states the
+ * reference call sequence it stands in for.  All of them are asynchronous on the handle
+ * stream (no host synchronisation inside), so they can be captured in a CUDA graph.
+ */
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+#include "cann_ops_solver_common.h"
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+#ifdef __cplusplus
+extern "C"
+{
+#endif
+
+    /* Switches the synchronous device-data checks of the real LU family on the handle:
+     * the non-finite scan (src/utils/real_lu_common.h:90, CheckFinite), the pivot-range
+     * read-back (:134, CheckPivots) and the pointer-table validation (:196, ArrayValidation)
+     * of aclsolverSgetrf, aclsolverSgetri, aclsolverSgetriBatched and aclsolverSmatinvBatched.
+     * enabled = 1 (the default) keeps the reference contract: those entries copy metadata
+     * back and synchronise the handle stream.  enabled = 0 skips them, which makes the
+     * entries asynchronous and capturable in a CUDA graph; argument checks stay, and the
+     * caller becomes responsible for finite inputs, valid pivots and disjoint outputs. */
+    aclsolverStatus_t aclsolverSetDeviceChecks(aclsolverHandle_t handle, int enabled);
+    aclsolverStatus_t aclsolverGetDeviceChecks(aclsolverHandle_t handle, int *enabled);
+
+    /* Batched P*A = L*U of square n x n matrices, the arithmetic of aclsolverSgetrf applied to
+     * every slot (first-maximum |a| pivot with the earliest row on ties, IEEE division of the
+     * column, FMA rank-1 updates).  PivotArray holds n pivots per matrix, 1-based (NULL = no
+     * pivoting).  infoArray[b] = first zero U(k,k) of matrix b, or -2 for a null slot.
+     * The reference exposes no batched getrf: its callers issue one aclsolverSgetrf
+     * (include/cann_ops_solver.h:101) per matrix, each with a synchronous finite check.
+     * This entry does not scan for non-finite values (they propagate, as in LAPACK).
+     * 0 <= n <= 4096.  Argument errors: INVALID_VALUE, infoArray filled with -i.  A null
+     * matrix slot sets its info to -2. */
+    aclsolverStatus_t aclsolverSgetrfBatched(aclsolverHandle_t handle, int n, float *const Aarray[], int lda,
+                                             int *PivotArray, int *infoArray, int batchSize);
+
+    /* Batched solve op(A_b) X_b = B_b from the factors of aclsolverSgetrfBatched, device
+     * column-major buffers (the reference aclsolverSgetrs, include/cann_ops_solver.h:1011, is
+     * host-buffer, row-major and synchronous).  trans: ACLSOLVER_OP_N or ACLSOLVER_OP_T.
+     * PivotArray n per matrix (NULL = no pivoting).  infoArray[b] = 0, or -i argument error,
+     * or -6 when matrix b's pivot k lies outside [k+1, n] (that slot is left unsolved).  0 <= n <= 4096, 0 <= nrhs. */
+    aclsolverStatus_t aclsolverSgetrsBatched(aclsolverHandle_t handle, aclsolverOperation_t trans, int n, int nrhs,
+                                             const float *const Aarray[], int lda, const int *PivotArray,
+                                             float *const Barray[], int ldb, int *infoArray, int batchSize);
+
+#ifdef __cplusplus
+}
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif

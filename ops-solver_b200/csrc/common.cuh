@@ -1,0 +1,38 @@
+// common.cuh -- device helpers shared by the sm_100a factor-and-solve kernels.
+//
+// All arithmetic on the plain (FP32) path goes through the explicitly rounded intrinsics
+// below so that the compiler can neither contract a multiply and an add into an FMA nor
+// split an FMA: the parity contract is bit-for-bit equality with the reference's
+// per-element operation order.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ops_solver
+{
+
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float sqrt_rn(float a) { return __fsqrt_rn(a); }
+// fma_rn(a, b, c) = a*b + c with one rounding.
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+// Matrix slot b of a device pointer table.  Loaded through the read-only path: the
+// tables are never written by a kernel.
+template <typename T>
+__device__ __forceinline__ T *slot(T *const *table, int64_t b)
+{
+    return reinterpret_cast<T *>(__ldg(reinterpret_cast<const unsigned long long *>(table) + b));
+}
+
+// Pivot-search key: larger |a| wins, NaN never wins (key 0); ties are broken separately
+// by the smallest row position.  Non-negative float bit patterns order like the values.
+__device__ __forceinline__ unsigned pivot_key(float v)
+{
+    float m = fabsf(v);
+    return m == m ? __float_as_uint(m) + 1u : 0u;
+}
+
+}  // namespace ops_solver

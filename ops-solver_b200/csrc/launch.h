@@ -1,0 +1,63 @@
+// launch.h -- the internal launcher interface between the host C++ layer (argument
+// ladders, dispatch, scratch) and the CUDA kernels.  Plain pointers and sizes only.
+//
+// Every launcher enqueues on `stream` and returns the cudaError_t of the launch
+// (cudaGetLastError after the <<<>>>), never synchronising.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ops_solver
+{
+
+// A batch of column-major float matrices: either a device pointer table (`table`, slot
+// first+q) or a single matrix (`single`).
+struct RealBatch
+{
+    float *single;
+    float *const *table;
+    int n;
+    int ld;
+    int first;
+    int count;
+};
+
+// ---- real Cholesky ---------------------------------------------------------------------
+// Fills info[0..count) with value.
+cudaError_t launch_fill_info(int *info, int value, int64_t count, cudaStream_t stream);
+// SpotrsBatched slot scan: info[0] = -4 if any A slot is null, else -6 if any B slot is
+// null, else 0 (cholesky_simt.cpp:28-48 contract).
+cudaError_t launch_solve_slot_check(int *info, float *const *a, float *const *b, int count, cudaStream_t stream);
+// In-place Cholesky of n <= 32 matrices, per-slot info (null slot -> -3).
+cudaError_t launch_potrf_small(const RealBatch &a, int upper, int *info, cudaStream_t stream);
+// In-place Cholesky of n > 32 matrices (FMA order, left-looking), per-slot info.
+cudaError_t launch_potrf_mid(const RealBatch &a, int upper, int *info, cudaStream_t stream);
+// Cholesky solve for n > 32: dot-accumulate order (dot_order = 1) or right-looking order.
+cudaError_t launch_potrs_generic(const RealBatch &a, const RealBatch &b, int nrhs, int upper, int dot_order,
+                                 const int *info, cudaStream_t stream);
+// Cholesky solve for n <= 32 (SolveKernel order), any nrhs; skipped when info[0] != 0.
+cudaError_t launch_potrs_small(const RealBatch &a, const RealBatch &b, int nrhs, int upper, const int *info,
+                               cudaStream_t stream);
+
+// ---- real LU ---------------------------------------------------------------------------
+// Batched LU of m x n matrices (a.n columns) for m, n <= 64.  ipiv: min(m, n) per matrix
+// (nullptr = no pivoting).  info: first zero pivot, -2 for a null slot.
+cudaError_t launch_getrf_small(const RealBatch &a, int m, int *ipiv, int *info, cudaStream_t stream);
+// Batched LU solve for n <= 64; trans 0/1; ipiv n per matrix or nullptr.
+cudaError_t launch_getrs_small(const RealBatch &a, const int *ipiv, const RealBatch &b, int nrhs, int trans,
+                               int *info, cudaStream_t stream);
+// Batched out-of-place inverse from LU for n <= 64 (c may alias a: the factors are staged
+// in shared memory before the inverse is written).
+cudaError_t launch_getri_small(const RealBatch &a, const int *ipiv, const RealBatch &c, int *info,
+                               cudaStream_t stream);
+
+// ---- validation and staging ------------------------------------------------------------
+// flag[0] |= 1 when any of the m x n leading entries of any matrix is NaN or infinite.
+cudaError_t launch_finite_scan(const RealBatch &a, int m, int *flag, cudaStream_t stream);
+// dst[i + j*ldd] = src[i + j*lds] for each matrix (copy of the leading m x n block).
+cudaError_t launch_copy_matrices(const RealBatch &src, const RealBatch &dst, int m, cudaStream_t stream);
+// dst (column-major, ldd) = transpose of src (column-major, lds), src rows x cols.
+cudaError_t launch_transpose(const float *src, int lds, float *dst, int ldd, int rows, int cols,
+                             cudaStream_t stream);
+
+}  // namespace ops_solver

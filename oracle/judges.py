@@ -1,0 +1,135 @@
+"""Residual judges restated from the reference's own test suite (test infrastructure).
+
+  cholesky_ratio / paired_cholesky   test/cholesky/lapack_residual.py:27-86
+      ||L L^T - A||_1 / (n ||A||_1 eps) for a factor, max_j ||b - A x||_1 /
+      (||A||_1 ||x||_1 eps) for a solve, in FP64 on the actual FP32 input, eps = 2^-23; the
+      device ratio passes when <= max(5 * ratio of FP32 LAPACK, 3 * batch mean) (:147-182).
+  lu_reconstruction_ok               test/sgetrf/real_lu_test_impl.h:199-214
+      |(P A)_ij - (L U)_ij| <= 1e-4 * max(1, |(P A)_ij|).
+  solve_compare_ok                   test/utils/lu_verify_utils.py:262-290
+      |err| <= 1e-3 or |err| / |x| <= 1e-3 on at least 99.99 % of entries.
+  solve_lu                           test/utils/lu_verify_utils.py:67-192 (numpy LU solve)
+  backward_error / forward_error     normwise errors against an FP64 LAPACK solve.
+"""
+
+import numpy as np
+import scipy.linalg as la
+from scipy.linalg.lapack import spotrf, spotrs
+
+EPS = 2.0**-23
+
+
+def symmetric(a32, upper):
+    a = np.asarray(a32, dtype=np.float64)
+    half = np.triu(a) if upper else np.tril(a)
+    return half + half.T - np.diag(np.diag(half))
+
+
+def cholesky_ratio(op, a32, out, upper=False, b32=None):
+    a = symmetric(a32, upper)
+    out = np.asarray(out, dtype=np.float64)
+    if not np.isfinite(a).all() or not np.isfinite(out).all():
+        return float("inf")
+    n = len(a)
+    anorm = np.linalg.norm(a, 1)
+    if op == "potrf":
+        f = np.triu(out) if upper else np.tril(out)
+        if np.any(np.diag(f) <= 0):
+            return float("inf")
+        err = f.T @ f - a if upper else f @ f.T - a
+        return float(np.linalg.norm(err, 1) / (n * anorm * EPS))
+    b = np.asarray(b32, dtype=np.float64)
+    num = np.abs(b - a @ out).sum(axis=0)
+    den = anorm * np.abs(out).sum(axis=0) * EPS
+    ratios = np.divide(num, den, out=np.full_like(num, np.inf), where=den > 0)
+    ratios[(num == 0) & (den == 0)] = 0
+    return float(np.max(ratios))
+
+
+def paired_cholesky(op, a32, out, upper=False, b32=None):
+    """(device ratio, FP32 LAPACK ratio) for one matrix."""
+    f, info = spotrf(np.array(a32, dtype=np.float32, order="F"), lower=not upper)
+    assert info == 0
+    if op == "potrf":
+        cpu = f
+    else:
+        cpu, info = spotrs(f, np.array(b32, dtype=np.float32, order="F"), lower=not upper)
+        assert info == 0
+    return cholesky_ratio(op, a32, out, upper, b32), cholesky_ratio(op, a32, cpu, upper, b32)
+
+
+def cholesky_batch_passes(op, a32, outs, upper=False, b32=None):
+    """The batched gate: every ratio <= max(5 * its CPU ratio, 3 * mean CPU ratio)."""
+    pairs = [paired_cholesky(op, a32[q], outs[q], upper, None if b32 is None else b32[q]) for q in range(len(outs))]
+    mean = float(np.mean([p[1] for p in pairs]))
+    bad = [q for q, (r, c) in enumerate(pairs) if not (np.isfinite(r) and r <= max(5 * c, 3 * mean))]
+    return not bad, pairs, bad
+
+
+def apply_pivots(a, ipiv):
+    """P A for 1-based LAPACK pivots applied in order."""
+    pa = np.array(a, dtype=np.float64)
+    for k, p in enumerate(np.asarray(ipiv) - 1):
+        if p != k:
+            pa[[k, p], :] = pa[[p, k], :]
+    return pa
+
+
+def lu_product(lu, m, n):
+    lu = np.asarray(lu, dtype=np.float64)
+    k = min(m, n)
+    lower = np.tril(lu[:, :k], -1)
+    lower[np.arange(k), np.arange(k)] = 1.0
+    upper = np.triu(lu[:k, :])
+    return lower @ upper
+
+
+def lu_reconstruction_ok(a, lu, ipiv):
+    m, n = a.shape
+    pa = apply_pivots(a, ipiv) if ipiv is not None else np.asarray(a, dtype=np.float64)
+    prod = lu_product(lu, m, n)
+    return bool(np.all(np.isfinite(prod)) and np.all(np.abs(prod - pa) <= 1e-4 * np.maximum(1.0, np.abs(pa))))
+
+
+def solve_compare_ok(actual, expected):
+    actual = np.asarray(actual, dtype=np.float64).ravel()
+    expected = np.asarray(expected, dtype=np.float64).ravel()
+    err = np.abs(actual - expected)
+    rel = err / np.maximum(np.abs(expected), 1e-12)
+    ok = (err <= 1e-3) | (rel <= 1e-3)
+    return bool(ok.mean() >= 0.9999)
+
+
+def solve_lu(lu, b, ipiv, trans=0):
+    """numpy LU solve: swaps in LAPACK order, unit-lower forward, upper backward."""
+    lu = np.asarray(lu, dtype=np.float64)
+    x = np.array(b, dtype=np.float64).reshape(len(lu), -1)
+    piv = np.asarray(ipiv) - 1
+    if trans == 0:
+        for i, p in enumerate(piv):
+            x[[i, p], :] = x[[p, i], :]
+        x = la.solve_triangular(lu, x, lower=True, unit_diagonal=True)
+        return la.solve_triangular(lu, x, lower=False)
+    w = la.solve_triangular(lu, x, lower=False, trans="T")
+    z = la.solve_triangular(lu, w, lower=True, unit_diagonal=True, trans="T")
+    perm = np.arange(len(lu))
+    for i, p in enumerate(piv):
+        perm[[i, p]] = perm[[p, i]]
+    out = np.empty_like(z)
+    out[perm, :] = z
+    return out
+
+
+def backward_error(a, x, b):
+    """||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) in FP64."""
+    a = np.asarray(a, dtype=np.float64)
+    x = np.asarray(x, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    r = b - a @ x
+    return float(np.abs(r).max() / (np.abs(a).sum(axis=1).max() * np.abs(x).max() + np.abs(b).max()))
+
+
+def forward_error(a, x, b):
+    """||x - x64||_inf / ||x64||_inf against an FP64 LAPACK solve."""
+    x64 = la.solve(np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64))
+    return float(np.abs(np.asarray(x, dtype=np.float64) - x64).max() / np.abs(x64).max())

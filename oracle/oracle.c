@@ -1,0 +1,494 @@
+/*
+ * oracle.c -- CPU restatement of the reference's factor-and-solve arithmetic.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker the parity tests, the smoke check
+ * and the benchmark's CPU-baseline leg compare the CUDA library against.  The library
+ * (libops_solver.so) never links, loads or calls it.
+ *
+ * Each routine restates one reference kernel's per-element operation order so that the
+ * CUDA kernels can be checked bit for bit (paths relative to the reference project root):
+ *   orc_spotrf_simt     src/cholesky/arch35/cholesky_simt.cpp:52-92        (n <= 8)
+ *   orc_spotrf_group    src/cholesky/arch35/cholesky_vector.cpp:588-794    (9 <= n <= 32)
+ *                       with StoreSmallCompleted :837-862 (failed slots keep unfinished columns)
+ *   orc_spotrs_simt     src/cholesky/arch35/cholesky_simt.cpp:93-117       (SolveKernel)
+ *   orc_spotrs_dot      src/cholesky/arch35/cholesky_vector.cpp:30-122     (VectorTriSolve, AccumulateDot)
+ *   orc_sgetrf          src/utils/kernel/real_lu.hpp:59-139 (first-max pivot, NaN rule),
+ *                       :216-311 (swap, IEEE division), :345-368 (FMA rank-1), :409-448 (loop, info)
+ *   orc_sgetri_vector   src/sgetri/real_lu_blocked_inverse_kernel.cpp:676-830,1040-1044
+ * Routines for sizes where the reference hands its arithmetic to a third-party Cube GEMM
+ * (CATLASS / CANN MatmulImpl) restate this build's own order instead, and say so:
+ *   orc_spotrf_fma      right-looking Cholesky with FMA updates in ascending k (n > 32)
+ *   orc_spotrs_right    right-looking Cholesky solve (n > 128)
+ *   orc_sgetrs          column-oriented LU solve (math of test/utils/lu_verify_utils.py:67-192)
+ *
+ * Compiled with -ffp-contract=off: every fused multiply-add is an explicit fmaf().
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define FLT_MAX_VALUE 3.402823466e38F
+
+/* Element (i, j) of the factor triangle: lower reads A[i + j*lda], upper reads the mirror
+ * A[j + i*lda] (cholesky_simt.cpp:19-22, Offset). */
+static inline int64_t tri_at(int lda, int upper, int i, int j)
+{
+    return upper ? (int64_t)i * lda + j : (int64_t)j * lda + i;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * Real Cholesky
+ * ------------------------------------------------------------------------------------- */
+
+/* n <= 8: left-looking dot products with fmaf, sqrt refined once by its FMA residual,
+ * IEEE division of the column (cholesky_simt.cpp:64-90).  Returns info. */
+int orc_spotrf_simt(int n, float *a, int lda, int upper)
+{
+    for (int k = 0; k < n; ++k)
+    {
+        float d = a[(int64_t)k * (lda + 1)];
+        for (int t = 0; t < k; ++t)
+        {
+            float f = a[tri_at(lda, upper, k, t)];
+            d = fmaf(-f, f, d);
+        }
+        if (!(d > 0)) return k + 1;
+        float root = sqrtf(d);
+        float correction = fmaf(-root, root, d);
+        d = fmaf(correction, 0.5f / root, root);
+        a[(int64_t)k * (lda + 1)] = d;
+        for (int i = k + 1; i < n; ++i)
+        {
+            float x = a[tri_at(lda, upper, i, k)];
+            for (int t = 0; t < k; ++t) x = fmaf(-a[tri_at(lda, upper, i, t)], a[tri_at(lda, upper, k, t)], x);
+            a[tri_at(lda, upper, i, k)] = x / d;
+        }
+    }
+    return 0;
+}
+
+/* 9 <= n <= 32 (any n is accepted): right-looking in groups of four columns.  Per column:
+ * pivot check d > 0 && d <= FLT_MAX, IEEE sqrt, IEEE division of the rows below, the
+ * diagonal stores sqrt(d) itself; in-group updates a -= (l * alpha) with separate rounding;
+ * after the group, a rank-4 trailing update a -= (((p0 + p1) + p2) + p3), every product and
+ * sum rounded separately (cholesky_vector.cpp:588-794).  A failed matrix keeps only its
+ * completed columns (StoreSmallCompleted, :837-862): columns >= info-1 of the caller's
+ * matrix are left as they were. */
+int orc_spotrf_group(int n, float *a, int lda, int upper)
+{
+    /* Work on a private dense lower copy w[j*n + i] = A(i, j). */
+    float *w = (float *)malloc(sizeof(float) * (size_t)n * (size_t)n + 4);
+    for (int j = 0; j < n; ++j)
+        for (int i = j; i < n; ++i) w[(size_t)j * n + i] = a[tri_at(lda, upper, i, j)];
+    int failure = 0;
+    for (int base = 0; base < n && !failure; base += 4)
+    {
+        int end = base + 4;
+        for (int k = base; k < end && k < n; ++k)
+        {
+            float d = w[(size_t)k * n + k];
+            if (!(d > 0.0f && d <= FLT_MAX_VALUE))
+            {
+                failure = k + 1;
+                break;
+            }
+            float s = sqrtf(d);
+            for (int i = k + 1; i < n; ++i) w[(size_t)k * n + i] = w[(size_t)k * n + i] / s;
+            w[(size_t)k * n + k] = s;
+            for (int j = k + 1; j < end && j < n; ++j)
+            {
+                float alpha = w[(size_t)k * n + j];
+                for (int i = j; i < n; ++i)
+                {
+                    float product = w[(size_t)k * n + i] * alpha;
+                    w[(size_t)j * n + i] = w[(size_t)j * n + i] - product;
+                }
+            }
+        }
+        if (failure) break;
+        for (int j = end; j < n; ++j)
+        {
+            float a0 = w[(size_t)base * n + j], a1 = w[(size_t)(base + 1) * n + j];
+            float a2 = w[(size_t)(base + 2) * n + j], a3 = w[(size_t)(base + 3) * n + j];
+            for (int i = j; i < n; ++i)
+            {
+                float sum = w[(size_t)base * n + i] * a0;
+                float p = w[(size_t)(base + 1) * n + i] * a1;
+                sum = sum + p;
+                p = w[(size_t)(base + 2) * n + i] * a2;
+                sum = sum + p;
+                p = w[(size_t)(base + 3) * n + i] * a3;
+                sum = sum + p;
+                w[(size_t)j * n + i] = w[(size_t)j * n + i] - sum;
+            }
+        }
+    }
+    int done = failure ? failure - 1 : n;
+    for (int j = 0; j < done; ++j)
+        for (int i = j; i < n; ++i) a[tri_at(lda, upper, i, j)] = w[(size_t)j * n + i];
+    free(w);
+    return failure;
+}
+
+/* n > 32 (this build's order; the reference uses a CATLASS FP32 Gram product here):
+ * right-looking, IEEE sqrt and division, trailing updates a = fmaf(-l_ik, l_jk, a) applied
+ * in ascending k.  Any blocking that keeps each element's ascending-k FMA sequence
+ * reproduces these bits.  A failed matrix keeps only its completed columns. */
+int orc_spotrf_fma(int n, float *a, int lda, int upper)
+{
+    float *w = (float *)malloc(sizeof(float) * (size_t)n * (size_t)n + 4);
+    for (int j = 0; j < n; ++j)
+        for (int i = j; i < n; ++i) w[(size_t)j * n + i] = a[tri_at(lda, upper, i, j)];
+    int failure = 0;
+    for (int k = 0; k < n; ++k)
+    {
+        float d = w[(size_t)k * n + k];
+        if (!(d > 0.0f && d <= FLT_MAX_VALUE))
+        {
+            failure = k + 1;
+            break;
+        }
+        float s = sqrtf(d);
+        w[(size_t)k * n + k] = s;
+        for (int i = k + 1; i < n; ++i) w[(size_t)k * n + i] = w[(size_t)k * n + i] / s;
+        for (int j = k + 1; j < n; ++j)
+        {
+            float ljk = w[(size_t)k * n + j];
+            for (int i = j; i < n; ++i) w[(size_t)j * n + i] = fmaf(-w[(size_t)k * n + i], ljk, w[(size_t)j * n + i]);
+        }
+    }
+    int done = failure ? failure - 1 : n;
+    for (int j = 0; j < done; ++j)
+        for (int i = j; i < n; ++i) a[tri_at(lda, upper, i, j)] = w[(size_t)j * n + i];
+    free(w);
+    return failure;
+}
+
+/* The size dispatch of SpotrfBatched / Spotrf in this build. */
+int orc_spotrf(int n, float *a, int lda, int upper)
+{
+    if (n <= 8) return orc_spotrf_simt(n, a, lda, upper);
+    if (n <= 32) return orc_spotrf_group(n, a, lda, upper);
+    return orc_spotrf_fma(n, a, lda, upper);
+}
+
+/* SolveKernel (cholesky_simt.cpp:93-117): per right-hand side a forward then a backward
+ * substitution, each x = fmaf(-l, b_j, x) in ascending (forward) or ascending-from-i+1
+ * (backward) j, then an IEEE division by the diagonal. */
+void orc_spotrs_simt(int n, int nrhs, const float *a, int lda, float *b, int ldb, int upper)
+{
+    for (int r = 0; r < nrhs; ++r)
+    {
+        float *pb = b + (int64_t)r * ldb;
+        for (int i = 0; i < n; ++i)
+        {
+            float x = pb[i];
+            for (int j = 0; j < i; ++j) x = fmaf(-a[tri_at(lda, upper, i, j)], pb[j], x);
+            pb[i] = x / a[(int64_t)i * (lda + 1)];
+        }
+        for (int i = n - 1; i >= 0; --i)
+        {
+            float x = pb[i];
+            for (int j = i + 1; j < n; ++j) x = fmaf(-a[tri_at(lda, upper, j, i)], pb[j], x);
+            pb[i] = x / a[(int64_t)i * (lda + 1)];
+        }
+    }
+}
+
+/* VectorTriSolve with AccumulateDot (cholesky_vector.cpp:30-122), used for 33..128 with one
+ * right-hand side: a dot accumulator starts at zero and takes dot_i = fmaf(l, x_k, dot_i)
+ * right-looking; each x_k = (b_k - dot_k) / l_kk, subtracted once. */
+void orc_spotrs_dot(int n, int nrhs, const float *a, int lda, float *b, int ldb, int upper)
+{
+    float *dot = (float *)malloc(sizeof(float) * (size_t)(n > 0 ? n : 1));
+    for (int r = 0; r < nrhs; ++r)
+    {
+        float *pb = b + (int64_t)r * ldb;
+        for (int i = 0; i < n; ++i) dot[i] = 0.0f;
+        for (int k = 0; k < n; ++k)
+        {
+            float x = (pb[k] - dot[k]) / a[(int64_t)k * (lda + 1)];
+            pb[k] = x;
+            for (int i = k + 1; i < n; ++i) dot[i] = fmaf(a[tri_at(lda, upper, i, k)], x, dot[i]);
+        }
+        for (int i = 0; i < n; ++i) dot[i] = 0.0f;
+        for (int k = n - 1; k >= 0; --k)
+        {
+            float x = (pb[k] - dot[k]) / a[(int64_t)k * (lda + 1)];
+            pb[k] = x;
+            for (int i = 0; i < k; ++i) dot[i] = fmaf(a[tri_at(lda, upper, k, i)], x, dot[i]);
+        }
+    }
+    free(dot);
+}
+
+/* n > 128 (this build's order; the reference solves panels with a Cube product here):
+ * right-looking sweeps, x_k = x_k / l_kk then x_i = fmaf(-l_ik, x_k, x_i) for i > k (k
+ * ascending), and the same with l_ki for i < k (k descending). */
+void orc_spotrs_right(int n, int nrhs, const float *a, int lda, float *b, int ldb, int upper)
+{
+    for (int r = 0; r < nrhs; ++r)
+    {
+        float *x = b + (int64_t)r * ldb;
+        for (int k = 0; k < n; ++k)
+        {
+            x[k] = x[k] / a[(int64_t)k * (lda + 1)];
+            for (int i = k + 1; i < n; ++i) x[i] = fmaf(-a[tri_at(lda, upper, i, k)], x[k], x[i]);
+        }
+        for (int k = n - 1; k >= 0; --k)
+        {
+            x[k] = x[k] / a[(int64_t)k * (lda + 1)];
+            for (int i = 0; i < k; ++i) x[i] = fmaf(-a[tri_at(lda, upper, k, i)], x[k], x[i]);
+        }
+    }
+}
+
+/* The solve dispatch of this build (cholesky_simt.cpp:186-199 with the batch always
+ * larger than the reference's core count): batched n <= 32 and single n <= 8 use the
+ * SolveKernel order; batched 33..128 and single 9..128 use the dot-accumulate order;
+ * above 128 the right-looking order. */
+void orc_spotrs(int n, int nrhs, const float *a, int lda, float *b, int ldb, int upper, int single)
+{
+    if (n > 128)
+        orc_spotrs_right(n, nrhs, a, lda, b, ldb, upper);
+    else if (single ? n > 8 : n > 32)
+        orc_spotrs_dot(n, nrhs, a, lda, b, ldb, upper);
+    else
+        orc_spotrs_simt(n, nrhs, a, lda, b, ldb, upper);
+}
+
+/* ---------------------------------------------------------------------------------------
+ * Real LU
+ * ------------------------------------------------------------------------------------- */
+
+/* Pivot row for column k (real_lu.hpp:59-139, PivotRF/PivotLocalRF): the first row with the
+ * largest |a| among rows k..m-1; a NaN in row k keeps row k; other NaNs never win. */
+static int lu_pivot(const float *col, int k, int m)
+{
+    float initial = col[k];
+    if (initial != initial) return k;
+    float best = fabsf(initial);
+    int row = k;
+    for (int i = k + 1; i < m; ++i)
+    {
+        float value = fabsf(col[i]);
+        if (value > best)
+        {
+            best = value;
+            row = i;
+        }
+    }
+    return row;
+}
+
+/* P*A = L*U in place (FactorLocalCore, real_lu.hpp:409-448).  ipiv may be NULL (no
+ * pivoting).  Returns info = first k+1 with U(k,k) == 0; such a column is neither scaled
+ * nor used for updates. */
+int orc_sgetrf(int m, int n, float *a, int lda, int *ipiv)
+{
+    int info = 0;
+    int steps = m < n ? m : n;
+    for (int k = 0; k < steps; ++k)
+    {
+        float *col = a + (int64_t)k * lda;
+        int p = ipiv ? lu_pivot(col, k, m) : k;
+        if (ipiv) ipiv[k] = p + 1;
+        if (p != k)
+            for (int j = 0; j < n; ++j)
+            {
+                float t = a[(int64_t)j * lda + k];
+                a[(int64_t)j * lda + k] = a[(int64_t)j * lda + p];
+                a[(int64_t)j * lda + p] = t;
+            }
+        float diagonal = col[k];
+        if (diagonal == 0)
+        {
+            if (info == 0) info = k + 1;
+            continue;
+        }
+        if (k + 1 == m) continue;
+        for (int i = k + 1; i < m; ++i) col[i] = col[i] / diagonal;
+        for (int j = k + 1; j < n; ++j)
+        {
+            float *cj = a + (int64_t)j * lda;
+            float u = cj[k];
+            for (int i = k + 1; i < m; ++i) cj[i] = fmaf(-col[i], u, cj[i]);
+        }
+    }
+    return info;
+}
+
+/* Inverse from packed LU (real_lu_blocked_inverse_kernel.cpp): the permutation is the
+ * identity with the pivot swaps applied in order (:676-714); info is the first zero U
+ * diagonal, a failed matrix stores nothing (:716-738, :958-961); reciprocals r_k = 1/U(k,k)
+ * by IEEE division; column c solves rhs = e with rhs[row] = (perm[row] == c); forward
+ * rhs_i = fmaf(-rhs_k, L(i,k), rhs_i) for i > k, k ascending; backward s = rhs_k * r_k,
+ * rhs_k = s, rhs_i = fmaf(-s, U(i,k), rhs_i) for i < k, k descending (:766-830). */
+int orc_sgetri_vector(int n, const float *lu, int lda, const int *ipiv, float *c, int ldc)
+{
+    int info = 0;
+    for (int k = 0; k < n; ++k)
+        if (lu[(int64_t)k * (lda + 1)] == 0.0f)
+        {
+            info = k + 1;
+            break;
+        }
+    if (info) return info;
+    int *perm = (int *)malloc(sizeof(int) * (size_t)n);
+    float *rec = (float *)malloc(sizeof(float) * (size_t)n);
+    float *rhs = (float *)malloc(sizeof(float) * (size_t)n);
+    for (int i = 0; i < n; ++i) perm[i] = i;
+    if (ipiv)
+        for (int k = 0; k < n; ++k)
+        {
+            int p = ipiv[k] - 1;
+            int t = perm[k];
+            perm[k] = perm[p];
+            perm[p] = t;
+        }
+    for (int k = 0; k < n; ++k) rec[k] = 1.0f / lu[(int64_t)k * (lda + 1)];
+    for (int col = 0; col < n; ++col)
+    {
+        for (int i = 0; i < n; ++i) rhs[i] = perm[i] == col ? 1.0f : 0.0f;
+        for (int k = 0; k < n; ++k)
+        {
+            float s = rhs[k];
+            for (int i = k + 1; i < n; ++i) rhs[i] = fmaf(-s, lu[(int64_t)k * lda + i], rhs[i]);
+        }
+        for (int k = n - 1; k >= 0; --k)
+        {
+            float s = rhs[k] * rec[k];
+            rhs[k] = s;
+            for (int i = 0; i < k; ++i) rhs[i] = fmaf(-s, lu[(int64_t)k * lda + i], rhs[i]);
+        }
+        for (int i = 0; i < n; ++i) c[(int64_t)col * ldc + i] = rhs[i];
+    }
+    free(perm);
+    free(rec);
+    free(rhs);
+    return 0;
+}
+
+/* LU solve, this build's order (the reference solve kernel is a CANN matmul chain; its
+ * test reference is the numpy solve_lu of test/utils/lu_verify_utils.py:67-192, whose
+ * mathematics this follows).  trans 0: row swaps k = 0..n-1, unit-lower forward
+ * b_i = fmaf(-L(i,k), b_k, b_i) for i > k, k ascending; upper backward b_k = b_k / U(k,k),
+ * b_i = fmaf(-U(i,k), b_k, b_i) for i < k, k descending.  trans 1: U^T w = b forward
+ * (w_k = w_k / U(k,k), w_i = fmaf(-U(k,i), w_k, w_i), i > k), L^T z = w backward
+ * (z_i = fmaf(-L(k,i), z_k, z_i), i < k, k descending), then the swaps in reverse order. */
+void orc_sgetrs(int trans, int n, int nrhs, const float *lu, int lda, const int *ipiv, float *b, int ldb)
+{
+    for (int r = 0; r < nrhs; ++r)
+    {
+        float *x = b + (int64_t)r * ldb;
+        if (trans == 0)
+        {
+            if (ipiv)
+                for (int k = 0; k < n; ++k)
+                {
+                    int p = ipiv[k] - 1;
+                    float t = x[k];
+                    x[k] = x[p];
+                    x[p] = t;
+                }
+            for (int k = 0; k < n; ++k)
+                for (int i = k + 1; i < n; ++i) x[i] = fmaf(-lu[(int64_t)k * lda + i], x[k], x[i]);
+            for (int k = n - 1; k >= 0; --k)
+            {
+                x[k] = x[k] / lu[(int64_t)k * (lda + 1)];
+                for (int i = 0; i < k; ++i) x[i] = fmaf(-lu[(int64_t)k * lda + i], x[k], x[i]);
+            }
+        }
+        else
+        {
+            for (int k = 0; k < n; ++k)
+            {
+                x[k] = x[k] / lu[(int64_t)k * (lda + 1)];
+                for (int i = k + 1; i < n; ++i) x[i] = fmaf(-lu[(int64_t)i * lda + k], x[k], x[i]);
+            }
+            for (int k = n - 1; k >= 0; --k)
+                for (int i = 0; i < k; ++i) x[i] = fmaf(-lu[(int64_t)i * lda + k], x[k], x[i]);
+            if (ipiv)
+                for (int k = n - 1; k >= 0; --k)
+                {
+                    int p = ipiv[k] - 1;
+                    float t = x[k];
+                    x[k] = x[p];
+                    x[p] = t;
+                }
+        }
+    }
+}
+
+/* ---------------------------------------------------------------------------------------
+ * Batched drivers over a contiguous slab (matrix b at base + b*stride), OpenMP over
+ * matrices; `threads` <= 0 uses the OpenMP default.  These are what the CPU baseline times.
+ * ------------------------------------------------------------------------------------- */
+
+static void set_threads(int threads)
+{
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#else
+    (void)threads;
+#endif
+}
+
+int orc_max_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void orc_spotrf_batched(int n, float *a, int lda, int64_t stride, int count, int upper, int *info, int threads)
+{
+    set_threads(threads);
+#pragma omp parallel for schedule(static)
+    for (int q = 0; q < count; ++q) info[q] = orc_spotrf(n, a + (int64_t)q * stride, lda, upper);
+}
+
+void orc_spotrs_batched(int n, int nrhs, const float *a, int lda, int64_t astride, float *b, int ldb,
+                        int64_t bstride, int count, int upper, int single, int threads)
+{
+    set_threads(threads);
+#pragma omp parallel for schedule(static)
+    for (int q = 0; q < count; ++q)
+        orc_spotrs(n, nrhs, a + (int64_t)q * astride, lda, b + (int64_t)q * bstride, ldb, upper, single);
+}
+
+void orc_sgetrf_batched(int m, int n, float *a, int lda, int64_t stride, int count, int *ipiv, int *info,
+                        int threads)
+{
+    set_threads(threads);
+    int steps = m < n ? m : n;
+#pragma omp parallel for schedule(static)
+    for (int q = 0; q < count; ++q)
+        info[q] = orc_sgetrf(m, n, a + (int64_t)q * stride, lda, ipiv ? ipiv + (int64_t)q * steps : NULL);
+}
+
+void orc_sgetrs_batched(int trans, int n, int nrhs, const float *lu, int lda, int64_t astride, const int *ipiv,
+                        float *b, int ldb, int64_t bstride, int count, int threads)
+{
+    set_threads(threads);
+#pragma omp parallel for schedule(static)
+    for (int q = 0; q < count; ++q)
+        orc_sgetrs(trans, n, nrhs, lu + (int64_t)q * astride, lda, ipiv ? ipiv + (int64_t)q * n : NULL,
+                   b + (int64_t)q * bstride, ldb);
+}
+
+void orc_sgetri_batched(int n, const float *lu, int lda, int64_t astride, const int *ipiv, float *c, int ldc,
+                        int64_t cstride, int count, int *info, int threads)
+{
+    set_threads(threads);
+#pragma omp parallel for schedule(static)
+    for (int q = 0; q < count; ++q)
+        info[q] = orc_sgetri_vector(n, lu + (int64_t)q * astride, lda, ipiv ? ipiv + (int64_t)q * n : NULL,
+                                    c + (int64_t)q * cstride, ldc);
+}
