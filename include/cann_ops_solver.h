@@ -58,6 +58,30 @@ extern "C"
     aclsolverStatus_t aclsolverSmatinvBatched(aclsolverHandle_t handle, int n, const float *const A[], int lda,
                                               float *const Ainv[], int lda_inv, int *info, int batchSize);
 
+    /* ---- complex Cholesky family; reference include/cann_ops_solver.h:135-247 ----------- */
+
+    /* replaces cann_ops_solver.h:135 (src/cpotrf/arch35). Lwork in complex elements. */
+    aclsolverStatus_t aclsolverCpotrf_bufferSize(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n,
+                                                 aclsolverFloatComplex *A, int lda, int *Lwork);
+    /* A = L*L^H (LOWER) or U^H*U (UPPER) in place; replaces cann_ops_solver.h:152. */
+    aclsolverStatus_t aclsolverCpotrf(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n,
+                                      aclsolverFloatComplex *A, int lda, aclsolverFloatComplex *Workspace, int Lwork,
+                                      int *devInfo);
+    /* Solve from a complex Cholesky factor, 0 <= nrhs <= 128; replaces cann_ops_solver.h:171. */
+    aclsolverStatus_t aclsolverCpotrs(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n, int nrhs,
+                                      const aclsolverFloatComplex *A, int lda, aclsolverFloatComplex *B, int ldb,
+                                      int *devInfo);
+    /* Batched complex Cholesky, uniform n; argument errors use infoArray[0];
+     * replaces cann_ops_solver.h:224 (src/cpotrf_batched/arch35/cpotrf_batched.cpp:14). */
+    aclsolverStatus_t aclsolverCpotrfBatched(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n,
+                                             aclsolverFloatComplex *Aarray[], int lda, int *infoArray, int batchSize);
+    /* Batched complex solve, nrhs must be 1 for non-empty problems; info is a device scalar;
+     * replaces cann_ops_solver.h:244 (src/cpotrs_batched/arch35/cpotrs_batched.cpp:14). */
+    aclsolverStatus_t aclsolverCpotrsBatched(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n, int nrhs,
+                                             const aclsolverFloatComplex *const Aarray[], int lda,
+                                             aclsolverFloatComplex *Barray[], int ldb, int *info, int batchSize);
+
+
     /* ---- real Cholesky family; reference include/cann_ops_solver.h:433-547 -------------- */
 
     /* replaces cann_ops_solver.h:433 (src/cholesky/arch35/cholesky_host.cpp:236). */

@@ -52,6 +52,15 @@ extern "C"
                                              const float *const Aarray[], int lda, const int *PivotArray,
                                              float *const Barray[], int ldb, int *infoArray, int batchSize);
 
+    /* aclsolverCpotrsBatched without its one-right-hand-side restriction: 0 <= nrhs <= 128
+     * columns per matrix, same arguments, info (device scalar) and argument-error rules.  The
+     * reference requires nrhs == 1 for non-empty batches (src/cpotrs_batched/arch35/
+     * cpotrs_batched.cpp:19-21), so a caller with k right-hand sides issues k calls there. */
+    aclsolverStatus_t aclsolverCpotrsBatchedMultiRhs(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n,
+                                                     int nrhs, const aclsolverFloatComplex *const Aarray[], int lda,
+                                                     aclsolverFloatComplex *Barray[], int ldb, int *info,
+                                                     int batchSize);
+
 #ifdef __cplusplus
 }
 #endif

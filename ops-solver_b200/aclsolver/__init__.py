@@ -70,6 +70,7 @@ ARGTYPES = {
     "aclsolverGetDeviceChecks": [VP, C.POINTER(I32)],
     "aclsolverSgetrfBatched": [VP, I32, VP, I32, VP, VP, I32],
     "aclsolverSgetrsBatched": [VP, I32, I32, I32, VP, I32, VP, VP, I32, VP, I32],
+    "aclsolverCpotrsBatchedMultiRhs": [VP, I32, I32, I32, VP, I32, VP, I32, VP, I32],
 }
 
 

@@ -386,6 +386,7 @@ __global__ void __launch_bounds__(RI_THREADS) getri_small_kernel(float *a_single
     __shared__ float rec[MPC][N];
     __shared__ int pv[MPC][N];
     __shared__ int zero_at[MPC];
+    __shared__ int bad_pivot[MPC];
     const int t = threadIdx.x % N;
     const int m = threadIdx.x / N;
     float *lu = buf[m];
@@ -402,7 +403,11 @@ __global__ void __launch_bounds__(RI_THREADS) getri_small_kernel(float *a_single
         }
         const bool live = pa != nullptr && pc != nullptr;
         __syncthreads();
-        if (t == 0) zero_at[m] = 0x7fffffff;
+        if (t == 0)
+        {
+            zero_at[m] = 0x7fffffff;
+            bad_pivot[m] = 0;
+        }
         for (int idx = t; idx < N * N; idx += N)
         {
             const int i = idx % N, j = idx / N;
@@ -415,16 +420,18 @@ __global__ void __launch_bounds__(RI_THREADS) getri_small_kernel(float *a_single
             const float u = lu[t * LP + t];
             rec[m][t] = div_rn(1.0f, u);
             if (u == 0.0f) atomicMin(&zero_at[m], t + 1);
-        }
-        // src: column of the inverse whose permuted unit vector has its 1 at row t.
-        int col = t;
-        for (int k = n - 1; k >= 0; --k)
-        {
-            const int pk = pv[m][k] - 1;
-            col = col == k ? pk : (col == pk ? k : col);
+            if (pv[m][t] < t + 1 || pv[m][t] > n) atomicOr(&bad_pivot[m], 1);
         }
         __syncthreads();
-        const int failed = zero_at[m] == 0x7fffffff ? 0 : zero_at[m];
+        // src: column of the inverse whose permuted unit vector has its 1 at row t.
+        int col = t;
+        if (!bad_pivot[m])
+            for (int k = n - 1; k >= 0; --k)
+            {
+                const int pk = pv[m][k] - 1;
+                col = col == k ? pk : (col == pk ? k : col);
+            }
+        const int failed = bad_pivot[m] ? -4 : (zero_at[m] == 0x7fffffff ? 0 : zero_at[m]);
 
         float rhs[N];
 #pragma unroll

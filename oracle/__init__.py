@@ -37,6 +37,8 @@ def lib():
         _lib.orc_sgetrf_batched.argtypes = [_i, _i, _F, _i, _l, _i, _VP, _I, _i]
         _lib.orc_sgetrs_batched.argtypes = [_i, _i, _i, _F, _i, _l, _VP, _F, _i, _l, _i, _i]
         _lib.orc_sgetri_batched.argtypes = [_i, _F, _i, _l, _VP, _F, _i, _l, _i, _I, _i]
+        _lib.orc_cpotrf_batched.argtypes = [_i, _F, _i, _l, _i, _i, _I, _i]
+        _lib.orc_cpotrs_batched.argtypes = [_i, _i, _F, _i, _l, _F, _i, _l, _i, _i, _i]
         _lib.orc_max_threads.restype = _i
     return _lib
 
@@ -112,3 +114,32 @@ def sgetri_batched(lu, ipiv, threads=0):
         n, ls, n, n * n, None if piv is None else piv.ctypes.data, out, n, n * n, count, info, threads
     )
     return _unslab(out), info
+
+
+def _cslab(a):
+    """(count, n, m) complex64 column-major matrices -> interleaved float32 slab."""
+    a = np.asarray(a, dtype=np.complex64)
+    t = np.array(a.transpose(0, 2, 1), dtype=np.complex64, order="C", copy=True)
+    return t.view(np.float32).reshape(-1).copy(), t.shape
+
+
+def _uncslab(flat, shape):
+    return np.ascontiguousarray(flat.view(np.complex64).reshape(shape).transpose(0, 2, 1))
+
+
+def cpotrf_batched(a, upper=False, threads=0):
+    """In-place complex Cholesky of each (n, n) matrix; returns (factors, info)."""
+    flat, shape = _cslab(a)
+    count, n = shape[0], shape[1]
+    info = np.zeros(count, dtype=np.int32)
+    lib().orc_cpotrf_batched(n, flat, n, n * n, count, int(upper), info, threads)
+    return _uncslab(flat, shape), info
+
+
+def cpotrs_batched(factors, b, upper=False, threads=0):
+    """Solve with complex Cholesky factors; b (count, n, nrhs)."""
+    fa, fshape = _cslab(factors)
+    fb, bshape = _cslab(b)
+    count, n, nrhs = fshape[0], fshape[1], bshape[1]
+    lib().orc_cpotrs_batched(n, nrhs, fa, n, n * n, fb, n, n * nrhs, count, int(upper), threads)
+    return _uncslab(fb, bshape)

@@ -133,3 +133,36 @@ def forward_error(a, x, b):
     """||x - x64||_inf / ||x64||_inf against an FP64 LAPACK solve."""
     x64 = la.solve(np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64))
     return float(np.abs(np.asarray(x, dtype=np.float64) - x64).max() / np.abs(x64).max())
+
+
+def complex_ratio(op, a, out, upper=False, b=None):
+    """The complex128 residual ratio of test/utils/cholesky/fixtures.py:446-484 (lapack_ratio)
+    for one matrix: ||L L^H - A||_1 / (n ||A||_1 eps) or max_j ||b - A x||_1 / (||A||_1 ||x||_1 eps)."""
+    a = np.asarray(a, dtype=np.complex128)
+    out = np.asarray(out, dtype=np.complex128)
+    n = a.shape[-1]
+    norm1 = lambda m: np.max(np.sum(np.abs(m), axis=-2), axis=-1)
+    if op == "potrs":
+        num = np.sum(np.abs(np.asarray(b, dtype=np.complex128) - a @ out), axis=-2)
+        den = norm1(a) * np.sum(np.abs(out), axis=-2) * EPS
+        r = np.divide(num, den, out=np.full_like(num, np.inf), where=den != 0)
+        return float(np.max(r))
+    tri = np.triu(out) if upper else np.tril(out)
+    adj = tri.conj().T
+    d = np.diagonal(tri)
+    if np.any(~np.isfinite(d) | (d.real <= 0) | (d.imag != 0)):
+        return float("inf")
+    rec = adj @ tri if upper else tri @ adj
+    return float(norm1(rec - a) / (n * norm1(a) * EPS))
+
+
+def complex_cpu_ratio(op, a, upper=False, b=None):
+    """The same ratio for scipy's complex64 LAPACK (the reference's CPU golden)."""
+    from scipy.linalg.lapack import cpotrf, cpotrs
+
+    f, info = cpotrf(np.array(a, dtype=np.complex64, order="F"), lower=not upper)
+    assert info == 0
+    if op == "potrf":
+        return complex_ratio(op, a, f, upper)
+    x, info = cpotrs(f, np.array(b, dtype=np.complex64, order="F"), lower=not upper)
+    return complex_ratio(op, a, x, upper, b)

@@ -20,6 +20,7 @@
  *   orc_spotrf_fma      right-looking Cholesky with FMA updates in ascending k (n > 32)
  *   orc_spotrs_right    right-looking Cholesky solve (n > 128)
  *   orc_sgetrs          column-oriented LU solve (math of test/utils/lu_verify_utils.py:67-192)
+ *   orc_cpotrf/cpotrs   complex64 Cholesky factor and solve, FMA order (see their comment)
  *
  * Compiled with -ffp-contract=off: every fused multiply-add is an explicit fmaf().
  */
@@ -425,6 +426,147 @@ void orc_sgetrs(int trans, int n, int nrhs, const float *lu, int lda, const int 
 }
 
 /* ---------------------------------------------------------------------------------------
+ * Complex64 Cholesky (this build's order; the reference keeps a compensated double-float
+ * first column and diagonal, src/cpotrf/arch35/cholesky_factor.cpp:17-215, and uses a
+ * CATLASS complex GEMM for n > 64, so the CUDA kernels and this restatement share the order
+ * below and parity with the reference is by tolerance).  Interleaved (re, im) floats.
+ * ------------------------------------------------------------------------------------- */
+
+/* Element (i, j), j <= i, of the lower factor; upper storage holds the conjugate mirror. */
+static inline void ctri_get(const float *a, int lda, int upper, int i, int j, float *re, float *im)
+{
+    if (upper)
+    {
+        const float *p = a + 2 * ((int64_t)i * lda + j);
+        *re = p[0];
+        *im = -p[1];
+    }
+    else
+    {
+        const float *p = a + 2 * ((int64_t)j * lda + i);
+        *re = p[0];
+        *im = p[1];
+    }
+}
+static inline void ctri_set(float *a, int lda, int upper, int i, int j, float re, float im)
+{
+    if (upper)
+    {
+        float *p = a + 2 * ((int64_t)i * lda + j);
+        p[0] = re;
+        p[1] = -im;
+    }
+    else
+    {
+        float *p = a + 2 * ((int64_t)j * lda + i);
+        p[0] = re;
+        p[1] = im;
+    }
+}
+
+/* Right-looking: d = Re(a_kk) (d > 0 and finite), s = sqrtf(d), l_kk = (s, 0),
+ * l_ik = a_ik / s per component; a_ij -= l_ik conj(l_jk) as
+ * re = fmaf(-ar, cr, re); re = fmaf(-ai, ci, re); im = fmaf(-ai, cr, im); im = fmaf(ar, ci, im). */
+int orc_cpotrf(int n, float *a, int lda, int upper)
+{
+    float *w = (float *)malloc(sizeof(float) * 2 * (size_t)n * (size_t)n + 8);
+    for (int j = 0; j < n; ++j)
+        for (int i = j; i < n; ++i) ctri_get(a, lda, upper, i, j, &w[2 * ((size_t)j * n + i)], &w[2 * ((size_t)j * n + i) + 1]);
+    int failure = 0;
+    for (int k = 0; k < n; ++k)
+    {
+        float d = w[2 * ((size_t)k * n + k)];
+        if (!(d > 0.0f && d <= FLT_MAX_VALUE))
+        {
+            failure = k + 1;
+            break;
+        }
+        float s = sqrtf(d);
+        w[2 * ((size_t)k * n + k)] = s;
+        w[2 * ((size_t)k * n + k) + 1] = 0.0f;
+        for (int i = k + 1; i < n; ++i)
+        {
+            float *v = &w[2 * ((size_t)k * n + i)];
+            v[0] = v[0] / s;
+            v[1] = v[1] / s;
+        }
+        for (int j = k + 1; j < n; ++j)
+        {
+            float cr = w[2 * ((size_t)k * n + j)], ci = w[2 * ((size_t)k * n + j) + 1];
+            for (int i = j; i < n; ++i)
+            {
+                float ar = w[2 * ((size_t)k * n + i)], ai = w[2 * ((size_t)k * n + i) + 1];
+                float *z = &w[2 * ((size_t)j * n + i)];
+                float re = z[0], im = z[1];
+                re = fmaf(-ar, cr, re);
+                re = fmaf(-ai, ci, re);
+                im = fmaf(-ai, cr, im);
+                im = fmaf(ar, ci, im);
+                z[0] = re;
+                z[1] = im;
+            }
+        }
+    }
+    int done = failure ? failure - 1 : n;
+    for (int j = 0; j < done; ++j)
+        for (int i = j; i < n; ++i) ctri_set(a, lda, upper, i, j, w[2 * ((size_t)j * n + i)], w[2 * ((size_t)j * n + i) + 1]);
+    free(w);
+    return failure;
+}
+
+/* Right-looking sweeps: y_k = z_k / l_kk, z_i -= l_ik y_k (i > k); then x_k = z_k / l_kk,
+ * z_i -= conj(l_ki) x_k (i < k, k descending); z -= l y as re = fmaf(-lr, yr, re);
+ * re = fmaf(li, yi, re); im = fmaf(-lr, yi, im); im = fmaf(-li, yr, im). */
+void orc_cpotrs(int n, int nrhs, const float *a, int lda, float *b, int ldb, int upper)
+{
+    for (int r = 0; r < nrhs; ++r)
+    {
+        float *x = b + 2 * (int64_t)r * ldb;
+        for (int k = 0; k < n; ++k)
+        {
+            float dr, di;
+            ctri_get(a, lda, upper, k, k, &dr, &di);
+            float yr = x[2 * k] / dr, yi = x[2 * k + 1] / dr;
+            for (int i = k + 1; i < n; ++i)
+            {
+                float lr, li;
+                ctri_get(a, lda, upper, i, k, &lr, &li);
+                float re = x[2 * i], im = x[2 * i + 1];
+                re = fmaf(-lr, yr, re);
+                re = fmaf(li, yi, re);
+                im = fmaf(-lr, yi, im);
+                im = fmaf(-li, yr, im);
+                x[2 * i] = re;
+                x[2 * i + 1] = im;
+            }
+            x[2 * k] = yr;
+            x[2 * k + 1] = yi;
+        }
+        for (int k = n - 1; k >= 0; --k)
+        {
+            float dr, di;
+            ctri_get(a, lda, upper, k, k, &dr, &di);
+            float yr = x[2 * k] / dr, yi = x[2 * k + 1] / dr;
+            for (int i = 0; i < k; ++i)
+            {
+                float lr, li;
+                ctri_get(a, lda, upper, k, i, &lr, &li);
+                li = -li; /* conj(l_ki) */
+                float re = x[2 * i], im = x[2 * i + 1];
+                re = fmaf(-lr, yr, re);
+                re = fmaf(li, yi, re);
+                im = fmaf(-lr, yi, im);
+                im = fmaf(-li, yr, im);
+                x[2 * i] = re;
+                x[2 * i + 1] = im;
+            }
+            x[2 * k] = yr;
+            x[2 * k + 1] = yi;
+        }
+    }
+}
+
+/* ---------------------------------------------------------------------------------------
  * Batched drivers over a contiguous slab (matrix b at base + b*stride), OpenMP over
  * matrices; `threads` <= 0 uses the OpenMP default.  These are what the CPU baseline times.
  * ------------------------------------------------------------------------------------- */
@@ -491,4 +633,21 @@ void orc_sgetri_batched(int n, const float *lu, int lda, int64_t astride, const 
     for (int q = 0; q < count; ++q)
         info[q] = orc_sgetri_vector(n, lu + (int64_t)q * astride, lda, ipiv ? ipiv + (int64_t)q * n : NULL,
                                     c + (int64_t)q * cstride, ldc);
+}
+
+/* Complex batches: matrix q at a + 2*q*astride floats (astride in complex elements). */
+void orc_cpotrf_batched(int n, float *a, int lda, int64_t stride, int count, int upper, int *info, int threads)
+{
+    set_threads(threads);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int q = 0; q < count; ++q) info[q] = orc_cpotrf(n, a + 2 * (int64_t)q * stride, lda, upper);
+}
+
+void orc_cpotrs_batched(int n, int nrhs, const float *a, int lda, int64_t astride, float *b, int ldb,
+                        int64_t bstride, int count, int upper, int threads)
+{
+    set_threads(threads);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int q = 0; q < count; ++q)
+        orc_cpotrs(n, nrhs, a + 2 * (int64_t)q * astride, lda, b + 2 * (int64_t)q * bstride, ldb, upper);
 }

@@ -375,7 +375,7 @@ def test_smatinv_known_answer(handle):
     handle.stream.synchronize()
     assert st == aclsolver.SUCCESS and info.cpu().tolist() == [0, 0]
     for q in range(2):
-        np.testing.assert_array_equal(dc.read()[q], np.asarray(case["inverse"][q]).reshape(2, 2))
+        np.testing.assert_array_equal(dc.read()[q], np.asarray(case["inverse"][q], dtype=np.float32).reshape(2, 2))
 
 
 def test_smatinv_rejects_order_above_32(handle):
