@@ -61,6 +61,35 @@ extern "C"
                                                      aclsolverFloatComplex *Barray[], int ldb, int *info,
                                                      int batchSize);
 
+    /* Uneven-order batches: factor A_b = L_b L_b^H (or U^H U) and solve A_b X_b = B_b for
+     * matrices of different orders in one persistent launch captured in a CUDA graph.  The
+     * reference factors one uniform order per call (aclsolverCpotrfBatched,
+     * include/cann_ops_solver.h:224) and solves one right-hand side per call
+     * (aclsolverCpotrsBatched, :244), so an uneven batch takes it one pair of calls per
+     * distinct order and right-hand side.
+     *
+     * Create: nArray, ldaArray, ldbArray are HOST arrays of batchSize entries (0 <= n <= 160,
+     * lda, ldb >= max(1, n)); 0 <= nrhs <= 128.  The plan sorts the matrices by order into
+     * size buckets, and with autotune = 1 times candidate launch shapes (warp-path cutoff,
+     * threads per matrix, persistent blocks per SM) on scratch matrices of the same orders,
+     * keeping the fastest; choices are cached in the file named by OPS_SOLVER_TUNE_CACHE
+     * (default $HOME/.cache/ops_solver_b200_vbatched_tune.txt).
+     * Execute: Aarray / Barray are device tables of device matrix pointers; infoArray
+     * (device, batchSize entries) receives each matrix's factor info (first non-positive
+     * pivot, or -3 for a null slot); a failed matrix keeps its completed columns and its B
+     * is left unsolved.  Asynchronous on the handle stream; the graph is instantiated on
+     * the first execution with a given set of tables and replayed afterwards.
+     * Argument errors return INVALID_VALUE (no device write at plan creation). */
+    typedef struct aclsolverVbatchedPlan_st *aclsolverVbatchedPlan_t;
+    aclsolverStatus_t aclsolverCposvVbatchedPlanCreate(aclsolverHandle_t handle, aclsolverFillMode_t uplo,
+                                                       const int *nArray, const int *ldaArray, const int *ldbArray,
+                                                       int nrhs, int batchSize, int autotune,
+                                                       aclsolverVbatchedPlan_t *plan);
+    aclsolverStatus_t aclsolverCposvVbatched(aclsolverHandle_t handle, aclsolverVbatchedPlan_t plan,
+                                             aclsolverFloatComplex *const Aarray[], aclsolverFloatComplex *const Barray[],
+                                             int *infoArray);
+    aclsolverStatus_t aclsolverVbatchedPlanDestroy(aclsolverVbatchedPlan_t plan);
+
 #ifdef __cplusplus
 }
 #endif

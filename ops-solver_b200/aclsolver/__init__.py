@@ -71,6 +71,9 @@ ARGTYPES = {
     "aclsolverSgetrfBatched": [VP, I32, VP, I32, VP, VP, I32],
     "aclsolverSgetrsBatched": [VP, I32, I32, I32, VP, I32, VP, VP, I32, VP, I32],
     "aclsolverCpotrsBatchedMultiRhs": [VP, I32, I32, I32, VP, I32, VP, I32, VP, I32],
+    "aclsolverCposvVbatchedPlanCreate": [VP, I32, VP, VP, VP, I32, I32, I32, C.POINTER(VP)],
+    "aclsolverCposvVbatched": [VP, VP, VP, VP, VP],
+    "aclsolverVbatchedPlanDestroy": [VP],
 }
 
 

@@ -16,6 +16,7 @@
 #include "handle.h"
 #include "launch.h"
 #include "launch_complex.h"
+#include "vbatched.h"
 
 using namespace ops_solver;
 
@@ -174,5 +175,50 @@ extern "C"
                                                      int batchSize)
     {
         return batched_solve(handle, uplo, n, nrhs, Aarray, lda, Barray, ldb, info, batchSize, false);
+    }
+
+    aclsolverStatus_t aclsolverCposvVbatchedPlanCreate(aclsolverHandle_t handle, aclsolverFillMode_t uplo,
+                                                       const int *nArray, const int *ldaArray, const int *ldbArray,
+                                                       int nrhs, int batchSize, int autotune,
+                                                       aclsolverVbatchedPlan_t *plan)
+    {
+        if (!handle) return ACLSOLVER_STATUS_NOT_INITIALIZED;
+        if (!plan || !valid_uplo(uplo) || nrhs < 0 || nrhs > MAX_RHS || batchSize < 0 || batchSize > MAX_BATCH ||
+            (batchSize > 0 && (!nArray || !ldaArray || !ldbArray)) || (autotune != 0 && autotune != 1))
+            return ACLSOLVER_STATUS_INVALID_VALUE;
+        for (int q = 0; q < batchSize; ++q)
+        {
+            const int n = nArray[q];
+            if (n < 0 || n > 160 || ldaArray[q] < (n > 0 ? n : 1) || ldbArray[q] < (n > 0 ? n : 1))
+                return ACLSOLVER_STATUS_INVALID_VALUE;
+        }
+        VbPlan *p = nullptr;
+        aclsolverStatus_t st =
+            vb_plan_create(to_handle(handle), uplo, nArray, ldaArray, ldbArray, nrhs, batchSize, autotune, &p);
+        if (st != ACLSOLVER_STATUS_SUCCESS) return st;
+        *plan = reinterpret_cast<aclsolverVbatchedPlan_t>(p);
+        return ACLSOLVER_STATUS_SUCCESS;
+    }
+
+    aclsolverStatus_t aclsolverCposvVbatched(aclsolverHandle_t handle, aclsolverVbatchedPlan_t plan,
+                                             aclsolverFloatComplex *const Aarray[], aclsolverFloatComplex *const Barray[],
+                                             int *infoArray)
+    {
+        if (!handle) return ACLSOLVER_STATUS_NOT_INITIALIZED;
+        VbPlan *p = reinterpret_cast<VbPlan *>(plan);
+        if (!p) return ACLSOLVER_STATUS_INVALID_VALUE;
+        if (p->count == 0) return ACLSOLVER_STATUS_SUCCESS;
+        if (!Aarray || !infoArray || (p->nrhs > 0 && !Barray)) return ACLSOLVER_STATUS_INVALID_VALUE;
+        aclsolverStatus_t span = info_span(infoArray, p->count);
+        if (span != ACLSOLVER_STATUS_SUCCESS) return span;
+        return vb_plan_execute(p, reinterpret_cast<float2 *const *>(Aarray), reinterpret_cast<float2 *const *>(Barray),
+                               infoArray, to_handle(handle)->stream);
+    }
+
+    aclsolverStatus_t aclsolverVbatchedPlanDestroy(aclsolverVbatchedPlan_t plan)
+    {
+        if (!plan) return ACLSOLVER_STATUS_INVALID_VALUE;
+        vb_plan_destroy(reinterpret_cast<VbPlan *>(plan));
+        return ACLSOLVER_STATUS_SUCCESS;
     }
 }

@@ -13,9 +13,10 @@
 // column and diagonal and hand n > 64 to a CATLASS complex GEMM, so parity with them is
 // held to the 1e-5 relative tolerance and the reference's complex128 residual gate.
 //
-// Layouts: n <= 32 -- a width-N sub-warp per matrix, lane i holds row i (re[], im[]) and the
-// finished column is broadcast through shared memory; 33..128 -- one block per matrix,
-// the lower triangle staged in shared memory column-major, thread i owns row i.
+// Layouts: n <= 16 -- a width-N sub-warp per matrix, lane i holds row i (re[], im[]) and the
+// finished column is broadcast through shared memory; 17..128 -- one block per matrix,
+// the lower triangle staged in shared memory column-major, threads stride over the rows.
+// (A 32-lane register version needs more than 255 registers per lane for the complex rows.)
 #include "common.cuh"
 #include "launch_complex.h"
 
@@ -65,6 +66,46 @@ __device__ __forceinline__ void store_tri(float2 *p, int lda, int upper, int i, 
 // ---------------------------------------------------------------------------------------
 // n <= N <= 32: sub-warp per matrix
 // ---------------------------------------------------------------------------------------
+// Column K of the right-looking factor, then column K + 1; the recursion keeps every
+// register index a compile-time constant.
+template <int N, int K>
+__device__ __forceinline__ void cfactor_step(float (&re)[N], float (&im)[N], int n, int row, float2 *col,
+                                             int &failure)
+{
+    if constexpr (K < N)
+    {
+        if (K < n)
+        {
+            const float d = __shfl_sync(0xffffffffu, re[K], K, N);
+            if (!(d > 0.0f && d <= FLT_MAX_VALUE) && failure == 0) failure = K + 1;
+            const float s = sqrt_rn(d);
+            if (row == K)
+            {
+                re[K] = s;
+                im[K] = 0.0f;
+            }
+            else
+            {
+                re[K] = div_rn(re[K], s);
+                im[K] = div_rn(im[K], s);
+            }
+            __syncwarp();
+            col[row] = make_float2(re[K], im[K]);
+            __syncwarp();
+#pragma unroll
+            for (int j = K + 1; j < N; ++j)
+            {
+                if (j < n)
+                {
+                    const float2 c = col[j];
+                    sub_lconj(re[j], im[j], re[K], im[K], c.x, c.y);
+                }
+            }
+            cfactor_step<N, K + 1>(re, im, n, row, col, failure);
+        }
+    }
+}
+
 template <int N>
 __device__ __forceinline__ void cpotrf_warp_matrix(float2 *p, int n, int lda, int upper, int row, float2 *col,
                                                    int &failure)
@@ -78,38 +119,7 @@ __device__ __forceinline__ void cpotrf_warp_matrix(float2 *p, int n, int lda, in
         re[j] = v.x;
         im[j] = v.y;
     }
-#pragma unroll
-    for (int k = 0; k < N; ++k)
-    {
-        if (k < n)
-        {
-            const float d = __shfl_sync(0xffffffffu, re[k], k, N);
-            if (!(d > 0.0f && d <= FLT_MAX_VALUE) && failure == 0) failure = k + 1;
-            const float s = sqrt_rn(d);
-            if (row == k)
-            {
-                re[k] = s;
-                im[k] = 0.0f;
-            }
-            else
-            {
-                re[k] = div_rn(re[k], s);
-                im[k] = div_rn(im[k], s);
-            }
-            __syncwarp();
-            col[row] = make_float2(re[k], im[k]);
-            __syncwarp();
-#pragma unroll
-            for (int j = k + 1; j < N; ++j)
-            {
-                if (j < n)
-                {
-                    const float2 c = col[j];
-                    sub_lconj(re[j], im[j], re[k], im[k], c.x, c.y);
-                }
-            }
-        }
-    }
+    cfactor_step<N, 0>(re, im, n, row, col, failure);
     if (p)
     {
         const int done = failure ? failure - 1 : n;
@@ -357,9 +367,6 @@ cudaError_t launch_cpotrf(float2 *single, float2 *const *table, int n, int lda, 
                                                                                        count, info);
     else if (n <= 16)
         cpotrf_warp_kernel<16><<<grid_of(count, 8, 148 * 64), CW_THREADS, 0, stream>>>(single, table, n, lda, upper,
-                                                                                       count, info);
-    else if (n <= 32)
-        cpotrf_warp_kernel<32><<<grid_of(count, 4, 148 * 64), CW_THREADS, 0, stream>>>(single, table, n, lda, upper,
                                                                                        count, info);
     else if (n <= 128)
     {
