@@ -48,12 +48,12 @@ class Uneven:
     def factor(self, q):
         n = self.orders[q]
         raw = self.da[q].cpu().numpy().view(np.complex64).reshape(max(n, 1), self.lda[q])
-        return raw[:n, :n].T
+        return np.ascontiguousarray(raw[:n, :n].T)
 
     def solution(self, q):
         n = self.orders[q]
         raw = self.db[q].cpu().numpy().view(np.complex64).reshape(max(self.nrhs, 1), self.ldb[q])
-        return raw[: self.nrhs, :n].T
+        return np.ascontiguousarray(raw[: self.nrhs, :n].T)
 
 
 def plan(handle, u, autotune=1, uplo=0):
@@ -87,8 +87,8 @@ def test_uneven_batch_matches_oracle(handle, seed, tmp_path, monkeypatch):
         f, _ = oracle.cpotrf_batched(u.a[q][None])
         x = oracle.cpotrs_batched(f, u.b[q][None])
         got_f = u.factor(q)
-        assert same_bits(np.tril(got_f).view(np.float32), np.tril(f[0]).view(np.float32)), (q, n)
-        assert same_bits(u.solution(q).view(np.float32), x[0].view(np.float32)), (q, n)
+        assert same_bits(np.ascontiguousarray(np.tril(got_f)).view(np.float32), np.ascontiguousarray(np.tril(f[0])).view(np.float32)), (q, n)
+        assert same_bits(u.solution(q).view(np.float32), np.ascontiguousarray(x[0]).view(np.float32)), (q, n)
     for q in range(0, len(orders), 37):
         if orders[q]:
             r = judges.complex_ratio("potrs", u.a[q], u.solution(q), False, u.b[q])
