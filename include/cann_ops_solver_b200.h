@@ -90,6 +90,22 @@ extern "C"
                                              int *infoArray);
     aclsolverStatus_t aclsolverVbatchedPlanDestroy(aclsolverVbatchedPlan_t plan);
 
+    /* aclsolverSmatinvBatched for callers that cannot let the library allocate device memory
+     * (hosts that hand out all device memory from their own pool and forbid allocations after
+     * start-up, and latency-critical loops where an allocation's implicit device
+     * synchronisation is not acceptable).  No counterpart in the reference: there the call
+     * takes its pivot scratch from the handle, which allocates it.  This variant keeps the
+     * LU pivots in an array compiled into the library (2^20 ints, 4 MiB, held by every GPU
+     * that loads the library until the process exits) and calls no allocator; n * batchSize
+     * above 2^20 is rejected with INVALID_VALUE and info = -7 (split the batch).  Same
+     * arguments, arithmetic, info and argument-error rules as aclsolverSmatinvBatched, except
+     * that the synchronous device-data checks (finite scan, pointer-table validation) are not
+     * run, since they need staging buffers.  The first call on each device resolves the
+     * array's device address and should come before any stream capture.  All calls share the
+     * array: calls whose executions overlap on the GPU race on it and must be serialised. */
+    aclsolverStatus_t aclsolverSmatinvBatchedNoAlloc(aclsolverHandle_t handle, int n, const float *const A[], int lda,
+                                                     float *const Ainv[], int lda_inv, int *info, int batchSize);
+
 #ifdef __cplusplus
 }
 #endif

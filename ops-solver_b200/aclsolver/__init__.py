@@ -74,6 +74,7 @@ ARGTYPES = {
     "aclsolverCposvVbatchedPlanCreate": [VP, I32, VP, VP, VP, I32, I32, I32, C.POINTER(VP)],
     "aclsolverCposvVbatched": [VP, VP, VP, VP, VP],
     "aclsolverVbatchedPlanDestroy": [VP],
+    "aclsolverSmatinvBatchedNoAlloc": [VP, I32, VP, I32, VP, I32, VP, I32],
 }
 
 
