@@ -318,8 +318,9 @@ extern "C"
             aclsolverStatus_t st = check_finite(h, a, m, devInfo, 1, 3);
             if (st != ACLSOLVER_STATUS_SUCCESS) return st;
         }
-        if (m > SMALL_N || n > SMALL_N) return ACLSOLVER_STATUS_NOT_SUPPORTED;
-        return launch_status(launch_getrf_small(a, m, devIpiv, devInfo, h->stream));
+        if (m <= SMALL_N && n <= SMALL_N) return launch_status(launch_getrf_small(a, m, devIpiv, devInfo, h->stream));
+        if (m == n && n <= BLOCKED_MAX_N) return launch_status(launch_getrf_blocked(a, devIpiv, devInfo, 0, h->stream));
+        return ACLSOLVER_STATUS_NOT_SUPPORTED;
     }
 
     aclsolverStatus_t aclsolverSgetri_bufferSize(aclsolverHandle_t handle, int n, float *A, int lda, int *Lwork)
@@ -448,9 +449,11 @@ extern "C"
         if (arg) return invalid(h, infoArray, batchSize < 0 ? 1 : batchSize, arg);
         if (batchSize == 0) return ACLSOLVER_STATUS_SUCCESS;
         if (n == 0) return launch_status(launch_fill_info(infoArray, 0, batchSize, h->stream));
-        if (n > SMALL_N) return ACLSOLVER_STATUS_NOT_SUPPORTED;
         RealBatch a{nullptr, Aarray, n, lda, 0, batchSize};
-        return launch_status(launch_getrf_small(a, n, PivotArray, infoArray, h->stream));
+        if (n <= SMALL_N) return launch_status(launch_getrf_small(a, n, PivotArray, infoArray, h->stream));
+        if (n <= BLOCKED_MAX_N)
+            return launch_status(launch_getrf_blocked(a, PivotArray, infoArray, 0, h->stream));
+        return ACLSOLVER_STATUS_NOT_SUPPORTED;
     }
 
     aclsolverStatus_t aclsolverSgetrsBatched(aclsolverHandle_t handle, aclsolverOperation_t trans, int n, int nrhs,
@@ -482,11 +485,14 @@ extern "C"
         if (arg) return invalid(h, infoArray, batchSize < 0 ? 1 : batchSize, arg);
         if (batchSize == 0) return ACLSOLVER_STATUS_SUCCESS;
         if (!used) return launch_status(launch_fill_info(infoArray, 0, batchSize, h->stream));
-        if (n > SMALL_N) return ACLSOLVER_STATUS_NOT_SUPPORTED;
         RealBatch a{nullptr, const_cast<float *const *>(Aarray), n, lda, 0, batchSize};
         RealBatch b{nullptr, Barray, n, ldb, 0, batchSize};
-        return launch_status(launch_getrs_small(a, PivotArray, b, nrhs, trans == ACLSOLVER_OP_T ? 1 : 0, infoArray,
-                                                h->stream));
+        if (n <= SMALL_N)
+            return launch_status(launch_getrs_small(a, PivotArray, b, nrhs, trans == ACLSOLVER_OP_T ? 1 : 0,
+                                                    infoArray, h->stream));
+        if (trans == ACLSOLVER_OP_N)
+            return launch_status(launch_getrs_blocked(a, PivotArray, b, nrhs, infoArray, nullptr, h->stream));
+        return ACLSOLVER_STATUS_NOT_SUPPORTED;
     }
 
     aclError aclsolverSgetrs(aclsolverHandle_t handle, const uint64_t trans, const int64_t n, const int64_t nrhs,
@@ -510,7 +516,7 @@ extern "C"
                 return ACL_ERROR_INVALID_PARAM;
             }
         cudaStream_t stream = handle ? to_handle(handle)->stream : nullptr;
-        if (n > SMALL_N) return (aclError)ACLSOLVER_STATUS_NOT_SUPPORTED;
+        if (n > SMALL_N && trans != 0) return (aclError)ACLSOLVER_STATUS_NOT_SUPPORTED;
         // Stage: row-major host A (lda) -> device raw -> column-major LU (n x n, ld n);
         // row-major host B (ldb) -> device raw -> column-major (n x nrhs, ld n).
         const size_t a_raw = (size_t)n * lda * sizeof(float), b_raw = (size_t)n * ldb * sizeof(float);
@@ -545,7 +551,8 @@ extern "C"
         {
             RealBatch a{d_a, nullptr, (int)n, (int)n, 0, 1};
             RealBatch b{d_b, nullptr, (int)n, (int)n, 0, 1};
-            e = launch_getrs_small(a, d_p, b, (int)nrhs, (int)trans, nullptr, stream);
+            e = n <= SMALL_N ? launch_getrs_small(a, d_p, b, (int)nrhs, (int)trans, nullptr, stream)
+                             : launch_getrs_blocked(a, d_p, b, (int)nrhs, nullptr, nullptr, stream);
         }
         if (e == cudaSuccess) e = launch_transpose(d_b, (int)n, d_braw, (int)ldb, (int)n, (int)nrhs, stream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(B, d_braw, b_raw, cudaMemcpyDeviceToHost, stream);

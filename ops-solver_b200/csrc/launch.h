@@ -51,11 +51,24 @@ cudaError_t launch_getrs_small(const RealBatch &a, const int *ipiv, const RealBa
 cudaError_t launch_getri_small(const RealBatch &a, const int *ipiv, const RealBatch &c, int *info,
                                cudaStream_t stream);
 
+// Blocked LU for 64 < n <= 512 (square), one 256-thread block per matrix.  mode 0: plain
+// FP32, bit-identical to the unblocked order; 1: BF16 tensor-core trailing update; 3: split
+// BF16 (three products).  ipiv n per matrix or nullptr; info as launch_getrf_small.
+constexpr int BLOCKED_MAX_N = 512;
+cudaError_t launch_getrf_blocked(const RealBatch &a, int *ipiv, int *info, int mode, cudaStream_t stream);
+// Blocked LU solve (trans 0) for 64 < n <= 8192.  `skip` (nullptr = none): per (matrix,
+// right-hand side) states; a group of right-hand sides whose states are all nonzero is
+// skipped (iterative refinement).  info may be null.
+cudaError_t launch_getrs_blocked(const RealBatch &a, const int *ipiv, const RealBatch &b, int nrhs, int *info,
+                                 const int *skip, cudaStream_t stream);
+
 // ---- validation and staging ------------------------------------------------------------
 // flag[0] |= 1 when any of the m x n leading entries of any matrix is NaN or infinite.
 cudaError_t launch_finite_scan(const RealBatch &a, int m, int *flag, cudaStream_t stream);
 // dst[i + j*ldd] = src[i + j*lds] for each matrix (copy of the leading m x n block).
 cudaError_t launch_copy_matrices(const RealBatch &src, const RealBatch &dst, int m, cudaStream_t stream);
+// table[q] = base + q * stride (floats), q < count.
+cudaError_t launch_strided_table(float **table, float *base, int64_t stride, int count, cudaStream_t stream);
 // dst (column-major, ldd) = transpose of src (column-major, lds), src rows x cols.
 cudaError_t launch_transpose(const float *src, int lds, float *dst, int ldd, int rows, int cols,
                              cudaStream_t stream);

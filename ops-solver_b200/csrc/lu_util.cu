@@ -67,7 +67,21 @@ __global__ void transpose_kernel(const float *src, int lds, float *dst, int ldd,
         if (i < cols && j < rows) dst[i + (int64_t)j * ldd] = tile[threadIdx.x][r];
     }
 }
+__global__ void strided_table_kernel(float **table, float *base, int64_t stride, int count)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x)
+        table[q] = base + (int64_t)q * stride;
+}
 }  // namespace
+
+cudaError_t launch_strided_table(float **table, float *base, int64_t stride, int count, cudaStream_t stream)
+{
+    int blocks = (count + 255) / 256;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks < 1) blocks = 1;
+    strided_table_kernel<<<blocks, 256, 0, stream>>>(table, base, stride, count);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_finite_scan(const RealBatch &a, int m, int *flag, cudaStream_t stream)
 {
