@@ -106,6 +106,38 @@ extern "C"
     aclsolverStatus_t aclsolverSmatinvBatchedNoAlloc(aclsolverHandle_t handle, int n, const float *const A[], int lda,
                                                      float *const Ainv[], int lda_inv, int *info, int batchSize);
 
+    /* Precision of the LU factorisation behind aclsolverSgesvIrBatched. */
+    typedef enum
+    {
+        ACLSOLVER_FACTOR_FP32 = 0,   /* plain FP32: the factors of aclsolverSgetrfBatched, bit for bit */
+        ACLSOLVER_FACTOR_BF16 = 1,   /* trailing update on the BF16 tensor cores, FP32 accumulation */
+        ACLSOLVER_FACTOR_BF16X3 = 3, /* split BF16 (a = hi + lo): hi*hi + hi*lo + lo*hi on the tensor
+                                        cores, FP32 accumulation, about FP32-level factors */
+    } aclsolverFactorPrecision_t;
+
+    /* Solve A_b X_b = B_b by an LU factorisation of the chosen precision plus iterative
+     * refinement whose residual r = B - A X and solution update run in FP64.  The reference
+     * solves with aclsolverSgetrf (include/cann_ops_solver.h:101) then aclsolverSgetrs
+     * (:1011), FP32 throughout and one matrix per call; this entry batches the pair and adds
+     * the refinement.  A (lda) and B (ldb) are read only; X (ldx) receives the FP32 solution
+     * and may be the same buffers as B.  Column-major, device pointer tables.
+     * Per right-hand side the loop stops when the normwise backward error
+     * berr = max|r| / (||A||_inf max|x| + max|b|) reaches tol, when it stops halving (the
+     * better of the last two iterates is kept) or after maxIter corrections.
+     * iterArray (device, may be NULL): corrections kept per matrix (maximum over its
+     * right-hand sides).  berrArray (device doubles, may be NULL): final berr per matrix
+     * (maximum over its right-hand sides; NaN when the factorisation failed).
+     * infoArray (device): the factorisation's info (first zero U(k,k), -2 for a null slot); a
+     * matrix with info != 0 is not solved and its X is left unchanged.
+     * 0 <= n <= 512, 0 <= nrhs, 0 <= maxIter, tol >= 0.  Argument errors: INVALID_VALUE,
+     * infoArray filled with -i (precision is argument 1).  Asynchronous on the handle stream;
+     * workspace comes from the handle (about 4 n^2 + 12 n nrhs bytes per matrix). */
+    aclsolverStatus_t aclsolverSgesvIrBatched(aclsolverHandle_t handle, aclsolverFactorPrecision_t precision, int n,
+                                              int nrhs, const float *const Aarray[], int lda,
+                                              const float *const Barray[], int ldb, float *const Xarray[], int ldx,
+                                              int maxIter, double tol, int *iterArray, double *berrArray,
+                                              int *infoArray, int batchSize);
+
 #ifdef __cplusplus
 }
 #endif

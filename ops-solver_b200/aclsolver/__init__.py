@@ -36,6 +36,9 @@ LOWER = 0
 UPPER = 1
 OP_N = 0
 OP_T = 1
+FACTOR_FP32 = 0
+FACTOR_BF16 = 1
+FACTOR_BF16X3 = 3
 
 _QUERY = [VP, I32, I32, VP, I32, C.POINTER(I32)]
 ARGTYPES = {
@@ -75,6 +78,7 @@ ARGTYPES = {
     "aclsolverCposvVbatched": [VP, VP, VP, VP, VP],
     "aclsolverVbatchedPlanDestroy": [VP],
     "aclsolverSmatinvBatchedNoAlloc": [VP, I32, VP, I32, VP, I32, VP, I32],
+    "aclsolverSgesvIrBatched": [VP, I32, I32, I32, VP, I32, VP, I32, VP, I32, I32, C.c_double, VP, VP, VP, I32],
 }
 
 

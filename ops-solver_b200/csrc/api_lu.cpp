@@ -491,7 +491,7 @@ extern "C"
             return launch_status(launch_getrs_small(a, PivotArray, b, nrhs, trans == ACLSOLVER_OP_T ? 1 : 0,
                                                     infoArray, h->stream));
         if (trans == ACLSOLVER_OP_N)
-            return launch_status(launch_getrs_blocked(a, PivotArray, b, nrhs, infoArray, nullptr, h->stream));
+            return launch_status(launch_getrs_blocked(a, PivotArray, nullptr, b, nrhs, infoArray, nullptr, h->stream));
         return ACLSOLVER_STATUS_NOT_SUPPORTED;
     }
 
@@ -552,7 +552,7 @@ extern "C"
             RealBatch a{d_a, nullptr, (int)n, (int)n, 0, 1};
             RealBatch b{d_b, nullptr, (int)n, (int)n, 0, 1};
             e = n <= SMALL_N ? launch_getrs_small(a, d_p, b, (int)nrhs, (int)trans, nullptr, stream)
-                             : launch_getrs_blocked(a, d_p, b, (int)nrhs, nullptr, nullptr, stream);
+                             : launch_getrs_blocked(a, d_p, nullptr, b, (int)nrhs, nullptr, nullptr, stream);
         }
         if (e == cudaSuccess) e = launch_transpose(d_b, (int)n, d_braw, (int)ldb, (int)n, (int)nrhs, stream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(B, d_braw, b_raw, cudaMemcpyDeviceToHost, stream);

@@ -56,11 +56,15 @@ cudaError_t launch_getri_small(const RealBatch &a, const int *ipiv, const RealBa
 // BF16 (three products).  ipiv n per matrix or nullptr; info as launch_getrf_small.
 constexpr int BLOCKED_MAX_N = 512;
 cudaError_t launch_getrf_blocked(const RealBatch &a, int *ipiv, int *info, int mode, cudaStream_t stream);
-// Blocked LU solve (trans 0) for 64 < n <= 8192.  `skip` (nullptr = none): per (matrix,
+// Blocked LU solve (trans 0) for 64 < n <= 8192.  Row interchanges from ipiv (LAPACK form,
+// applied in order) or, when perm is given, from the permutation perm (P b = b[perm], see
+// launch_permutation); both may be null.  `skip` (nullptr = none): per (matrix,
 // right-hand side) states; a group of right-hand sides whose states are all nonzero is
 // skipped (iterative refinement).  info may be null.
-cudaError_t launch_getrs_blocked(const RealBatch &a, const int *ipiv, const RealBatch &b, int nrhs, int *info,
-                                 const int *skip, cudaStream_t stream);
+cudaError_t launch_getrs_blocked(const RealBatch &a, const int *ipiv, const int *perm, const RealBatch &b, int nrhs,
+                                 int *info, const int *skip, cudaStream_t stream);
+// perm[q*n + i] = row of b that the interchanges ipiv[q*n ..] bring to position i.
+cudaError_t launch_permutation(const int *ipiv, int *perm, int n, int count, cudaStream_t stream);
 
 // ---- validation and staging ------------------------------------------------------------
 // flag[0] |= 1 when any of the m x n leading entries of any matrix is NaN or infinite.

@@ -93,3 +93,18 @@ def spd_batch(count, n, seed, scale_by_n=True):
     g = rng.standard_normal((count, n, n), dtype=np.float32)
     a = np.matmul(g, g.transpose(0, 2, 1)) / (n if scale_by_n else 1) + np.eye(n, dtype=np.float32)
     return a.astype(np.float32)
+
+
+def conditioned_batch(count, n, kappa, seed):
+    """A = U diag(s) V^T with U, V Haar-random orthogonal (QR of N(0,1), signs fixed by R's
+    diagonal) and s log-spaced from 1 to 1/kappa; FP32 matrices of 2-norm condition ~kappa."""
+    rng = np.random.default_rng(seed)
+    s = np.logspace(0.0, -np.log10(kappa), n)
+    out = np.empty((count, n, n), dtype=np.float32)
+    for q in range(count):
+        u, ru = np.linalg.qr(rng.standard_normal((n, n)))
+        v, rv = np.linalg.qr(rng.standard_normal((n, n)))
+        u *= np.sign(np.diag(ru))
+        v *= np.sign(np.diag(rv))
+        out[q] = ((u * s) @ v.T).astype(np.float32)
+    return out

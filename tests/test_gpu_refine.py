@@ -1,0 +1,160 @@
+"""aclsolverSgesvIrBatched on the GPU: LU in FP32, BF16 or split-BF16 precision plus FP64
+iterative refinement, judged against an FP64 LAPACK solve (backward and forward error) and,
+with no refinement in FP32 mode, bit for bit against the oracle's sgetrf + sgetrs."""
+
+import numpy as np
+import pytest
+import torch
+
+import aclsolver
+import oracle
+from oracle import judges
+from helpers import DeviceMatrices, conditioned_batch, first_mismatch, info_buffer, same_bits
+
+pytestmark = pytest.mark.gpu
+
+
+def gesv_ir(handle, a, b, precision, max_iter=10, tol=1e-7, x_init=None):
+    lib = aclsolver.library()
+    count, n, _ = a.shape
+    nrhs = b.shape[2]
+    da = DeviceMatrices(a, ld=n + 1)
+    db = DeviceMatrices(b, ld=n + 2)
+    dx = DeviceMatrices(np.zeros_like(b) if x_init is None else x_init, ld=n + 3)
+    iters = torch.full((count,), -5, dtype=torch.int32, device="cuda")
+    berr = torch.full((count,), -1.0, dtype=torch.float64, device="cuda")
+    info = info_buffer(count)
+    st = lib.aclsolverSgesvIrBatched(handle.value, precision, n, nrhs, da.table_ptr, da.ld, db.table_ptr, db.ld,
+                                    dx.table_ptr, dx.ld, max_iter, tol, iters.data_ptr(), berr.data_ptr(),
+                                    info.data_ptr(), count)
+    handle.stream.synchronize()
+    assert da.unchanged() and db.unchanged(), "A and B must be left as they were"
+    return st, dx.read(), iters.cpu().numpy(), berr.cpu().numpy(), info.cpu().numpy()
+
+
+def rhs(count, n, nrhs, seed):
+    return np.random.default_rng(seed).standard_normal((count, n, nrhs)).astype(np.float32)
+
+
+@pytest.mark.parametrize("n", [40, 100, 512])
+def test_fp32_without_refinement_is_sgetrf_sgetrs(handle, n):
+    a = np.random.default_rng(n).standard_normal((3, n, n)).astype(np.float32)
+    b = rhs(3, n, 2, n + 1)
+    st, x, iters, berr, info = gesv_ir(handle, a, b, aclsolver.FACTOR_FP32, max_iter=0)
+    assert st == aclsolver.SUCCESS and np.all(info == 0) and np.all(iters == 0)
+    lu, ipiv, _ = oracle.sgetrf_batched(a)
+    want = oracle.sgetrs_batched(lu, ipiv, b)
+    assert same_bits(x, want), first_mismatch(x, want)
+    for q in range(3):  # the reported berr is that of the (FP64) iterate, i.e. of x here
+        want = max(judges.backward_error(a[q], x[q][:, j], b[q][:, j]) for j in range(2))
+        assert berr[q] == pytest.approx(want, rel=1e-6)
+
+
+@pytest.mark.parametrize("precision", ["FACTOR_FP32", "FACTOR_BF16X3"])
+@pytest.mark.parametrize("kappa", [1e2, 1e4, 1e5])
+def test_refinement_reaches_fp32_backward_error(handle, precision, kappa):
+    n, count = 256, 4
+    a = conditioned_batch(count, n, kappa, seed=int(np.log10(kappa)))
+    b = rhs(count, n, 1, 9)
+    st, x, iters, berr, info = gesv_ir(handle, a, b, getattr(aclsolver, precision), max_iter=10, tol=1e-7)
+    assert st == aclsolver.SUCCESS and np.all(info == 0)
+    for q in range(count):
+        be = judges.backward_error(a[q], x[q], b[q])
+        fe = judges.forward_error(a[q], x[q], b[q])
+        assert be <= 1e-6, (q, be, berr[q], iters[q])
+        assert berr[q] <= 1e-6
+        assert fe <= kappa * 1e-6, (q, fe)
+        assert 0 <= iters[q] <= 10
+
+
+def test_bf16_refinement_well_conditioned(handle):
+    """Plain BF16 trailing updates (unit roundoff 2^-8) still refine to FP32 backward error
+    when kappa * u stays well below one."""
+    n, count = 200, 3
+    a = conditioned_batch(count, n, 10.0, seed=21)
+    b = rhs(count, n, 3, 22)
+    st, x, iters, berr, info = gesv_ir(handle, a, b, aclsolver.FACTOR_BF16, max_iter=30, tol=1e-7)
+    assert st == aclsolver.SUCCESS and np.all(info == 0)
+    for q in range(count):
+        assert judges.backward_error(a[q], x[q], b[q]) <= 1e-6
+        assert iters[q] >= 1  # BF16 factors alone are far from FP32 accuracy
+
+
+def test_bf16_reports_honest_error_when_it_cannot_converge(handle):
+    """At kappa = 1e5 BF16 LU is too inaccurate for classic refinement: the call must stop
+    (stall rule) and report a backward error that matches the returned solution."""
+    n, count = 256, 2
+    a = conditioned_batch(count, n, 1e5, seed=5)
+    b = rhs(count, n, 1, 6)
+    st, x, iters, berr, info = gesv_ir(handle, a, b, aclsolver.FACTOR_BF16, max_iter=10, tol=1e-7)
+    assert st == aclsolver.SUCCESS and np.all(info == 0)
+    for q in range(count):
+        be = judges.backward_error(a[q], x[q], b[q])
+        assert np.isfinite(berr[q])
+        # berr is that of the FP64 iterate; X is its FP32 rounding (relative 6e-8 per entry)
+        assert abs(be - berr[q]) <= 1e-7 + 0.05 * berr[q]
+
+
+def test_small_orders_and_several_rhs(handle):
+    n, count = 48, 5
+    a = conditioned_batch(count, n, 1e3, seed=2)
+    b = rhs(count, n, 4, 3)
+    st, x, iters, berr, info = gesv_ir(handle, a, b, aclsolver.FACTOR_BF16X3, max_iter=5, tol=1e-7)
+    assert st == aclsolver.SUCCESS and np.all(info == 0)
+    for q in range(count):
+        assert judges.backward_error(a[q], x[q], b[q]) <= 1e-6
+
+
+def test_singular_matrix_is_not_solved(handle):
+    n = 90
+    a = conditioned_batch(3, n, 10.0, seed=4)
+    a[1, :, 7] = 0.0
+    b = rhs(3, n, 1, 5)
+    x0 = np.full_like(b, 2.5)
+    st, x, iters, berr, info = gesv_ir(handle, a, b, aclsolver.FACTOR_BF16X3, x_init=x0)
+    assert st == aclsolver.SUCCESS
+    assert info[0] == 0 and info[1] > 0 and info[2] == 0
+    assert np.all(x[1] == 2.5)
+    assert np.isnan(berr[1]) and iters[1] == 0
+    assert judges.backward_error(a[2], x[2], b[2]) <= 1e-6
+
+
+def test_solution_may_overwrite_b(handle):
+    lib = aclsolver.library()
+    n, count = 130, 2
+    a = conditioned_batch(count, n, 100.0, seed=8)
+    b = rhs(count, n, 1, 9)
+    da = DeviceMatrices(a, ld=n)
+    db = DeviceMatrices(b, ld=n)
+    info = info_buffer(count)
+    st = lib.aclsolverSgesvIrBatched(handle.value, aclsolver.FACTOR_BF16X3, n, 1, da.table_ptr, n, db.table_ptr, n,
+                                    db.table_ptr, n, 10, 1e-7, None, None, info.data_ptr(), count)
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS
+    x = db.read()
+    for q in range(count):
+        assert judges.backward_error(a[q], x[q], b[q]) <= 1e-6
+
+
+@pytest.mark.parametrize(
+    "field,value,arg",
+    [("precision", 2, 1), ("n", 513, 2), ("nrhs", -1, 3), ("lda", 5, 5), ("ldb", 5, 7), ("ldx", 5, 9),
+     ("max_iter", -1, 10), ("tol", -1.0, 11), ("batch", -1, 15)],
+)
+def test_argument_errors(handle, field, value, arg):
+    lib = aclsolver.library()
+    n, count = 16, 2
+    a = conditioned_batch(count, n, 10.0, seed=1)
+    da = DeviceMatrices(a, ld=n)
+    db = DeviceMatrices(rhs(count, n, 1, 2), ld=n)
+    dx = DeviceMatrices(rhs(count, n, 1, 3), ld=n)
+    args = dict(precision=aclsolver.FACTOR_FP32, n=n, nrhs=1, lda=n, ldb=n, ldx=n, max_iter=3, tol=1e-7, batch=count)
+    args[field] = value
+    info = info_buffer(count)
+    st = lib.aclsolverSgesvIrBatched(handle.value, args["precision"], args["n"], args["nrhs"], da.table_ptr,
+                                    args["lda"], db.table_ptr, args["ldb"], dx.table_ptr, args["ldx"],
+                                    args["max_iter"], args["tol"], None, None, info.data_ptr(), args["batch"])
+    handle.stream.synchronize()
+    assert st == aclsolver.INVALID_VALUE
+    got = info.cpu().numpy()
+    assert got[0] == -arg
