@@ -138,6 +138,17 @@ extern "C"
                                               int maxIter, double tol, int *iterArray, double *berrArray,
                                               int *infoArray, int batchSize);
 
+    /* aclsolverSgetrfBatched with a choice of precision for the trailing updates, for callers
+     * that run their own refinement or reuse the factors: ACLSOLVER_FACTOR_FP32 gives exactly
+     * the factors, pivots and info of aclsolverSgetrfBatched; the BF16 precisions form the
+     * trailing products on the tensor cores (the panels, pivot search and triangular solves
+     * stay FP32).  Orders n <= 64 always factor in plain FP32.  0 <= n <= 512; arguments,
+     * info and errors as aclsolverSgetrfBatched (precision is argument 1, the others shift
+     * by one).  No counterpart in the reference, whose factorisations are FP32 only. */
+    aclsolverStatus_t aclsolverSgetrfBatchedMixed(aclsolverHandle_t handle, aclsolverFactorPrecision_t precision,
+                                                  int n, float *const Aarray[], int lda, int *PivotArray,
+                                                  int *infoArray, int batchSize);
+
 #ifdef __cplusplus
 }
 #endif

@@ -78,6 +78,7 @@ ARGTYPES = {
     "aclsolverCposvVbatched": [VP, VP, VP, VP, VP],
     "aclsolverVbatchedPlanDestroy": [VP],
     "aclsolverSmatinvBatchedNoAlloc": [VP, I32, VP, I32, VP, I32, VP, I32],
+    "aclsolverSgetrfBatchedMixed": [VP, I32, I32, VP, I32, VP, VP, I32],
     "aclsolverSgesvIrBatched": [VP, I32, I32, I32, VP, I32, VP, I32, VP, I32, I32, C.c_double, VP, VP, VP, I32],
 }
 

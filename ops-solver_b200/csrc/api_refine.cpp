@@ -156,3 +156,32 @@ extern "C" aclsolverStatus_t aclsolverSgesvIrBatched(aclsolverHandle_t handle, a
     aclsolverStatus_t fin = finish_scratch(h, blk);
     return launched != ACLSOLVER_STATUS_SUCCESS ? launched : fin;
 }
+
+extern "C" aclsolverStatus_t aclsolverSgetrfBatchedMixed(aclsolverHandle_t handle, aclsolverFactorPrecision_t precision,
+                                                         int n, float *const Aarray[], int lda, int *PivotArray,
+                                                         int *infoArray, int batchSize)
+{
+    if (!handle) return ACLSOLVER_STATUS_HANDLE_IS_NULLPTR;
+    Handle *h = to_handle(handle);
+    int arg = 0;
+    if (precision != ACLSOLVER_FACTOR_FP32 && precision != ACLSOLVER_FACTOR_BF16 &&
+        precision != ACLSOLVER_FACTOR_BF16X3)
+        arg = 1;
+    else if (n < 0 || n > BLOCKED_MAX_N)
+        arg = 2;
+    else if (n > 0 && batchSize > 0 && !Aarray)
+        arg = 3;
+    else if (lda < std::max(1, n))
+        arg = 4;
+    else if (batchSize > 0 && !infoArray)
+        arg = 6;
+    else if (batchSize < 0)
+        arg = 7;
+    if (arg) return fail_args(h, infoArray, batchSize < 0 ? 1 : batchSize, arg);
+    if (batchSize == 0) return ACLSOLVER_STATUS_SUCCESS;
+    if (n == 0) return launch_status(launch_fill_info(infoArray, 0, batchSize, h->stream));
+    RealBatch a{nullptr, Aarray, n, lda, 0, batchSize};
+    const int mode = precision == ACLSOLVER_FACTOR_FP32 ? 0 : (precision == ACLSOLVER_FACTOR_BF16 ? 1 : 3);
+    if (n <= SMALL_N) return launch_status(launch_getrf_small(a, n, PivotArray, infoArray, h->stream));
+    return launch_status(launch_getrf_blocked(a, PivotArray, infoArray, mode, h->stream));
+}

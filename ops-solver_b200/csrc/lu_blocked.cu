@@ -9,13 +9,15 @@
 //     never moved while the panel is factored: each carries its current position, and the
 //     pivot search is one barrier per column (warp redux of an order-preserving |a| key and
 //     of the position, then the eight warp winners through double-buffered shared slots that
-//     also carry the winning row, so the pivot row needs no second broadcast);
-//  2. the panel goes back to global memory in its final row order and its L is staged in
-//     shared memory (FP32, or negated BF16 hi/lo for the tensor cores);
-//  3. the trailing columns go in tiles of 64: a warp per column gathers the 32 U12 rows
-//     through the panel permutation and moves the rows whose position changed (coalesced
-//     column segments), U12 = L11^-1 A12 is solved in shared memory by four threads per
-//     column, and A22 -= L21 U12 runs over 128-row tiles;
+//     also carry the winning row, so the pivot row needs no second broadcast); final values
+//     go to the row's own place in A as they are produced;
+//  2. the panel and trailing columns take the panel's row interchanges (a warp per column,
+//     eight columns in flight, only the rows whose position changed) and the panel's L is
+//     staged in shared memory (FP32, or negated BF16 hi/lo for the tensor cores);
+//  3. U12 = L11^-1 A12 (a thread per column, in registers), then A22 -= L21 U12 over
+//     128 x 64 tiles whose U12
+//     block is prefetched into the other half of a double-buffered shared tile and whose C
+//     is prefetched into registers one row tile ahead;
 //  4. after the last panel, the row interchanges of every later panel are applied to each
 //     panel's L columns in one gather per column (LAPACK's final row order).
 // Plain mode: every element takes a = fma(-l_ik, u_kj, a) in ascending k, the order of the
@@ -39,49 +41,60 @@ constexpr int BT = 256;  // threads per block
 constexpr int NW = BT / 32;
 constexpr int NB = 32;   // panel width
 constexpr int MAXN = BLOCKED_MAX_N;
+constexpr int NPANEL = MAXN / NB;
 constexpr int CT = 64;   // trailing column tile
 constexpr int RT = 128;  // trailing row tile
 constexpr int UP = CT + 4;  // pitch of the FP32 U12 tile
 constexpr int HP = NB + 8;  // pitch (halfs) of the BF16 tiles: 80 bytes, ldmatrix conflict-free
+constexpr int L11P = NB + 4;
+constexpr int SWAP_COLS = 8;  // columns in flight per warp during the row interchanges
 constexpr unsigned FULL = 0xffffffffu;
 
 struct __align__(16) Shared
 {
     float slot[2][NW][NB];     // each warp's best pivot row, double buffered by column parity
-    unsigned key[2][NW][2];    // each warp's (best key, its position)
+    uint2 key[2][NW];          // each warp's (best key, its position)
+    int krow[2][NW];           // each warp's best row (panel-relative index)
     short perm[MAXN];          // perm[p]: panel-relative row now at panel position p
-    short tmap[MAXN];          // left-column permutation (epilogue)
-    short umap[MAXN];
     int changed[2 * NB];       // panel positions whose row changed
+    short chg[NPANEL][2 * NB];  // per panel: changed positions and the rows they received,
+    short src[NPANEL][2 * NB];  // kept for the epilogue
+    int nchg[NPANEL];
     int nchanged;
     unsigned zmask;            // bit j: panel column j had a zero pivot (not used for updates)
     int state;                 // info of the matrix
 };
 
-// Staged rows per panel: the trailing tiles start at position NB and cover RT rows each, so
-// the last tile reads up to NB + round_up(m - NB, RT) - 1 < round_up(n, RT) + NB.
-__host__ __device__ constexpr int round_rows(int n) { return (n + RT - 1) / RT * RT + NB; }
+__host__ __device__ constexpr int lp_pitch(int n) { return (n + 3) / 4 * 4 + 4; }
 
 // Dynamic shared memory (bytes) for order n.
-//   plain: L (NB x LP floats, L[k][p]), U12 tile (NB x UP floats)
-//   mixed: L11 (NB x (NB + 4) floats), U12 tile, L21 hi/lo (rows x HP bf16), U12 hi/lo (CT x HP)
-__host__ __device__ constexpr size_t lp_pitch(int n) { return (size_t)round_rows(n) + 4; }
+//   plain: L (NB x lp floats, L[k][p]), U12 tiles (2 x NB x UP floats)
+//   mixed: L11 (NB x L11P floats), L21 hi/lo (n x HP bf16 each), U12 hi/lo tiles (2 x CT x HP each)
 __host__ __device__ size_t dyn_bytes(int n, int mode)
 {
-    if (mode == 0) return ((size_t)NB * lp_pitch(n) + (size_t)NB * UP) * sizeof(float);
+    if (mode == 0) return ((size_t)NB * lp_pitch(n) + 2 * (size_t)NB * UP) * sizeof(float);
     const int terms = mode == 1 ? 1 : 2;
-    return ((size_t)NB * (NB + 4) + (size_t)NB * UP) * sizeof(float) +
-           (size_t)terms * ((size_t)round_rows(n) * HP + (size_t)CT * HP) * sizeof(__nv_bfloat16);
+    return (size_t)NB * L11P * sizeof(float) +
+           (size_t)terms * ((size_t)n * HP + 2 * (size_t)CT * HP) * sizeof(__nv_bfloat16);
 }
 
 // ---------------------------------------------------------------------------------------
 // panel
 // ---------------------------------------------------------------------------------------
+// The panel's rows stay in registers, but rotated: in a group of four steps the current
+// column is r[s][u] (u = 0..3), and after the group every row shifts left by four, so all
+// register indices are compile-time constants inside a short loop body.  Each value that
+// becomes final is stored at its row's place in A as it is produced (an L entry at its
+// step, the pivot row's U entries at the pivot step, from the slot); rows are brought into
+// their final order afterwards, with the interchanges of the trailing columns.
 __device__ __forceinline__ void panel_factor(float *A, int lda, int n, int k0, int w, int *ipiv, bool pivoting,
-                                             Shared &sh, float (&r)[2][NB], int (&pos)[2])
+                                             Shared &sh, int (&pos)[2])
 {
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int m = n - k0;
+    const bool active = warp * 32 < m;  // warp-uniform: some row of this warp is in the panel
+    float *pan = A + (int64_t)k0 * lda + k0;  // panel element (row i, column c) at pan[c * lda + i]
+    float r[2][NB];
     bool valid[2];
 #pragma unroll
     for (int s = 0; s < 2; ++s)
@@ -90,87 +103,134 @@ __device__ __forceinline__ void panel_factor(float *A, int lda, int n, int k0, i
         valid[s] = i < m;
         pos[s] = i;
 #pragma unroll
-        for (int c = 0; c < NB; ++c) r[s][c] = (valid[s] && c < w) ? A[(int64_t)(k0 + c) * lda + k0 + i] : 0.0f;
+        for (int c = 0; c < NB; ++c) r[s][c] = (valid[s] && c < w) ? pan[(int64_t)c * lda + i] : 0.0f;
     }
-#pragma unroll
-    for (int j = 0; j < NB; ++j)
+    for (int j0 = 0; j0 < w; j0 += 4)
     {
-        if (j >= w) break;  // uniform
-        const int buf = j & 1;
-        unsigned key[2];
 #pragma unroll
-        for (int s = 0; s < 2; ++s)
+        for (int u = 0; u < 4; ++u)
         {
-            const float v = r[s][j];
-            if (!valid[s])
-                key[s] = 0u;
-            else if (pivoting)
-                key[s] = pos[s] == j && v != v ? 0xffffffffu : (pos[s] >= j ? pivot_key(v) : 0u);
-            else
-                key[s] = pos[s] == j ? 1u : 0u;
-        }
-        const unsigned wmax = __reduce_max_sync(FULL, max(key[0], key[1]));
-        unsigned cand = 0xffffffffu;
-#pragma unroll
-        for (int s = 0; s < 2; ++s)
-            if (valid[s] && key[s] == wmax) cand = min(cand, (unsigned)pos[s]);
-        const unsigned wpos = __reduce_min_sync(FULL, cand);
-#pragma unroll
-        for (int s = 0; s < 2; ++s)
-            if (valid[s] && key[s] == wmax && (unsigned)pos[s] == wpos)
+            const int j = j0 + u;
+            if (j >= w) break;  // uniform
+            const int buf = j & 1;
+            if (active)
             {
-                float4 *dst = reinterpret_cast<float4 *>(sh.slot[buf][warp]);
+                unsigned key[2];
 #pragma unroll
-                for (int c = 0; c < NB; c += 4) dst[c / 4] = make_float4(r[s][c], r[s][c + 1], r[s][c + 2], r[s][c + 3]);
-            }
-        if (lane == 0)
-        {
-            sh.key[buf][warp][0] = wmax;
-            sh.key[buf][warp][1] = wpos;
-        }
-        __syncthreads();
-        // the block's winner: largest key, then the smallest position (a warp without
-        // candidates reports key 0 and always loses: the position-j row has key >= 1)
-        unsigned gmax = 0u, gpos = 0xffffffffu;
-        int gw = 0;
-#pragma unroll
-        for (int q = 0; q < NW; ++q)
-        {
-            const unsigned kq = sh.key[buf][q][0], pq = sh.key[buf][q][1];
-            if (kq > gmax || (kq == gmax && pq < gpos))
-            {
-                gmax = kq;
-                gpos = pq;
-                gw = q;
-            }
-        }
-        const int pr = (int)gpos;
-        const float *prow = sh.slot[buf][gw];
-        if (pivoting && t == 0) ipiv[k0 + j] = k0 + pr + 1;
-#pragma unroll
-        for (int s = 0; s < 2; ++s) pos[s] = pos[s] == j ? pr : (pos[s] == pr ? j : pos[s]);
-        const float d = prow[j];
-        if (d == 0.0f)
-        {
-            if (t == 0)
-            {
-                if (sh.state == 0) sh.state = k0 + j + 1;
-                sh.zmask |= 1u << j;
-            }
-        }
-        else if (k0 + j + 1 < n)
-        {
-#pragma unroll
-            for (int s = 0; s < 2; ++s)
-            {
-                if (valid[s] && pos[s] > j)
+                for (int s = 0; s < 2; ++s)
                 {
-                    const float l = div_rn(r[s][j], d);
-                    r[s][j] = l;
+                    const float v = r[s][u];
+                    if (!valid[s])
+                        key[s] = 0u;
+                    else if (pivoting)
+                        key[s] = pos[s] == j && v != v ? 0xffffffffu : (pos[s] >= j ? pivot_key(v) : 0u);
+                    else
+                        key[s] = pos[s] == j ? 1u : 0u;
+                }
+                const unsigned wmax = __reduce_max_sync(FULL, max(key[0], key[1]));
+                unsigned cand = 0xffffffffu;
 #pragma unroll
-                    for (int c = j + 1; c < NB; ++c) r[s][c] = fma_rn(-l, prow[c], r[s][c]);
+                for (int s = 0; s < 2; ++s)
+                    if (valid[s] && key[s] == wmax) cand = min(cand, (unsigned)pos[s]);
+                const unsigned wpos = __reduce_min_sync(FULL, cand);
+#pragma unroll
+                for (int s = 0; s < 2; ++s)
+                    if (valid[s] && key[s] == wmax && (unsigned)pos[s] == wpos)
+                    {
+                        float4 *dst = reinterpret_cast<float4 *>(sh.slot[buf][warp]);
+#pragma unroll
+                        for (int c = 0; c < NB; c += 4)
+                            dst[c / 4] = make_float4(r[s][c], r[s][c + 1], r[s][c + 2], r[s][c + 3]);
+                        sh.krow[buf][warp] = t + s * BT;
+                    }
+                if (lane == 0) sh.key[buf][warp] = make_uint2(wmax, wpos);
+            }
+            else if (lane == 0)
+                sh.key[buf][warp] = make_uint2(0u, 0xffffffffu);
+            __syncthreads();
+            if (!active) continue;  // no rows here: nothing to eliminate
+            // the block's winner: largest key, then the smallest position (a warp without
+            // candidates reports key 0 and always loses: the position-j row has key >= 1)
+            const uint4 *kv = reinterpret_cast<const uint4 *>(sh.key[buf]);
+            unsigned gmax = 0u, gpos = 0xffffffffu;
+            int gw = 0;
+#pragma unroll
+            for (int q2 = 0; q2 < NW / 2; ++q2)
+            {
+                const uint4 k2 = kv[q2];
+                if (k2.x > gmax || (k2.x == gmax && k2.y < gpos))
+                {
+                    gmax = k2.x;
+                    gpos = k2.y;
+                    gw = 2 * q2;
+                }
+                if (k2.z > gmax || (k2.z == gmax && k2.w < gpos))
+                {
+                    gmax = k2.z;
+                    gpos = k2.w;
+                    gw = 2 * q2 + 1;
                 }
             }
+            const int pr = (int)gpos;
+            const float *prow = sh.slot[buf][gw];  // prow[c]: the pivot row at column j0 + c
+            if (pivoting && t == 0) ipiv[k0 + j] = k0 + pr + 1;
+            // the pivot row's U entries (columns j .. w - 1) are final now
+            if (t < w - j) pan[(int64_t)(j + t) * lda + sh.krow[buf][gw]] = prow[u + t];
+#pragma unroll
+            for (int s = 0; s < 2; ++s) pos[s] = pos[s] == j ? pr : (pos[s] == pr ? j : pos[s]);
+            const float d = prow[u];
+            bool go[2];
+#pragma unroll
+            for (int s = 0; s < 2; ++s) go[s] = valid[s] && pos[s] > j;
+            if (d == 0.0f)
+            {
+                if (t == 0)
+                {
+                    if (sh.state == 0) sh.state = k0 + j + 1;
+                    sh.zmask |= 1u << j;
+                }
+                // a zero pivot scales nothing: the column keeps its values as L entries
+#pragma unroll
+                for (int s = 0; s < 2; ++s)
+                    if (go[s]) pan[(int64_t)j * lda + t + s * BT] = r[s][u];
+            }
+            else
+            {
+                float l[2];
+#pragma unroll
+                for (int s = 0; s < 2; ++s)
+                {
+                    l[s] = go[s] ? div_rn(r[s][u], d) : 0.0f;
+                    if (go[s]) pan[(int64_t)j * lda + t + s * BT] = l[s];
+                }
+                // the pivot row four columns at a time, shared by both rows
+                const float4 *p4 = reinterpret_cast<const float4 *>(prow);
+#pragma unroll
+                for (int c4 = 0; c4 < NB / 4; ++c4)
+                {
+                    if (c4 * 4 + 3 <= u) continue;
+                    const float4 v = p4[c4];
+                    const float pv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                    for (int e = 0; e < 4; ++e)
+                    {
+                        const int c = c4 * 4 + e;
+                        if (c <= u) continue;
+#pragma unroll
+                        for (int s = 0; s < 2; ++s)
+                            if (go[s]) r[s][c] = fma_rn(-l[s], pv[e], r[s][c]);
+                    }
+                }
+            }
+        }
+        // rotate: the next four columns move to the front
+#pragma unroll
+        for (int s = 0; s < 2; ++s)
+        {
+#pragma unroll
+            for (int c = 0; c < NB - 4; ++c) r[s][c] = r[s][c + 4];
+#pragma unroll
+            for (int c = NB - 4; c < NB; ++c) r[s][c] = 0.0f;
         }
     }
 }
@@ -178,49 +238,80 @@ __device__ __forceinline__ void panel_factor(float *A, int lda, int n, int k0, i
 // ---------------------------------------------------------------------------------------
 // trailing update tiles: C (positions r0.., columns j0..) -= L21 U12
 // ---------------------------------------------------------------------------------------
-// Plain: thread (tr, tc) owns rows {tr*4 + i, 64 + tr*4 + i} x columns tc*4 + j; ascending k.
-__device__ __forceinline__ void tile_plain(float *A, int lda, int m, int k0, int j0, int nc, int r0, unsigned zmask,
-                                           const float *L, int lp, const float *us, bool vec)
+// Plain: thread (tr, tc) owns rows {tr*4 + i, 64 + tr*4 + i} x columns tc*4 + j.
+__device__ __forceinline__ void plain_c_load(const float *A, int lda, int m, int k0, int j0, int nc, int r0, bool vec,
+                                             float (&c)[8][4])
 {
     const int t = threadIdx.x;
     const int tr = t & 15, tc = t >> 4;
-    float acc[8][4];
-    int rows[8];
-#pragma unroll
-    for (int h = 0; h < 2; ++h)
-#pragma unroll
-        for (int i = 0; i < 4; ++i) rows[h * 4 + i] = r0 + h * 64 + tr * 4 + i;
 #pragma unroll
     for (int j = 0; j < 4; ++j)
     {
         const int cj = tc * 4 + j;
-        const float *col = A + (int64_t)(j0 + cj) * lda + k0;
+        const float *col = A + (int64_t)(j0 + min(cj, nc - 1)) * lda + k0;
 #pragma unroll
         for (int h = 0; h < 2; ++h)
         {
-            const int rb = rows[h * 4];
-            if (vec && cj < nc && rb + 3 < m)
+            const int rb = r0 + h * 64 + tr * 4;
+            if (vec && rb + 3 < m)
             {
                 const float4 v = *reinterpret_cast<const float4 *>(col + rb);
-                acc[h * 4 + 0][j] = v.x;
-                acc[h * 4 + 1][j] = v.y;
-                acc[h * 4 + 2][j] = v.z;
-                acc[h * 4 + 3][j] = v.w;
+                c[h * 4 + 0][j] = v.x;
+                c[h * 4 + 1][j] = v.y;
+                c[h * 4 + 2][j] = v.z;
+                c[h * 4 + 3][j] = v.w;
             }
             else
             {
 #pragma unroll
-                for (int i = 0; i < 4; ++i)
-                    acc[h * 4 + i][j] = (cj < nc && rows[h * 4 + i] < m) ? col[rows[h * 4 + i]] : 0.0f;
+                for (int i = 0; i < 4; ++i) c[h * 4 + i][j] = rb + i < m ? col[rb + i] : 0.0f;
             }
         }
     }
+}
+
+__device__ __forceinline__ void plain_c_store(float *A, int lda, int m, int k0, int j0, int nc, int r0, bool vec,
+                                              const float (&c)[8][4])
+{
+    const int t = threadIdx.x;
+    const int tr = t & 15, tc = t >> 4;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+    {
+        const int cj = tc * 4 + j;
+        if (cj >= nc) continue;
+        float *col = A + (int64_t)(j0 + cj) * lda + k0;
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+        {
+            const int rb = r0 + h * 64 + tr * 4;
+            if (vec && rb + 3 < m)
+                *reinterpret_cast<float4 *>(col + rb) =
+                    make_float4(c[h * 4 + 0][j], c[h * 4 + 1][j], c[h * 4 + 2][j], c[h * 4 + 3][j]);
+            else
+            {
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    if (rb + i < m) col[rb + i] = c[h * 4 + i][j];
+            }
+        }
+    }
+}
+
+// acc -= L21 U12 in ascending k (zero-pivot columns skipped).  Rows past the staged ones
+// read clamped (in-range, unused) entries.
+__device__ __forceinline__ void plain_c_update(float (&acc)[8][4], const float *L, int lp, int r0, unsigned zmask,
+                                               const float *us)
+{
+    const int t = threadIdx.x;
+    const int tr = t & 15, tc = t >> 4;
+    const int ra = min(r0 + tr * 4, lp - 4), rb = min(r0 + 64 + tr * 4, lp - 4);
 #pragma unroll 8
     for (int k = 0; k < NB; ++k)
     {
         if ((zmask >> k) & 1u) continue;  // uniform
-        const float4 a0 = *reinterpret_cast<const float4 *>(L + k * lp + r0 + tr * 4);
-        const float4 a1 = *reinterpret_cast<const float4 *>(L + k * lp + r0 + 64 + tr * 4);
+        const float4 a0 = *reinterpret_cast<const float4 *>(L + k * lp + ra);
+        const float4 a1 = *reinterpret_cast<const float4 *>(L + k * lp + rb);
         const float4 b = *reinterpret_cast<const float4 *>(us + k * UP + tc * 4);
         const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
         const float bb[4] = {b.x, b.y, b.z, b.w};
@@ -228,26 +319,6 @@ __device__ __forceinline__ void tile_plain(float *A, int lda, int m, int k0, int
         for (int i = 0; i < 8; ++i)
 #pragma unroll
             for (int j = 0; j < 4; ++j) acc[i][j] = fma_rn(-a[i], bb[j], acc[i][j]);
-    }
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-    {
-        const int cj = tc * 4 + j;
-        float *col = A + (int64_t)(j0 + cj) * lda + k0;
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-        {
-            const int rb = rows[h * 4];
-            if (vec && cj < nc && rb + 3 < m)
-                *reinterpret_cast<float4 *>(col + rb) =
-                    make_float4(acc[h * 4 + 0][j], acc[h * 4 + 1][j], acc[h * 4 + 2][j], acc[h * 4 + 3][j]);
-            else
-            {
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-                    if (cj < nc && rows[h * 4 + i] < m) col[rows[h * 4 + i]] = acc[h * 4 + i][j];
-            }
-        }
     }
 }
 
@@ -268,19 +339,15 @@ __device__ __forceinline__ void mma_bf16(float (&c)[4], const unsigned (&a)[4], 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// Mixed: warp (wm = warp & 3, wn = warp >> 2) owns rows r0 + wm*32 .. +31, columns
-// wn*32 .. +31 of the tile: 2 x 4 mma tiles of 16 x 8, K = 32 in two k16 steps.  The staged
-// L21 halves are negated, so C + (-L) U accumulates the update.
-template <int TERMS>
-__device__ __forceinline__ void tile_mixed(float *A, int lda, int m, int k0, int j0, int nc, int r0,
-                                           const __nv_bfloat16 *lh, const __nv_bfloat16 *ll,
-                                           const __nv_bfloat16 *uh, const __nv_bfloat16 *ul)
+// Mixed: warp (wm = warp & 3, wn = warp >> 2) owns rows r0 + wm*32 .. +31 and columns
+// wn*32 .. +31 of the tile: 2 x 4 mma tiles of 16 x 8, K = 32 in two k16 steps.  Element
+// e of mma tile (mi, ni) is row g + 8*(e >= 2) + 16 mi, column 2q + (e & 1) + 8 ni.
+__device__ __forceinline__ void mixed_c_load(const float *A, int lda, int m, int k0, int j0, int nc, int r0,
+                                             float (&c)[2][4][4])
 {
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int wr = r0 + (warp & 3) * 32;
-    const int wc = (warp >> 2) * 32;
+    const int wr = r0 + (warp & 3) * 32, wc = (warp >> 2) * 32;
     const int g = lane >> 2, q = lane & 3;
-    float acc[2][4][4];
 #pragma unroll
     for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
@@ -290,8 +357,37 @@ __device__ __forceinline__ void tile_mixed(float *A, int lda, int m, int k0, int
             {
                 const int row = wr + mi * 16 + g + (e >= 2 ? 8 : 0);
                 const int cj = wc + ni * 8 + q * 2 + (e & 1);
-                acc[mi][ni][e] = (row < m && cj < nc) ? A[(int64_t)(j0 + cj) * lda + k0 + row] : 0.0f;
+                c[mi][ni][e] = (row < m && cj < nc) ? A[(int64_t)(j0 + cj) * lda + k0 + row] : 0.0f;
             }
+}
+
+__device__ __forceinline__ void mixed_c_store(float *A, int lda, int m, int k0, int j0, int nc, int r0,
+                                              const float (&c)[2][4][4])
+{
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int wr = r0 + (warp & 3) * 32, wc = (warp >> 2) * 32;
+    const int g = lane >> 2, q = lane & 3;
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+            {
+                const int row = wr + mi * 16 + g + (e >= 2 ? 8 : 0);
+                const int cj = wc + ni * 8 + q * 2 + (e & 1);
+                if (row < m && cj < nc) A[(int64_t)(j0 + cj) * lda + k0 + row] = c[mi][ni][e];
+            }
+}
+
+// The staged L21 halves are negated, so C + (-L) U accumulates the update.
+template <int TERMS>
+__device__ __forceinline__ void mixed_c_update(float (&acc)[2][4][4], int n, int r0, const __nv_bfloat16 *lh,
+                                               const __nv_bfloat16 *ll, const __nv_bfloat16 *uh,
+                                               const __nv_bfloat16 *ul)
+{
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int wr = r0 + (warp & 3) * 32, wc = (warp >> 2) * 32;
 #pragma unroll
     for (int ks = 0; ks < 2; ++ks)
     {
@@ -299,7 +395,7 @@ __device__ __forceinline__ void tile_mixed(float *A, int lda, int m, int k0, int
 #pragma unroll
         for (int mi = 0; mi < 2; ++mi)
         {
-            const int row = wr + mi * 16 + (lane & 15);
+            const int row = min(wr + mi * 16 + (lane & 15), n - 1);  // rows past n: unused
             const int kk = ks * 16 + (lane >> 4) * 8;
             ldsm_x4(ah[mi], lh + (size_t)row * HP + kk);
             if (TERMS > 1) ldsm_x4(al[mi], ll + (size_t)row * HP + kk);
@@ -330,23 +426,56 @@ __device__ __forceinline__ void tile_mixed(float *A, int lda, int m, int k0, int
             }
         }
     }
-#pragma unroll
-    for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-        for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-            for (int e = 0; e < 4; ++e)
-            {
-                const int row = wr + mi * 16 + g + (e >= 2 ? 8 : 0);
-                const int cj = wc + ni * 8 + q * 2 + (e & 1);
-                if (row < m && cj < nc) A[(int64_t)(j0 + cj) * lda + k0 + row] = acc[mi][ni][e];
-            }
 }
 
 __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16 &hi, __nv_bfloat16 &lo)
 {
     hi = __float2bfloat16_rn(v);
     lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+}
+
+// U12 tile prefetch: thread t holds rows kq .. kq + 7 (kq = 8 (t & 3)) of column t >> 2.
+__device__ __forceinline__ void u_load(const float *A, int lda, int k0, int j0, int nc, bool vec, float (&u)[8])
+{
+    const int t = threadIdx.x;
+    const int cc = t >> 2, kq = (t & 3) * 8;
+    const float *src = A + (int64_t)(j0 + min(cc, nc - 1)) * lda + k0 + kq;
+    if (vec)
+    {
+        const float4 a = *reinterpret_cast<const float4 *>(src);
+        const float4 b = *reinterpret_cast<const float4 *>(src + 4);
+        u[0] = a.x, u[1] = a.y, u[2] = a.z, u[3] = a.w, u[4] = b.x, u[5] = b.y, u[6] = b.z, u[7] = b.w;
+    }
+    else
+    {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) u[i] = src[i];
+    }
+    if (cc >= nc)
+    {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) u[i] = 0.0f;
+    }
+}
+
+template <int MODE, int TERMS>
+__device__ __forceinline__ void u_store(const float (&u)[8], float *us, __nv_bfloat16 *uh, __nv_bfloat16 *ul)
+{
+    const int t = threadIdx.x;
+    const int cc = t >> 2, kq = (t & 3) * 8;
+    if (MODE == 0)
+    {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) us[(kq + i) * UP + cc] = u[i];
+    }
+    else
+    {
+        __nv_bfloat16 h[8], l[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) split_bf16(u[i], h[i], l[i]);
+        *reinterpret_cast<uint4 *>(uh + (size_t)cc * HP + kq) = *reinterpret_cast<const uint4 *>(h);
+        if (TERMS > 1) *reinterpret_cast<uint4 *>(ul + (size_t)cc * HP + kq) = *reinterpret_cast<const uint4 *>(l);
+    }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -360,16 +489,16 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
     extern __shared__ __align__(16) unsigned char dyn[];
     __shared__ Shared sh;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int rows = round_rows(n);
-    const int lp = (int)lp_pitch(n);
+    const int lp = lp_pitch(n);
     // carve the dynamic area
-    float *L = reinterpret_cast<float *>(dyn);  // plain: NB x lp; mixed: L11 NB x (NB + 4)
-    float *us = L + (MODE == 0 ? (size_t)NB * lp : (size_t)NB * (NB + 4));
-    __nv_bfloat16 *lh = reinterpret_cast<__nv_bfloat16 *>(us + (size_t)NB * UP);
-    __nv_bfloat16 *ll = lh + (size_t)rows * HP;
-    __nv_bfloat16 *uh = ll + (TERMS > 1 ? (size_t)rows * HP : 0);
-    __nv_bfloat16 *ul = uh + (size_t)CT * HP;
-    const int l11p = MODE == 0 ? lp : NB + 4;
+    float *L = reinterpret_cast<float *>(dyn);  // plain: NB x lp; mixed: L11 NB x L11P
+    float *us = L + (MODE == 0 ? (size_t)NB * lp : (size_t)NB * L11P);  // plain: 2 x NB x UP
+    __nv_bfloat16 *lh = reinterpret_cast<__nv_bfloat16 *>(us);          // mixed: after L11
+    __nv_bfloat16 *ll = lh + (size_t)n * HP;
+    __nv_bfloat16 *uh = lh + (size_t)(TERMS > 1 ? 2 : 1) * n * HP;      // 2 x CT x HP
+    __nv_bfloat16 *ul = uh + 2 * (size_t)CT * HP;
+    const float *l11 = L;
+    const int l11p = MODE == 0 ? lp : L11P;
 
     for (int64_t q = blockIdx.x; q < count; q += gridDim.x)
     {
@@ -391,52 +520,102 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
                 sh.zmask = 0u;
                 sh.nchanged = 0;
             }
-            float r[2][NB];
             int pos[2];
-            panel_factor(A, lda, n, k0, w, piv, piv != nullptr, sh, r, pos);
-            // write back in final order, stage L, record the permutation
+            panel_factor(A, lda, n, k0, w, piv, piv != nullptr, sh, pos);
+            // the permutation and the positions whose row changed
 #pragma unroll
             for (int s = 0; s < 2; ++s)
-            {
-                const int i = t + s * BT;
-                if (i < m)
+                if (t + s * BT < m) sh.perm[pos[s]] = (short)(t + s * BT);
+            __syncthreads();
+            for (int p = t; p < m; p += BT)
+                if (sh.perm[p] != p)
                 {
-                    const int p = pos[s];
+                    const int at = atomicAdd(&sh.nchanged, 1);
+                    if (at < 2 * NB) sh.changed[at] = p;
+                }
+            __syncthreads();
+            const int nch = min(sh.nchanged, 2 * NB);
+            if (t < nch)
+            {
+                const int p = sh.changed[t];
+                sh.chg[k0 / NB][t] = (short)p;
+                sh.src[k0 / NB][t] = sh.perm[p];
+            }
+            if (t == 0) sh.nchg[k0 / NB] = nch;
+            // (1) row interchanges on the panel and trailing columns: a warp per column,
+            //     SWAP_COLS columns in flight, every source read before any destination is
+            //     written
+            {
+                int p0 = -1, p1 = -1, s0 = 0, s1 = 0;
+                if (lane < nch)
+                {
+                    p0 = sh.changed[lane];
+                    s0 = sh.perm[p0];
+                }
+                if (lane + 32 < nch)
+                {
+                    p1 = sh.changed[lane + 32];
+                    s1 = sh.perm[p1];
+                }
+                for (int base = warp * SWAP_COLS; base < m; base += NW * SWAP_COLS)
+                {
+                    float v0[SWAP_COLS], v1[SWAP_COLS];
 #pragma unroll
-                    for (int c = 0; c < NB; ++c)
-                        if (c < w) A[(int64_t)(k0 + c) * lda + k0 + p] = r[s][c];
-                    sh.perm[p] = (short)i;
+                    for (int c = 0; c < SWAP_COLS; ++c)
+                    {
+                        const float *col = A + (int64_t)(k0 + min(base + c, m - 1)) * lda + k0;
+                        v0[c] = p0 >= 0 ? col[s0] : 0.0f;
+                        v1[c] = p1 >= 0 ? col[s1] : 0.0f;
+                    }
+                    __syncwarp();
+#pragma unroll
+                    for (int c = 0; c < SWAP_COLS; ++c)
+                    {
+                        if (base + c < m)
+                        {
+                            float *col = A + (int64_t)(k0 + base + c) * lda + k0;
+                            if (p0 >= 0) col[p0] = v0[c];
+                            if (p1 >= 0) col[p1] = v1[c];
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            if (k0 + w >= n) break;  // last panel: no trailing columns (w == NB below)
+            // stage L from the panel, now in final order: plain FP32 L[k][p]; mixed FP32 L11
+            // and the negated BF16 split of L21 (zero-pivot columns zeroed)
+            {
+                const unsigned zm = sh.zmask;
+                const float *pan = A + (int64_t)k0 * lda + k0;
+#pragma unroll
+                for (int s = 0; s < 2; ++s)
+                {
+                    const int p = t + s * BT;
+                    if (p >= m) continue;
+                    float v[NB];
+#pragma unroll
+                    for (int c = 0; c < NB; ++c) v[c] = pan[(int64_t)c * lda + p];
                     if (MODE == 0)
                     {
 #pragma unroll
-                        for (int c = 0; c < NB; ++c) L[c * lp + p] = r[s][c];
+                        for (int c = 0; c < NB; ++c) L[c * lp + p] = v[c];
                     }
                     else if (p < NB)
                     {
 #pragma unroll
-                        for (int c = 0; c < NB; ++c) L[c * l11p + p] = r[s][c];
+                        for (int c = 0; c < NB; ++c) L[c * L11P + p] = v[c];
                     }
-                }
-            }
-            __syncthreads();  // perm, zmask and the staged L are complete
-            if (MODE != 0 && k0 + w < n)
-            {
-                const unsigned zm = sh.zmask;
-#pragma unroll
-                for (int s = 0; s < 2; ++s)
-                {
-                    const int i = t + s * BT;
-                    if (i < m && pos[s] >= NB)
+                    else
                     {
                         __nv_bfloat16 h[NB], l[NB];
 #pragma unroll
                         for (int c = 0; c < NB; ++c)
                         {
-                            const float v = ((zm >> c) & 1u) ? 0.0f : -r[s][c];
-                            split_bf16(v, h[c], l[c]);
+                            const float x = ((zm >> c) & 1u) ? 0.0f : -v[c];
+                            split_bf16(x, h[c], l[c]);
                         }
-                        uint4 *dh = reinterpret_cast<uint4 *>(lh + (size_t)pos[s] * HP);
-                        uint4 *dl = reinterpret_cast<uint4 *>(ll + (size_t)pos[s] * HP);
+                        uint4 *dh = reinterpret_cast<uint4 *>(lh + (size_t)p * HP);
+                        uint4 *dl = reinterpret_cast<uint4 *>(ll + (size_t)p * HP);
 #pragma unroll
                         for (int c = 0; c < NB; c += 8)
                         {
@@ -446,125 +625,158 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
                     }
                 }
             }
-            for (int p = t; p < m; p += BT)
-                if (sh.perm[p] != p)
-                {
-                    const int at = atomicAdd(&sh.nchanged, 1);
-                    if (at < 2 * NB) sh.changed[at] = p;
-                }
             __syncthreads();
-            if (k0 + w >= n) break;  // last panel: no trailing columns (w == NB below)
             const unsigned zmask = sh.zmask;
-            const int nch = min(sh.nchanged, 2 * NB);
-            for (int j0 = k0 + NB; j0 < n; j0 += CT)
+            const int jt = k0 + NB;   // first trailing column
+            const int ntr = n - jt;   // trailing columns
+            // (2) U12 = L11^-1 A12: a thread per column, ascending k, zero pivots skipped
+            for (int jc = t; jc < ntr; jc += BT)
             {
-                const int nc = min(CT, n - j0);
-                // (a) a warp per column: U12 rows through the permutation, moved rows in place
-                for (int jj = warp; jj < nc; jj += NW)
+                float *col = A + (int64_t)(jt + jc) * lda + k0;
+                float v[NB];
+                if (vec)
                 {
-                    float *col = A + (int64_t)(j0 + jj) * lda + k0;
-                    const float top = col[sh.perm[lane]];
-                    int p0 = -1, p1 = -1;
-                    float v0 = 0.0f, v1 = 0.0f;
-                    if (lane < nch)
+#pragma unroll
+                    for (int i = 0; i < NB; i += 4)
                     {
-                        p0 = sh.changed[lane];
-                        v0 = col[sh.perm[p0]];
+                        const float4 a = *reinterpret_cast<const float4 *>(col + i);
+                        v[i] = a.x, v[i + 1] = a.y, v[i + 2] = a.z, v[i + 3] = a.w;
                     }
-                    if (lane + 32 < nch)
-                    {
-                        p1 = sh.changed[lane + 32];
-                        v1 = col[sh.perm[p1]];
-                    }
-                    __syncwarp();
-                    if (p0 >= NB) col[p0] = v0;
-                    if (p1 >= NB) col[p1] = v1;
-                    us[lane * UP + jj] = top;
                 }
-                __syncthreads();
-                // (b) U12 = L11^-1 A12: four threads per column, thread part owns rows part + 4s
+                else
                 {
-                    const int jj = t >> 2, part = t & 3;
-                    float v[8];
 #pragma unroll
-                    for (int s = 0; s < 8; ++s) v[s] = jj < nc ? us[(part + 4 * s) * UP + jj] : 0.0f;
+                    for (int i = 0; i < NB; ++i) v[i] = col[i];
+                }
 #pragma unroll
-                    for (int k = 0; k < NB; ++k)
+                for (int k = 0; k < NB; ++k)
+                {
+                    if ((zmask >> k) & 1u) continue;  // uniform
+                    const float u = v[k];
+#pragma unroll
+                    for (int i4 = 0; i4 < NB; i4 += 4)
                     {
-                        if ((zmask >> k) & 1u) continue;  // uniform
-                        const float u = __shfl_sync(FULL, v[k >> 2], (lane & ~3) | (k & 3));
+                        if (i4 + 3 <= k) continue;
+                        const float4 l4 = *reinterpret_cast<const float4 *>(l11 + k * l11p + i4);
+                        const float lv[4] = {l4.x, l4.y, l4.z, l4.w};
 #pragma unroll
-                        for (int s = 0; s < 8; ++s)
+                        for (int e = 0; e < 4; ++e)
+                            if (i4 + e > k) v[i4 + e] = fma_rn(-lv[e], u, v[i4 + e]);
+                    }
+                }
+                if (vec)
+                {
+#pragma unroll
+                    for (int i = 0; i < NB; i += 4)
+                        *reinterpret_cast<float4 *>(col + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+                }
+                else
+                {
+#pragma unroll
+                    for (int i = 0; i < NB; ++i) col[i] = v[i];
+                }
+            }
+            __syncthreads();
+            // (3) A22 -= L21 U12 over 128 x 64 tiles (positions NB..m-1)
+            const int nct = (ntr + CT - 1) / CT;
+            {
+                float u[8];
+                u_load(A, lda, k0, jt, min(CT, ntr), vec, u);
+                u_store<MODE, TERMS>(u, us, uh, ul);
+            }
+            __syncthreads();
+            for (int ct = 0; ct < nct; ++ct)
+            {
+                const int j0 = jt + ct * CT;
+                const int nc = min(CT, n - j0);
+                const int buf = ct & 1;
+                float u[8];
+                if (ct + 1 < nct) u_load(A, lda, k0, j0 + CT, min(CT, n - j0 - CT), vec, u);
+                if (MODE == 0)
+                {
+                    const float *ub = us + (size_t)buf * NB * UP;
+                    float acc[8][4], nxt[8][4];
+                    plain_c_load(A, lda, m, k0, j0, nc, NB, vec, acc);
+                    for (int r0 = NB; r0 < m; r0 += RT)
+                    {
+                        const bool more = r0 + RT < m;
+                        if (more) plain_c_load(A, lda, m, k0, j0, nc, r0 + RT, vec, nxt);
+                        plain_c_update(acc, L, lp, r0, zmask, ub);
+                        plain_c_store(A, lda, m, k0, j0, nc, r0, vec, acc);
+                        if (more)
                         {
-                            const int i = part + 4 * s;
-                            if (i > k) v[s] = fma_rn(-L[k * l11p + i], u, v[s]);
+#pragma unroll
+                            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                                for (int j = 0; j < 4; ++j) acc[i][j] = nxt[i][j];
                         }
                     }
-                    if (jj < nc)
+                }
+                else
+                {
+                    const __nv_bfloat16 *bh = uh + (size_t)buf * CT * HP;
+                    const __nv_bfloat16 *bl = ul + (size_t)buf * CT * HP;
+                    float acc[2][4][4], nxt[2][4][4];
+                    mixed_c_load(A, lda, m, k0, j0, nc, NB, acc);
+                    for (int r0 = NB; r0 < m; r0 += RT)
                     {
+                        const bool more = r0 + RT < m;
+                        if (more) mixed_c_load(A, lda, m, k0, j0, nc, r0 + RT, nxt);
+                        mixed_c_update<TERMS>(acc, n, r0, lh, ll, bh, bl);
+                        mixed_c_store(A, lda, m, k0, j0, nc, r0, acc);
+                        if (more)
+                        {
 #pragma unroll
-                        for (int s = 0; s < 8; ++s) us[(part + 4 * s) * UP + jj] = v[s];
+                            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                                for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                                    for (int e = 0; e < 4; ++e) acc[mi][ni][e] = nxt[mi][ni][e];
+                        }
                     }
                 }
-                __syncthreads();
-                // (c) U12 to global; mixed: its BF16 split, stored [column][k]
-                for (int jj = warp; jj < nc; jj += NW) A[(int64_t)(j0 + jj) * lda + k0 + lane] = us[lane * UP + jj];
-                if (MODE != 0)
-                {
-                    for (int e = t; e < CT * (NB / 2); e += BT)
-                    {
-                        const int jj = e / (NB / 2), k = (e % (NB / 2)) * 2;
-                        const float u0 = jj < nc ? us[k * UP + jj] : 0.0f;
-                        const float u1 = jj < nc ? us[(k + 1) * UP + jj] : 0.0f;
-                        __nv_bfloat16 h0, l0, h1, l1;
-                        split_bf16(u0, h0, l0);
-                        split_bf16(u1, h1, l1);
-                        *reinterpret_cast<__nv_bfloat162 *>(uh + (size_t)jj * HP + k) = __halves2bfloat162(h0, h1);
-                        if (TERMS > 1)
-                            *reinterpret_cast<__nv_bfloat162 *>(ul + (size_t)jj * HP + k) = __halves2bfloat162(l0, l1);
-                    }
-                    __syncthreads();
-                }
-                // (d) A22 -= L21 U12 over 128-row tiles (positions NB..m-1)
-                for (int r0 = NB; r0 < m; r0 += RT)
-                {
-                    if (MODE == 0)
-                        tile_plain(A, lda, m, k0, j0, nc, r0, zmask, L, lp, us, vec);
-                    else
-                        tile_mixed<TERMS>(A, lda, m, k0, j0, nc, r0, lh, ll, uh, ul);
-                }
+                if (ct + 1 < nct)
+                    u_store<MODE, TERMS>(u, us + (size_t)(buf ^ 1) * NB * UP, uh + (size_t)(buf ^ 1) * CT * HP,
+                                         ul + (size_t)(buf ^ 1) * CT * HP);
                 __syncthreads();
             }
         }
         // Epilogue: the L columns of panel p take the row interchanges of panels p+1.. as
-        // one gather, final[pos] = stored[T[pos]], T composed from the last panel backwards.
+        // one gather, final[pos] = stored[T[pos]], T composed from the last panel backwards
+        // (T = U_{p+1}[T], U_{p+1} the identity with panel p+1's changed positions).
         const int npanel = (n + NB - 1) / NB;
         if (piv && npanel > 1)
         {
-            for (int i = t; i < n; i += BT) sh.tmap[i] = (short)i;
-            float *stage = L + (size_t)warp * MAXN;  // the L staging area is free now
+            // the staging area is free now: two maps of n shorts, then 2 n floats per warp
+            short *tmap = reinterpret_cast<short *>(dyn);
+            short *umap = tmap + ((n + 7) / 8) * 8;
+            float *stage = reinterpret_cast<float *>(umap + ((n + 7) / 8) * 8) + (size_t)warp * 2 * n;
+            for (int i = t; i < n; i += BT) tmap[i] = (short)i;
             for (int p = npanel - 2; p >= 0; --p)
             {
-                const int kq = (p + 1) * NB, wq = min(NB, n - kq);
-                for (int i = t; i < n; i += BT) sh.umap[i] = (short)i;
+                const int kq = (p + 1) * NB;
+                for (int i = t; i < n; i += BT) umap[i] = (short)i;
                 __syncthreads();
-                if (t == 0)
-                    for (int k = kq; k < kq + wq; ++k)
-                    {
-                        const int s = piv[k] - 1;
-                        const short a = sh.umap[k];
-                        sh.umap[k] = sh.umap[s];
-                        sh.umap[s] = a;
-                    }
+                if (t < sh.nchg[p + 1]) umap[kq + sh.chg[p + 1][t]] = (short)(kq + sh.src[p + 1][t]);
                 __syncthreads();
-                for (int i = kq + t; i < n; i += BT) sh.tmap[i] = sh.umap[sh.tmap[i]];
+                for (int i = kq + t; i < n; i += BT) tmap[i] = umap[tmap[i]];
                 __syncthreads();
-                for (int c = warp; c < NB; c += NW)
+                for (int c = 2 * warp; c < NB; c += 2 * NW)
                 {
-                    float *col = A + (int64_t)(p * NB + c) * lda;
-                    for (int i = kq + lane; i < n; i += 32) stage[i - kq] = col[i];
+                    float *c0 = A + (int64_t)(p * NB + c) * lda;
+                    float *c1 = c0 + lda;
+                    for (int i = kq + lane; i < n; i += 32)
+                    {
+                        stage[i - kq] = c0[i];
+                        stage[n + i - kq] = c1[i];
+                    }
                     __syncwarp();
-                    for (int i = kq + lane; i < n; i += 32) col[i] = stage[sh.tmap[i] - kq];
+                    for (int i = kq + lane; i < n; i += 32)
+                    {
+                        const int from = tmap[i] - kq;
+                        c0[i] = stage[from];
+                        c1[i] = stage[n + from];
+                    }
                     __syncwarp();
                 }
             }

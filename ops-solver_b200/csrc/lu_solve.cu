@@ -9,10 +9,10 @@
 // takes its block's 32 updates in order.
 //
 // The solution vectors stay in shared memory.  The factor is streamed from global memory
-// once: thread t owns one row of each 256-row strip and keeps that row's 32 entries of the
-// block column in registers, so a warp's loads are 128-byte coalesced column segments.  The
-// strips form one software pipeline over the whole sweep: the registers for the next strip
-// (or the next block's diagonal triangle) are loaded while the current one is applied.
+// once, as a queue of tiles (a block's 32 x 32 diagonal triangle, then its 32-column strips
+// of up to 256 rows) copied by cp.async into a three-stage shared ring: two tiles are in
+// flight while the third is applied, so the sweep runs at the copy rate rather than paying
+// the memory latency per tile.
 #include "common.cuh"
 #include "launch.h"
 
@@ -24,6 +24,10 @@ constexpr int ST = 256;  // threads per block
 constexpr int KB = 32;   // column block
 constexpr int MAX_RHS_PER_BLOCK = 8;
 
+constexpr int SR = 256;      // rows of a strip
+constexpr int SP = SR + 4;   // stage pitch (floats)
+constexpr int STAGES = 3;    // tiles in flight: the one in use and two being copied
+
 // One unit of the sweep: the diagonal triangle of block `blk` (strip < 0) or a strip of up
 // to 256 rows off the diagonal block (below it going forward, above it going backward).
 struct Task
@@ -33,35 +37,12 @@ struct Task
 };
 
 template <bool FORWARD>
-__device__ __forceinline__ int task_row(int n, Task task)
-{
-    const int t = threadIdx.x, lane = t & 31;
-    const int kb = task.blk * KB;
-    const int w = min(KB, n - kb);
-    if (task.strip < 0) return (t < 32 && lane < w) ? kb + lane : -1;
-    const int r = task.strip * ST + t;
-    if (FORWARD) return kb + w + r < n ? kb + w + r : -1;
-    return r < kb ? r : -1;
-}
-
-// Thread t's registers for a task: the entries of its row in the block column.
-template <bool FORWARD>
-__device__ __forceinline__ void load_task(const float *A, int lda, int n, Task task, float (&v)[KB])
-{
-    const int kb = task.blk * KB;
-    const int w = min(KB, n - kb);
-    const int row = task_row<FORWARD>(n, task);
-#pragma unroll
-    for (int k = 0; k < KB; ++k) v[k] = (row >= 0 && k < w) ? A[(int64_t)(kb + k) * lda + row] : 0.0f;
-}
-
-template <bool FORWARD>
 __device__ __forceinline__ int strips(int n, int blk)
 {
     const int kb = blk * KB;
     const int w = min(KB, n - kb);
     const int rows = FORWARD ? n - kb - w : kb;
-    return (rows + ST - 1) / ST;
+    return (rows + SR - 1) / SR;
 }
 
 // Advances to the next task of the sweep; false past the end.
@@ -78,41 +59,120 @@ __device__ __forceinline__ bool next_task(int n, int nblk, Task &task)
     return FORWARD ? task.blk < nblk : task.blk >= 0;
 }
 
-// Thread t < 32 (warp 0) holds row kb + t of a diagonal triangle: publish it.
-__device__ __forceinline__ void store_triangle(float (*tri)[KB + 1], const float (&v)[KB])
+// First row and row count of a task's tile (columns kb .. kb + w - 1).
+template <bool FORWARD>
+__device__ __forceinline__ void task_rows(int n, Task task, int &row0, int &rows)
 {
-    if (threadIdx.x < 32)
+    const int kb = task.blk * KB;
+    const int w = min(KB, n - kb);
+    if (task.strip < 0)
     {
-#pragma unroll
-        for (int k = 0; k < KB; ++k) tri[k][threadIdx.x] = v[k];
+        row0 = kb;
+        rows = w;
+    }
+    else if (FORWARD)
+    {
+        row0 = kb + w + task.strip * SR;
+        rows = min(SR, n - row0);
+    }
+    else
+    {
+        row0 = task.strip * SR;
+        rows = min(SR, kb - row0);
+    }
+}
+
+__device__ __forceinline__ void cp_async16(float *dst, const float *src, int bytes)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async4(float *dst, const float *src, int bytes)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Starts the copy of a task's tile into stage[k][r] (k < 32 columns, r < rows); entries past
+// the tile are zero-filled.  vec: 16-byte copies (the matrix is 16-byte aligned, lda % 4 == 0).
+template <bool FORWARD>
+__device__ __forceinline__ void issue_task(const float *A, int lda, int n, Task task, float *stage, bool vec)
+{
+    int row0, rows;
+    task_rows<FORWARD>(n, task, row0, rows);
+    const int kb = task.blk * KB;
+    const int w = min(KB, n - kb);
+    const int span = task.strip < 0 ? KB : SR;  // rows to fill
+    if (vec)
+    {
+        const int per = span / 4;  // 16-byte chunks per column
+        for (int c = threadIdx.x; c < KB * per; c += ST)
+        {
+            const int k = c / per, r = (c % per) * 4;
+            const int valid = k < w ? max(0, min(4, rows - r)) : 0;
+            const float *src = valid ? A + (int64_t)(kb + k) * lda + row0 + r : A;
+            cp_async16(stage + k * SP + r, src, valid * 4);
+        }
+    }
+    else
+    {
+        for (int c = threadIdx.x; c < KB * span; c += ST)
+        {
+            const int k = c / span, r = c % span;
+            const bool valid = k < w && r < rows;
+            const float *src = valid ? A + (int64_t)(kb + k) * lda + row0 + r : A;
+            cp_async4(stage + k * SP + r, src, valid ? 4 : 0);
+        }
     }
 }
 
 template <bool FORWARD>
-__device__ void sweep(const float *A, int lda, int n, float *x, int nr, float (*tri)[KB][KB + 1])
+__device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *stages, bool vec)
 {
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int nblk = (n + KB - 1) / KB;
-    Task cur{FORWARD ? 0 : nblk - 1, -1};
-    float v[KB], nv[KB];
-    load_task<FORWARD>(A, lda, n, cur, v);
-    store_triangle(tri[cur.blk & 1], v);
-    __syncthreads();
-    bool more = true;
-    while (more)
+    // the task queue: q[0] is applied while the next STAGES - 1 are in flight
+    Task q[STAGES];
+    bool live[STAGES];
+    q[0] = Task{FORWARD ? 0 : nblk - 1, -1};
+    live[0] = true;
+#pragma unroll
+    for (int i = 1; i < STAGES; ++i)
     {
-        Task nxt = cur;
-        more = next_task<FORWARD>(n, nblk, nxt);
-        if (more) load_task<FORWARD>(A, lda, n, nxt, nv);
+        q[i] = q[i - 1];
+        live[i] = live[i - 1] && next_task<FORWARD>(n, nblk, q[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < STAGES - 1; ++i)
+    {
+        if (live[i]) issue_task<FORWARD>(A, lda, n, q[i], stages + (size_t)i * KB * SP, vec);
+        cp_commit();
+    }
+    int slot = 0;
+    while (live[0])
+    {
+        // refill: the task STAGES - 1 ahead goes to the stage freed by the previous task
+        if (live[STAGES - 1])
+            issue_task<FORWARD>(A, lda, n, q[STAGES - 1],
+                                stages + (size_t)((slot + STAGES - 1) % STAGES) * KB * SP, vec);
+        cp_commit();
+        cp_wait<STAGES - 1>();  // this task's tile has landed (for this thread's copies)
+        __syncthreads();        // ... and for everyone's
+        const float *tile = stages + (size_t)slot * KB * SP;
+        const Task cur = q[0];
         const int kb = cur.blk * KB;
         const int w = min(KB, n - kb);
         if (cur.strip < 0)
         {
-            // diagonal triangle (published in shared memory): warp r solves right-hand side
-            // r, lane i on row kb + i
+            // diagonal triangle: warp r solves right-hand side r, lane i on row kb + i
             if (warp < nr)
             {
-                const float(*d)[KB + 1] = tri[cur.blk & 1];
                 float *xr = x + (size_t)warp * n;
                 float xv = lane < w ? xr[kb + lane] : 0.0f;
                 if (FORWARD)
@@ -121,7 +181,7 @@ __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float (*
                     for (int k = 0; k < KB; ++k)
                     {
                         const float xk = __shfl_sync(0xffffffffu, xv, k);
-                        if (lane > k && lane < w) xv = fma_rn(-d[k][lane], xk, xv);
+                        if (lane > k && lane < w) xv = fma_rn(-tile[k * SP + lane], xk, xv);
                     }
                 }
                 else
@@ -131,9 +191,9 @@ __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float (*
                     {
                         if (k < w)
                         {
-                            if (lane == k) xv = div_rn(xv, d[k][lane]);
+                            if (lane == k) xv = div_rn(xv, tile[k * SP + lane]);
                             const float xk = __shfl_sync(0xffffffffu, xv, k);
-                            if (lane < k) xv = fma_rn(-d[k][lane], xk, xv);
+                            if (lane < k) xv = fma_rn(-tile[k * SP + lane], xk, xv);
                         }
                     }
                 }
@@ -142,37 +202,45 @@ __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float (*
         }
         else
         {
-            const int row = task_row<FORWARD>(n, cur);
-            if (row >= 0)
+            int row0, rows;
+            task_rows<FORWARD>(n, cur, row0, rows);
+            if (t < rows)
             {
-                for (int q = 0; q < nr; ++q)
+                const int row = row0 + t;
+                for (int r = 0; r < nr; ++r)
                 {
-                    float *xr = x + (size_t)q * n;
+                    float *xr = x + (size_t)r * n;
                     float acc = xr[row];
                     if (FORWARD)
                     {
 #pragma unroll
                         for (int k = 0; k < KB; ++k)
-                            if (k < w) acc = fma_rn(-v[k], xr[kb + k], acc);
+                            if (k < w) acc = fma_rn(-tile[k * SP + t], xr[kb + k], acc);
                     }
                     else
                     {
 #pragma unroll
                         for (int k = KB - 1; k >= 0; --k)
-                            if (k < w) acc = fma_rn(-v[k], xr[kb + k], acc);
+                            if (k < w) acc = fma_rn(-tile[k * SP + t], xr[kb + k], acc);
                     }
                     xr[row] = acc;
                 }
             }
         }
-        // the next diagonal triangle goes to the other buffer (the current one may be in use)
-        if (more && nxt.strip < 0) store_triangle(tri[nxt.blk & 1], nv);
-        // a diagonal solve feeds its strips, and a block's strips feed the next diagonal
+        // a diagonal solve feeds its strips, a block's strips feed the next diagonal, and
+        // this stage is refilled two iterations on
         __syncthreads();
 #pragma unroll
-        for (int k = 0; k < KB; ++k) v[k] = nv[k];
-        cur = nxt;
+        for (int i = 0; i < STAGES - 1; ++i)
+        {
+            q[i] = q[i + 1];
+            live[i] = live[i + 1];
+        }
+        q[STAGES - 1] = q[STAGES - 2];
+        live[STAGES - 1] = live[STAGES - 2] && next_task<FORWARD>(n, nblk, q[STAGES - 1]);
+        slot = (slot + 1) % STAGES;
     }
+    cp_wait<0>();
 }
 
 __global__ void __launch_bounds__(ST, 2) getrs_blocked_kernel(float *a_single, float *const *a_table, int a_first,
@@ -181,8 +249,9 @@ __global__ void __launch_bounds__(ST, 2) getrs_blocked_kernel(float *a_single, f
                                                             int ldb, int nrhs, int count, int RHS, int *info,
                                                             const int *skip)
 {
-    extern __shared__ float x[];  // RHS x n
-    __shared__ float tri[2][KB][KB + 1];
+    extern __shared__ __align__(16) float dyn[];
+    float *stages = dyn;                          // STAGES x KB x SP
+    float *x = dyn + (size_t)STAGES * KB * SP;    // RHS x n
     __shared__ int bad;
     const int groups = (nrhs + RHS - 1) / RHS;
     const int t = threadIdx.x;
@@ -240,8 +309,9 @@ __global__ void __launch_bounds__(ST, 2) getrs_blocked_kernel(float *a_single, f
             }
         }
         __syncthreads();
-        sweep<true>(A, lda, n, x, nr, tri);
-        sweep<false>(A, lda, n, x, nr, tri);
+        const bool vec = (reinterpret_cast<uintptr_t>(A) & 15u) == 0 && (lda & 3) == 0;
+        sweep<true>(A, lda, n, x, nr, stages, vec);
+        sweep<false>(A, lda, n, x, nr, stages, vec);
         for (int e = t; e < nr * n; e += ST)
         {
             const int r = e / n, i = e % n;
@@ -278,12 +348,14 @@ __global__ void permutation_kernel(const int *ipiv, int *perm, int n, int count)
 cudaError_t launch_getrs_blocked(const RealBatch &a, const int *ipiv, const int *perm, const RealBatch &b, int nrhs,
                                  int *info, const int *skip, cudaStream_t stream)
 {
-    const size_t budget = 100 * 1024 / sizeof(float);  // two blocks per SM
-    int rpb = (int)(budget / (size_t)a.n);
+    const size_t stage_floats = (size_t)STAGES * KB * SP;
+    // two blocks per SM when the vectors fit beside the ring, else one
+    int rpb = (int)((110 * 1024 / sizeof(float) - stage_floats) / (size_t)a.n);
+    if (rpb < 1) rpb = (int)((220 * 1024 / sizeof(float) - stage_floats) / (size_t)a.n);
     if (rpb > MAX_RHS_PER_BLOCK) rpb = MAX_RHS_PER_BLOCK;
     if (rpb > nrhs) rpb = nrhs;
     if (rpb < 1) return cudaErrorInvalidValue;
-    const size_t smem = (size_t)rpb * a.n * sizeof(float);
+    const size_t smem = (stage_floats + (size_t)rpb * a.n) * sizeof(float);
     cudaFuncSetAttribute(getrs_blocked_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int groups = (nrhs + rpb - 1) / rpb;
     int64_t jobs = (int64_t)a.count * groups;

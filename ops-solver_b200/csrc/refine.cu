@@ -17,33 +17,13 @@ namespace ops_solver
 {
 namespace
 {
-constexpr int RT = 256;  // residual block: 64 rows x 4 column quarters
-constexpr int RQ = 4;
+constexpr int RT = 256;  // residual block
 
 __device__ __forceinline__ double warp_max_d(double v)
 {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
-}
-
-// Block maximum of four values at once (one barrier pair).
-__device__ void block_max4(double (&v)[4], double *red)
-{
-#pragma unroll
-    for (int e = 0; e < 4; ++e) v[e] = warp_max_d(v[e]);
-    if ((threadIdx.x & 31) == 0)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) red[e * (RT / 32) + (threadIdx.x >> 5)] = v[e];
-    __syncthreads();
-#pragma unroll
-    for (int e = 0; e < 4; ++e)
-    {
-        double r = red[e * (RT / 32)];
-        for (int w = 1; w < RT / 32; ++w) r = fmax(r, red[e * (RT / 32) + w]);
-        v[e] = r;
-    }
-    __syncthreads();
 }
 
 __global__ void ir_init_kernel(const IrState s, const float *const *b, int ldb, const int *factor_info, int n,
@@ -80,85 +60,188 @@ __global__ void ir_update_kernel(const IrState s, int assign, int n, int nrhs, i
     }
 }
 
-// One block per running job; rows go in chunks of 64.  Thread (g = t % 64, c = t / 64)
-// forms the partial sum of row i0 + g over column quarter c; the four partials are added in
-// a fixed order, so the result does not depend on scheduling.
+// One block per (matrix, group of up to RG right-hand sides), so A is read once per group.
+// Thread (g = t % 128, c = t / 128) owns rows i0 + 4g .. +3 of a 512-row pass and column half
+// c; its four row chains are independent FP64 fused multiply-adds over ascending columns, the
+// loads are 16-byte vectors when the layout allows.  The two halves are added in a fixed
+// order (c = 0 then c = 1), so the result does not depend on scheduling.
+constexpr int RG = 4;
 __global__ void __launch_bounds__(RT) ir_residual_kernel(const IrState s, const float *const *a, int lda,
                                                           const float *const *b, int ldb, int n, int nrhs, int count,
                                                           double tol)
 {
-    extern __shared__ double xs[];  // n
-    __shared__ double part[RQ][RT / RQ], rowsum[RQ][RT / RQ];
-    __shared__ double red[4 * (RT / 32)];
-    const int t = threadIdx.x;
-    const int g = t % (RT / RQ), c = t / (RT / RQ);
-    const int span = (n + RQ - 1) / RQ;
-    const int j0 = min(n, c * span), j1 = min(n, j0 + span);
-    for (int64_t job = blockIdx.x; job < (int64_t)count * nrhs; job += gridDim.x)
+    extern __shared__ double xs[];               // RG x n
+    __shared__ double part[RG][512], rsum[512];  // the c = 1 half's partial sums
+    __shared__ double red[(2 + 3 * RG) * (RT / 32)];
+    __shared__ int decide[RG];                   // per right-hand side: 1 accept, 2 first, 0 take back, 3 idle
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int g = t & 127, c = t >> 7;
+    const int groups = (nrhs + RG - 1) / RG;
+    const int half = (n + 1) / 2;
+    const int jb = c == 0 ? 0 : half, je = c == 0 ? half : n;
+    for (int64_t job = blockIdx.x; job < (int64_t)count * groups; job += gridDim.x)
     {
-        if (s.state[job] != IR_RUNNING) continue;  // uniform
-        const int64_t q = job / nrhs;
-        const int r = (int)(job % nrhs);
+        const int64_t q = job / groups;
+        const int r0 = (int)(job % groups) * RG;
+        const int nr = min(RG, nrhs - r0);
+        bool any = false;
+        for (int r = 0; r < nr; ++r) any = any || s.state[q * nrhs + r0 + r] == IR_RUNNING;
+        if (!any) continue;  // uniform
         const float *A = slot(a, q);
-        const float *bq = slot(b, q) + (int64_t)r * ldb;
-        double *x = s.x64 + job * (int64_t)n;
-        float *rv = s.r32 + job * (int64_t)n;
-        double m[4] = {0.0, 0.0, 0.0, 0.0};  // max |r|, ||A||_inf, max |b|, max |x|
-        for (int i = t; i < n; i += RT)
+        const float *B = slot(b, q);
+        const bool vec = (reinterpret_cast<uintptr_t>(A) & 15u) == 0 && (lda & 3) == 0;
+        double mx[RG];
+#pragma unroll
+        for (int r = 0; r < RG; ++r) mx[r] = 0.0;
+        for (int e = t; e < nr * n; e += RT)
         {
-            xs[i] = x[i];
-            m[3] = fmax(m[3], fabs(xs[i]));
+            const int r = e / n, i = e % n;
+            const double v = s.x64[(q * nrhs + r0 + r) * (int64_t)n + i];
+            xs[e] = v;
+#pragma unroll
+            for (int rr = 0; rr < RG; ++rr)
+                if (rr == r) mx[rr] = fmax(mx[rr], fabs(v));
         }
         __syncthreads();
-        const double prev = s.berr[job];
-        for (int i0 = 0; i0 < n; i0 += RT / RQ)
+        double mr[RG], mb[RG], ma = 0.0;
+#pragma unroll
+        for (int r = 0; r < RG; ++r) mr[r] = mb[r] = 0.0;
+        for (int i0 = 0; i0 < n; i0 += 512)
         {
-            const int i = i0 + g;
-            double acc = 0.0, arow = 0.0;
-            if (i < n)
+            const int ib = i0 + 4 * g;
+            double acc[RG][4], arow[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int r = 0; r < RG; ++r)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) acc[r][e] = 0.0;
+            if (ib < n)
             {
-                const float *col = A + i;
-#pragma unroll 8
-                for (int j = j0; j < j1; ++j)
+                const float *base = A + ib;
+                const bool full = vec && ib + 3 < n;
+#pragma unroll 4
+                for (int j = jb; j < je; ++j)
                 {
-                    const double aij = (double)col[(int64_t)j * lda];
-                    acc = fma(aij, xs[j], acc);
-                    arow += fabs(aij);
+                    float v[4];
+                    if (full)
+                    {
+                        const float4 f = __ldg(reinterpret_cast<const float4 *>(base + (int64_t)j * lda));
+                        v[0] = f.x, v[1] = f.y, v[2] = f.z, v[3] = f.w;
+                    }
+                    else
+                    {
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) v[e] = ib + e < n ? base[(int64_t)j * lda + e] : 0.0f;
+                    }
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) arow[e] += fabs((double)v[e]);
+#pragma unroll
+                    for (int r = 0; r < RG; ++r)
+                    {
+                        if (r < nr)
+                        {
+                            const double xj = xs[r * n + j];
+#pragma unroll
+                            for (int e = 0; e < 4; ++e) acc[r][e] = fma((double)v[e], xj, acc[r][e]);
+                        }
+                    }
                 }
             }
-            part[c][g] = acc;
-            rowsum[c][g] = arow;
-            __syncthreads();
-            if (c == 0 && i < n)
+            if (c == 1)
             {
-                const double ax = ((part[0][g] + part[1][g]) + part[2][g]) + part[3][g];
-                const double as = ((rowsum[0][g] + rowsum[1][g]) + rowsum[2][g]) + rowsum[3][g];
-                const double bi = (double)bq[i];
-                const double ri = bi - ax;
-                m[0] = fmax(m[0], fabs(ri));
-                m[1] = fmax(m[1], as);
-                m[2] = fmax(m[2], fabs(bi));
-                x[i] = ri;  // x64 holds r until the decision below (xs keeps x)
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                {
+                    rsum[4 * g + e] = arow[e];
+#pragma unroll
+                    for (int r = 0; r < RG; ++r) part[r][4 * g + e] = acc[r][e];
+                }
+            }
+            __syncthreads();
+            if (c == 0)
+            {
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                {
+                    const int i = ib + e;
+                    if (i < n)
+                    {
+                        ma = fmax(ma, arow[e] + rsum[4 * g + e]);
+#pragma unroll
+                        for (int r = 0; r < RG; ++r)
+                        {
+                            if (r < nr)
+                            {
+                                const double bi = (double)B[(int64_t)(r0 + r) * ldb + i];
+                                const double ri = bi - (acc[r][e] + part[r][4 * g + e]);
+                                mr[r] = fmax(mr[r], fabs(ri));
+                                mb[r] = fmax(mb[r], fabs(bi));
+                                // x64 holds r until the decision below (xs keeps x)
+                                s.x64[(q * nrhs + r0 + r) * (int64_t)n + i] = ri;
+                            }
+                        }
+                    }
+                }
             }
             __syncthreads();
         }
-        block_max4(m, red);
-        const double den = m[1] * m[3] + m[2];
-        const double berr = den > 0.0 ? m[0] / den : 0.0;
-        const bool better = berr < prev;        // false for a NaN berr
-        const bool first = !(prev < HUGE_VAL);  // x is the first solve: nothing to take back
-        for (int i = t; i < n; i += RT)
+        // block maxima: ||A||_inf, then max |r|, max |b|, max |x| per right-hand side
         {
-            const double ri = x[i];
-            if (better) rv[i] = (float)ri;
-            x[i] = better || first ? xs[i] : xs[i] - (double)rv[i];  // else: the last correction back
+            double v[2 + 3 * RG];
+            v[0] = ma;
+            v[1] = 0.0;
+#pragma unroll
+            for (int r = 0; r < RG; ++r)
+            {
+                v[2 + r] = mr[r];
+                v[2 + RG + r] = mb[r];
+                v[2 + 2 * RG + r] = mx[r];
+            }
+#pragma unroll
+            for (int e = 0; e < 2 + 3 * RG; ++e)
+            {
+                const double x = warp_max_d(v[e]);
+                if (lane == 0) red[e * (RT / 32) + warp] = x;
+            }
+            __syncthreads();
+            if (t < nr)
+            {
+                double m4[4];
+                const int idx[4] = {2 + t, 0, 2 + RG + t, 2 + 2 * RG + t};
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                {
+                    double x = red[idx[k] * (RT / 32)];
+                    for (int w = 1; w < RT / 32; ++w) x = fmax(x, red[idx[k] * (RT / 32) + w]);
+                    m4[k] = x;
+                }
+                const int64_t job_r = q * nrhs + r0 + t;
+                const double den = m4[1] * m4[3] + m4[2];
+                const double berr = den > 0.0 ? m4[0] / den : 0.0;
+                const double prev = s.berr[job_r];
+                const bool better = berr < prev;        // false for a NaN berr
+                const bool first = !(prev < HUGE_VAL);  // x is the first solve: nothing to take back
+                if (s.state[job_r] != IR_RUNNING)
+                    decide[t] = 3;  // not refined in this pass: x stays as it was
+                else
+                {
+                    decide[t] = better ? 1 : (first ? 2 : 0);
+                    if (better || first) s.berr[job_r] = berr;
+                    if (!better && !first) s.iters[job_r] -= 1;
+                    s.state[job_r] = !better ? IR_STALLED
+                                             : (berr <= tol ? IR_CONVERGED
+                                                            : (berr > 0.5 * prev ? IR_STALLED : IR_RUNNING));
+                }
+            }
+            __syncthreads();
         }
-        if (t == 0)
+        for (int e = t; e < nr * n; e += RT)
         {
-            if (better || first) s.berr[job] = berr;
-            if (!better && !first) s.iters[job] -= 1;
-            s.state[job] = !better ? IR_STALLED
-                                   : (berr <= tol ? IR_CONVERGED : (berr > 0.5 * prev ? IR_STALLED : IR_RUNNING));
+            const int r = e / n, i = e % n;
+            const int64_t off = (q * nrhs + r0 + r) * (int64_t)n + i;
+            const int d = decide[r];
+            if (d == 1) s.r32[off] = (float)s.x64[off];
+            // accept, first or idle: x stays; take back: x minus the last correction
+            s.x64[off] = d == 0 ? xs[e] - (double)s.r32[off] : xs[e];
         }
         __syncthreads();
     }
@@ -197,7 +280,7 @@ __global__ void ir_finish_kernel(const IrState s, float *const *xout, int ldx, i
 unsigned grid(int64_t jobs) { return (unsigned)(jobs < 148 * 8 ? (jobs < 1 ? 1 : jobs) : 148 * 8); }
 }  // namespace
 
-size_t ir_residual_smem(int n) { return (size_t)n * sizeof(double); }
+size_t ir_residual_smem(int n) { return (size_t)RG * n * sizeof(double); }
 
 cudaError_t launch_ir_init(const IrState &s, const float *const *b, int ldb, const int *factor_info, int n, int nrhs,
                            int count, cudaStream_t stream)
@@ -218,7 +301,8 @@ cudaError_t launch_ir_residual(const IrState &s, const float *const *a, int lda,
     const size_t smem = ir_residual_smem(n);
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
     cudaFuncSetAttribute(ir_residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    ir_residual_kernel<<<grid((int64_t)count * nrhs), RT, smem, stream>>>(s, a, lda, b, ldb, n, nrhs, count, tol);
+    const int64_t groups = (nrhs + RG - 1) / RG;
+    ir_residual_kernel<<<grid((int64_t)count * groups), RT, smem, stream>>>(s, a, lda, b, ldb, n, nrhs, count, tol);
     return cudaGetLastError();
 }
 
