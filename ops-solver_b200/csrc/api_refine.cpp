@@ -136,11 +136,20 @@ extern "C" aclsolverStatus_t aclsolverSgesvIrBatched(aclsolverHandle_t handle, a
     };
     cudaError_t e = launch_strided_table(lu_table, lu, (int64_t)n * n, batchSize, st);
     if (e == cudaSuccess) e = launch_strided_table(r_table, s.r32, (int64_t)n * nrhs, batchSize, st);
-    if (e == cudaSuccess) e = launch_copy_matrices(src, fac, n, st);
     if (e == cudaSuccess)
-        e = n <= SMALL_N ? launch_getrf_small(fac, n, ipiv, infoArray, st)
-                         : launch_getrf_blocked(fac, ipiv, infoArray, mode, st);
-    if (e == cudaSuccess && n > SMALL_N) e = launch_permutation(ipiv, perm, n, batchSize, st);
+    {
+        if (n <= SMALL_N)
+        {
+            e = launch_copy_matrices(src, fac, n, st);
+            if (e == cudaSuccess) e = launch_getrf_small(fac, n, ipiv, infoArray, st);
+        }
+        else
+        {
+            // the factorisation copies A into the workspace itself and reports the composed
+            // row permutation used by the solves
+            e = launch_getrf_blocked(fac, ipiv, infoArray, mode, st, src.table, lda, perm);
+        }
+    }
     if (e == cudaSuccess) e = launch_ir_init(s, Barray, ldb, infoArray, n, nrhs, batchSize, st);
     if (e == cudaSuccess) e = solve(s.state);
     if (e == cudaSuccess) e = launch_ir_update(s, 1, n, nrhs, batchSize, st);

@@ -54,8 +54,11 @@ cudaError_t launch_getri_small(const RealBatch &a, const int *ipiv, const RealBa
 // Blocked LU for 64 < n <= 512 (square), one 256-thread block per matrix.  mode 0: plain
 // FP32, bit-identical to the unblocked order; 1: BF16 tensor-core trailing update; 3: split
 // BF16 (three products).  ipiv n per matrix or nullptr; info as launch_getrf_small.
+// src (optional): factor a copy of src[q] (leading dimension src_ld) into a's slot q.
+// perm (optional): n per matrix, the composed row permutation (P b = b[perm]).
 constexpr int BLOCKED_MAX_N = 512;
-cudaError_t launch_getrf_blocked(const RealBatch &a, int *ipiv, int *info, int mode, cudaStream_t stream);
+cudaError_t launch_getrf_blocked(const RealBatch &a, int *ipiv, int *info, int mode, cudaStream_t stream,
+                                 const float *const *src = nullptr, int src_ld = 0, int *perm = nullptr);
 // Blocked LU solve (trans 0) for 64 < n <= 8192.  Row interchanges from ipiv (LAPACK form,
 // applied in order) or, when perm is given, from the permutation perm (P b = b[perm], see
 // launch_permutation); both may be null.  `skip` (nullptr = none): per (matrix,

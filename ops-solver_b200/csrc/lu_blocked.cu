@@ -483,7 +483,8 @@ __device__ __forceinline__ void u_store(const float (&u)[8], float *us, __nv_bfl
 // ---------------------------------------------------------------------------------------
 template <int MODE>  // 0 plain FP32, 1 BF16, 3 split BF16 (three products)
 __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, float *const *table, int first, int n,
-                                                               int lda, int *ipiv, int *info, int count)
+                                                               int lda, int *ipiv, int *info, int count,
+                                                               const float *const *src, int src_ld, int *perm_out)
 {
     constexpr int TERMS = MODE == 1 ? 1 : 3;
     extern __shared__ __align__(16) unsigned char dyn[];
@@ -510,6 +511,36 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
         }
         int *piv = ipiv ? ipiv + q * n : nullptr;
         const bool vec = (reinterpret_cast<uintptr_t>(A) & 15u) == 0 && (lda & 3) == 0;
+        if (src)
+        {
+            // out of place: the matrix is first copied from its source slot
+            const float *S = slot(src, q);
+            if (!S)
+            {
+                if (t == 0) info[q] = -2;
+                continue;
+            }
+            const bool v4 = vec && (reinterpret_cast<uintptr_t>(S) & 15u) == 0 && (src_ld & 3) == 0 && (n & 3) == 0;
+            if (v4)
+            {
+                const int per = n / 4;
+                for (int e = t; e < n * per; e += BT)
+                {
+                    const int c = e / per, r4 = (e % per) * 4;
+                    *reinterpret_cast<float4 *>(A + (int64_t)c * lda + r4) =
+                        __ldg(reinterpret_cast<const float4 *>(S + (int64_t)c * src_ld + r4));
+                }
+            }
+            else
+            {
+                for (int e = t; e < n * n; e += BT)
+                {
+                    const int c = e / n, r = e % n;
+                    A[(int64_t)c * lda + r] = S[(int64_t)c * src_ld + r];
+                }
+            }
+            __syncthreads();
+        }
         if (t == 0) sh.state = 0;
         for (int k0 = 0; k0 < n; k0 += NB)
         {
@@ -741,6 +772,29 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
                 __syncthreads();
             }
         }
+        const int npanel_all = (n + NB - 1) / NB;
+        if (perm_out && piv)
+        {
+            // the composed permutation: position i of the factors holds original row P[i]
+            short *P = reinterpret_cast<short *>(dyn);
+            for (int i = t; i < n; i += BT) P[i] = (short)i;
+            for (int p = 0; p < npanel_all; ++p)
+            {
+                __syncthreads();
+                const int kp = p * NB;
+                short v = 0;
+                if (t < sh.nchg[p]) v = P[kp + sh.src[p][t]];
+                __syncthreads();
+                if (t < sh.nchg[p]) P[kp + sh.chg[p][t]] = v;
+            }
+            __syncthreads();
+            for (int i = t; i < n; i += BT) perm_out[q * n + i] = P[i];
+            __syncthreads();
+        }
+        else if (perm_out)
+        {
+            for (int i = t; i < n; i += BT) perm_out[q * n + i] = i;
+        }
         // Epilogue: the L columns of panel p take the row interchanges of panels p+1.. as
         // one gather, final[pos] = stored[T[pos]], T composed from the last panel backwards
         // (T = U_{p+1}[T], U_{p+1} the identity with panel p+1's changed positions).
@@ -788,7 +842,8 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
 }
 
 template <int MODE>
-cudaError_t launch_mode(const RealBatch &a, int *ipiv, int *info, cudaStream_t stream)
+cudaError_t launch_mode(const RealBatch &a, int *ipiv, int *info, const float *const *src, int src_ld, int *perm,
+                        cudaStream_t stream)
 {
     const size_t smem = dyn_bytes(a.n, MODE);
     cudaError_t e = cudaFuncSetAttribute(getrf_blocked_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -797,22 +852,23 @@ cudaError_t launch_mode(const RealBatch &a, int *ipiv, int *info, cudaStream_t s
     int64_t blocks = a.count < 148 * 2 ? a.count : 148 * 2;
     if (blocks < 1) blocks = 1;
     getrf_blocked_kernel<MODE><<<(unsigned)blocks, BT, smem, stream>>>(a.single, a.table, a.first, a.n, a.ld, ipiv,
-                                                                       info, a.count);
+                                                                       info, a.count, src, src_ld, perm);
     return cudaGetLastError();
 }
 }  // namespace
 
-cudaError_t launch_getrf_blocked(const RealBatch &a, int *ipiv, int *info, int mode, cudaStream_t stream)
+cudaError_t launch_getrf_blocked(const RealBatch &a, int *ipiv, int *info, int mode, cudaStream_t stream,
+                                 const float *const *src, int src_ld, int *perm)
 {
     if (a.n > MAXN || a.n < 1) return cudaErrorInvalidValue;
     switch (mode)
     {
         case 0:
-            return launch_mode<0>(a, ipiv, info, stream);
+            return launch_mode<0>(a, ipiv, info, src, src_ld, perm, stream);
         case 1:
-            return launch_mode<1>(a, ipiv, info, stream);
+            return launch_mode<1>(a, ipiv, info, src, src_ld, perm, stream);
         default:
-            return launch_mode<3>(a, ipiv, info, stream);
+            return launch_mode<3>(a, ipiv, info, src, src_ld, perm, stream);
     }
 }
 

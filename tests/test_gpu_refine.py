@@ -158,3 +158,36 @@ def test_argument_errors(handle, field, value, arg):
     assert st == aclsolver.INVALID_VALUE
     got = info.cpu().numpy()
     assert got[0] == -arg
+
+
+@pytest.mark.parametrize("n", [96, 512])
+def test_sgetrf_batched_mixed(handle, n):
+    """FP32 precision is aclsolverSgetrfBatched bit for bit; the split-BF16 factors reproduce
+    P A = L U to about FP32 accuracy."""
+    lib = aclsolver.library()
+    a = conditioned_batch(3, n, 1e3, seed=n)
+    lu, wpiv, winfo = oracle.sgetrf_batched(a)
+    for precision in (aclsolver.FACTOR_FP32, aclsolver.FACTOR_BF16X3):
+        dm = DeviceMatrices(a, ld=n + 2)
+        piv = torch.zeros(3 * n, dtype=torch.int32, device="cuda")
+        info = info_buffer(3)
+        st = lib.aclsolverSgetrfBatchedMixed(handle.value, precision, n, dm.table_ptr, dm.ld, piv.data_ptr(),
+                                            info.data_ptr(), 3)
+        handle.stream.synchronize()
+        assert st == aclsolver.SUCCESS and np.all(info.cpu().numpy() == 0)
+        got = dm.read()
+        ipiv = piv.cpu().numpy().reshape(3, n)
+        if precision == aclsolver.FACTOR_FP32:
+            assert np.array_equal(ipiv, wpiv)
+            assert same_bits(got, lu), first_mismatch(got, lu)
+        else:
+            for q in range(3):
+                L = np.tril(got[q].astype(np.float64), -1) + np.eye(n)
+                U = np.triu(got[q].astype(np.float64))
+                pa = a[q].astype(np.float64).copy()
+                for k in range(n):
+                    r = ipiv[q][k] - 1
+                    if r != k:
+                        pa[[k, r]] = pa[[r, k]]
+                rel = np.abs(L @ U - pa).max() / np.abs(a[q]).max()
+                assert rel < 1e-4, rel
