@@ -12,14 +12,15 @@
 //     also carry the winning row, so the pivot row needs no second broadcast); final values
 //     go to the row's own place in A as they are produced;
 //  2. the panel and trailing columns take the panel's row interchanges (a warp per column,
-//     eight columns in flight, only the rows whose position changed) and the panel's L is
+//     32 columns in flight, only the rows whose position changed) and the panel's L is
 //     staged in shared memory (FP32, or negated BF16 hi/lo for the tensor cores);
 //  3. U12 = L11^-1 A12 (a thread per column, in registers), then A22 -= L21 U12 over
 //     128 x 64 tiles whose U12
 //     block is prefetched into the other half of a double-buffered shared tile and whose C
 //     is prefetched into registers one row tile ahead;
-//  4. after the last panel, the row interchanges of every later panel are applied to each
-//     panel's L columns in one gather per column (LAPACK's final row order).
+//  4. a second kernel, one block per (matrix, panel), applies the row interchanges of every
+//     later panel to that panel's L columns in one gather per column (LAPACK's final row
+//     order): bandwidth-bound work that no longer waits behind the factorisation.
 // Plain mode: every element takes a = fma(-l_ik, u_kj, a) in ascending k, the order of the
 // unblocked reference (real_lu.hpp:345-368, FactorLocalCore :409-448), so factors, pivots and
 // info are bit-identical to the oracle's orc_sgetrf at every n.  (The reference itself
@@ -47,7 +48,7 @@ constexpr int RT = 128;  // trailing row tile
 constexpr int UP = CT + 4;  // pitch of the FP32 U12 tile
 constexpr int HP = NB + 8;  // pitch (halfs) of the BF16 tiles: 80 bytes, ldmatrix conflict-free
 constexpr int L11P = NB + 4;
-constexpr int SWAP_COLS = 8;  // columns in flight per warp during the row interchanges
+constexpr int SWAP_COLS = 32;  // columns in flight per warp during the row interchanges
 constexpr unsigned FULL = 0xffffffffu;
 
 struct __align__(16) Shared
@@ -716,6 +717,13 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
                 u_store<MODE, TERMS>(u, us, uh, ul);
             }
             __syncthreads();
+            // the C tile of the next (column tile, row tile) pair is loaded while the current
+            // one is updated, across column-tile boundaries too
+            float acc[MODE == 0 ? 32 : 32], nxt[32];
+            if (MODE == 0)
+                plain_c_load(A, lda, m, k0, jt, min(CT, ntr), NB, vec, *reinterpret_cast<float(*)[8][4]>(acc));
+            else
+                mixed_c_load(A, lda, m, k0, jt, min(CT, ntr), NB, *reinterpret_cast<float(*)[2][4][4]>(acc));
             for (int ct = 0; ct < nct; ++ct)
             {
                 const int j0 = jt + ct * CT;
@@ -723,47 +731,33 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
                 const int buf = ct & 1;
                 float u[8];
                 if (ct + 1 < nct) u_load(A, lda, k0, j0 + CT, min(CT, n - j0 - CT), vec, u);
-                if (MODE == 0)
+                for (int r0 = NB; r0 < m; r0 += RT)
                 {
-                    const float *ub = us + (size_t)buf * NB * UP;
-                    float acc[8][4], nxt[8][4];
-                    plain_c_load(A, lda, m, k0, j0, nc, NB, vec, acc);
-                    for (int r0 = NB; r0 < m; r0 += RT)
+                    const bool more_rows = r0 + RT < m;
+                    const bool more = more_rows || ct + 1 < nct;
+                    const int nj0 = more_rows ? j0 : j0 + CT;
+                    const int nnc = min(CT, n - nj0);
+                    const int nr0 = more_rows ? r0 + RT : NB;
+                    if (MODE == 0)
                     {
-                        const bool more = r0 + RT < m;
-                        if (more) plain_c_load(A, lda, m, k0, j0, nc, r0 + RT, vec, nxt);
-                        plain_c_update(acc, L, lp, r0, zmask, ub);
-                        plain_c_store(A, lda, m, k0, j0, nc, r0, vec, acc);
-                        if (more)
-                        {
-#pragma unroll
-                            for (int i = 0; i < 8; ++i)
-#pragma unroll
-                                for (int j = 0; j < 4; ++j) acc[i][j] = nxt[i][j];
-                        }
+                        auto &ca = *reinterpret_cast<float(*)[8][4]>(acc);
+                        auto &cn = *reinterpret_cast<float(*)[8][4]>(nxt);
+                        if (more) plain_c_load(A, lda, m, k0, nj0, nnc, nr0, vec, cn);
+                        plain_c_update(ca, L, lp, r0, zmask, us + (size_t)buf * NB * UP);
+                        plain_c_store(A, lda, m, k0, j0, nc, r0, vec, ca);
                     }
-                }
-                else
-                {
-                    const __nv_bfloat16 *bh = uh + (size_t)buf * CT * HP;
-                    const __nv_bfloat16 *bl = ul + (size_t)buf * CT * HP;
-                    float acc[2][4][4], nxt[2][4][4];
-                    mixed_c_load(A, lda, m, k0, j0, nc, NB, acc);
-                    for (int r0 = NB; r0 < m; r0 += RT)
+                    else
                     {
-                        const bool more = r0 + RT < m;
-                        if (more) mixed_c_load(A, lda, m, k0, j0, nc, r0 + RT, nxt);
-                        mixed_c_update<TERMS>(acc, n, r0, lh, ll, bh, bl);
-                        mixed_c_store(A, lda, m, k0, j0, nc, r0, acc);
-                        if (more)
-                        {
+                        auto &ca = *reinterpret_cast<float(*)[2][4][4]>(acc);
+                        auto &cn = *reinterpret_cast<float(*)[2][4][4]>(nxt);
+                        if (more) mixed_c_load(A, lda, m, k0, nj0, nnc, nr0, cn);
+                        mixed_c_update<TERMS>(ca, n, r0, lh, ll, uh + (size_t)buf * CT * HP, ul + (size_t)buf * CT * HP);
+                        mixed_c_store(A, lda, m, k0, j0, nc, r0, ca);
+                    }
+                    if (more)
+                    {
 #pragma unroll
-                            for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-                                for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-                                    for (int e = 0; e < 4; ++e) acc[mi][ni][e] = nxt[mi][ni][e];
-                        }
+                        for (int i = 0; i < 32; ++i) acc[i] = nxt[i];
                     }
                 }
                 if (ct + 1 < nct)
@@ -795,49 +789,50 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
         {
             for (int i = t; i < n; i += BT) perm_out[q * n + i] = i;
         }
-        // Epilogue: the L columns of panel p take the row interchanges of panels p+1.. as
-        // one gather, final[pos] = stored[T[pos]], T composed from the last panel backwards
-        // (T = U_{p+1}[T], U_{p+1} the identity with panel p+1's changed positions).
-        const int npanel = (n + NB - 1) / NB;
-        if (piv && npanel > 1)
-        {
-            // the staging area is free now: two maps of n shorts, then 2 n floats per warp
-            short *tmap = reinterpret_cast<short *>(dyn);
-            short *umap = tmap + ((n + 7) / 8) * 8;
-            float *stage = reinterpret_cast<float *>(umap + ((n + 7) / 8) * 8) + (size_t)warp * 2 * n;
-            for (int i = t; i < n; i += BT) tmap[i] = (short)i;
-            for (int p = npanel - 2; p >= 0; --p)
-            {
-                const int kq = (p + 1) * NB;
-                for (int i = t; i < n; i += BT) umap[i] = (short)i;
-                __syncthreads();
-                if (t < sh.nchg[p + 1]) umap[kq + sh.chg[p + 1][t]] = (short)(kq + sh.src[p + 1][t]);
-                __syncthreads();
-                for (int i = kq + t; i < n; i += BT) tmap[i] = umap[tmap[i]];
-                __syncthreads();
-                for (int c = 2 * warp; c < NB; c += 2 * NW)
-                {
-                    float *c0 = A + (int64_t)(p * NB + c) * lda;
-                    float *c1 = c0 + lda;
-                    for (int i = kq + lane; i < n; i += 32)
-                    {
-                        stage[i - kq] = c0[i];
-                        stage[n + i - kq] = c1[i];
-                    }
-                    __syncwarp();
-                    for (int i = kq + lane; i < n; i += 32)
-                    {
-                        const int from = tmap[i] - kq;
-                        c0[i] = stage[from];
-                        c1[i] = stage[n + from];
-                    }
-                    __syncwarp();
-                }
-            }
-        }
         __syncthreads();
         if (t == 0) info[q] = sh.state;
         __syncthreads();
+    }
+}
+
+// The L columns of panel p (rows below the panel) take the row interchanges of panels
+// p+1..: final[pos] = stored[T[pos]], T the interchanges ipiv[k], k >= (p+1) NB, applied in
+// order to the identity.  One block per (matrix, panel); a warp per column.
+__global__ void __launch_bounds__(BT) left_swaps_kernel(float *single, float *const *table, int first, int n, int lda,
+                                                         const int *ipiv, int count)
+{
+    __shared__ short T[MAXN];
+    __shared__ float stage[NW][MAXN];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int64_t q = blockIdx.x;
+    const int p = blockIdx.y;
+    if (q >= count) return;
+    float *A = table ? slot(table, first + q) : single;
+    if (!A) return;
+    const int *piv = ipiv + q * n;
+    const int kq = (p + 1) * NB;
+    if (kq >= n) return;
+    for (int i = kq + t; i < n; i += BT) T[i] = (short)i;
+    __syncthreads();
+    if (t == 0)
+        for (int k = kq; k < n; ++k)
+        {
+            const int s = piv[k] - 1;
+            if (s > k && s < n)
+            {
+                const short v = T[k];
+                T[k] = T[s];
+                T[s] = v;
+            }
+        }
+    __syncthreads();
+    for (int c = warp; c < NB; c += NW)
+    {
+        float *col = A + (int64_t)(p * NB + c) * lda;
+        for (int i = kq + lane; i < n; i += 32) stage[warp][i - kq] = col[i];
+        __syncwarp();
+        for (int i = kq + lane; i < n; i += 32) col[i] = stage[warp][T[i] - kq];
+        __syncwarp();
     }
 }
 
@@ -853,6 +848,14 @@ cudaError_t launch_mode(const RealBatch &a, int *ipiv, int *info, const float *c
     if (blocks < 1) blocks = 1;
     getrf_blocked_kernel<MODE><<<(unsigned)blocks, BT, smem, stream>>>(a.single, a.table, a.first, a.n, a.ld, ipiv,
                                                                        info, a.count, src, src_ld, perm);
+    const int npanel = (a.n + NB - 1) / NB;
+    if (ipiv && npanel > 1)
+    {
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        left_swaps_kernel<<<dim3((unsigned)a.count, (unsigned)(npanel - 1)), BT, 0, stream>>>(
+            a.single, a.table, a.first, a.n, a.ld, ipiv, a.count);
+    }
     return cudaGetLastError();
 }
 }  // namespace
