@@ -11,16 +11,21 @@
 //     of the position, then the eight warp winners through double-buffered shared slots that
 //     also carry the winning row, so the pivot row needs no second broadcast); final values
 //     go to the row's own place in A as they are produced;
-//  2. the panel and trailing columns take the panel's row interchanges (a warp per column,
-//     32 columns in flight, only the rows whose position changed) and the panel's L is
-//     staged in shared memory (FP32, or negated BF16 hi/lo for the tensor cores);
-//  3. U12 = L11^-1 A12 (a thread per column, in registers), then A22 -= L21 U12 over
-//     128 x 64 tiles whose U12
+//  2. the columns of the panel's outer block (W2 = 128 columns) take the panel's row
+//     interchanges (a warp per column, 32 columns in flight, only the rows whose position
+//     changed) and the panel's L is staged in shared memory (FP32, or negated BF16 hi/lo for
+//     the tensor cores);
+//  3. inside the outer block: U12 = L11^-1 A12 (a thread per column, in registers), then
+//     A22 -= L21 U12 over 128 x 64 tiles whose U12
 //     block is prefetched into the other half of a double-buffered shared tile and whose C
 //     is prefetched into registers one row tile ahead;
-//  4. a second kernel, one block per (matrix, panel), applies the row interchanges of every
-//     later panel to that panel's L columns in one gather per column (LAPACK's final row
-//     order): bandwidth-bound work that no longer waits behind the factorisation.
+//  4. after the block's four panels, the columns right of it take the block's composed
+//     interchanges, U12 = L11^-1 A12 with the block's 128 x 128 L11 (in 32-row chunks), and
+//     one rank-128 update A22 -= L21 U12 (128 x 64 tiles, L21 row tile staged once), so the
+//     trailing matrix makes one trip through memory per 128 columns instead of per 32;
+//  5. a second kernel, one block per (matrix, panel), applies the row interchanges of the
+//     later outer blocks to that panel's L columns in one gather per column (LAPACK's final
+//     row order): bandwidth-bound work that no longer waits behind the factorisation.
 // Plain mode: every element takes a = fma(-l_ik, u_kj, a) in ascending k, the order of the
 // unblocked reference (real_lu.hpp:345-368, FactorLocalCore :409-448), so factors, pivots and
 // info are bit-identical to the oracle's orc_sgetrf at every n.  (The reference itself
@@ -49,6 +54,13 @@ constexpr int UP = CT + 4;  // pitch of the FP32 U12 tile
 constexpr int HP = NB + 8;  // pitch (halfs) of the BF16 tiles: 80 bytes, ldmatrix conflict-free
 constexpr int L11P = NB + 4;
 constexpr int SWAP_COLS = 32;  // columns in flight per warp during the row interchanges
+constexpr int W2 = 128;       // outer block: inner panels update only its columns; the rest of the
+                              // matrix takes one rank-128 update per outer block
+constexpr int LTP = RT + 4;   // plain outer update: L21 tile Lt[k][row] pitch (floats)
+constexpr int UTP = CT + 4;   // plain outer update: U12 tile Ut[k][col] pitch (floats)
+constexpr int BHP = W2 + 8;   // mixed outer update: [row][k] and [col][k] BF16 pitch (272 bytes)
+constexpr int LOP = W2 + 4;   // outer L11 Lo[k][i] pitch (floats)
+constexpr int BSWAP = 4;      // columns in flight per warp in the outer row interchanges
 constexpr unsigned FULL = 0xffffffffu;
 
 struct __align__(16) Shared
@@ -62,6 +74,7 @@ struct __align__(16) Shared
     short src[NPANEL][2 * NB];  // kept for the epilogue
     int nchg[NPANEL];
     int nchanged;
+    unsigned bz[W2 / NB];      // zero-pivot bits of the outer block's panels
     unsigned zmask;            // bit j: panel column j had a zero pivot (not used for updates)
     int state;                 // info of the matrix
 };
@@ -73,10 +86,16 @@ __host__ __device__ constexpr int lp_pitch(int n) { return (n + 3) / 4 * 4 + 4; 
 //   mixed: L11 (NB x L11P floats), L21 hi/lo (n x HP bf16 each), U12 hi/lo tiles (2 x CT x HP each)
 __host__ __device__ size_t dyn_bytes(int n, int mode)
 {
-    if (mode == 0) return ((size_t)NB * lp_pitch(n) + 2 * (size_t)NB * UP) * sizeof(float);
     const int terms = mode == 1 ? 1 : 2;
-    return (size_t)NB * L11P * sizeof(float) +
-           (size_t)terms * ((size_t)n * HP + 2 * (size_t)CT * HP) * sizeof(__nv_bfloat16);
+    const size_t inner = mode == 0 ? ((size_t)NB * lp_pitch(n) + 2 * (size_t)NB * UP) * sizeof(float)
+                                   : (size_t)NB * L11P * sizeof(float) +
+                                         (size_t)terms * ((size_t)n * HP + 2 * (size_t)CT * HP) * sizeof(__nv_bfloat16);
+    if (n <= W2) return inner;
+    const size_t trsm = ((size_t)W2 * LOP + (size_t)CT * LOP) * sizeof(float);
+    const size_t tiles = mode == 0 ? ((size_t)W2 * LTP + (size_t)W2 * UTP) * sizeof(float)
+                                   : (size_t)terms * ((size_t)RT * BHP + (size_t)CT * BHP) * sizeof(__nv_bfloat16);
+    size_t need = inner > trsm ? inner : trsm;
+    return need > tiles ? need : tiles;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -307,6 +326,25 @@ __device__ __forceinline__ void plain_c_update(float (&acc)[8][4], const float *
     const int t = threadIdx.x;
     const int tr = t & 15, tc = t >> 4;
     const int ra = min(r0 + tr * 4, lp - 4), rb = min(r0 + 64 + tr * 4, lp - 4);
+    if (zmask == 0u)
+    {
+        // no zero pivot in the panel (the usual case): a branch-free loop the compiler can
+        // software-pipeline
+#pragma unroll 8
+        for (int k = 0; k < NB; ++k)
+        {
+            const float4 a0 = *reinterpret_cast<const float4 *>(L + k * lp + ra);
+            const float4 a1 = *reinterpret_cast<const float4 *>(L + k * lp + rb);
+            const float4 b = *reinterpret_cast<const float4 *>(us + k * UP + tc * 4);
+            const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float bb[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fma_rn(-a[i], bb[j], acc[i][j]);
+        }
+        return;
+    }
 #pragma unroll 8
     for (int k = 0; k < NB; ++k)
     {
@@ -480,6 +518,332 @@ __device__ __forceinline__ void u_store(const float (&u)[8], float *us, __nv_bfl
 }
 
 // ---------------------------------------------------------------------------------------
+// outer-block update: the trailing columns take the outer block's interchanges, its U12
+// (rank-W2 triangular solve) and one rank-W2 update
+// ---------------------------------------------------------------------------------------
+// Plain: acc -= Lt[k][rows] Ut[k][cols] over k < W2 in ascending order, zero pivots skipped.
+__device__ __forceinline__ void plain_outer_update(float (&acc)[8][4], const float *Lt, const float *Ut,
+                                                   const unsigned *bz)
+{
+    const int t = threadIdx.x;
+    const int tr = t & 15, tc = t >> 4;
+    if ((bz[0] | bz[1] | bz[2] | bz[3]) == 0u)
+    {
+#pragma unroll 8
+        for (int kk = 0; kk < W2; ++kk)
+        {
+            const float4 a0 = *reinterpret_cast<const float4 *>(Lt + kk * LTP + tr * 4);
+            const float4 a1 = *reinterpret_cast<const float4 *>(Lt + kk * LTP + 64 + tr * 4);
+            const float4 b = *reinterpret_cast<const float4 *>(Ut + kk * UTP + tc * 4);
+            const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float bb[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fma_rn(-a[i], bb[j], acc[i][j]);
+        }
+        return;
+    }
+#pragma unroll 1
+    for (int kb = 0; kb < W2; kb += 32)
+    {
+        const unsigned z = bz[kb / 32];
+#pragma unroll 8
+        for (int k = 0; k < 32; ++k)
+        {
+            if ((z >> k) & 1u) continue;  // uniform
+            const int kk = kb + k;
+            const float4 a0 = *reinterpret_cast<const float4 *>(Lt + kk * LTP + tr * 4);
+            const float4 a1 = *reinterpret_cast<const float4 *>(Lt + kk * LTP + 64 + tr * 4);
+            const float4 b = *reinterpret_cast<const float4 *>(Ut + kk * UTP + tc * 4);
+            const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float bb[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fma_rn(-a[i], bb[j], acc[i][j]);
+        }
+    }
+}
+
+// Mixed: the tile's negated L21 halves Lh/Ll[row][k] and U12 halves Uh/Ul[col][k], K = W2.
+template <int TERMS>
+__device__ __forceinline__ void mixed_outer_update(float (&acc)[2][4][4], const __nv_bfloat16 *lh,
+                                                   const __nv_bfloat16 *ll, const __nv_bfloat16 *uh,
+                                                   const __nv_bfloat16 *ul)
+{
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int wr = (warp & 3) * 32, wc = (warp >> 2) * 32;
+#pragma unroll 2
+    for (int ks = 0; ks < W2 / 16; ++ks)
+    {
+        unsigned ah[2][4], al[2][4];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+        {
+            const int row = wr + mi * 16 + (lane & 15);
+            const int kk = ks * 16 + (lane >> 4) * 8;
+            ldsm_x4(ah[mi], lh + (size_t)row * BHP + kk);
+            if (TERMS > 1) ldsm_x4(al[mi], ll + (size_t)row * BHP + kk);
+        }
+#pragma unroll
+        for (int np = 0; np < 2; ++np)
+        {
+            const int mt = lane >> 3, rr = lane & 7;
+            const int col = wc + np * 16 + (mt >> 1) * 8 + rr;
+            const int kk = ks * 16 + (mt & 1) * 8;
+            unsigned bh[4], bl[4];
+            ldsm_x4(bh, uh + (size_t)col * BHP + kk);
+            if (TERMS > 1) ldsm_x4(bl, ul + (size_t)col * BHP + kk);
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+            {
+                const int ni = np * 2 + h;
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+                {
+                    if (TERMS > 1)
+                    {
+                        mma_bf16(acc[mi][ni], al[mi], bh[2 * h], bh[2 * h + 1]);
+                        mma_bf16(acc[mi][ni], ah[mi], bl[2 * h], bl[2 * h + 1]);
+                    }
+                    mma_bf16(acc[mi][ni], ah[mi], bh[2 * h], bh[2 * h + 1]);
+                }
+            }
+        }
+    }
+}
+
+template <int MODE, int TERMS>
+__device__ void outer_update(float *A, int lda, int n, int K0, bool vec, Shared &sh, unsigned char *dyn)
+{
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int kend = K0 + W2;
+    const int mb = n - K0;  // rows (positions) of the outer block and below
+    // (a) the block's composed permutation P (position -> row, relative to K0) and the
+    //     positions whose row changed
+    short *P = reinterpret_cast<short *>(dyn);
+    int *bch = reinterpret_cast<int *>(dyn + 2 * MAXN);
+    for (int i = t; i < mb; i += BT) P[i] = (short)i;
+    if (t == 0) sh.nchanged = 0;
+    __syncthreads();
+    for (int ip = 0; ip < W2 / NB; ++ip)
+    {
+        const int pidx = K0 / NB + ip, rel = ip * NB;
+        short v = 0;
+        if (t < sh.nchg[pidx]) v = P[rel + sh.src[pidx][t]];
+        __syncthreads();
+        if (t < sh.nchg[pidx]) P[rel + sh.chg[pidx][t]] = v;
+        __syncthreads();
+    }
+    for (int p = t; p < mb; p += BT)
+        if (P[p] != p) bch[atomicAdd(&sh.nchanged, 1)] = p;
+    __syncthreads();
+    const int nb = sh.nchanged;  // at most 2 NB per inner panel
+    // (b) the interchanges on the trailing columns: a warp per column, BSWAP columns in flight
+    {
+        constexpr int PER = (W2 / NB) * 2 * NB / 32;  // changed positions per lane, at most
+        int dst[PER], srcr[PER];
+#pragma unroll
+        for (int j = 0; j < PER; ++j)
+        {
+            const int e = lane + 32 * j;
+            dst[j] = e < nb ? bch[e] : -1;
+            srcr[j] = e < nb ? P[dst[j]] : 0;
+        }
+        const int ntr = n - kend;
+        for (int base = warp * BSWAP; base < ntr; base += NW * BSWAP)
+        {
+            float v[BSWAP][PER];
+#pragma unroll
+            for (int c = 0; c < BSWAP; ++c)
+            {
+                const float *col = A + (int64_t)(kend + min(base + c, ntr - 1)) * lda + K0;
+#pragma unroll
+                for (int j = 0; j < PER; ++j) v[c][j] = dst[j] >= 0 ? col[srcr[j]] : 0.0f;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int c = 0; c < BSWAP; ++c)
+            {
+                if (base + c >= ntr) continue;
+                float *col = A + (int64_t)(kend + base + c) * lda + K0;
+#pragma unroll
+                for (int j = 0; j < PER; ++j)
+                    if (dst[j] >= 0) col[dst[j]] = v[c][j];
+            }
+        }
+    }
+    __syncthreads();
+    // (c) U12 = L11^-1 A12 with the block's unit-lower L11 (staged), per 64-column tile held
+    //     in shared memory: four threads per column, each owning eight consecutive rows of
+    //     every 32-row chunk; chunk ci is solved (shuffles among the four), then applied to
+    //     the rows of the later chunks, in ascending k for every element
+    float *Lo = reinterpret_cast<float *>(dyn);
+    float *Ub = Lo + (size_t)W2 * LOP;  // CT columns x LOP: Ub[col][row]
+    for (int e = t; e < W2 * W2; e += BT)
+    {
+        const int k = e / W2, i = e % W2;
+        Lo[k * LOP + i] = A[(int64_t)(K0 + k) * lda + K0 + i];
+    }
+    for (int j0 = kend; j0 < n; j0 += CT)
+    {
+        const int nc = min(CT, n - j0);
+        for (int e = t; e < W2 * CT; e += BT)
+        {
+            const int cc = e / W2, r = e % W2;
+            Ub[cc * LOP + r] = cc < nc ? A[(int64_t)(j0 + cc) * lda + K0 + r] : 0.0f;
+        }
+        __syncthreads();
+        {
+            // thread (cc, part) owns rows 8 part .. 8 part + 7 of every chunk of column cc
+            const int cc = t >> 2, part = t & 3;
+            float *ucol = Ub + cc * LOP;
+#pragma unroll 1
+            for (int ci = 0; ci < W2 / 32; ++ci)
+            {
+                const unsigned z = sh.bz[ci];
+                float v[8];
+                {
+                    const float4 p0 = *reinterpret_cast<const float4 *>(ucol + ci * 32 + 8 * part);
+                    const float4 p1 = *reinterpret_cast<const float4 *>(ucol + ci * 32 + 8 * part + 4);
+                    v[0] = p0.x, v[1] = p0.y, v[2] = p0.z, v[3] = p0.w, v[4] = p1.x, v[5] = p1.y, v[6] = p1.z, v[7] = p1.w;
+                }
+#pragma unroll
+                for (int k = 0; k < 32; ++k)
+                {
+                    if ((z >> k) & 1u) continue;  // uniform
+                    const float u = __shfl_sync(FULL, v[k & 7], (lane & ~3) | (k >> 3));
+                    const float4 l0 = *reinterpret_cast<const float4 *>(Lo + (ci * 32 + k) * LOP + ci * 32 + 8 * part);
+                    const float4 l1 = *reinterpret_cast<const float4 *>(Lo + (ci * 32 + k) * LOP + ci * 32 + 8 * part + 4);
+                    const float lv[8] = {l0.x, l0.y, l0.z, l0.w, l1.x, l1.y, l1.z, l1.w};
+#pragma unroll
+                    for (int s = 0; s < 8; ++s)
+                        if (8 * part + s > k) v[s] = fma_rn(-lv[s], u, v[s]);
+                }
+                *reinterpret_cast<float4 *>(ucol + ci * 32 + 8 * part) = make_float4(v[0], v[1], v[2], v[3]);
+                *reinterpret_cast<float4 *>(ucol + ci * 32 + 8 * part + 4) = make_float4(v[4], v[5], v[6], v[7]);
+                __syncwarp();
+#pragma unroll 1
+                for (int cj = ci + 1; cj < W2 / 32; ++cj)
+                {
+                    float x[8];
+                    {
+                        const float4 p0 = *reinterpret_cast<const float4 *>(ucol + cj * 32 + 8 * part);
+                        const float4 p1 = *reinterpret_cast<const float4 *>(ucol + cj * 32 + 8 * part + 4);
+                        x[0] = p0.x, x[1] = p0.y, x[2] = p0.z, x[3] = p0.w, x[4] = p1.x, x[5] = p1.y, x[6] = p1.z, x[7] = p1.w;
+                    }
+#pragma unroll 4
+                    for (int k4 = 0; k4 < 32; k4 += 4)
+                    {
+                        const float4 u4 = *reinterpret_cast<const float4 *>(ucol + ci * 32 + k4);
+                        const float uu[4] = {u4.x, u4.y, u4.z, u4.w};
+#pragma unroll
+                        for (int e = 0; e < 4; ++e)
+                        {
+                            const int k = k4 + e;
+                            if ((z >> k) & 1u) continue;
+                            const float4 l0 = *reinterpret_cast<const float4 *>(Lo + (ci * 32 + k) * LOP + cj * 32 + 8 * part);
+                            const float4 l1 =
+                                *reinterpret_cast<const float4 *>(Lo + (ci * 32 + k) * LOP + cj * 32 + 8 * part + 4);
+                            const float lv[8] = {l0.x, l0.y, l0.z, l0.w, l1.x, l1.y, l1.z, l1.w};
+#pragma unroll
+                            for (int s = 0; s < 8; ++s) x[s] = fma_rn(-lv[s], uu[e], x[s]);
+                        }
+                    }
+                    *reinterpret_cast<float4 *>(ucol + cj * 32 + 8 * part) = make_float4(x[0], x[1], x[2], x[3]);
+                    *reinterpret_cast<float4 *>(ucol + cj * 32 + 8 * part + 4) = make_float4(x[4], x[5], x[6], x[7]);
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        for (int e = t; e < W2 * CT; e += BT)
+        {
+            const int cc = e / W2, r = e % W2;
+            if (cc < nc) A[(int64_t)(j0 + cc) * lda + K0 + r] = Ub[cc * LOP + r];
+        }
+        __syncthreads();
+    }
+    // (d) A22 -= L21 U12, K = W2: a row tile of L21 staged once, then every column tile
+    for (int r0 = W2; r0 < mb; r0 += RT)
+    {
+        if (MODE == 0)
+        {
+            float *Lt = reinterpret_cast<float *>(dyn);
+            for (int e = t; e < W2 * RT; e += BT)
+            {
+                const int k = e / RT, rr = e % RT;
+                Lt[k * LTP + rr] = r0 + rr < mb ? A[(int64_t)(K0 + k) * lda + K0 + r0 + rr] : 0.0f;
+            }
+        }
+        else
+        {
+            __nv_bfloat16 *lh = reinterpret_cast<__nv_bfloat16 *>(dyn);
+            __nv_bfloat16 *ll = lh + (size_t)RT * BHP;
+            for (int e = t; e < W2 * RT; e += BT)
+            {
+                const int k = e / RT, rr = e % RT;
+                float v = r0 + rr < mb ? -A[(int64_t)(K0 + k) * lda + K0 + r0 + rr] : 0.0f;
+                if ((sh.bz[k / 32] >> (k & 31)) & 1u) v = 0.0f;
+                __nv_bfloat16 h, l;
+                split_bf16(v, h, l);
+                lh[(size_t)rr * BHP + k] = h;
+                if (TERMS > 1) ll[(size_t)rr * BHP + k] = l;
+            }
+        }
+        for (int c0 = kend; c0 < n; c0 += CT)
+        {
+            const int nc = min(CT, n - c0);
+            if (MODE == 0)
+            {
+                float *Ut = reinterpret_cast<float *>(dyn) + (size_t)W2 * LTP;
+                for (int e = t; e < W2 * CT; e += BT)
+                {
+                    const int cc = e / W2, k = e % W2;
+                    Ut[k * UTP + cc] = cc < nc ? A[(int64_t)(c0 + cc) * lda + K0 + k] : 0.0f;
+                }
+            }
+            else
+            {
+                __nv_bfloat16 *uh = reinterpret_cast<__nv_bfloat16 *>(dyn) + (size_t)(TERMS > 1 ? 2 : 1) * RT * BHP;
+                __nv_bfloat16 *ul = uh + (size_t)CT * BHP;
+                for (int e = t; e < W2 * CT; e += BT)
+                {
+                    const int cc = e / W2, k = e % W2;
+                    const float v = cc < nc ? A[(int64_t)(c0 + cc) * lda + K0 + k] : 0.0f;
+                    __nv_bfloat16 h, l;
+                    split_bf16(v, h, l);
+                    uh[(size_t)cc * BHP + k] = h;
+                    if (TERMS > 1) ul[(size_t)cc * BHP + k] = l;
+                }
+            }
+            __syncthreads();
+            if (MODE == 0)
+            {
+                float acc[8][4];
+                plain_c_load(A, lda, mb, K0, c0, nc, r0, vec, acc);
+                plain_outer_update(acc, reinterpret_cast<float *>(dyn), reinterpret_cast<float *>(dyn) + (size_t)W2 * LTP,
+                                   sh.bz);
+                plain_c_store(A, lda, mb, K0, c0, nc, r0, vec, acc);
+            }
+            else
+            {
+                const __nv_bfloat16 *lh = reinterpret_cast<const __nv_bfloat16 *>(dyn);
+                const __nv_bfloat16 *ll = lh + (size_t)RT * BHP;
+                const __nv_bfloat16 *uh = lh + (size_t)(TERMS > 1 ? 2 : 1) * RT * BHP;
+                const __nv_bfloat16 *ul = uh + (size_t)CT * BHP;
+                float acc[2][4][4];
+                mixed_c_load(A, lda, mb, K0, c0, nc, r0, acc);
+                mixed_outer_update<TERMS>(acc, lh, ll, uh, ul);
+                mixed_c_store(A, lda, mb, K0, c0, nc, r0, acc);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // the kernel
 // ---------------------------------------------------------------------------------------
 template <int MODE>  // 0 plain FP32, 1 BF16, 3 split BF16 (three products)
@@ -543,7 +907,10 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
             __syncthreads();
         }
         if (t == 0) sh.state = 0;
-        for (int k0 = 0; k0 < n; k0 += NB)
+        for (int K0 = 0; K0 < n; K0 += W2)
+        {
+        const int kend = min(n, K0 + W2);
+        for (int k0 = K0; k0 < kend; k0 += NB)
         {
             const int w = min(NB, n - k0);
             const int m = n - k0;
@@ -589,13 +956,16 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
                     p1 = sh.changed[lane + 32];
                     s1 = sh.perm[p1];
                 }
-                for (int base = warp * SWAP_COLS; base < m; base += NW * SWAP_COLS)
+                // every column of the outer block: the block's earlier panels (their L), the
+                // panel and the block's later columns
+                const int mc = kend - K0;
+                for (int base = warp * SWAP_COLS; base < mc; base += NW * SWAP_COLS)
                 {
                     float v0[SWAP_COLS], v1[SWAP_COLS];
 #pragma unroll
                     for (int c = 0; c < SWAP_COLS; ++c)
                     {
-                        const float *col = A + (int64_t)(k0 + min(base + c, m - 1)) * lda + k0;
+                        const float *col = A + (int64_t)(K0 + min(base + c, mc - 1)) * lda + k0;
                         v0[c] = p0 >= 0 ? col[s0] : 0.0f;
                         v1[c] = p1 >= 0 ? col[s1] : 0.0f;
                     }
@@ -603,17 +973,18 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
 #pragma unroll
                     for (int c = 0; c < SWAP_COLS; ++c)
                     {
-                        if (base + c < m)
+                        if (base + c < mc)
                         {
-                            float *col = A + (int64_t)(k0 + base + c) * lda + k0;
+                            float *col = A + (int64_t)(K0 + base + c) * lda + k0;
                             if (p0 >= 0) col[p0] = v0[c];
                             if (p1 >= 0) col[p1] = v1[c];
                         }
                     }
                 }
             }
+            if (t == 0) sh.bz[(k0 - K0) / NB] = sh.zmask;
             __syncthreads();
-            if (k0 + w >= n) break;  // last panel: no trailing columns (w == NB below)
+            if (k0 + w >= kend) continue;  // last panel of the block: nothing inside it to update (w == NB below)
             // stage L from the panel, now in final order: plain FP32 L[k][p]; mixed FP32 L11
             // and the negated BF16 split of L21 (zero-pivot columns zeroed)
             {
@@ -660,7 +1031,7 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
             __syncthreads();
             const unsigned zmask = sh.zmask;
             const int jt = k0 + NB;   // first trailing column
-            const int ntr = n - jt;   // trailing columns
+            const int ntr = kend - jt;  // the rest of the outer block
             // (2) U12 = L11^-1 A12: a thread per column, ascending k, zero pivots skipped
             for (int jc = t; jc < ntr; jc += BT)
             {
@@ -727,16 +1098,16 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
             for (int ct = 0; ct < nct; ++ct)
             {
                 const int j0 = jt + ct * CT;
-                const int nc = min(CT, n - j0);
+                const int nc = min(CT, kend - j0);
                 const int buf = ct & 1;
                 float u[8];
-                if (ct + 1 < nct) u_load(A, lda, k0, j0 + CT, min(CT, n - j0 - CT), vec, u);
+                if (ct + 1 < nct) u_load(A, lda, k0, j0 + CT, min(CT, kend - j0 - CT), vec, u);
                 for (int r0 = NB; r0 < m; r0 += RT)
                 {
                     const bool more_rows = r0 + RT < m;
                     const bool more = more_rows || ct + 1 < nct;
                     const int nj0 = more_rows ? j0 : j0 + CT;
-                    const int nnc = min(CT, n - nj0);
+                    const int nnc = min(CT, kend - nj0);
                     const int nr0 = more_rows ? r0 + RT : NB;
                     if (MODE == 0)
                     {
@@ -765,6 +1136,10 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
                                          ul + (size_t)(buf ^ 1) * CT * HP);
                 __syncthreads();
             }
+        }
+        __syncthreads();
+        if (kend < n) outer_update<MODE, TERMS>(A, lda, n, K0, vec, sh, dyn);
+        __syncthreads();
         }
         const int npanel_all = (n + NB - 1) / NB;
         if (perm_out && piv)
@@ -795,9 +1170,11 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
     }
 }
 
-// The L columns of panel p (rows below the panel) take the row interchanges of panels
-// p+1..: final[pos] = stored[T[pos]], T the interchanges ipiv[k], k >= (p+1) NB, applied in
-// order to the identity.  One block per (matrix, panel); a warp per column.
+// The L columns of panel p take the row interchanges of the panels of later outer blocks
+// (those of its own block were applied to the whole block as they were made):
+// final[pos] = stored[T[pos]], T the interchanges ipiv[k], k >= kq (the next block's first
+// column), applied in order to the identity.  One block per (matrix, panel); a warp per
+// column.
 __global__ void __launch_bounds__(BT) left_swaps_kernel(float *single, float *const *table, int first, int n, int lda,
                                                          const int *ipiv, int count)
 {
@@ -810,7 +1187,7 @@ __global__ void __launch_bounds__(BT) left_swaps_kernel(float *single, float *co
     float *A = table ? slot(table, first + q) : single;
     if (!A) return;
     const int *piv = ipiv + q * n;
-    const int kq = (p + 1) * NB;
+    const int kq = (p * NB / W2 + 1) * W2;
     if (kq >= n) return;
     for (int i = kq + t; i < n; i += BT) T[i] = (short)i;
     __syncthreads();
