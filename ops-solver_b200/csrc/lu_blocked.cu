@@ -517,6 +517,31 @@ __device__ __forceinline__ void u_store(const float (&u)[8], float *us, __nv_bfl
     }
 }
 
+// Global -> shared staging with BATCH loads in flight per thread: the loads of a batch are
+// issued before any of its shared stores, so the copy is paced by bandwidth rather than by
+// one memory round trip per element (the compiler cannot reorder a global load past a store
+// through a generic pointer on its own).
+template <int BATCH, typename Load, typename Store>
+__device__ __forceinline__ void staged_copy(int total, Load load, Store store)
+{
+    for (int e0 = threadIdx.x; e0 < total; e0 += BT * BATCH)
+    {
+        float v[BATCH];
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u)
+        {
+            const int e = e0 + u * BT;
+            v[u] = e < total ? load(e) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u)
+        {
+            const int e = e0 + u * BT;
+            if (e < total) store(e, v[u]);
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 // outer-block update: the trailing columns take the outer block's interchanges, its U12
 // (rank-W2 triangular solve) and one rank-W2 update
@@ -681,19 +706,16 @@ __device__ void outer_update(float *A, int lda, int n, int K0, bool vec, Shared 
     //     the rows of the later chunks, in ascending k for every element
     float *Lo = reinterpret_cast<float *>(dyn);
     float *Ub = Lo + (size_t)W2 * LOP;  // CT columns x LOP: Ub[col][row]
-    for (int e = t; e < W2 * W2; e += BT)
-    {
-        const int k = e / W2, i = e % W2;
-        Lo[k * LOP + i] = A[(int64_t)(K0 + k) * lda + K0 + i];
-    }
+    staged_copy<16>(
+        W2 * W2, [&](int e) { return A[(int64_t)(K0 + e / W2) * lda + K0 + e % W2]; },
+        [&](int e, float v) { Lo[(e / W2) * LOP + e % W2] = v; });
     for (int j0 = kend; j0 < n; j0 += CT)
     {
         const int nc = min(CT, n - j0);
-        for (int e = t; e < W2 * CT; e += BT)
-        {
-            const int cc = e / W2, r = e % W2;
-            Ub[cc * LOP + r] = cc < nc ? A[(int64_t)(j0 + cc) * lda + K0 + r] : 0.0f;
-        }
+        staged_copy<16>(
+            W2 * CT,
+            [&](int e) { return e / W2 < nc ? A[(int64_t)(j0 + e / W2) * lda + K0 + e % W2] : 0.0f; },
+            [&](int e, float v) { Ub[(e / W2) * LOP + e % W2] = v; });
         __syncthreads();
         {
             // thread (cc, part) owns rows 8 part .. 8 part + 7 of every chunk of column cc
@@ -771,26 +793,26 @@ __device__ void outer_update(float *A, int lda, int n, int K0, bool vec, Shared 
         if (MODE == 0)
         {
             float *Lt = reinterpret_cast<float *>(dyn);
-            for (int e = t; e < W2 * RT; e += BT)
-            {
-                const int k = e / RT, rr = e % RT;
-                Lt[k * LTP + rr] = r0 + rr < mb ? A[(int64_t)(K0 + k) * lda + K0 + r0 + rr] : 0.0f;
-            }
+            staged_copy<16>(
+                W2 * RT,
+                [&](int e) { return r0 + e % RT < mb ? A[(int64_t)(K0 + e / RT) * lda + K0 + r0 + e % RT] : 0.0f; },
+                [&](int e, float v) { Lt[(e / RT) * LTP + e % RT] = v; });
         }
         else
         {
             __nv_bfloat16 *lh = reinterpret_cast<__nv_bfloat16 *>(dyn);
             __nv_bfloat16 *ll = lh + (size_t)RT * BHP;
-            for (int e = t; e < W2 * RT; e += BT)
-            {
-                const int k = e / RT, rr = e % RT;
-                float v = r0 + rr < mb ? -A[(int64_t)(K0 + k) * lda + K0 + r0 + rr] : 0.0f;
-                if ((sh.bz[k / 32] >> (k & 31)) & 1u) v = 0.0f;
-                __nv_bfloat16 h, l;
-                split_bf16(v, h, l);
-                lh[(size_t)rr * BHP + k] = h;
-                if (TERMS > 1) ll[(size_t)rr * BHP + k] = l;
-            }
+            staged_copy<16>(
+                W2 * RT,
+                [&](int e) { return r0 + e % RT < mb ? A[(int64_t)(K0 + e / RT) * lda + K0 + r0 + e % RT] : 0.0f; },
+                [&](int e, float a) {
+                    const int k = e / RT, rr = e % RT;
+                    const float v = ((sh.bz[k / 32] >> (k & 31)) & 1u) ? 0.0f : -a;
+                    __nv_bfloat16 h, l;
+                    split_bf16(v, h, l);
+                    lh[(size_t)rr * BHP + k] = h;
+                    if (TERMS > 1) ll[(size_t)rr * BHP + k] = l;
+                });
         }
         for (int c0 = kend; c0 < n; c0 += CT)
         {
@@ -798,25 +820,24 @@ __device__ void outer_update(float *A, int lda, int n, int K0, bool vec, Shared 
             if (MODE == 0)
             {
                 float *Ut = reinterpret_cast<float *>(dyn) + (size_t)W2 * LTP;
-                for (int e = t; e < W2 * CT; e += BT)
-                {
-                    const int cc = e / W2, k = e % W2;
-                    Ut[k * UTP + cc] = cc < nc ? A[(int64_t)(c0 + cc) * lda + K0 + k] : 0.0f;
-                }
+                staged_copy<16>(
+                    W2 * CT,
+                    [&](int e) { return e / W2 < nc ? A[(int64_t)(c0 + e / W2) * lda + K0 + e % W2] : 0.0f; },
+                    [&](int e, float v) { Ut[(e % W2) * UTP + e / W2] = v; });
             }
             else
             {
                 __nv_bfloat16 *uh = reinterpret_cast<__nv_bfloat16 *>(dyn) + (size_t)(TERMS > 1 ? 2 : 1) * RT * BHP;
                 __nv_bfloat16 *ul = uh + (size_t)CT * BHP;
-                for (int e = t; e < W2 * CT; e += BT)
-                {
-                    const int cc = e / W2, k = e % W2;
-                    const float v = cc < nc ? A[(int64_t)(c0 + cc) * lda + K0 + k] : 0.0f;
-                    __nv_bfloat16 h, l;
-                    split_bf16(v, h, l);
-                    uh[(size_t)cc * BHP + k] = h;
-                    if (TERMS > 1) ul[(size_t)cc * BHP + k] = l;
-                }
+                staged_copy<16>(
+                    W2 * CT,
+                    [&](int e) { return e / W2 < nc ? A[(int64_t)(c0 + e / W2) * lda + K0 + e % W2] : 0.0f; },
+                    [&](int e, float v) {
+                        __nv_bfloat16 h, l;
+                        split_bf16(v, h, l);
+                        uh[(size_t)(e / W2) * BHP + e % W2] = h;
+                        if (TERMS > 1) ul[(size_t)(e / W2) * BHP + e % W2] = l;
+                    });
             }
             __syncthreads();
             if (MODE == 0)
@@ -1206,7 +1227,19 @@ __global__ void __launch_bounds__(BT) left_swaps_kernel(float *single, float *co
     for (int c = warp; c < NB; c += NW)
     {
         float *col = A + (int64_t)(p * NB + c) * lda;
-        for (int i = kq + lane; i < n; i += 32) stage[warp][i - kq] = col[i];
+        float v[MAXN / 32];
+#pragma unroll
+        for (int u = 0; u < MAXN / 32; ++u)
+        {
+            const int i = kq + lane + 32 * u;
+            v[u] = i < n ? col[i] : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < MAXN / 32; ++u)
+        {
+            const int i = kq + lane + 32 * u;
+            if (i < n) stage[warp][i - kq] = v[u];
+        }
         __syncwarp();
         for (int i = kq + lane; i < n; i += 32) col[i] = stage[warp][T[i] - kq];
         __syncwarp();
