@@ -93,7 +93,8 @@ extern "C" aclsolverStatus_t aclsolverSgesvIrBatched(aclsolverHandle_t handle, a
     // per-job berr and state, per-matrix iterations.
     const size_t jobs = (size_t)batchSize * nrhs;
     const size_t vec = (size_t)n * jobs;
-    const size_t sizes[9] = {(size_t)n * n * batchSize * sizeof(float),
+    const int nblk = (n + 31) / 32;
+    const size_t sizes[10] = {(size_t)n * n * batchSize * sizeof(float),
                              (size_t)n * batchSize * sizeof(int),
                              (size_t)n * batchSize * sizeof(int),
                              (size_t)batchSize * sizeof(float *),
@@ -101,14 +102,15 @@ extern "C" aclsolverStatus_t aclsolverSgesvIrBatched(aclsolverHandle_t handle, a
                              vec * sizeof(double),
                              vec * sizeof(float),
                              jobs * sizeof(double),
-                             2 * jobs * sizeof(int)};
+                             2 * jobs * sizeof(int),
+                             (size_t)batchSize * nblk * 2 * 32 * 32 * sizeof(float)};
     size_t total = 0;
     for (size_t v : sizes) total += round_up(v);
     ScratchBlock *blk = acquire_scratch(h, total);
     if (!blk) return ACLSOLVER_STATUS_ALLOC_FAILED;
     char *p = static_cast<char *>(blk->ptr);
-    void *part[9];
-    for (int i = 0; i < 9; ++i)
+    void *part[10];
+    for (int i = 0; i < 10; ++i)
     {
         part[i] = p;
         p += round_up(sizes[i]);
@@ -124,6 +126,7 @@ extern "C" aclsolverStatus_t aclsolverSgesvIrBatched(aclsolverHandle_t handle, a
     s.berr = static_cast<double *>(part[7]);
     s.state = static_cast<int *>(part[8]);
     s.iters = s.state + jobs;
+    float *dinv = static_cast<float *>(part[9]);  // inverses of the factors' diagonal blocks
 
     RealBatch src{nullptr, const_cast<float *const *>(Aarray), n, lda, 0, batchSize};
     RealBatch fac{nullptr, lu_table, n, n, 0, batchSize};
@@ -132,7 +135,7 @@ extern "C" aclsolverStatus_t aclsolverSgesvIrBatched(aclsolverHandle_t handle, a
     auto solve = [&](const int *skip)
     {
         return n <= SMALL_N ? launch_getrs_small(fac, ipiv, rhs, nrhs, 0, nullptr, st)
-                            : launch_getrs_blocked(fac, nullptr, perm, rhs, nrhs, nullptr, skip, st);
+                            : launch_getrs_blocked(fac, nullptr, perm, rhs, nrhs, nullptr, skip, st, dinv);
     };
     cudaError_t e = launch_strided_table(lu_table, lu, (int64_t)n * n, batchSize, st);
     if (e == cudaSuccess) e = launch_strided_table(r_table, s.r32, (int64_t)n * nrhs, batchSize, st);
@@ -148,6 +151,7 @@ extern "C" aclsolverStatus_t aclsolverSgesvIrBatched(aclsolverHandle_t handle, a
             // the factorisation copies A into the workspace itself and reports the composed
             // row permutation used by the solves
             e = launch_getrf_blocked(fac, ipiv, infoArray, mode, st, src.table, lda, perm);
+            if (e == cudaSuccess) e = launch_diag_inverses(fac, dinv, st);
         }
     }
     if (e == cudaSuccess) e = launch_ir_init(s, Barray, ldb, infoArray, n, nrhs, batchSize, st);

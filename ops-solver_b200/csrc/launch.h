@@ -64,8 +64,14 @@ cudaError_t launch_getrf_blocked(const RealBatch &a, int *ipiv, int *info, int m
 // launch_permutation); both may be null.  `skip` (nullptr = none): per (matrix,
 // right-hand side) states; a group of right-hand sides whose states are all nonzero is
 // skipped (iterative refinement).  info may be null.
+// dinv (optional, refinement solves): the diagonal blocks' inverses from
+// launch_diag_inverses; the 32 x 32 triangles are then applied as products (not in the
+// oracle's order: used where the result is refined, not where it must match bit for bit).
 cudaError_t launch_getrs_blocked(const RealBatch &a, const int *ipiv, const int *perm, const RealBatch &b, int nrhs,
-                                 int *info, const int *skip, cudaStream_t stream);
+                                 int *info, const int *skip, cudaStream_t stream, const float *dinv = nullptr);
+// dinv[(q * nblk + b) * 2 + {0: L, 1: U}] = inverse of the 32 x 32 diagonal block b of the
+// factors of matrix q (column-major 32 x 32, nblk = ceil(n / 32)).
+cudaError_t launch_diag_inverses(const RealBatch &a, float *dinv, cudaStream_t stream);
 // perm[q*n + i] = row of b that the interchanges ipiv[q*n ..] bring to position i.
 cudaError_t launch_permutation(const int *ipiv, int *perm, int n, int count, cudaStream_t stream);
 

@@ -54,7 +54,7 @@ constexpr int UP = CT + 4;  // pitch of the FP32 U12 tile
 constexpr int HP = NB + 8;  // pitch (halfs) of the BF16 tiles: 80 bytes, ldmatrix conflict-free
 constexpr int L11P = NB + 4;
 constexpr int SWAP_COLS = 32;  // columns in flight per warp during the row interchanges
-constexpr int W2 = 128;       // outer block: inner panels update only its columns; the rest of the
+constexpr int W2 = 128;        // outer block: inner panels update only its columns; the rest of the
                               // matrix takes one rank-128 update per outer block
 constexpr int LTP = RT + 4;   // plain outer update: L21 tile Lt[k][row] pitch (floats)
 constexpr int UTP = CT + 4;   // plain outer update: U12 tile Ut[k][col] pitch (floats)
@@ -552,7 +552,10 @@ __device__ __forceinline__ void plain_outer_update(float (&acc)[8][4], const flo
 {
     const int t = threadIdx.x;
     const int tr = t & 15, tc = t >> 4;
-    if ((bz[0] | bz[1] | bz[2] | bz[3]) == 0u)
+    unsigned any_zero = 0u;
+#pragma unroll
+    for (int i = 0; i < W2 / 32; ++i) any_zero |= bz[i];
+    if (any_zero == 0u)
     {
 #pragma unroll 8
         for (int kk = 0; kk < W2; ++kk)

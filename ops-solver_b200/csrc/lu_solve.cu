@@ -102,12 +102,24 @@ __device__ __forceinline__ void cp_wait()
 // Starts the copy of a task's tile into stage[k][r] (k < 32 columns, r < rows); entries past
 // the tile are zero-filled.  vec: 16-byte copies (the matrix is 16-byte aligned, lda % 4 == 0).
 template <bool FORWARD>
-__device__ __forceinline__ void issue_task(const float *A, int lda, int n, Task task, float *stage, bool vec)
+__device__ __forceinline__ void issue_task(const float *A, int lda, int n, Task task, float *stage, bool vec,
+                                          const float *dinv)
 {
     int row0, rows;
     task_rows<FORWARD>(n, task, row0, rows);
     const int kb = task.blk * KB;
     const int w = min(KB, n - kb);
+    if (dinv && task.strip < 0)
+    {
+        // the block's inverse triangle (32 x 32, column-major): always 16-byte aligned
+        const float *src = dinv + ((size_t)task.blk * 2 + (FORWARD ? 0 : 1)) * KB * KB;
+        for (int c = threadIdx.x; c < KB * KB / 4; c += ST)
+        {
+            const int k = c / (KB / 4), r = (c % (KB / 4)) * 4;
+            cp_async16(stage + k * SP + r, src + k * KB + r, 16);
+        }
+        return;
+    }
     const int span = task.strip < 0 ? KB : SR;  // rows to fill
     if (vec)
     {
@@ -133,7 +145,7 @@ __device__ __forceinline__ void issue_task(const float *A, int lda, int n, Task 
 }
 
 template <bool FORWARD>
-__device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *stages, bool vec)
+__device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *stages, bool vec, const float *dinv)
 {
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int nblk = (n + KB - 1) / KB;
@@ -151,7 +163,7 @@ __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *s
 #pragma unroll
     for (int i = 0; i < STAGES - 1; ++i)
     {
-        if (live[i]) issue_task<FORWARD>(A, lda, n, q[i], stages + (size_t)i * KB * SP, vec);
+        if (live[i]) issue_task<FORWARD>(A, lda, n, q[i], stages + (size_t)i * KB * SP, vec, dinv);
         cp_commit();
     }
     int slot = 0;
@@ -160,7 +172,7 @@ __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *s
         // refill: the task STAGES - 1 ahead goes to the stage freed by the previous task
         if (live[STAGES - 1])
             issue_task<FORWARD>(A, lda, n, q[STAGES - 1],
-                                stages + (size_t)((slot + STAGES - 1) % STAGES) * KB * SP, vec);
+                                stages + (size_t)((slot + STAGES - 1) % STAGES) * KB * SP, vec, dinv);
         cp_commit();
         cp_wait<STAGES - 1>();  // this task's tile has landed (for this thread's copies)
         __syncthreads();        // ... and for everyone's
@@ -171,7 +183,21 @@ __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *s
         if (cur.strip < 0)
         {
             // diagonal triangle: warp r solves right-hand side r, lane i on row kb + i
-            if (warp < nr)
+            if (warp < nr && dinv)
+            {
+                // with the block's inverse: x_blk = inv x_blk, four partial sums per lane
+                float *xr = x + (size_t)warp * n;
+                const float xv = lane < w ? xr[kb + lane] : 0.0f;
+                float s4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+                for (int k = 0; k < KB; ++k)
+                {
+                    const float xk = __shfl_sync(0xffffffffu, xv, k);
+                    s4[k & 3] = fma_rn(tile[k * SP + lane], xk, s4[k & 3]);
+                }
+                if (lane < w) xr[kb + lane] = (s4[0] + s4[1]) + (s4[2] + s4[3]);
+            }
+            else if (warp < nr)
             {
                 float *xr = x + (size_t)warp * n;
                 float xv = lane < w ? xr[kb + lane] : 0.0f;
@@ -247,7 +273,7 @@ __global__ void __launch_bounds__(ST, 2) getrs_blocked_kernel(float *a_single, f
                                                             const int *ipiv, const int *perm, float *b_single,
                                                             float *const *b_table, int b_first, int n, int lda,
                                                             int ldb, int nrhs, int count, int RHS, int *info,
-                                                            const int *skip)
+                                                            const int *skip, const float *dinv_all, int nblk)
 {
     extern __shared__ __align__(16) float dyn[];
     float *stages = dyn;                          // STAGES x KB x SP
@@ -310,8 +336,9 @@ __global__ void __launch_bounds__(ST, 2) getrs_blocked_kernel(float *a_single, f
         }
         __syncthreads();
         const bool vec = (reinterpret_cast<uintptr_t>(A) & 15u) == 0 && (lda & 3) == 0;
-        sweep<true>(A, lda, n, x, nr, stages, vec);
-        sweep<false>(A, lda, n, x, nr, stages, vec);
+        const float *dinv = dinv_all ? dinv_all + (size_t)q * nblk * 2 * KB * KB : nullptr;
+        sweep<true>(A, lda, n, x, nr, stages, vec, dinv);
+        sweep<false>(A, lda, n, x, nr, stages, vec, dinv);
         for (int e = t; e < nr * n; e += ST)
         {
             const int r = e / n, i = e % n;
@@ -320,6 +347,57 @@ __global__ void __launch_bounds__(ST, 2) getrs_blocked_kernel(float *a_single, f
         if (t == 0 && info && r0 == 0) info[q] = 0;
         __syncthreads();
     }
+}
+
+// The inverses of the 32 x 32 diagonal blocks of the factors: warp 0 the unit-lower L
+// block's, warp 1 the upper U block's; lane j computes column j by substitution against
+// e_j.  Stored column-major, per (matrix, block): L inverse then U inverse.  (A ragged last
+// block of order w is inverted as w x w, the rest of the 32 x 32 identity.)
+__global__ void __launch_bounds__(64) diag_inverse_kernel(float *single, float *const *table, int first, int n,
+                                                          int lda, int count, float *dinv)
+{
+    __shared__ float D[KB][KB + 1];  // D[k][i] = factor element (row kb + i, column kb + k)
+    const int nblk = (n + KB - 1) / KB;
+    const int64_t q = blockIdx.x;
+    const int b = blockIdx.y;
+    if (q >= count) return;
+    const float *A = table ? slot(table, first + q) : single;
+    if (!A) return;
+    const int kb = b * KB, w = min(KB, n - kb);
+    for (int e = threadIdx.x; e < KB * KB; e += 64)
+    {
+        const int k = e / KB, i = e % KB;
+        D[k][i] = (k < w && i < w) ? A[(int64_t)(kb + k) * lda + kb + i] : (k == i ? 1.0f : 0.0f);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, which = threadIdx.x >> 5;
+    float y[KB];
+#pragma unroll
+    for (int r = 0; r < KB; ++r) y[r] = r == lane ? 1.0f : 0.0f;
+    if (which == 0)
+    {
+#pragma unroll
+        for (int k = 0; k < KB; ++k)
+        {
+            const float yk = y[k];
+#pragma unroll
+            for (int r = k + 1; r < KB; ++r) y[r] = fma_rn(-D[k][r], yk, y[r]);
+        }
+    }
+    else
+    {
+#pragma unroll
+        for (int k = KB - 1; k >= 0; --k)
+        {
+            y[k] = div_rn(y[k], D[k][k]);
+            const float yk = y[k];
+#pragma unroll
+            for (int r = 0; r < k; ++r) y[r] = fma_rn(-D[k][r], yk, y[r]);
+        }
+    }
+    float *dst = dinv + (((size_t)q * nblk + b) * 2 + which) * KB * KB + (size_t)lane * KB;
+#pragma unroll
+    for (int r = 0; r < KB; r += 4) *reinterpret_cast<float4 *>(dst + r) = make_float4(y[r], y[r + 1], y[r + 2], y[r + 3]);
 }
 
 // perm = the interchanges of ipiv applied in order to the identity: P b = b[perm].  One
@@ -346,7 +424,7 @@ __global__ void permutation_kernel(const int *ipiv, int *perm, int n, int count)
 }  // namespace
 
 cudaError_t launch_getrs_blocked(const RealBatch &a, const int *ipiv, const int *perm, const RealBatch &b, int nrhs,
-                                 int *info, const int *skip, cudaStream_t stream)
+                                 int *info, const int *skip, cudaStream_t stream, const float *dinv)
 {
     const size_t stage_floats = (size_t)STAGES * KB * SP;
     // two blocks per SM when the vectors fit beside the ring, else one
@@ -363,7 +441,15 @@ cudaError_t launch_getrs_blocked(const RealBatch &a, const int *ipiv, const int 
     if (blocks < 1) blocks = 1;
     getrs_blocked_kernel<<<(unsigned)blocks, ST, smem, stream>>>(a.single, a.table, a.first, ipiv, perm, b.single,
                                                                  b.table, b.first, a.n, a.ld, b.ld, nrhs, a.count,
-                                                                 rpb, info, skip);
+                                                                 rpb, info, skip, dinv, (a.n + KB - 1) / KB);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_diag_inverses(const RealBatch &a, float *dinv, cudaStream_t stream)
+{
+    const int nblk = (a.n + KB - 1) / KB;
+    diag_inverse_kernel<<<dim3((unsigned)a.count, (unsigned)nblk), 64, 0, stream>>>(a.single, a.table, a.first, a.n,
+                                                                                   a.ld, a.count, dinv);
     return cudaGetLastError();
 }
 
