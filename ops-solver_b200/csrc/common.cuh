@@ -19,6 +19,23 @@ __device__ __forceinline__ float sqrt_rn(float a) { return __fsqrt_rn(a); }
 // fma_rn(a, b, c) = a*b + c with one rounding.
 __device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 
+// Two FP32 lanes in one 64-bit register pair (sm_100 paired FP32 arithmetic): each lane of
+// fma2 is an IEEE fma rounded to nearest, i.e. exactly fma_rn on that lane.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 f2_pack(float lo, float hi)
+{
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float f2_lo(f32x2 v) { return __uint_as_float((unsigned)v); }
+__device__ __forceinline__ float f2_hi(f32x2 v) { return __uint_as_float((unsigned)(v >> 32)); }
+// d = a * b + d, lane by lane
+__device__ __forceinline__ void fma2(f32x2 &d, f32x2 a, f32x2 b)
+{
+    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d) : "l"(a), "l"(b));
+}
+
 // Matrix slot b of a device pointer table.  Loaded through the read-only path: the
 // tables are never written by a kernel.
 template <typename T>

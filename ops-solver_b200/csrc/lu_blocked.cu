@@ -62,6 +62,7 @@ constexpr int BHP = W2 + 8;   // mixed outer update: [row][k] and [col][k] BF16 
 constexpr int LOP = W2 + 4;   // outer L11 Lo[k][i] pitch (floats)
 constexpr int BSWAP = 4;      // columns in flight per warp in the outer row interchanges
 constexpr unsigned FULL = 0xffffffffu;
+static_assert(MAXN == 512, "the mixed panel's packed pivot key holds a 9-bit position");
 
 struct __align__(16) Shared
 {
@@ -94,7 +95,12 @@ __host__ __device__ size_t dyn_bytes(int n, int mode)
     const size_t trsm = ((size_t)W2 * LOP + (size_t)CT * LOP) * sizeof(float);
     const size_t tiles = mode == 0 ? ((size_t)W2 * LTP + (size_t)W2 * UTP) * sizeof(float)
                                    : (size_t)terms * ((size_t)RT * BHP + (size_t)CT * BHP) * sizeof(__nv_bfloat16);
+    // mixed U12 through X = L11^-1: the A12 tile's and X's BF16 halves (X behind FP32 L11 in BF16 mode)
+    const size_t xsplit = mode == 0 ? 0
+                          : mode == 1 ? (size_t)W2 * LOP * sizeof(float) + (size_t)RT * BHP * sizeof(__nv_bfloat16)
+                                      : 2 * ((size_t)CT * BHP + (size_t)RT * BHP) * sizeof(__nv_bfloat16);
     size_t need = inner > trsm ? inner : trsm;
+    need = need > xsplit ? need : xsplit;
     return need > tiles ? need : tiles;
 }
 
@@ -103,43 +109,62 @@ __host__ __device__ size_t dyn_bytes(int n, int mode)
 // ---------------------------------------------------------------------------------------
 // The panel's rows stay in registers, but rotated: in a group of four steps the current
 // column is r[s][u] (u = 0..3), and after the group every row shifts left by four, so all
-// register indices are compile-time constants inside a short loop body.  Each value that
-// becomes final is stored at its row's place in A as it is produced (an L entry at its
-// step, the pivot row's U entries at the pivot step, from the slot); rows are brought into
-// their final order afterwards, with the interchanges of the trailing columns.
-__device__ __forceinline__ void panel_factor(float *A, int lda, int n, int k0, int w, int *ipiv, bool pivoting,
-                                             Shared &sh, int (&pos)[2])
+// register indices are compile-time constants inside a short loop body.  Columns are held
+// in pairs (r[s][p] = columns 2p, 2p + 1) and updated with paired FMAs; a pair whose first
+// column is the step's own takes a dead update there.  Only the window's live columns
+// (< w - j0) are updated and published.  Each value that becomes final is stored at its
+// row's place in A as it is produced (an L entry at its step, the pivot row's U entries at
+// the pivot step, from the slot); rows are brought into their final order afterwards, with
+// the interchanges of the trailing columns.
+// EXACT (plain mode): largest |a| with the earliest position on ties, IEEE division.  The
+// mixed modes, whose factors are refined, take one warp reduction over a packed key (the
+// |a| key's top 22 bits above the position's complement: ties within 2^-13 relative go to
+// the earliest position) and multiply by the pivot's reciprocal.
+template <bool EXACT, int NR>
+__device__ __forceinline__ void panel_rows(float *A, int lda, int n, int k0, int w, int *ipiv, bool pivoting,
+                                           Shared &sh, int (&pos)[2])
 {
+    constexpr int NP = NB / 2;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int m = n - k0;
     const bool active = warp * 32 < m;  // warp-uniform: some row of this warp is in the panel
     float *pan = A + (int64_t)k0 * lda + k0;  // panel element (row i, column c) at pan[c * lda + i]
-    float r[2][NB];
-    bool valid[2];
+    f32x2 r[NR][NP];
+    bool valid[NR];
+    pos[1] = t + BT;  // one row per thread: the second is past the panel
 #pragma unroll
-    for (int s = 0; s < 2; ++s)
+    for (int s = 0; s < NR; ++s)
     {
         const int i = t + s * BT;
         valid[s] = i < m;
         pos[s] = i;
 #pragma unroll
-        for (int c = 0; c < NB; ++c) r[s][c] = (valid[s] && c < w) ? pan[(int64_t)c * lda + i] : 0.0f;
+        for (int p = 0; p < NP; ++p)
+        {
+            const float lo = (valid[s] && 2 * p < w) ? pan[(int64_t)(2 * p) * lda + i] : 0.0f;
+            const float hi = (valid[s] && 2 * p + 1 < w) ? pan[(int64_t)(2 * p + 1) * lda + i] : 0.0f;
+            r[s][p] = f2_pack(lo, hi);
+        }
     }
     for (int j0 = 0; j0 < w; j0 += 4)
     {
+        const int wl = w - j0;  // live columns of the window
 #pragma unroll
         for (int u = 0; u < 4; ++u)
         {
             const int j = j0 + u;
             if (j >= w) break;  // uniform
             const int buf = j & 1;
+            float cur[NR];
+#pragma unroll
+            for (int s = 0; s < NR; ++s) cur[s] = (u & 1) ? f2_hi(r[s][u / 2]) : f2_lo(r[s][u / 2]);
             if (active)
             {
-                unsigned key[2];
+                unsigned key[NR];
 #pragma unroll
-                for (int s = 0; s < 2; ++s)
+                for (int s = 0; s < NR; ++s)
                 {
-                    const float v = r[s][u];
+                    const float v = cur[s];
                     if (!valid[s])
                         key[s] = 0u;
                     else if (pivoting)
@@ -147,20 +172,32 @@ __device__ __forceinline__ void panel_factor(float *A, int lda, int n, int k0, i
                     else
                         key[s] = pos[s] == j ? 1u : 0u;
                 }
-                const unsigned wmax = __reduce_max_sync(FULL, max(key[0], key[1]));
-                unsigned cand = 0xffffffffu;
+                unsigned wmax, wpos;
+                if (EXACT)
+                {
+                    wmax = __reduce_max_sync(FULL, NR > 1 ? max(key[0], key[NR - 1]) : key[0]);
+                    unsigned cand = 0xffffffffu;
 #pragma unroll
-                for (int s = 0; s < 2; ++s)
-                    if (valid[s] && key[s] == wmax) cand = min(cand, (unsigned)pos[s]);
-                const unsigned wpos = __reduce_min_sync(FULL, cand);
+                    for (int s = 0; s < NR; ++s)
+                        if (valid[s] && key[s] == wmax) cand = min(cand, (unsigned)pos[s]);
+                    wpos = __reduce_min_sync(FULL, cand);
+                }
+                else
+                {
 #pragma unroll
-                for (int s = 0; s < 2; ++s)
+                    for (int s = 0; s < NR; ++s)
+                        key[s] = key[s] == 0u ? 0u : (((key[s] >> 10) + 1u) << 9) | (unsigned)(MAXN - 1 - pos[s]);
+                    wmax = __reduce_max_sync(FULL, NR > 1 ? max(key[0], key[NR - 1]) : key[0]);
+                    wpos = wmax == 0u ? 0xffffffffu : (unsigned)(MAXN - 1) - (wmax & (MAXN - 1));
+                }
+#pragma unroll
+                for (int s = 0; s < NR; ++s)
                     if (valid[s] && key[s] == wmax && (unsigned)pos[s] == wpos)
                     {
-                        float4 *dst = reinterpret_cast<float4 *>(sh.slot[buf][warp]);
+                        ulonglong2 *dst = reinterpret_cast<ulonglong2 *>(sh.slot[buf][warp]);
 #pragma unroll
-                        for (int c = 0; c < NB; c += 4)
-                            dst[c / 4] = make_float4(r[s][c], r[s][c + 1], r[s][c + 2], r[s][c + 3]);
+                        for (int q = 0; q < NP / 2; ++q)
+                            if (4 * q < wl) dst[q] = make_ulonglong2(r[s][2 * q], r[s][2 * q + 1]);
                         sh.krow[buf][warp] = t + s * BT;
                     }
                 if (lane == 0) sh.key[buf][warp] = make_uint2(wmax, wpos);
@@ -170,38 +207,23 @@ __device__ __forceinline__ void panel_factor(float *A, int lda, int n, int k0, i
             __syncthreads();
             if (!active) continue;  // no rows here: nothing to eliminate
             // the block's winner: largest key, then the smallest position (a warp without
-            // candidates reports key 0 and always loses: the position-j row has key >= 1)
-            const uint4 *kv = reinterpret_cast<const uint4 *>(sh.key[buf]);
-            unsigned gmax = 0u, gpos = 0xffffffffu;
-            int gw = 0;
-#pragma unroll
-            for (int q2 = 0; q2 < NW / 2; ++q2)
-            {
-                const uint4 k2 = kv[q2];
-                if (k2.x > gmax || (k2.x == gmax && k2.y < gpos))
-                {
-                    gmax = k2.x;
-                    gpos = k2.y;
-                    gw = 2 * q2;
-                }
-                if (k2.z > gmax || (k2.z == gmax && k2.w < gpos))
-                {
-                    gmax = k2.z;
-                    gpos = k2.w;
-                    gw = 2 * q2 + 1;
-                }
-            }
+            // candidates reports key 0 and always loses: the position-j row has key >= 1).
+            // Lane i reads warp i & 7's report; the lowest matching lane names the warp.
+            const uint2 kw = sh.key[buf][lane & (NW - 1)];
+            const unsigned gmax = __reduce_max_sync(FULL, kw.x);
+            const unsigned gpos = __reduce_min_sync(FULL, kw.x == gmax ? kw.y : 0xffffffffu);
+            const int gw = __ffs(__ballot_sync(FULL, kw.x == gmax && kw.y == gpos)) - 1;
             const int pr = (int)gpos;
             const float *prow = sh.slot[buf][gw];  // prow[c]: the pivot row at column j0 + c
             if (pivoting && t == 0) ipiv[k0 + j] = k0 + pr + 1;
             // the pivot row's U entries (columns j .. w - 1) are final now
             if (t < w - j) pan[(int64_t)(j + t) * lda + sh.krow[buf][gw]] = prow[u + t];
 #pragma unroll
-            for (int s = 0; s < 2; ++s) pos[s] = pos[s] == j ? pr : (pos[s] == pr ? j : pos[s]);
+            for (int s = 0; s < NR; ++s) pos[s] = pos[s] == j ? pr : (pos[s] == pr ? j : pos[s]);
             const float d = prow[u];
-            bool go[2];
+            bool go[NR];
 #pragma unroll
-            for (int s = 0; s < 2; ++s) go[s] = valid[s] && pos[s] > j;
+            for (int s = 0; s < NR; ++s) go[s] = valid[s] && pos[s] > j;
             if (d == 0.0f)
             {
                 if (t == 0)
@@ -211,48 +233,64 @@ __device__ __forceinline__ void panel_factor(float *A, int lda, int n, int k0, i
                 }
                 // a zero pivot scales nothing: the column keeps its values as L entries
 #pragma unroll
-                for (int s = 0; s < 2; ++s)
-                    if (go[s]) pan[(int64_t)j * lda + t + s * BT] = r[s][u];
+                for (int s = 0; s < NR; ++s)
+                    if (go[s]) pan[(int64_t)j * lda + t + s * BT] = cur[s];
             }
             else
             {
-                float l[2];
+                float l[NR];
+                const float rinv = EXACT ? 0.0f : __frcp_rn(d);
 #pragma unroll
-                for (int s = 0; s < 2; ++s)
+                for (int s = 0; s < NR; ++s)
                 {
-                    l[s] = go[s] ? div_rn(r[s][u], d) : 0.0f;
+                    l[s] = go[s] ? (EXACT ? div_rn(cur[s], d) : cur[s] * rinv) : 0.0f;
                     if (go[s]) pan[(int64_t)j * lda + t + s * BT] = l[s];
                 }
-                // the pivot row four columns at a time, shared by both rows
-                const float4 *p4 = reinterpret_cast<const float4 *>(prow);
+                f32x2 nl[NR];
 #pragma unroll
-                for (int c4 = 0; c4 < NB / 4; ++c4)
+                for (int s = 0; s < NR; ++s) nl[s] = f2_pack(-l[s], -l[s]);
+                // the pivot row four columns (two pairs) at a time, shared by both rows
+                const ulonglong2 *p2 = reinterpret_cast<const ulonglong2 *>(prow);
+#pragma unroll
+                for (int q = 0; q < NP / 2; ++q)
                 {
-                    if (c4 * 4 + 3 <= u) continue;
-                    const float4 v = p4[c4];
-                    const float pv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-                    for (int e = 0; e < 4; ++e)
+                    if (4 * q + 3 <= u) continue;  // compile-time: columns already final
+                    if (4 * q >= wl) break;        // uniform: past the panel
+                    const ulonglong2 v = p2[q];
+                    if (4 * q + 1 > u)
                     {
-                        const int c = c4 * 4 + e;
-                        if (c <= u) continue;
 #pragma unroll
-                        for (int s = 0; s < 2; ++s)
-                            if (go[s]) r[s][c] = fma_rn(-l[s], pv[e], r[s][c]);
+                        for (int s = 0; s < NR; ++s)
+                            if (go[s]) fma2(r[s][2 * q], nl[s], v.x);
                     }
+#pragma unroll
+                    for (int s = 0; s < NR; ++s)
+                        if (go[s]) fma2(r[s][2 * q + 1], nl[s], v.y);
                 }
             }
         }
-        // rotate: the next four columns move to the front
+        // rotate: the next four columns (two pairs) move to the front
 #pragma unroll
-        for (int s = 0; s < 2; ++s)
+        for (int s = 0; s < NR; ++s)
         {
 #pragma unroll
-            for (int c = 0; c < NB - 4; ++c) r[s][c] = r[s][c + 4];
-#pragma unroll
-            for (int c = NB - 4; c < NB; ++c) r[s][c] = 0.0f;
+            for (int p = 0; p < NP - 2; ++p) r[s][p] = r[s][p + 2];
+            r[s][NP - 2] = 0ull;
+            r[s][NP - 1] = 0ull;
         }
     }
+}
+
+
+// Two rows per thread while the panel is taller than the block, one row after.
+template <bool EXACT>
+__device__ __forceinline__ void panel_factor(float *A, int lda, int n, int k0, int w, int *ipiv, bool pivoting,
+                                             Shared &sh, int (&pos)[2])
+{
+    if (n - k0 > BT)
+        panel_rows<EXACT, 2>(A, lda, n, k0, w, ipiv, pivoting, sh, pos);
+    else
+        panel_rows<EXACT, 1>(A, lda, n, k0, w, ipiv, pivoting, sh, pos);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -642,6 +680,162 @@ __device__ __forceinline__ void mixed_outer_update(float (&acc)[2][4][4], const 
     }
 }
 
+// Mixed modes, U12 of the outer block: X = L11^-1 (unit lower, 128 x 128) is built once in
+// FP32 -- the four 32 x 32 diagonal inverses by substitution (a warp each, a lane per
+// column), then the off-diagonal blocks by distance, X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj
+// -- split into BF16 halves, and every 64-column tile of A12 becomes U12 = X A12 on the
+// tensor cores (three products).  Zero-pivot columns of L are zeroed first, so they take
+// no part, as in the plain solve.  Layout while X is built: L(i, k) (i > k) at Lo[k][i] and
+// X(r, c) (c <= r) at Lo[r][c], the staged block's upper triangle being free.
+template <int TERMS>
+__device__ void mixed_outer_u12(float *A, int lda, int n, int K0, Shared &sh, unsigned char *dyn)
+{
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int kend = K0 + W2;
+    float *Lo = reinterpret_cast<float *>(dyn);
+    float *T = Lo + (size_t)W2 * LOP;  // S blocks of one distance: T[b][r][c], pitch 33
+    staged_copy<16>(
+        W2 * W2,
+        [&](int e) {
+            const int k = e / W2, i = e % W2;
+            const bool zero = i > k && ((sh.bz[k / 32] >> (k & 31)) & 1u);
+            return zero ? 0.0f : A[(int64_t)(K0 + k) * lda + K0 + i];
+        },
+        [&](int e, float v) { Lo[(e / W2) * LOP + e % W2] = v; });
+    __syncthreads();
+    // (1) diagonal blocks: warp b inverts L_bb, lane j computing column j of the inverse
+    if (warp < W2 / 32)
+    {
+        const int b0 = warp * 32;
+        float y[32];
+#pragma unroll
+        for (int r = 0; r < 32; ++r) y[r] = r == lane ? 1.0f : 0.0f;
+#pragma unroll
+        for (int k = 0; k < 32; ++k)
+        {
+            const float yk = y[k];
+#pragma unroll
+            for (int r = k + 1; r < 32; ++r) y[r] = fma_rn(-Lo[(b0 + k) * LOP + b0 + r], yk, y[r]);
+        }
+        // reads were of the lower triangle, writes go to the upper one (and the diagonal)
+#pragma unroll
+        for (int r = 0; r < 32; ++r)
+            if (r >= lane) Lo[(b0 + r) * LOP + b0 + lane] = y[r];
+    }
+    __syncthreads();
+    // (2) off-diagonal blocks, distance d = i - j: thread (warp, lane) owns rows 4 warp .. +3
+    //     and column lane of every block
+    const int rq = warp * 4, c = lane;
+#pragma unroll 1
+    for (int d = 1; d < W2 / 32; ++d)
+    {
+        const int nblk = W2 / 32 - d;
+#pragma unroll 1
+        for (int b = 0; b < nblk; ++b)
+        {
+            const int j = b, i = b + d;
+            float sv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll 1
+            for (int kb = j; kb < i; ++kb)
+            {
+#pragma unroll 8
+                for (int kk = 0; kk < 32; ++kk)
+                {
+                    const int K = kb * 32 + kk;
+                    // X(K, 32 j + c): zero above the diagonal of X_jj
+                    const float x = (kb > j || kk >= c) ? Lo[K * LOP + j * 32 + c] : 0.0f;
+                    const float4 l = *reinterpret_cast<const float4 *>(Lo + (size_t)K * LOP + i * 32 + rq);
+                    sv[0] = fma_rn(l.x, x, sv[0]);
+                    sv[1] = fma_rn(l.y, x, sv[1]);
+                    sv[2] = fma_rn(l.z, x, sv[2]);
+                    sv[3] = fma_rn(l.w, x, sv[3]);
+                }
+            }
+#pragma unroll
+            for (int e = 0; e < 4; ++e) T[(b * 32 + rq + e) * 33 + c] = sv[e];
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int b = 0; b < nblk; ++b)
+        {
+            const int j = b, i = b + d;
+            float xv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll 8
+            for (int kk = 0; kk < 32; ++kk)
+            {
+                const float s = T[(b * 32 + kk) * 33 + c];
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    if (kk <= rq + e) xv[e] = fma_rn(Lo[(i * 32 + rq + e) * LOP + i * 32 + kk], s, xv[e]);
+            }
+#pragma unroll
+            for (int e = 0; e < 4; ++e) Lo[(i * 32 + rq + e) * LOP + j * 32 + c] = -xv[e];
+        }
+        __syncthreads();
+    }
+    // (3) X into BF16 halves xh/xl[row][k] at byte XO, behind the A12 tile's halves.  The
+    //     halves overlap FP32 rows >= 64 of X (split BF16) or nothing (BF16): those rows are
+    //     read into registers first, rows < 64 stay untouched in place until converted.
+    constexpr int XO = TERMS > 1 ? 2 * CT * BHP * 2 : W2 * LOP * 4;
+    __nv_bfloat16 *xh = reinterpret_cast<__nv_bfloat16 *>(dyn + XO);
+    __nv_bfloat16 *xl = xh + (size_t)RT * BHP;
+    {
+        constexpr int PER = (W2 - 64) * W2 / BT;
+        float hv[PER];
+#pragma unroll
+        for (int u = 0; u < PER; ++u)
+        {
+            const int e = t + u * BT, row = 64 + e / W2, k = e % W2;
+            hv[u] = k <= row ? Lo[row * LOP + k] : 0.0f;
+        }
+        __syncthreads();
+        auto put = [&](int row, int k, float v) {
+            __nv_bfloat16 h, l;
+            split_bf16(v, h, l);
+            xh[(size_t)row * BHP + k] = h;
+            if (TERMS > 1) xl[(size_t)row * BHP + k] = l;
+        };
+#pragma unroll
+        for (int u = 0; u < PER; ++u)
+        {
+            const int e = t + u * BT;
+            put(64 + e / W2, e % W2, hv[u]);
+        }
+        for (int e = t; e < 64 * W2; e += BT)
+        {
+            const int row = e / W2, k = e % W2;
+            put(row, k, k <= row ? Lo[row * LOP + k] : 0.0f);
+        }
+        __syncthreads();
+    }
+    // (4) U12 = X A12, a 64-column tile at a time
+    __nv_bfloat16 *uh = reinterpret_cast<__nv_bfloat16 *>(dyn);
+    __nv_bfloat16 *ul = uh + (size_t)CT * BHP;
+    for (int c0 = kend; c0 < n; c0 += CT)
+    {
+        const int nc = min(CT, n - c0);
+        staged_copy<16>(
+            W2 * CT, [&](int e) { return e / W2 < nc ? A[(int64_t)(c0 + e / W2) * lda + K0 + e % W2] : 0.0f; },
+            [&](int e, float v) {
+                __nv_bfloat16 h, l;
+                split_bf16(v, h, l);
+                uh[(size_t)(e / W2) * BHP + e % W2] = h;
+                if (TERMS > 1) ul[(size_t)(e / W2) * BHP + e % W2] = l;
+            });
+        __syncthreads();
+        float acc[2][4][4];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) acc[mi][ni][e] = 0.0f;
+        mixed_outer_update<TERMS>(acc, xh, xl, uh, ul);
+        mixed_c_store(A, lda, W2, K0, c0, nc, 0, acc);
+        __syncthreads();
+    }
+}
+
 template <int MODE, int TERMS>
 __device__ void outer_update(float *A, int lda, int n, int K0, bool vec, Shared &sh, unsigned char *dyn)
 {
@@ -703,10 +897,15 @@ __device__ void outer_update(float *A, int lda, int n, int K0, bool vec, Shared 
         }
     }
     __syncthreads();
-    // (c) U12 = L11^-1 A12 with the block's unit-lower L11 (staged), per 64-column tile held
+    // (c) U12 = L11^-1 A12.  Mixed modes: through X = L11^-1 on the tensor cores.  Plain: with the
+    //     block's unit-lower L11 (staged), per 64-column tile held
     //     in shared memory: four threads per column, each owning eight consecutive rows of
     //     every 32-row chunk; chunk ci is solved (shuffles among the four), then applied to
     //     the rows of the later chunks, in ascending k for every element
+    if (MODE != 0)
+        mixed_outer_u12<TERMS>(A, lda, n, K0, sh, dyn);
+    else
+    {
     float *Lo = reinterpret_cast<float *>(dyn);
     float *Ub = Lo + (size_t)W2 * LOP;  // CT columns x LOP: Ub[col][row]
     staged_copy<16>(
@@ -789,6 +988,7 @@ __device__ void outer_update(float *A, int lda, int n, int K0, bool vec, Shared 
             if (cc < nc) A[(int64_t)(j0 + cc) * lda + K0 + r] = Ub[cc * LOP + r];
         }
         __syncthreads();
+    }
     }
     // (d) A22 -= L21 U12, K = W2: a row tile of L21 staged once, then every column tile
     for (int r0 = W2; r0 < mb; r0 += RT)
@@ -944,7 +1144,7 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
                 sh.nchanged = 0;
             }
             int pos[2];
-            panel_factor(A, lda, n, k0, w, piv, piv != nullptr, sh, pos);
+            panel_factor<MODE == 0>(A, lda, n, k0, w, piv, piv != nullptr, sh, pos);
             // the permutation and the positions whose row changed
 #pragma unroll
             for (int s = 0; s < 2; ++s)
