@@ -232,11 +232,14 @@ aclsolverStatus_t check_arrays(Handle *h, int n, const float *const *a, int lda,
     return ACLSOLVER_STATUS_SUCCESS;
 }
 
+// The small and batched-blocked factorisations run in place (a token buffer keeps the
+// reference contract); the whole-GPU path above them keeps its per-panel pivot lists and
+// zero-pivot bits there.
+bool large_path(int m, int n) { return !(m <= SMALL_N && n <= SMALL_N) && !(m == n && n <= BLOCKED_MAX_N) && m >= n; }
+
 int factor_workspace(int m, int n)
 {
-    (void)m;
-    (void)n;
-    return 8;  // the factorisation runs in place; a token buffer keeps the reference contract
+    return large_path(m, n) ? (int)((sizeof(LargeStatus) + sizeof(float) - 1) / sizeof(float)) : 8;
 }
 
 int inverse_workspace(int n)
@@ -320,6 +323,12 @@ extern "C"
         }
         if (m <= SMALL_N && n <= SMALL_N) return launch_status(launch_getrf_small(a, m, devIpiv, devInfo, h->stream));
         if (m == n && n <= BLOCKED_MAX_N) return launch_status(launch_getrf_blocked(a, devIpiv, devInfo, 0, h->stream));
+        if (large_path(m, n))
+        {
+            if (reinterpret_cast<uintptr_t>(Workspace) % alignof(LargeStatus)) return invalid(h, devInfo, 1, 5);
+            return launch_status(launch_getrf_large(A, m, n, lda, devIpiv, devInfo,
+                                                    reinterpret_cast<LargeStatus *>(Workspace), h->stream));
+        }
         return ACLSOLVER_STATUS_NOT_SUPPORTED;
     }
 

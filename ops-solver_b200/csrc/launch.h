@@ -64,6 +64,24 @@ cudaError_t launch_getrf_blocked(const RealBatch &a, int *ipiv, int *info, int m
 // launch_permutation); both may be null.  `skip` (nullptr = none): per (matrix,
 // right-hand side) states; a group of right-hand sides whose states are all nonzero is
 // skipped (iterative refinement).  info may be null.
+// ---- large single-matrix LU (lu_large.cu) ---------------------------------------------
+constexpr int LARGE_MAX_ROWS = 8192;  // one panel row per thread of an 8 x 1024-thread cluster
+constexpr int LARGE_MAX_COLS = 8192;
+// Device scratch of one factorisation: info, per 32-column panel its zero-pivot bits and
+// its changed positions (position, physical row), at most 64.
+struct LargeStatus
+{
+    int info;
+    int pad[3];
+    unsigned zmask[LARGE_MAX_COLS / 32];
+    int nchg[LARGE_MAX_COLS / 32];
+    int2 chg[LARGE_MAX_COLS / 32][64];
+};
+// P A = L U of one m x n matrix (n <= m <= LARGE_MAX_ROWS) over the whole GPU; ipiv may be
+// null (no pivoting); *info receives the first zero pivot (1-based) or 0.
+cudaError_t launch_getrf_large(float *A, int m, int n, int lda, int *ipiv, int *info, LargeStatus *st,
+                               cudaStream_t stream);
+
 // dinv (optional, refinement solves): the diagonal blocks' inverses from
 // launch_diag_inverses; the 32 x 32 triangles are then applied as products (not in the
 // oracle's order: used where the result is refined, not where it must match bit for bit).
