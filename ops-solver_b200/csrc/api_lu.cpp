@@ -327,7 +327,7 @@ extern "C"
         {
             if (reinterpret_cast<uintptr_t>(Workspace) % alignof(LargeStatus)) return invalid(h, devInfo, 1, 5);
             return launch_status(launch_getrf_large(A, m, n, lda, devIpiv, devInfo,
-                                                    reinterpret_cast<LargeStatus *>(Workspace), h->stream));
+                                                    reinterpret_cast<LargeStatus *>(Workspace), 0, h->stream));
         }
         return ACLSOLVER_STATUS_NOT_SUPPORTED;
     }
@@ -475,7 +475,7 @@ extern "C"
         int arg = 0;
         if (trans != ACLSOLVER_OP_N && trans != ACLSOLVER_OP_T)
             arg = 1;
-        else if (n < 0 || n > 4096)
+        else if (n < 0 || n > LARGE_MAX_COLS)
             arg = 2;
         else if (nrhs < 0)
             arg = 3;
@@ -499,6 +499,19 @@ extern "C"
         if (n <= SMALL_N)
             return launch_status(launch_getrs_small(a, PivotArray, b, nrhs, trans == ACLSOLVER_OP_T ? 1 : 0,
                                                     infoArray, h->stream));
+        if (trans == ACLSOLVER_OP_N && batchSize == 1 && n > BLOCKED_MAX_N && nrhs <= LARGE_SOLVE_MAX_RHS)
+        {
+            // one large system: the whole GPU sweeps it (same order, same bad-pivot contract)
+            const size_t bytes = large_solve_scratch_bytes(n, nrhs) + 256;
+            ScratchBlock *blk = acquire_scratch(h, bytes);
+            if (!blk) return ACLSOLVER_STATUS_ALLOC_FAILED;
+            int *bad = reinterpret_cast<int *>(static_cast<char *>(blk->ptr) + ((bytes - 256 + 15) & ~size_t(15)));
+            aclsolverStatus_t launched = launch_status(launch_getrs_large(nullptr, Aarray, lda, n, PivotArray, nullptr,
+                                                                          Barray, ldb, nrhs, blk->ptr, bad, infoArray,
+                                                                          h->stream));
+            aclsolverStatus_t fin = finish_scratch(h, blk);
+            return launched != ACLSOLVER_STATUS_SUCCESS ? launched : fin;
+        }
         if (trans == ACLSOLVER_OP_N)
             return launch_status(launch_getrs_blocked(a, PivotArray, nullptr, b, nrhs, infoArray, nullptr, h->stream));
         return ACLSOLVER_STATUS_NOT_SUPPORTED;

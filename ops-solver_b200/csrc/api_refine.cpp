@@ -27,6 +27,66 @@ constexpr int SMALL_N = 64;
 
 size_t round_up(size_t v) { return (v + 255) & ~size_t(255); }
 
+// One matrix above the batched orders: the whole-GPU factorisation and solves, the residual
+// split over the GPU.  Unlike the batched schedule this one reads two flags back (info after
+// the factorisation, and whether a system still refines after each residual), so the call
+// returns after its work is done.
+aclsolverStatus_t gesv_ir_large(Handle *h, int mode, int n, int nrhs, const float *const Aarray[], int lda,
+                                const float *const Barray[], int ldb, float *const Xarray[], int ldx, int maxIter,
+                                double tol, int *iterArray, double *berrArray, int *infoArray)
+{
+    cudaStream_t st = h->stream;
+    const size_t sizes[6] = {(size_t)n * n * sizeof(float), (size_t)n * sizeof(int), sizeof(LargeStatus),
+                             large_solve_scratch_bytes(n, nrhs), 256, large_ir_bytes(n, nrhs)};
+    size_t total = 0;
+    for (size_t v : sizes) total += round_up(v);
+    ScratchBlock *blk = acquire_scratch(h, total);
+    if (!blk) return ACLSOLVER_STATUS_ALLOC_FAILED;
+    char *p = static_cast<char *>(blk->ptr);
+    void *part[6];
+    for (int i = 0; i < 6; ++i)
+    {
+        part[i] = p;
+        p += round_up(sizes[i]);
+    }
+    float *lu = static_cast<float *>(part[0]);
+    int *ipiv = static_cast<int *>(part[1]);
+    LargeStatus *status = static_cast<LargeStatus *>(part[2]);
+    void *solve_scratch = part[3];
+    int *flags = static_cast<int *>(part[4]);  // [0] bad pivot (unused: pivots are ours)
+    LargeIr s = large_ir_carve(part[5], n, nrhs);
+    RealBatch src{nullptr, const_cast<float *const *>(Aarray), n, lda, 0, 1};
+    RealBatch fac{lu, nullptr, n, n, 0, 1};
+    int hinfo = 0, running = 0;
+    cudaError_t e = launch_copy_matrices(src, fac, n, st);
+    if (e == cudaSuccess) e = launch_getrf_large(lu, n, n, n, ipiv, infoArray, status, mode, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hinfo, infoArray, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    auto solve = [&]() {
+        return launch_getrs_large(lu, nullptr, n, n, ipiv, s.r32, nullptr, n, nrhs, solve_scratch, flags, nullptr, st);
+    };
+    if (e == cudaSuccess && hinfo == 0)
+    {
+        e = launch_lir_init(s, Barray, ldb, n, nrhs, st);
+        if (e == cudaSuccess) e = solve();
+        if (e == cudaSuccess) e = launch_lir_update(s, n, nrhs, 1, st);
+        if (e == cudaSuccess) e = launch_lir_residual(s, Aarray, lda, Barray, ldb, n, nrhs, tol, 1, st);
+        for (int it = 0; it < maxIter && e == cudaSuccess; ++it)
+        {
+            e = cudaMemcpyAsync(&running, s.running, sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess || !running) break;
+            e = solve();
+            if (e == cudaSuccess) e = launch_lir_update(s, n, nrhs, 0, st);
+            if (e == cudaSuccess) e = launch_lir_residual(s, Aarray, lda, Barray, ldb, n, nrhs, tol, 0, st);
+        }
+    }
+    if (e == cudaSuccess) e = launch_lir_finish(s, Xarray, ldx, n, nrhs, berrArray, iterArray, hinfo != 0, st);
+    aclsolverStatus_t launched = launch_status(e);
+    aclsolverStatus_t fin = finish_scratch(h, blk);
+    return launched != ACLSOLVER_STATUS_SUCCESS ? launched : fin;
+}
+
 aclsolverStatus_t fail_args(Handle *h, int *info, int count, int arg)
 {
     if (info && count > 0 && is_device_pointer(info))
@@ -50,7 +110,7 @@ extern "C" aclsolverStatus_t aclsolverSgesvIrBatched(aclsolverHandle_t handle, a
     if (precision != ACLSOLVER_FACTOR_FP32 && precision != ACLSOLVER_FACTOR_BF16 &&
         precision != ACLSOLVER_FACTOR_BF16X3)
         arg = 1;
-    else if (n < 0 || n > BLOCKED_MAX_N)
+    else if (n < 0 || n > LARGE_MAX_COLS)
         arg = 2;
     else if (nrhs < 0)
         arg = 3;
@@ -87,6 +147,15 @@ extern "C" aclsolverStatus_t aclsolverSgesvIrBatched(aclsolverHandle_t handle, a
         if (e == cudaSuccess && iterArray) e = launch_fill_info(iterArray, 0, batchSize, st);
         if (e == cudaSuccess && berrArray) e = cudaMemsetAsync(berrArray, 0, sizeof(double) * batchSize, st);
         return launch_status(e);
+    }
+
+    const int mode = precision == ACLSOLVER_FACTOR_FP32 ? 0 : (precision == ACLSOLVER_FACTOR_BF16 ? 1 : 3);
+    if (n > BLOCKED_MAX_N)
+    {
+        // one system at a time over the whole GPU, at most 16 right-hand sides
+        if (batchSize != 1 || nrhs > LARGE_SOLVE_MAX_RHS) return ACLSOLVER_STATUS_NOT_SUPPORTED;
+        return gesv_ir_large(h, mode, n, nrhs, Aarray, lda, Barray, ldb, Xarray, ldx, maxIter, tol, iterArray,
+                             berrArray, infoArray);
     }
 
     // Workspace: LU copies, pivots and their permutation, two pointer tables, FP64 solutions, FP32 staging,
@@ -131,7 +200,6 @@ extern "C" aclsolverStatus_t aclsolverSgesvIrBatched(aclsolverHandle_t handle, a
     RealBatch src{nullptr, const_cast<float *const *>(Aarray), n, lda, 0, batchSize};
     RealBatch fac{nullptr, lu_table, n, n, 0, batchSize};
     RealBatch rhs{nullptr, r_table, n, n, 0, batchSize};
-    const int mode = precision == ACLSOLVER_FACTOR_FP32 ? 0 : (precision == ACLSOLVER_FACTOR_BF16 ? 1 : 3);
     auto solve = [&](const int *skip)
     {
         return n <= SMALL_N ? launch_getrs_small(fac, ipiv, rhs, nrhs, 0, nullptr, st)

@@ -36,6 +36,49 @@ __device__ __forceinline__ void fma2(f32x2 &d, f32x2 a, f32x2 b)
     asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d) : "l"(a), "l"(b));
 }
 
+// Copy a rows x cols column-major tile (element (i, k) at src[k * lds + i]) into shared
+// memory at dst[k * ldd + i], every thread of the block taking part.  vec: 16-byte cp.async
+// (src and dst 16-byte aligned per column, rows, lds and ldd multiples of 4); otherwise
+// eight plain loads in flight per thread before their stores.  Entries past rows / cols are
+// not written.  Callers wait with tile_wait() and a block barrier.
+__device__ __forceinline__ void stage_tile(float *dst, int ldd, const float *src, int64_t lds, int rows, int cols,
+                                           bool vec)
+{
+    const int nt = blockDim.x, t = threadIdx.x;
+    if (vec)
+    {
+        const int per = rows / 4;
+        for (int e = t; e < per * cols; e += nt)
+        {
+            const int k = e / per, i = (e % per) * 4;
+            const unsigned d = (unsigned)__cvta_generic_to_shared(dst + k * ldd + i);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src + k * lds + i) : "memory");
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    else
+    {
+        const int total = rows * cols;
+        for (int e0 = t; e0 < total; e0 += nt * 8)
+        {
+            float v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+            {
+                const int e = e0 + u * nt;
+                v[u] = e < total ? src[(e / rows) * lds + e % rows] : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+            {
+                const int e = e0 + u * nt;
+                if (e < total) dst[(e / rows) * ldd + e % rows] = v[u];
+            }
+        }
+    }
+}
+__device__ __forceinline__ void tile_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Matrix slot b of a device pointer table.  Loaded through the read-only path: the
 // tables are never written by a kernel.
 template <typename T>

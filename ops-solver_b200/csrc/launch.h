@@ -65,22 +65,61 @@ cudaError_t launch_getrf_blocked(const RealBatch &a, int *ipiv, int *info, int m
 // right-hand side) states; a group of right-hand sides whose states are all nonzero is
 // skipped (iterative refinement).  info may be null.
 // ---- large single-matrix LU (lu_large.cu) ---------------------------------------------
-constexpr int LARGE_MAX_ROWS = 8192;  // one panel row per thread of an 8 x 1024-thread cluster
+constexpr int LARGE_MAX_ROWS = 8192;  // up to four panel rows per thread of an 8 x 256-thread cluster
 constexpr int LARGE_MAX_COLS = 8192;
+constexpr int LARGE_WAIT_ERROR = -1000;  // info when a cluster panel's bounded wait ran out
 // Device scratch of one factorisation: info, per 32-column panel its zero-pivot bits and
 // its changed positions (position, physical row), at most 64.
 struct LargeStatus
 {
     int info;
-    int pad[3];
+    int error;  // a bounded wait of the cluster panel ran out (the factors are not valid)
+    int pad[2];
     unsigned zmask[LARGE_MAX_COLS / 32];
     int nchg[LARGE_MAX_COLS / 32];
     int2 chg[LARGE_MAX_COLS / 32][64];
 };
 // P A = L U of one m x n matrix (n <= m <= LARGE_MAX_ROWS) over the whole GPU; ipiv may be
-// null (no pivoting); *info receives the first zero pivot (1-based) or 0.
-cudaError_t launch_getrf_large(float *A, int m, int n, int lda, int *ipiv, int *info, LargeStatus *st,
+// null (no pivoting); *info receives the first zero pivot (1-based) or 0.  mode 0: plain
+// FP32 in the oracle's order; 1 / 3: BF16 / split-BF16 trailing updates on the tensor cores.
+cudaError_t launch_getrf_large(float *A, int m, int n, int lda, int *ipiv, int *info, LargeStatus *st, int mode,
                                cudaStream_t stream);
+
+// Solve with the factors of launch_getrf_large (or any LAPACK-layout LU) over the whole GPU:
+// A is A1 or slot 0 of At, X (n x nrhs, ldx) is X1 or slot 0 of Xt and is overwritten; ipiv
+// may be null.  scratch: large_solve_scratch_bytes(n, nrhs) of device memory.  An out-of-range
+// pivot sets *bad (device) and leaves X unchanged; info (device, optional) receives -6 then,
+// 0 otherwise.  Same per-element order as the oracle's sgetrs.
+constexpr int LARGE_SOLVE_MAX_RHS = 16;
+size_t large_solve_scratch_bytes(int n, int nrhs);
+cudaError_t launch_getrs_large(const float *A1, const float *const *At, int lda, int n, const int *ipiv, float *X1,
+                               float *const *Xt, int ldx, int nrhs, void *scratch, int *bad, int *info,
+                               cudaStream_t stream);
+
+// ---- refinement of one large matrix (lu_large_refine.cu) ---------------------------------
+enum
+{
+    LIR_RUNNING = 0,
+    LIR_CONVERGED = 1,
+    LIR_STALLED = 2
+};
+struct LargeIr
+{
+    double *x64, *xprev;  // n x nrhs (ld n): the iterate and the one before the last correction
+    float *r32;           // n x nrhs: residual, then correction (the solves work in place)
+    double *part, *apart;  // per column chunk: partial A x and |A| row sums
+    double *bmax, *amax;   // per row block: max |r|, |x|, |b| per right-hand side; max |A| row sum
+    double *berr;          // per right-hand side
+    int *state, *iters, *take, *running;
+};
+size_t large_ir_bytes(int n, int nrhs);
+LargeIr large_ir_carve(void *base, int n, int nrhs);
+cudaError_t launch_lir_init(const LargeIr &s, const float *const *B, int ldb, int n, int nrhs, cudaStream_t st);
+cudaError_t launch_lir_update(const LargeIr &s, int n, int nrhs, int first, cudaStream_t st);
+cudaError_t launch_lir_residual(const LargeIr &s, const float *const *A, int lda, const float *const *B, int ldb,
+                                int n, int nrhs, double tol, int first, cudaStream_t st);
+cudaError_t launch_lir_finish(const LargeIr &s, float *const *X, int ldx, int n, int nrhs, double *berr, int *iters,
+                              int failed, cudaStream_t st);
 
 // dinv (optional, refinement solves): the diagonal blocks' inverses from
 // launch_diag_inverses; the 32 x 32 triangles are then applied as products (not in the

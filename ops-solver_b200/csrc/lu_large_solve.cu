@@ -1,0 +1,220 @@
+// lu_large_solve.cu -- P A = L U solves of one large matrix over the whole GPU (the solve
+// half of the reference's single-matrix path: src/sgetrs/sgetrs_kernel.cpp:76-80 laswp,
+// custom_trsm, custom_trsm_upper).
+//
+// X (n x nrhs, column-major) first takes the pivots (the LAPACK swap sequence composed into
+// one gather), then one launch per 128-row block and sweep: every block of the launch solves
+// the diagonal 128 x 128 triangle for all right-hand sides in shared memory (redundantly, it
+// is small) and then subtracts the block's contribution from one 128-row strip of the rows
+// still to come.  Every element of X receives its updates as fma(-l, x, acc) in ascending k
+// (forward) or descending k (backward, after the IEEE division by U(k,k)), which is the
+// oracle's sgetrs order bit for bit.
+#include "common.cuh"
+#include "launch.h"
+
+namespace ops_solver
+{
+namespace
+{
+constexpr int SB = 128;  // rows per block
+constexpr int ST = 256;  // threads
+constexpr int SBP4 = SB + 4;  // shared pitch of the staged 128 x 128 tiles (16-byte rows)
+
+// perm[i] = the original row that ends at position i after the swaps ipiv[0..n-1].
+__global__ void __launch_bounds__(1024) large_perm_kernel(const int *ipiv, int n, int *perm, int *bad)
+{
+    __shared__ short P[LARGE_MAX_COLS];
+    __shared__ short Q[LARGE_MAX_COLS];  // the pivots (0-based, -1 when out of range), read once
+    const int t = threadIdx.x;
+    for (int i = t; i < n; i += blockDim.x)
+    {
+        P[i] = (short)i;
+        const int r = ipiv[i] - 1;
+        Q[i] = (short)(r < i || r >= n ? -1 : r);
+    }
+    __syncthreads();
+    if (t == 0)
+    {
+        int b = 0;
+        for (int k = 0; k < n; ++k)
+        {
+            const int r = Q[k];
+            if (r < 0)
+            {
+                b = 1;  // the whole solve is skipped
+                continue;
+            }
+            const short v = P[k];
+            P[k] = P[r];
+            P[r] = v;
+        }
+        *bad = b;
+    }
+    __syncthreads();
+    for (int i = t; i < n; i += blockDim.x) perm[i] = P[i];
+}
+
+// Y = X permuted (Y[i] = X[perm[i]]) for every right-hand side; Y is scratch (n x nrhs, ld n).
+// X is X1, or slot 0 of the table Xt.
+__global__ void large_gather_kernel(const float *X1, const float *const *Xt, int ldx, int n, int nrhs, const int *perm,
+                                    float *Y)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)n * nrhs) return;
+    const float *X = Xt ? slot(Xt, 0) : X1;
+    const int r = (int)(e / n), i = (int)(e % n);
+    Y[(int64_t)r * n + i] = X[(int64_t)r * ldx + (perm ? perm[i] : i)];
+}
+
+// X = Y, unless a pivot was out of range (X is then left as it was and info, if given, is
+// the reference's -6; 0 otherwise)
+__global__ void large_scatter_kernel(float *X1, float *const *Xt, int ldx, int n, int nrhs, const float *Y,
+                                     const int *bad, int *info)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool b = bad && *bad;
+    if (e == 0 && info) *info = b ? -6 : 0;
+    if (b || e >= (int64_t)n * nrhs) return;
+    float *X = Xt ? slot(Xt, 0) : X1;
+    const int r = (int)(e / n), i = (int)(e % n);
+    X[(int64_t)r * ldx + i] = Y[(int64_t)r * n + i];
+}
+
+// One block step of a sweep over Y (n x nrhs, ld n).  FORWARD: diagonal block b of the unit
+// lower L, then strips below; backward: diagonal block b of U (divisions), then strips above.
+// Grid: 1 + the strips to update; block 0 also writes the solved block back.
+template <bool FORWARD>
+__global__ void __launch_bounds__(ST) large_sweep_kernel(const float *A1, const float *const *At, int lda, int n,
+                                                          float *Y, int nrhs, int b, const int *bad)
+{
+    if (bad && *bad) return;  // uniform: nothing is solved with invalid pivots
+    const float *A = At ? slot(At, 0) : A1;
+    extern __shared__ __align__(16) float sm[];
+    float *D = sm;                   // D[k][i] = A(b0 + i, b0 + k), pitch SBP4
+    float *xs = D + SB * SBP4;       // xs[r][i]: the block's solution, pitch SB
+    const int t = threadIdx.x;
+    const int b0 = b * SB, w = min(SB, n - b0);
+    const bool vec = (reinterpret_cast<uintptr_t>(A) & 15u) == 0 && (lda & 3) == 0 && w == SB;
+    stage_tile(D, SBP4, A + (int64_t)b0 * lda + b0, lda, w, w, vec);
+    stage_tile(xs, SB, Y + b0, n, w, nrhs, (n & 3) == 0 && w == SB);
+    tile_wait();
+    __syncthreads();
+    // the diagonal triangle: column-oriented substitution, one k at a time; thread (r, part)
+    // owns right-hand side r and rows part, part + 16, ... of the block
+    {
+        const int r = t / 16, part = t % 16;
+        const bool live = r < nrhs;
+        float *x = xs + r * SB;
+        if (FORWARD)
+        {
+            for (int k = 0; k < w; ++k)
+            {
+                const float xk = live ? x[k] : 0.0f;
+                if (live)
+                    for (int i = k + 1 + ((part - (k + 1)) % 16 + 16) % 16; i < w; i += 16)
+                        x[i] = fma_rn(-D[k * SBP4 + i], xk, x[i]);
+                __syncthreads();
+            }
+        }
+        else
+        {
+            for (int k = w - 1; k >= 0; --k)
+            {
+                if (live && part == 0) x[k] = div_rn(x[k], D[k * SBP4 + k]);
+                __syncthreads();
+                const float xk = live ? x[k] : 0.0f;
+                if (live)
+                    for (int i = part; i < k; i += 16) x[i] = fma_rn(-D[k * SBP4 + i], xk, x[i]);
+                __syncthreads();
+            }
+        }
+    }
+    if (blockIdx.x == 0)
+    {
+        for (int e = t; e < nrhs * SB; e += ST)
+        {
+            const int r = e / SB, i = e % SB;
+            if (i < w) Y[(int64_t)r * n + b0 + i] = xs[r * SB + i];
+        }
+        return;
+    }
+    // a strip of 128 rows below (forward) or above (backward): Y[rows] -= A[rows, block] x
+    const int s = FORWARD ? b + blockIdx.x : b - blockIdx.x;
+    const int s0 = s * SB, sw = min(SB, n - s0);
+    // thread: row s0 + (t % 128), right-hand sides (t / 128), +2, ... (at most eight)
+    constexpr int RPT = LARGE_SOLVE_MAX_RHS / (ST / SB);
+    const int i = t % SB, r0 = t / SB;
+    // the strip's L (or U) columns into the diagonal block's buffer (its solve is done)
+    __syncthreads();
+    stage_tile(D, SBP4, A + (int64_t)b0 * lda + s0, lda, sw, w, vec && sw == SB);
+    tile_wait();
+    __syncthreads();
+    float acc[RPT];
+    if (i >= sw) return;
+#pragma unroll
+    for (int q = 0; q < RPT; ++q)
+    {
+        const int r = r0 + q * (ST / SB);
+        acc[q] = r < nrhs ? Y[(int64_t)r * n + s0 + i] : 0.0f;
+    }
+    for (int kk = 0; kk < w; ++kk)
+    {
+        const int k = FORWARD ? kk : w - 1 - kk;
+        const float l = D[k * SBP4 + i];
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) acc[q] = fma_rn(-l, xs[(r0 + q * (ST / SB)) * SB + k], acc[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < RPT; ++q)
+    {
+        const int r = r0 + q * (ST / SB);
+        if (r < nrhs) Y[(int64_t)r * n + s0 + i] = acc[q];
+    }
+}
+
+}  // namespace
+
+size_t large_solve_scratch_bytes(int n, int nrhs)
+{
+    return (size_t)n * nrhs * sizeof(float) + (size_t)n * sizeof(int) + 16;
+}
+
+cudaError_t launch_getrs_large(const float *A, const float *const *At, int lda, int n, const int *ipiv, float *X,
+                               float *const *Xt, int ldx, int nrhs, void *scratch, int *bad, int *info,
+                               cudaStream_t stream)
+{
+    if (n > LARGE_MAX_COLS || nrhs > LARGE_SOLVE_MAX_RHS) return cudaErrorInvalidValue;
+    float *Y = static_cast<float *>(scratch);
+    int *perm = reinterpret_cast<int *>(Y + (size_t)n * nrhs);
+    const size_t smem = (SB * SBP4 + (size_t)LARGE_SOLVE_MAX_RHS * SB) * sizeof(float);
+    static bool attr = false;
+    if (!attr)
+    {
+        cudaError_t e = cudaFuncSetAttribute(large_sweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(large_sweep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    if (ipiv)
+        large_perm_kernel<<<1, 1024, 0, stream>>>(ipiv, n, perm, bad);
+    else
+    {
+        cudaError_t e = cudaMemsetAsync(bad, 0, sizeof(int), stream);
+        if (e != cudaSuccess) return e;
+    }
+    const int64_t total = (int64_t)n * nrhs;
+    large_gather_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(X, Xt, ldx, n, nrhs,
+                                                                             ipiv ? perm : nullptr, Y);
+    const int nb = (n + SB - 1) / SB;
+    for (int b = 0; b < nb; ++b)
+        large_sweep_kernel<true><<<nb - b, ST, smem, stream>>>(A, At, lda, n, Y, nrhs, b, bad);
+    for (int b = nb - 1; b >= 0; --b)
+        large_sweep_kernel<false><<<b + 1, ST, smem, stream>>>(A, At, lda, n, Y, nrhs, b, bad);
+    large_scatter_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(X, Xt, ldx, n, nrhs, Y, bad, info);
+    return cudaGetLastError();
+}
+
+}  // namespace ops_solver

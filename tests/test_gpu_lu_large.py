@@ -12,7 +12,8 @@ import torch
 
 import aclsolver
 import oracle
-from helpers import DeviceMatrices, device_ints, first_mismatch, info_buffer, same_bits
+from oracle import judges
+from helpers import DeviceMatrices, conditioned_batch, device_ints, first_mismatch, info_buffer, same_bits
 
 pytestmark = pytest.mark.gpu
 
@@ -104,3 +105,135 @@ def test_large_sgetrf_8192_backward_error(handle):
     a64 = a.astype(np.float64)
     berr = np.abs(b - a64 @ x).max() / (np.abs(a64).sum(axis=1).max() * np.abs(x).max() + np.abs(b).max())
     assert berr < 1e-6, berr
+
+
+# ---- refinement of one large system (aclsolverSgesvIrBatched, batchSize 1, n > 512) ------
+
+def gesv_ir_one(handle, a, b, precision, max_iter=10, tol=1e-7):
+    lib = aclsolver.library()
+    n = a.shape[0]
+    nrhs = b.shape[1]
+    da = DeviceMatrices(a[None], ld=n + 1)
+    db = DeviceMatrices(b[None], ld=n + 2)
+    dx = DeviceMatrices(np.zeros_like(b)[None], ld=n + 3)
+    iters = torch.full((1,), -5, dtype=torch.int32, device="cuda")
+    berr = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
+    info = info_buffer(1)
+    st = lib.aclsolverSgesvIrBatched(handle.value, precision, n, nrhs, da.table_ptr, da.ld, db.table_ptr, db.ld,
+                                    dx.table_ptr, dx.ld, max_iter, tol, iters.data_ptr(), berr.data_ptr(),
+                                    info.data_ptr(), 1)
+    handle.stream.synchronize()
+    assert da.unchanged() and db.unchanged(), "A and B must be left as they were"
+    return st, dx.read()[0], int(iters.cpu()[0]), float(berr.cpu()[0]), int(info.cpu()[0])
+
+
+def test_large_ir_fp32_without_refinement_is_sgetrf_sgetrs(handle):
+    """maxIter 0 in FP32: the whole-GPU factorisation and solve in the oracle's order."""
+    n = 700
+    a = gaussian(n, n, seed=21)
+    b = np.random.default_rng(22).standard_normal((n, 3)).astype(np.float32)
+    st, x, iters, berr, info = gesv_ir_one(handle, a, b, aclsolver.FACTOR_FP32, max_iter=0)
+    assert st == aclsolver.SUCCESS and info == 0 and iters == 0
+    lu, ipiv, _ = oracle.sgetrf_batched(a[None])
+    want = oracle.sgetrs_batched(lu, ipiv, b[None])[0]
+    assert same_bits(x, want), first_mismatch(x, want)
+    be = max(judges.backward_error(a, x[:, j], b[:, j]) for j in range(3))
+    assert berr == pytest.approx(be, rel=1e-6)
+
+
+@pytest.mark.parametrize("precision", ["FACTOR_BF16X3", "FACTOR_FP32"])
+@pytest.mark.parametrize("n,kappa", [(1000, 1e4), (2048, 1e3)])
+def test_large_ir_reaches_fp32_backward_error(handle, precision, n, kappa):
+    a = conditioned_batch(1, n, kappa, seed=n)[0]
+    b = np.random.default_rng(n + 1).standard_normal((n, 4)).astype(np.float32)
+    st, x, iters, berr, info = gesv_ir_one(handle, a, b, getattr(aclsolver, precision), max_iter=10, tol=1e-7)
+    assert st == aclsolver.SUCCESS and info == 0
+    for j in range(4):
+        be = judges.backward_error(a, x[:, j], b[:, j])
+        assert be <= 1e-6, (j, be, berr, iters)
+        assert judges.forward_error(a, x[:, j], b[:, j]) <= kappa * 1e-6
+    assert 0 <= iters <= 10 and berr <= 1e-6
+
+
+def test_large_ir_singular_is_not_solved(handle):
+    n = 600
+    a = gaussian(n, n, seed=31)
+    a[:, 100] = 0.0
+    b = np.ones((n, 1), dtype=np.float32)
+    st, x, iters, berr, info = gesv_ir_one(handle, a, b, aclsolver.FACTOR_BF16X3)
+    assert st == aclsolver.SUCCESS and info == 101
+    assert np.all(x == 0.0) and np.isnan(berr) and iters == 0
+
+
+def test_large_ir_8192_split_bf16(handle):
+    """The single large system of the benchmark family: 8192 x 8192, A = U diag(s) V^T with
+    kappa = 1e3 (generated on the GPU), 16 right-hand sides, split-BF16 factorisation plus
+    FP64 refinement to FP32-level backward error (checked in FP64 on the GPU)."""
+    n, nrhs = 8192, 16
+    g = torch.Generator(device="cuda").manual_seed(6)
+    u, _ = torch.linalg.qr(torch.randn(n, n, device="cuda", dtype=torch.float64, generator=g))
+    v, _ = torch.linalg.qr(torch.randn(n, n, device="cuda", dtype=torch.float64, generator=g))
+    s = torch.logspace(0.0, -3.0, n, device="cuda", dtype=torch.float64)
+    a64 = (u * s) @ v.T
+    del u, v
+    a = a64.float()
+    b = torch.randn(n, nrhs, device="cuda", generator=g).float()
+    lib = aclsolver.library()
+    # column-major device buffers: the transposes of the row-major torch tensors
+    at = a.T.contiguous()
+    bt = b.T.contiguous()
+    xt = torch.zeros_like(bt)
+    tables = [aclsolver.pointer_table(t, 1, 0) for t in (at, bt, xt)]
+    iters = torch.zeros(1, dtype=torch.int32, device="cuda")
+    berr = torch.zeros(1, dtype=torch.float64, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    st = lib.aclsolverSgesvIrBatched(handle.value, aclsolver.FACTOR_BF16X3, n, nrhs, tables[0].data_ptr(), n,
+                                    tables[1].data_ptr(), n, tables[2].data_ptr(), n, 10, 1e-7, iters.data_ptr(),
+                                    berr.data_ptr(), info.data_ptr(), 1)
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.item()) == 0
+    x = xt.T.double()
+    a32 = a.double()
+    r = b.double() - a32 @ x
+    be = (r.abs().amax(dim=0) / (a32.abs().sum(dim=1).max() * x.abs().amax(dim=0) + b.double().abs().amax(dim=0)))
+    assert float(be.max()) <= 1e-6, (be.max(), berr, iters)
+    assert 0 <= int(iters.item()) <= 10
+
+
+@pytest.mark.parametrize("n,nrhs", [(700, 1), (1000, 16), (2048, 5)])
+def test_large_sgetrs_one_system_matches_oracle(handle, n, nrhs):
+    """aclsolverSgetrsBatched with one system above 512: the whole-GPU sweep, bit for bit."""
+    lib = aclsolver.library()
+    a = gaussian(n, n, seed=n + 40)
+    lu, ipiv, _ = oracle.sgetrf_batched(a[None])
+    b = np.random.default_rng(n + 41).standard_normal((n, nrhs)).astype(np.float32)
+    da = DeviceMatrices(lu, ld=n + 1)
+    db = DeviceMatrices(b[None], ld=n + 3)
+    piv = device_ints(ipiv.reshape(-1))
+    info = info_buffer(1)
+    st = lib.aclsolverSgetrsBatched(handle.value, 0, n, nrhs, da.table_ptr, da.ld, piv.data_ptr(), db.table_ptr,
+                                   db.ld, info.data_ptr(), 1)
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 0
+    want = oracle.sgetrs_batched(lu, ipiv, b[None])[0]
+    got = db.read()[0]
+    assert same_bits(got, want), first_mismatch(got, want)
+
+
+def test_large_sgetrs_bad_pivot_leaves_b(handle):
+    lib = aclsolver.library()
+    n = 640
+    a = gaussian(n, n, seed=50)
+    lu, ipiv, _ = oracle.sgetrf_batched(a[None])
+    ipiv = ipiv.copy()
+    ipiv[0, 300] = n + 5
+    b = np.random.default_rng(51).standard_normal((n, 2)).astype(np.float32)
+    da = DeviceMatrices(lu, ld=n)
+    db = DeviceMatrices(b[None], ld=n)
+    piv = device_ints(ipiv.reshape(-1))
+    info = info_buffer(1)
+    st = lib.aclsolverSgetrsBatched(handle.value, 0, n, 2, da.table_ptr, da.ld, piv.data_ptr(), db.table_ptr, db.ld,
+                                   info.data_ptr(), 1)
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == -6
+    assert np.array_equal(db.read()[0], b)

@@ -147,7 +147,7 @@ def test_solution_may_overwrite_b(handle):
 
 @pytest.mark.parametrize(
     "field,value,arg",
-    [("precision", 2, 1), ("n", 513, 2), ("nrhs", -1, 3), ("lda", 5, 5), ("ldb", 5, 7), ("ldx", 5, 9),
+    [("precision", 2, 1), ("n", 8193, 2), ("nrhs", -1, 3), ("lda", 5, 5), ("ldb", 5, 7), ("ldx", 5, 9),
      ("max_iter", -1, 10), ("tol", -1.0, 11), ("batch", -1, 15)],
 )
 def test_argument_errors(handle, field, value, arg):
