@@ -99,34 +99,72 @@ __global__ void __launch_bounds__(ST) large_sweep_kernel(const float *A1, const 
     stage_tile(xs, SB, Y + b0, n, w, nrhs, (n & 3) == 0 && w == SB);
     tile_wait();
     __syncthreads();
-    // the diagonal triangle: column-oriented substitution, one k at a time; thread (r, part)
-    // owns right-hand side r and rows part, part + 16, ... of the block
+    // the diagonal block in 32-row sub-blocks: each sub-block's triangle by one warp per two
+    // right-hand sides (a lane per row, the solved entry broadcast by shuffle), then the
+    // block's remaining rows take that sub-block's columns; per element still ascending k
+    // (forward) or descending k after the division (backward)
     {
-        const int r = t / 16, part = t % 16;
-        const bool live = r < nrhs;
-        float *x = xs + r * SB;
-        if (FORWARD)
+        const int lane = t & 31, warp = t >> 5;
+        const int nsub = (w + 31) / 32;
+        for (int si = 0; si < nsub; ++si)
         {
-            for (int k = 0; k < w; ++k)
+            const int cb = 32 * (FORWARD ? si : nsub - 1 - si), cw = min(32, w - cb);
+            const int ra = warp, rb2 = warp + ST / 32;  // this warp's right-hand sides
+            float *xa = xs + ra * SB + cb, *xb = xs + rb2 * SB + cb;
+            const bool la = ra < nrhs, lb = rb2 < nrhs;  // warp-uniform
+            float va = la && lane < cw ? xa[lane] : 0.0f;
+            float vb = lb && lane < cw ? xb[lane] : 0.0f;
+            if (FORWARD)
             {
-                const float xk = live ? x[k] : 0.0f;
-                if (live)
-                    for (int i = k + 1 + ((part - (k + 1)) % 16 + 16) % 16; i < w; i += 16)
-                        x[i] = fma_rn(-D[k * SBP4 + i], xk, x[i]);
-                __syncthreads();
+                for (int k = 0; k < cw; ++k)
+                {
+                    const float ka = __shfl_sync(0xffffffffu, va, k), kb = __shfl_sync(0xffffffffu, vb, k);
+                    if (lane > k && lane < cw)
+                    {
+                        const float l = D[(cb + k) * SBP4 + cb + lane];
+                        va = fma_rn(-l, ka, va);
+                        vb = fma_rn(-l, kb, vb);
+                    }
+                }
             }
-        }
-        else
-        {
-            for (int k = w - 1; k >= 0; --k)
+            else
             {
-                if (live && part == 0) x[k] = div_rn(x[k], D[k * SBP4 + k]);
-                __syncthreads();
-                const float xk = live ? x[k] : 0.0f;
-                if (live)
-                    for (int i = part; i < k; i += 16) x[i] = fma_rn(-D[k * SBP4 + i], xk, x[i]);
-                __syncthreads();
+                for (int k = cw - 1; k >= 0; --k)
+                {
+                    if (lane == k)
+                    {
+                        const float d = D[(cb + k) * SBP4 + cb + k];
+                        va = div_rn(va, d);
+                        vb = div_rn(vb, d);
+                    }
+                    const float ka = __shfl_sync(0xffffffffu, va, k), kb = __shfl_sync(0xffffffffu, vb, k);
+                    if (lane < k)
+                    {
+                        const float u = D[(cb + k) * SBP4 + cb + lane];
+                        va = fma_rn(-u, ka, va);
+                        vb = fma_rn(-u, kb, vb);
+                    }
+                }
             }
+            if (la && lane < cw) xa[lane] = va;
+            if (lb && lane < cw) xb[lane] = vb;
+            __syncthreads();
+            // the rest of the block: rows after the sub-block (forward) or before it (backward)
+            const int r0 = FORWARD ? cb + cw : 0, r1 = FORWARD ? w : cb;
+            const int nrow = r1 - r0;
+            for (int e = t; e < nrow * nrhs; e += ST)
+            {
+                const int i = r0 + e % nrow, r = e / nrow;
+                float *x = xs + r * SB;
+                float acc = x[i];
+                for (int kk = 0; kk < cw; ++kk)
+                {
+                    const int k = FORWARD ? kk : cw - 1 - kk;
+                    acc = fma_rn(-D[(cb + k) * SBP4 + i], x[cb + k], acc);
+                }
+                x[i] = acc;
+            }
+            __syncthreads();
         }
     }
     if (blockIdx.x == 0)
