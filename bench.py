@@ -323,6 +323,7 @@ def run_b200(args, rank, world):
         achieved = FACTOR_BYTES * COUNT / (factor_ms * 1e-3) / 1e9
         roof_ms = max(FACTOR_BYTES * COUNT / (hbm * 1e9), FACTOR_FLOPS * COUNT / (bf16 * 1e12)) * 1e3
         cpu = cpu_baseline(args)
+        large = measure_large(handle) if args.large else None
         by_kappa = {}
         for k, kappa in enumerate(KAPPAS):
             idx = list(range(k, COUNT, len(KAPPAS)))
@@ -397,9 +398,102 @@ def run_b200(args, rank, world):
             "clocks": clocks.summary(),
             "wall_s_timed": round(wall, 4),
             "cpu_baseline": cpu,
+            "large": large,
         }
         print(json.dumps(line), flush=True)
     handle.close()
+
+
+LARGE_N, LARGE_NRHS, LARGE_KAPPA = 8192, 16, 1e3
+
+
+def measure_large(handle, steps=3):
+    """The single large system beside the batched headline: one 8192 x 8192 A = U diag(s) V^T
+    (Haar U, V from an FP64 QR on the GPU, kappa 1e3), 16 N(0,1) right-hand sides.  Plain:
+    aclsolverSgetrf + aclsolverSgetrsBatched (FP32, the oracle's order) on device-resident
+    copies; mixed: aclsolverSgesvIrBatched(BF16X3, tol 1e-7, maxIter 4).  Backward errors in
+    FP64 on the GPU; forward errors against an FP64 LU solve (torch.linalg.solve)."""
+    import ctypes as C
+    import math
+
+    import torch
+
+    import aclsolver
+
+    check = aclsolver.check
+    lib = aclsolver.library()
+    n, nrhs = LARGE_N, LARGE_NRHS
+    g = torch.Generator(device="cuda").manual_seed(6)
+    u, _ = torch.linalg.qr(torch.randn(n, n, device="cuda", dtype=torch.float64, generator=g))
+    v, _ = torch.linalg.qr(torch.randn(n, n, device="cuda", dtype=torch.float64, generator=g))
+    sv = torch.logspace(0.0, -math.log10(LARGE_KAPPA), n, device="cuda", dtype=torch.float64)
+    a = ((u * sv) @ v.T).float()
+    del u, v
+    b = torch.randn(n, nrhs, device="cuda", generator=g)
+    at, bt = a.T.contiguous(), b.T.contiguous()
+    xt, work_a = torch.zeros_like(bt), torch.empty_like(at)
+    ta, tb, tx, tw = (aclsolver.pointer_table(t, 1, 0) for t in (at, bt, xt, work_a))
+    piv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    iters = torch.zeros(1, dtype=torch.int32, device="cuda")
+    berr = torch.zeros(1, dtype=torch.float64, device="cuda")
+    lw = C.c_int(0)
+    check(lib.aclsolverSgetrf_bufferSize(handle.value, n, n, work_a.data_ptr(), n, C.byref(lw)))
+    work = torch.empty(max(1, lw.value), device="cuda")
+    stream = handle.stream
+
+    def plain():
+        check(lib.aclsolverSgetrf(handle.value, n, n, work_a.data_ptr(), n, work.data_ptr(), piv.data_ptr(),
+                                  info.data_ptr()))
+        check(lib.aclsolverSgetrsBatched(handle.value, 0, n, nrhs, tw.data_ptr(), n, piv.data_ptr(), tx.data_ptr(), n,
+                                         info.data_ptr(), 1))
+
+    def mixed():
+        check(lib.aclsolverSgesvIrBatched(handle.value, aclsolver.FACTOR_BF16X3, n, nrhs, ta.data_ptr(), n,
+                                          tb.data_ptr(), n, tx.data_ptr(), n, 4, 1e-7, iters.data_ptr(),
+                                          berr.data_ptr(), info.data_ptr(), 1))
+
+    def timed(fn, restore):
+        best = []
+        for _ in range(steps + 1):
+            if restore:
+                work_a.copy_(at)
+                xt.copy_(bt)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            best.append(e0.elapsed_time(e1))
+        rest = sorted(best[1:]) or best
+        return rest[len(rest) // 2]  # median of the timed repetitions (after the first)
+
+    a64, b64 = a.double(), b.double()
+    x64 = torch.linalg.solve(a64, b64)
+    anorm = a64.abs().sum(dim=1).max()
+
+    def errors():
+        x = xt.T.double()
+        r = b64 - a64 @ x
+        be = r.abs().amax(dim=0) / (anorm * x.abs().amax(dim=0) + b64.abs().amax(dim=0))
+        fe = (x - x64).abs().amax(dim=0) / x64.abs().amax(dim=0)
+        return float(be.max()), float(fe.max())
+
+    plain_ms = timed(plain, True)
+    plain_be, plain_fe = errors()
+    mixed_ms = timed(mixed, False)
+    mixed_be, mixed_fe = errors()
+    flops = 2.0 * n ** 3 / 3 + 2.0 * n * n * nrhs
+    return {
+        "workload": f"one {n} x {n} system, A = U diag(s) V^T, kappa {LARGE_KAPPA:.0e}, {nrhs} right-hand sides",
+        "plain": {"path": "Sgetrf + SgetrsBatched (FP32)", "ms": round(plain_ms, 3),
+                  "gflops": round(flops / (plain_ms * 1e-3) / 1e9, 1), "berr_max": plain_be, "ferr_max": plain_fe},
+        "mixed": {"path": "SgesvIrBatched(BF16X3, tol 1e-7, maxIter 4)", "ms": round(mixed_ms, 3),
+                  "gflops": round(flops / (mixed_ms * 1e-3) / 1e9, 1), "berr_max": mixed_be, "ferr_max": mixed_fe,
+                  "iterations": int(iters.item()), "berr_reported": float(berr.item())},
+        "mixed_over_plain": round(plain_ms / mixed_ms, 3),
+    }
 
 
 def cpu_sample(count):
@@ -515,6 +609,17 @@ def run_profile():
     handle.close()
 
 
+def run_profile_large():
+    """The single large system for an ncu launch list: one plain factorisation and solve and
+    one split-BF16 refinement call (the measurement of the 'large' key, one repetition)."""
+    import aclsolver
+
+    handle = aclsolver.Handle()
+    out = measure_large(handle, steps=0)
+    print(json.dumps({"profile": "ok", "large": out}))
+    handle.close()
+
+
 def barrier(world):
     if world > 1:
         import torch.distributed as dist
@@ -540,6 +645,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-large", dest="large", action="store_false",
+                    help="skip the single 8192 x 8192 system reported under the 'large' key")
+    ap.add_argument("--profile-large", action="store_true",
+                    help="one large plain factorisation + solve and one large refinement call, for ncu")
     ap.add_argument("--profile", action="store_true",
                     help="run each hot kernel once on the workload (for an ncu capture) and exit")
     args = ap.parse_args()
@@ -557,6 +666,8 @@ def main():
     try:
         if args.profile:
             run_profile()
+        elif args.profile_large:
+            run_profile_large()
         elif args.impl == "reference":
             run_reference(args, rank, world)
         else:

@@ -95,10 +95,8 @@ __host__ __device__ size_t dyn_bytes(int n, int mode)
     const size_t trsm = ((size_t)W2 * LOP + (size_t)CT * LOP) * sizeof(float);
     const size_t tiles = mode == 0 ? ((size_t)W2 * LTP + (size_t)W2 * UTP) * sizeof(float)
                                    : (size_t)terms * ((size_t)RT * BHP + (size_t)CT * BHP) * sizeof(__nv_bfloat16);
-    // mixed U12 through X = L11^-1: the A12 tile's and X's BF16 halves (X behind FP32 L11 in BF16 mode)
-    const size_t xsplit = mode == 0 ? 0
-                          : mode == 1 ? (size_t)W2 * LOP * sizeof(float) + (size_t)RT * BHP * sizeof(__nv_bfloat16)
-                                      : 2 * ((size_t)CT * BHP + (size_t)RT * BHP) * sizeof(__nv_bfloat16);
+    // mixed U12 through X = L11^-1: X (FP32, 128 x LOP) and the A12 tile (128 x UTP), both FP32
+    const size_t xsplit = mode == 0 ? 0 : ((size_t)W2 * LOP + (size_t)W2 * UTP) * sizeof(float);
     size_t need = inner > trsm ? inner : trsm;
     need = need > xsplit ? need : xsplit;
     return need > tiles ? need : tiles;
@@ -683,11 +681,11 @@ __device__ __forceinline__ void mixed_outer_update(float (&acc)[2][4][4], const 
 // Mixed modes, U12 of the outer block: X = L11^-1 (unit lower, 128 x 128) is built once in
 // FP32 -- the four 32 x 32 diagonal inverses by substitution (a warp each, a lane per
 // column), then the off-diagonal blocks by distance, X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj
-// -- split into BF16 halves, and every 64-column tile of A12 becomes U12 = X A12 on the
-// tensor cores (three products).  Zero-pivot columns of L are zeroed first, so they take
+// -- and every 64-column tile of A12 becomes U12 = X A12 by FP32 FMAs: no serial chain over
+// the 128 rows, and FP32-level accuracy (a BF16 split of X and A12 cost the refinement a
+// correction on the worst-conditioned systems).  Zero-pivot columns of L are zeroed first, so they take
 // no part, as in the plain solve.  Layout while X is built: L(i, k) (i > k) at Lo[k][i] and
 // X(r, c) (c <= r) at Lo[r][c], the staged block's upper triangle being free.
-template <int TERMS>
 __device__ void mixed_outer_u12(float *A, int lda, int n, int K0, Shared &sh, unsigned char *dyn)
 {
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -773,67 +771,64 @@ __device__ void mixed_outer_u12(float *A, int lda, int n, int K0, Shared &sh, un
         }
         __syncthreads();
     }
-    // (3) X into BF16 halves xh/xl[row][k] at byte XO, behind the A12 tile's halves.  The
-    //     halves overlap FP32 rows >= 64 of X (split BF16) or nothing (BF16): those rows are
-    //     read into registers first, rows < 64 stay untouched in place until converted.
-    constexpr int XO = TERMS > 1 ? 2 * CT * BHP * 2 : W2 * LOP * 4;
-    __nv_bfloat16 *xh = reinterpret_cast<__nv_bfloat16 *>(dyn + XO);
-    __nv_bfloat16 *xl = xh + (size_t)RT * BHP;
+    // (3) X complete: the strictly upper part of Lo (the staged L values) is cleared, so
+    //     Lo[r][k] = X(r, k) for every k
+    for (int e = t; e < W2 * W2; e += BT)
     {
-        constexpr int PER = (W2 - 64) * W2 / BT;
-        float hv[PER];
-#pragma unroll
-        for (int u = 0; u < PER; ++u)
-        {
-            const int e = t + u * BT, row = 64 + e / W2, k = e % W2;
-            hv[u] = k <= row ? Lo[row * LOP + k] : 0.0f;
-        }
-        __syncthreads();
-        auto put = [&](int row, int k, float v) {
-            __nv_bfloat16 h, l;
-            split_bf16(v, h, l);
-            xh[(size_t)row * BHP + k] = h;
-            if (TERMS > 1) xl[(size_t)row * BHP + k] = l;
-        };
-#pragma unroll
-        for (int u = 0; u < PER; ++u)
-        {
-            const int e = t + u * BT;
-            put(64 + e / W2, e % W2, hv[u]);
-        }
-        for (int e = t; e < 64 * W2; e += BT)
-        {
-            const int row = e / W2, k = e % W2;
-            put(row, k, k <= row ? Lo[row * LOP + k] : 0.0f);
-        }
-        __syncthreads();
+        const int r = e / W2, k = e % W2;
+        if (k > r) Lo[r * LOP + k] = 0.0f;
     }
-    // (4) U12 = X A12, a 64-column tile at a time
-    __nv_bfloat16 *uh = reinterpret_cast<__nv_bfloat16 *>(dyn);
-    __nv_bfloat16 *ul = uh + (size_t)CT * BHP;
+    // (4) U12 = X A12 in FP32, a 64-column tile at a time: the tile staged k-major, thread
+    //     (tr, tc) computing rows tr + 16 i (i < 8, conflict-free X reads) by columns 4tc..+3
+    float *At = Lo + (size_t)W2 * LOP;  // At[k][col], pitch UTP
+    const int tr = t & 15, tc = t >> 4;
     for (int c0 = kend; c0 < n; c0 += CT)
     {
         const int nc = min(CT, n - c0);
+        __syncthreads();  // the previous tile's products are done with At (and (3) with Lo)
         staged_copy<16>(
             W2 * CT, [&](int e) { return e / W2 < nc ? A[(int64_t)(c0 + e / W2) * lda + K0 + e % W2] : 0.0f; },
-            [&](int e, float v) {
-                __nv_bfloat16 h, l;
-                split_bf16(v, h, l);
-                uh[(size_t)(e / W2) * BHP + e % W2] = h;
-                if (TERMS > 1) ul[(size_t)(e / W2) * BHP + e % W2] = l;
-            });
+            [&](int e, float v) { At[(e % W2) * UTP + e / W2] = v; });
         __syncthreads();
-        float acc[2][4][4];
+        float acc[8][4];
 #pragma unroll
-        for (int mi = 0; mi < 2; ++mi)
+        for (int i = 0; i < 8; ++i)
 #pragma unroll
-            for (int ni = 0; ni < 4; ++ni)
+            for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+#pragma unroll 2
+        for (int k4 = 0; k4 < W2; k4 += 4)
+        {
+            float4 xr[8];
 #pragma unroll
-                for (int e = 0; e < 4; ++e) acc[mi][ni][e] = 0.0f;
-        mixed_outer_update<TERMS>(acc, xh, xl, uh, ul);
-        mixed_c_store(A, lda, W2, K0, c0, nc, 0, acc);
-        __syncthreads();
+            for (int i = 0; i < 8; ++i)
+                xr[i] = *reinterpret_cast<const float4 *>(Lo + (size_t)(16 * i + tr) * LOP + k4);
+            float4 ak[4];
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) ak[kk] = *reinterpret_cast<const float4 *>(At + (k4 + kk) * UTP + 4 * tc);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)
+            {
+                const float a4[4] = {ak[kk].x, ak[kk].y, ak[kk].z, ak[kk].w};
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+                {
+                    const float xv = kk == 0 ? xr[i].x : kk == 1 ? xr[i].y : kk == 2 ? xr[i].z : xr[i].w;
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] = fma_rn(xv, a4[j], acc[i][j]);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            const int cj = 4 * tc + j;
+            if (cj >= nc) continue;
+            float *col = A + (int64_t)(c0 + cj) * lda + K0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) col[16 * i + tr] = acc[i][j];
+        }
     }
+    __syncthreads();  // the next stage reuses the shared area
 }
 
 template <int MODE, int TERMS>
@@ -903,7 +898,7 @@ __device__ void outer_update(float *A, int lda, int n, int K0, bool vec, Shared 
     //     every 32-row chunk; chunk ci is solved (shuffles among the four), then applied to
     //     the rows of the later chunks, in ascending k for every element
     if (MODE != 0)
-        mixed_outer_u12<TERMS>(A, lda, n, K0, sh, dyn);
+        mixed_outer_u12(A, lda, n, K0, sh, dyn);
     else
     {
     float *Lo = reinterpret_cast<float *>(dyn);
