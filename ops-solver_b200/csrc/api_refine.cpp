@@ -36,15 +36,16 @@ aclsolverStatus_t gesv_ir_large(Handle *h, int mode, int n, int nrhs, const floa
                                 double tol, int *iterArray, double *berrArray, int *infoArray)
 {
     cudaStream_t st = h->stream;
-    const size_t sizes[6] = {(size_t)n * n * sizeof(float), (size_t)n * sizeof(int), sizeof(LargeStatus),
-                             large_solve_scratch_bytes(n, nrhs), 256, large_ir_bytes(n, nrhs)};
+    const size_t sizes[7] = {(size_t)n * n * sizeof(float), (size_t)n * sizeof(int), sizeof(LargeStatus),
+                             large_solve_scratch_bytes(n, nrhs), 256, large_ir_bytes(n, nrhs),
+                             mode != 0 ? umma_scratch_bytes(n, n) : 0};
     size_t total = 0;
     for (size_t v : sizes) total += round_up(v);
     ScratchBlock *blk = acquire_scratch(h, total);
     if (!blk) return ACLSOLVER_STATUS_ALLOC_FAILED;
     char *p = static_cast<char *>(blk->ptr);
-    void *part[6];
-    for (int i = 0; i < 6; ++i)
+    void *part[7];
+    for (int i = 0; i < 7; ++i)
     {
         part[i] = p;
         p += round_up(sizes[i]);
@@ -59,7 +60,8 @@ aclsolverStatus_t gesv_ir_large(Handle *h, int mode, int n, int nrhs, const floa
     RealBatch fac{lu, nullptr, n, n, 0, 1};
     int hinfo = 0, running = 0;
     cudaError_t e = launch_copy_matrices(src, fac, n, st);
-    if (e == cudaSuccess) e = launch_getrf_large(lu, n, n, n, ipiv, infoArray, status, mode, st);
+    if (e == cudaSuccess)
+        e = launch_getrf_large(lu, n, n, n, ipiv, infoArray, status, mode, st, mode != 0 ? part[6] : nullptr);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&hinfo, infoArray, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     auto solve = [&]() {

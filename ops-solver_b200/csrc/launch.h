@@ -83,7 +83,12 @@ struct LargeStatus
 // null (no pivoting); *info receives the first zero pivot (1-based) or 0.  mode 0: plain
 // FP32 in the oracle's order; 1 / 3: BF16 / split-BF16 trailing updates on the tensor cores.
 cudaError_t launch_getrf_large(float *A, int m, int n, int lda, int *ipiv, int *info, LargeStatus *st, int mode,
-                               cudaStream_t stream);
+                               cudaStream_t stream, void *umma_scratch = nullptr);
+// Mixed modes: the rank-128 outer updates on tcgen05 tensor cores (lu_large_umma.cu), with
+// umma_scratch_bytes(m, n) of device scratch for the operands' BF16 halves.
+size_t umma_scratch_bytes(int m, int n);
+cudaError_t launch_umma_update(float *A, int lda, int m, int n, int K0, int kend, int bend, int terms,
+                               LargeStatus *st, void *scratch, cudaStream_t stream);
 
 // Solve with the factors of launch_getrf_large (or any LAPACK-layout LU) over the whole GPU:
 // A is A1 or slot 0 of At, X (n x nrhs, ldx) is X1 or slot 0 of Xt and is overwritten; ipiv

@@ -12,7 +12,8 @@
 //   * interchanges: the panel's changed positions moved in every column of the matrix;
 //   * inside the outer block: U12 = L11^-1 A12 and A22 -= L21 U12 on its columns only;
 //   * once per outer block: U12 with the 128 x 128 L11 and one rank-128 update of the
-//     trailing matrix (FP32 FFMA2 tiles, or split-BF16 tensor-core tiles in mixed mode).
+//     trailing matrix (FP32 FFMA2 tiles; in mixed mode split-BF16 products on the tcgen05
+//     tensor cores with the accumulator in tensor memory, lu_large_umma.cu).
 // Plain mode keeps the oracle's per-element order -- every element receives fma(-l, u, a)
 // in ascending k, zero-pivot columns skipped, IEEE division by the pivot -- so factors,
 // pivots and info equal the unblocked order bit for bit.
@@ -871,7 +872,7 @@ void gemm_launch(int mode, float *A, int lda, int r0, int rows, int c0, int cols
 // One matrix, m x n, n <= m <= LARGE_MAX_ROWS; mode 0 plain FP32 (the oracle's order), 1 BF16,
 // 3 split BF16 trailing updates (pivot search by packed key, reciprocal multiply).
 cudaError_t launch_getrf_large(float *A, int m, int n, int lda, int *ipiv, int *info, LargeStatus *st, int mode,
-                               cudaStream_t stream)
+                               cudaStream_t stream, void *umma_scratch)
 {
     if (m > LARGE_MAX_ROWS || n > LARGE_MAX_COLS) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(st, 0, sizeof(LargeStatus), stream);
@@ -918,7 +919,13 @@ cudaError_t launch_getrf_large(float *A, int m, int n, int lda, int *ipiv, int *
             {
                 large_trsm_kernel<OB><<<(n - bend + 63) / 64, 256, (OB * (OB + 4) + 64 * (OB + 4)) * sizeof(float),
                                         stream>>>(A, lda, K0, bend, n - bend, st);
-                gemm_launch(mode, A, lda, kend, m - kend, bend, n - bend, K0, OB, st, stream);
+                if (mode != 0 && umma_scratch)
+                {
+                    e = launch_umma_update(A, lda, m, n, K0, kend, bend, mode == 1 ? 1 : 3, st, umma_scratch, stream);
+                    if (e != cudaSuccess) return e;
+                }
+                else
+                    gemm_launch(mode, A, lda, kend, m - kend, bend, n - bend, K0, OB, st, stream);
             }
         }
         e = cudaGetLastError();
