@@ -92,12 +92,17 @@ __global__ void __launch_bounds__(ST) large_sweep_kernel(const float *A1, const 
     extern __shared__ __align__(16) float sm[];
     float *D = sm;                   // D[k][i] = A(b0 + i, b0 + k), pitch SBP4
     float *xs = D + SB * SBP4;       // xs[r][i]: the block's solution, pitch SB
+    float *S = xs + LARGE_SOLVE_MAX_RHS * SB;  // S[k][i]: the strip's columns, pitch SBP4
     const int t = threadIdx.x;
     const int b0 = b * SB, w = min(SB, n - b0);
     const bool vec = (reinterpret_cast<uintptr_t>(A) & 15u) == 0 && (lda & 3) == 0 && w == SB;
     stage_tile(D, SBP4, A + (int64_t)b0 * lda + b0, lda, w, w, vec);
     stage_tile(xs, SB, Y + b0, n, w, nrhs, (n & 3) == 0 && w == SB);
-    tile_wait();
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    // the strip's columns are fetched while the diagonal block is solved
+    const int s = FORWARD ? b + blockIdx.x : b - blockIdx.x;
+    const int s0 = s * SB, sw = min(SB, n - s0);
+    if (blockIdx.x > 0) stage_tile(S, SBP4, A + (int64_t)b0 * lda + s0, lda, sw, w, vec && sw == SB);
     __syncthreads();
     // the diagonal block in 32-row sub-blocks: each sub-block's triangle by one warp per two
     // right-hand sides (a lane per row, the solved entry broadcast by shuffle), then the
@@ -177,15 +182,10 @@ __global__ void __launch_bounds__(ST) large_sweep_kernel(const float *A1, const 
         return;
     }
     // a strip of 128 rows below (forward) or above (backward): Y[rows] -= A[rows, block] x
-    const int s = FORWARD ? b + blockIdx.x : b - blockIdx.x;
-    const int s0 = s * SB, sw = min(SB, n - s0);
     // thread: row s0 + (t % 128), right-hand sides (t / 128), +2, ... (at most eight)
     constexpr int RPT = LARGE_SOLVE_MAX_RHS / (ST / SB);
     const int i = t % SB, r0 = t / SB;
-    // the strip's L (or U) columns into the diagonal block's buffer (its solve is done)
-    __syncthreads();
-    stage_tile(D, SBP4, A + (int64_t)b0 * lda + s0, lda, sw, w, vec && sw == SB);
-    tile_wait();
+    tile_wait();  // the strip (each thread its own copies), then everyone's
     __syncthreads();
     float acc[RPT];
     if (i >= sw) return;
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(ST) large_sweep_kernel(const float *A1, const 
     for (int kk = 0; kk < w; ++kk)
     {
         const int k = FORWARD ? kk : w - 1 - kk;
-        const float l = D[k * SBP4 + i];
+        const float l = S[k * SBP4 + i];
 #pragma unroll
         for (int q = 0; q < RPT; ++q) acc[q] = fma_rn(-l, xs[(r0 + q * (ST / SB)) * SB + k], acc[q]);
     }
@@ -224,7 +224,7 @@ cudaError_t launch_getrs_large(const float *A, const float *const *At, int lda, 
     if (n > LARGE_MAX_COLS || nrhs > LARGE_SOLVE_MAX_RHS) return cudaErrorInvalidValue;
     float *Y = static_cast<float *>(scratch);
     int *perm = reinterpret_cast<int *>(Y + (size_t)n * nrhs);
-    const size_t smem = (SB * SBP4 + (size_t)LARGE_SOLVE_MAX_RHS * SB) * sizeof(float);
+    const size_t smem = (2 * SB * SBP4 + (size_t)LARGE_SOLVE_MAX_RHS * SB) * sizeof(float);
     static bool attr = false;
     if (!attr)
     {
