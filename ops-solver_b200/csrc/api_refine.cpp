@@ -36,16 +36,16 @@ aclsolverStatus_t gesv_ir_large(Handle *h, int mode, int n, int nrhs, const floa
                                 double tol, int *iterArray, double *berrArray, int *infoArray)
 {
     cudaStream_t st = h->stream;
-    const size_t sizes[7] = {(size_t)n * n * sizeof(float), (size_t)n * sizeof(int), sizeof(LargeStatus),
+    const size_t sizes[8] = {(size_t)n * n * sizeof(float), (size_t)n * sizeof(int), sizeof(LargeStatus),
                              large_solve_scratch_bytes(n, nrhs), 256, large_ir_bytes(n, nrhs),
-                             mode != 0 ? umma_scratch_bytes(n, n) : 0};
+                             mode != 0 ? umma_scratch_bytes(n, n) : 0, (size_t)n * sizeof(int)};
     size_t total = 0;
     for (size_t v : sizes) total += round_up(v);
     ScratchBlock *blk = acquire_scratch(h, total);
     if (!blk) return ACLSOLVER_STATUS_ALLOC_FAILED;
     char *p = static_cast<char *>(blk->ptr);
-    void *part[7];
-    for (int i = 0; i < 7; ++i)
+    void *part[8];
+    for (int i = 0; i < 8; ++i)
     {
         part[i] = p;
         p += round_up(sizes[i]);
@@ -64,12 +64,15 @@ aclsolverStatus_t gesv_ir_large(Handle *h, int mode, int n, int nrhs, const floa
         e = launch_getrf_large(lu, n, n, n, ipiv, infoArray, status, mode, st, mode != 0 ? part[6] : nullptr);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&hinfo, infoArray, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    int *perm = static_cast<int *>(part[7]);  // the pivots composed once for every solve
     auto solve = [&]() {
-        return launch_getrs_large(lu, nullptr, n, n, ipiv, s.r32, nullptr, n, nrhs, solve_scratch, flags, nullptr, st);
+        return launch_getrs_large(lu, nullptr, n, n, nullptr, s.r32, nullptr, n, nrhs, solve_scratch, flags, nullptr, st,
+                                  perm);
     };
     if (e == cudaSuccess && hinfo == 0)
     {
-        e = launch_lir_init(s, Barray, ldb, n, nrhs, st);
+        e = launch_large_perm(ipiv, n, perm, flags, st);
+        if (e == cudaSuccess) e = launch_lir_init(s, Barray, ldb, n, nrhs, st);
         if (e == cudaSuccess) e = solve();
         if (e == cudaSuccess) e = launch_lir_update(s, n, nrhs, 1, st);
         if (e == cudaSuccess) e = launch_lir_residual(s, Aarray, lda, Barray, ldb, n, nrhs, tol, 1, st);

@@ -47,7 +47,7 @@ __global__ void lir_update(LargeIr s, int n, int nrhs, int first)
 // chunk's |A| row sums
 __global__ void __launch_bounds__(RB) lir_partial(const float *const *Aarr, int lda, int n, int nrhs, LargeIr s)
 {
-    __shared__ double xs[XS][MAXR];
+    __shared__ double xs[XS][MAXR + 1];
     const float *A = slot(Aarr, 0);
     const int t = threadIdx.x;
     const int i = blockIdx.x * RB + t;
@@ -61,20 +61,20 @@ __global__ void __launch_bounds__(RB) lir_partial(const float *const *Aarr, int 
         __syncthreads();
         for (int e = t; e < XS * MAXR; e += RB)
         {
-            const int jj = e / MAXR, r = e % MAXR;
+            const int r = e / XS, jj = e % XS;  // consecutive threads: consecutive columns of x
             xs[jj][r] = (jb + jj < j1 && r < nrhs) ? s.x64[(int64_t)r * n + jb + jj] : 0.0;
         }
         __syncthreads();
         if (i < n)
         {
             const int je = min(XS, j1 - jb);
-            for (int jj = 0; jj < je; jj += 8)
+            for (int jj = 0; jj < je; jj += 16)
             {
-                double av[8];  // eight loads in flight before their products
+                double av[16];  // sixteen loads in flight before their products
 #pragma unroll
-                for (int u = 0; u < 8; ++u) av[u] = jj + u < je ? (double)A[(int64_t)(jb + jj + u) * lda + i] : 0.0;
+                for (int u = 0; u < 16; ++u) av[u] = jj + u < je ? (double)A[(int64_t)(jb + jj + u) * lda + i] : 0.0;
 #pragma unroll
-                for (int u = 0; u < 8; ++u)
+                for (int u = 0; u < 16; ++u)
                 {
                     asum += fabs(av[u]);
 #pragma unroll
@@ -85,7 +85,9 @@ __global__ void __launch_bounds__(RB) lir_partial(const float *const *Aarr, int 
     }
     if (i >= n) return;
     const int nch = gridDim.y;
-    for (int r = 0; r < nrhs; ++r) s.part[((int64_t)blockIdx.y * MAXR + r) * n + i] = acc[r];
+#pragma unroll
+    for (int r = 0; r < MAXR; ++r)  // static indices: acc stays in registers
+        if (r < nrhs) s.part[((int64_t)blockIdx.y * MAXR + r) * n + i] = acc[r];
     s.apart[(int64_t)blockIdx.y * n + i] = asum;
     (void)nch;
 }

@@ -217,9 +217,16 @@ size_t large_solve_scratch_bytes(int n, int nrhs)
     return (size_t)n * nrhs * sizeof(float) + (size_t)n * sizeof(int) + 16;
 }
 
+cudaError_t launch_large_perm(const int *ipiv, int n, int *perm, int *bad, cudaStream_t stream)
+{
+    if (n > LARGE_MAX_COLS) return cudaErrorInvalidValue;
+    large_perm_kernel<<<1, 1024, 0, stream>>>(ipiv, n, perm, bad);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_getrs_large(const float *A, const float *const *At, int lda, int n, const int *ipiv, float *X,
                                float *const *Xt, int ldx, int nrhs, void *scratch, int *bad, int *info,
-                               cudaStream_t stream)
+                               cudaStream_t stream, const int *perm_in)
 {
     if (n > LARGE_MAX_COLS || nrhs > LARGE_SOLVE_MAX_RHS) return cudaErrorInvalidValue;
     float *Y = static_cast<float *>(scratch);
@@ -236,16 +243,19 @@ cudaError_t launch_getrs_large(const float *A, const float *const *At, int lda, 
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    if (ipiv)
+    const int *use = perm_in;  // a permutation composed earlier (its *bad already set)
+    if (!use && ipiv)
+    {
         large_perm_kernel<<<1, 1024, 0, stream>>>(ipiv, n, perm, bad);
-    else
+        use = perm;
+    }
+    else if (!use)
     {
         cudaError_t e = cudaMemsetAsync(bad, 0, sizeof(int), stream);
         if (e != cudaSuccess) return e;
     }
     const int64_t total = (int64_t)n * nrhs;
-    large_gather_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(X, Xt, ldx, n, nrhs,
-                                                                             ipiv ? perm : nullptr, Y);
+    large_gather_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(X, Xt, ldx, n, nrhs, use, Y);
     const int nb = (n + SB - 1) / SB;
     for (int b = 0; b < nb; ++b)
         large_sweep_kernel<true><<<nb - b, ST, smem, stream>>>(A, At, lda, n, Y, nrhs, b, bad);
