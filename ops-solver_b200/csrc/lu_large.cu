@@ -4,7 +4,8 @@
 // swap/trsm, product and subtract kernels; host entry src/sgetrf/sgetrf_host.cpp:96-124).
 //
 // Right-looking, two-level: 32-column panels inside 128-column outer blocks.
-//   * panel (a cluster of eight 256-thread blocks, up to four panel rows per thread): per column,
+//   * panel (a cluster of sixteen 256-thread blocks, or eight where sixteen cannot be placed;
+//     up to two / four panel rows per thread): per column,
 //     each block finds its candidate (warp reduction, block barrier), publishes it into
 //     every block of the cluster through distributed shared memory, one cluster barrier,
 //     and every block picks the same winner; rows are never moved during the panel, final
@@ -32,7 +33,7 @@ namespace
 constexpr int LT = 256;       // panel threads per block (one block per SM: up to 255 registers)
 constexpr int LNW = LT / 32;  // panel warps per block
 constexpr int PW = 32;        // panel width
-constexpr int CSZ = 8;        // blocks per panel cluster
+// blocks per panel cluster: 16 where the GPU can place it, else 8 (panel_cluster_size)
 constexpr int OB = 128;       // outer block
 constexpr unsigned FULL = 0xffffffffu;
 static_assert(32 % LNW == 0, "the block winner is read one warp report per lane group");
@@ -44,7 +45,6 @@ static_assert(32 % LNW == 0, "the block winner is read one warp report per lane 
 // sets the status's error flag, and from then on no panel waits again (the factors are
 // invalid and reported so), which keeps the whole factorisation's run time bounded.
 constexpr unsigned CAND_BYTES = PW * sizeof(float) + sizeof(uint4);
-constexpr unsigned STEP_BYTES = CSZ * CAND_BYTES;
 constexpr long long WAIT_LIMIT = 1ll << 16;  // try_wait rounds (each suspends for a while)
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -89,13 +89,14 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity)
     return false;
 }
 
+template <int CS>
 struct __align__(16) PanelShared
 {
     float slot[2][LNW][PW];  // each warp's best row, double buffered by column parity
     uint2 key[2][LNW];       // each warp's (best key, its position)
     int krow[2][LNW];        // each warp's best row (panel-relative)
-    float cand[2][CSZ][PW];  // each cluster block's candidate row (written by that block)
-    uint4 ckey[2][CSZ];      // each cluster block's (key, position, row, 0)
+    float cand[2][CS][PW];   // each cluster block's candidate row (written by that block)
+    uint4 ckey[2][CS];       // each cluster block's (key, position, row, 0)
     unsigned long long bar[2];  // per column parity: the cluster's candidates have landed
     unsigned zmask;
     int first_zero;
@@ -104,17 +105,20 @@ struct __align__(16) PanelShared
 // ---------------------------------------------------------------------------------------
 // panel: rows k0 .. m-1, columns k0 .. k0+w-1 of A (positions relative to k0)
 // ---------------------------------------------------------------------------------------
-template <bool EXACT, int NR>
-__global__ void __cluster_dims__(CSZ, 1, 1) __launch_bounds__(LT, 1)
+template <bool EXACT, int NR, int CS>
+__global__ void __launch_bounds__(LT, 1)
     large_panel_kernel(float *A, int lda, int m, int k0, int w, int *ipiv, LargeStatus *st)
 {
     constexpr int NP = PW / 2;
-    __shared__ PanelShared sh;
+    constexpr unsigned STEP_BYTES = CS * CAND_BYTES;
+    constexpr int PL = 32 / CS;   // lanes of warp 0 per destination block
+    constexpr int PER = PW / PL;  // candidate values each of them sends
+    __shared__ PanelShared<CS> sh;
     cg::cluster_group cluster = cg::this_cluster();
     const int c = (int)cluster.block_rank();
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int mr = m - k0;
-    const int R = (mr + CSZ - 1) / CSZ;  // rows per block, at most NR * LT
+    const int R = (mr + CS - 1) / CS;  // rows per block, at most NR * LT
     const int r0 = c * R;
     const int mine = max(0, min(R, mr - r0));  // rows of this block
     const bool active = warp * 32 < mine;      // warp-uniform: its first row is present
@@ -207,19 +211,19 @@ __global__ void __cluster_dims__(CSZ, 1, 1) __launch_bounds__(LT, 1)
                 const unsigned gmax = __reduce_max_sync(FULL, kw.x);
                 const unsigned gpos = __reduce_min_sync(FULL, kw.x == gmax ? kw.y : 0xffffffffu);
                 const int gw = __ffs(__ballot_sync(FULL, kw.x == gmax && kw.y == gpos)) - 1;
-                const unsigned dest = lane >> 2, part = lane & 3;
-                const float4 *src = reinterpret_cast<const float4 *>(sh.slot[buf][gw]) + 2 * part;
+                const unsigned dest = lane / PL, part = lane % PL;
+                const float4 *src = reinterpret_cast<const float4 *>(sh.slot[buf][gw]) + (PER / 4) * part;
                 const unsigned rbar = cluster_addr(smem_addr(&sh.bar[buf]), dest);
-                const unsigned rc = cluster_addr(smem_addr(&sh.cand[buf][c][8 * part]), dest);
-                st_async_v4(rc, src[0], rbar);
-                st_async_v4(rc + 16, src[1], rbar);
+                const unsigned rc = cluster_addr(smem_addr(&sh.cand[buf][c][PER * part]), dest);
+#pragma unroll
+                for (int v = 0; v < PER / 4; ++v) st_async_v4(rc + 16 * v, src[v], rbar);
                 if (part == 0)
                     st_async_v4u(cluster_addr(smem_addr(&sh.ckey[buf][c]), dest),
                                  make_uint4(gmax, gpos, (unsigned)sh.krow[buf][gw], 0u), rbar);
             }
             if (ok && !mbar_wait(smem_addr(&sh.bar[buf]), (unsigned)(j >> 1) & 1u)) ok = false;
             // (3) the cluster's winner: largest key, then the smallest position
-            const uint4 kc = lane < CSZ ? sh.ckey[buf][lane] : make_uint4(0u, 0xffffffffu, 0u, 0u);
+            const uint4 kc = lane < CS ? sh.ckey[buf][lane] : make_uint4(0u, 0xffffffffu, 0u, 0u);
             const unsigned gmax = __reduce_max_sync(FULL, kc.x);
             const unsigned gpos = __reduce_min_sync(FULL, kc.x == gmax ? kc.y : 0xffffffffu);
             const int gc = __ffs(__ballot_sync(FULL, kc.x == gmax && kc.y == gpos)) - 1;
@@ -842,18 +846,68 @@ __global__ void large_info_kernel(int *info, const LargeStatus *st) { *info = st
 
 namespace
 {
-template <bool EXACT>
-void panel_launch(float *A, int lda, int m, int k0, int w, int *ipiv, LargeStatus *st, cudaStream_t stream)
+template <bool EXACT, int NR, int CS>
+cudaError_t panel_launch_cs(float *A, int lda, int m, int k0, int w, int *ipiv, LargeStatus *st, cudaStream_t stream)
 {
-    const int per = ((m - k0 + CSZ - 1) / CSZ + LT - 1) / LT;  // rows per thread
-    if (per <= 1)
-        large_panel_kernel<EXACT, 1><<<CSZ, LT, 0, stream>>>(A, lda, m, k0, w, ipiv, st);
-    else if (per == 2)
-        large_panel_kernel<EXACT, 2><<<CSZ, LT, 0, stream>>>(A, lda, m, k0, w, ipiv, st);
-    else if (per == 3)
-        large_panel_kernel<EXACT, 3><<<CSZ, LT, 0, stream>>>(A, lda, m, k0, w, ipiv, st);
-    else
-        large_panel_kernel<EXACT, 4><<<CSZ, LT, 0, stream>>>(A, lda, m, k0, w, ipiv, st);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(CS);
+    cfg.blockDim = dim3(LT);
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = CS;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, large_panel_kernel<EXACT, NR, CS>, A, lda, m, k0, w, ipiv, st);
+}
+
+// The cluster size: 16 blocks (two panel rows per thread at 8192) when the device can place
+// such a cluster of this kernel, otherwise the portable 8.
+int panel_cluster_size()
+{
+    static int cs = 0;
+    if (cs) return cs;
+    cs = 8;
+    const void *fn = reinterpret_cast<const void *>(large_panel_kernel<true, 2, 16>);
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess &&
+        cudaFuncSetAttribute(reinterpret_cast<const void *>(large_panel_kernel<false, 2, 16>),
+                             cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess &&
+        cudaFuncSetAttribute(reinterpret_cast<const void *>(large_panel_kernel<true, 1, 16>),
+                             cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess &&
+        cudaFuncSetAttribute(reinterpret_cast<const void *>(large_panel_kernel<false, 1, 16>),
+                             cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess)
+    {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(16);
+        cfg.blockDim = dim3(LT);
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 16;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, fn, &cfg) == cudaSuccess && clusters >= 1) cs = 16;
+    }
+    cudaGetLastError();  // a refused query leaves no error behind
+    return cs;
+}
+
+template <bool EXACT>
+cudaError_t panel_launch(float *A, int lda, int m, int k0, int w, int *ipiv, LargeStatus *st, cudaStream_t stream)
+{
+    const int cs = panel_cluster_size();
+    const int per = ((m - k0 + cs - 1) / cs + LT - 1) / LT;  // rows per thread
+    if (cs == 16)
+        return per <= 1 ? panel_launch_cs<EXACT, 1, 16>(A, lda, m, k0, w, ipiv, st, stream)
+                        : panel_launch_cs<EXACT, 2, 16>(A, lda, m, k0, w, ipiv, st, stream);
+    if (per <= 1) return panel_launch_cs<EXACT, 1, 8>(A, lda, m, k0, w, ipiv, st, stream);
+    if (per == 2) return panel_launch_cs<EXACT, 2, 8>(A, lda, m, k0, w, ipiv, st, stream);
+    if (per == 3) return panel_launch_cs<EXACT, 3, 8>(A, lda, m, k0, w, ipiv, st, stream);
+    return panel_launch_cs<EXACT, 4, 8>(A, lda, m, k0, w, ipiv, st, stream);
 }
 
 void gemm_launch(int mode, float *A, int lda, int r0, int rows, int c0, int cols, int K0, int KW, LargeStatus *st,
@@ -895,10 +949,9 @@ cudaError_t launch_getrf_large(float *A, int m, int n, int lda, int *ipiv, int *
         for (int k0 = K0; k0 < kend; k0 += PW)
         {
             const int w = std::min(PW, kmin - k0);
-            if (mode == 0)
-                panel_launch<true>(A, lda, m, k0, w, ipiv, st, stream);
-            else
-                panel_launch<false>(A, lda, m, k0, w, ipiv, st, stream);
+            e = mode == 0 ? panel_launch<true>(A, lda, m, k0, w, ipiv, st, stream)
+                          : panel_launch<false>(A, lda, m, k0, w, ipiv, st, stream);
+            if (e != cudaSuccess) return e;
             // the outer block's columns (the panel's included: it holds final values by row)
             large_swap_kernel<<<(bend - K0 + 8 * SW_COLS - 1) / (8 * SW_COLS), 256, 0, stream>>>(A, lda, K0, bend, k0,
                                                                                             st);
