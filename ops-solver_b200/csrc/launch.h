@@ -89,6 +89,12 @@ cudaError_t launch_getrf_large(float *A, int m, int n, int lda, int *ipiv, int *
 size_t umma_scratch_bytes(int m, int n);
 cudaError_t launch_umma_update(float *A, int lda, int m, int n, int K0, int kend, int bend, int terms,
                                LargeStatus *st, void *scratch, cudaStream_t stream);
+// The same in two steps: the BF16 halves of L21 and U12 (columns [bend, n)), then the update
+// of columns [c_begin, c_end) within them.
+cudaError_t launch_umma_split(float *A, int lda, int m, int n, int K0, int kend, int bend, LargeStatus *st,
+                              void *scratch, cudaStream_t stream);
+cudaError_t launch_umma_range(float *A, int lda, int m, int n, int kend, int bend, int c_begin, int c_end, int terms,
+                              LargeStatus *st, void *scratch, cudaStream_t stream);
 
 // Solve with the factors of launch_getrf_large (or any LAPACK-layout LU) over the whole GPU:
 // A is A1 or slot 0 of At, X (n x nrhs, ldx) is X1 or slot 0 of Xt and is overwritten; ipiv

@@ -21,6 +21,8 @@
 #include <cooperative_groups.h>
 #include <cuda_bf16.h>
 
+#include <mutex>
+
 #include "common.cuh"
 #include "launch.h"
 
@@ -925,14 +927,47 @@ void gemm_launch(int mode, float *A, int lda, int r0, int rows, int c0, int cols
 
 // One matrix, m x n, n <= m <= LARGE_MAX_ROWS; mode 0 plain FP32 (the oracle's order), 1 BF16,
 // 3 split BF16 trailing updates (pivot search by packed key, reciprocal multiply).
+namespace
+{
+// Look-ahead streams of one device: the panel chain runs on a high-priority stream, the bulk
+// of each outer block's trailing update on a low-priority one, forked from and joined back to
+// the caller's stream with events (capturable).  Created on first use, kept for the process;
+// calls from several host threads enqueue one at a time (their work then runs in order).
+struct LookAhead
+{
+    cudaStream_t hi = nullptr, lo = nullptr;
+    cudaEvent_t fork = nullptr, part_a = nullptr, part_b = nullptr, join_hi = nullptr, join_lo = nullptr;
+};
+cudaError_t look_ahead(LookAhead *&out)
+{
+    static LookAhead devs[64];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    LookAhead &la = devs[dev];
+    if (!la.hi)
+    {
+        int least = 0, greatest = 0;
+        e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&la.hi, cudaStreamNonBlocking, greatest);
+        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&la.lo, cudaStreamNonBlocking, least);
+        cudaEvent_t *evs[5] = {&la.fork, &la.part_a, &la.part_b, &la.join_hi, &la.join_lo};
+        for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(evs[i], cudaEventDisableTiming);
+        if (e != cudaSuccess) return e;
+    }
+    out = &la;
+    return cudaSuccess;
+}
+}  // namespace
+
 cudaError_t launch_getrf_large(float *A, int m, int n, int lda, int *ipiv, int *info, LargeStatus *st, int mode,
                                cudaStream_t stream, void *umma_scratch)
 {
     if (m > LARGE_MAX_ROWS || n > LARGE_MAX_COLS) return cudaErrorInvalidValue;
-    cudaError_t e = cudaMemsetAsync(st, 0, sizeof(LargeStatus), stream);
-    if (e != cudaSuccess) return e;
     const int kmin = std::min(m, n);
     static bool attr = false;
+    cudaError_t e = cudaSuccess;
     if (!attr)
     {
         e = cudaFuncSetAttribute(large_trsm_kernel<OB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -942,6 +977,18 @@ cudaError_t launch_getrf_large(float *A, int m, int n, int lda, int *ipiv, int *
         if (e != cudaSuccess) return e;
         attr = true;
     }
+    static std::mutex enqueue;
+    std::lock_guard<std::mutex> lock(enqueue);
+    LookAhead *la = nullptr;
+    e = look_ahead(la);
+    if (e != cudaSuccess) return e;
+    cudaStream_t hs = la->hi, ls = la->lo;
+    e = cudaEventRecord(la->fork, stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(hs, la->fork, 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ls, la->fork, 0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(st, 0, sizeof(LargeStatus), hs);
+    if (e != cudaSuccess) return e;
+    const bool tcgen = mode != 0 && umma_scratch;
     for (int K0 = 0; K0 < kmin; K0 += OB)
     {
         const int kend = std::min(kmin, K0 + OB);
@@ -949,45 +996,75 @@ cudaError_t launch_getrf_large(float *A, int m, int n, int lda, int *ipiv, int *
         for (int k0 = K0; k0 < kend; k0 += PW)
         {
             const int w = std::min(PW, kmin - k0);
-            e = mode == 0 ? panel_launch<true>(A, lda, m, k0, w, ipiv, st, stream)
-                          : panel_launch<false>(A, lda, m, k0, w, ipiv, st, stream);
+            e = mode == 0 ? panel_launch<true>(A, lda, m, k0, w, ipiv, st, hs)
+                          : panel_launch<false>(A, lda, m, k0, w, ipiv, st, hs);
             if (e != cudaSuccess) return e;
             // the outer block's columns (the panel's included: it holds final values by row)
-            large_swap_kernel<<<(bend - K0 + 8 * SW_COLS - 1) / (8 * SW_COLS), 256, 0, stream>>>(A, lda, K0, bend, k0,
-                                                                                            st);
+            large_swap_kernel<<<(bend - K0 + 8 * SW_COLS - 1) / (8 * SW_COLS), 256, 0, hs>>>(A, lda, K0, bend, k0, st);
             const int jt = k0 + w;
             if (jt < bend && k0 + w < m)
             {
                 large_trsm_kernel<PW><<<(bend - jt + 63) / 64, 256, (PW * (PW + 4) + 64 * (PW + 4)) * sizeof(float),
-                                        stream>>>(A, lda, k0, jt, bend - jt, st);
-                gemm_launch(mode, A, lda, jt, m - jt, jt, bend - jt, k0, PW, st, stream);
+                                        hs>>>(A, lda, k0, jt, bend - jt, st);
+                gemm_launch(mode, A, lda, jt, m - jt, jt, bend - jt, k0, PW, st, hs);
             }
         }
         if (bend < n)
         {
-            // the block's interchanges on the columns to its right, then its U12 and update
-            large_block_swap_kernel<<<std::min(148, (n - bend + 7) / 8), 256, 0, stream>>>(
+            // the previous block's update of these columns is complete; then this block's
+            // interchanges on the columns to its right, its U12, and its update: the next
+            // block's columns on the high-priority stream (its panels follow at once), the
+            // rest on the low-priority stream while those panels run
+            e = cudaStreamWaitEvent(hs, la->part_b, 0);
+            if (e != cudaSuccess) return e;
+            large_block_swap_kernel<<<std::min(148, (n - bend + 7) / 8), 256, 0, hs>>>(
                 A, lda, m, K0, (kend - K0 + PW - 1) / PW, bend, n, st);
             if (kend < m && kend - K0 == OB)
             {
                 large_trsm_kernel<OB><<<(n - bend + 63) / 64, 256, (OB * (OB + 4) + 64 * (OB + 4)) * sizeof(float),
-                                        stream>>>(A, lda, K0, bend, n - bend, st);
-                if (mode != 0 && umma_scratch)
+                                        hs>>>(A, lda, K0, bend, n - bend, st);
+                const int split = std::min(n, bend + OB);
+                if (tcgen)
                 {
-                    e = launch_umma_update(A, lda, m, n, K0, kend, bend, mode == 1 ? 1 : 3, st, umma_scratch, stream);
-                    if (e != cudaSuccess) return e;
+                    e = launch_umma_split(A, lda, m, n, K0, kend, bend, st, umma_scratch, hs);
+                    if (e == cudaSuccess)
+                        e = launch_umma_range(A, lda, m, n, kend, bend, bend, split, mode == 1 ? 1 : 3, st,
+                                              umma_scratch, hs);
                 }
                 else
-                    gemm_launch(mode, A, lda, kend, m - kend, bend, n - bend, K0, OB, st, stream);
+                    gemm_launch(mode, A, lda, kend, m - kend, bend, split - bend, K0, OB, st, hs);
+                if (e == cudaSuccess) e = cudaEventRecord(la->part_a, hs);
+                if (e == cudaSuccess && split < n)
+                {
+                    e = cudaStreamWaitEvent(ls, la->part_a, 0);
+                    if (e == cudaSuccess)
+                    {
+                        if (tcgen)
+                            e = launch_umma_range(A, lda, m, n, kend, bend, split, n, mode == 1 ? 1 : 3, st,
+                                                  umma_scratch, ls);
+                        else
+                            gemm_launch(mode, A, lda, kend, m - kend, split, n - split, K0, OB, st, ls);
+                    }
+                    if (e == cudaSuccess) e = cudaEventRecord(la->part_b, ls);
+                }
+                if (e != cudaSuccess) return e;
             }
         }
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
+    e = cudaStreamWaitEvent(hs, la->part_b, 0);
+    if (e != cudaSuccess) return e;
     // every panel's L columns take the later panels' interchanges
     const int npanels = (kmin + PW - 1) / PW;
-    if (npanels > 1) large_left_swap_kernel<<<npanels - 1, 256, 0, stream>>>(A, lda, m, npanels, st);
-    large_info_kernel<<<1, 1, 0, stream>>>(info, st);
+    if (npanels > 1) large_left_swap_kernel<<<npanels - 1, 256, 0, hs>>>(A, lda, m, npanels, st);
+    large_info_kernel<<<1, 1, 0, hs>>>(info, st);
+    // join both streams back into the caller's
+    e = cudaEventRecord(la->join_hi, hs);
+    if (e == cudaSuccess) e = cudaEventRecord(la->join_lo, ls);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, la->join_hi, 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, la->join_lo, 0);
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 

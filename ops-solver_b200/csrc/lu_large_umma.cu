@@ -233,8 +233,35 @@ __global__ void __launch_bounds__(UT, 1) umma_update_kernel(float *A, int lda, i
 
 size_t umma_scratch_bytes(int m, int n) { return ((size_t)m + n) * UK * 2 * sizeof(__nv_bfloat16) + 256; }
 
-cudaError_t launch_umma_update(float *A, int lda, int m, int n, int K0, int kend, int bend, int terms,
-                               LargeStatus *st, void *scratch, cudaStream_t stream)
+namespace
+{
+struct UmmaHalves
+{
+    __nv_bfloat16 *Lh, *Ll, *Uh, *Ul;
+};
+UmmaHalves halves(void *scratch, int m, int n)
+{
+    UmmaHalves h;
+    h.Lh = static_cast<__nv_bfloat16 *>(scratch);
+    h.Ll = h.Lh + (size_t)m * UK;
+    h.Uh = h.Ll + (size_t)m * UK;
+    h.Ul = h.Uh + (size_t)n * UK;
+    return h;
+}
+}  // namespace
+
+cudaError_t launch_umma_split(float *A, int lda, int m, int n, int K0, int kend, int bend, LargeStatus *st,
+                              void *scratch, cudaStream_t stream)
+{
+    const int rows = m - kend, cols = n - bend;
+    const UmmaHalves h = halves(scratch, m, n);
+    umma_split_l<<<(rows + 31) / 32, 256, 0, stream>>>(A, lda, kend, rows, K0, st, h.Lh, h.Ll);
+    umma_split_u<<<(unsigned)(((int64_t)cols * UK + 255) / 256), 256, 0, stream>>>(A, lda, K0, bend, cols, h.Uh, h.Ul);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_umma_range(float *A, int lda, int m, int n, int kend, int bend, int c_begin, int c_end, int terms,
+                              LargeStatus *st, void *scratch, cudaStream_t stream)
 {
     static bool attr = false;
     if (!attr)
@@ -244,16 +271,22 @@ cudaError_t launch_umma_update(float *A, int lda, int m, int n, int K0, int kend
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    const int rows = m - kend, cols = n - bend;
-    __nv_bfloat16 *Lh = static_cast<__nv_bfloat16 *>(scratch);
-    __nv_bfloat16 *Ll = Lh + (size_t)m * UK;
-    __nv_bfloat16 *Uh = Ll + (size_t)m * UK;
-    __nv_bfloat16 *Ul = Uh + (size_t)n * UK;
-    umma_split_l<<<(rows + 31) / 32, 256, 0, stream>>>(A, lda, kend, rows, K0, st, Lh, Ll);
-    umma_split_u<<<(unsigned)(((int64_t)cols * UK + 255) / 256), 256, 0, stream>>>(A, lda, K0, bend, cols, Uh, Ul);
+    const int rows = m - kend, cols = c_end - c_begin;
+    if (rows <= 0 || cols <= 0) return cudaSuccess;
+    const UmmaHalves h = halves(scratch, m, n);
+    const size_t off = (size_t)(c_begin - bend) * UK;  // the range's first column among the split ones
     dim3 g((rows + UM - 1) / UM, (cols + UN - 1) / UN);
-    umma_update_kernel<<<g, UT, UMMA_SMEM, stream>>>(A, lda, kend, rows, bend, cols, Lh, Ll, Uh, Ul, terms, st);
+    umma_update_kernel<<<g, UT, UMMA_SMEM, stream>>>(A, lda, kend, rows, c_begin, cols, h.Lh, h.Ll, h.Uh + off,
+                                                     h.Ul + off, terms, st);
     return cudaGetLastError();
+}
+
+cudaError_t launch_umma_update(float *A, int lda, int m, int n, int K0, int kend, int bend, int terms,
+                               LargeStatus *st, void *scratch, cudaStream_t stream)
+{
+    cudaError_t e = launch_umma_split(A, lda, m, n, K0, kend, bend, st, scratch, stream);
+    if (e != cudaSuccess) return e;
+    return launch_umma_range(A, lda, m, n, kend, bend, bend, n, terms, st, scratch, stream);
 }
 
 }  // namespace ops_solver
