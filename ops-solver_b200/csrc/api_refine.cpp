@@ -36,16 +36,17 @@ aclsolverStatus_t gesv_ir_large(Handle *h, int mode, int n, int nrhs, const floa
                                 double tol, int *iterArray, double *berrArray, int *infoArray)
 {
     cudaStream_t st = h->stream;
-    const size_t sizes[8] = {(size_t)n * n * sizeof(float), (size_t)n * sizeof(int), sizeof(LargeStatus),
+    const size_t sizes[9] = {(size_t)n * n * sizeof(float), (size_t)n * sizeof(int), sizeof(LargeStatus),
                              large_solve_scratch_bytes(n, nrhs), 256, large_ir_bytes(n, nrhs),
-                             mode != 0 ? umma_scratch_bytes(n, n) : 0, (size_t)n * sizeof(int)};
+                             mode != 0 ? umma_scratch_bytes(n, n) : 0, (size_t)n * sizeof(int),
+                             large_diag_inverse_bytes(n)};
     size_t total = 0;
     for (size_t v : sizes) total += round_up(v);
     ScratchBlock *blk = acquire_scratch(h, total);
     if (!blk) return ACLSOLVER_STATUS_ALLOC_FAILED;
     char *p = static_cast<char *>(blk->ptr);
-    void *part[8];
-    for (int i = 0; i < 8; ++i)
+    void *part[9];
+    for (int i = 0; i < 9; ++i)
     {
         part[i] = p;
         p += round_up(sizes[i]);
@@ -65,13 +66,15 @@ aclsolverStatus_t gesv_ir_large(Handle *h, int mode, int n, int nrhs, const floa
     if (e == cudaSuccess) e = cudaMemcpyAsync(&hinfo, infoArray, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     int *perm = static_cast<int *>(part[7]);  // the pivots composed once for every solve
+    float *dinv = static_cast<float *>(part[8]);  // the factors' diagonal blocks, inverted once
     auto solve = [&]() {
         return launch_getrs_large(lu, nullptr, n, n, nullptr, s.r32, nullptr, n, nrhs, solve_scratch, flags, nullptr, st,
-                                  perm);
+                                  perm, dinv);
     };
     if (e == cudaSuccess && hinfo == 0)
     {
         e = launch_large_perm(ipiv, n, perm, flags, st);
+        if (e == cudaSuccess) e = launch_large_diag_inverses(lu, n, n, dinv, st);
         if (e == cudaSuccess) e = launch_lir_init(s, Barray, ldb, n, nrhs, st);
         if (e == cudaSuccess) e = solve();
         if (e == cudaSuccess) e = launch_lir_update(s, n, nrhs, 1, st);

@@ -105,7 +105,11 @@ constexpr int LARGE_SOLVE_MAX_RHS = 16;
 size_t large_solve_scratch_bytes(int n, int nrhs);
 cudaError_t launch_getrs_large(const float *A1, const float *const *At, int lda, int n, const int *ipiv, float *X1,
                                float *const *Xt, int ldx, int nrhs, void *scratch, int *bad, int *info,
-                               cudaStream_t stream, const int *perm_in = nullptr);
+                               cudaStream_t stream, const int *perm_in = nullptr, const float *dinv = nullptr);
+// dinv (refinement solves only: not the oracle's order): the inverses of the factors' 128 x 128
+// diagonal blocks (large_diag_inverse_bytes(n) of device memory), applied as products.
+size_t large_diag_inverse_bytes(int n);
+cudaError_t launch_large_diag_inverses(const float *A, int lda, int n, float *inv, cudaStream_t stream);
 // perm[i] = the row that ipiv's swaps bring to position i (n ints), for repeated solves
 // (perm_in above); *bad as above.
 cudaError_t launch_large_perm(const int *ipiv, int n, int *perm, int *bad, cudaStream_t stream);

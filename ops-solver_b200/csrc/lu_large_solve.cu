@@ -212,6 +212,51 @@ __global__ void __launch_bounds__(ST) large_sweep_kernel(const float *A1, const 
 }
 
 
+// Inverses of the 128 x 128 diagonal blocks of the factors, for the refinement's solves (whose
+// results need not follow the oracle's order): block (b, which) inverts the unit-lower L
+// block (which 0) or the upper U block (which 1) of diagonal block b, thread j computing
+// column j by substitution against e_j in shared memory.  Stored column-major per (b, which);
+// a ragged last block of order w is inverted as w x w (the rest of the 128 x 128 identity).
+__global__ void __launch_bounds__(SB, 1) large_diag_inverse(const float *A, int lda, int n, float *inv)
+{
+    extern __shared__ __align__(16) float dsm[];
+    float *T = dsm;              // T[k][i] = A(b0 + i, b0 + k), pitch SBP4
+    float *Y = dsm + SB * SBP4;  // Y[j][i]: column j of the inverse, pitch SBP4
+    const int b = blockIdx.x, which = blockIdx.y, j = threadIdx.x;
+    const int b0 = b * SB, w = min(SB, n - b0);
+    const bool vec = (reinterpret_cast<uintptr_t>(A) & 15u) == 0 && (lda & 3) == 0 && w == SB;
+    stage_tile(T, SBP4, A + (int64_t)b0 * lda + b0, lda, w, w, vec);
+    tile_wait();
+    __syncthreads();
+    float *y = Y + j * SBP4;
+    for (int i = 0; i < SB; ++i) y[i] = 0.0f;
+    if (j >= w)
+        y[j] = 1.0f;
+    else if (which == 0)
+    {
+        y[j] = 1.0f;
+        for (int i = j + 1; i < w; ++i)
+        {
+            float acc = 0.0f;
+            for (int k = j; k < i; ++k) acc = fma_rn(-T[k * SBP4 + i], y[k], acc);
+            y[i] = acc;
+        }
+    }
+    else
+    {
+        y[j] = 1.0f / T[j * SBP4 + j];
+        for (int i = j - 1; i >= 0; --i)
+        {
+            float acc = 0.0f;
+            for (int k = i + 1; k <= j; ++k) acc = fma_rn(-T[k * SBP4 + i], y[k], acc);
+            y[i] = acc / T[i * SBP4 + i];
+        }
+    }
+    __syncthreads();
+    float *dst = inv + ((size_t)b * 2 + which) * SB * SB;
+    for (int e = threadIdx.x; e < SB * SB; e += SB) dst[e] = Y[(e / SB) * SBP4 + e % SB];
+}
+
 // The same sweep as one cooperative launch: block s owns 128-row strip s for the whole sweep.
 // It applies the finished blocks b in order (forward: b < s ascending; backward: b > s
 // descending), each as soon as block b has published its solution (flag[b] == epoch), with
@@ -224,7 +269,8 @@ constexpr long long FLAG_WAIT = 1ll << 22;
 
 template <bool FORWARD>
 __global__ void __launch_bounds__(ST, 1) large_sweep_coop(const float *A1, const float *const *At, int lda, int n,
-                                                           float *Y, int nrhs, int *flags, int epoch, int *bad)
+                                                           float *Y, int nrhs, int *flags, int epoch, int *bad,
+                                                           const float *dinv)
 {
     extern __shared__ __align__(16) float sm[];
     float *D = sm;                            // this strip's diagonal block, pitch SBP4
@@ -240,7 +286,10 @@ __global__ void __launch_bounds__(ST, 1) large_sweep_coop(const float *A1, const
     const int s = FORWARD ? sidx : nb - 1 - sidx;  // the strip; forward strips start at the top
     const int s0 = s * SB, sw = min(SB, n - s0);
     const bool vec = (reinterpret_cast<uintptr_t>(A) & 15u) == 0 && (lda & 3) == 0;
-    stage_tile(D, SBP4, A + (int64_t)s0 * lda + s0, lda, sw, sw, vec && sw == SB);
+    if (dinv)  // the diagonal block's inverse (128 x 128, column-major, 16-byte aligned)
+        stage_tile(D, SBP4, dinv + ((size_t)s * 2 + (FORWARD ? 0 : 1)) * SB * SB, SB, SB, SB, true);
+    else
+        stage_tile(D, SBP4, A + (int64_t)s0 * lda + s0, lda, sw, sw, vec && sw == SB);
     stage_tile(xs, SB, Y + s0, n, sw, nrhs, (n & 3) == 0 && sw == SB);
     if (t == 0) stop = 0;
     const int nprev = FORWARD ? s : nb - 1 - s;  // blocks applied before this strip's own
@@ -309,6 +358,26 @@ __global__ void __launch_bounds__(ST, 1) large_sweep_coop(const float *A1, const
             __syncthreads();
         }
     }
+    if (dinv)
+    {
+        // x = inv xs, a thread per (row, right-hand sides r0, r0 + 2, ...), into xb
+        if (i < sw)
+        {
+#pragma unroll
+            for (int u = 0; u < RPT; ++u)
+            {
+                const int r = r0 + u * (ST / SB);
+                if (r >= nrhs) continue;
+                float acc = 0.0f;
+                for (int k = 0; k < sw; ++k) acc = fma_rn(D[k * SBP4 + i], xs[r * SB + k], acc);
+                xb[r * SB + i] = acc;
+            }
+        }
+        __syncthreads();
+        for (int e = t; e < nrhs * SB; e += ST) xs[e] = xb[e];
+        __syncthreads();
+    }
+    else
     // the diagonal block: as in the per-block sweep
     {
         const int nsub = (sw + 31) / 32;
@@ -402,9 +471,25 @@ cudaError_t launch_large_perm(const int *ipiv, int n, int *perm, int *bad, cudaS
     return cudaGetLastError();
 }
 
+cudaError_t launch_large_diag_inverses(const float *A, int lda, int n, float *inv, cudaStream_t stream)
+{
+    static bool attr = false;
+    const size_t smem = 2 * (size_t)SB * SBP4 * sizeof(float);
+    if (!attr)
+    {
+        cudaError_t e = cudaFuncSetAttribute(large_diag_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    large_diag_inverse<<<dim3((n + SB - 1) / SB, 2), SB, smem, stream>>>(A, lda, n, inv);
+    return cudaGetLastError();
+}
+
+size_t large_diag_inverse_bytes(int n) { return (size_t)((n + SB - 1) / SB) * 2 * SB * SB * sizeof(float); }
+
 cudaError_t launch_getrs_large(const float *A, const float *const *At, int lda, int n, const int *ipiv, float *X,
                                float *const *Xt, int ldx, int nrhs, void *scratch, int *bad, int *info,
-                               cudaStream_t stream, const int *perm_in)
+                               cudaStream_t stream, const int *perm_in, const float *dinv)
 {
     if (n > LARGE_MAX_COLS || nrhs > LARGE_SOLVE_MAX_RHS) return cudaErrorInvalidValue;
     float *Y = static_cast<float *>(scratch);
@@ -465,16 +550,28 @@ cudaError_t launch_getrs_large(const float *A, const float *const *At, int lda, 
         const float *const *at = At;
         float *y = Y;
         int nn = n, nr = nrhs, ld = lda, epv = ep;
-        int *fl = flags;
+        int *fl = flags, *fb = flags + nb;
+        const float *dv = dinv;
         void *fwd[] = {(void *)&a1, (void *)&at, (void *)&ld, (void *)&nn, (void *)&y, (void *)&nr, (void *)&fl,
-                       (void *)&epv, (void *)&bad};
+                       (void *)&epv, (void *)&bad, (void *)&dv};
         cudaError_t e = cudaLaunchCooperativeKernel((const void *)large_sweep_coop<true>, dim3(nb), dim3(ST), fwd,
                                                     csmem, stream);
         if (e != cudaSuccess) return e;
-        // the backward sweep stays one launch per block: its chain of IEEE divisions makes the
-        // cooperative form slower there (2.7 vs 2.1 ms at 8192 measured), the forward one faster
-        for (int b = nb - 1; b >= 0; --b)
-            large_sweep_kernel<false><<<b + 1, ST, smem, stream>>>(A, At, lda, n, Y, nrhs, b, bad);
+        if (dinv)
+        {
+            void *bwd[] = {(void *)&a1, (void *)&at, (void *)&ld, (void *)&nn, (void *)&y, (void *)&nr, (void *)&fb,
+                           (void *)&epv, (void *)&bad, (void *)&dv};
+            e = cudaLaunchCooperativeKernel((const void *)large_sweep_coop<false>, dim3(nb), dim3(ST), bwd, csmem,
+                                            stream);
+            if (e != cudaSuccess) return e;
+        }
+        else
+        {
+            // in the oracle's order the backward sweep stays one launch per block: its chain of
+            // IEEE divisions makes the cooperative form slower there (2.7 vs 2.1 ms at 8192)
+            for (int b = nb - 1; b >= 0; --b)
+                large_sweep_kernel<false><<<b + 1, ST, smem, stream>>>(A, At, lda, n, Y, nrhs, b, bad);
+        }
     }
     else
     {
