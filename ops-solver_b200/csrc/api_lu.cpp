@@ -402,8 +402,19 @@ extern "C"
             st = check_finite(h, a, n, infoArray, batchSize, 2);
             if (st != ACLSOLVER_STATUS_SUCCESS) return st;
         }
-        if (n > SMALL_N) return ACLSOLVER_STATUS_NOT_SUPPORTED;
         RealBatch c{nullptr, Carray, n, ldc, 0, batchSize};
+        if (n > SMALL_N)
+        {
+            // above the register-resident orders: the blocked solve against the identity
+            // (within tolerance of the reference's inverse order, not bit for bit)
+            if (n > BLOCKED_SOLVE_MAX_N) return ACLSOLVER_STATUS_NOT_SUPPORTED;
+            ScratchBlock *blk = acquire_scratch(h, getri_blocked_scratch_bytes(n, batchSize));
+            if (!blk) return ACLSOLVER_STATUS_ALLOC_FAILED;
+            aclsolverStatus_t launched = launch_status(launch_getri_blocked(
+                a, layout.identity ? nullptr : PivotArray, c, infoArray, blk->ptr, h->stream));
+            aclsolverStatus_t fin = finish_scratch(h, blk);
+            return launched != ACLSOLVER_STATUS_SUCCESS ? launched : fin;
+        }
         return launch_status(
             launch_getri_small(a, layout.identity ? nullptr : PivotArray, c, infoArray, h->stream));
     }
@@ -462,7 +473,27 @@ extern "C"
         if (n <= SMALL_N) return launch_status(launch_getrf_small(a, n, PivotArray, infoArray, h->stream));
         if (n <= BLOCKED_MAX_N)
             return launch_status(launch_getrf_blocked(a, PivotArray, infoArray, 0, h->stream));
-        return ACLSOLVER_STATUS_NOT_SUPPORTED;
+        // above the batched orders: one matrix at a time over the whole GPU; the pointer table
+        // is read back first (this call synchronises once)
+        std::vector<float *> ptrs((size_t)batchSize);
+        cudaError_t e = cudaMemcpyAsync(ptrs.data(), Aarray, sizeof(float *) * (size_t)batchSize,
+                                        cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) return launch_status(e);
+        ScratchBlock *blk = acquire_scratch(h, sizeof(LargeStatus) + 256);
+        if (!blk) return ACLSOLVER_STATUS_ALLOC_FAILED;
+        LargeStatus *status = static_cast<LargeStatus *>(blk->ptr);
+        for (int q = 0; q < batchSize && e == cudaSuccess; ++q)
+        {
+            if (!ptrs[q])
+                e = launch_fill_info(infoArray + q, -2, 1, h->stream);
+            else
+                e = launch_getrf_large(ptrs[q], n, n, lda, PivotArray ? PivotArray + (size_t)q * n : nullptr,
+                                       infoArray + q, status, 0, h->stream);
+        }
+        aclsolverStatus_t launched = launch_status(e);
+        aclsolverStatus_t fin = finish_scratch(h, blk);
+        return launched != ACLSOLVER_STATUS_SUCCESS ? launched : fin;
     }
 
     aclsolverStatus_t aclsolverSgetrsBatched(aclsolverHandle_t handle, aclsolverOperation_t trans, int n, int nrhs,

@@ -57,6 +57,7 @@ cudaError_t launch_getri_small(const RealBatch &a, const int *ipiv, const RealBa
 // src (optional): factor a copy of src[q] (leading dimension src_ld) into a's slot q.
 // perm (optional): n per matrix, the composed row permutation (P b = b[perm]).
 constexpr int BLOCKED_MAX_N = 512;
+constexpr int BLOCKED_SOLVE_MAX_N = 8192;  // the blocked solve: x of one right-hand side in shared memory
 cudaError_t launch_getrf_blocked(const RealBatch &a, int *ipiv, int *info, int mode, cudaStream_t stream,
                                  const float *const *src = nullptr, int src_ld = 0, int *perm = nullptr);
 // Blocked LU solve (trans 0) for 64 < n <= 8192.  Row interchanges from ipiv (LAPACK form,
@@ -142,6 +143,12 @@ cudaError_t launch_lir_finish(const LargeIr &s, float *const *X, int ldx, int n,
 // dinv (optional, refinement solves): the diagonal blocks' inverses from
 // launch_diag_inverses; the 32 x 32 triangles are then applied as products (not in the
 // oracle's order: used where the result is refined, not where it must match bit for bit).
+// Inverses above the small orders (tables only): C = A^-1 from LU factors and pivots as the
+// blocked solve against the identity; info as the small inverse reports it; scratch:
+// getri_blocked_scratch_bytes(n, count).
+cudaError_t launch_getri_blocked(const RealBatch &a, const int *ipiv, const RealBatch &c, int *info, void *scratch,
+                                 cudaStream_t stream);
+size_t getri_blocked_scratch_bytes(int n, int count);
 cudaError_t launch_getrs_blocked(const RealBatch &a, const int *ipiv, const int *perm, const RealBatch &b, int nrhs,
                                  int *info, const int *skip, cudaStream_t stream, const float *dinv = nullptr);
 // dinv[(q * nblk + b) * 2 + {0: L, 1: U}] = inverse of the 32 x 32 diagonal block b of the

@@ -113,3 +113,73 @@ cudaError_t launch_transpose(const float *src, int lds, float *dst, int ldd, int
 }
 
 }  // namespace ops_solver
+
+namespace ops_solver
+{
+namespace
+{
+// Per matrix: info for the inverse above the small orders, in the small path's convention
+// (-2 a null A or C slot, -4 a pivot outside [k+1, n], else the first zero diagonal of U,
+// 1-based, else 0); C set to the identity where the inverse is computed; fail[q] = info != 0.
+__global__ void getri_prepare_kernel(float *const *a_table, const int *ipiv, float *const *c_table, int n, int lda,
+                                     int ldc, int count, int *info, int *fail)
+{
+    __shared__ int bad, zero;
+    const int64_t q = blockIdx.x;
+    if (q >= count) return;
+    const float *A = slot(a_table, q);
+    float *C = slot(c_table, q);
+    if (threadIdx.x == 0)
+    {
+        bad = 0;
+        zero = 0x7fffffff;
+    }
+    __syncthreads();
+    if (A && C)
+        for (int k = threadIdx.x; k < n; k += blockDim.x)
+        {
+            if (ipiv && (ipiv[q * n + k] < k + 1 || ipiv[q * n + k] > n)) bad = 1;
+            if (A[(int64_t)k * lda + k] == 0.0f) atomicMin(&zero, k + 1);
+        }
+    __syncthreads();
+    const int v = !(A && C) ? -2 : bad ? -4 : (zero == 0x7fffffff ? 0 : zero);
+    if (threadIdx.x == 0)
+    {
+        info[q] = v;
+        fail[q] = v != 0;
+    }
+    if (v != 0) return;  // uniform
+    for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += blockDim.x)
+    {
+        const int i = (int)(e % n), j = (int)(e / n);
+        C[(int64_t)j * ldc + i] = i == j ? 1.0f : 0.0f;
+    }
+}
+
+// skip[q * n + r] = fail[q]: the solve's per right-hand side switch
+__global__ void getri_skip_kernel(const int *fail, int n, int count, int *skip)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)count * n) return;
+    skip[e] = fail[e / n];
+}
+}  // namespace
+
+cudaError_t launch_getri_blocked(const RealBatch &a, const int *ipiv, const RealBatch &c, int *info, void *scratch,
+                                 cudaStream_t stream)
+{
+    const int n = a.n, count = a.count;
+    int *fail = static_cast<int *>(scratch);
+    int *skip = fail + count;
+    getri_prepare_kernel<<<count, 256, 0, stream>>>(a.table, ipiv, c.table, n, a.ld, c.ld, count, info, fail);
+    const int64_t total = (int64_t)count * n;
+    getri_skip_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(fail, n, count, skip);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    // C = A^-1 as the solve of A X = I, the identity already in C
+    return launch_getrs_blocked(a, ipiv, nullptr, c, n, nullptr, skip, stream);
+}
+
+size_t getri_blocked_scratch_bytes(int n, int count) { return ((size_t)count * (n + 1)) * sizeof(int) + 256; }
+
+}  // namespace ops_solver
