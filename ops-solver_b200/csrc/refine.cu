@@ -117,21 +117,7 @@ __global__ void __launch_bounds__(RT) ir_residual_kernel(const IrState s, const 
             if (ib < n)
             {
                 const float *base = A + ib;
-                const bool full = vec && ib + 3 < n;
-#pragma unroll 4
-                for (int j = jb; j < je; ++j)
-                {
-                    float v[4];
-                    if (full)
-                    {
-                        const float4 f = __ldg(reinterpret_cast<const float4 *>(base + (int64_t)j * lda));
-                        v[0] = f.x, v[1] = f.y, v[2] = f.z, v[3] = f.w;
-                    }
-                    else
-                    {
-#pragma unroll
-                        for (int e = 0; e < 4; ++e) v[e] = ib + e < n ? base[(int64_t)j * lda + e] : 0.0f;
-                    }
+                auto column = [&](int j, const float (&v)[4]) {
 #pragma unroll
                     for (int e = 0; e < 4; ++e) arow[e] += fabs((double)v[e]);
 #pragma unroll
@@ -143,6 +129,40 @@ __global__ void __launch_bounds__(RT) ir_residual_kernel(const IrState s, const 
 #pragma unroll
                             for (int e = 0; e < 4; ++e) acc[r][e] = fma((double)v[e], xj, acc[r][e]);
                         }
+                    }
+                };
+                if (vec && ib + 3 < n)
+                {
+                    // 16-byte loads, eight columns in flight before their products (same order)
+                    int j = jb;
+                    for (; j + 8 <= je; j += 8)
+                    {
+                        float4 f[8];
+#pragma unroll
+                        for (int u = 0; u < 8; ++u)
+                            f[u] = __ldg(reinterpret_cast<const float4 *>(base + (int64_t)(j + u) * lda));
+#pragma unroll
+                        for (int u = 0; u < 8; ++u)
+                        {
+                            const float v[4] = {f[u].x, f[u].y, f[u].z, f[u].w};
+                            column(j + u, v);
+                        }
+                    }
+                    for (; j < je; ++j)
+                    {
+                        const float4 f = __ldg(reinterpret_cast<const float4 *>(base + (int64_t)j * lda));
+                        const float v[4] = {f.x, f.y, f.z, f.w};
+                        column(j, v);
+                    }
+                }
+                else
+                {
+                    for (int j = jb; j < je; ++j)
+                    {
+                        float v[4];
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) v[e] = ib + e < n ? base[(int64_t)j * lda + e] : 0.0f;
+                        column(j, v);
                     }
                 }
             }
