@@ -166,14 +166,14 @@ extern "C" aclsolverStatus_t aclsolverSgesvIrBatched(aclsolverHandle_t handle, a
                              berrArray, infoArray);
     }
 
-    // Workspace: LU copies, pivots and their permutation, two pointer tables, FP64 solutions, FP32 staging,
+    // Workspace: LU copies, pivots and the panels' row changes, two pointer tables, FP64 solutions, FP32 staging,
     // per-job berr and state, per-matrix iterations.
     const size_t jobs = (size_t)batchSize * nrhs;
     const size_t vec = (size_t)n * jobs;
     const int nblk = (n + 31) / 32;
     const size_t sizes[10] = {(size_t)n * n * batchSize * sizeof(float),
                              (size_t)n * batchSize * sizeof(int),
-                             (size_t)n * batchSize * sizeof(int),
+                             (size_t)batchSize * BLOCKED_PANELS * PANEL_LIST_SHORTS * sizeof(short),
                              (size_t)batchSize * sizeof(float *),
                              (size_t)batchSize * sizeof(float *),
                              vec * sizeof(double),
@@ -194,7 +194,7 @@ extern "C" aclsolverStatus_t aclsolverSgesvIrBatched(aclsolverHandle_t handle, a
     }
     float *lu = static_cast<float *>(part[0]);
     int *ipiv = static_cast<int *>(part[1]);
-    int *perm = static_cast<int *>(part[2]);
+    short *lists = static_cast<short *>(part[2]);  // the panels' row changes
     float **lu_table = static_cast<float **>(part[3]);
     float **r_table = static_cast<float **>(part[4]);
     IrState s;
@@ -211,7 +211,8 @@ extern "C" aclsolverStatus_t aclsolverSgesvIrBatched(aclsolverHandle_t handle, a
     auto solve = [&](const int *skip)
     {
         return n <= SMALL_N ? launch_getrs_small(fac, ipiv, rhs, nrhs, 0, nullptr, st)
-                            : launch_getrs_blocked(fac, nullptr, perm, rhs, nrhs, nullptr, skip, st, dinv);
+                            : launch_getrs_blocked(fac, nullptr, nullptr, rhs, nrhs, nullptr, skip, st, dinv,
+                                                   lists);
     };
     cudaError_t e = launch_strided_table(lu_table, lu, (int64_t)n * n, batchSize, st);
     if (e == cudaSuccess) e = launch_strided_table(r_table, s.r32, (int64_t)n * nrhs, batchSize, st);
@@ -224,9 +225,9 @@ extern "C" aclsolverStatus_t aclsolverSgesvIrBatched(aclsolverHandle_t handle, a
         }
         else
         {
-            // the factorisation copies A into the workspace itself and reports the composed
-            // row permutation used by the solves
-            e = launch_getrf_blocked(fac, ipiv, infoArray, mode, st, src.table, lda, perm);
+            // the factorisation copies A into the workspace itself; its L columns keep their
+            // block's row order and the solves apply the panels' row changes as they go
+            e = launch_getrf_blocked(fac, ipiv, infoArray, mode, st, src.table, lda, nullptr, lists);
             if (e == cudaSuccess) e = launch_diag_inverses(fac, dinv, st);
         }
     }

@@ -56,15 +56,27 @@ cudaError_t launch_getri_small(const RealBatch &a, const int *ipiv, const RealBa
 // BF16 (three products).  ipiv n per matrix or nullptr; info as launch_getrf_small.
 // src (optional): factor a copy of src[q] (leading dimension src_ld) into a's slot q.
 // perm (optional): n per matrix, the composed row permutation (P b = b[perm]).
+// lists (optional, for the blocked solve's `lists`): the factorisation's row changes panel by
+// panel, and the L columns of each 128-column block keep the row order they had when the
+// block was finished (the interchanges of later blocks are not applied to them, so ipiv and
+// the factors are not in LAPACK form).  Per matrix BLOCKED_PANELS entries of
+// PANEL_LIST_SHORTS shorts: [count, position[64], source[64], pad]; panel p moves the row at
+// 32p + source[i] to 32p + position[i] (all moves of the entry at once).
 constexpr int BLOCKED_MAX_N = 512;
 constexpr int BLOCKED_SOLVE_MAX_N = 8192;  // the blocked solve: x of one right-hand side in shared memory
+constexpr int BLOCKED_PANELS = BLOCKED_MAX_N / 32;
+constexpr int BLOCKED_OUTER_COLS = 128;  // columns of the blocks whose L keeps its row order
+constexpr int PANEL_LIST_SHORTS = 132;
 cudaError_t launch_getrf_blocked(const RealBatch &a, int *ipiv, int *info, int mode, cudaStream_t stream,
-                                 const float *const *src = nullptr, int src_ld = 0, int *perm = nullptr);
+                                 const float *const *src = nullptr, int src_ld = 0, int *perm = nullptr,
+                                 short *lists = nullptr);
 // Blocked LU solve (trans 0) for 64 < n <= 8192.  Row interchanges from ipiv (LAPACK form,
 // applied in order) or, when perm is given, from the permutation perm (P b = b[perm], see
 // launch_permutation); both may be null.  `skip` (nullptr = none): per (matrix,
 // right-hand side) states; a group of right-hand sides whose states are all nonzero is
-// skipped (iterative refinement).  info may be null.
+// skipped (iterative refinement).  info may be null.  lists (with ipiv and perm null):
+// factors from launch_getrf_blocked with `lists`; the forward sweep applies each 128-column
+// block's row changes to the vectors before that block's columns.
 // ---- large single-matrix LU (lu_large.cu) ---------------------------------------------
 constexpr int LARGE_MAX_ROWS = 8192;  // up to four panel rows per thread of an 8 x 256-thread cluster
 constexpr int LARGE_MAX_COLS = 8192;
@@ -150,7 +162,8 @@ cudaError_t launch_getri_blocked(const RealBatch &a, const int *ipiv, const Real
                                  cudaStream_t stream);
 size_t getri_blocked_scratch_bytes(int n, int count);
 cudaError_t launch_getrs_blocked(const RealBatch &a, const int *ipiv, const int *perm, const RealBatch &b, int nrhs,
-                                 int *info, const int *skip, cudaStream_t stream, const float *dinv = nullptr);
+                                 int *info, const int *skip, cudaStream_t stream, const float *dinv = nullptr,
+                                 const short *lists = nullptr);
 // dinv[(q * nblk + b) * 2 + {0: L, 1: U}] = inverse of the 32 x 32 diagonal block b of the
 // factors of matrix q (column-major 32 x 32, nblk = ceil(n / 32)).
 cudaError_t launch_diag_inverses(const RealBatch &a, float *dinv, cudaStream_t stream);

@@ -63,6 +63,8 @@ constexpr int LOP = W2 + 4;   // outer L11 Lo[k][i] pitch (floats)
 constexpr int BSWAP = 4;      // columns in flight per warp in the outer row interchanges
 constexpr unsigned FULL = 0xffffffffu;
 static_assert(MAXN == 512, "the mixed panel's packed pivot key holds a 9-bit position");
+static_assert(NPANEL == BLOCKED_PANELS && PANEL_LIST_SHORTS >= 1 + 4 * NB && W2 == BLOCKED_OUTER_COLS,
+              "panel change lists");
 
 struct __align__(16) Shared
 {
@@ -1068,7 +1070,8 @@ __device__ void outer_update(float *A, int lda, int n, int K0, bool vec, Shared 
 template <int MODE>  // 0 plain FP32, 1 BF16, 3 split BF16 (three products)
 __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, float *const *table, int first, int n,
                                                                int lda, int *ipiv, int *info, int count,
-                                                               const float *const *src, int src_ld, int *perm_out)
+                                                               const float *const *src, int src_ld, int *perm_out,
+                                                               short *lists_out)
 {
     constexpr int TERMS = MODE == 1 ? 1 : 3;
     extern __shared__ __align__(16) unsigned char dyn[];
@@ -1361,6 +1364,24 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
         __syncthreads();
         }
         const int npanel_all = (n + NB - 1) / NB;
+        if (lists_out)
+        {
+            // the panels' row changes, for a solve over factors without the left interchanges
+            short *lq = lists_out + (size_t)q * BLOCKED_PANELS * PANEL_LIST_SHORTS;
+            for (int e = t; e < npanel_all * (2 * NB + 1); e += BT)
+            {
+                const int p = e / (2 * NB + 1), i = e % (2 * NB + 1);
+                const int cnt = piv ? sh.nchg[p] : 0;
+                short *entry = lq + (size_t)p * PANEL_LIST_SHORTS;
+                if (i == 2 * NB)
+                    entry[0] = (short)cnt;
+                else if (i < cnt)
+                {
+                    entry[1 + i] = sh.chg[p][i];
+                    entry[1 + 2 * NB + i] = sh.src[p][i];
+                }
+            }
+        }
         if (perm_out && piv)
         {
             // the composed permutation: position i of the factors holds original row P[i]
@@ -1446,7 +1467,7 @@ __global__ void __launch_bounds__(BT) left_swaps_kernel(float *single, float *co
 
 template <int MODE>
 cudaError_t launch_mode(const RealBatch &a, int *ipiv, int *info, const float *const *src, int src_ld, int *perm,
-                        cudaStream_t stream)
+                        short *lists, cudaStream_t stream)
 {
     const size_t smem = dyn_bytes(a.n, MODE);
     cudaError_t e = cudaFuncSetAttribute(getrf_blocked_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1455,9 +1476,9 @@ cudaError_t launch_mode(const RealBatch &a, int *ipiv, int *info, const float *c
     int64_t blocks = a.count < 148 * 2 ? a.count : 148 * 2;
     if (blocks < 1) blocks = 1;
     getrf_blocked_kernel<MODE><<<(unsigned)blocks, BT, smem, stream>>>(a.single, a.table, a.first, a.n, a.ld, ipiv,
-                                                                       info, a.count, src, src_ld, perm);
+                                                                       info, a.count, src, src_ld, perm, lists);
     const int npanel = (a.n + NB - 1) / NB;
-    if (ipiv && npanel > 1)
+    if (ipiv && !lists && npanel > 1)
     {
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -1469,17 +1490,17 @@ cudaError_t launch_mode(const RealBatch &a, int *ipiv, int *info, const float *c
 }  // namespace
 
 cudaError_t launch_getrf_blocked(const RealBatch &a, int *ipiv, int *info, int mode, cudaStream_t stream,
-                                 const float *const *src, int src_ld, int *perm)
+                                 const float *const *src, int src_ld, int *perm, short *lists)
 {
     if (a.n > MAXN || a.n < 1) return cudaErrorInvalidValue;
     switch (mode)
     {
         case 0:
-            return launch_mode<0>(a, ipiv, info, src, src_ld, perm, stream);
+            return launch_mode<0>(a, ipiv, info, src, src_ld, perm, lists, stream);
         case 1:
-            return launch_mode<1>(a, ipiv, info, src, src_ld, perm, stream);
+            return launch_mode<1>(a, ipiv, info, src, src_ld, perm, lists, stream);
         default:
-            return launch_mode<3>(a, ipiv, info, src, src_ld, perm, stream);
+            return launch_mode<3>(a, ipiv, info, src, src_ld, perm, lists, stream);
     }
 }
 

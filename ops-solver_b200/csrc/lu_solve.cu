@@ -23,6 +23,8 @@ namespace
 constexpr int ST = 256;  // threads per block
 constexpr int KB = 32;   // column block
 constexpr int MAX_RHS_PER_BLOCK = 8;
+constexpr int OUTER = BLOCKED_OUTER_COLS / KB;  // column blocks per block of a factorisation's change lists
+static_assert(2 * ST >= 2 * KB * MAX_RHS_PER_BLOCK, "a panel's moves for all right-hand sides, two per thread");
 
 constexpr int SR = 256;      // rows of a strip
 constexpr int SP = SR + 4;   // stage pitch (floats)
@@ -144,8 +146,46 @@ __device__ __forceinline__ void issue_task(const float *A, int lda, int n, Task 
     }
 }
 
+// Factors whose L columns keep their 128-column block's row order (launch_getrf_blocked with
+// `lists`): before the forward sweep reaches such a block's first column, the vectors take the
+// row changes of that block's (up to four) 32-column panels, in order, so that every L column meets the
+// vectors in the row order it was stored in.  Each panel's moves are read before any is
+// written.  Block-uniform control flow (the counts come from global memory).
+__device__ __forceinline__ void apply_block_changes(const short *lists, int blk, int n, float *x, int nr)
+{
+    const int t = threadIdx.x;
+    const int npanel = (n + KB - 1) / KB;
+    for (int p = blk; p < min(blk + OUTER, npanel); ++p)
+    {
+        const short *entry = lists + (size_t)p * PANEL_LIST_SHORTS;
+        const int cnt = entry[0];
+        if (cnt == 0) continue;
+        const int kp = p * KB;
+        float v[2];
+        int dst[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+        {
+            const int e = t + h * ST;
+            dst[h] = -1;
+            if (e < cnt * nr)
+            {
+                const int r = e / cnt, i = e % cnt;
+                dst[h] = r * n + kp + entry[1 + i];
+                v[h] = x[r * n + kp + entry[1 + 2 * KB + i]];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+            if (dst[h] >= 0) x[dst[h]] = v[h];
+        __syncthreads();
+    }
+}
+
 template <bool FORWARD>
-__device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *stages, bool vec, const float *dinv)
+__device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *stages, bool vec, const float *dinv,
+                      const short *lists)
 {
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int nblk = (n + KB - 1) / KB;
@@ -180,6 +220,7 @@ __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *s
         const Task cur = q[0];
         const int kb = cur.blk * KB;
         const int w = min(KB, n - kb);
+        if (FORWARD && lists && cur.strip < 0 && cur.blk % OUTER == 0) apply_block_changes(lists, cur.blk, n, x, nr);
         if (cur.strip < 0)
         {
             // diagonal triangle: warp r solves right-hand side r, lane i on row kb + i
@@ -273,7 +314,8 @@ __global__ void __launch_bounds__(ST, 2) getrs_blocked_kernel(float *a_single, f
                                                             const int *ipiv, const int *perm, float *b_single,
                                                             float *const *b_table, int b_first, int n, int lda,
                                                             int ldb, int nrhs, int count, int RHS, int *info,
-                                                            const int *skip, const float *dinv_all, int nblk)
+                                                            const int *skip, const float *dinv_all, int nblk,
+                                                            const short *lists_all)
 {
     extern __shared__ __align__(16) float dyn[];
     float *stages = dyn;                          // STAGES x KB x SP
@@ -337,8 +379,9 @@ __global__ void __launch_bounds__(ST, 2) getrs_blocked_kernel(float *a_single, f
         __syncthreads();
         const bool vec = (reinterpret_cast<uintptr_t>(A) & 15u) == 0 && (lda & 3) == 0;
         const float *dinv = dinv_all ? dinv_all + (size_t)q * nblk * 2 * KB * KB : nullptr;
-        sweep<true>(A, lda, n, x, nr, stages, vec, dinv);
-        sweep<false>(A, lda, n, x, nr, stages, vec, dinv);
+        const short *lists = lists_all ? lists_all + (size_t)q * BLOCKED_PANELS * PANEL_LIST_SHORTS : nullptr;
+        sweep<true>(A, lda, n, x, nr, stages, vec, dinv, lists);
+        sweep<false>(A, lda, n, x, nr, stages, vec, dinv, nullptr);
         for (int e = t; e < nr * n; e += ST)
         {
             const int r = e / n, i = e % n;
@@ -424,8 +467,10 @@ __global__ void permutation_kernel(const int *ipiv, int *perm, int n, int count)
 }  // namespace
 
 cudaError_t launch_getrs_blocked(const RealBatch &a, const int *ipiv, const int *perm, const RealBatch &b, int nrhs,
-                                 int *info, const int *skip, cudaStream_t stream, const float *dinv)
+                                 int *info, const int *skip, cudaStream_t stream, const float *dinv,
+                                 const short *lists)
 {
+    if (lists && (a.n > BLOCKED_MAX_N || ipiv || perm)) return cudaErrorInvalidValue;
     const size_t stage_floats = (size_t)STAGES * KB * SP;
     // two blocks per SM when the vectors fit beside the ring, else one
     int rpb = (int)((110 * 1024 / sizeof(float) - stage_floats) / (size_t)a.n);
@@ -441,7 +486,8 @@ cudaError_t launch_getrs_blocked(const RealBatch &a, const int *ipiv, const int 
     if (blocks < 1) blocks = 1;
     getrs_blocked_kernel<<<(unsigned)blocks, ST, smem, stream>>>(a.single, a.table, a.first, ipiv, perm, b.single,
                                                                  b.table, b.first, a.n, a.ld, b.ld, nrhs, a.count,
-                                                                 rpb, info, skip, dinv, (a.n + KB - 1) / KB);
+                                                                 rpb, info, skip, dinv, (a.n + KB - 1) / KB,
+                                                                 lists);
     return cudaGetLastError();
 }
 
