@@ -1156,13 +1156,29 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
                 }
             __syncthreads();
             const int nch = min(sh.nchanged, 2 * NB);
-            if (t < nch)
             {
-                const int p = sh.changed[t];
-                sh.chg[k0 / NB][t] = (short)p;
-                sh.src[k0 / NB][t] = sh.perm[p];
+                // kept for the epilogue, and written out for a solve over factors without the
+                // left interchanges
+                short *entry = lists_out ? lists_out + ((size_t)q * BLOCKED_PANELS + k0 / NB) * PANEL_LIST_SHORTS
+                                         : nullptr;
+                if (t < nch)
+                {
+                    const int p = sh.changed[t];
+                    const short from = sh.perm[p];
+                    sh.chg[k0 / NB][t] = (short)p;
+                    sh.src[k0 / NB][t] = from;
+                    if (entry)
+                    {
+                        entry[1 + t] = (short)p;
+                        entry[1 + 2 * NB + t] = from;
+                    }
+                }
+                if (t == 0)
+                {
+                    sh.nchg[k0 / NB] = nch;
+                    if (entry) entry[0] = (short)nch;
+                }
             }
-            if (t == 0) sh.nchg[k0 / NB] = nch;
             // (1) row interchanges on the panel and trailing columns: a warp per column,
             //     SWAP_COLS columns in flight, every source read before any destination is
             //     written
@@ -1364,24 +1380,6 @@ __global__ void __launch_bounds__(BT, 2) getrf_blocked_kernel(float *single, flo
         __syncthreads();
         }
         const int npanel_all = (n + NB - 1) / NB;
-        if (lists_out)
-        {
-            // the panels' row changes, for a solve over factors without the left interchanges
-            short *lq = lists_out + (size_t)q * BLOCKED_PANELS * PANEL_LIST_SHORTS;
-            for (int e = t; e < npanel_all * (2 * NB + 1); e += BT)
-            {
-                const int p = e / (2 * NB + 1), i = e % (2 * NB + 1);
-                const int cnt = piv ? sh.nchg[p] : 0;
-                short *entry = lq + (size_t)p * PANEL_LIST_SHORTS;
-                if (i == 2 * NB)
-                    entry[0] = (short)cnt;
-                else if (i < cnt)
-                {
-                    entry[1 + i] = sh.chg[p][i];
-                    entry[1 + 2 * NB + i] = sh.src[p][i];
-                }
-            }
-        }
         if (perm_out && piv)
         {
             // the composed permutation: position i of the factors holds original row P[i]

@@ -183,9 +183,37 @@ __device__ __forceinline__ void apply_block_changes(const short *lists, int blk,
     }
 }
 
+// The interchanges of ipiv in order (LAPACK form, validated by the caller): warp r applies them
+// to right-hand side r; the pivots come 32 at a time into the lanes' registers, so the
+// serial chain of swaps runs on shared memory and shuffles alone.
+__device__ __forceinline__ void apply_pivots(const int *piv, int n, float *x, int nr)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp >= nr) return;
+    float *xr = x + (size_t)warp * n;
+    for (int c0 = 0; c0 < n; c0 += 32)
+    {
+        const int k = c0 + lane;
+        const int pv = k < n ? piv[k] - 1 : k;
+        const int cnt = min(32, n - c0);
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+        {
+            if (j >= cnt) break;  // uniform
+            const int p = __shfl_sync(0xffffffffu, pv, j);
+            if (lane == 0 && p != c0 + j)
+            {
+                const float a = xr[c0 + j];
+                xr[c0 + j] = xr[p];
+                xr[p] = a;
+            }
+        }
+    }
+}
+
 template <bool FORWARD>
 __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *stages, bool vec, const float *dinv,
-                      const short *lists)
+                      const short *lists, const int *piv)
 {
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int nblk = (n + KB - 1) / KB;
@@ -206,6 +234,9 @@ __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *s
         if (live[i]) issue_task<FORWARD>(A, lda, n, q[i], stages + (size_t)i * KB * SP, vec, dinv);
         cp_commit();
     }
+    // the row interchanges run while the first tiles are copied (the loop's first barrier
+    // publishes them)
+    if (FORWARD && piv) apply_pivots(piv, n, x, nr);
     int slot = 0;
     while (live[0])
     {
@@ -361,27 +392,11 @@ __global__ void __launch_bounds__(ST, 2) getrs_blocked_kernel(float *a_single, f
             __syncthreads();
             continue;
         }
-        // interchanges, in order: one thread per right-hand side
-        if (piv && !sig && t < nr)
-        {
-            float *xr = x + (size_t)t * n;
-            for (int k = 0; k < n; ++k)
-            {
-                const int p = piv[k] - 1;
-                if (p != k)
-                {
-                    const float a = xr[k];
-                    xr[k] = xr[p];
-                    xr[p] = a;
-                }
-            }
-        }
-        __syncthreads();
         const bool vec = (reinterpret_cast<uintptr_t>(A) & 15u) == 0 && (lda & 3) == 0;
         const float *dinv = dinv_all ? dinv_all + (size_t)q * nblk * 2 * KB * KB : nullptr;
         const short *lists = lists_all ? lists_all + (size_t)q * BLOCKED_PANELS * PANEL_LIST_SHORTS : nullptr;
-        sweep<true>(A, lda, n, x, nr, stages, vec, dinv, lists);
-        sweep<false>(A, lda, n, x, nr, stages, vec, dinv, nullptr);
+        sweep<true>(A, lda, n, x, nr, stages, vec, dinv, lists, sig ? nullptr : piv);
+        sweep<false>(A, lda, n, x, nr, stages, vec, dinv, nullptr, nullptr);
         for (int e = t; e < nr * n; e += ST)
         {
             const int r = e / n, i = e % n;
