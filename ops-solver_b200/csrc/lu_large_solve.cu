@@ -260,12 +260,13 @@ __global__ void __launch_bounds__(SB, 1) large_diag_inverse(const float *A, int 
 // The same sweep as one cooperative launch: block s owns 128-row strip s for the whole sweep.
 // It applies the finished blocks b in order (forward: b < s ascending; backward: b > s
 // descending), each as soon as block b has published its solution (flag[b] == epoch), with
-// the factor tile prefetched while it waits, then solves its own diagonal block and publishes
-// it.  Per element the order is that of the per-block sweep (bit-identical results).  Waits
+// the next factor tile streaming into a second buffer meanwhile, then solves its own diagonal
+// block and publishes it.  Per element the order is that of the per-block sweep (bit-identical results).  Waits
 // are bounded: one that runs out sets *bad to 2 and the block goes on (the solve is then
 // reported failed, never hangs).  All blocks are resident (cooperative launch), so every
 // flag is eventually set.
 constexpr long long FLAG_WAIT = 1ll << 22;
+static_assert(SB == 16 * (ST / 32) && LARGE_SOLVE_MAX_RHS == 16, "a warp's 16 rows, a lane's four rows and two right-hand sides");
 
 template <bool FORWARD>
 __global__ void __launch_bounds__(ST, 1) large_sweep_coop(const float *A1, const float *const *At, int lda, int n,
@@ -274,8 +275,8 @@ __global__ void __launch_bounds__(ST, 1) large_sweep_coop(const float *A1, const
 {
     extern __shared__ __align__(16) float sm[];
     float *D = sm;                            // this strip's diagonal block, pitch SBP4
-    float *L = D + SB * SBP4;                 // the factor tile of the block being applied
-    float *xs = L + SB * SBP4;                // this strip's right-hand sides, xs[r][i]
+    float *Lbuf = D + SB * SBP4;              // two factor tiles: the one applied, the next one
+    float *xs = Lbuf + 2 * SB * SBP4;         // this strip's right-hand sides, xs[r][i]
     float *xb = xs + LARGE_SOLVE_MAX_RHS * SB;  // the applied block's solution
     __shared__ int stop;
     if (*bad == 1) return;  // uniform: invalid pivots, nothing is solved
@@ -294,18 +295,25 @@ __global__ void __launch_bounds__(ST, 1) large_sweep_coop(const float *A1, const
     if (t == 0) stop = 0;
     const int nprev = FORWARD ? s : nb - 1 - s;  // blocks applied before this strip's own
     auto block_of = [&](int q) { return FORWARD ? q : nb - 1 - q; };
-    if (nprev > 0)
+    auto stage_block = [&](int q)
     {
-        const int b = block_of(0);
-        stage_tile(L, SBP4, A + (int64_t)(b * SB) * lda + s0, lda, sw, min(SB, n - b * SB), vec && sw == SB);
-    }
+        const int b = block_of(q);
+        stage_tile(Lbuf + (size_t)(q & 1) * SB * SBP4, SBP4, A + (int64_t)(b * SB) * lda + s0, lda, sw,
+                   min(SB, n - b * SB), vec && sw == SB);
+    };
+    if (nprev > 0) stage_block(0);
     tile_wait();
     __syncthreads();
-    constexpr int RPT = LARGE_SOLVE_MAX_RHS / (ST / SB);
-    const int i = t % SB, r0 = t / SB;
+    // register blocking: warp w owns rows 16w .. 16w + 15 of the strip for every right-hand
+    // side, lane l rows 16w + 4(l % 4) .. + 3 and the right-hand sides 2(l / 4), 2(l / 4) + 1,
+    // so that each warp reads a factor tile's rows once (the lanes of a row quad share the
+    // loads) and the applied solution is kept k-major, xb[k][r].  Per element the updates still
+    // run in the sweep's order; the columns past nrhs compute on junk and are never stored.
+    const int row4 = 16 * warp + 4 * (lane & 3), rp = 2 * (lane >> 2);
     for (int q = 0; q < nprev; ++q)
     {
         const int b = block_of(q), b0 = b * SB, bw = min(SB, n - b0);
+        if (q + 1 < nprev) stage_block(q + 1);  // the next tile streams in during this one
         // block b's solution
         if (t == 0)
         {
@@ -329,52 +337,65 @@ __global__ void __launch_bounds__(ST, 1) large_sweep_coop(const float *A1, const
         for (int e = t; e < nrhs * SB; e += ST)
         {
             const int r = e / SB, k = e % SB;
-            xb[r * SB + k] = k < bw ? __ldcg(Y + (int64_t)r * n + b0 + k) : 0.0f;
+            xb[k * LARGE_SOLVE_MAX_RHS + r] = k < bw ? __ldcg(Y + (int64_t)r * n + b0 + k) : 0.0f;
         }
+        if (q + 1 < nprev)
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        else
+            tile_wait();
         __syncthreads();
         // this strip minus L(s, b) x_b (or U(s, b) x_b), ascending (descending) k
-        if (i < sw)
+        const float *L = Lbuf + (size_t)(q & 1) * SB * SBP4;
         {
-#pragma unroll
-            for (int u = 0; u < RPT; ++u)
+            float4 a0 = *reinterpret_cast<const float4 *>(xs + rp * SB + row4);
+            float4 a1 = *reinterpret_cast<const float4 *>(xs + (rp + 1) * SB + row4);
+#pragma unroll 8
+            for (int kk = 0; kk < bw; ++kk)
             {
-                const int r = r0 + u * (ST / SB);
-                if (r >= nrhs) continue;
-                float acc = xs[r * SB + i];
-                for (int kk = 0; kk < bw; ++kk)
-                {
-                    const int k = FORWARD ? kk : bw - 1 - kk;
-                    acc = fma_rn(-L[k * SBP4 + i], xb[r * SB + k], acc);
-                }
-                xs[r * SB + i] = acc;
+                const int k = FORWARD ? kk : bw - 1 - kk;
+                const float4 l = *reinterpret_cast<const float4 *>(L + k * SBP4 + row4);
+                const float2 x = *reinterpret_cast<const float2 *>(xb + k * LARGE_SOLVE_MAX_RHS + rp);
+                a0.x = fma_rn(-l.x, x.x, a0.x);
+                a0.y = fma_rn(-l.y, x.x, a0.y);
+                a0.z = fma_rn(-l.z, x.x, a0.z);
+                a0.w = fma_rn(-l.w, x.x, a0.w);
+                a1.x = fma_rn(-l.x, x.y, a1.x);
+                a1.y = fma_rn(-l.y, x.y, a1.y);
+                a1.z = fma_rn(-l.z, x.y, a1.z);
+                a1.w = fma_rn(-l.w, x.y, a1.w);
             }
+            *reinterpret_cast<float4 *>(xs + rp * SB + row4) = a0;
+            *reinterpret_cast<float4 *>(xs + (rp + 1) * SB + row4) = a1;
         }
         __syncthreads();
-        if (q + 1 < nprev)
-        {
-            const int nbk = block_of(q + 1);
-            stage_tile(L, SBP4, A + (int64_t)(nbk * SB) * lda + s0, lda, sw, min(SB, n - nbk * SB), vec && sw == SB);
-            tile_wait();
-            __syncthreads();
-        }
     }
+    tile_wait();  // nothing of a stopped sweep is left in flight
     if (dinv)
     {
-        // x = inv xs, a thread per (row, right-hand sides r0, r0 + 2, ...), into xb
-        if (i < sw)
+        // x = inv xs (ascending k from zero): xs goes k-major into xb, the product back into xs
+        for (int e = t; e < LARGE_SOLVE_MAX_RHS * SB; e += ST)
         {
-#pragma unroll
-            for (int u = 0; u < RPT; ++u)
-            {
-                const int r = r0 + u * (ST / SB);
-                if (r >= nrhs) continue;
-                float acc = 0.0f;
-                for (int k = 0; k < sw; ++k) acc = fma_rn(D[k * SBP4 + i], xs[r * SB + k], acc);
-                xb[r * SB + i] = acc;
-            }
+            const int r = e / SB, k = e % SB;
+            xb[k * LARGE_SOLVE_MAX_RHS + r] = r < nrhs ? xs[r * SB + k] : 0.0f;
         }
         __syncthreads();
-        for (int e = t; e < nrhs * SB; e += ST) xs[e] = xb[e];
+        float4 a0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), a1 = a0;
+#pragma unroll 8
+        for (int k = 0; k < sw; ++k)
+        {
+            const float4 d = *reinterpret_cast<const float4 *>(D + k * SBP4 + row4);
+            const float2 x = *reinterpret_cast<const float2 *>(xb + k * LARGE_SOLVE_MAX_RHS + rp);
+            a0.x = fma_rn(d.x, x.x, a0.x);
+            a0.y = fma_rn(d.y, x.x, a0.y);
+            a0.z = fma_rn(d.z, x.x, a0.z);
+            a0.w = fma_rn(d.w, x.x, a0.w);
+            a1.x = fma_rn(d.x, x.y, a1.x);
+            a1.y = fma_rn(d.y, x.y, a1.y);
+            a1.z = fma_rn(d.z, x.y, a1.z);
+            a1.w = fma_rn(d.w, x.y, a1.w);
+        }
+        *reinterpret_cast<float4 *>(xs + rp * SB + row4) = a0;
+        *reinterpret_cast<float4 *>(xs + (rp + 1) * SB + row4) = a1;
         __syncthreads();
     }
     else
@@ -520,10 +541,10 @@ cudaError_t launch_getrs_large(const float *A, const float *const *At, int lda, 
     const int64_t total = (int64_t)n * nrhs;
     large_gather_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(X, Xt, ldx, n, nrhs, use, Y);
     const int nb = (n + SB - 1) / SB;
-    // the forward sweep as one cooperative launch where all its blocks can be resident, else a
-    // launch per 128-row block
+    // each sweep as one cooperative launch where all its blocks can be resident, else a launch
+    // per 128-row block
     static int coop_ok = -1;
-    const size_t csmem = (2 * SB * SBP4 + 2 * (size_t)LARGE_SOLVE_MAX_RHS * SB) * sizeof(float);
+    const size_t csmem = (3 * SB * SBP4 + 2 * (size_t)LARGE_SOLVE_MAX_RHS * SB) * sizeof(float);
     if (coop_ok < 0)
     {
         int dev = 0, attr_coop = 0, per_sm = 0, sms = 0;
@@ -557,21 +578,10 @@ cudaError_t launch_getrs_large(const float *A, const float *const *At, int lda, 
         cudaError_t e = cudaLaunchCooperativeKernel((const void *)large_sweep_coop<true>, dim3(nb), dim3(ST), fwd,
                                                     csmem, stream);
         if (e != cudaSuccess) return e;
-        if (dinv)
-        {
-            void *bwd[] = {(void *)&a1, (void *)&at, (void *)&ld, (void *)&nn, (void *)&y, (void *)&nr, (void *)&fb,
-                           (void *)&epv, (void *)&bad, (void *)&dv};
-            e = cudaLaunchCooperativeKernel((const void *)large_sweep_coop<false>, dim3(nb), dim3(ST), bwd, csmem,
-                                            stream);
-            if (e != cudaSuccess) return e;
-        }
-        else
-        {
-            // in the oracle's order the backward sweep stays one launch per block: its chain of
-            // IEEE divisions makes the cooperative form slower there (2.7 vs 2.1 ms at 8192)
-            for (int b = nb - 1; b >= 0; --b)
-                large_sweep_kernel<false><<<b + 1, ST, smem, stream>>>(A, At, lda, n, Y, nrhs, b, bad);
-        }
+        void *bwd[] = {(void *)&a1, (void *)&at, (void *)&ld, (void *)&nn, (void *)&y, (void *)&nr, (void *)&fb,
+                       (void *)&epv, (void *)&bad, (void *)&dv};
+        e = cudaLaunchCooperativeKernel((const void *)large_sweep_coop<false>, dim3(nb), dim3(ST), bwd, csmem, stream);
+        if (e != cudaSuccess) return e;
     }
     else
     {
