@@ -21,36 +21,91 @@ constexpr int ST = 256;  // threads
 constexpr int SBP4 = SB + 4;  // shared pitch of the staged 128 x 128 tiles (16-byte rows)
 
 // perm[i] = the original row that ends at position i after the swaps ipiv[0..n-1].
+// Two phases instead of one serial chain of n swaps.  (1) A warp per chunk of 32 swaps
+// composes the chunk into a list of moves "position p takes the row that was at position q
+// before the chunk": lane l holds position k0 + l and, when it is the first lane naming it,
+// its swap's target outside the chunk; each swap exchanges two such slots by shuffles.
+// (2) One warp applies the chunks' lists in order to the identity.  An out-of-range pivot
+// (below its own index or past n) counts as no swap and sets *bad = 1 (the solve is skipped).
+constexpr int PERM_CHUNK = 32;
+constexpr int PERM_MAX_CHUNKS = LARGE_MAX_COLS / PERM_CHUNK;
+constexpr size_t PERM_SMEM = (size_t)LARGE_MAX_COLS * sizeof(short) +
+                             (size_t)PERM_MAX_CHUNKS * 2 * PERM_CHUNK * sizeof(int) + PERM_MAX_CHUNKS * sizeof(int);
+
 __global__ void __launch_bounds__(1024) large_perm_kernel(const int *ipiv, int n, int *perm, int *bad)
 {
-    __shared__ short P[LARGE_MAX_COLS];
-    __shared__ short Q[LARGE_MAX_COLS];  // the pivots (0-based, -1 when out of range), read once
-    const int t = threadIdx.x;
-    for (int i = t; i < n; i += blockDim.x)
-    {
-        P[i] = (short)i;
-        const int r = ipiv[i] - 1;
-        Q[i] = (short)(r < i || r >= n ? -1 : r);
-    }
+    extern __shared__ __align__(16) unsigned char psm[];
+    short *P = reinterpret_cast<short *>(psm);
+    int *moves = reinterpret_cast<int *>(P + LARGE_MAX_COLS);  // per chunk: (position << 16) | source
+    int *count = moves + PERM_MAX_CHUNKS * 2 * PERM_CHUNK;
+    __shared__ int bflag;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int nch = (n + PERM_CHUNK - 1) / PERM_CHUNK;
+    if (t == 0) bflag = 0;
     __syncthreads();
-    if (t == 0)
+    for (int c = warp; c < nch; c += blockDim.x / 32)
     {
-        int b = 0;
-        for (int k = 0; k < n; ++k)
+        const int k0 = c * PERM_CHUNK, kend = min(n, k0 + PERM_CHUNK);
+        const int k = k0 + lane;
+        int r = k < n ? ipiv[k] - 1 : k;
+        if (k < n && (r < k || r >= n))
         {
-            const int r = Q[k];
-            if (r < 0)
-            {
-                b = 1;  // the whole solve is skipped
-                continue;
-            }
-            const short v = P[k];
-            P[k] = P[r];
-            P[r] = v;
+            bflag = 1;
+            r = k;
         }
-        *bad = b;
+        const bool outside = r >= kend;
+        const unsigned same = __match_any_sync(0xffffffffu, r);
+        const bool ownb = outside && lane == __ffs(same) - 1;  // this lane's slot B holds position r
+        int srca = k, srcb = r;
+        for (int j = 0; j < kend - k0; ++j)
+        {
+            const int bpos = __shfl_sync(0xffffffffu, r, j);
+            const int owner = __ffs(__ballot_sync(0xffffffffu, ownb && r == bpos)) - 1;  // -1 inside the chunk
+            const int va = __shfl_sync(0xffffffffu, srca, j);
+            const bool in = bpos < kend;
+            const int vin = __shfl_sync(0xffffffffu, srca, in ? bpos - k0 : 0);
+            const int vout = __shfl_sync(0xffffffffu, srcb, in ? 0 : owner);
+            const int vb = in ? vin : vout;
+            if (lane == j) srca = vb;
+            if (in && lane == bpos - k0) srca = va;
+            if (!in && lane == owner) srcb = va;
+        }
+        const bool ma = k < kend && srca != k, mb = ownb && srcb != r;
+        const unsigned ba = __ballot_sync(0xffffffffu, ma), bb = __ballot_sync(0xffffffffu, mb);
+        const unsigned below = (1u << lane) - 1u;
+        int *list = moves + (size_t)c * 2 * PERM_CHUNK;
+        if (ma) list[__popc(ba & below)] = (k << 16) | srca;
+        if (mb) list[__popc(ba) + __popc(bb & below)] = (r << 16) | srcb;
+        if (lane == 0) count[c] = __popc(ba) + __popc(bb);
+    }
+    for (int i = t; i < n; i += blockDim.x) P[i] = (short)i;
+    __syncthreads();
+    if (warp == 0)
+    {
+        for (int c = 0; c < nch; ++c)
+        {
+            const int cnt = count[c];
+            const int *list = moves + (size_t)c * 2 * PERM_CHUNK;
+            int m0 = -1, m1 = -1;
+            short v0 = 0, v1 = 0;
+            if (lane < cnt)
+            {
+                m0 = list[lane];
+                v0 = P[m0 & 0xffff];
+            }
+            if (lane + 32 < cnt)
+            {
+                m1 = list[lane + 32];
+                v1 = P[m1 & 0xffff];
+            }
+            __syncwarp();
+            if (m0 >= 0) P[m0 >> 16] = v0;
+            if (m1 >= 0) P[m1 >> 16] = v1;
+            __syncwarp();
+        }
     }
     __syncthreads();
+    if (t == 0) *bad = bflag;
     for (int i = t; i < n; i += blockDim.x) perm[i] = P[i];
 }
 
@@ -120,7 +175,12 @@ __global__ void __launch_bounds__(ST) large_sweep_kernel(const float *A1, const 
             const bool la = ra < nrhs, lb = rb2 < nrhs;  // warp-uniform
             float va = la && lane < cw ? xa[lane] : 0.0f;
             float vb = lb && lane < cw ? xb[lane] : 0.0f;
-            if (FORWARD)
+            if (!la && !lb)
+            {
+                // no right-hand side in this warp (and no dummy divisions: a zero dividend
+                // takes the division's slow path)
+            }
+            else if (FORWARD)
             {
                 for (int k = 0; k < cw; ++k)
                 {
@@ -141,7 +201,7 @@ __global__ void __launch_bounds__(ST) large_sweep_kernel(const float *A1, const 
                     {
                         const float d = D[(cb + k) * SBP4 + cb + k];
                         va = div_rn(va, d);
-                        vb = div_rn(vb, d);
+                        if (lb) vb = div_rn(vb, d);
                     }
                     const float ka = __shfl_sync(0xffffffffu, va, k), kb = __shfl_sync(0xffffffffu, vb, k);
                     if (lane < k)
@@ -410,7 +470,12 @@ __global__ void __launch_bounds__(ST, 1) large_sweep_coop(const float *A1, const
             const bool la = ra < nrhs, lb = rb2 < nrhs;
             float va = la && lane < cw ? xa[lane] : 0.0f;
             float vb = lb && lane < cw ? xc[lane] : 0.0f;
-            if (FORWARD)
+            if (!la && !lb)
+            {
+                // no right-hand side in this warp (and no dummy divisions: a zero dividend
+                // takes the division's slow path)
+            }
+            else if (FORWARD)
             {
                 for (int k = 0; k < cw; ++k)
                 {
@@ -431,7 +496,7 @@ __global__ void __launch_bounds__(ST, 1) large_sweep_coop(const float *A1, const
                     {
                         const float d = D[(cb + k) * SBP4 + cb + k];
                         va = div_rn(va, d);
-                        vb = div_rn(vb, d);
+                        if (lb) vb = div_rn(vb, d);
                     }
                     const float ka = __shfl_sync(0xffffffffu, va, k), kb = __shfl_sync(0xffffffffu, vb, k);
                     if (lane < k)
@@ -488,7 +553,14 @@ size_t large_solve_scratch_bytes(int n, int nrhs)
 cudaError_t launch_large_perm(const int *ipiv, int n, int *perm, int *bad, cudaStream_t stream)
 {
     if (n > LARGE_MAX_COLS) return cudaErrorInvalidValue;
-    large_perm_kernel<<<1, 1024, 0, stream>>>(ipiv, n, perm, bad);
+    static bool attr = false;
+    if (!attr)
+    {
+        cudaError_t e = cudaFuncSetAttribute(large_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PERM_SMEM);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    large_perm_kernel<<<1, 1024, PERM_SMEM, stream>>>(ipiv, n, perm, bad);
     return cudaGetLastError();
 }
 
@@ -530,7 +602,8 @@ cudaError_t launch_getrs_large(const float *A, const float *const *At, int lda, 
     const int *use = perm_in;  // a permutation composed earlier (its *bad already set)
     if (!use && ipiv)
     {
-        large_perm_kernel<<<1, 1024, 0, stream>>>(ipiv, n, perm, bad);
+        cudaError_t e = launch_large_perm(ipiv, n, perm, bad, stream);
+        if (e != cudaSuccess) return e;
         use = perm;
     }
     else if (!use)
