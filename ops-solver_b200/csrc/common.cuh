@@ -19,6 +19,31 @@ __device__ __forceinline__ float sqrt_rn(float a) { return __fsqrt_rn(a); }
 // fma_rn(a, b, c) = a*b + c with one rounding.
 __device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 
+// x / d rounded to nearest even when the reciprocal y = RN(1/d) is at hand (a divisor known
+// ahead of a dependent chain): q = RN(x y), then two remainder corrections r = x - d q (one
+// FMA), q = RN(q + r y).  After the first, q lies within one ulp of x / d; with y within half
+// an ulp of 1/d, Markstein's theorem (P. Markstein, IBM J. Res. Dev. 34(1), 1990; the
+// handbook form: Muller et al., Handbook of Floating-Point Arithmetic, the division
+// correction theorem) makes the second exactly RN(x / d), provided nothing overflows or
+// underflows: d_ok (|d| in [2^-60, 2^60], from div_prepare) and |x| in the same range keep
+// every intermediate a normal number.  Other operands (zeros, subnormals, infinities, NaN,
+// extreme exponents) take the IEEE division.  Tested against IEEE division in the tests.
+__device__ __forceinline__ bool div_range(float v)
+{
+    const float a = fabsf(v);
+    return a >= 0x1p-60f && a <= 0x1p60f;
+}
+__device__ __forceinline__ float div_prepare(float d) { return __frcp_rn(d); }
+__device__ __forceinline__ float div_by(float x, float d, float y, bool d_ok)
+{
+    if (!d_ok || !div_range(x)) return __fdiv_rn(x, d);
+    float q = __fmul_rn(x, y);
+    float r = __fmaf_rn(-q, d, x);
+    q = __fmaf_rn(r, y, q);
+    r = __fmaf_rn(-q, d, x);
+    return __fmaf_rn(r, y, q);
+}
+
 // Two FP32 lanes in one 64-bit register pair (sm_100 paired FP32 arithmetic): each lane of
 // fma2 is an IEEE fma rounded to nearest, i.e. exactly fma_rn on that lane.
 typedef unsigned long long f32x2;

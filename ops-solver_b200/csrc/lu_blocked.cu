@@ -239,11 +239,14 @@ __device__ __forceinline__ void panel_rows(float *A, int lda, int n, int k0, int
             else
             {
                 float l[NR];
-                const float rinv = EXACT ? 0.0f : __frcp_rn(d);
+                // the reciprocal serves both: the refined modes multiply by it, the plain mode
+                // divides through it (div_by: IEEE-exact)
+                const float rinv = __frcp_rn(d);
+                const bool dok = div_range(d);
 #pragma unroll
                 for (int s = 0; s < NR; ++s)
                 {
-                    l[s] = go[s] ? (EXACT ? div_rn(cur[s], d) : cur[s] * rinv) : 0.0f;
+                    l[s] = go[s] ? (EXACT ? div_by(cur[s], d, rinv, dok) : cur[s] * rinv) : 0.0f;
                     if (go[s]) pan[(int64_t)j * lda + t + s * BT] = l[s];
                 }
                 f32x2 nl[NR];

@@ -258,12 +258,15 @@ __global__ void __launch_bounds__(LT, 1)
             }
             else
             {
-                const float rinv = EXACT ? 0.0f : __frcp_rn(d);
+                // the reciprocal serves both: the refined modes multiply by it, the plain mode
+                // divides through it (div_by: IEEE-exact)
+                const float rinv = __frcp_rn(d);
+                const bool dok = div_range(d);
                 f32x2 nl[NR];
 #pragma unroll
                 for (int s = 0; s < NR; ++s)
                 {
-                    const float l = go[s] ? (EXACT ? div_rn(cur[s], d) : cur[s] * rinv) : 0.0f;
+                    const float l = go[s] ? (EXACT ? div_by(cur[s], d, rinv, dok) : cur[s] * rinv) : 0.0f;
                     if (go[s]) pan[(int64_t)j * lda + r0 + t + s * LT] = l;
                     nl[s] = f2_pack(-l, -l);
                 }

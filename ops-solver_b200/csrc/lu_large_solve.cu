@@ -195,13 +195,16 @@ __global__ void __launch_bounds__(ST) large_sweep_kernel(const float *A1, const 
             }
             else
             {
+                // each lane's divisor is its own diagonal entry: reciprocal ahead of the chain
+                const float dl = lane < cw ? D[(cb + lane) * SBP4 + cb + lane] : 1.0f;
+                const float yl = div_prepare(dl);
+                const bool okl = div_range(dl);
                 for (int k = cw - 1; k >= 0; --k)
                 {
                     if (lane == k)
                     {
-                        const float d = D[(cb + k) * SBP4 + cb + k];
-                        va = div_rn(va, d);
-                        if (lb) vb = div_rn(vb, d);
+                        va = div_by(va, dl, yl, okl);
+                        if (lb) vb = div_by(vb, dl, yl, okl);
                     }
                     const float ka = __shfl_sync(0xffffffffu, va, k), kb = __shfl_sync(0xffffffffu, vb, k);
                     if (lane < k)
@@ -490,13 +493,16 @@ __global__ void __launch_bounds__(ST, 1) large_sweep_coop(const float *A1, const
             }
             else
             {
+                // each lane's divisor is its own diagonal entry: reciprocal ahead of the chain
+                const float dl = lane < cw ? D[(cb + lane) * SBP4 + cb + lane] : 1.0f;
+                const float yl = div_prepare(dl);
+                const bool okl = div_range(dl);
                 for (int k = cw - 1; k >= 0; --k)
                 {
                     if (lane == k)
                     {
-                        const float d = D[(cb + k) * SBP4 + cb + k];
-                        va = div_rn(va, d);
-                        if (lb) vb = div_rn(vb, d);
+                        va = div_by(va, dl, yl, okl);
+                        if (lb) vb = div_by(vb, dl, yl, okl);
                     }
                     const float ka = __shfl_sync(0xffffffffu, va, k), kb = __shfl_sync(0xffffffffu, vb, k);
                     if (lane < k)

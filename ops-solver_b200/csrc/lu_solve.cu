@@ -284,12 +284,16 @@ __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *s
                 }
                 else
                 {
+                    // each lane's divisor is its own diagonal entry: reciprocal ahead of the chain
+                    const float dl = lane < w ? tile[lane * SP + lane] : 1.0f;
+                    const float yl = div_prepare(dl);
+                    const bool okl = div_range(dl);
 #pragma unroll
                     for (int k = KB - 1; k >= 0; --k)
                     {
                         if (k < w)
                         {
-                            if (lane == k) xv = div_rn(xv, tile[k * SP + lane]);
+                            if (lane == k) xv = div_by(xv, dl, yl, okl);
                             const float xk = __shfl_sync(0xffffffffu, xv, k);
                             if (lane < k) xv = fma_rn(-tile[k * SP + lane], xk, xv);
                         }

@@ -36,7 +36,7 @@ def rhs(count, n, nrhs, seed):
     return np.random.default_rng(seed).standard_normal((count, n, nrhs)).astype(np.float32)
 
 
-@pytest.mark.parametrize("n", [40, 100, 512])
+@pytest.mark.parametrize("n", [40, 100, 129, 333, 512])
 def test_fp32_without_refinement_is_sgetrf_sgetrs(handle, n):
     """maxIter 0 in FP32: the oracle's sgetrf + sgetrs (bit for bit up to order 64)."""
     a = np.random.default_rng(n).standard_normal((3, n, n)).astype(np.float32)
@@ -102,6 +102,26 @@ def test_bf16_reports_honest_error_when_it_cannot_converge(handle):
         assert np.isfinite(berr[q])
         # berr is that of the FP64 iterate; X is its FP32 rounding (relative 6e-8 per entry)
         assert abs(be - berr[q]) <= 1e-7 + 0.05 * berr[q]
+
+
+@pytest.mark.parametrize("n, nrhs", [(257, 9), (333, 3), (130, 17)])
+def test_ragged_orders_and_rhs_groups(handle, n, nrhs):
+    """Orders with a partial last panel and outer block, and right-hand sides spread over
+    several solve blocks: the refinement's solves apply the panels' row changes block by
+    block (no left interchanges) and must match the LAPACK-form solve's accuracy."""
+    count = 4
+    a = conditioned_batch(count, n, 1e4, seed=n)
+    b = rhs(count, n, nrhs, n + 7)
+    st, x, iters, berr, info = gesv_ir(handle, a, b, aclsolver.FACTOR_FP32, max_iter=0)
+    assert st == aclsolver.SUCCESS and np.all(info == 0)
+    lu, ipiv, _ = oracle.sgetrf_batched(a)
+    want = oracle.sgetrs_batched(lu, ipiv, b)
+    assert np.max(np.abs(x - want)) <= 1e-3 * np.max(np.abs(want))
+    st, x, iters, berr, info = gesv_ir(handle, a, b, aclsolver.FACTOR_BF16X3, max_iter=5, tol=1e-7)
+    assert st == aclsolver.SUCCESS and np.all(info == 0)
+    for q in range(count):
+        for j in range(nrhs):
+            assert judges.backward_error(a[q], x[q][:, j], b[q][:, j]) <= 1e-6, (q, j)
 
 
 def test_small_orders_and_several_rhs(handle):
