@@ -426,10 +426,21 @@ __global__ void __launch_bounds__(64) diag_inverse_kernel(float *single, float *
     const float *A = table ? slot(table, first + q) : single;
     if (!A) return;
     const int kb = b * KB, w = min(KB, n - kb);
-    for (int e = threadIdx.x; e < KB * KB; e += 64)
     {
-        const int k = e / KB, i = e % KB;
-        D[k][i] = (k < w && i < w) ? A[(int64_t)(kb + k) * lda + kb + i] : (k == i ? 1.0f : 0.0f);
+        // all sixteen loads of a thread in flight before its stores
+        float v[KB * KB / 64];
+#pragma unroll
+        for (int u = 0; u < KB * KB / 64; ++u)
+        {
+            const int e = threadIdx.x + 64 * u, k = e / KB, i = e % KB;
+            v[u] = (k < w && i < w) ? A[(int64_t)(kb + k) * lda + kb + i] : (k == i ? 1.0f : 0.0f);
+        }
+#pragma unroll
+        for (int u = 0; u < KB * KB / 64; ++u)
+        {
+            const int e = threadIdx.x + 64 * u;
+            D[e / KB][e % KB] = v[u];
+        }
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, which = threadIdx.x >> 5;
