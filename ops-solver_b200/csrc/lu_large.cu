@@ -115,6 +115,7 @@ __global__ void __launch_bounds__(LT, 1)
     constexpr unsigned STEP_BYTES = CS * CAND_BYTES;
     constexpr int PL = 32 / CS;   // lanes of warp 0 per destination block
     constexpr int PER = PW / PL;  // candidate values each of them sends
+    static_assert(PER % 4 == 0 && PER >= 4, "candidate values go out in 16-byte pieces: at least four blocks per cluster");
     __shared__ PanelShared<CS> sh;
     cg::cluster_group cluster = cg::this_cluster();
     const int c = (int)cluster.block_rank();
