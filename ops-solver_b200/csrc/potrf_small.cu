@@ -280,7 +280,7 @@ __global__ void fill_info_kernel(int *info, int value, int64_t count)
         info[i] = value;
 }
 
-// One block scans both pointer tables; a single thread writes the verdict.
+// One block scans both pointer tables; a single thread writes the outcome.
 __global__ void __launch_bounds__(1024) solve_slot_check_kernel(int *info, float *const *a, float *const *b,
                                                                 int count)
 {
