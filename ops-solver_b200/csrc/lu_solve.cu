@@ -240,13 +240,17 @@ __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *s
     int slot = 0;
     while (live[0])
     {
+        // One barrier per task.  This task's tile has landed (for this thread's copies: the
+        // group that may still be in flight is the next task's) ...
+        cp_wait<STAGES - 2>();
+        // ... and for everyone's; every thread is also done with the previous task, so its
+        // updates of x are visible and its stage may be refilled
+        __syncthreads();
         // refill: the task STAGES - 1 ahead goes to the stage freed by the previous task
         if (live[STAGES - 1])
             issue_task<FORWARD>(A, lda, n, q[STAGES - 1],
                                 stages + (size_t)((slot + STAGES - 1) % STAGES) * KB * SP, vec, dinv);
         cp_commit();
-        cp_wait<STAGES - 1>();  // this task's tile has landed (for this thread's copies)
-        __syncthreads();        // ... and for everyone's
         const float *tile = stages + (size_t)slot * KB * SP;
         const Task cur = q[0];
         const int kb = cur.blk * KB;
@@ -329,9 +333,8 @@ __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *s
                 }
             }
         }
-        // a diagonal solve feeds its strips, a block's strips feed the next diagonal, and
-        // this stage is refilled two iterations on
-        __syncthreads();
+        // a diagonal solve feeds its strips and a block's strips feed the next diagonal: the
+        // next iteration's barrier orders them
 #pragma unroll
         for (int i = 0; i < STAGES - 1; ++i)
         {
@@ -343,6 +346,7 @@ __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *s
         slot = (slot + 1) % STAGES;
     }
     cp_wait<0>();
+    __syncthreads();  // the last task is done before the caller reuses the stages and reads x
 }
 
 __global__ void __launch_bounds__(ST, 2) getrs_blocked_kernel(float *a_single, float *const *a_table, int a_first,
