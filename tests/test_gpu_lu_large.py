@@ -223,6 +223,43 @@ def test_large_sgetrs_one_system_matches_oracle(handle, n, nrhs):
     assert same_bits(got, want), first_mismatch(got, want)
 
 
+@pytest.mark.parametrize("pattern", ["identity", "last_row", "adjacent", "chunk_edges", "random"])
+def test_large_sgetrs_pivot_patterns(handle, pattern):
+    """Pivot sequences that no factorisation of a random matrix produces -- every swap with the
+    last row, a chain of adjacent swaps, swaps across the 32-swap chunks the composition works
+    in -- through the one-system solve, bit for bit against the oracle's sequential swaps."""
+    lib = aclsolver.library()
+    n, nrhs = 1100, 3
+    rng = np.random.default_rng(60)
+    lu = np.tril(rng.standard_normal((n, n)), -1) * 0.05 + np.triu(rng.standard_normal((n, n)), 1) * 0.05
+    lu[np.arange(n), np.arange(n)] = 2.0 + rng.random(n)
+    lu = lu.astype(np.float32)[None]
+    k = np.arange(n)
+    if pattern == "identity":
+        ipiv = k + 1
+    elif pattern == "last_row":
+        ipiv = np.full(n, n)
+    elif pattern == "adjacent":
+        ipiv = np.minimum(k + 2, n)
+    elif pattern == "chunk_edges":
+        ipiv = np.where(k % 32 == 31, np.minimum(k + 33, n), np.minimum(k + 32 - k % 32, n))
+    else:
+        ipiv = k + 1 + (rng.random(n) * (n - k)).astype(np.int64)
+    ipiv = ipiv.astype(np.int32).reshape(1, n)
+    b = rng.standard_normal((n, nrhs)).astype(np.float32)
+    da = DeviceMatrices(lu, ld=n)
+    db = DeviceMatrices(b[None], ld=n)
+    piv = device_ints(ipiv.reshape(-1))
+    info = info_buffer(1)
+    st = lib.aclsolverSgetrsBatched(handle.value, 0, n, nrhs, da.table_ptr, da.ld, piv.data_ptr(), db.table_ptr,
+                                   db.ld, info.data_ptr(), 1)
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 0
+    want = oracle.sgetrs_batched(lu, ipiv, b[None])[0]
+    got = db.read()[0]
+    assert same_bits(got, want), first_mismatch(got, want)
+
+
 def test_large_sgetrs_bad_pivot_leaves_b(handle):
     lib = aclsolver.library()
     n = 640
