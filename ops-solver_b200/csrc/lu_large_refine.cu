@@ -17,6 +17,7 @@ constexpr int RB = 128;    // rows per block
 constexpr int CC = 1024;   // columns per chunk
 constexpr int XS = 64;     // x rows staged at a time
 constexpr int MAXR = LARGE_SOLVE_MAX_RHS;
+static_assert(MAXR == 16 && RB % 2 == 0, "two rows and eight right-hand sides per thread");
 
 __global__ void lir_copy_in(const float *const *B, int ldb, int n, int nrhs, float *r32)
 {
@@ -47,49 +48,77 @@ __global__ void lir_update(LargeIr s, int n, int nrhs, int first)
 // chunk's |A| row sums
 __global__ void __launch_bounds__(RB) lir_partial(const float *const *Aarr, int lda, int n, int nrhs, LargeIr s)
 {
-    __shared__ double xs[XS][MAXR + 1];
+    // register blocking: thread (p = t % 64, h = t / 64) owns rows 2p, 2p + 1 of the block and
+    // right-hand sides 8h .. 8h + 7, so each staged x pair feeds four FMAs; per element the
+    // products still accumulate in ascending column order
+    __shared__ __align__(16) double xs[XS][MAXR];
     const float *A = slot(Aarr, 0);
     const int t = threadIdx.x;
-    const int i = blockIdx.x * RB + t;
+    const int p = t % (RB / 2), h = t / (RB / 2);
+    const int i0 = blockIdx.x * RB + 2 * p;
     const int j0 = blockIdx.y * CC, j1 = min(n, j0 + CC);
-    double acc[MAXR];
+    double acc[2][MAXR / 2];
 #pragma unroll
-    for (int r = 0; r < MAXR; ++r) acc[r] = 0.0;
-    double asum = 0.0;
+    for (int e = 0; e < 2; ++e)
+#pragma unroll
+        for (int r = 0; r < MAXR / 2; ++r) acc[e][r] = 0.0;
+    double asum[2] = {0.0, 0.0};
+    const bool r0ok = i0 < n, r1ok = i0 + 1 < n;
     for (int jb = j0; jb < j1; jb += XS)
     {
         __syncthreads();
         for (int e = t; e < XS * MAXR; e += RB)
         {
-            const int r = e / XS, jj = e % XS;  // consecutive threads: consecutive columns of x
+            // consecutive threads: consecutive right-hand sides (conflict-free shared stores;
+            // x is small and read from L2)
+            const int r = e % MAXR, jj = e / MAXR;
             xs[jj][r] = (jb + jj < j1 && r < nrhs) ? s.x64[(int64_t)r * n + jb + jj] : 0.0;
         }
         __syncthreads();
-        if (i < n)
+        if (r0ok)
         {
             const int je = min(XS, j1 - jb);
             for (int jj = 0; jj < je; jj += 16)
             {
-                double av[16];  // sixteen loads in flight before their products
-#pragma unroll
-                for (int u = 0; u < 16; ++u) av[u] = jj + u < je ? (double)A[(int64_t)(jb + jj + u) * lda + i] : 0.0;
+                float av[16][2];  // sixteen columns of the row pair in flight before their products
 #pragma unroll
                 for (int u = 0; u < 16; ++u)
                 {
-                    asum += fabs(av[u]);
+                    const float *col = A + (int64_t)(jb + jj + u) * lda + i0;
+                    av[u][0] = jj + u < je ? col[0] : 0.0f;
+                    av[u][1] = jj + u < je && r1ok ? col[1] : 0.0f;
+                }
 #pragma unroll
-                    for (int r = 0; r < MAXR; ++r) acc[r] = fma(av[u], xs[jj + u][r], acc[r]);
+                for (int u = 0; u < 16; ++u)
+                {
+                    const double a0 = (double)av[u][0], a1 = (double)av[u][1];
+                    asum[0] += fabs(a0);
+                    asum[1] += fabs(a1);
+                    const double2 *xr = reinterpret_cast<const double2 *>(&xs[jj + u][h * (MAXR / 2)]);
+#pragma unroll
+                    for (int q = 0; q < MAXR / 4; ++q)
+                    {
+                        const double2 x = xr[q];
+                        acc[0][2 * q] = fma(a0, x.x, acc[0][2 * q]);
+                        acc[0][2 * q + 1] = fma(a0, x.y, acc[0][2 * q + 1]);
+                        acc[1][2 * q] = fma(a1, x.x, acc[1][2 * q]);
+                        acc[1][2 * q + 1] = fma(a1, x.y, acc[1][2 * q + 1]);
+                    }
                 }
             }
         }
     }
-    if (i >= n) return;
-    const int nch = gridDim.y;
+    if (!r0ok) return;
 #pragma unroll
-    for (int r = 0; r < MAXR; ++r)  // static indices: acc stays in registers
-        if (r < nrhs) s.part[((int64_t)blockIdx.y * MAXR + r) * n + i] = acc[r];
-    s.apart[(int64_t)blockIdx.y * n + i] = asum;
-    (void)nch;
+    for (int e = 0; e < 2; ++e)
+    {
+        if (e == 1 && !r1ok) break;
+#pragma unroll
+        for (int r = 0; r < MAXR / 2; ++r)  // static indices: acc stays in registers
+            if (h * (MAXR / 2) + r < nrhs)
+                s.part[((int64_t)blockIdx.y * MAXR + h * (MAXR / 2) + r) * n + i0 + e] = acc[e][r];
+        if (h == 0) s.apart[(int64_t)blockIdx.y * n + i0 + e] = asum[e];
+    }
 }
 
 // r = b - sum of the chunks (in chunk order) for every right-hand side; the FP32 copy for the
