@@ -211,7 +211,10 @@ __device__ __forceinline__ void panel_rows(float *A, int lda, int n, int k0, int
             // Lane i reads warp i & 7's report; the lowest matching lane names the warp.
             const uint2 kw = sh.key[buf][lane & (NW - 1)];
             const unsigned gmax = __reduce_max_sync(FULL, kw.x);
-            const unsigned gpos = __reduce_min_sync(FULL, kw.x == gmax ? kw.y : 0xffffffffu);
+            // the refined modes' keys carry the position, so the largest one names it (a live
+            // row always has a nonzero key); the exact mode settles ties by a second reduction
+            const unsigned gpos = EXACT ? __reduce_min_sync(FULL, kw.x == gmax ? kw.y : 0xffffffffu)
+                                        : (unsigned)(MAXN - 1) - (gmax & (MAXN - 1));
             const int gw = __ffs(__ballot_sync(FULL, kw.x == gmax && kw.y == gpos)) - 1;
             const int pr = (int)gpos;
             const float *prow = sh.slot[buf][gw];  // prow[c]: the pivot row at column j0 + c
