@@ -48,6 +48,38 @@ def test_null_handle_is_reported(name, args):
     assert getattr(lib, name)(None, *args) == aclsolver.HANDLE_IS_NULLPTR
 
 
+@pytest.mark.parametrize(
+    "name,args",
+    [
+        ("aclsolverSgetrsBatched", [0, 4, 1, None, 4, None, None, 4, None, 1]),
+        ("aclsolverSgetrfBatchedMixed", [3, 4, None, 4, None, None, 1]),
+        ("aclsolverSgesvIrBatched", [3, 4, 1, None, 4, None, 4, None, 4, 2, 1e-7, None, None, None, 1]),
+        ("aclsolverSmatinvBatchedNoAlloc", [4, None, 4, None, 4, None, 1]),
+        ("aclsolverSetDeviceChecks", [0]),
+    ],
+)
+def test_null_handle_is_reported_by_the_additions(name, args):
+    """The real-family additions follow the real family: HANDLE_IS_NULLPTR before any
+    argument is looked at."""
+    lib = aclsolver.library()
+    assert getattr(lib, name)(None, *args) == aclsolver.HANDLE_IS_NULLPTR
+
+
+@pytest.mark.parametrize(
+    "name,args",
+    [
+        ("aclsolverCpotrfBatched", [0, 4, None, 4, None, 1]),
+        ("aclsolverCpotrsBatched", [0, 4, 1, None, 4, None, 4, None, 1]),
+        ("aclsolverCpotrsBatchedMultiRhs", [0, 4, 2, None, 4, None, 4, None, 1]),
+    ],
+)
+def test_null_handle_in_the_complex_family(name, args):
+    """The complex entries keep the reference's own convention for a null handle:
+    NOT_INITIALIZED."""
+    lib = aclsolver.library()
+    assert getattr(lib, name)(None, *args) == aclsolver.NOT_INITIALIZED
+
+
 def test_get_stream_contract():
     lib = aclsolver.library()
     out = C.c_void_p()
