@@ -1,10 +1,11 @@
 """Benchmark: mixed-precision LU with FP64 iterative refinement against plain FP32 LU + solve,
-on B200, through the aclsolver C ABI.
+on B200, through the aclsolver C ABI, with the plain batched factor-and-solve workloads
+measured beside it.
 
-Workload (the mixed-precision batched LU configuration): 256 matrices of order 512,
-A = U diag(s) V^T with U, V Haar-random orthogonal (QR of N(0,1)) and s log-spaced from 1 to
-1/kappa, kappa cycling through 1e2, 1e4, 1e5 over the batch; one N(0,1) right-hand side each.
-The data is synthetic (seeded); no benchmark suite is involved.
+Headline workload (the mixed-precision batched LU configuration): 256 matrices of order
+512, A = U diag(s) V^T with U, V Haar-random orthogonal (QR of N(0,1)) and s log-spaced from
+1 to 1/kappa, kappa cycling through 1e2, 1e4, 1e5 over the batch; one N(0,1) right-hand side
+each.  All data is synthetic (seeded); no benchmark suite is involved.
 
 One step = one aclsolverSgesvIrBatched call over the batch (split-BF16 tensor-core trailing
 updates, FP32 panels and solves, FP64 residual and update, tolerance 1e-7 on the normwise
@@ -16,9 +17,21 @@ timed the same way and reported beside it with both backward errors (`plain`, `m
 ratio is taken at equal (FP32-level) backward error.  `e2e` is the refinement call with
 pinned host buffers: A and b copied in and x copied out inside the timed region.
 
-`python bench.py --impl reference` times the reference's CPU path (the oracle, a C
-restatement of the reference's FP32 LU and solve arithmetic) on this host with all its
-threads, on a bounded sample of the same workload.
+`configs` carries the plain batched workloads, each timed on the device the same way (inputs
+restored from a pristine copy and a 256 MiB buffer written before every step, so the timed
+bytes come from HBM) with its roofline and its own CPU baseline:
+  c1  10,000 SPD 32x32, SpotrfBatched + SpotrsBatched (fp32, lower, 1 RHS);
+  c2  4,096 N(0,1) 64x64, SgetrfBatched + SgetrsBatched + SgetriBatched (fp32, 1 RHS);
+  c3  20,000 HPD complex64 of orders U{8..128}, 4 RHS, one CposvVbatched call (persistent,
+      size-bucketed, graph-captured, autotuned).
+`large` carries the single 8192 x 8192 system (plain and mixed).
+
+CPU baseline: the host LAPACK the reference's tests use as their golden (scipy's bundled
+OpenBLAS, FP32 sgetrf/sgetrs/sgetri/spotrf/spotrs/cpotrf/cpotrs) on this host's cores, OpenMP
+over matrices with one OpenBLAS thread per call (OpenBLAS threaded for the single system).
+
+`python bench.py --impl reference` times that same host LAPACK on the headline workload (all
+256 systems, the same step count).
 
 Multi-GPU (`torchrun ... bench.py --gpus N`): every rank solves its own batch of 256 systems
 (independent matrices: replicas, no data-path collective); time is the maximum over ranks and
@@ -56,6 +69,8 @@ SOLVE_FLOPS = 2 * N**3 / 3 + 2 * N * N * NRHS
 FACTOR_BYTES = 2 * N * N * 4
 FACTOR_FLOPS = 2 * N**3 / 3
 FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+SMS = 148
+FLUSH_BYTES = 256 << 20
 
 
 def peaks():
@@ -64,6 +79,16 @@ def peaks():
         d = json.loads(p.read_text())
         return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
     return FALLBACK["hbm_gbs"], FALLBACK["bf16_tflops"], "fallback"
+
+
+def fp32_peak_tflops():
+    """FP32 FMA peak of the chip at its maximum SM clock: 148 SMs x 128 lanes x 2 flops.
+    No measured FP32 figure exists for this pool, so this one is nominal."""
+    mhz = 1965.0
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        mhz = float(json.loads(p.read_text()).get("sm_max_mhz", mhz))
+    return SMS * 128 * 2 * mhz * 1e6 / 1e12
 
 
 def traffic_summary():
@@ -75,6 +100,31 @@ def traffic_summary():
         except ValueError:
             return {}
     return {}
+
+
+def roofline(bytes_, flops, ms, kernel, traffic_key=None):
+    """Roofline of one timed region: the floor is the slower of the algorithmic bytes at the
+    measured HBM bandwidth and the flops at the FP32 FMA peak; `frac` is achieved / peak on
+    the bound that sets the floor."""
+    hbm, _, kind = peaks()
+    fp32 = fp32_peak_tflops()
+    t_hbm = bytes_ / (hbm * 1e9) * 1e3
+    t_fp32 = flops / (fp32 * 1e12) * 1e3
+    gbs = bytes_ / (ms * 1e-3) / 1e9
+    tflops = flops / (ms * 1e-3) / 1e12
+    out = {"kernel": kernel}
+    if t_hbm >= t_fp32:
+        out.update({"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s",
+                    "frac": round(gbs / hbm, 4), "peak_kind": kind})
+    else:
+        out.update({"bound": "fp32", "achieved": round(tflops, 2), "peak": round(fp32, 1), "unit": "TFLOP/s",
+                    "frac": round(tflops / fp32, 4), "peak_kind": "nominal FP32 FMA at the max SM clock"})
+    out.update({"hbm_frac": round(gbs / hbm, 4), "fp32_frac": round(tflops / fp32, 4),
+                "floor_ms": round(max(t_hbm, t_fp32), 5), "measured_ms": round(ms, 5),
+                "floor_over_measured": round(max(t_hbm, t_fp32) / ms, 4),
+                "algorithmic_bytes": int(bytes_), "algorithmic_flops": int(flops),
+                "traffic": traffic_summary().get(traffic_key) if traffic_key else None})
+    return out
 
 
 class ClockSampler:
@@ -176,15 +226,60 @@ def backward_errors(a_cm, x_cm, b_cm, count, device):
     return (num / den).cpu().numpy()
 
 
-def forward_errors(a, b, x, sample):
-    """||x - x64||_inf / ||x64||_inf against FP64 LAPACK (numpy) on a sample of matrices."""
+def fp64_solutions(a, b):
+    """FP64 LAPACK (numpy's gesv) solutions of every system: the forward-error oracle."""
     import numpy as np
 
-    out = []
-    for q in sample:
-        x64 = np.linalg.solve(a[q].astype(np.float64), b[q].astype(np.float64))
-        out.append(float(np.abs(x[q].astype(np.float64) - x64).max() / np.abs(x64).max()))
-    return out
+    return np.linalg.solve(a.astype(np.float64), b.astype(np.float64))
+
+
+def forward_errors(x64, x):
+    """||x - x64||_inf / ||x64||_inf per system."""
+    import numpy as np
+
+    d = np.abs(x.astype(np.float64) - x64).max(axis=(1, 2))
+    return d / np.abs(x64).max(axis=(1, 2))
+
+
+class DeviceTimer:
+    """Per-step device time of `fn` on `stream`: `before()` runs first (untimed: restore the
+    inputs, then overwrite L2 with a 256 MiB buffer), then CUDA events bracket `fn`."""
+
+    def __init__(self, stream, device):
+        import torch
+
+        self.torch = torch
+        self.stream = stream
+        self.flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=device)
+        self.ev0 = torch.cuda.Event(enable_timing=True)
+        self.ev1 = torch.cuda.Event(enable_timing=True)
+
+    def __call__(self, fn, steps, before=None):
+        torch = self.torch
+        total = 0.0
+        for i in range(steps):
+            with torch.cuda.stream(self.stream):
+                if before:
+                    before()
+                self.flush.fill_(i & 0xFF)
+                self.ev0.record(self.stream)
+                fn()
+                self.ev1.record(self.stream)
+            self.ev1.synchronize()
+            total += self.ev0.elapsed_time(self.ev1)
+        return total / max(1, steps)
+
+
+def cpu_timed(fn, seconds, min_reps=2, max_reps=200):
+    """Passes of `fn` for about `seconds` (at least `min_reps`); returns (s per pass, reps)."""
+    fn()  # warm-up (page-in, thread pool start)
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        fn()
+        reps += 1
+        dt = time.perf_counter() - t0
+        if (dt > seconds and reps >= min_reps) or reps >= max_reps:
+            return dt / reps, reps
 
 
 def run_b200(args, rank, world):
@@ -217,7 +312,7 @@ def run_b200(args, rank, world):
     info_s = torch.empty(COUNT, dtype=torch.int32, device=dev)
     iters = torch.empty(COUNT, dtype=torch.int32, device=dev)
     berr = torch.empty(COUNT, dtype=torch.float64, device=dev)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    timer = DeviceTimer(stream, dev)
     # kernels launched by one refinement call: two pointer tables, the factorisation (with the
     # copy of A and the permutation) and its later-interchange pass, the diagonal-block
     # inverses, init, solve, update, MAX_ITER x (residual, solve, update), residual, finish
@@ -239,32 +334,19 @@ def run_b200(args, rank, world):
         aclsolver.check(lib.aclsolverSgetrfBatchedMixed(handle.value, PRECISION, N, tw.data_ptr(), N,
                                                         piv.data_ptr(), info.data_ptr(), COUNT))
 
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-
-    def timed(fn, steps, restore):
-        total = 0.0
-        for i in range(steps):
-            with torch.cuda.stream(stream):
-                if restore:
-                    W.copy_(A)
-                    XP.copy_(B)
-                flush.fill_(i & 0xFF)
-                ev0.record(stream)
-                fn()
-                ev1.record(stream)
-            ev1.synchronize()
-            total += ev0.elapsed_time(ev1)
-        return total / max(1, steps)
+    def restore():
+        W.copy_(A)
+        XP.copy_(B)
 
     for _ in range(args.warmup):
-        timed(mixed, 1, False)
+        timer(mixed, 1)
     torch.cuda.synchronize()
     assert int(info.abs().max()) == 0, "unexpected info"
     barrier(world)
     torch.cuda.synchronize()
     with ClockSampler(torch.cuda.current_device()) as clocks:
         wall0 = time.perf_counter()
-        ms = timed(mixed, args.steps, False)
+        ms = timer(mixed, args.steps)
         torch.cuda.synchronize()
         wall = time.perf_counter() - wall0
     barrier(world)
@@ -274,17 +356,17 @@ def run_b200(args, rank, world):
     x_mixed = X.cpu().numpy().reshape(COUNT, NRHS, N).transpose(0, 2, 1)
 
     # plain FP32 path, same inputs (its working copy restored outside the timed region)
-    for _ in range(max(1, args.warmup // 2)):
-        timed(plain, 1, True)
-    plain_ms = max_over_ranks(timed(plain, max(3, args.steps // 2), True), world)
+    for _ in range(max(3, args.warmup // 2)):
+        timer(plain, 1, restore)
+    plain_ms = max_over_ranks(timer(plain, max(3, args.steps // 2), restore), world)
     assert int(info.abs().max()) == 0 and int(info_s.abs().max()) == 0
     plain_berr = backward_errors(A, XP, B, COUNT, dev)
     x_plain = XP.cpu().numpy().reshape(COUNT, NRHS, N).transpose(0, 2, 1)
 
     # the dominant kernel alone (the split-BF16 factorisation) for the roofline
-    for _ in range(2):
-        timed(factor_only, 1, True)
-    factor_ms = timed(factor_only, max(3, args.steps // 2), True)
+    for _ in range(3):
+        timer(factor_only, 1, restore)
+    factor_ms = timer(factor_only, max(3, args.steps // 2), restore)
 
     # e2e: host buffers, copies inside the timed region
     a_pin = torch.from_numpy(a_cm.reshape(-1)).pin_memory()
@@ -333,24 +415,37 @@ def run_b200(args, rank, world):
     assert bool(np.isfinite(x_pins[0].numpy()).all()) and bool(np.isfinite(x_pins[1].numpy()).all())
     h2d = COUNT * N * N * 4 + COUNT * N * NRHS * 4
     d2h = COUNT * N * NRHS * 4
+    del A2, B2, X2, sets, x_pins
+
+    configs = None
+    if rank != 0:
+        args.cpu_seconds = 0.0  # CPU baselines are taken on rank 0 only
+    if args.configs:
+        configs = {
+            "c1": measure_c1(handle, timer, args),
+            "c2": measure_c2(handle, timer, args),
+            "c3": measure_c3(handle, timer, args),
+        }
 
     if rank == 0:
         hbm, bf16, peak_kind = peaks()
-        sample = list(range(0, COUNT, COUNT // 12))[:12]
-        fe_mixed = forward_errors(a_host, b_host, x_mixed, sample)
-        fe_plain = forward_errors(a_host, b_host, x_plain, sample)
+        x64 = fp64_solutions(a_host, b_host)
+        fe_mixed = forward_errors(x64, x_mixed)
+        fe_plain = forward_errors(x64, x_plain)
         value = COUNT * world / (ms * 1e-3)
         plain_value = COUNT * world / (plain_ms * 1e-3)
         achieved = FACTOR_BYTES * COUNT / (factor_ms * 1e-3) / 1e9
         roof_ms = max(FACTOR_BYTES * COUNT / (hbm * 1e9), FACTOR_FLOPS * COUNT / (bf16 * 1e12)) * 1e3
-        cpu = cpu_baseline(args)
-        large = measure_large(handle) if args.large else None
+        cpu = cpu_baseline_headline(args, a_cm, b_cm, x64)
+        large = measure_large(handle, args) if args.large else None
         by_kappa = {}
         for k, kappa in enumerate(KAPPAS):
             idx = list(range(k, COUNT, len(KAPPAS)))
             by_kappa[f"{kappa:.0e}"] = {
                 "mixed_berr_max": float(mixed_berr[idx].max()),
                 "plain_berr_max": float(plain_berr[idx].max()),
+                "mixed_ferr_max": float(fe_mixed[idx].max()),
+                "plain_ferr_max": float(fe_plain[idx].max()),
                 "iterations_max": int(mixed_iters[idx].max()),
             }
         line = {
@@ -383,14 +478,16 @@ def run_b200(args, rank, world):
                 "berr_max": float(mixed_berr.max()),
                 "berr_reported_max": float(berr.max().item()),
                 "iterations_max": int(mixed_iters.max()),
-                "ferr_vs_fp64_max": max(fe_mixed),
+                "ferr_vs_fp64_max": float(fe_mixed.max()),
+                "ferr_systems": COUNT,
             },
             "plain": {
                 "solves_per_s": round(plain_value, 1),
                 "ms": round(plain_ms, 4),
                 "gflops": round(plain_value * SOLVE_FLOPS / 1e9, 1),
                 "berr_max": float(plain_berr.max()),
-                "ferr_vs_fp64_max": max(fe_plain),
+                "ferr_vs_fp64_max": float(fe_plain.max()),
+                "ferr_systems": COUNT,
             },
             "mixed_over_plain": round(value / plain_value, 3),
             "by_kappa": by_kappa,
@@ -421,16 +518,309 @@ def run_b200(args, rank, world):
             "clocks": clocks.summary(),
             "wall_s_timed": round(wall, 4),
             "cpu_baseline": cpu,
+            "configs": configs,
             "large": large,
         }
         print(json.dumps(line), flush=True)
     handle.close()
 
 
+# ---------------------------------------------------------------------------------------
+# The plain batched workloads (configs 1-3)
+# ---------------------------------------------------------------------------------------
+
+def measure_c1(handle, timer, args):
+    """10,000 SPD matrices of order 32, A = G G^T / 32 + I (G ~ N(0,1), seed 0), lower,
+    lda 32, one N(0,1) right-hand side: SpotrfBatched + SpotrsBatched."""
+    import numpy as np
+    import torch
+
+    import aclsolver
+    from oracle import host_lapack
+
+    lib, check = aclsolver.library(), aclsolver.check
+    count, n, nrhs = 10_000, 32, 1
+    rng = np.random.default_rng(0)
+    g = rng.standard_normal((count, n, n), dtype=np.float32)
+    a = (np.matmul(g, g.transpose(0, 2, 1)) / n + np.eye(n, dtype=np.float32)).astype(np.float32)
+    b = rng.standard_normal((count, n, nrhs), dtype=np.float32)
+    a_cm, b_cm = colmajor(a).reshape(-1), colmajor(b).reshape(-1)
+    A0 = torch.from_numpy(a_cm).cuda()
+    B0 = torch.from_numpy(b_cm).cuda()
+    A, B = torch.empty_like(A0), torch.empty_like(B0)
+    ta, tb = aclsolver.pointer_table(A, count, n * n * 4), aclsolver.pointer_table(B, count, n * nrhs * 4)
+    info = torch.empty(count, dtype=torch.int32, device="cuda")
+    sinfo = torch.empty(1, dtype=torch.int32, device="cuda")
+    h = handle.value
+
+    def potrf():
+        check(lib.aclsolverSpotrfBatched(h, 0, n, ta.data_ptr(), n, info.data_ptr(), count))
+
+    def potrs():
+        check(lib.aclsolverSpotrsBatched(h, 0, n, nrhs, ta.data_ptr(), n, tb.data_ptr(), n, sinfo.data_ptr(), count))
+
+    def both():
+        potrf()
+        potrs()
+
+    def restore():
+        A.copy_(A0)
+        B.copy_(B0)
+
+    steps = max(5, args.steps)
+    for _ in range(3):
+        timer(both, 1, restore)
+    ms = timer(both, steps, restore)
+    assert int(info.abs().max()) == 0 and int(sinfo.item()) == 0
+    x = B.cpu().numpy().reshape(count, nrhs, n).transpose(0, 2, 1)
+    ms_f = timer(potrf, steps, restore)
+    ms_s = timer(potrs, steps, lambda: B.copy_(B0))
+    # accuracy: normwise backward error of every solution in FP64
+    r = b.astype(np.float64) - np.matmul(a.astype(np.float64), x.astype(np.float64))
+    be = np.abs(r).max(axis=(1, 2)) / (np.abs(a).sum(axis=2).max(axis=1) * np.abs(x).max(axis=(1, 2))
+                                       + np.abs(b).max(axis=(1, 2)))
+    tri = n * (n + 1) // 2 * 4
+    bytes_f, bytes_s = 2 * tri, tri + 2 * n * nrhs * 4
+    flops_f, flops_s = n**3 / 3, 2 * n * n * nrhs
+
+    cpu = None
+    if args.cpu_seconds > 0:
+        threads = host_lapack.max_threads()
+        cpu_s, reps = cpu_timed(lambda: host_lapack.potrf_potrs(n, nrhs, a_cm, b_cm, count, threads=threads),
+                                args.cpu_seconds)
+        _, xc, ci = host_lapack.potrf_potrs(n, nrhs, a_cm, b_cm, count, threads=threads)
+        xc = xc.reshape(count, nrhs, n).transpose(0, 2, 1)
+        rc = b.astype(np.float64) - np.matmul(a.astype(np.float64), xc.astype(np.float64))
+        bec = np.abs(rc).max(axis=(1, 2)) / (np.abs(a).sum(axis=2).max(axis=1) * np.abs(xc).max(axis=(1, 2))
+                                             + np.abs(b).max(axis=(1, 2)))
+        cpu = dict(host_lapack.describe(threads), value=round(count / cpu_s, 1), unit="solves/s", kind="openblas",
+                   berr_max=float(bec.max()), info_max=int(ci.max()),
+                   sample=f"all {count} matrices per pass (spotrf + spotrs, FP32 LAPACKE), {reps} passes")
+    return {
+        "workload": "10,000 SPD 32x32 (A = G G^T/32 + I), lower, lda 32, 1 RHS: SpotrfBatched + SpotrsBatched, fp32",
+        "value": round(count / (ms * 1e-3), 1), "unit": "solves/s", "ms": round(ms, 5),
+        "gflops": round(count * (flops_f + flops_s) / (ms * 1e-3) / 1e9, 1),
+        "berr_max": float(be.max()),
+        "roofline": roofline(count * (bytes_f + bytes_s), count * (flops_f + flops_s), ms,
+                             "potrf_small_kernel<32> + potrs_small_kernel<32>", "c1_potrf_potrs"),
+        "kernels": {
+            "potrf": roofline(count * bytes_f, count * flops_f, ms_f, "potrf_small_kernel<32>", "c1_potrf"),
+            "potrs": roofline(count * bytes_s, count * flops_s, ms_s, "potrs_small_kernel<32>", "c1_potrs"),
+        },
+        "l2": "inputs restored from a pristine copy, then a 256 MiB buffer written, before each step",
+        "cpu_baseline": cpu,
+    }
+
+
+def measure_c2(handle, timer, args):
+    """4,096 matrices of order 64 with N(0,1) entries (seed 1), one N(0,1) right-hand side:
+    SgetrfBatched + SgetrsBatched + SgetriBatched (inverse out of place)."""
+    import numpy as np
+    import torch
+
+    import aclsolver
+    from oracle import host_lapack
+
+    lib, check = aclsolver.library(), aclsolver.check
+    count, n, nrhs = 4096, 64, 1
+    rng = np.random.default_rng(1)
+    a = rng.standard_normal((count, n, n), dtype=np.float32)
+    b = rng.standard_normal((count, n, nrhs), dtype=np.float32)
+    a_cm, b_cm = colmajor(a).reshape(-1), colmajor(b).reshape(-1)
+    A0 = torch.from_numpy(a_cm).cuda()
+    B0 = torch.from_numpy(b_cm).cuda()
+    A, B, Cinv = torch.empty_like(A0), torch.empty_like(B0), torch.empty_like(A0)
+    ta, tb = aclsolver.pointer_table(A, count, n * n * 4), aclsolver.pointer_table(B, count, n * nrhs * 4)
+    tc = aclsolver.pointer_table(Cinv, count, n * n * 4)
+    piv = torch.empty(count * n, dtype=torch.int32, device="cuda")
+    info = torch.empty(count, dtype=torch.int32, device="cuda")
+    sinfo = torch.empty(1, dtype=torch.int32, device="cuda")
+    iinfo = torch.empty(count, dtype=torch.int32, device="cuda")
+    h = handle.value
+
+    def getrf():
+        check(lib.aclsolverSgetrfBatched(h, n, ta.data_ptr(), n, piv.data_ptr(), info.data_ptr(), count))
+
+    def getrs():
+        check(lib.aclsolverSgetrsBatched(h, 0, n, nrhs, ta.data_ptr(), n, piv.data_ptr(), tb.data_ptr(), n,
+                                         sinfo.data_ptr(), count))
+
+    def getri():
+        check(lib.aclsolverSgetriBatched(h, n, ta.data_ptr(), n, piv.data_ptr(), tc.data_ptr(), n, iinfo.data_ptr(),
+                                         count))
+
+    def all3():
+        getrf()
+        getrs()
+        getri()
+
+    def restore():
+        A.copy_(A0)
+        B.copy_(B0)
+
+    steps = max(5, args.steps)
+    for _ in range(3):
+        timer(all3, 1, restore)
+    ms = timer(all3, steps, restore)
+    assert int(info.abs().max()) == 0 and int(sinfo.item()) == 0 and int(iinfo.abs().max()) == 0
+    x = B.cpu().numpy().reshape(count, nrhs, n).transpose(0, 2, 1)
+    inv = Cinv.cpu().numpy().reshape(count, n, n).transpose(0, 2, 1)
+    gpu_piv = piv.cpu().numpy().reshape(count, n)
+    ms_f = timer(getrf, steps, restore)
+    ms_s = timer(getrs, steps, lambda: B.copy_(B0))
+    ms_i = timer(getri, steps)
+    a64 = a.astype(np.float64)
+    r = b.astype(np.float64) - np.matmul(a64, x.astype(np.float64))
+    anorm = np.abs(a64).sum(axis=2).max(axis=1)
+    be = np.abs(r).max(axis=(1, 2)) / (anorm * np.abs(x).max(axis=(1, 2)) + np.abs(b).max(axis=(1, 2)))
+    # inverse: ||A X - I||_inf / (||A||_inf ||X||_inf) per matrix
+    ri = np.matmul(a64, inv.astype(np.float64)) - np.eye(n)
+    be_inv = np.abs(ri).sum(axis=2).max(axis=1) / (anorm * np.abs(inv).sum(axis=2).max(axis=1))
+
+    mat, piv_b, vec = n * n * 4, n * 4, n * nrhs * 4
+    bytes_f, bytes_s, bytes_i = 2 * mat + piv_b, mat + piv_b + 2 * vec, 2 * mat + piv_b
+    flops_f, flops_s, flops_i = 2 * n**3 / 3, 2 * n * n * nrhs, 4 * n**3 / 3
+    total_b, total_f = count * (bytes_f + bytes_s + bytes_i), count * (flops_f + flops_s + flops_i)
+
+    cpu, cpiv = None, None
+    if args.cpu_seconds > 0:
+        threads = host_lapack.max_threads()
+        cpu_s, reps = cpu_timed(lambda: host_lapack.getrf_getrs(n, nrhs, a_cm, b_cm, count, inverse=True,
+                                                               threads=threads), args.cpu_seconds)
+        _, _, _, cpiv, ci = host_lapack.getrf_getrs(n, nrhs, a_cm, b_cm, count, inverse=True, threads=threads)
+        cpu = dict(host_lapack.describe(threads), value=round(count / cpu_s, 1),
+                   unit="matrices/s (factor + solve + inverse)", kind="openblas", info_max=int(ci.max()),
+                   sample=f"all {count} matrices per pass (sgetrf + sgetrs + sgetri, FP32 LAPACKE), {reps} passes")
+    return {
+        "workload": "4,096 N(0,1) 64x64, 1 RHS: SgetrfBatched + SgetrsBatched + SgetriBatched, fp32",
+        "value": round(count / (ms * 1e-3), 1), "unit": "matrices/s (factor + solve + inverse)",
+        "ms": round(ms, 5), "gflops": round(total_f / (ms * 1e-3) / 1e9, 1),
+        "berr_max": float(be.max()), "inverse_residual_max": float(be_inv.max()),
+        "ipiv_equal_openblas": None if cpiv is None else bool(np.array_equal(gpu_piv, cpiv.reshape(count, n))),
+        "roofline": roofline(total_b, total_f, ms, "getrf_small_kernel<64> + getrs_small + getri_small_kernel<64>",
+                             "c2_all"),
+        "kernels": {
+            "getrf": roofline(count * bytes_f, count * flops_f, ms_f, "getrf_small_kernel<64>", "c2_getrf"),
+            "getrs": roofline(count * bytes_s, count * flops_s, ms_s, "getrs_small_kernel<64>", "c2_getrs"),
+            "getri": roofline(count * bytes_i, count * flops_i, ms_i, "getri_small_kernel<64>", "c2_getri"),
+        },
+        "l2": "inputs restored from a pristine copy, then a 256 MiB buffer written, before each step",
+        "cpu_baseline": cpu,
+    }
+
+
+def make_c3_inputs(count=20_000, nrhs=4, seed=2):
+    """Orders n_q ~ U{8..128}; A_q = G G^H / n + I with G's real and imaginary parts N(0,1);
+    4 right-hand sides CN(0,1).  Returns flat column-major complex64 slabs (as float32) with
+    per-matrix float offsets, lda = ldb = n."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    orders = rng.integers(8, 129, size=count).astype(np.int32)
+    a_off = np.zeros(count, dtype=np.int64)
+    b_off = np.zeros(count, dtype=np.int64)
+    a_off[1:] = np.cumsum(2 * orders.astype(np.int64) ** 2)[:-1]
+    b_off[1:] = np.cumsum(2 * orders.astype(np.int64) * nrhs)[:-1]
+    a = np.empty(int(2 * (orders.astype(np.int64) ** 2).sum()), dtype=np.float32)
+    b = rng.standard_normal(int(2 * orders.sum() * nrhs), dtype=np.float32) * np.float32(np.sqrt(0.5))
+    for n in np.unique(orders):
+        idx = np.nonzero(orders == n)[0]
+        g = (rng.standard_normal((len(idx), n, n), dtype=np.float32)
+             + 1j * rng.standard_normal((len(idx), n, n), dtype=np.float32)).astype(np.complex64)
+        m = (np.matmul(g, np.conj(g.transpose(0, 2, 1))) / np.float32(n) + np.eye(n, dtype=np.complex64))
+        m = m.astype(np.complex64)
+        for k, q in enumerate(idx):
+            # column-major: the transpose in C order, interleaved re/im
+            a[a_off[q]:a_off[q] + 2 * n * n] = np.ascontiguousarray(m[k].T).view(np.float32).reshape(-1)
+    return orders, a_off, b_off, a, b
+
+
+def measure_c3(handle, timer, args):
+    """20,000 HPD complex64 matrices of orders U{8..128}, 4 right-hand sides, one
+    aclsolverCposvVbatched call (the persistent, size-bucketed, graph-captured launch)."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    import aclsolver
+    from oracle import host_lapack
+
+    lib, check = aclsolver.library(), aclsolver.check
+    count, nrhs = 20_000, 4
+    orders, a_off, b_off, a, b = make_c3_inputs(count, nrhs)
+    A0 = torch.from_numpy(a).cuda()
+    B0 = torch.from_numpy(b).cuda()
+    A, B = torch.empty_like(A0), torch.empty_like(B0)
+    ta = torch.from_numpy(a_off * 4).cuda() + A.data_ptr()
+    tb = torch.from_numpy(b_off * 4).cuda() + B.data_ptr()
+    info = torch.empty(count, dtype=torch.int32, device="cuda")
+    ld = np.ascontiguousarray(orders, dtype=np.int32)
+    plan = C.c_void_p()
+    t0 = time.perf_counter()
+    check(lib.aclsolverCposvVbatchedPlanCreate(handle.value, 0, ld.ctypes.data, ld.ctypes.data, ld.ctypes.data, nrhs,
+                                               count, 1, C.byref(plan)))
+    plan_s = time.perf_counter() - t0
+
+    def solve():
+        check(lib.aclsolverCposvVbatched(handle.value, plan, ta.data_ptr(), tb.data_ptr(), info.data_ptr()))
+
+    def restore():
+        A.copy_(A0)
+        B.copy_(B0)
+
+    steps = max(5, args.steps // 2)
+    for _ in range(3):
+        timer(solve, 1, restore)
+    ms = timer(solve, steps, restore)
+    assert int(info.abs().max()) == 0
+    xs = B.cpu().numpy()
+    lib.aclsolverVbatchedPlanDestroy(plan)
+    # backward error against FP64 on every 20th matrix
+    be = []
+    for q in range(0, count, 20):
+        n = int(orders[q])
+        m = a[a_off[q]:a_off[q] + 2 * n * n].view(np.complex64).reshape(n, n).T.astype(np.complex128)
+        bq = b[b_off[q]:b_off[q] + 2 * n * nrhs].view(np.complex64).reshape(nrhs, n).T.astype(np.complex128)
+        xq = xs[b_off[q]:b_off[q] + 2 * n * nrhs].view(np.complex64).reshape(nrhs, n).T.astype(np.complex128)
+        r = bq - m @ xq
+        be.append(np.abs(r).max() / (np.abs(m).sum(axis=1).max() * np.abs(xq).max() + np.abs(bq).max()))
+    n64 = orders.astype(np.float64)
+    tri = n64 * (n64 + 1) / 2 * 8
+    total_b = float((3 * tri + 2 * n64 * nrhs * 8).sum())
+    total_f = float((4 * n64**3 / 3 + 8 * n64**2 * nrhs).sum())
+
+    cpu = None
+    if args.cpu_seconds > 0:
+        threads = host_lapack.max_threads()
+        cpu_s, reps = cpu_timed(lambda: host_lapack.cpotrf_cpotrs_vbatched(orders, a_off, b_off, a, b, nrhs,
+                                                                          threads=threads), args.cpu_seconds)
+        _, _, ci = host_lapack.cpotrf_cpotrs_vbatched(orders, a_off, b_off, a, b, nrhs, threads=threads)
+        cpu = dict(host_lapack.describe(threads), value=round(count / cpu_s, 1), unit="solves/s (4 RHS each)",
+                   kind="openblas", info_max=int(ci.max()),
+                   sample=f"all {count} matrices per pass (cpotrf + cpotrs, complex64 LAPACKE, dynamic chunks of "
+                          f"4 matrices), {reps} passes")
+    return {
+        "workload": "20,000 HPD complex64, n ~ U{8..128}, A = G G^H/n + I, 4 RHS: one CposvVbatched call "
+                    "(persistent, size-bucketed, graph-captured, autotuned)",
+        "value": round(count / (ms * 1e-3), 1), "unit": "solves/s (4 RHS each)", "ms": round(ms, 5),
+        "gflops": round(total_f / (ms * 1e-3) / 1e9, 1), "berr_max_sampled": float(max(be)),
+        "berr_sample": f"every 20th matrix ({len(be)}), FP64",
+        "plan_create_s": round(plan_s, 3),
+        "roofline": roofline(total_b, total_f, ms, "vb_warp_kernel + vb_block_kernel (one graph)", "c3_vbatched"),
+        "l2": "inputs (0.93 GB) restored from a pristine copy, then a 256 MiB buffer written, before each step",
+        "cpu_baseline": cpu,
+    }
+
+
+# ---------------------------------------------------------------------------------------
+# The single large system (config 5)
+# ---------------------------------------------------------------------------------------
+
 LARGE_N, LARGE_NRHS, LARGE_KAPPA = 8192, 16, 1e3
 
 
-def measure_large(handle, steps=3):
+def measure_large(handle, args, steps=3):
     """The single large system beside the batched headline: one 8192 x 8192 A = U diag(s) V^T
     (Haar U, V from an FP64 QR on the GPU, kappa 1e3), 16 N(0,1) right-hand sides.  Plain:
     aclsolverSgetrf + aclsolverSgetrsBatched (FP32, the oracle's order) on device-resident
@@ -496,19 +886,19 @@ def measure_large(handle, steps=3):
     x64 = torch.linalg.solve(a64, b64)
     anorm = a64.abs().sum(dim=1).max()
 
-    def errors():
-        x = xt.T.double()
+    def errors(x):
+        x = x.double()
         r = b64 - a64 @ x
         be = r.abs().amax(dim=0) / (anorm * x.abs().amax(dim=0) + b64.abs().amax(dim=0))
         fe = (x - x64).abs().amax(dim=0) / x64.abs().amax(dim=0)
         return float(be.max()), float(fe.max())
 
     plain_ms = timed(plain, True)
-    plain_be, plain_fe = errors()
+    plain_be, plain_fe = errors(xt.T)
     mixed_ms = timed(mixed, False)
-    mixed_be, mixed_fe = errors()
+    mixed_be, mixed_fe = errors(xt.T)
     flops = 2.0 * n ** 3 / 3 + 2.0 * n * n * nrhs
-    return {
+    out = {
         "workload": f"one {n} x {n} system, A = U diag(s) V^T, kappa {LARGE_KAPPA:.0e}, {nrhs} right-hand sides",
         "plain": {"path": "Sgetrf + SgetrsBatched (FP32)", "ms": round(plain_ms, 3),
                   "gflops": round(flops / (plain_ms * 1e-3) / 1e9, 1), "berr_max": plain_be, "ferr_max": plain_fe},
@@ -517,66 +907,79 @@ def measure_large(handle, steps=3):
                   "iterations": int(iters.item()), "berr_reported": float(berr.item())},
         "mixed_over_plain": round(plain_ms / mixed_ms, 3),
     }
+    if args is not None and args.cpu_seconds > 0:
+        from oracle import host_lapack
+
+        threads = host_lapack.max_threads()
+        a_h = at.cpu().numpy().reshape(-1)
+        b_h = bt.cpu().numpy().reshape(-1)
+        t0 = time.perf_counter()
+        xc, st = host_lapack.sgesv(n, nrhs, a_h, b_h, threads=threads)
+        dt = time.perf_counter() - t0
+        be, fe = errors(torch.from_numpy(xc.reshape(nrhs, n)).cuda().T)
+        out["cpu_baseline"] = dict(host_lapack.describe(threads), value=round(1.0 / dt, 3), unit="solves/s",
+                                   ms=round(dt * 1e3, 1), kind="openblas", berr_max=be, ferr_max=fe, info=int(st),
+                                   sample=f"one sgetrf + sgetrs ({nrhs} RHS, FP32 LAPACKE), OpenBLAS on {threads} threads")
+    return out
 
 
-def cpu_sample(count):
-    """A bounded sample of the workload for the host: the first `count` matrices."""
-    a, b = make_inputs(1, count=count)
-    return a, b
+# ---------------------------------------------------------------------------------------
+# CPU baselines
+# ---------------------------------------------------------------------------------------
 
+def cpu_baseline_headline(args, a_cm, b_cm, x64):
+    """The host LAPACK (OpenBLAS FP32 sgetrf + sgetrs) over all 256 systems of the headline
+    workload, OpenMP over matrices, with the backward and forward errors of its solutions."""
+    import numpy as np
 
-def cpu_baseline(args):
-    """The oracle (the reference's plain FP32 LU + solve, restated) on this host's cores."""
-    import oracle
+    from oracle import host_lapack
 
-    count = 24
-    a, b = cpu_sample(count)
-    threads = oracle.max_threads()
-    reps, t0 = 0, time.perf_counter()
-    while True:
-        lu, ipiv, info = oracle.sgetrf_batched(a, threads=threads)
-        oracle.sgetrs_batched(lu, ipiv, b, threads=threads)
-        reps += 1
-        if time.perf_counter() - t0 > args.cpu_seconds or reps >= 100:
-            break
-    dt = time.perf_counter() - t0
-    return {
-        "value": round(reps * count / dt, 2),
-        "unit": UNIT,
-        "cores": threads,
-        "kind": "port",
-        "sample": f"{reps} passes over {count} of the {COUNT} 512x512 systems (sgetrf + sgetrs, FP32), {dt:.1f} s",
-    }
+    threads = host_lapack.max_threads()
+    a_flat, b_flat = a_cm.reshape(-1), b_cm.reshape(-1)
+    per_pass, reps = cpu_timed(lambda: host_lapack.getrf_getrs(N, NRHS, a_flat, b_flat, COUNT, threads=threads),
+                               args.cpu_seconds)
+    _, x, _, _, info = host_lapack.getrf_getrs(N, NRHS, a_flat, b_flat, COUNT, threads=threads)
+    x = x.reshape(COUNT, NRHS, N).transpose(0, 2, 1)
+    a = a_cm.transpose(0, 2, 1).astype(np.float64)
+    b = b_cm.transpose(0, 2, 1).astype(np.float64)
+    r = b - np.matmul(a, x.astype(np.float64))
+    be = np.abs(r).max(axis=(1, 2)) / (np.abs(a).sum(axis=2).max(axis=1) * np.abs(x).max(axis=(1, 2))
+                                       + np.abs(b).max(axis=(1, 2)))
+    return dict(host_lapack.describe(threads), value=round(COUNT / per_pass, 2), unit=UNIT, kind="openblas",
+                berr_max=float(be.max()), ferr_vs_fp64_max=float(forward_errors(x64, x).max()),
+                info_max=int(info.max()),
+                sample=f"all {COUNT} 512x512 systems per pass (sgetrf + sgetrs, FP32 LAPACKE, OpenMP over "
+                       f"matrices, one OpenBLAS thread each), {reps} passes")
 
 
 def run_reference(args, rank, world):
-    import oracle
+    """The reference's CPU path for this workload: the host FP32 LAPACK its tests use as the
+    golden (OpenBLAS), over the same 256 systems, the same step count."""
+    from oracle import host_lapack
 
     if rank != 0:
         return
-    count = 24
-    a, b = cpu_sample(count)
-    threads = oracle.max_threads()
+    a, b = make_inputs(1)
+    a_flat, b_flat = colmajor(a).reshape(-1), colmajor(b).reshape(-1)
+    threads = host_lapack.max_threads()
 
     def step():
-        lu, ipiv, info = oracle.sgetrf_batched(a, threads=threads)
-        oracle.sgetrs_batched(lu, ipiv, b, threads=threads)
+        host_lapack.getrf_getrs(N, NRHS, a_flat, b_flat, COUNT, threads=threads)
 
-    for _ in range(min(args.warmup, 2)):
+    for _ in range(args.warmup):
         step()
     t0 = time.perf_counter()
-    steps = min(args.steps, 10)
-    for _ in range(steps):
+    for _ in range(args.steps):
         step()
-    dt = (time.perf_counter() - t0) / max(1, steps)
-    value = count / dt
+    dt = (time.perf_counter() - t0) / max(1, args.steps)
+    value = COUNT / dt
     line = {
         "impl": "reference",
         "metric": METRIC,
         "value": round(value, 2),
         "unit": UNIT,
         "n_gpus": world,
-        "steps": steps,
+        "steps": args.steps,
         "warmup": args.warmup,
         "ms_per_step": round(dt * 1e3, 3),
         "higher_is_better": True,
@@ -584,18 +987,19 @@ def run_reference(args, rank, world):
         "vs_baseline": None,
         "dtype": "fp32",
         "data": "synthetic: seeded U diag(s) V^T matrices and N(0,1) right-hand sides",
-        "config": {"workload": WORKLOAD, "batch_per_gpu": COUNT, "n": N, "nrhs": NRHS, "kappa": list(KAPPAS)},
-        "cpu_baseline": {
-            "value": round(value, 2),
-            "unit": UNIT,
-            "cores": threads,
-            "kind": "port",
-            "sample": f"each step {count} of the {COUNT} 512x512 systems on the host (OpenMP over matrices)",
-        },
+        "config": {"workload": WORKLOAD, "batch_per_gpu": COUNT, "n": N, "nrhs": NRHS, "kappa": list(KAPPAS),
+                   "parallelism": f"replicas x{world}"},
+        "cpu_baseline": dict(host_lapack.describe(threads), value=round(value, 2), unit=UNIT, kind="openblas",
+                             sample=f"each step all {COUNT} 512x512 systems (sgetrf + sgetrs, FP32 LAPACKE, "
+                                    "OpenMP over matrices, one OpenBLAS thread each)"),
         "e2e": {"value": round(value, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
+
+# ---------------------------------------------------------------------------------------
+# Profiling entry points (one launch of each hot kernel, for ncu)
+# ---------------------------------------------------------------------------------------
 
 def run_profile():
     """One launch of each hot kernel on the benchmark's inputs, for an ncu capture: the FP32
@@ -632,13 +1036,33 @@ def run_profile():
     handle.close()
 
 
+def run_profile_small(args):
+    """The plain batched workloads (configs 1-3) once each at full size, for an ncu launch
+    list (`gpu__time_duration.sum` only), no CPU baselines."""
+    import torch
+
+    import aclsolver
+
+    handle = aclsolver.Handle()
+    aclsolver.check(aclsolver.library().aclsolverSetDeviceChecks(handle.value, 0))
+    timer = DeviceTimer(handle.stream, torch.device("cuda"))
+    args.cpu_seconds = 0.0
+    args.steps = 1
+    out = {}
+    for key, fn in (("c1", measure_c1), ("c2", measure_c2), ("c3", measure_c3)):
+        if key in args.profile_small:
+            out[key] = fn(handle, timer, args)["ms"]
+    print(json.dumps({"profile": "ok", "ms": out}))
+    handle.close()
+
+
 def run_profile_large():
     """The single large system for an ncu launch list: one plain factorisation and solve and
     one split-BF16 refinement call (the measurement of the 'large' key, one repetition)."""
     import aclsolver
 
     handle = aclsolver.Handle()
-    out = measure_large(handle, steps=0)
+    out = measure_large(handle, None, steps=0)
     print(json.dumps({"profile": "ok", "large": out}))
     handle.close()
 
@@ -667,13 +1091,17 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--cpu-seconds", type=float, default=3.0)
     ap.add_argument("--no-large", dest="large", action="store_false",
                     help="skip the single 8192 x 8192 system reported under the 'large' key")
+    ap.add_argument("--no-configs", dest="configs", action="store_false",
+                    help="skip the plain batched workloads reported under the 'configs' key")
     ap.add_argument("--profile-large", action="store_true",
                     help="one large plain factorisation + solve and one large refinement call, for ncu")
     ap.add_argument("--profile", action="store_true",
                     help="run each hot kernel once on the workload (for an ncu capture) and exit")
+    ap.add_argument("--profile-small", default="",
+                    help="comma list of c1,c2,c3: run those plain batched workloads once (for ncu) and exit")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -689,6 +1117,8 @@ def main():
     try:
         if args.profile:
             run_profile()
+        elif args.profile_small:
+            run_profile_small(args)
         elif args.profile_large:
             run_profile_large()
         elif args.impl == "reference":

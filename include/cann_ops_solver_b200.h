@@ -4,7 +4,8 @@
  * None of these names exists in the reference; the existing entry points of
  * cann_ops_solver.h keep their reference contracts unchanged.  Each addition states the
  * reference call sequence it stands in for.  All of them are asynchronous on the handle
- * stream (no host synchronisation inside), so they can be captured in a CUDA graph.
+ * stream (no host synchronisation inside), so they can be captured in a CUDA graph, except
+ * where an entry's comment says otherwise (aclsolverSgesvIrBatched above order 512).
  */
 #pragma once
 #include <stddef.h>
@@ -47,7 +48,8 @@ extern "C"
      * column-major buffers (the reference aclsolverSgetrs, include/cann_ops_solver.h:1011, is
      * host-buffer, row-major and synchronous).  trans: ACLSOLVER_OP_N or ACLSOLVER_OP_T.
      * PivotArray n per matrix (NULL = no pivoting).  infoArray[b] = 0, or -i argument error,
-     * or -6 when matrix b's pivot k lies outside [k+1, n] (that slot is left unsolved).  0 <= n <= 4096, 0 <= nrhs. */
+     * or -6 when matrix b's pivot k lies outside [k+1, n] (that slot is left unsolved).
+     * 0 <= n <= 8192, 0 <= nrhs (both trans codes at every order). */
     aclsolverStatus_t aclsolverSgetrsBatched(aclsolverHandle_t handle, aclsolverOperation_t trans, int n, int nrhs,
                                              const float *const Aarray[], int lda, const int *PivotArray,
                                              float *const Barray[], int ldb, int *infoArray, int batchSize);
@@ -101,8 +103,11 @@ extern "C"
      * arguments, arithmetic, info and argument-error rules as aclsolverSmatinvBatched, except
      * that the synchronous device-data checks (finite scan, pointer-table validation) are not
      * run, since they need staging buffers.  The first call on each device resolves the
-     * array's device address and should come before any stream capture.  All calls share the
-     * array: calls whose executions overlap on the GPU race on it and must be serialised. */
+     * array's device address and should come before any stream capture; so should the first
+     * call after the device's context was reset (cudaDeviceReset or a released primary
+     * context), which resolves it again.  The current device must be the handle's device
+     * (EXECUTION_FAILED otherwise).  All calls share the array: calls whose executions
+     * overlap on the GPU race on it and must be serialised. */
     aclsolverStatus_t aclsolverSmatinvBatchedNoAlloc(aclsolverHandle_t handle, int n, const float *const A[], int lda,
                                                      float *const Ainv[], int lda_inv, int *info, int batchSize);
 
@@ -129,9 +134,12 @@ extern "C"
      * (maximum over its right-hand sides; NaN when the factorisation failed).
      * infoArray (device): the factorisation's info (first zero U(k,k), -2 for a null slot); a
      * matrix with info != 0 is not solved and its X is left unchanged.
-     * 0 <= n <= 512, 0 <= nrhs, 0 <= maxIter, tol >= 0.  Argument errors: INVALID_VALUE,
-     * infoArray filled with -i (precision is argument 1).  Asynchronous on the handle stream;
-     * workspace comes from the handle (about 4 n^2 + 12 n nrhs bytes per matrix). */
+     * 0 <= n <= 8192, 0 <= nrhs, 0 <= maxIter, tol >= 0.  Up to n = 512 the batch is refined
+     * together, asynchronously on the handle stream, with workspace from the handle (about
+     * 4 n^2 + 12 n nrhs bytes per matrix).  Above 512 the systems are refined one after another
+     * over the whole GPU, each with at most 16 right-hand sides (NOT_SUPPORTED beyond), and the
+     * call reads one status word back per correction (it returns after its work).  Argument
+     * errors: INVALID_VALUE, infoArray filled with -i (precision is argument 1). */
     aclsolverStatus_t aclsolverSgesvIrBatched(aclsolverHandle_t handle, aclsolverFactorPrecision_t precision, int n,
                                               int nrhs, const float *const Aarray[], int lda,
                                               const float *const Barray[], int ldb, float *const Xarray[], int ldx,

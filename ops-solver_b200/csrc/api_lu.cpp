@@ -543,9 +543,8 @@ extern "C"
             aclsolverStatus_t fin = finish_scratch(h, blk);
             return launched != ACLSOLVER_STATUS_SUCCESS ? launched : fin;
         }
-        if (trans == ACLSOLVER_OP_N)
-            return launch_status(launch_getrs_blocked(a, PivotArray, nullptr, b, nrhs, infoArray, nullptr, h->stream));
-        return ACLSOLVER_STATUS_NOT_SUPPORTED;
+        return launch_status(launch_getrs_blocked(a, PivotArray, nullptr, b, nrhs, infoArray, nullptr, h->stream,
+                                                  nullptr, nullptr, trans == ACLSOLVER_OP_T ? 1 : 0));
     }
 
     aclError aclsolverSgetrs(aclsolverHandle_t handle, const uint64_t trans, const int64_t n, const int64_t nrhs,
@@ -569,7 +568,6 @@ extern "C"
                 return ACL_ERROR_INVALID_PARAM;
             }
         cudaStream_t stream = handle ? to_handle(handle)->stream : nullptr;
-        if (n > SMALL_N && trans != 0) return (aclError)ACLSOLVER_STATUS_NOT_SUPPORTED;
         // Stage: row-major host A (lda) -> device raw -> column-major LU (n x n, ld n);
         // row-major host B (ldb) -> device raw -> column-major (n x nrhs, ld n).
         const size_t a_raw = (size_t)n * lda * sizeof(float), b_raw = (size_t)n * ldb * sizeof(float);
@@ -605,7 +603,8 @@ extern "C"
             RealBatch a{d_a, nullptr, (int)n, (int)n, 0, 1};
             RealBatch b{d_b, nullptr, (int)n, (int)n, 0, 1};
             e = n <= SMALL_N ? launch_getrs_small(a, d_p, b, (int)nrhs, (int)trans, nullptr, stream)
-                             : launch_getrs_blocked(a, d_p, nullptr, b, (int)nrhs, nullptr, nullptr, stream);
+                             : launch_getrs_blocked(a, d_p, nullptr, b, (int)nrhs, nullptr, nullptr, stream, nullptr,
+                                                    nullptr, (int)trans);
         }
         if (e == cudaSuccess) e = launch_transpose(d_b, (int)n, d_braw, (int)ldb, (int)n, (int)nrhs, stream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(B, d_braw, b_raw, cudaMemcpyDeviceToHost, stream);

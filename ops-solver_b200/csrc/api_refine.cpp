@@ -161,9 +161,15 @@ extern "C" aclsolverStatus_t aclsolverSgesvIrBatched(aclsolverHandle_t handle, a
     if (n > BLOCKED_MAX_N)
     {
         // one system at a time over the whole GPU, at most 16 right-hand sides
-        if (batchSize != 1 || nrhs > LARGE_SOLVE_MAX_RHS) return ACLSOLVER_STATUS_NOT_SUPPORTED;
-        return gesv_ir_large(h, mode, n, nrhs, Aarray, lda, Barray, ldb, Xarray, ldx, maxIter, tol, iterArray,
-                             berrArray, infoArray);
+        if (nrhs > LARGE_SOLVE_MAX_RHS) return ACLSOLVER_STATUS_NOT_SUPPORTED;
+        for (int q = 0; q < batchSize; ++q)
+        {
+            aclsolverStatus_t r = gesv_ir_large(h, mode, n, nrhs, Aarray + q, lda, Barray + q, ldb, Xarray + q, ldx,
+                                                maxIter, tol, iterArray ? iterArray + q : nullptr,
+                                                berrArray ? berrArray + q : nullptr, infoArray + q);
+            if (r != ACLSOLVER_STATUS_SUCCESS) return r;
+        }
+        return ACLSOLVER_STATUS_SUCCESS;
     }
 
     // Workspace: LU copies, pivots and the panels' row changes, two pointer tables, FP64 solutions, FP32 staging,

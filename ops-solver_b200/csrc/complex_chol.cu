@@ -14,10 +14,13 @@
 // held to the 1e-5 relative tolerance and the reference's complex128 residual gate.
 //
 // Layouts: n <= 16 -- a width-N sub-warp per matrix, lane i holds row i (re[], im[]) and the
-// finished column is broadcast through shared memory; 17..128 -- one block per matrix,
-// the lower triangle staged in shared memory column-major, threads stride over the rows.
+// finished column is broadcast through shared memory; 17..128 -- one block per matrix, the
+// lower triangle packed in shared memory, a thread per row, factored left-looking in blocks
+// of 16 columns and solved in blocks of 16 rows (complex_block.cuh); above 128 -- one block
+// per matrix working in global memory.
 // (A 32-lane register version needs more than 255 registers per lane for the complex rows.)
 #include "common.cuh"
+#include "complex_block.cuh"
 #include "launch_complex.h"
 
 namespace ops_solver
@@ -225,6 +228,49 @@ __global__ void __launch_bounds__(T) cpotrf_block_kernel(float2 *single, float2 
     }
 }
 
+// 17..128: the packed-triangle block routine, a matrix per block (grid-stride).
+template <int T>
+__global__ void __launch_bounds__(T) cpotrf_cb_kernel(float2 *single, float2 *const *table, int n, int lda, int upper,
+                                                      int count, int *info)
+{
+    extern __shared__ __align__(16) float cb_mem[];
+    const CbShared s = cb_carve(cb_mem, n);
+    for (int64_t q = blockIdx.x; q < count; q += gridDim.x)
+    {
+        float2 *p = table ? slot(table, q) : single;
+        if (!p)
+        {
+            if (threadIdx.x == 0) info[q] = -3;
+            continue;
+        }
+        cb_load<T>(s, p, lda, upper, n);
+        __syncthreads();
+        const int failure = cb_factor<T>(s, n);
+        cb_store<T>(s, p, lda, upper, n, failure ? failure - 1 : n);
+        if (threadIdx.x == 0) info[q] = failure;
+        __syncthreads();
+    }
+}
+
+template <int T>
+__global__ void __launch_bounds__(T) cpotrs_cb_kernel(const float2 *a_single, const float2 *const *a_table,
+                                                      float2 *b_single, float2 *const *b_table, int n, int lda, int ldb,
+                                                      int nrhs, int upper, int count, const int *info)
+{
+    extern __shared__ __align__(16) float cb_mem[];
+    if (info && info[0] != 0) return;
+    const CbShared s = cb_carve(cb_mem, n);
+    for (int64_t q = blockIdx.x; q < count; q += gridDim.x)
+    {
+        const float2 *pa = a_table ? slot(a_table, q) : a_single;
+        float2 *pb = b_table ? slot(b_table, q) : b_single;
+        if (!pa || !pb) continue;
+        cb_load<T>(s, pa, lda, upper, n);
+        __syncthreads();
+        cb_solve<T>(s, n, pb, ldb, nrhs);
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 // n > 128: left-looking in global memory (same per-element order)
 // ---------------------------------------------------------------------------------------
@@ -368,12 +414,19 @@ cudaError_t launch_cpotrf(float2 *single, float2 *const *table, int n, int lda, 
     else if (n <= 16)
         cpotrf_warp_kernel<16><<<grid_of(count, 8, 148 * 64), CW_THREADS, 0, stream>>>(single, table, n, lda, upper,
                                                                                        count, info);
+    else if (n <= 64)
+    {
+        const size_t smem = cb_smem_bytes(n);
+        cudaFuncSetAttribute(cpotrf_cb_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cpotrf_cb_kernel<64><<<grid_of(count, 1, 148 * 16), 64, smem, stream>>>(single, table, n, lda, upper, count,
+                                                                                info);
+    }
     else if (n <= 128)
     {
-        size_t smem = (size_t)n * (n + 1) * sizeof(float2);
-        cudaFuncSetAttribute(cpotrf_block_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cpotrf_block_kernel<128><<<grid_of(count, 1, 148 * 8), 128, smem, stream>>>(single, table, n, lda, upper,
-                                                                                    count, info);
+        const size_t smem = cb_smem_bytes(n);
+        cudaFuncSetAttribute(cpotrf_cb_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cpotrf_cb_kernel<128><<<grid_of(count, 1, 148 * 8), 128, smem, stream>>>(single, table, n, lda, upper,
+                                                                                count, info);
     }
     else
     {
@@ -390,6 +443,23 @@ cudaError_t launch_cpotrs(const float2 *a_single, const float2 *const *a_table, 
                           float2 *const *b_table, int n, int lda, int ldb, int nrhs, int upper, int count,
                           const int *info, cudaStream_t stream)
 {
+    if (n > 16 && n <= 128)
+    {
+        const size_t smem = cb_smem_bytes(n);
+        if (n <= 64)
+        {
+            cudaFuncSetAttribute(cpotrs_cb_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cpotrs_cb_kernel<64><<<grid_of(count, 1, 148 * 16), 64, smem, stream>>>(
+                a_single, a_table, b_single, b_table, n, lda, ldb, nrhs, upper, count, info);
+        }
+        else
+        {
+            cudaFuncSetAttribute(cpotrs_cb_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cpotrs_cb_kernel<128><<<grid_of(count, 1, 148 * 8), 128, smem, stream>>>(
+                a_single, a_table, b_single, b_table, n, lda, ldb, nrhs, upper, count, info);
+        }
+        return cudaGetLastError();
+    }
     size_t staged = ((size_t)n * (n + 1) + n) * sizeof(float2);
     if (staged <= 200 * 1024)
     {

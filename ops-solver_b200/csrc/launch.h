@@ -163,7 +163,7 @@ cudaError_t launch_getri_blocked(const RealBatch &a, const int *ipiv, const Real
 size_t getri_blocked_scratch_bytes(int n, int count);
 cudaError_t launch_getrs_blocked(const RealBatch &a, const int *ipiv, const int *perm, const RealBatch &b, int nrhs,
                                  int *info, const int *skip, cudaStream_t stream, const float *dinv = nullptr,
-                                 const short *lists = nullptr);
+                                 const short *lists = nullptr, int trans = 0);
 // dinv[(q * nblk + b) * 2 + {0: L, 1: U}] = inverse of the 32 x 32 diagonal block b of the
 // factors of matrix q (column-major 32 x 32, nblk = ceil(n / 32)).
 cudaError_t launch_diag_inverses(const RealBatch &a, float *dinv, cudaStream_t stream);

@@ -24,6 +24,7 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "device_once.h"
 #include "launch.h"
 
 namespace cg = cooperative_groups;
@@ -871,11 +872,9 @@ cudaError_t panel_launch_cs(float *A, int lda, int m, int k0, int w, int *ipiv, 
 
 // The cluster size: 16 blocks (two panel rows per thread at 8192) when the device can place
 // such a cluster of this kernel, otherwise the portable 8.
-int panel_cluster_size()
+int query_cluster_size()
 {
-    static int cs = 0;
-    if (cs) return cs;
-    cs = 8;
+    int cs = 8;
     const void *fn = reinterpret_cast<const void *>(large_panel_kernel<true, 2, 16>);
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess &&
         cudaFuncSetAttribute(reinterpret_cast<const void *>(large_panel_kernel<false, 2, 16>),
@@ -900,6 +899,13 @@ int panel_cluster_size()
     }
     cudaGetLastError();  // a refused query leaves no error behind
     return cs;
+}
+
+// ... asked once per device (the non-portable size attribute is set per device).
+int panel_cluster_size()
+{
+    static std::atomic<int> cache[ONCE_MAX_DEVICES];
+    return value_per_device(cache, query_cluster_size);
 }
 
 template <bool EXACT>
@@ -970,17 +976,15 @@ cudaError_t launch_getrf_large(float *A, int m, int n, int lda, int *ipiv, int *
 {
     if (m > LARGE_MAX_ROWS || n > LARGE_MAX_COLS) return cudaErrorInvalidValue;
     const int kmin = std::min(m, n);
-    static bool attr = false;
-    cudaError_t e = cudaSuccess;
-    if (!attr)
-    {
-        e = cudaFuncSetAttribute(large_trsm_kernel<OB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)((OB * (OB + 4) + 64 * (OB + 4)) * sizeof(float)));
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(large_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    cudaError_t e = once_per_device(attr, [] {
+        cudaError_t r = cudaFuncSetAttribute(large_trsm_kernel<OB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)((OB * (OB + 4) + 64 * (OB + 4)) * sizeof(float)));
+        if (r == cudaSuccess)
+            r = cudaFuncSetAttribute(large_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM);
+        return r;
+    });
+    if (e != cudaSuccess) return e;
     static std::mutex enqueue;
     std::lock_guard<std::mutex> lock(enqueue);
     LookAhead *la = nullptr;

@@ -10,6 +10,7 @@
 // (forward) or descending k (backward, after the IEEE division by U(k,k)), which is the
 // oracle's sgetrs order bit for bit.
 #include "common.cuh"
+#include "device_once.h"
 #include "launch.h"
 
 namespace ops_solver
@@ -559,27 +560,23 @@ size_t large_solve_scratch_bytes(int n, int nrhs)
 cudaError_t launch_large_perm(const int *ipiv, int n, int *perm, int *bad, cudaStream_t stream)
 {
     if (n > LARGE_MAX_COLS) return cudaErrorInvalidValue;
-    static bool attr = false;
-    if (!attr)
-    {
-        cudaError_t e = cudaFuncSetAttribute(large_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PERM_SMEM);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    cudaError_t e = once_per_device(attr, [] {
+        return cudaFuncSetAttribute(large_perm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PERM_SMEM);
+    });
+    if (e != cudaSuccess) return e;
     large_perm_kernel<<<1, 1024, PERM_SMEM, stream>>>(ipiv, n, perm, bad);
     return cudaGetLastError();
 }
 
 cudaError_t launch_large_diag_inverses(const float *A, int lda, int n, float *inv, cudaStream_t stream)
 {
-    static bool attr = false;
+    static std::atomic<unsigned long long> attr{0};
     const size_t smem = 2 * (size_t)SB * SBP4 * sizeof(float);
-    if (!attr)
-    {
-        cudaError_t e = cudaFuncSetAttribute(large_diag_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    cudaError_t e = once_per_device(attr, [smem] {
+        return cudaFuncSetAttribute(large_diag_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    });
+    if (e != cudaSuccess) return e;
     large_diag_inverse<<<dim3((n + SB - 1) / SB, 2), SB, smem, stream>>>(A, lda, n, inv);
     return cudaGetLastError();
 }
@@ -594,16 +591,17 @@ cudaError_t launch_getrs_large(const float *A, const float *const *At, int lda, 
     float *Y = static_cast<float *>(scratch);
     int *perm = reinterpret_cast<int *>(Y + (size_t)n * nrhs);
     const size_t smem = (2 * SB * SBP4 + (size_t)LARGE_SOLVE_MAX_RHS * SB) * sizeof(float);
-    static bool attr = false;
-    if (!attr)
+    static std::atomic<unsigned long long> attr{0};
     {
-        cudaError_t e = cudaFuncSetAttribute(large_sweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(large_sweep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem);
+        cudaError_t e = once_per_device(attr, [smem] {
+            cudaError_t r = cudaFuncSetAttribute(large_sweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (r == cudaSuccess)
+                r = cudaFuncSetAttribute(large_sweep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+            return r;
+        });
         if (e != cudaSuccess) return e;
-        attr = true;
     }
     const int *use = perm_in;  // a permutation composed earlier (its *bad already set)
     if (!use && ipiv)
@@ -622,12 +620,10 @@ cudaError_t launch_getrs_large(const float *A, const float *const *At, int lda, 
     const int nb = (n + SB - 1) / SB;
     // each sweep as one cooperative launch where all its blocks can be resident, else a launch
     // per 128-row block
-    static int coop_ok = -1;
+    static std::atomic<int> coop_cache[ONCE_MAX_DEVICES];
     const size_t csmem = (3 * SB * SBP4 + 2 * (size_t)LARGE_SOLVE_MAX_RHS * SB) * sizeof(float);
-    if (coop_ok < 0)
-    {
-        int dev = 0, attr_coop = 0, per_sm = 0, sms = 0;
-        coop_ok = 0;
+    const int coop_ok = value_per_device(coop_cache, [csmem] {
+        int dev = 0, attr_coop = 0, per_sm = 0, sms = 0, ok = 0;
         if (cudaGetDevice(&dev) == cudaSuccess &&
             cudaDeviceGetAttribute(&attr_coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && attr_coop &&
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
@@ -636,16 +632,17 @@ cudaError_t launch_getrs_large(const float *A, const float *const *At, int lda, 
             cudaFuncSetAttribute(large_sweep_coop<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem) ==
                 cudaSuccess &&
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, large_sweep_coop<true>, ST, csmem) == cudaSuccess)
-            coop_ok = per_sm * sms;  // blocks that can be resident at once
+            ok = per_sm * sms;  // blocks that can be resident at once
         cudaGetLastError();
-    }
+        return ok;
+    });
     if (coop_ok >= nb)
     {
         int *flags = perm + n;  // two sweeps' flags, cleared for this solve
         cudaError_t e0 = cudaMemsetAsync(flags, 0, 2 * (size_t)nb * sizeof(int), stream);
         if (e0 != cudaSuccess) return e0;
-        static int epoch = 0;
-        const int ep = ++epoch > 0 ? epoch : (epoch = 1);
+        static std::atomic<int> epoch{0};
+        const int ep = (epoch.fetch_add(1) & 0x3fffffff) + 1;  // positive, differs from the cleared 0
         const float *a1 = A;
         const float *const *at = At;
         float *y = Y;

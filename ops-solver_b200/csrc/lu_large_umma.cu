@@ -13,6 +13,7 @@
 #include <cuda_bf16.h>
 
 #include "common.cuh"
+#include "device_once.h"
 #include "launch.h"
 
 namespace ops_solver
@@ -263,14 +264,11 @@ cudaError_t launch_umma_split(float *A, int lda, int m, int n, int K0, int kend,
 cudaError_t launch_umma_range(float *A, int lda, int m, int n, int kend, int bend, int c_begin, int c_end, int terms,
                               LargeStatus *st, void *scratch, cudaStream_t stream)
 {
-    static bool attr = false;
-    if (!attr)
-    {
-        cudaError_t e =
-            cudaFuncSetAttribute(umma_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UMMA_SMEM);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    cudaError_t ea = once_per_device(attr, [] {
+        return cudaFuncSetAttribute(umma_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UMMA_SMEM);
+    });
+    if (ea != cudaSuccess) return ea;
     const int rows = m - kend, cols = c_end - c_begin;
     if (rows <= 0 || cols <= 0) return cudaSuccess;
     const UmmaHalves h = halves(scratch, m, n);

@@ -1,12 +1,16 @@
 // lu_solve.cu -- LU solve P A X = B for orders above the register-resident kernels
 // (64 < n <= 8192), one 256-thread block per (matrix, group of up to 8 right-hand sides).
 //
-// Order (the oracle's orc_sgetrs, trans 0): row interchanges applied in sequence, then the
+// Order (the oracle's orc_sgetrs).  trans 0: row interchanges applied in sequence, then the
 // unit-lower forward sweep x_i = fma(-l_ik, x_k, x_i) in ascending k, then the upper sweep
-// x_k = x_k / u_kk, x_i = fma(-u_ik, x_k, x_i) in descending k.  Blocking keeps every
-// element's sequence: columns go in blocks of 32 (the last one ragged); the 32 x 32 diagonal
-// triangle is solved by one warp per right-hand side with shuffles, then every other row
-// takes its block's 32 updates in order.
+// x_k = x_k / u_kk, x_i = fma(-u_ik, x_k, x_i) in descending k.  trans 1 (A^T x = b): the
+// forward sweep with U^T, x_k = x_k / u_kk, x_i = fma(-u_ki, x_k, x_i) in ascending k, the
+// backward sweep with L^T, x_i = fma(-l_ki, x_k, x_i) in descending k, then the interchanges
+// in reverse.  Blocking keeps every element's sequence: columns go in blocks of 32 (the last
+// one ragged); the 32 x 32 diagonal triangle is solved by one warp per right-hand side with
+// shuffles, then every other row takes its block's 32 updates in order.  Transposed strips
+// are 32 rows of the factor (32 contiguous floats per column), staged row-major at a pitch of
+// 36 floats so a thread's four-wide reads of its own row are free of bank conflicts.
 //
 // The solution vectors stay in shared memory.  The factor is streamed from global memory
 // once, as a queue of tiles (a block's 32 x 32 diagonal triangle, then its 32-column strips
@@ -29,6 +33,9 @@ static_assert(2 * ST >= 2 * KB * MAX_RHS_PER_BLOCK, "a panel's moves for all rig
 constexpr int SR = 256;      // rows of a strip
 constexpr int SP = SR + 4;   // stage pitch (floats)
 constexpr int STAGES = 3;    // tiles in flight: the one in use and two being copied
+constexpr int SRT = 224;     // rows (factor columns) of a transposed strip
+constexpr int TP = KB + 4;   // transposed stage pitch (floats)
+static_assert(SRT * TP <= KB * SP, "a transposed strip fits a stage");
 
 // One unit of the sweep: the diagonal triangle of block `blk` (strip < 0) or a strip of up
 // to 256 rows off the diagonal block (below it going forward, above it going backward).
@@ -38,20 +45,26 @@ struct Task
     int strip;
 };
 
-template <bool FORWARD>
+template <bool TRANS>
+__device__ __forceinline__ constexpr int strip_rows()
+{
+    return TRANS ? SRT : SR;
+}
+
+template <bool FORWARD, bool TRANS>
 __device__ __forceinline__ int strips(int n, int blk)
 {
     const int kb = blk * KB;
     const int w = min(KB, n - kb);
     const int rows = FORWARD ? n - kb - w : kb;
-    return (rows + SR - 1) / SR;
+    return (rows + strip_rows<TRANS>() - 1) / strip_rows<TRANS>();
 }
 
 // Advances to the next task of the sweep; false past the end.
-template <bool FORWARD>
+template <bool FORWARD, bool TRANS>
 __device__ __forceinline__ bool next_task(int n, int nblk, Task &task)
 {
-    if (task.strip + 1 < strips<FORWARD>(n, task.blk))
+    if (task.strip + 1 < strips<FORWARD, TRANS>(n, task.blk))
     {
         ++task.strip;
         return true;
@@ -61,10 +74,12 @@ __device__ __forceinline__ bool next_task(int n, int nblk, Task &task)
     return FORWARD ? task.blk < nblk : task.blk >= 0;
 }
 
-// First row and row count of a task's tile (columns kb .. kb + w - 1).
-template <bool FORWARD>
+// First row and row count of a task's tile (columns kb .. kb + w - 1; transposed: the rows
+// of x it updates, which are columns of the factor).
+template <bool FORWARD, bool TRANS>
 __device__ __forceinline__ void task_rows(int n, Task task, int &row0, int &rows)
 {
+    constexpr int R = strip_rows<TRANS>();
     const int kb = task.blk * KB;
     const int w = min(KB, n - kb);
     if (task.strip < 0)
@@ -74,13 +89,13 @@ __device__ __forceinline__ void task_rows(int n, Task task, int &row0, int &rows
     }
     else if (FORWARD)
     {
-        row0 = kb + w + task.strip * SR;
-        rows = min(SR, n - row0);
+        row0 = kb + w + task.strip * R;
+        rows = min(R, n - row0);
     }
     else
     {
-        row0 = task.strip * SR;
-        rows = min(SR, kb - row0);
+        row0 = task.strip * R;
+        rows = min(R, kb - row0);
     }
 }
 
@@ -103,14 +118,40 @@ __device__ __forceinline__ void cp_wait()
 
 // Starts the copy of a task's tile into stage[k][r] (k < 32 columns, r < rows); entries past
 // the tile are zero-filled.  vec: 16-byte copies (the matrix is 16-byte aligned, lda % 4 == 0).
-template <bool FORWARD>
+// A transposed strip goes to stage[r][k] = A(kb + k, row0 + r) (pitch TP): factor column
+// row0 + r, rows kb .. kb + 31.
+template <bool FORWARD, bool TRANS>
 __device__ __forceinline__ void issue_task(const float *A, int lda, int n, Task task, float *stage, bool vec,
                                           const float *dinv)
 {
     int row0, rows;
-    task_rows<FORWARD>(n, task, row0, rows);
+    task_rows<FORWARD, TRANS>(n, task, row0, rows);
     const int kb = task.blk * KB;
     const int w = min(KB, n - kb);
+    if (TRANS && task.strip >= 0)
+    {
+        if (vec)
+        {
+            for (int c = threadIdx.x; c < SRT * (KB / 4); c += ST)
+            {
+                const int r = c / (KB / 4), k = (c % (KB / 4)) * 4;
+                const int valid = r < rows ? max(0, min(4, w - k)) : 0;
+                const float *src = valid ? A + (int64_t)(row0 + r) * lda + kb + k : A;
+                cp_async16(stage + r * TP + k, src, valid * 4);
+            }
+        }
+        else
+        {
+            for (int c = threadIdx.x; c < SRT * KB; c += ST)
+            {
+                const int r = c / KB, k = c % KB;
+                const bool valid = r < rows && k < w;
+                const float *src = valid ? A + (int64_t)(row0 + r) * lda + kb + k : A;
+                cp_async4(stage + r * TP + k, src, valid ? 4 : 0);
+            }
+        }
+        return;
+    }
     if (dinv && task.strip < 0)
     {
         // the block's inverse triangle (32 x 32, column-major): always 16-byte aligned
@@ -211,7 +252,34 @@ __device__ __forceinline__ void apply_pivots(const int *piv, int n, float *x, in
     }
 }
 
-template <bool FORWARD>
+// The interchanges of ipiv in reverse order (the transposed solve's last step, x = P^T z):
+// warp r on right-hand side r, the pivots 32 at a time from the last chunk down.
+__device__ __forceinline__ void apply_pivots_reverse(const int *piv, int n, float *x, int nr)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp >= nr) return;
+    float *xr = x + (size_t)warp * n;
+    for (int c0 = ((n - 1) / 32) * 32; c0 >= 0; c0 -= 32)
+    {
+        const int k = c0 + lane;
+        const int pv = k < n ? piv[k] - 1 : k;
+        const int cnt = min(32, n - c0);
+#pragma unroll
+        for (int j = 31; j >= 0; --j)
+        {
+            if (j >= cnt) continue;  // uniform
+            const int p = __shfl_sync(0xffffffffu, pv, j);
+            if (lane == 0 && p != c0 + j)
+            {
+                const float a = xr[c0 + j];
+                xr[c0 + j] = xr[p];
+                xr[p] = a;
+            }
+        }
+    }
+}
+
+template <bool FORWARD, bool TRANS>
 __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *stages, bool vec, const float *dinv,
                       const short *lists, const int *piv)
 {
@@ -226,17 +294,17 @@ __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *s
     for (int i = 1; i < STAGES; ++i)
     {
         q[i] = q[i - 1];
-        live[i] = live[i - 1] && next_task<FORWARD>(n, nblk, q[i]);
+        live[i] = live[i - 1] && next_task<FORWARD, TRANS>(n, nblk, q[i]);
     }
 #pragma unroll
     for (int i = 0; i < STAGES - 1; ++i)
     {
-        if (live[i]) issue_task<FORWARD>(A, lda, n, q[i], stages + (size_t)i * KB * SP, vec, dinv);
+        if (live[i]) issue_task<FORWARD, TRANS>(A, lda, n, q[i], stages + (size_t)i * KB * SP, vec, dinv);
         cp_commit();
     }
     // the row interchanges run while the first tiles are copied (the loop's first barrier
     // publishes them)
-    if (FORWARD && piv) apply_pivots(piv, n, x, nr);
+    if (FORWARD && !TRANS && piv) apply_pivots(piv, n, x, nr);
     int slot = 0;
     while (live[0])
     {
@@ -248,7 +316,7 @@ __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *s
         __syncthreads();
         // refill: the task STAGES - 1 ahead goes to the stage freed by the previous task
         if (live[STAGES - 1])
-            issue_task<FORWARD>(A, lda, n, q[STAGES - 1],
+            issue_task<FORWARD, TRANS>(A, lda, n, q[STAGES - 1],
                                 stages + (size_t)((slot + STAGES - 1) % STAGES) * KB * SP, vec, dinv);
         cp_commit();
         const float *tile = stages + (size_t)slot * KB * SP;
@@ -272,6 +340,39 @@ __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *s
                     s4[k & 3] = fma_rn(tile[k * SP + lane], xk, s4[k & 3]);
                 }
                 if (lane < w) xr[kb + lane] = (s4[0] + s4[1]) + (s4[2] + s4[3]);
+            }
+            else if (TRANS && warp < nr)
+            {
+                // U^T forward (divide, then update the rows below) or L^T backward (unit); lane
+                // i reads factor element (kb + k, kb + i) = tile[i][k]
+                float *xr = x + (size_t)warp * n;
+                float xv = lane < w ? xr[kb + lane] : 0.0f;
+                if (FORWARD)
+                {
+                    const float dl = lane < w ? tile[lane * SP + lane] : 1.0f;
+                    const float yl = div_prepare(dl);
+                    const bool okl = div_range(dl);
+#pragma unroll
+                    for (int k = 0; k < KB; ++k)
+                    {
+                        if (k < w)
+                        {
+                            if (lane == k) xv = div_by(xv, dl, yl, okl);
+                            const float xk = __shfl_sync(0xffffffffu, xv, k);
+                            if (lane > k && lane < w) xv = fma_rn(-tile[lane * SP + k], xk, xv);
+                        }
+                    }
+                }
+                else
+                {
+#pragma unroll
+                    for (int k = KB - 1; k >= 0; --k)
+                    {
+                        const float xk = __shfl_sync(0xffffffffu, xv, k);
+                        if (lane < k && k < w) xv = fma_rn(-tile[lane * SP + k], xk, xv);
+                    }
+                }
+                if (lane < w) xr[kb + lane] = xv;
             }
             else if (warp < nr)
             {
@@ -309,8 +410,44 @@ __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *s
         else
         {
             int row0, rows;
-            task_rows<FORWARD>(n, cur, row0, rows);
-            if (t < rows)
+            task_rows<FORWARD, TRANS>(n, cur, row0, rows);
+            if (TRANS && t < rows)
+            {
+                // this thread's factor column, rows kb .. kb + 31, four at a time
+                const float *col = tile + t * TP;
+                const int row = row0 + t;
+                for (int r = 0; r < nr; ++r)
+                {
+                    float *xr = x + (size_t)r * n;
+                    float acc = xr[row];
+                    if (FORWARD)
+                    {
+#pragma unroll
+                        for (int k4 = 0; k4 < KB; k4 += 4)
+                        {
+                            const float4 u = *reinterpret_cast<const float4 *>(col + k4);
+                            if (k4 < w) acc = fma_rn(-u.x, xr[kb + k4], acc);
+                            if (k4 + 1 < w) acc = fma_rn(-u.y, xr[kb + k4 + 1], acc);
+                            if (k4 + 2 < w) acc = fma_rn(-u.z, xr[kb + k4 + 2], acc);
+                            if (k4 + 3 < w) acc = fma_rn(-u.w, xr[kb + k4 + 3], acc);
+                        }
+                    }
+                    else
+                    {
+#pragma unroll
+                        for (int k4 = KB - 4; k4 >= 0; k4 -= 4)
+                        {
+                            const float4 u = *reinterpret_cast<const float4 *>(col + k4);
+                            if (k4 + 3 < w) acc = fma_rn(-u.w, xr[kb + k4 + 3], acc);
+                            if (k4 + 2 < w) acc = fma_rn(-u.z, xr[kb + k4 + 2], acc);
+                            if (k4 + 1 < w) acc = fma_rn(-u.y, xr[kb + k4 + 1], acc);
+                            if (k4 < w) acc = fma_rn(-u.x, xr[kb + k4], acc);
+                        }
+                    }
+                    xr[row] = acc;
+                }
+            }
+            else if (!TRANS && t < rows)
             {
                 const int row = row0 + t;
                 for (int r = 0; r < nr; ++r)
@@ -342,7 +479,7 @@ __device__ void sweep(const float *A, int lda, int n, float *x, int nr, float *s
             live[i] = live[i + 1];
         }
         q[STAGES - 1] = q[STAGES - 2];
-        live[STAGES - 1] = live[STAGES - 2] && next_task<FORWARD>(n, nblk, q[STAGES - 1]);
+        live[STAGES - 1] = live[STAGES - 2] && next_task<FORWARD, TRANS>(n, nblk, q[STAGES - 1]);
         slot = (slot + 1) % STAGES;
     }
     cp_wait<0>();
@@ -354,7 +491,7 @@ __global__ void __launch_bounds__(ST, 2) getrs_blocked_kernel(float *a_single, f
                                                             float *const *b_table, int b_first, int n, int lda,
                                                             int ldb, int nrhs, int count, int RHS, int *info,
                                                             const int *skip, const float *dinv_all, int nblk,
-                                                            const short *lists_all)
+                                                            const short *lists_all, int trans)
 {
     extern __shared__ __align__(16) float dyn[];
     float *stages = dyn;                          // STAGES x KB x SP
@@ -391,7 +528,8 @@ __global__ void __launch_bounds__(ST, 2) getrs_blocked_kernel(float *a_single, f
         {
             const int r = e / n, i = e % n;
             // with a permutation, x = P b directly: row i of the permuted vector is b[perm[i]]
-            x[e] = B[(int64_t)(r0 + r) * ldb + (sig ? sig[i] : i)];
+            // (transposed: the permutation is applied on the way out)
+            x[e] = B[(int64_t)(r0 + r) * ldb + (sig && !trans ? sig[i] : i)];
         }
         __syncthreads();
         if (bad)
@@ -403,12 +541,26 @@ __global__ void __launch_bounds__(ST, 2) getrs_blocked_kernel(float *a_single, f
         const bool vec = (reinterpret_cast<uintptr_t>(A) & 15u) == 0 && (lda & 3) == 0;
         const float *dinv = dinv_all ? dinv_all + (size_t)q * nblk * 2 * KB * KB : nullptr;
         const short *lists = lists_all ? lists_all + (size_t)q * BLOCKED_PANELS * PANEL_LIST_SHORTS : nullptr;
-        sweep<true>(A, lda, n, x, nr, stages, vec, dinv, lists, sig ? nullptr : piv);
-        sweep<false>(A, lda, n, x, nr, stages, vec, dinv, nullptr, nullptr);
+        if (trans)
+        {
+            sweep<true, true>(A, lda, n, x, nr, stages, vec, nullptr, nullptr, nullptr);
+            sweep<false, true>(A, lda, n, x, nr, stages, vec, nullptr, nullptr, nullptr);
+            if (piv && !sig)
+            {
+                apply_pivots_reverse(piv, n, x, nr);
+                __syncthreads();
+            }
+        }
+        else
+        {
+            sweep<true, false>(A, lda, n, x, nr, stages, vec, dinv, lists, sig ? nullptr : piv);
+            sweep<false, false>(A, lda, n, x, nr, stages, vec, dinv, nullptr, nullptr);
+        }
         for (int e = t; e < nr * n; e += ST)
         {
             const int r = e / n, i = e % n;
-            B[(int64_t)(r0 + r) * ldb + i] = x[e];
+            // transposed with a permutation: x = P^T z, so z[i] lands on row perm[i]
+            B[(int64_t)(r0 + r) * ldb + (sig && trans ? sig[i] : i)] = x[e];
         }
         if (t == 0 && info && r0 == 0) info[q] = 0;
         __syncthreads();
@@ -502,9 +654,10 @@ __global__ void permutation_kernel(const int *ipiv, int *perm, int n, int count)
 
 cudaError_t launch_getrs_blocked(const RealBatch &a, const int *ipiv, const int *perm, const RealBatch &b, int nrhs,
                                  int *info, const int *skip, cudaStream_t stream, const float *dinv,
-                                 const short *lists)
+                                 const short *lists, int trans)
 {
     if (lists && (a.n > BLOCKED_MAX_N || ipiv || perm)) return cudaErrorInvalidValue;
+    if (trans && (dinv || lists)) return cudaErrorInvalidValue;
     const size_t stage_floats = (size_t)STAGES * KB * SP;
     // two blocks per SM when the vectors fit beside the ring, else one
     int rpb = (int)((110 * 1024 / sizeof(float) - stage_floats) / (size_t)a.n);
@@ -521,7 +674,7 @@ cudaError_t launch_getrs_blocked(const RealBatch &a, const int *ipiv, const int 
     getrs_blocked_kernel<<<(unsigned)blocks, ST, smem, stream>>>(a.single, a.table, a.first, ipiv, perm, b.single,
                                                                  b.table, b.first, a.n, a.ld, b.ld, nrhs, a.count,
                                                                  rpb, info, skip, dinv, (a.n + KB - 1) / KB,
-                                                                 lists);
+                                                                 lists, trans);
     return cudaGetLastError();
 }
 

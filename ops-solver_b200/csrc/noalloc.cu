@@ -7,14 +7,16 @@
 // all device memory out from their own pool and forbid allocations after start-up, and
 // latency-critical loops where an allocation's implicit device synchronisation is not
 // acceptable.  This entry keeps the pivots in a fixed array compiled into the library
-// instead, so a call allocates nothing.  Its first call on a device resolves the array's
-// device address (cudaGetSymbolAddress) and should come before any stream capture.
+// instead, so a call allocates nothing.  Its first call on a device (and the first call
+// after that device's context was reset) resolves the array's device address
+// (cudaGetSymbolAddress) and should come before any stream capture.
 //
 // The array (PIVOT_CAPACITY ints, 4 MiB) lives in every GPU that loads the library until the
 // process exits.  All calls share it and it keeps the last call's contents; the LU step
 // writes every pivot of every matrix before the inverse step reads it, so nothing needs
 // clearing.  Calls whose executions overlap on the GPU (different streams or handles, or
 // different host threads) race on the array: serialise them.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdio.h>
 
@@ -28,33 +30,88 @@ namespace ops_solver
 namespace
 {
 constexpr int PIVOT_CAPACITY = 1 << 20;  // ints: n * batchSize must not exceed this
+constexpr int MAX_BATCH = 10000000;      // the batched inverse's limit (real_lu_common.h:18)
 constexpr int MAX_DEVICES = 64;
 
 static __device__ __align__(256) int pivot_scratch[PIVOT_CAPACITY];
 
-// Device address of pivot_scratch, resolved once per device.  In host code the symbol
-// names a host-side stand-in, never the device array, so the address must come from
-// cudaGetSymbolAddress with the device current.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+
+// Process-unique id of the current context (cuCtxGetId never reuses an id, unlike the
+// CUcontext handle, which a context created after a reset may share with its predecessor).
+// 0 when the driver does not offer the query.
+unsigned long long current_context_id()
+{
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, []
+    {
+        void *p = nullptr, *q = nullptr;
+        cudaDriverEntryPointQueryResult r1, r2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &r1) == cudaSuccess &&
+            r1 == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &q, cudaEnableDefault, &r2) == cudaSuccess &&
+            r2 == cudaDriverEntryPointSuccess)
+        {
+            get_current = reinterpret_cast<CtxGetCurrentFn>(p);
+            get_id = reinterpret_cast<CtxGetIdFn>(q);
+        }
+        cudaGetLastError();
+    });
+    if (!get_current || !get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Device address of pivot_scratch for the current device and context.  In host code the
+// symbol names a host-side stand-in, never the device array, so the address must come from
+// cudaGetSymbolAddress with the device current.  It is resolved once per device and
+// context: a reset device gets a new context (new id), whose module holds the array at a
+// new address.  Without the context query the address is resolved on every call.
 int *pivot_address(int device)
 {
     static std::mutex lock;
     static int *address[MAX_DEVICES] = {nullptr};
+    static unsigned long long context[MAX_DEVICES] = {0};
     if (device < 0 || device >= MAX_DEVICES) return nullptr;
     std::lock_guard<std::mutex> guard(lock);
-    if (!address[device])
+    const unsigned long long id = current_context_id();
+    if (id != 0 && address[device] && context[device] == id) return address[device];
+    int *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&ptr), pivot_scratch);
+    if (e != cudaSuccess)
     {
-        int *ptr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&ptr), pivot_scratch);
-        if (e != cudaSuccess)
-        {
-            cudaGetLastError();
-            fprintf(stderr, "[aclsolver] aclsolverSmatinvBatchedNoAlloc: cudaGetSymbolAddress failed: %s\n",
-                    cudaGetErrorString(e));
-            return nullptr;
-        }
-        address[device] = ptr;
+        cudaGetLastError();
+        fprintf(stderr, "[aclsolver] aclsolverSmatinvBatchedNoAlloc: cudaGetSymbolAddress failed: %s\n",
+                cudaGetErrorString(e));
+        return nullptr;
     }
-    return address[device];
+    // The runtime has set the context up by now; its id keys the cached address (0, no
+    // query available: nothing is cached and the next call resolves the address again).
+    address[device] = ptr;
+    context[device] = current_context_id();
+    return ptr;
+}
+
+// True when info[0..count) is an aligned span inside one device allocation (the rule the
+// batched LU entries apply before they write argument errors to info).
+bool info_fits(const int *info, int64_t count)
+{
+    return info && reinterpret_cast<uintptr_t>(info) % alignof(int) == 0 && is_device_pointer(info) &&
+           device_span(info, (size_t)count * sizeof(int));
+}
+
+aclsolverStatus_t invalid(Handle *h, int *info, int64_t count, int argument)
+{
+    if (count > 0 && info_fits(info, count))
+    {
+        if (launch_fill_info(info, -argument, count, h->stream) != cudaSuccess) cudaGetLastError();
+    }
+    return ACLSOLVER_STATUS_INVALID_VALUE;
 }
 }  // namespace
 }  // namespace ops_solver
@@ -83,27 +140,30 @@ extern "C" __attribute__((visibility("default"))) aclsolverStatus_t aclsolverSma
         arg = 6;
     else if (batchSize < 0)
         arg = 7;
-    else if ((int64_t)n * batchSize > PIVOT_CAPACITY)
+    if (arg) return invalid(h, info, batchSize < 0 ? 1 : batchSize, arg);
+    if (batchSize > MAX_BATCH) return invalid(h, info, batchSize, 7);
+    if ((int64_t)n * batchSize > PIVOT_CAPACITY)
     {
         fprintf(stderr,
                 "[aclsolver] aclsolverSmatinvBatchedNoAlloc: n * batchSize = %lld exceeds the fixed pivot array "
                 "(%d entries); split the batch\n",
                 (long long)n * batchSize, PIVOT_CAPACITY);
-        arg = 7;
-    }
-    if (arg)
-    {
-        const int64_t count = batchSize < 0 ? 1 : batchSize;
-        if (info && count > 0 && is_device_pointer(info)) launch_fill_info(info, -arg, count, h->stream);
-        cudaGetLastError();
-        return ACLSOLVER_STATUS_INVALID_VALUE;
+        return invalid(h, info, batchSize, 7);
     }
     if (batchSize == 0) return ACLSOLVER_STATUS_SUCCESS;
+    if (!info_fits(info, batchSize)) return ACLSOLVER_STATUS_INVALID_VALUE;
     if (n == 0) return launch_status(launch_fill_info(info, 0, batchSize, h->stream));
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess)
     {
         cudaGetLastError();
+        return ACLSOLVER_STATUS_EXECUTION_FAILED;
+    }
+    if (device != h->device)
+    {
+        fprintf(stderr,
+                "[aclsolver] aclsolverSmatinvBatchedNoAlloc: the current device (%d) is not the handle's (%d)\n",
+                device, h->device);
         return ACLSOLVER_STATUS_EXECUTION_FAILED;
     }
     int *pivots = pivot_address(device);

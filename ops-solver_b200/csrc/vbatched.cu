@@ -9,7 +9,10 @@
 //   warp tasks  (n <= cutoff): one matrix per warp (or per 8/16-lane sub-warp), the factor
 //               rows in registers, then the solve of every right-hand side in place;
 //   block tasks (n >  cutoff): one matrix per block, the lower triangle in shared memory,
-//               factor and solve without leaving shared memory.
+//               factor and solve without leaving shared memory -- orders up to 128 through
+//               the packed-triangle routine of complex_block.cuh (a thread per row, in two
+//               launches sized for 65..128 and for up to 64, so small matrices pack more
+//               blocks per SM), larger ones through a generic block kernel.
 // Two persistent kernels drain the queues through atomic task counters (no waiting: a
 // block that finds the queue empty exits) and run as parallel branches of one graph.
 // The arithmetic is that of complex_chol.cu (same per-element order), so results are
@@ -27,6 +30,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "complex_block.cuh"
 #include "handle.h"
 #include "vbatched.h"
 
@@ -348,6 +352,39 @@ __global__ void __launch_bounds__(T) vb_block_kernel(VbDesc d, const VbTask *tas
     }
 }
 
+// Orders up to T: one matrix per block through the packed-triangle routine.
+template <int T>
+__global__ void __launch_bounds__(T) vb_cb_kernel(VbDesc d, const VbTask *tasks, int ntasks, int *counter)
+{
+    extern __shared__ __align__(16) float cb_mem[];
+    __shared__ int task_id;
+    for (;;)
+    {
+        if (threadIdx.x == 0) task_id = atomicAdd(counter, 1);
+        __syncthreads();
+        const int id = task_id;
+        __syncthreads();
+        if (id >= ntasks) return;
+        const int q = d.order[tasks[id].first];
+        const int n = d.n[q];
+        float2 *pa = slot(d.a, q);
+        float2 *pb = slot(d.b, q);
+        if (!pa)
+        {
+            if (threadIdx.x == 0) d.info[q] = -3;
+            continue;
+        }
+        const CbShared s = cb_carve(cb_mem, n);
+        cb_load<T>(s, pa, d.lda[q], d.upper, n);
+        __syncthreads();
+        const int failure = cb_factor<T>(s, n);
+        cb_store<T>(s, pa, d.lda[q], d.upper, n, failure ? failure - 1 : n);
+        if (threadIdx.x == 0) d.info[q] = failure;
+        if (!failure && pb) cb_solve<T>(s, n, pb, d.ldb[q], d.nrhs);
+        __syncthreads();
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 // host side: buckets, tasks, launch shapes, autotuning and the graph
 // ---------------------------------------------------------------------------------------
@@ -386,7 +423,33 @@ cudaError_t launch_shape(const VbPlan *p, const Shape &s, const VbDesc &d, cudaS
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
-    const auto &bt = p->block_tasks.at(s.cutoff);
+    // packed-triangle launches: 65..128 (128 threads), then up to 64 (64 threads)
+    for (int part = 0; part < 2 && e == cudaSuccess; ++part)
+    {
+        const auto &range = part == 0 ? p->mid_tasks.at(s.cutoff) : p->small_tasks.at(s.cutoff);
+        if (range.second == 0) continue;
+        const int nmax = part == 0 ? p->mid_nmax.at(s.cutoff) : p->small_nmax.at(s.cutoff);
+        const size_t smem = cb_smem_bytes(nmax);
+        const VbTask *tasks = p->d_tasks + range.first;
+        int per_sm = 1;
+        if (part == 0)
+        {
+            cudaFuncSetAttribute(vb_cb_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vb_cb_kernel<128>, 128, smem);
+            const int blocks = std::min(range.second, sms * std::max(1, per_sm));
+            vb_cb_kernel<128><<<blocks, 128, smem, main>>>(d, tasks, range.second, p->d_counters + 2);
+        }
+        else
+        {
+            cudaFuncSetAttribute(vb_cb_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vb_cb_kernel<64>, 64, smem);
+            const int blocks = std::min(range.second, sms * std::max(1, per_sm));
+            vb_cb_kernel<64><<<blocks, 64, smem, main>>>(d, tasks, range.second, p->d_counters + 3);
+        }
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return e;
+    const auto &bt = p->big_tasks.at(s.cutoff);
     if (bt.second > 0)
     {
         const int nmax = p->block_nmax.at(s.cutoff);
@@ -418,7 +481,7 @@ cudaError_t launch_shape(const VbPlan *p, const Shape &s, const VbDesc &d, cudaS
 // Enqueue one full execution: reset counters, fork the warp branch, block branch, join.
 cudaError_t enqueue(VbPlan *p, const Shape &s, const VbDesc &d, cudaStream_t stream)
 {
-    cudaError_t e = cudaMemsetAsync(p->d_counters, 0, 2 * sizeof(int), stream);
+    cudaError_t e = cudaMemsetAsync(p->d_counters, 0, 4 * sizeof(int), stream);
     if (e == cudaSuccess) e = cudaEventRecord(p->fork, stream);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(p->side, p->fork, 0);
     if (e == cudaSuccess) e = launch_shape(p, s, d, stream, p->side);
@@ -621,8 +684,18 @@ aclsolverStatus_t vb_plan_create(Handle *h, int uplo, const int *n, const int *l
         p->warp_tasks[cutoff] = {(int)tasks.size(), (int)warp.size()};
         tasks.insert(tasks.end(), warp.begin(), warp.end());
         p->block_tasks[cutoff] = {(int)tasks.size(), (int)block.size()};
-        tasks.insert(tasks.end(), block.begin(), block.end());
         p->block_nmax[cutoff] = nmax;
+        // the block tasks are in descending order: split them at 128 and 64
+        int big = 0, mid = 0;
+        while (big < (int)block.size() && n[order[block[big].first]] > 128) ++big;
+        while (big + mid < (int)block.size() && n[order[block[big + mid].first]] > 64) ++mid;
+        const int base = (int)tasks.size();
+        p->big_tasks[cutoff] = {base, big};
+        p->mid_tasks[cutoff] = {base + big, mid};
+        p->small_tasks[cutoff] = {base + big + mid, (int)block.size() - big - mid};
+        p->mid_nmax[cutoff] = mid ? n[order[block[big].first]] : 0;
+        p->small_nmax[cutoff] = big + mid < (int)block.size() ? n[order[block[big + mid].first]] : 0;
+        tasks.insert(tasks.end(), block.begin(), block.end());
     }
     cudaError_t e = cudaSuccess;
     auto alloc = [&](void **ptr, size_t bytes)
@@ -634,7 +707,7 @@ aclsolverStatus_t vb_plan_create(Handle *h, int uplo, const int *n, const int *l
     alloc((void **)&p->d_ldb, count * sizeof(int));
     alloc((void **)&p->d_order, count * sizeof(int));
     alloc((void **)&p->d_tasks, tasks.size() * sizeof(VbTask));
-    alloc((void **)&p->d_counters, 2 * sizeof(int));
+    alloc((void **)&p->d_counters, 4 * sizeof(int));
     if (e == cudaSuccess) e = cudaMemcpy(p->d_n, n, count * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(p->d_lda, lda, count * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(p->d_ldb, ldb, count * sizeof(int), cudaMemcpyHostToDevice);

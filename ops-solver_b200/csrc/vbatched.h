@@ -43,6 +43,11 @@ struct VbPlan
     // largest order
     std::map<int, std::pair<int, int>> warp_tasks, block_tasks;
     std::map<int, int> block_nmax;
+    // the block tasks of each cutoff split by order: above 128 (generic block kernel), 65..128
+    // and up to 64 (packed-triangle kernels of 128 and 64 threads): (offset, count) and the
+    // largest order of each part
+    std::map<int, std::pair<int, int>> big_tasks, mid_tasks, small_tasks;
+    std::map<int, int> mid_nmax, small_nmax;
     VbDesc desc;
     int cutoff = 32, threads = 128, warp_blocks = 8;  // the tuned launch shape
     cudaStream_t side = nullptr;

@@ -166,3 +166,15 @@ def complex_cpu_ratio(op, a, upper=False, b=None):
         return complex_ratio(op, a, f, upper)
     x, info = cpotrs(f, np.array(b, dtype=np.complex64, order="F"), lower=not upper)
     return complex_ratio(op, a, x, upper, b)
+
+
+def residual_gate(ratios, cpu_ratios):
+    """The reference's batched residual gate (test/utils/cholesky/fixtures.py:513-528,
+    verify_residuals): each device ratio must be finite and at most
+    max(5 x its CPU-LAPACK ratio, 3 x the batch mean of the CPU ratios).  Returns the list of
+    (index, ratio, threshold) that fail."""
+    ratios = np.asarray(ratios, dtype=np.float64)
+    cpu = np.asarray(cpu_ratios, dtype=np.float64)
+    threshold = np.maximum(5.0 * cpu, 3.0 * cpu.mean()) if cpu.size else cpu
+    bad = ~np.isfinite(ratios) | (ratios > threshold)
+    return [(int(i), float(ratios[i]), float(threshold[i])) for i in np.flatnonzero(bad)]

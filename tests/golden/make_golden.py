@@ -2,7 +2,7 @@
 
 Run in a container where the reference tree is mounted (it reads it, never writes it):
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <root of the reference project>
 
 Outputs (committed; the tests read only these files, never the reference tree):
 
@@ -163,4 +163,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <root of the reference project>")
+    main(sys.argv[1])

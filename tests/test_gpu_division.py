@@ -15,9 +15,13 @@ import aclsolver
 pytestmark = pytest.mark.gpu
 
 
+SELFTEST = aclsolver.LIBRARY.parent / "libops_solver_selftest.so"
+
+
 def gpu_divide(x, d):
-    lib = aclsolver.library()
-    fn = lib.lib.ops_solver_selftest_divide
+    # the helper is exported by a test-only library built beside the product one
+    assert SELFTEST.exists(), f"{SELFTEST} is missing: build it with `make -C ops-solver_b200`"
+    fn = C.CDLL(str(SELFTEST)).ops_solver_selftest_divide
     fn.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong]
     fn.restype = C.c_int
     xd = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float32)).cuda()

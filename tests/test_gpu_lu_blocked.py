@@ -139,14 +139,14 @@ def test_blocked_sgetrf_single(handle, m, n):
     assert same_bits(dm.read(), lu)
 
 
-def getrs_batched(handle, lu, ipiv, b, pad=1):
+def getrs_batched(handle, lu, ipiv, b, pad=1, trans=0):
     lib = aclsolver.library()
     count, n, _ = lu.shape
     da = DeviceMatrices(lu, ld=n + pad)
     db = DeviceMatrices(b, ld=n + pad + 1)
     piv = None if ipiv is None else device_ints(ipiv.reshape(-1))
     info = info_buffer(count)
-    st = lib.aclsolverSgetrsBatched(handle.value, 0, n, b.shape[2], da.table_ptr, da.ld,
+    st = lib.aclsolverSgetrsBatched(handle.value, trans, n, b.shape[2], da.table_ptr, da.ld,
                                    None if piv is None else piv.data_ptr(), db.table_ptr, db.ld, info.data_ptr(),
                                    count)
     handle.stream.synchronize()
@@ -165,6 +165,41 @@ def test_blocked_sgetrs_matches_oracle(handle, n, nrhs):
     got = db.read()
     assert same_bits(got, want), first_mismatch(got, want)
     assert judges.solve_compare_ok(got[0], judges.solve_lu(lu[0], b[0], ipiv[0], 0))
+
+
+@pytest.mark.parametrize("n,nrhs,pad", [(65, 1, 1), (96, 2, 0), (100, 3, 1), (225, 4, 3), (513, 9, 0), (1000, 2, 1),
+                                        (2049, 1, 0)])
+def test_blocked_sgetrs_transposed_matches_oracle(handle, n, nrhs, pad):
+    """A^T x = b above the register-resident orders: U^T forward, L^T backward, then the
+    interchanges in reverse, bit for bit the oracle's order (strips of 224 factor columns,
+    ragged last blocks, 16-byte and 4-byte staging)."""
+    a = gaussian(2, n, seed=n + 21)
+    lu, ipiv, _ = oracle.sgetrf_batched(a)
+    b = gaussian(2, nrhs, seed=n + 22, m=n)
+    st, da, db, info = getrs_batched(handle, lu, ipiv, b, pad=pad, trans=1)
+    assert st == aclsolver.SUCCESS and np.all(info == 0)
+    assert da.unchanged()
+    want = oracle.sgetrs_batched(lu, ipiv, b, trans=1)
+    got = db.read()
+    assert same_bits(got, want), first_mismatch(got, want)
+    assert judges.solve_compare_ok(got[1], judges.solve_lu(lu[1], b[1], ipiv[1], 1))
+
+
+def test_blocked_sgetrs_transposed_without_pivots_and_bad_pivot(handle):
+    n = 130
+    a = gaussian(2, n, seed=7) + 6 * np.eye(n, dtype=np.float32)
+    lu, _, _ = oracle.sgetrf_batched(a, pivoting=False)
+    b = gaussian(2, 2, seed=8, m=n)
+    st, _, db, info = getrs_batched(handle, lu, None, b, trans=1)
+    assert st == aclsolver.SUCCESS and np.all(info == 0)
+    assert same_bits(db.read(), oracle.sgetrs_batched(lu, None, b, trans=1))
+    lu, ipiv, _ = oracle.sgetrf_batched(a)
+    ipiv = ipiv.copy()
+    ipiv[1, 77] = 0  # below 1
+    st, _, db, info = getrs_batched(handle, lu, ipiv, b, trans=1)
+    assert info.tolist() == [0, -6]
+    assert np.array_equal(db.read()[1], b[1])
+    assert same_bits(db.read()[0], oracle.sgetrs_batched(lu[:1], ipiv[:1], b[:1], trans=1)[0])
 
 
 def test_blocked_sgetrs_without_pivots(handle):
@@ -189,9 +224,10 @@ def test_blocked_sgetrs_bad_pivot(handle):
     assert np.array_equal(db.read()[2], b[2])
 
 
-@pytest.mark.parametrize("n,nrhs", [(100, 1), (520, 3)])
-def test_blocked_sgetrs_host_buffers(handle, n, nrhs):
-    """The host-buffer, row-major aclsolverSgetrs above the register-resident orders."""
+@pytest.mark.parametrize("n,nrhs,trans", [(100, 1, 0), (520, 3, 0), (100, 2, 1), (520, 3, 1)])
+def test_blocked_sgetrs_host_buffers(handle, n, nrhs, trans):
+    """The host-buffer, row-major aclsolverSgetrs above the register-resident orders, both
+    trans codes."""
     lib = aclsolver.library()
     a = gaussian(1, n, seed=n)
     lu, ipiv, _ = oracle.sgetrf_batched(a)
@@ -203,9 +239,9 @@ def test_blocked_sgetrs_host_buffers(handle, n, nrhs):
     B[:, :nrhs] = b
     P = np.ascontiguousarray(ipiv[0], dtype=np.int32)
     info = np.array([99], dtype=np.int32)
-    st = lib.aclsolverSgetrs(handle.value, 0, n, nrhs, A.ctypes.data, lda, P.ctypes.data, B.ctypes.data, ldb,
+    st = lib.aclsolverSgetrs(handle.value, trans, n, nrhs, A.ctypes.data, lda, P.ctypes.data, B.ctypes.data, ldb,
                              info.ctypes.data)
     assert st == 0 and info[0] == 0
     assert np.all(B[:, nrhs:] == 3.25)
-    want = oracle.sgetrs_batched(lu, ipiv, b[None])[0]
+    want = oracle.sgetrs_batched(lu, ipiv, b[None], trans=trans)[0]
     assert same_bits(B[:, :nrhs], want), first_mismatch(B[:, :nrhs], want)

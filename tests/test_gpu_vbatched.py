@@ -89,11 +89,12 @@ def test_uneven_batch_matches_oracle(handle, seed, tmp_path, monkeypatch):
         got_f = u.factor(q)
         assert same_bits(np.ascontiguousarray(np.tril(got_f)).view(np.float32), np.ascontiguousarray(np.tril(f[0])).view(np.float32)), (q, n)
         assert same_bits(u.solution(q).view(np.float32), np.ascontiguousarray(x[0]).view(np.float32)), (q, n)
-    for q in range(0, len(orders), 37):
+    ratios, cpu = [], []
+    for q in range(0, len(orders), 7):
         if orders[q]:
-            r = judges.complex_ratio("potrs", u.a[q], u.solution(q), False, u.b[q])
-            c = judges.complex_cpu_ratio("potrs", u.a[q], False, u.b[q])
-            assert r <= max(5 * c, 1.0)
+            ratios.append(judges.complex_ratio("potrs", u.a[q], u.solution(q), False, u.b[q]))
+            cpu.append(judges.complex_cpu_ratio("potrs", u.a[q], False, u.b[q]))
+    assert not judges.residual_gate(ratios, cpu), judges.residual_gate(ratios, cpu)
     assert lib.aclsolverVbatchedPlanDestroy(p) == aclsolver.SUCCESS
 
 
@@ -144,3 +145,62 @@ def test_plan_argument_checks(handle):
                                                0, C.byref(p)) == aclsolver.INVALID_VALUE
     assert lib.aclsolverCposvVbatchedPlanCreate(None, 0, n.ctypes.data, ld.ctypes.data, ld.ctypes.data, 1, 2, 0,
                                                C.byref(p)) == aclsolver.NOT_INITIALIZED
+
+
+def test_uneven_batch_full_workload(handle, tmp_path, monkeypatch):
+    """The uneven-order workload at full size: 20,000 HPD matrices of orders U{8..128},
+    A = G G^H / n + I (real and imaginary parts of G N(0,1)), 4 right-hand sides, one plan
+    and one call.  Every factor and solution bit for bit against the oracle (grouped by
+    order), info all 0, and the reference's residual gate on a sample."""
+    import torch
+
+    monkeypatch.setenv("OPS_SOLVER_TUNE_CACHE", str(tmp_path / "tune.txt"))
+    count, nrhs = 20_000, 4
+    rng = np.random.default_rng(2)
+    orders = rng.integers(8, 129, size=count).astype(np.int32)
+    a_off = np.zeros(count, dtype=np.int64)
+    b_off = np.zeros(count, dtype=np.int64)
+    a_off[1:] = np.cumsum(orders.astype(np.int64) ** 2)[:-1]
+    b_off[1:] = np.cumsum(orders.astype(np.int64) * nrhs)[:-1]
+    a_flat = np.empty(int((orders.astype(np.int64) ** 2).sum()), dtype=np.complex64)
+    b_flat = ((rng.standard_normal(int(orders.sum()) * nrhs) + 1j * rng.standard_normal(int(orders.sum()) * nrhs))
+              * np.sqrt(0.5)).astype(np.complex64)
+    groups = {}
+    for n in np.unique(orders):
+        idx = np.nonzero(orders == n)[0]
+        g = (rng.standard_normal((len(idx), n, n)) + 1j * rng.standard_normal((len(idx), n, n))).astype(np.complex64)
+        m = (g @ np.conj(g.transpose(0, 2, 1)) / np.float32(n) + np.eye(n, dtype=np.complex64)).astype(np.complex64)
+        groups[int(n)] = (idx, m)
+        for k, q in enumerate(idx):
+            a_flat[a_off[q]:a_off[q] + n * n] = m[k].T.reshape(-1)
+    da = torch.from_numpy(a_flat.view(np.float32).copy()).cuda()
+    db = torch.from_numpy(b_flat.view(np.float32).copy()).cuda()
+    ta = torch.from_numpy(a_off * 8).cuda() + da.data_ptr()
+    tb = torch.from_numpy(b_off * 8).cuda() + db.data_ptr()
+    lib = aclsolver.library()
+    ld = np.ascontiguousarray(orders)
+    p = C.c_void_p()
+    assert lib.aclsolverCposvVbatchedPlanCreate(handle.value, 0, ld.ctypes.data, ld.ctypes.data, ld.ctypes.data, nrhs,
+                                               count, 1, C.byref(p)) == aclsolver.SUCCESS
+    info = info_buffer(count)
+    st = lib.aclsolverCposvVbatched(handle.value, p, ta.data_ptr(), tb.data_ptr(), info.data_ptr())
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS
+    assert np.all(info.cpu().numpy() == 0)
+    lib.aclsolverVbatchedPlanDestroy(p)
+    fa = da.cpu().numpy().view(np.complex64)
+    xb = db.cpu().numpy().view(np.complex64)
+    ratios, cpu = [], []
+    for n, (idx, m) in groups.items():
+        bq = np.stack([b_flat[b_off[q]:b_off[q] + n * nrhs].reshape(nrhs, n).T for q in idx])
+        f, winfo = oracle.cpotrf_batched(m)
+        assert np.all(winfo == 0)
+        x = oracle.cpotrs_batched(f, bq)
+        got_f = np.ascontiguousarray(np.stack([fa[a_off[q]:a_off[q] + n * n].reshape(n, n).T for q in idx]))
+        got_x = np.ascontiguousarray(np.stack([xb[b_off[q]:b_off[q] + n * nrhs].reshape(nrhs, n).T for q in idx]))
+        assert same_bits(np.tril(got_f).view(np.float32), np.tril(f).view(np.float32)), n
+        assert same_bits(got_x.view(np.float32), np.ascontiguousarray(x).view(np.float32)), n
+        k = 0  # one matrix per order for the residual gate
+        ratios.append(judges.complex_ratio("potrs", m[k], got_x[k], False, bq[k]))
+        cpu.append(judges.complex_cpu_ratio("potrs", m[k], False, bq[k]))
+    assert not judges.residual_gate(ratios, cpu), judges.residual_gate(ratios, cpu)

@@ -159,3 +159,15 @@ def test_lu_zero_pivot_continues():
     lu, ipiv, info = oracle.sgetrf_batched(a)
     assert info[0] == 1  # first zero pivot, factorisation continues
     assert ipiv[0].tolist()[0] == 1
+
+
+def test_residual_gate_flags_an_inflated_ratio():
+    """The reference's batched gate max(5 x cpu, 3 x mean(cpu)): a device ratio planted above
+    its threshold, and a non-finite one, are reported; the rest pass."""
+    cpu = np.array([1.0, 2.0, 0.5, 0.5])
+    ok = np.array([4.9, 9.9, 3.0, 0.1])
+    assert judges.residual_gate(ok, cpu) == []
+    bad = ok.copy()
+    bad[2] = 3.1  # threshold max(2.5, 3 * 1.0) = 3.0
+    bad[3] = np.inf
+    assert [i for i, _, _ in judges.residual_gate(bad, cpu)] == [2, 3]
