@@ -177,7 +177,9 @@ extern "C"
         if (!used) return launch_status(launch_fill_info(info, 0, 1, h->stream));
         aclsolverStatus_t span = info_span(info, count);
         if (span != ACLSOLVER_STATUS_SUCCESS) return span;
-        cudaError_t e = launch_solve_slot_check(info, Aarray, Barray, count, h->stream);
+        int *flags = device_flags(h);
+        if (!flags) return ACLSOLVER_STATUS_ALLOC_FAILED;
+        cudaError_t e = launch_solve_slot_check(info, Aarray, Barray, count, flags + SLOT_CHECK_FLAGS, h->stream);
         if (e == cudaSuccess)
         {
             RealBatch a{nullptr, Aarray, n, lda, 0, count};

@@ -165,9 +165,11 @@ int *device_flags(Handle *h)
 {
     if (!h->dev_flags)
     {
-        if (cudaMalloc(&h->dev_flags, 64 * sizeof(int)) != cudaSuccess)
+        if (cudaMalloc(&h->dev_flags, 64 * sizeof(int)) != cudaSuccess ||
+            cudaMemset(h->dev_flags, 0, 64 * sizeof(int)) != cudaSuccess)
         {
             cudaGetLastError();
+            cudaFree(h->dev_flags);
             h->dev_flags = nullptr;
         }
     }

@@ -51,8 +51,11 @@ aclsolverStatus_t finish_scratch(Handle *h, ScratchBlock *b);
 
 // Pinned host staging of at least `bytes` (grown on demand, freed at Destroy).
 void *host_stage(Handle *h, size_t bytes);
-// Device flag words (count <= 64), zeroed on the handle stream before use.
+// Device flag words (64 ints, zeroed when first allocated).  Words 0..31 are zeroed by their
+// users before each use; words 60..63 belong to the batched solves' slot check, which leaves
+// them zero after every launch.
 int *device_flags(Handle *h);
+constexpr int SLOT_CHECK_FLAGS = 60;
 
 // Pointer classification: true for device (or managed) memory of the current context.
 bool is_device_pointer(const void *p);

@@ -27,7 +27,9 @@ struct RealBatch
 cudaError_t launch_fill_info(int *info, int value, int64_t count, cudaStream_t stream);
 // SpotrsBatched slot scan: info[0] = -4 if any A slot is null, else -6 if any B slot is
 // null, else 0 (cholesky_simt.cpp:28-48 contract).
-cudaError_t launch_solve_slot_check(int *info, float *const *a, float *const *b, int count, cudaStream_t stream);
+// flags: two device words that are zero on entry (left zero on exit).
+cudaError_t launch_solve_slot_check(int *info, float *const *a, float *const *b, int count, int *flags,
+                                    cudaStream_t stream);
 // In-place Cholesky of n <= 32 matrices, per-slot info (null slot -> -3).
 cudaError_t launch_potrf_small(const RealBatch &a, int upper, int *info, cudaStream_t stream);
 // In-place Cholesky of n > 32 matrices (FMA order, left-looking), per-slot info.
