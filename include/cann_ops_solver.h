@@ -71,6 +71,15 @@ extern "C"
     aclsolverStatus_t aclsolverCpotrs(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n, int nrhs,
                                       const aclsolverFloatComplex *A, int lda, aclsolverFloatComplex *B, int ldb,
                                       int *devInfo);
+    /* replaces cann_ops_solver.h:185 (src/cpotri/arch35/cpotri.cpp). Lwork = n*n complex. */
+    aclsolverStatus_t aclsolverCpotri_bufferSize(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n,
+                                                 aclsolverFloatComplex *A, int lda, int *Lwork);
+    /* The selected triangle of A^-1 from a complex Cholesky factor, in place; devInfo = first
+     * invalid factor diagonal (real part <= 0, imaginary part != 0 or non-finite), 1-based,
+     * with A unchanged; replaces cann_ops_solver.h:203 (src/cpotri/arch35/cpotri.cpp). */
+    aclsolverStatus_t aclsolverCpotri(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n,
+                                      aclsolverFloatComplex *A, int lda, aclsolverFloatComplex *Workspace, int Lwork,
+                                      int *devInfo);
     /* Batched complex Cholesky, uniform n; argument errors use infoArray[0];
      * replaces cann_ops_solver.h:224 (src/cpotrf_batched/arch35/cpotrf_batched.cpp:14). */
     aclsolverStatus_t aclsolverCpotrfBatched(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n,
@@ -96,6 +105,11 @@ extern "C"
     /* replaces cann_ops_solver.h:484 (src/cholesky/arch35/cholesky_host.cpp:241). */
     aclsolverStatus_t aclsolverSpotri_bufferSize(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n, float *A,
                                                  int lda, int *Lwork);
+    /* The selected triangle of A^-1 from a real Cholesky factor, in place (Lwork = n*n);
+     * devInfo = first non-positive or non-finite factor diagonal, 1-based, with A unchanged;
+     * replaces cann_ops_solver.h:504 (src/cholesky/arch35/cholesky_host.cpp:277). */
+    aclsolverStatus_t aclsolverSpotri(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n, float *A, int lda,
+                                      float *Workspace, int Lwork, int *devInfo);
     /* Batched in-place Cholesky; a null slot sets only its info to -3; host argument errors
      * fill every info entry; replaces cann_ops_solver.h:524 (cholesky_host.cpp:283). */
     aclsolverStatus_t aclsolverSpotrfBatched(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n, float *Aarray[],

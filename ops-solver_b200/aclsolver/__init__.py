@@ -58,6 +58,8 @@ ARGTYPES = {
     "aclsolverCpotrf_bufferSize": _QUERY,
     "aclsolverCpotrf": [VP, I32, I32, VP, I32, VP, I32, VP],
     "aclsolverCpotrs": [VP, I32, I32, I32, VP, I32, VP, I32, VP],
+    "aclsolverCpotri_bufferSize": _QUERY,
+    "aclsolverCpotri": [VP, I32, I32, VP, I32, VP, I32, VP],
     "aclsolverCpotrfBatched": [VP, I32, I32, VP, I32, VP, I32],
     "aclsolverCpotrsBatched": [VP, I32, I32, I32, VP, I32, VP, I32, VP, I32],
     # real LU

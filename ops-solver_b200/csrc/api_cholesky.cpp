@@ -9,6 +9,8 @@
 // and return INVALID_VALUE; numerical failures are reported in info with SUCCESS.
 #include <algorithm>
 
+#include <vector>
+
 #include "handle.h"
 #include "launch.h"
 
@@ -50,18 +52,48 @@ aclsolverStatus_t info_span(const int *info, int64_t count)
     return ACLSOLVER_STATUS_SUCCESS;
 }
 
-// This build's factorisation needs no caller workspace at any order.
+// This build's factorisation needs no caller workspace at any order; the inverse needs the
+// n x n right-hand side the identity is solved in.
 int required_workspace(int n, bool inverse)
 {
-    (void)n;
-    (void)inverse;
-    return 0;
+    return inverse ? n * n : 0;
 }
 
-cudaError_t factor(const RealBatch &a, int upper, int *info, cudaStream_t s)
+// The single-matrix solve's dispatch (aclsolverSpotrs), info-gated: the kernels skip their
+// work when info[0] != 0.
+cudaError_t single_solve(const RealBatch &a, const RealBatch &b, int nrhs, int uplo, int *info, cudaStream_t s)
 {
-    if (a.n <= 32) return launch_potrf_small(a, upper, info, s);
-    return launch_potrf_mid(a, upper, info, s);
+    if (a.n <= 8) return launch_potrs_small(a, b, nrhs, uplo, info, s);
+    return launch_potrs_generic(a, b, nrhs, uplo, a.n <= 128 ? 1 : 0, info, s);
+}
+
+// Factor dispatch by order: up to 32 the register kernels, up to 256 a block per matrix
+// with the packed triangle in shared memory, above that one matrix at a time over the whole
+// GPU (a backup of the triangle in handle scratch; a batch's pointer table is read back, so
+// that case synchronises with the host).
+aclsolverStatus_t factor(Handle *h, const RealBatch &a, int upper, int *info)
+{
+    cudaStream_t s = h->stream;
+    if (a.n <= 32) return launch_status(launch_potrf_small(a, upper, info, s));
+    if (a.n <= POTRF_PACKED_MAX) return launch_status(launch_potrf_packed(a, upper, info, s));
+    ScratchBlock *blk = acquire_scratch(h, potrf_large_scratch_bytes(a.n));
+    if (!blk) return ACLSOLVER_STATUS_ALLOC_FAILED;
+    cudaError_t e = cudaSuccess;
+    if (!a.table)
+        e = launch_potrf_large(a.single, a.ld, upper, a.n, info, blk->ptr, s);
+    else
+    {
+        std::vector<float *> ptrs((size_t)a.count);
+        e = cudaMemcpyAsync(ptrs.data(), a.table + a.first, (size_t)a.count * sizeof(float *), cudaMemcpyDeviceToHost,
+                            s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        for (int64_t q = 0; q < a.count && e == cudaSuccess; ++q)
+            e = ptrs[q] ? launch_potrf_large(ptrs[q], a.ld, upper, a.n, info + q, blk->ptr, s)
+                        : launch_fill_info(info + q, -3, 1, s);
+    }
+    aclsolverStatus_t launched = launch_status(e);
+    aclsolverStatus_t fin = finish_scratch(h, blk);
+    return launched != ACLSOLVER_STATUS_SUCCESS ? launched : fin;
 }
 
 aclsolverStatus_t query(aclsolverHandle_t handle, int u, int n, float *a, int ld, int *lw, bool inverse)
@@ -100,7 +132,27 @@ extern "C"
         if (error) return arg_error(h, devInfo, error);
         if (!n) return launch_status(launch_fill_info(devInfo, 0, 1, h->stream));
         RealBatch a{A, nullptr, n, lda, 0, 1};
-        return launch_status(factor(a, uplo, devInfo, h->stream));
+        return factor(h, a, uplo, devInfo);
+    }
+
+    aclsolverStatus_t aclsolverSpotri(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n, float *A, int lda,
+                                      float *Workspace, int Lwork, int *devInfo)
+    {
+        if (!handle) return ACLSOLVER_STATUS_HANDLE_IS_NULLPTR;
+        Handle *h = to_handle(handle);
+        const int need = required_workspace(n, true);
+        int error = matrix_error(uplo, n, A, lda, n > 0);
+        if (!error && n > 0 && !Workspace) error = 5;
+        if (!error && (Lwork < 0 || Lwork < need)) error = 6;
+        if (!error && !devInfo) error = 7;
+        if (error) return arg_error(h, devInfo, error);
+        if (!n) return launch_status(launch_fill_info(devInfo, 0, 1, h->stream));
+        RealBatch a{A, nullptr, n, lda, 0, 1};
+        RealBatch w{Workspace, nullptr, n, n, 0, 1};
+        cudaError_t e = launch_potri_prepare(A, lda, n, Workspace, devInfo, h->stream);
+        if (e == cudaSuccess) e = single_solve(a, w, n, uplo, devInfo, h->stream);
+        if (e == cudaSuccess) e = launch_potri_store(A, lda, uplo, n, Workspace, devInfo, h->stream);
+        return launch_status(e);
     }
 
     aclsolverStatus_t aclsolverSpotrfBatched(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n,
@@ -124,7 +176,7 @@ extern "C"
             return ACLSOLVER_STATUS_SUCCESS;
         }
         RealBatch a{nullptr, Aarray, n, lda, 0, count};
-        return launch_status(factor(a, uplo, infoArray, h->stream));
+        return factor(h, a, uplo, infoArray);
     }
 
     aclsolverStatus_t aclsolverSpotrs(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n, int nrhs,
@@ -147,10 +199,7 @@ extern "C"
         {
             RealBatch a{const_cast<float *>(A), nullptr, n, lda, 0, 1};
             RealBatch b{B, nullptr, n, ldb, 0, 1};
-            if (n <= 8)
-                e = launch_potrs_small(a, b, nrhs, uplo, devInfo, h->stream);
-            else
-                e = launch_potrs_generic(a, b, nrhs, uplo, n <= 128 ? 1 : 0, devInfo, h->stream);
+            e = single_solve(a, b, nrhs, uplo, devInfo, h->stream);
         }
         return launch_status(e);
     }

@@ -125,6 +125,40 @@ extern "C"
         return launch_status(launch_cpotrf(reinterpret_cast<float2 *>(A), nullptr, n, lda, uplo, 1, devInfo, h->stream));
     }
 
+    aclsolverStatus_t aclsolverCpotri_bufferSize(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n,
+                                                 aclsolverFloatComplex *A, int lda, int *Lwork)
+    {
+        if (!handle) return ACLSOLVER_STATUS_NOT_INITIALIZED;
+        if (factor_arg(uplo, n, A, lda, false) || !Lwork) return ACLSOLVER_STATUS_INVALID_VALUE;
+        *Lwork = n * n;  // the identity the factor is solved against
+        return ACLSOLVER_STATUS_SUCCESS;
+    }
+
+    aclsolverStatus_t aclsolverCpotri(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n,
+                                      aclsolverFloatComplex *A, int lda, aclsolverFloatComplex *Workspace, int Lwork,
+                                      int *devInfo)
+    {
+        int arg = factor_arg(uplo, n, A, lda, false);
+        const int required = n * n;
+        if (!arg && !Workspace && n > 0) arg = 5;
+        if (!arg && Lwork < required) arg = 6;
+        if (!arg && !devInfo) arg = 7;
+        if (devInfo)
+        {
+            aclsolverStatus_t span = info_span(devInfo, 1);
+            if (span != ACLSOLVER_STATUS_SUCCESS) return span;
+        }
+        aclsolverStatus_t st = finish(handle, devInfo, arg);
+        if (st != ACLSOLVER_STATUS_SUCCESS || n == 0) return st;
+        Handle *h = to_handle(handle);
+        float2 *a = reinterpret_cast<float2 *>(A);
+        float2 *w = reinterpret_cast<float2 *>(Workspace);
+        cudaError_t e = launch_cpotri_prepare(a, lda, n, w, devInfo, h->stream);
+        if (e == cudaSuccess) e = launch_cpotrs(a, nullptr, w, nullptr, n, lda, n, n, uplo, 1, devInfo, h->stream);
+        if (e == cudaSuccess) e = launch_cpotri_store(a, lda, uplo, n, w, devInfo, h->stream);
+        return launch_status(e);
+    }
+
     aclsolverStatus_t aclsolverCpotrs(aclsolverHandle_t handle, aclsolverFillMode_t uplo, int n, int nrhs,
                                       const aclsolverFloatComplex *A, int lda, aclsolverFloatComplex *B, int ldb,
                                       int *devInfo)

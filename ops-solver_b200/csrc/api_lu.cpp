@@ -376,7 +376,20 @@ extern "C"
             st = check_finite(h, a, n, devInfo, 1, 2);
             if (st != ACLSOLVER_STATUS_SUCCESS) return st;
         }
-        if (n > SMALL_N) return ACLSOLVER_STATUS_NOT_SUPPORTED;
+        if (n > SMALL_N)
+        {
+            // above the register-resident orders: the factors copied to the workspace, A set to
+            // the identity and solved in place by the blocked solve (the batched entry's path)
+            ScratchBlock *blk = acquire_scratch(h, getri_blocked_scratch_bytes(n, 1));
+            if (!blk) return ACLSOLVER_STATUS_ALLOC_FAILED;
+            RealBatch w{Workspace, nullptr, n, n, 0, 1};
+            cudaError_t e = launch_copy_matrices(a, w, n, h->stream);
+            if (e == cudaSuccess)
+                e = launch_getri_blocked(w, identity ? nullptr : devIpiv, a, devInfo, blk->ptr, h->stream);
+            aclsolverStatus_t launched = launch_status(e);
+            aclsolverStatus_t fin = finish_scratch(h, blk);
+            return launched != ACLSOLVER_STATUS_SUCCESS ? launched : fin;
+        }
         return launch_status(launch_getri_small(a, identity ? nullptr : devIpiv, a, devInfo, h->stream));
     }
 

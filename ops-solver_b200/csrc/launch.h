@@ -27,6 +27,15 @@ struct RealBatch
 cudaError_t launch_fill_info(int *info, int value, int64_t count, cudaStream_t stream);
 // SpotrsBatched slot scan: info[0] = -4 if any A slot is null, else -6 if any B slot is
 // null, else 0 (cholesky_simt.cpp:28-48 contract).
+// The inverse from a Cholesky factor (potri.cu): diagonal check into info[0] and the n x n
+// identity into w (ld n); then, after the solve, the selected triangle of A from w's lower
+// triangle when info[0] == 0.
+cudaError_t launch_potri_prepare(const float *a, int lda, int n, float *w, int *info, cudaStream_t stream);
+cudaError_t launch_potri_store(float *a, int lda, int upper, int n, const float *w, const int *info,
+                               cudaStream_t stream);
+cudaError_t launch_cpotri_prepare(const float2 *a, int lda, int n, float2 *w, int *info, cudaStream_t stream);
+cudaError_t launch_cpotri_store(float2 *a, int lda, int upper, int n, const float2 *w, const int *info,
+                                cudaStream_t stream);
 // flags: two device words that are zero on entry (left zero on exit).
 cudaError_t launch_solve_slot_check(int *info, float *const *a, float *const *b, int count, int *flags,
                                     cudaStream_t stream);
@@ -34,6 +43,13 @@ cudaError_t launch_solve_slot_check(int *info, float *const *a, float *const *b,
 cudaError_t launch_potrf_small(const RealBatch &a, int upper, int *info, cudaStream_t stream);
 // In-place Cholesky of n > 32 matrices (FMA order, left-looking), per-slot info.
 cudaError_t launch_potrf_mid(const RealBatch &a, int upper, int *info, cudaStream_t stream);
+// Real Cholesky above order 32 (potrf_blocked.cu): a block per matrix with the packed
+// triangle in shared memory up to POTRF_PACKED_MAX; above, one matrix over the whole GPU
+// (scratch: potrf_large_scratch_bytes, a backup of the lower triangle).
+constexpr int POTRF_PACKED_MAX = 256;
+cudaError_t launch_potrf_packed(const RealBatch &a, int upper, int *info, cudaStream_t stream);
+size_t potrf_large_scratch_bytes(int n);
+cudaError_t launch_potrf_large(float *A, int lda, int upper, int n, int *info, void *scratch, cudaStream_t stream);
 // Cholesky solve for n > 32: dot-accumulate order (dot_order = 1) or right-looking order.
 cudaError_t launch_potrs_generic(const RealBatch &a, const RealBatch &b, int nrhs, int upper, int dot_order,
                                  const int *info, cudaStream_t stream);

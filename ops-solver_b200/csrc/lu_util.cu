@@ -121,14 +121,14 @@ namespace
 // Per matrix: info for the inverse above the small orders, in the small path's convention
 // (-2 a null A or C slot, -4 a pivot outside [k+1, n], else the first zero diagonal of U,
 // 1-based, else 0); C set to the identity where the inverse is computed; fail[q] = info != 0.
-__global__ void getri_prepare_kernel(float *const *a_table, const int *ipiv, float *const *c_table, int n, int lda,
-                                     int ldc, int count, int *info, int *fail)
+__global__ void getri_prepare_kernel(float *a_single, float *const *a_table, const int *ipiv, float *c_single,
+                                     float *const *c_table, int n, int lda, int ldc, int count, int *info, int *fail)
 {
     __shared__ int bad, zero;
     const int64_t q = blockIdx.x;
     if (q >= count) return;
-    const float *A = slot(a_table, q);
-    float *C = slot(c_table, q);
+    const float *A = a_table ? slot(a_table, q) : a_single;
+    float *C = c_table ? slot(c_table, q) : c_single;
     if (threadIdx.x == 0)
     {
         bad = 0;
@@ -171,7 +171,8 @@ cudaError_t launch_getri_blocked(const RealBatch &a, const int *ipiv, const Real
     const int n = a.n, count = a.count;
     int *fail = static_cast<int *>(scratch);
     int *skip = fail + count;
-    getri_prepare_kernel<<<count, 256, 0, stream>>>(a.table, ipiv, c.table, n, a.ld, c.ld, count, info, fail);
+    getri_prepare_kernel<<<count, 256, 0, stream>>>(a.single, a.table, ipiv, c.single, c.table, n, a.ld, c.ld, count,
+                                                    info, fail);
     const int64_t total = (int64_t)count * n;
     getri_skip_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(fail, n, count, skip);
     cudaError_t e = cudaGetLastError();

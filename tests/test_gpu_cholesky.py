@@ -204,3 +204,100 @@ def test_repeat_calls_are_bitwise_identical(handle):
         st, dm, info = potrf_batched(handle, a, False)
         outs.append(dm.read())
     assert same_bits(outs[0], outs[1]) and same_bits(outs[1], outs[2])
+
+
+@pytest.mark.parametrize("upper", [False, True])
+@pytest.mark.parametrize("n", [1, 5, 8, 9, 32, 33, 100, 129, 300])
+def test_spotri_matches_the_solve_of_the_identity(handle, n, upper):
+    """aclsolverSpotri: the selected triangle of A^-1 from the factor, in place -- the
+    reference's solve of L L^T X = I (cholesky_simt.cpp:220-254) with this build's single
+    solve, so bit for bit the oracle's Spotrs on the identity; the other triangle and the
+    padding untouched; close to the FP64 inverse."""
+    import torch
+
+    lib = aclsolver.library()
+    a = spd_batch(1, n, seed=13 * n + int(upper))
+    f, winfo = oracle.spotrf_batched(a, upper=upper)
+    assert winfo[0] == 0
+    tri = np.triu(f[0]) if upper else np.tril(f[0])
+    other = np.tril(np.full((n, n), 7.5, dtype=np.float32), -1) if upper else np.triu(np.full((n, n), 7.5, dtype=np.float32), 1)
+    dm = DeviceMatrices((tri + other)[None], ld=n + 2)
+    lw = C.c_int(-1)
+    assert lib.aclsolverSpotri_bufferSize(handle.value, int(upper), n, dm.ptr, dm.ld, C.byref(lw)) == aclsolver.SUCCESS
+    work = torch.empty(max(1, lw.value), dtype=torch.float32, device="cuda")
+    info = info_buffer(1)
+    st = lib.aclsolverSpotri(handle.value, int(upper), n, dm.ptr, dm.ld, work.data_ptr(), lw.value, info.data_ptr())
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 0
+    got = dm.read()[0]
+    x = oracle.spotrs_batched(f, np.eye(n, dtype=np.float32)[None], upper=upper, single=True)[0]
+    want = np.triu(x.T) if upper else np.tril(x)
+    got_tri = np.triu(got) if upper else np.tril(got)
+    assert same_bits(got_tri, want), first_mismatch(got_tri, want)
+    assert np.array_equal(got - got_tri, other), "the other triangle must stay intact"
+    inv64 = np.linalg.inv(a[0].astype(np.float64))
+    ref_tri = np.triu(inv64) if upper else np.tril(inv64)
+    assert np.abs(got_tri - ref_tri).max() <= 1e-4 * np.abs(inv64).max()
+
+
+def test_spotri_bad_diagonal_leaves_a_unchanged(handle):
+    import torch
+
+    lib = aclsolver.library()
+    n = 40
+    f, _ = oracle.spotrf_batched(spd_batch(1, n, seed=2))
+    f = np.tril(f)
+    f[0, 17, 17] = -1.0
+    dm = DeviceMatrices(f, ld=n)
+    work = torch.empty(n * n, dtype=torch.float32, device="cuda")
+    info = info_buffer(1)
+    st = lib.aclsolverSpotri(handle.value, 0, n, dm.ptr, n, work.data_ptr(), n * n, info.data_ptr())
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 18
+    assert dm.unchanged()
+    info = info_buffer(1)
+    st = lib.aclsolverSpotri(handle.value, 0, n, dm.ptr, n, work.data_ptr(), n * n - 1, info.data_ptr())
+    assert st == aclsolver.INVALID_VALUE and int(info.cpu()[0]) == -6
+
+
+@pytest.mark.parametrize("n,upper", [(257, False), (300, True), (513, False), (1024, False), (2048, False),
+                                     (4096, False)])
+def test_spotrf_large_matches_oracle(handle, n, upper):
+    """Above order 256 one matrix runs over the whole GPU (diagonal block, panel rows and a
+    TMA-fed lower-triangle update per 32-column panel): bit for bit the oracle's FMA order."""
+    lib = aclsolver.library()
+    a = spd_batch(1, n, seed=n + int(upper))
+    da = DeviceMatrices(a, ld=n + (4 if n % 2 == 0 else 1))
+    info = info_buffer(1)
+    st = lib.aclsolverSpotrf(handle.value, int(upper), n, da.ptr, da.ld, None, 0, info.data_ptr())
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 0
+    want, winfo = oracle.spotrf_batched(a, upper=upper)
+    got = da.read()
+    tri = (lambda m: np.triu(m)) if upper else (lambda m: np.tril(m))
+    assert same_bits(tri(got[0]), tri(want[0])), first_mismatch(tri(got[0]), tri(want[0]))
+    assert np.array_equal(got[0] - tri(got[0]), a[0] - tri(a[0])), "the other triangle must stay intact"
+
+
+@pytest.mark.parametrize("n,bad", [(300, 100), (300, 290), (520, 33), (520, 511)])
+def test_spotrf_large_failure_keeps_unfinished_columns(handle, n, bad):
+    lib = aclsolver.library()
+    a = spd_batch(1, n, seed=4)
+    a[0, bad, bad] = -1.0
+    da = DeviceMatrices(a, ld=n)
+    info = info_buffer(1)
+    st = lib.aclsolverSpotrf(handle.value, 0, n, da.ptr, n, None, 0, info.data_ptr())
+    handle.stream.synchronize()
+    want, winfo = oracle.spotrf_batched(a)
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == int(winfo[0]) > 0
+    got = da.read()
+    assert same_bits(np.tril(got[0]), np.tril(want[0])), first_mismatch(np.tril(got[0]), np.tril(want[0]))
+
+
+def test_spotrf_batched_above_packed_orders(handle):
+    a = spd_batch(3, 300, seed=12)
+    a[1, 150, 150] = 0.0
+    st, dm, info = potrf_batched(handle, a, False)
+    want, winfo = oracle.spotrf_batched(a)
+    assert st == aclsolver.SUCCESS and info.tolist() == winfo.tolist()
+    assert same_bits(np.tril(dm.read()), np.tril(want))

@@ -188,3 +188,54 @@ def test_cpotrf_cpotrs_single(handle, n, nrhs):
     handle.stream.synchronize()
     assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 0
     assert cbits(db.read(), oracle.cpotrs_batched(want, b))
+
+
+@pytest.mark.parametrize("upper", [False, True])
+@pytest.mark.parametrize("n", [1, 7, 16, 17, 64, 100, 128, 140])
+def test_cpotri_matches_the_solve_of_the_identity(handle, n, upper):
+    """aclsolverCpotri: the selected triangle of A^-1 from a complex factor, in place, as the
+    solve of L L^H X = I (the reference's cpotri, src/cpotri/arch35/cpotri.cpp) with this
+    build's solve: bit for bit the oracle's cpotrs on the identity, Hermitian mirror in upper
+    storage, padding untouched, close to the FP64 inverse."""
+    import torch
+
+    lib = aclsolver.library()
+    a = hpd(1, n, seed=3 * n + int(upper))
+    f, winfo = oracle.cpotrf_batched(a, upper=upper)
+    assert winfo[0] == 0
+    tri = np.triu(f[0]) if upper else np.tril(f[0])
+    dm = CMatrices(tri[None], n + 1)
+    lw = C.c_int(-1)
+    assert lib.aclsolverCpotri_bufferSize(handle.value, int(upper), n, dm.table[0].item(), dm.ld,
+                                         C.byref(lw)) == aclsolver.SUCCESS
+    work = torch.empty(2 * max(1, lw.value), dtype=torch.float32, device="cuda")
+    info = info_buffer(1)
+    st = lib.aclsolverCpotri(handle.value, int(upper), n, dm.table[0].item(), dm.ld, work.data_ptr(), lw.value,
+                             info.data_ptr())
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 0
+    got = dm.read()[0]
+    x = oracle.cpotrs_batched(f, np.eye(n, dtype=np.complex64)[None], upper=upper)[0]
+    want = np.triu(np.conj(x.T)) if upper else np.tril(x)
+    got_tri = np.triu(got) if upper else np.tril(got)
+    assert cbits(got_tri, want)
+    inv64 = np.linalg.inv(a[0].astype(np.complex128))
+    ref = np.triu(inv64) if upper else np.tril(inv64)
+    assert np.abs(got_tri - ref).max() <= 1e-4 * np.abs(inv64).max()
+
+
+def test_cpotri_invalid_diagonal(handle):
+    import torch
+
+    lib = aclsolver.library()
+    n = 20
+    f, _ = oracle.cpotrf_batched(hpd(1, n, seed=9))
+    f = np.tril(f)
+    f[0, 6, 6] = 1.0 + 0.5j  # a non-zero imaginary part on the diagonal
+    dm = CMatrices(f, n)
+    work = torch.empty(2 * n * n, dtype=torch.float32, device="cuda")
+    info = info_buffer(1)
+    st = lib.aclsolverCpotri(handle.value, 0, n, dm.table[0].item(), n, work.data_ptr(), n * n, info.data_ptr())
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 7
+    assert dm.unchanged()

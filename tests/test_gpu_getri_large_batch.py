@@ -106,3 +106,60 @@ def test_sgetrf_batched_above_512_matches_oracle(handle):
     assert np.array_equal(ipiv[[0, 2]], wpiv)
     assert same_bits(got[[0, 2]], lu), first_mismatch(got[[0, 2]], lu)
     assert np.array_equal(got[1], a[1])
+
+
+@pytest.mark.parametrize("n,pivoting", [(65, True), (200, True), (129, False), (1000, True)])
+def test_getri_single_above_small_orders(handle, n, pivoting):
+    """aclsolverSgetri (in place, caller workspace) above order 64: the factors copied to the
+    workspace, A solved against the identity; tolerance against the oracle's inverse and
+    FP64, the workspace query and info conventions of the small path."""
+    import ctypes as C
+
+    lib = aclsolver.library()
+    # without pivoting, a diagonally dominant matrix keeps the factors' growth small
+    a = gaussian(1, n, seed=3 * n) + (3 if pivoting else 2 * n) * np.eye(n, dtype=np.float32)
+    lu, ipiv, _ = oracle.sgetrf_batched(a, pivoting=pivoting)
+    dm = DeviceMatrices(lu, ld=n + 3)
+    lw = C.c_int(-1)
+    assert lib.aclsolverSgetri_bufferSize(handle.value, n, dm.ptr, dm.ld, C.byref(lw)) == aclsolver.SUCCESS
+    assert lw.value >= n * n
+    work = torch.empty(lw.value, dtype=torch.float32, device="cuda")
+    piv = device_ints(ipiv[0]) if pivoting else None
+    info = info_buffer(1)
+    st = lib.aclsolverSgetri(handle.value, n, dm.ptr, dm.ld, None if piv is None else piv.data_ptr(),
+                             work.data_ptr(), lw.value, info.data_ptr())
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 0
+    got = dm.read()[0]
+    want, _ = oracle.sgetri_batched(lu, ipiv if pivoting else None)
+    scale = np.abs(want[0]).max()
+    assert np.abs(got - want[0]).max() <= 1e-4 * scale
+
+    # the reference's inverse residual gate: ||I - A X||_1 / (n ||A||_1 ||X||_1 eps) within
+    # max(5 x the FP32 oracle's ratio, 0.1) (test/cholesky/lapack_residual.py, INVERSE floor)
+    def ratio(x):
+        a64, x64 = a[0].astype(np.float64), x.astype(np.float64)
+        norm1 = lambda m: np.abs(m).sum(axis=0).max()
+        return norm1(np.eye(n) - a64 @ x64) / (n * norm1(a64) * norm1(x64) * np.finfo(np.float32).eps)
+
+    assert ratio(got) <= max(5 * ratio(want[0]), 0.1)
+
+
+def test_getri_single_zero_diagonal(handle):
+    import ctypes as C
+
+    lib = aclsolver.library()
+    aclsolver.check(lib.aclsolverSetDeviceChecks(handle.value, 0))
+    n = 100
+    a = gaussian(1, n, seed=8) + 3 * np.eye(n, dtype=np.float32)
+    lu, ipiv, _ = oracle.sgetrf_batched(a)
+    lu[0, 40, 40] = 0.0
+    dm = DeviceMatrices(lu, ld=n)
+    work = torch.empty(n * n, dtype=torch.float32, device="cuda")
+    piv = device_ints(ipiv[0])
+    info = info_buffer(1)
+    st = lib.aclsolverSgetri(handle.value, n, dm.ptr, n, piv.data_ptr(), work.data_ptr(), n * n, info.data_ptr())
+    handle.stream.synchronize()
+    aclsolver.check(lib.aclsolverSetDeviceChecks(handle.value, 1))
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 41
+    assert dm.unchanged(), "a singular factor is left as it was"
