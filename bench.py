@@ -907,6 +907,7 @@ def measure_large(handle, args, steps=3):
                   "iterations": int(iters.item()), "berr_reported": float(berr.item())},
         "mixed_over_plain": round(plain_ms / mixed_ms, 3),
     }
+    out["cholesky"] = measure_spotrf_large(handle, args)
     if args is not None and args.cpu_seconds > 0:
         from oracle import host_lapack
 
@@ -920,6 +921,56 @@ def measure_large(handle, args, steps=3):
         out["cpu_baseline"] = dict(host_lapack.describe(threads), value=round(1.0 / dt, 3), unit="solves/s",
                                    ms=round(dt * 1e3, 1), kind="openblas", berr_max=be, ferr_max=fe, info=int(st),
                                    sample=f"one sgetrf + sgetrs ({nrhs} RHS, FP32 LAPACKE), OpenBLAS on {threads} threads")
+    return out
+
+
+def measure_spotrf_large(handle, args, n=4096, steps=3):
+    """One 4096 x 4096 SPD matrix, A = G G^T / n + I (G ~ N(0,1) on the GPU, seed 7), lower:
+    aclsolverSpotrf over the whole GPU (32-column panels, TMA-fed lower-triangle updates),
+    device time of the call with the matrix restored before each repetition."""
+    import torch
+
+    import aclsolver
+
+    lib = aclsolver.library()
+    g = torch.Generator(device="cuda").manual_seed(7)
+    G = torch.randn(n, n, device="cuda", generator=g)
+    A0 = (G @ G.T / n + torch.eye(n, device="cuda")).contiguous()  # symmetric: its own column-major form
+    del G
+    A = torch.empty_like(A0)
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    stream = handle.stream
+    times = []
+    for _ in range(steps + 1):
+        A.copy_(A0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        aclsolver.check(lib.aclsolverSpotrf(handle.value, 0, n, A.data_ptr(), n, None, 0, info.data_ptr()))
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    assert int(info.item()) == 0
+    ms = sorted(times[1:])[len(times[1:]) // 2]
+    # backward error of the factor: ||A - L L^T||_1 / ||A||_1 in FP64
+    L = torch.triu(A).T.double()  # the column-major lower factor seen through torch's row-major view
+    a64 = A0.double()
+    rel = float((a64 - L @ L.T).abs().sum(dim=0).max() / a64.abs().sum(dim=0).max())
+    out = {"workload": f"one {n} x {n} SPD matrix (G G^T / n + I), lower: aclsolverSpotrf",
+           "ms": round(ms, 3), "gflops": round(n ** 3 / 3 / (ms * 1e-3) / 1e9, 1),
+           "roofline": roofline(2.0 * n * (n + 1) / 2 * 4, n ** 3 / 3, ms, "potrf_syrk_kernel + diag + rows (per panel)"),
+           "factor_residual": rel}
+    if args is not None and args.cpu_seconds > 0:
+        from oracle import host_lapack
+
+        a_h = A0.cpu().numpy().reshape(-1)
+        threads = host_lapack.max_threads()
+        t0 = time.perf_counter()
+        _, st = host_lapack.spotrf(n, a_h, threads=threads)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = dict(host_lapack.describe(threads), value=round(1.0 / dt, 3), unit="factorisations/s",
+                                   ms=round(dt * 1e3, 1), kind="openblas", info=int(st),
+                                   sample=f"one spotrf of the same matrix, OpenBLAS on {threads} threads")
     return out
 
 

@@ -42,7 +42,6 @@ cudaError_t launch_solve_slot_check(int *info, float *const *a, float *const *b,
 // In-place Cholesky of n <= 32 matrices, per-slot info (null slot -> -3).
 cudaError_t launch_potrf_small(const RealBatch &a, int upper, int *info, cudaStream_t stream);
 // In-place Cholesky of n > 32 matrices (FMA order, left-looking), per-slot info.
-cudaError_t launch_potrf_mid(const RealBatch &a, int upper, int *info, cudaStream_t stream);
 // Real Cholesky above order 32 (potrf_blocked.cu): a block per matrix with the packed
 // triangle in shared memory up to POTRF_PACKED_MAX; above, one matrix over the whole GPU
 // (scratch: potrf_large_scratch_bytes, a backup of the lower triangle).

@@ -16,13 +16,13 @@
 // diagonal so the square roots need no second exchange.  Untouched columns stay untouched,
 // which keeps the failure contract for free.
 //
-// n > 256 (one matrix over the whole GPU, 32-column panels): the matrix is first copied to
+// n > 256 (one matrix over the whole GPU, 64-column panels): the matrix is first copied to
 // a backup; per panel
-//   diag:  one block factors the 32 x 32 diagonal block in shared memory (right-looking);
+//   diag:  one block factors the 64 x 64 diagonal block in shared memory (right-looking);
 //   rows:  a thread per row below it forms L21 = A21 L11^-T row by row (ascending k, IEEE
 //          division by the diagonal), 128 rows per block;
 //   syrk:  the trailing lower triangle takes A22 -= L21 L21^T over 64 x 64 tiles (lower tiles
-//          only), each tile's two 64 x 32 operand panels loaded by TMA (a 2-D tensor map of
+//          only), each tile's two 64 x 64 operand panels loaded by TMA (a 2-D tensor map of
 //          the matrix, completion on an mbarrier with a bounded wait) when the matrix is
 //          16-byte aligned with lda % 4 == 0, by plain loads otherwise; FP32 FMAs in ascending
 //          k into a 4 x 4 register tile per thread.
@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(T) potrf_packed_kernel(float *single, float *c
 // ---------------------------------------------------------------------------------------
 // n > 256: right-looking 32-column panels over the whole GPU
 // ---------------------------------------------------------------------------------------
-constexpr int PB = 32;        // panel width
+constexpr int PB = 64;        // panel width
 constexpr int ST = 64;        // syrk tile (rows and columns)
 constexpr int ROWS_T = 128;   // panel rows per block
 constexpr long long WAIT_LIMIT = 1ll << 20;  // mbarrier try_wait rounds before giving up
@@ -185,7 +185,7 @@ constexpr long long WAIT_LIMIT = 1ll << 20;  // mbarrier try_wait rounds before 
 // wait ran out.  Kernels read it first and return when it is set.
 __device__ __forceinline__ int stopped(const int *info) { return *(volatile const int *)info; }
 
-// The 32 x 32 diagonal block at k0, right-looking in shared memory.
+// The 64 x 64 diagonal block at k0, right-looking in shared memory.
 __global__ void __launch_bounds__(256) potrf_diag_kernel(float *A, int lda, int upper, int k0, int n, int *info)
 {
     __shared__ float D[PB][PB + 1];  // D[j][i] = element (k0 + i, k0 + j), i >= j
@@ -367,15 +367,33 @@ __global__ void __launch_bounds__(256) potrf_syrk_kernel(const __grid_constant__
     }
     // thread (tr, tc): rows r0 + 4 tr .. +3, columns c0 + 4 tc .. +3
     const int tr = t & 15, tc = t >> 4;
+    const int i0 = r0 + 4 * tr;
+    // a thread's four rows in one 16-byte piece per column when the matrix is aligned (rows
+    // start at multiples of 4) and the piece lies wholly below the diagonal and inside n
+    const bool vec = tma && i0 + 3 < n && c0 + 4 * tc + 3 <= i0;
     float c[4][4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v)
+    for (int v = 0; v < 4; ++v)
+    {
+        const int j = c0 + 4 * tc + v;
+        if (vec)
         {
-            const int i = r0 + 4 * tr + u, j = c0 + 4 * tc + v;
-            c[u][v] = (i < n && j <= i) ? A[tri_at(lda, upper, i, j)] : 0.0f;
+            const float4 x = *reinterpret_cast<const float4 *>(A + (int64_t)j * lda + i0);
+            c[0][v] = x.x;
+            c[1][v] = x.y;
+            c[2][v] = x.z;
+            c[3][v] = x.w;
         }
+        else
+        {
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+            {
+                const int i = i0 + u;
+                c[u][v] = (i < n && j <= i) ? A[tri_at(lda, upper, i, j)] : 0.0f;
+            }
+        }
+    }
 #pragma unroll 8
     for (int k = 0; k < PB; ++k)
     {
@@ -389,13 +407,21 @@ __global__ void __launch_bounds__(256) potrf_syrk_kernel(const __grid_constant__
             for (int v = 0; v < 4; ++v) c[u][v] = fma_rn(-ar[u], bc[v], c[u][v]);
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v)
+    for (int v = 0; v < 4; ++v)
+    {
+        const int j = c0 + 4 * tc + v;
+        if (vec)
+            *reinterpret_cast<float4 *>(A + (int64_t)j * lda + i0) = make_float4(c[0][v], c[1][v], c[2][v], c[3][v]);
+        else
         {
-            const int i = r0 + 4 * tr + u, j = c0 + 4 * tc + v;
-            if (i < n && j <= i) A[tri_at(lda, upper, i, j)] = c[u][v];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+            {
+                const int i = i0 + u;
+                if (i < n && j <= i) A[tri_at(lda, upper, i, j)] = c[u][v];
+            }
         }
+    }
 }
 
 // Backup copy of the lower triangle (element (i, j) at W[j * n + i]) and its restore of the

@@ -1,13 +1,5 @@
-// potrf_generic.cu -- real Cholesky factor and solve for 32 < n <= 4096, any batch.
-//
-// Factor (FMA order): left-looking, one block per matrix.  Column j's entries are formed
-// as a_ij = fma(-l_ik, l_jk, a_ij) over ascending k < j -- the same per-element sequence as
-// the right-looking FMA order of the oracle (orc_spotrf_fma), so both give identical bits
-// -- then checked (d > 0 and finite), square-rooted (IEEE) and divided (IEEE).  Columns at
-// and beyond a failed pivot are never written, so they keep the caller's input (the
-// reference's left-looking batched path keeps the unfactored triangle the same way).
-// The finished part of the factor is read back from global memory (L1/L2 resident for
-// the column block being formed); the column under construction lives in shared memory.
+// potrf_generic.cu -- real Cholesky solve for 32 < n <= 4096, any batch (the factorisation
+// above order 32 is in potrf_blocked.cu).
 //
 // Solve orders (the parity contract, oracle orc_spotrs):
 //   DOT   (33..128): dot accumulators, x_k = (b_k - dot_k) / l_kk   (cholesky_vector.cpp:30-122)
@@ -20,52 +12,10 @@ namespace ops_solver
 namespace
 {
 constexpr int GT = 256;
-constexpr float FLT_MAX_VALUE = 3.402823466e38F;
 
 __device__ __forceinline__ int64_t tri(int lda, int upper, int i, int j)
 {
     return upper ? (int64_t)i * lda + j : (int64_t)j * lda + i;
-}
-
-__global__ void __launch_bounds__(GT) potrf_left_kernel(float *single, float *const *table, int first, int n, int lda,
-                                                        int upper, int count, int *info)
-{
-    extern __shared__ float col[];  // n floats
-    __shared__ int failed;
-    for (int64_t q = blockIdx.x; q < count; q += gridDim.x)
-    {
-        float *p = table ? slot(table, first + q) : single;
-        if (!p)
-        {
-            if (threadIdx.x == 0) info[q] = -3;
-            continue;
-        }
-        if (threadIdx.x == 0) failed = 0;
-        __syncthreads();
-        for (int j = 0; j < n; ++j)
-        {
-            for (int i = j + threadIdx.x; i < n; i += GT)
-            {
-                float v = p[tri(lda, upper, i, j)];
-                for (int k = 0; k < j; ++k) v = fma_rn(-p[tri(lda, upper, i, k)], p[tri(lda, upper, j, k)], v);
-                col[i] = v;
-            }
-            __syncthreads();
-            const float d = col[j];
-            if (!(d > 0.0f && d <= FLT_MAX_VALUE))
-            {
-                if (threadIdx.x == 0) failed = j + 1;
-                __syncthreads();
-                break;
-            }
-            const float s = sqrt_rn(d);
-            for (int i = j + threadIdx.x; i < n; i += GT) p[tri(lda, upper, i, j)] = i == j ? s : div_rn(col[i], s);
-            __syncthreads();
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) info[q] = failed;
-        __syncthreads();
-    }
 }
 
 constexpr int ORDER_DOT = 1;
@@ -152,18 +102,6 @@ unsigned grid_for(int count)
     return (unsigned)g;
 }
 }  // namespace
-
-cudaError_t launch_potrf_mid(const RealBatch &a, int upper, int *info, cudaStream_t stream)
-{
-    size_t smem = (size_t)a.n * sizeof(float);
-    if (smem > 48 * 1024)
-    {
-        cudaFuncSetAttribute(potrf_left_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    }
-    potrf_left_kernel<<<grid_for(a.count), GT, smem, stream>>>(a.single, a.table, a.first, a.n, a.ld, upper, a.count,
-                                                               info);
-    return cudaGetLastError();
-}
 
 cudaError_t launch_potrs_generic(const RealBatch &a, const RealBatch &b, int nrhs, int upper, int dot_order,
                                  const int *info, cudaStream_t stream)

@@ -53,6 +53,7 @@ def lib():
         h.lh_getrf_getrs_batched.argtypes = [_i, _i, _F, _F, _F, _F, C.c_void_p, _I, _i, _I, _i]
         h.lh_cpotrf_cpotrs_vbatched.argtypes = [_I, _L, _L, _F, _F, _F, _F, _i, _i, _I, _i]
         h.lh_sgesv_single.argtypes = [_i, _i, _F, _F, _F, _F, _I, _i]
+        h.lh_spotrf_single.argtypes = [_i, _F, _F, _i]
         if h.lh_open(str(openblas_path()).encode()) != 0:
             raise RuntimeError(f"could not load the LAPACKE symbols from {openblas_path()}")
         _lib = h
@@ -113,3 +114,10 @@ def sgesv(n, nrhs, a, b, threads=0):
     ipiv = np.zeros(n, dtype=np.int32)
     st = lib().lh_sgesv_single(n, nrhs, a, w, b, x, ipiv, threads or max_threads())
     return x, st
+
+
+def spotrf(n, a, threads=0):
+    """One matrix: spotrf (lower) with OpenBLAS threaded; returns (factor, info)."""
+    w = np.empty_like(a)
+    st = lib().lh_spotrf_single(n, a, w, threads or max_threads())
+    return w, st

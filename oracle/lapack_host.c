@@ -158,3 +158,13 @@ int lh_sgesv_single(int n, int nrhs, const float *a, float *w, const float *b, f
     set_threads(1);
     return st;
 }
+
+/* One large SPD matrix: spotrf (lower) with OpenBLAS threaded (blas_threads). */
+int lh_spotrf_single(int n, const float *a, float *w, int blas_threads)
+{
+    set_threads(blas_threads);
+    memcpy(w, a, sizeof(float) * (int64_t)n * n);
+    int st = spotrf(COL_MAJOR, 'L', n, w, n);
+    set_threads(1);
+    return st;
+}
