@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(RS_THREADS) getrs_small_kernel(float *a_single
 constexpr int RI_THREADS = 64;
 
 template <int N>
-__global__ void __launch_bounds__(RI_THREADS) getri_small_kernel(float *a_single, float *const *a_table,
+__global__ void __launch_bounds__(RI_THREADS, 6) getri_small_kernel(float *a_single, float *const *a_table,
                                                                   int a_first, const int *ipiv, float *c_single,
                                                                   float *const *c_table, int c_first, int n, int lda,
                                                                   int ldc, int count, int *info)
@@ -433,45 +433,40 @@ __global__ void __launch_bounds__(RI_THREADS) getri_small_kernel(float *a_single
             }
         const int failed = bad_pivot[m] ? -4 : (zero_at[m] == 0x7fffffff ? 0 : zero_at[m]);
 
-        float rhs[N];
+        // the right-hand side in pairs of rows, r2[c] = (rhs[2c], rhs[2c + 1]); every update is
+        // rhs_i = fma(-s, a_ik, rhs_i), two rows per paired FMA (lane by lane the same rounding)
+        f32x2 r2[N / 2];
 #pragma unroll
-        for (int i = 0; i < N; ++i) rhs[i] = i == t ? 1.0f : 0.0f;
+        for (int c = 0; c < N / 2; ++c) r2[c] = f2_pack(2 * c == t ? 1.0f : 0.0f, 2 * c + 1 == t ? 1.0f : 0.0f);
         const int kstart = (t / 32) * 32;  // warp-uniform: rows below the warp's first row are zero
-        // forward, unit lower
+        // forward, unit lower; the pivot row's partner row (k + 1 for even k) separately
 #pragma unroll
         for (int k = 0; k < N; ++k)
         {
             if (k >= kstart && k < n)
             {
-                const float s = rhs[k];
+                const float s = (k & 1) ? f2_hi(r2[k / 2]) : f2_lo(r2[k / 2]);
+                const f32x2 ns = f2_pack(-s, -s);
+                if (!(k & 1) && k + 1 < N)
+                    r2[k / 2] = f2_pack(s, fma_rn(-s, lu[k * LP + k + 1], f2_hi(r2[k / 2])));
 #pragma unroll
-                for (int i4 = ((k + 1) & ~3); i4 < N; i4 += 4)
-                {
-                    const float4 l = *reinterpret_cast<const float4 *>(lu + k * LP + i4);
-                    if (i4 + 0 > k) rhs[i4 + 0] = fma_rn(-s, l.x, rhs[i4 + 0]);
-                    if (i4 + 1 > k) rhs[i4 + 1] = fma_rn(-s, l.y, rhs[i4 + 1]);
-                    if (i4 + 2 > k) rhs[i4 + 2] = fma_rn(-s, l.z, rhs[i4 + 2]);
-                    if (i4 + 3 > k) rhs[i4 + 3] = fma_rn(-s, l.w, rhs[i4 + 3]);
-                }
+                for (int c = k / 2 + 1; c < N / 2; ++c) fma2(r2[c], ns, *reinterpret_cast<const f32x2 *>(lu + k * LP + 2 * c));
             }
         }
-        // backward, upper with reciprocal diagonal
+        // backward, upper with reciprocal diagonal; the row above k in k's pair separately
 #pragma unroll
         for (int k = N - 1; k >= 0; --k)
         {
             if (k < n)
             {
-                const float s = mul_rn(rhs[k], rec[m][k]);
-                rhs[k] = s;
+                const float s = mul_rn((k & 1) ? f2_hi(r2[k / 2]) : f2_lo(r2[k / 2]), rec[m][k]);
+                const f32x2 ns = f2_pack(-s, -s);
+                if (k & 1)
+                    r2[k / 2] = f2_pack(fma_rn(-s, lu[k * LP + k - 1], f2_lo(r2[k / 2])), s);
+                else
+                    r2[k / 2] = f2_pack(s, f2_hi(r2[k / 2]));
 #pragma unroll
-                for (int i4 = 0; i4 < k; i4 += 4)
-                {
-                    const float4 u = *reinterpret_cast<const float4 *>(lu + k * LP + i4);
-                    if (i4 + 0 < k) rhs[i4 + 0] = fma_rn(-s, u.x, rhs[i4 + 0]);
-                    if (i4 + 1 < k) rhs[i4 + 1] = fma_rn(-s, u.y, rhs[i4 + 1]);
-                    if (i4 + 2 < k) rhs[i4 + 2] = fma_rn(-s, u.z, rhs[i4 + 2]);
-                    if (i4 + 3 < k) rhs[i4 + 3] = fma_rn(-s, u.w, rhs[i4 + 3]);
-                }
+                for (int c = 0; c < k / 2; ++c) fma2(r2[c], ns, *reinterpret_cast<const f32x2 *>(lu + k * LP + 2 * c));
             }
         }
         __syncthreads();
@@ -479,7 +474,11 @@ __global__ void __launch_bounds__(RI_THREADS) getri_small_kernel(float *a_single
         if (t < n)
         {
 #pragma unroll
-            for (int i = 0; i < N; ++i) stage[col * SP + i] = rhs[i];
+            for (int c = 0; c < N / 2; ++c)
+            {
+                stage[col * SP + 2 * c] = f2_lo(r2[c]);
+                stage[col * SP + 2 * c + 1] = f2_hi(r2[c]);
+            }
         }
         __syncthreads();
         if (live && !failed)

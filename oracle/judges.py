@@ -178,3 +178,21 @@ def residual_gate(ratios, cpu_ratios):
     threshold = np.maximum(5.0 * cpu, 3.0 * cpu.mean()) if cpu.size else cpu
     bad = ~np.isfinite(ratios) | (ratios > threshold)
     return [(int(i), float(ratios[i]), float(threshold[i])) for i in np.flatnonzero(bad)]
+
+
+def inverse_judge(a, x):
+    """The reference's inverse acceptance (test/utils/verify_utils.py:60-88, verify_inverse):
+    A @ X compared with the identity by numpy isclose at rtol = atol = 5e-3, in the input's
+    precision; the inverse passes when at most 1e-4 of the entries miss (and everything is
+    finite).  Returns (passed, mismatch ratio)."""
+    a = np.asarray(a)
+    x = np.asarray(x)
+    if not (np.isfinite(a).all() and np.isfinite(x).all()):
+        return False, 1.0
+    out = np.dot(a, x).reshape(-1)
+    if not np.isfinite(out).all():
+        return False, 1.0
+    golden = np.eye(a.shape[0], dtype=a.dtype).reshape(-1)
+    miss = ~np.isclose(out, golden, rtol=5e-3, atol=5e-3, equal_nan=True)
+    ratio = float(miss.sum()) / golden.size
+    return ratio <= 1e-4, ratio

@@ -171,3 +171,16 @@ def test_residual_gate_flags_an_inflated_ratio():
     bad[2] = 3.1  # threshold max(2.5, 3 * 1.0) = 3.0
     bad[3] = np.inf
     assert [i for i, _, _ in judges.residual_gate(bad, cpu)] == [2, 3]
+
+
+def test_inverse_judge_accepts_the_oracle_and_rejects_a_planted_error():
+    rng = np.random.default_rng(3)
+    a = (rng.standard_normal((1, 24, 24)) + 4 * np.eye(24)).astype(np.float32)
+    lu, ipiv, _ = oracle.sgetrf_batched(a)
+    x, _ = oracle.sgetri_batched(lu, ipiv)
+    ok, ratio = judges.inverse_judge(a[0], x[0])
+    assert ok and ratio == 0.0
+    bad = x[0].copy()
+    bad[3, 5] += 0.5  # a planted error spoils a row of A @ X
+    ok, ratio = judges.inverse_judge(a[0], bad)
+    assert not ok and ratio > 1e-4
