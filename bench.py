@@ -602,10 +602,10 @@ def measure_c1(handle, timer, args):
         "gflops": round(count * (flops_f + flops_s) / (ms * 1e-3) / 1e9, 1),
         "berr_max": float(be.max()),
         "roofline": roofline(count * (bytes_f + bytes_s), count * (flops_f + flops_s), ms,
-                             "potrf_small_kernel<32> + potrs_small_kernel<32>", "c1_potrf_potrs"),
+                             "potrf_group_kernel<32,16> + solve_slot_check_kernel + potrs_lane_kernel<32>", "c1_potrf_potrs"),
         "kernels": {
-            "potrf": roofline(count * bytes_f, count * flops_f, ms_f, "potrf_small_kernel<32>", "c1_potrf"),
-            "potrs": roofline(count * bytes_s, count * flops_s, ms_s, "potrs_small_kernel<32>", "c1_potrs"),
+            "potrf": roofline(count * bytes_f, count * flops_f, ms_f, "potrf_group_kernel<32,16>", "c1_potrf"),
+            "potrs": roofline(count * bytes_s, count * flops_s, ms_s, "potrs_lane_kernel<32>", "c1_potrs"),
         },
         "l2": "inputs restored from a pristine copy, then a 256 MiB buffer written, before each step",
         "cpu_baseline": cpu,
@@ -697,11 +697,11 @@ def measure_c2(handle, timer, args):
         "ms": round(ms, 5), "gflops": round(total_f / (ms * 1e-3) / 1e9, 1),
         "berr_max": float(be.max()), "inverse_residual_max": float(be_inv.max()),
         "ipiv_equal_openblas": None if cpiv is None else bool(np.array_equal(gpu_piv, cpiv.reshape(count, n))),
-        "roofline": roofline(total_b, total_f, ms, "getrf_small_kernel<64> + getrs_small + getri_small_kernel<64>",
+        "roofline": roofline(total_b, total_f, ms, "getrf_small_kernel<64> + getrs_small_kernel<64,0> + getri_small_kernel<64>",
                              "c2_all"),
         "kernels": {
             "getrf": roofline(count * bytes_f, count * flops_f, ms_f, "getrf_small_kernel<64>", "c2_getrf"),
-            "getrs": roofline(count * bytes_s, count * flops_s, ms_s, "getrs_small_kernel<64>", "c2_getrs"),
+            "getrs": roofline(count * bytes_s, count * flops_s, ms_s, "getrs_small_kernel<64,0>", "c2_getrs"),
             "getri": roofline(count * bytes_i, count * flops_i, ms_i, "getri_small_kernel<64>", "c2_getri"),
         },
         "l2": "inputs restored from a pristine copy, then a 256 MiB buffer written, before each step",
@@ -807,7 +807,7 @@ def measure_c3(handle, timer, args):
         "gflops": round(total_f / (ms * 1e-3) / 1e9, 1), "berr_max_sampled": float(max(be)),
         "berr_sample": f"every 20th matrix ({len(be)}), FP64",
         "plan_create_s": round(plan_s, 3),
-        "roofline": roofline(total_b, total_f, ms, "vb_warp_kernel + vb_block_kernel (one graph)", "c3_vbatched"),
+        "roofline": roofline(total_b, total_f, ms, "vb_warp_kernel<32> + vb_cb_kernel<64> + vb_cb_kernel<128> (one graph)", "c3_vbatched"),
         "l2": "inputs (0.93 GB) restored from a pristine copy, then a 256 MiB buffer written, before each step",
         "cpu_baseline": cpu,
     }
