@@ -7,15 +7,16 @@
 // s = sqrt(Re a_jj); the solves take their right-looking updates in ascending (forward) or
 // descending (backward) k before their division.  Only the schedule differs from a plain
 // right-looking loop, and no element sees its operations in another order:
-//   factor, left-looking in blocks of CB = 16 columns: thread t owns row J0 + t of block
-//   column J0 (in registers) and first applies every earlier column k < J0 to it (the
-//   block's sixteen L(J0 + j, k) are broadcast loads; a thread's row value L(i, k) is its own
-//   load), then the sixteen panel steps run with one barrier each (the column's L values
-//   for the block rows go through a double-buffered shared slot; every thread keeps the
-//   block's diagonal real parts, so the square roots need no second exchange);
-//   solve, blocked by 16 rows: the warp owning a block's rows solves its triangle by
-//   shuffles, the block's solution values are published once, and every other row applies
-//   the block's sixteen updates in order.
+//   factor, left-looking in blocks of CB = 16 columns: every earlier column k < J0 is first
+//   applied to block column J0 in shared memory, 16 / C threads per remaining row with C
+//   adjacent columns each (the row's L(i, k) is a thread's own load, the block's L(J0 + j, k)
+//   broadcast loads); then thread t takes row J0 + t into registers and the sixteen panel
+//   steps run with one barrier each (the column's L values for the block rows go through a
+//   double-buffered shared slot; every thread keeps the block's diagonal real parts, so the
+//   square roots need no second exchange);
+//   solve, a warp per right-hand side (or per group of them) with no block barrier: the
+//   owner lane of row k divides, one shuffle per component broadcasts the quotient, and
+//   every lane updates its rows from the packed triangle.
 // Shared memory: the lower triangle packed by columns (column j holds rows j..n-1), plus a
 // 16-element tail so the broadcast loads of a ragged last block stay inside the buffer, plus
 // small exchange slots.  cb_smem_bytes(n) gives the size; n = 128 takes 66 KB, so three
@@ -25,16 +26,15 @@
 
 namespace ops_solver
 {
-constexpr int CB = 16;               // columns per block, rows per solve block
-constexpr int CB_RHS = 4;            // right-hand sides solved together
+constexpr int CB = 16;               // columns per factor block
+constexpr int CB_RHS = 4;            // right-hand sides a block keeps in flight in the solve
 constexpr float CB_FLT_MAX = 3.402823466e38F;
 
 __host__ __device__ constexpr int cb_tri(int n) { return n * (n + 1) / 2; }
-// floats of shared memory: packed triangle + tail, two column slots, block diagonal, solve
-// exchange (two buffers of CB rows x CB_RHS complex)
+// floats of shared memory: packed triangle + tail, two column slots, block diagonal
 __host__ __device__ constexpr size_t cb_smem_bytes(int n)
 {
-    return ((size_t)(cb_tri(n) + CB) * 2 + 2 * CB * 2 + CB + 2 * CB * CB_RHS * 2) * sizeof(float);
+    return ((size_t)(cb_tri(n) + CB) * 2 + 2 * CB * 2 + CB) * sizeof(float);
 }
 // packed offset of column j (rows j..n-1)
 __device__ __forceinline__ int cb_col(int j, int n) { return j * n - (j * (j - 1)) / 2; }
@@ -44,7 +44,6 @@ struct CbShared
     float2 *tri;    // packed lower triangle
     float2 *slot;   // [2][CB] column exchange
     float *diag;    // [CB] block diagonal real parts
-    float2 *ybuf;   // [2][CB][CB_RHS] solve exchange
 };
 
 __device__ __forceinline__ CbShared cb_carve(float *base, int n)
@@ -53,7 +52,6 @@ __device__ __forceinline__ CbShared cb_carve(float *base, int n)
     s.tri = reinterpret_cast<float2 *>(base);
     s.slot = s.tri + cb_tri(n) + CB;
     s.diag = reinterpret_cast<float *>(s.slot + 2 * CB);
-    s.ybuf = reinterpret_cast<float2 *>(s.diag + CB + (CB & 1));
     return s;
 }
 
@@ -125,15 +123,80 @@ __device__ __forceinline__ void cb_store(const CbShared &s, float2 *pa, int lda,
     }
 }
 
+// The left-looking update of block column J0 (rows J0..n-1, its w columns) by every earlier
+// column k < J0, in shared memory: G = CB / C threads share a row, each taking C adjacent
+// columns of it, so that the whole block works however few rows remain below J0 (the rows
+// shrink from n to 16 over the factorisation; one thread per row left most of the block
+// waiting at the next barrier).  Every element still takes its updates one after another in
+// ascending k, from one thread.
+template <int C>
+__device__ __forceinline__ void cb_left(const CbShared &s, int n, int J0, int w)
+{
+    constexpr int G = CB / C;
+    const int t = threadIdx.x;
+    const int i = J0 + t / G;    // row
+    const int j0 = (t % G) * C;  // first column of this thread within the block
+    if (i >= n) return;
+    float zr[C], zi[C];
+#pragma unroll
+    for (int u = 0; u < C; ++u)
+    {
+        const int j = j0 + u;
+        zr[u] = 0.0f;
+        zi[u] = 0.0f;
+        if (j < w && J0 + j <= i)
+        {
+            const float2 v = s.tri[cb_col(J0 + j, n) + i - (J0 + j)];
+            zr[u] = v.x;
+            zi[u] = v.y;
+        }
+    }
+    int ok = 0;  // packed offset of column k
+    for (int k = 0; k < J0; ++k)
+    {
+        const float2 a = s.tri[ok + i - k];
+        const float2 *c = s.tri + ok + J0 - k + j0;  // c[u] = L(J0 + j0 + u, k)
+#pragma unroll
+        for (int u = 0; u < C; ++u)
+        {
+            const float2 cj = c[u];
+            cb_sub_lconj(zr[u], zi[u], a.x, a.y, cj.x, cj.y);
+        }
+        ok += n - k;
+    }
+#pragma unroll
+    for (int u = 0; u < C; ++u)
+    {
+        const int j = j0 + u;
+        if (j < w && J0 + j <= i) s.tri[cb_col(J0 + j, n) + i - (J0 + j)] = make_float2(zr[u], zi[u]);
+    }
+}
+
 // Factor the packed triangle in place.  Returns info (0, or the first failed column + 1),
 // the same on every thread.  Columns before a failure are final in shared memory.
 template <int T>
-__device__ int cb_factor(const CbShared &s, int n)
+__device__ __forceinline__ int cb_factor(const CbShared &s, int n)
 {
     const int t = threadIdx.x;
     for (int J0 = 0; J0 < n; J0 += CB)
     {
         const int w = min(CB, n - J0);
+        if (J0 > 0)
+        {
+            // threads per row: the most that fit the rows left (uniform over the block)
+            const int rows = n - J0;
+            if (rows > T / 2)
+                cb_left<16>(s, n, J0, w);
+            else if (rows > T / 4)
+                cb_left<8>(s, n, J0, w);
+            else if (rows > T / 8)
+                cb_left<4>(s, n, J0, w);
+            else if (rows > T / 16)
+                cb_left<2>(s, n, J0, w);
+            else
+                cb_left<1>(s, n, J0, w);
+            __syncthreads();
+        }
         const int i = J0 + t;  // this thread's row
         const bool own = i < n;
         float zr[CB], zi[CB];
@@ -149,23 +212,6 @@ __device__ int cb_factor(const CbShared &s, int n)
                 const float2 v = s.tri[cb_col(J0 + j, n) + i - (J0 + j)];
                 zr[j] = v.x;
                 zi[j] = v.y;
-            }
-        }
-        // every earlier column, ascending k
-        if (own)
-        {
-            int ok = 0;  // packed offset of column k
-            for (int k = 0; k < J0; ++k)
-            {
-                const float2 a = s.tri[ok + i - k];
-                const float2 *c = s.tri + ok + J0 - k;
-#pragma unroll
-                for (int j = 0; j < CB; ++j)
-                {
-                    const float2 cj = c[j];
-                    cb_sub_lconj(zr[j], zi[j], a.x, a.y, cj.x, cj.y);
-                }
-                ok += n - k;
             }
         }
         // the block's diagonal real parts to every thread
@@ -202,7 +248,7 @@ __device__ int cb_factor(const CbShared &s, int n)
                         lr = sq;
                         li = 0.0f;
                     }
-                    else if (i > k)
+                    else if (i > k && own)  // rows past n would take the slow division on junk
                     {
                         lr = div_by(lr, sq, y, ok);
                         li = div_by(li, sq, y, ok);
@@ -240,163 +286,129 @@ __device__ int cb_factor(const CbShared &s, int n)
 }
 
 // Solve L L^H X = B for nrhs columns of B (global, ldb) with the factor in shared memory.
-// Rows are owned by threads (row t), CB_RHS right-hand sides at a time.
+// Each warp solves its own right-hand sides (T / 32 warps; up to four right-hand sides in
+// flight per warp when the block has fewer than four warps) with no block barrier: lane l
+// keeps rows l, l + 32, ... in registers; step k divides row k on its owner lane (the
+// lane's own diagonal entries and their reciprocals are taken once, ahead of both sweeps,
+// and every other lane divides 1 by its own diagonal so that no lane leaves the fast
+// division), broadcasts the quotient with one shuffle per component, and every row below
+// (forward) or above (backward) takes its update from the packed triangle.  Each element
+// receives its updates in ascending (forward) or descending (backward) k, as before.
 template <int T>
-__device__ void cb_solve(const CbShared &s, int n, float2 *pb, int ldb, int nrhs)
+__device__ __forceinline__ void cb_solve(const CbShared &s, int n, float2 *pb, int ldb, int nrhs)
 {
-    const int t = threadIdx.x, warp = t >> 5;
-    const int i = t;
-    const bool own = i < n;
-    const int nblk = (n + CB - 1) / CB;
-    for (int r0 = 0; r0 < nrhs; r0 += CB_RHS)
+    constexpr int NW = T / 32;                    // warps
+    constexpr int M = T / 32;                     // rows per lane (n <= T)
+    constexpr int RW = NW >= CB_RHS ? 1 : CB_RHS / NW;  // right-hand sides per warp in flight
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float dd[M], rd[M];
+    bool dk[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m)
     {
-        const int nr = min(CB_RHS, nrhs - r0);
-        float zr[CB_RHS], zi[CB_RHS];
+        const int row = lane + 32 * m;
+        dd[m] = row < n ? s.tri[cb_col(row, n)].x : 1.0f;
+        rd[m] = div_prepare(dd[m]);
+        dk[m] = div_range(dd[m]);
+    }
+    for (int r0 = warp * RW; r0 < nrhs; r0 += NW * RW)
+    {
+        // rows past n hold 1 (never stored), so their junk divisions stay on the fast path
+        float zr[RW][M], zi[RW][M];
 #pragma unroll
-        for (int r = 0; r < CB_RHS; ++r)
-        {
-            zr[r] = 0.0f;
-            zi[r] = 0.0f;
-            if (own && r < nr)
-            {
-                const float2 v = pb[(int64_t)(r0 + r) * ldb + i];
-                zr[r] = v.x;
-                zi[r] = v.y;
-            }
-        }
-        // forward: y_k = z_k / l_kk, z_i -= l_ik y_k for i > k
-        for (int b = 0; b < nblk; ++b)
-        {
-            const int J0 = b * CB, w = min(CB, n - J0);
-            float2 *yb = s.ybuf + (b & 1) * CB * CB_RHS;
-            if (warp == J0 / 32)
-            {
+        for (int u = 0; u < RW; ++u)
 #pragma unroll
-                for (int kk = 0; kk < CB; ++kk)
+            for (int m = 0; m < M; ++m)
+            {
+                const int row = lane + 32 * m;
+                zr[u][m] = 1.0f;
+                zi[u][m] = 1.0f;
+                if (r0 + u < nrhs && row < n)
                 {
-                    if (kk < w)
-                    {
-                        const int k = J0 + kk;
-                        const float d = s.tri[cb_col(k, n)].x;
-                        const float yv = div_prepare(d);
-                        const bool okd = div_range(d);
-                        const int src = k & 31;
-                        float lr = 0.0f, li = 0.0f;
-                        if (i > k && i < J0 + w)
-                        {
-                            const float2 l = s.tri[cb_col(k, n) + i - k];
-                            lr = l.x;
-                            li = l.y;
-                        }
+                    const float2 v = pb[(int64_t)(r0 + u) * ldb + row];
+                    zr[u][m] = v.x;
+                    zi[u][m] = v.y;
+                }
+            }
+        // forward: y_k = z_k / l_kk, z_i -= l_ik y_k for i > k, k ascending
 #pragma unroll
-                        for (int r = 0; r < CB_RHS; ++r)
-                        {
-                            const float qr = __shfl_sync(0xffffffffu, div_by(zr[r], d, yv, okd), src);
-                            const float qi = __shfl_sync(0xffffffffu, div_by(zi[r], d, yv, okd), src);
-                            if (i == k)
-                            {
-                                zr[r] = qr;
-                                zi[r] = qi;
-                            }
-                            else if (i > k && i < J0 + w)
-                                cb_sub_prod(zr[r], zi[r], lr, li, qr, qi);
-                        }
+        for (int m = 0; m < M; ++m)
+        {
+#pragma unroll 2
+            for (int k0 = 0; k0 < 32; ++k0)
+            {
+                const int k = 32 * m + k0;
+                if (k >= n) break;
+                const float2 *col = s.tri + cb_col(k, n) - k;  // col[i] = L(i, k)
+                float qr[RW], qi[RW];
+#pragma unroll
+                for (int u = 0; u < RW; ++u)
+                {
+                    const float nr = lane == k0 ? zr[u][m] : 1.0f, ni = lane == k0 ? zi[u][m] : 1.0f;
+                    qr[u] = __shfl_sync(0xffffffffu, div_by(nr, dd[m], rd[m], dk[m]), k0);
+                    qi[u] = __shfl_sync(0xffffffffu, div_by(ni, dd[m], rd[m], dk[m]), k0);
+                    if (lane == k0)
+                    {
+                        zr[u][m] = qr[u];
+                        zi[u][m] = qi[u];
                     }
                 }
-                if (i >= J0 && i < J0 + w)
-                {
 #pragma unroll
-                    for (int r = 0; r < CB_RHS; ++r) yb[(i - J0) * CB_RHS + r] = make_float2(zr[r], zi[r]);
-                }
-            }
-            __syncthreads();
-            if (own && i >= J0 + w)
-            {
-                for (int kk = 0; kk < w; ++kk)
+                for (int mm = m; mm < M; ++mm)
                 {
-                    const int k = J0 + kk;
-                    const float2 l = s.tri[cb_col(k, n) + i - k];
-#pragma unroll
-                    for (int r = 0; r < CB_RHS; ++r)
+                    const int row = lane + 32 * mm;
+                    if (row > k && row < n)
                     {
-                        const float2 y = yb[kk * CB_RHS + r];
-                        cb_sub_prod(zr[r], zi[r], l.x, l.y, y.x, y.y);
+                        const float2 l = col[row];
+#pragma unroll
+                        for (int u = 0; u < RW; ++u) cb_sub_prod(zr[u][mm], zi[u][mm], l.x, l.y, qr[u], qi[u]);
                     }
                 }
             }
         }
-        // backward: x_k = z_k / l_kk, z_i -= conj(l_ki) x_k for i < k, k descending.  The
-        // exchange slots alternate by block, so one barrier per block suffices once the
-        // forward sweep's last readers are done.
-        __syncthreads();
-        for (int b = nblk - 1; b >= 0; --b)
+        // backward: x_k = z_k / l_kk, z_i -= conj(l_ki) x_k for i < k, k descending
+#pragma unroll
+        for (int m = M - 1; m >= 0; --m)
         {
-            const int J0 = b * CB, w = min(CB, n - J0);
-            float2 *yb = s.ybuf + (b & 1) * CB * CB_RHS;
-            if (warp == J0 / 32)
+#pragma unroll 2
+            for (int k0 = 31; k0 >= 0; --k0)
             {
+                const int k = 32 * m + k0;
+                if (k >= n) continue;
+                float qr[RW], qi[RW];
 #pragma unroll
-                for (int kk = CB - 1; kk >= 0; --kk)
+                for (int u = 0; u < RW; ++u)
                 {
-                    if (kk < w)
+                    const float nr = lane == k0 ? zr[u][m] : 1.0f, ni = lane == k0 ? zi[u][m] : 1.0f;
+                    qr[u] = __shfl_sync(0xffffffffu, div_by(nr, dd[m], rd[m], dk[m]), k0);
+                    qi[u] = __shfl_sync(0xffffffffu, div_by(ni, dd[m], rd[m], dk[m]), k0);
+                    if (lane == k0)
                     {
-                        const int k = J0 + kk;
-                        const float d = s.tri[cb_col(k, n)].x;
-                        const float yv = div_prepare(d);
-                        const bool okd = div_range(d);
-                        const int src = k & 31;
-                        float lr = 0.0f, li = 0.0f;
-                        if (i < k && i >= J0)
-                        {
-                            const float2 l = s.tri[cb_col(i, n) + k - i];  // L(k, i)
-                            lr = l.x;
-                            li = -l.y;  // conj
-                        }
-#pragma unroll
-                        for (int r = 0; r < CB_RHS; ++r)
-                        {
-                            const float qr = __shfl_sync(0xffffffffu, div_by(zr[r], d, yv, okd), src);
-                            const float qi = __shfl_sync(0xffffffffu, div_by(zi[r], d, yv, okd), src);
-                            if (i == k)
-                            {
-                                zr[r] = qr;
-                                zi[r] = qi;
-                            }
-                            else if (i < k && i >= J0)
-                                cb_sub_prod(zr[r], zi[r], lr, li, qr, qi);
-                        }
+                        zr[u][m] = qr[u];
+                        zi[u][m] = qi[u];
                     }
                 }
-                if (i >= J0 && i < J0 + w)
-                {
 #pragma unroll
-                    for (int r = 0; r < CB_RHS; ++r) yb[(i - J0) * CB_RHS + r] = make_float2(zr[r], zi[r]);
-                }
-            }
-            __syncthreads();
-            if (i < J0)
-            {
-                const float2 *col = s.tri + cb_col(i, n) - i;  // col[k] = L(k, i)
-                for (int kk = w - 1; kk >= 0; --kk)
+                for (int mm = 0; mm <= m; ++mm)
                 {
-                    const int k = J0 + kk;
-                    const float2 l = col[k];
-#pragma unroll
-                    for (int r = 0; r < CB_RHS; ++r)
+                    const int row = lane + 32 * mm;
+                    if (row < k)
                     {
-                        const float2 x = yb[kk * CB_RHS + r];
-                        cb_sub_prod(zr[r], zi[r], l.x, -l.y, x.x, x.y);
+                        const float2 l = s.tri[cb_col(row, n) + k - row];  // L(k, row)
+#pragma unroll
+                        for (int u = 0; u < RW; ++u) cb_sub_prod(zr[u][mm], zi[u][mm], l.x, -l.y, qr[u], qi[u]);
                     }
                 }
             }
         }
-        if (own)
-        {
 #pragma unroll
-            for (int r = 0; r < CB_RHS; ++r)
-                if (r < nr) pb[(int64_t)(r0 + r) * ldb + i] = make_float2(zr[r], zi[r]);
-        }
-        __syncthreads();  // the exchange slots are free for the next group
+        for (int u = 0; u < RW; ++u)
+#pragma unroll
+            for (int m = 0; m < M; ++m)
+            {
+                const int row = lane + 32 * m;
+                if (r0 + u < nrhs && row < n) pb[(int64_t)(r0 + u) * ldb + row] = make_float2(zr[u][m], zi[u][m]);
+            }
     }
 }
 

@@ -229,6 +229,19 @@ __global__ void __launch_bounds__(RS_THREADS) getrs_small_kernel(float *a_single
             pb = b_table ? slot(b_table, b_first + q) : b_single;
         }
         bool live = pa != nullptr && pb != nullptr;
+        float a[RPL][N];
+        if (trans == 0)
+        {
+            // issued before the pivot check so that both wait on memory together; a matrix
+            // whose pivots fail the check is loaded but never written back
+#pragma unroll
+            for (int s = 0; s < RPL; ++s)
+            {
+                const int r = lrow + s * SUBW;
+#pragma unroll
+                for (int j = 0; j < N; ++j) a[s][j] = (live && r < n && j < n) ? pa[r + (int64_t)j * lda] : 0.0f;
+            }
+        }
         // Pivots of this matrix, validated: each must lie in [k+1, n].
         __syncwarp();
         bool bad = false;
@@ -244,18 +257,7 @@ __global__ void __launch_bounds__(RS_THREADS) getrs_small_kernel(float *a_single
         const unsigned bad_any = warp_max_u32<SUBW>(bad ? 1u : 0u);
         if (bad_any) live = false;
 
-        float a[RPL][N];
-        if (trans == 0)
-        {
-#pragma unroll
-            for (int s = 0; s < RPL; ++s)
-            {
-                const int r = lrow + s * SUBW;
-#pragma unroll
-                for (int j = 0; j < N; ++j) a[s][j] = (live && r < n && j < n) ? pa[r + (int64_t)j * lda] : 0.0f;
-            }
-        }
-        else if constexpr (TRANS != 0)
+        if constexpr (TRANS != 0)
         {
             // tile[j*P + i] = A(i, j); lane r then reads row r of A^T = column r of A.
             for (int idx = lrow; idx < N * N; idx += SUBW)
@@ -315,7 +317,12 @@ __global__ void __launch_bounds__(RS_THREADS) getrs_small_kernel(float *a_single
                 {
                     if (k < n)
                     {
-                        if (lrow == k % SUBW) x[k / SUBW] = div_rn(x[k / SUBW], a[k / SUBW][k]);
+                        {
+                            // the reciprocal does not depend on x: it is taken off the chain
+                            const float d = a[k / SUBW][k];
+                            const float y = div_prepare(d);
+                            if (lrow == k % SUBW) x[k / SUBW] = div_by(x[k / SUBW], d, y, div_range(d));
+                        }
                         const float xk = __shfl_sync(0xffffffffu, x[k / SUBW], k % SUBW, SUBW);
 #pragma unroll
                         for (int s = 0; s < RPL; ++s)
@@ -336,7 +343,12 @@ __global__ void __launch_bounds__(RS_THREADS) getrs_small_kernel(float *a_single
                 {
                     if (k < n)
                     {
-                        if (lrow == k % SUBW) x[k / SUBW] = div_rn(x[k / SUBW], a[k / SUBW][k]);
+                        {
+                            // the reciprocal does not depend on x: it is taken off the chain
+                            const float d = a[k / SUBW][k];
+                            const float y = div_prepare(d);
+                            if (lrow == k % SUBW) x[k / SUBW] = div_by(x[k / SUBW], d, y, div_range(d));
+                        }
                         const float xk = __shfl_sync(0xffffffffu, x[k / SUBW], k % SUBW, SUBW);
 #pragma unroll
                         for (int s = 0; s < RPL; ++s)
@@ -408,10 +420,21 @@ __global__ void __launch_bounds__(RI_THREADS, 6) getri_small_kernel(float *a_sin
             zero_at[m] = 0x7fffffff;
             bad_pivot[m] = 0;
         }
-        for (int idx = t; idx < N * N; idx += N)
         {
-            const int i = idx % N, j = idx / N;
-            lu[j * LP + i] = (live && i < n && j < n) ? pa[i + (int64_t)j * lda] : (i == j ? 1.0f : 0.0f);
+            // row t of every column, in batches of up to 32 loads issued before their stores, so
+            // a block waits for memory once or twice per matrix rather than once per column
+            constexpr int LB = N < 32 ? N : 32;
+            const float *src = live && t < n ? pa + t : nullptr;
+#pragma unroll
+            for (int j0 = 0; j0 < N; j0 += LB)
+            {
+                float v[LB];
+#pragma unroll
+                for (int j = 0; j < LB; ++j)
+                    v[j] = (src && j0 + j < n) ? src[(int64_t)(j0 + j) * lda] : (t == j0 + j ? 1.0f : 0.0f);
+#pragma unroll
+                for (int j = 0; j < LB; ++j) lu[(j0 + j) * LP + t] = v[j];
+            }
         }
         pv[m][t] = (live && ipiv && t < n) ? ipiv[q * n + t] : t + 1;
         __syncthreads();

@@ -320,8 +320,27 @@ __global__ void __launch_bounds__(32) potrs_lane_kernel(float *a_single, float *
     if (q < count) mine = a_table ? slot(a_table, a_first + q) : a_single;
     // 16-byte copies when every column of every matrix starts 16-byte aligned (lower
     // storage, lda % 4 == 0, aligned bases); else element copies
-    const bool vec = !upper && (lda & 3) == 0 &&
+    const bool vec = !upper && (lda & 3) == 0 && lda <= (1 << 25) &&
                      __all_sync(0xffffffffu, (reinterpret_cast<uintptr_t>(mine) & 15u) == 0);
+    // The 16-byte pieces a lane copies are the same for every matrix of the warp (one n and
+    // lda per call): column j holds pieces 4 floor(j / 4) .. n - 1 rounded up to 4 (inside
+    // the column).  Offsets are taken once here; per matrix a lane then issues at most PPL
+    // copies with one add each, so the warp streams its 32 triangles back to back.
+    constexpr int PPL = (N * (N / 4) + 31) / 32;  // pieces per lane
+    unsigned piece_dst[PPL];                      // byte offset in the matrix's trapezoid
+    int piece_src[PPL];                           // float offset j * lda + r4 (< 2^31 / 4)
+    int piece_bytes[PPL];                         // 0: nothing to copy
+#pragma unroll
+    for (int it = 0; it < PPL; ++it)
+    {
+        const int e = lane + 32 * it;
+        const int j = e / (N / 4), r4 = (e % (N / 4)) * 4;
+        const bool ok = e < N * (N / 4) && j < n && r4 >= 4 * (j / 4) && r4 < n;
+        piece_dst[it] = ok ? (unsigned)(trap_at<N>(r4, j) * 4) : 0u;
+        piece_src[it] = ok ? j * lda + r4 : 0;
+        piece_bytes[it] = ok ? min(4, n - r4) * 4 : 0;
+    }
+    const unsigned mem0 = (unsigned)__cvta_generic_to_shared(lane_mem);
     for (int mm = 0; mm < 32; ++mm)
     {
         const float *pa =
@@ -330,19 +349,13 @@ __global__ void __launch_bounds__(32) potrs_lane_kernel(float *a_single, float *
         float *dst = lane_mem + mm * P;
         if (vec)
         {
-            // column j: pieces 4 floor(j / 4) .. n - 1 rounded up to 4 (inside the column)
-            for (int e = lane; e < N * (N / 4); e += 32)
-            {
-                const int j = e / (N / 4), r4 = (e % (N / 4)) * 4;
-                if (j < n && r4 >= 4 * (j / 4) && r4 < n)
-                {
-                    const unsigned d = (unsigned)__cvta_generic_to_shared(dst + trap_at<N>(r4, j));
-                    const int bytes = min(4, n - r4) * 4;
-                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d),
-                                 "l"(pa + (int64_t)j * lda + r4), "r"(bytes)
+            const unsigned d0 = mem0 + (unsigned)(mm * P * 4);
+#pragma unroll
+            for (int it = 0; it < PPL; ++it)
+                if (piece_bytes[it])
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d0 + piece_dst[it]),
+                                 "l"(pa + piece_src[it]), "r"(piece_bytes[it])
                                  : "memory");
-                }
-            }
         }
         else
         {
