@@ -550,7 +550,8 @@ def measure_c1(handle, timer, args):
     A, B = torch.empty_like(A0), torch.empty_like(B0)
     ta, tb = aclsolver.pointer_table(A, count, n * n * 4), aclsolver.pointer_table(B, count, n * nrhs * 4)
     info = torch.empty(count, dtype=torch.int32, device="cuda")
-    sinfo = torch.empty(1, dtype=torch.int32, device="cuda")
+    # SpotrsBatched reports through info[0] but, as the reference, takes batchSize entries
+    sinfo = torch.empty(count, dtype=torch.int32, device="cuda")
     h = handle.value
 
     def potrf():
@@ -571,7 +572,7 @@ def measure_c1(handle, timer, args):
     for _ in range(3):
         timer(both, 1, restore)
     ms = timer(both, steps, restore)
-    assert int(info.abs().max()) == 0 and int(sinfo.item()) == 0
+    assert int(info.abs().max()) == 0 and int(sinfo[0].item()) == 0
     x = B.cpu().numpy().reshape(count, nrhs, n).transpose(0, 2, 1)
     ms_f = timer(potrf, steps, restore)
     ms_s = timer(potrs, steps, lambda: B.copy_(B0))
@@ -634,7 +635,7 @@ def measure_c2(handle, timer, args):
     tc = aclsolver.pointer_table(Cinv, count, n * n * 4)
     piv = torch.empty(count * n, dtype=torch.int32, device="cuda")
     info = torch.empty(count, dtype=torch.int32, device="cuda")
-    sinfo = torch.empty(1, dtype=torch.int32, device="cuda")
+    sinfo = torch.empty(count, dtype=torch.int32, device="cuda")  # SgetrsBatched: one entry per matrix
     iinfo = torch.empty(count, dtype=torch.int32, device="cuda")
     h = handle.value
 
@@ -662,7 +663,7 @@ def measure_c2(handle, timer, args):
     for _ in range(3):
         timer(all3, 1, restore)
     ms = timer(all3, steps, restore)
-    assert int(info.abs().max()) == 0 and int(sinfo.item()) == 0 and int(iinfo.abs().max()) == 0
+    assert int(info.abs().max()) == 0 and int(sinfo.abs().max()) == 0 and int(iinfo.abs().max()) == 0
     x = B.cpu().numpy().reshape(count, nrhs, n).transpose(0, 2, 1)
     inv = Cinv.cpu().numpy().reshape(count, n, n).transpose(0, 2, 1)
     gpu_piv = piv.cpu().numpy().reshape(count, n)
