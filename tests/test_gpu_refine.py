@@ -71,7 +71,10 @@ def test_refinement_reaches_fp32_backward_error(handle, precision, kappa):
         be = judges.backward_error(a[q], x[q], b[q])
         fe = judges.forward_error(a[q], x[q], b[q])
         assert be <= 1e-6, (q, be, berr[q], iters[q])
-        assert berr[q] <= 1e-6
+        # the reported error is that of the FP64 iterate; x is its FP32 rounding, so the two
+        # agree to within the rounding's share (a zero or stale report fails here)
+        assert 0.0 < berr[q] <= 1e-6
+        assert berr[q] <= 2.0 * be + 1e-7 and be <= 2.0 * berr[q] + 1e-7, (q, be, berr[q])
         assert fe <= kappa * 1e-6, (q, fe)
         assert 0 <= iters[q] <= 10
 
