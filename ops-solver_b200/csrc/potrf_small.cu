@@ -19,6 +19,8 @@
 //   ORDER_GROUP (9..32)    cholesky_vector.cpp:588-794  groups of four, separate rounding
 // Solve: cholesky_simt.cpp:93-117 (SolveKernel): forward fmaf chain then IEEE division,
 // backward fmaf chain over ascending j then IEEE division.
+#include <algorithm>
+
 #include "common.cuh"
 #include "launch.h"
 
@@ -378,15 +380,12 @@ __global__ void __launch_bounds__(32) potrs_lane_kernel(float *a_single, float *
     if (q < count) pb = b_table ? slot(b_table, b_first + q) : b_single;
     if (!mine || !pb) return;
     const float *tri = lane_mem + lane * P;
-    float diag[N], rd[N];
-    bool rok[N];
-#pragma unroll
-    for (int i = 0; i < N; ++i)
-    {
-        diag[i] = i < n ? tri[trap_at<N>(i, i)] : 1.0f;
-        rd[i] = div_prepare(diag[i]);
-        rok[i] = div_range(diag[i]);
-    }
+    // x_i / L(i, i): the diagonal and its reciprocal are read and formed at the step (they do
+    // not depend on x, so they are off the dependent chain)
+    auto divide = [&](float v, int i) {
+        const float d = tri[trap_at<N>(i, i)];
+        return div_by(v, d, div_prepare(d), div_range(d));
+    };
     for (int rhs = 0; rhs < nrhs; ++rhs)
     {
         float *xb = pb + (int64_t)rhs * ldb;
@@ -399,7 +398,7 @@ __global__ void __launch_bounds__(32) potrs_lane_kernel(float *a_single, float *
         {
             if (j < n)
             {
-                x[j] = div_by(x[j], diag[j], rd[j], rok[j]);
+                x[j] = divide(x[j], j);
 #pragma unroll
                 for (int i4 = 4 * (j / 4); i4 < N; i4 += 4)
                 {
@@ -427,7 +426,7 @@ __global__ void __launch_bounds__(32) potrs_lane_kernel(float *a_single, float *
                     if (j4 + 2 > i && j4 + 2 < n) acc = fma_rn(-l.z, x[j4 + 2], acc);
                     if (j4 + 3 > i && j4 + 3 < n) acc = fma_rn(-l.w, x[j4 + 3], acc);
                 }
-                x[i] = div_by(acc, diag[i], rd[i], rok[i]);
+                x[i] = divide(acc, i);
             }
         }
 #pragma unroll
@@ -577,9 +576,9 @@ cudaError_t potrs_lane_n(const RealBatch &a, const RealBatch &b, int nrhs, int u
     const size_t smem = (size_t)32 * trap_pitch<N>() * sizeof(float);
     cudaError_t e = cudaFuncSetAttribute(potrs_lane_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const int64_t blocks = (a.count + 31) / 32;
-    potrs_lane_kernel<N><<<(unsigned)(blocks < 1 ? 1 : blocks), 32, smem, stream>>>(
-        a.single, a.table, a.first, b.single, b.table, b.first, a.n, a.ld, b.ld, nrhs, upper, a.count, info);
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, (a.count + 31) / 32);
+    potrs_lane_kernel<N><<<blocks, 32, smem, stream>>>(a.single, a.table, a.first, b.single, b.table, b.first, a.n,
+                                                       a.ld, b.ld, nrhs, upper, a.count, info);
     return cudaGetLastError();
 }
 
