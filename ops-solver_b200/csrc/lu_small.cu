@@ -1,7 +1,8 @@
 // lu_small.cu -- batched real LU factor, solve and inverse for n <= 64 on sm_100a.
 //
 // getrf: one warp (or a width-N sub-warp for N < 32) owns a matrix; lane l holds rows
-// l and l+32 (N = 64) in registers.  Row interchanges are never moved in memory: each row
+// l and l+32 (N = 64) in registers (order 64: getrf_rot_kernel, the columns rotated through
+// the registers four at a time so that the step loop stays small).  Row interchanges are never moved in memory: each row
 // carries its current position and the pivot search reduces (|a| key, position) with
 // redux.sync, so the earliest-row tie rule of the reference sees the swapped order.  The
 // pivot row is broadcast through a per-warp shared-memory row buffer; every other row
@@ -186,6 +187,174 @@ __global__ void __launch_bounds__(LU_THREADS) getrf_small_kernel(float *single, 
             }
         }
         if (in_batch && lrow == 0) info[q] = live ? state : -2;
+    }
+}
+
+// Order 64 (m, n <= 64), the same arithmetic as getrf_small_kernel<64> with the columns
+// rotated through the registers in blocks of KB: the step loop is KB steps long and runs
+// 64 / KB times, so the kernel body fits the instruction cache (the fully unrolled 64-step
+// body did not: its warps stalled on instruction fetch).  Register column c holds matrix
+// column K0 + c.  After each block of KB steps its KB columns are final; they are parked
+// in a per-warp shared-memory copy indexed by physical row (pitch 65 floats: the lanes'
+// rows fall in different banks) and the remaining register columns shift down by KB.  The
+// final store reads the parked copy, each row to its final position.
+constexpr int ROT_N = 64;
+constexpr int ROT_PITCH = ROT_N + 1;
+constexpr size_t rot_smem_bytes()
+{
+    return (size_t)(LU_THREADS / 32) * (ROT_N + ROT_N * ROT_PITCH) * sizeof(float);
+}
+
+template <int KB>
+__global__ void __launch_bounds__(LU_THREADS, 3) getrf_rot_kernel(float *single, float *const *table, int first, int m,
+                                                               int n, int lda, int count, int *ipiv, int *info)
+{
+    constexpr int N = ROT_N, SUBW = 32, RPL = 2;
+    static_assert(KB % 4 == 0 && N % KB == 0, "blocks of whole 16-byte column groups");
+    extern __shared__ __align__(16) float rot_mem[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    float *prow = rot_mem + warp * N;
+    float *fin = rot_mem + (LU_THREADS / 32) * N + warp * N * ROT_PITCH;
+    const int warp_global = (blockIdx.x * LU_THREADS + threadIdx.x) >> 5;
+    const int warps_total = (gridDim.x * LU_THREADS) >> 5;
+    const bool pivoting = ipiv != nullptr;
+    const int steps = m < n ? m : n;
+
+    for (int64_t q = warp_global; q < count; q += warps_total)
+    {
+        float *p = table ? slot(table, first + q) : single;
+        const bool live = p != nullptr;
+
+        float a[RPL][N];
+        int pos[RPL];
+        int pv[RPL];
+#pragma unroll
+        for (int s = 0; s < RPL; ++s)
+        {
+            const int phys = lane + s * SUBW;
+            pos[s] = phys;
+            pv[s] = phys + 1;
+#pragma unroll
+            for (int j = 0; j < N; ++j)
+                a[s][j] = (live && phys < m && j < n) ? p[phys + (int64_t)j * lda] : 0.0f;
+        }
+        int state = 0;
+
+#pragma unroll 1
+        for (int K0 = 0; K0 < N; K0 += KB)
+        {
+            const int width = N - K0;  // register columns that hold matrix columns
+#pragma unroll
+            for (int kk = 0; kk < KB; ++kk)
+            {
+                const int k = K0 + kk;
+                if (k < steps)
+                {
+                    int pr = k, ph = k;
+                    if (pivoting)
+                    {
+                        unsigned key[RPL];
+#pragma unroll
+                        for (int s = 0; s < RPL; ++s)
+                        {
+                            const int phys = lane + s * SUBW;
+                            const float v = a[s][kk];
+                            key[s] = (pos[s] >= k && phys < m) ? pivot_key(v) : 0u;
+                            if (pos[s] == k && v != v) key[s] = 0xffffffffu;
+                        }
+                        const unsigned mx = warp_max_u32<SUBW>(max(key[0], key[1]));
+                        unsigned cand = 0xffffffffu;
+#pragma unroll
+                        for (int s = 0; s < RPL; ++s)
+                            if (key[s] == mx) cand = min(cand, (unsigned)((pos[s] << 8) | (lane + s * SUBW)));
+                        const unsigned mn = warp_min_u32<SUBW>(cand);
+                        pr = (int)(mn >> 8);
+                        ph = (int)(mn & 255u);
+                        if (lane == k % SUBW)
+                        {
+                            if (k < SUBW)
+                                pv[0] = pr + 1;
+                            else
+                                pv[1] = pr + 1;
+                        }
+#pragma unroll
+                        for (int s = 0; s < RPL; ++s) pos[s] = pos[s] == k ? pr : (pos[s] == pr ? k : pos[s]);
+                    }
+                    // the pivot row's register columns >= kk (aligned down to 4) to the row buffer
+                    __syncwarp();
+                    {
+                        const int owner_slot = ph / SUBW;
+                        const bool owner = lane == (ph % SUBW);
+#pragma unroll
+                        for (int s = 0; s < RPL; ++s)
+                        {
+                            if (owner && owner_slot == s)
+                            {
+#pragma unroll
+                                for (int j = (kk & ~3); j < N; j += 4)
+                                    if (j < width)
+                                        *reinterpret_cast<float4 *>(prow + j) =
+                                            make_float4(a[s][j], a[s][j + 1], a[s][j + 2], a[s][j + 3]);
+                            }
+                        }
+                    }
+                    __syncwarp();
+                    const float d = prow[kk];
+                    if (d == 0.0f && state == 0) state = k + 1;
+                    const bool update = d != 0.0f && k + 1 < m;
+#pragma unroll
+                    for (int s = 0; s < RPL; ++s)
+                    {
+                        const int phys = lane + s * SUBW;
+                        if (update && pos[s] > k && phys < m)
+                        {
+                            const float l = div_rn(a[s][kk], d);
+                            a[s][kk] = l;
+#pragma unroll
+                            for (int j4 = ((kk + 1) & ~3); j4 < N; j4 += 4)
+                            {
+                                if (j4 < width)
+                                {
+                                    const float4 u = *reinterpret_cast<const float4 *>(prow + j4);
+                                    if (j4 + 0 > kk) a[s][j4 + 0] = fma_rn(-l, u.x, a[s][j4 + 0]);
+                                    if (j4 + 1 > kk) a[s][j4 + 1] = fma_rn(-l, u.y, a[s][j4 + 1]);
+                                    if (j4 + 2 > kk) a[s][j4 + 2] = fma_rn(-l, u.z, a[s][j4 + 2]);
+                                    if (j4 + 3 > kk) a[s][j4 + 3] = fma_rn(-l, u.w, a[s][j4 + 3]);
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            // columns K0 .. K0 + KB - 1 are final: park them, shift the rest down
+#pragma unroll
+            for (int s = 0; s < RPL; ++s)
+            {
+                float *row = fin + (lane + s * SUBW) * ROT_PITCH + K0;
+#pragma unroll
+                for (int c = 0; c < KB; ++c) row[c] = a[s][c];
+#pragma unroll
+                for (int j = 0; j + KB < N; ++j) a[s][j] = a[s][j + KB];
+            }
+        }
+        __syncwarp();
+        if (live)
+        {
+#pragma unroll
+            for (int s = 0; s < RPL; ++s)
+            {
+                const int phys = lane + s * SUBW;
+                if (phys < m)
+                {
+                    const float *row = fin + phys * ROT_PITCH;
+                    for (int j = 0; j < n; ++j) p[pos[s] + (int64_t)j * lda] = row[j];
+                    if (pivoting && phys < steps) ipiv[q * steps + phys] = pv[s];
+                }
+            }
+        }
+        if (lane == 0) info[q] = live ? state : -2;
+        __syncwarp();  // the parked copy and the row buffer are rewritten by the next matrix
     }
 }
 
@@ -529,6 +698,22 @@ cudaError_t getrf_n(const RealBatch &a, int m, int *ipiv, int *info, cudaStream_
     return cudaGetLastError();
 }
 
+constexpr int GETRF_ROT_KB = 4;  // columns per rotation block of the order-64 factorisation
+
+template <int KB>
+cudaError_t getrf_rot(const RealBatch &a, int m, int *ipiv, int *info, cudaStream_t stream)
+{
+    const size_t smem = rot_smem_bytes();
+    cudaError_t e = cudaFuncSetAttribute(getrf_rot_kernel<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int64_t blocks = (a.count * 32 + LU_THREADS - 1) / LU_THREADS;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    if (blocks < 1) blocks = 1;
+    getrf_rot_kernel<KB><<<(unsigned)blocks, LU_THREADS, smem, stream>>>(a.single, a.table, a.first, m, a.n, a.ld,
+                                                                        a.count, ipiv, info);
+    return cudaGetLastError();
+}
+
 template <int N>
 cudaError_t getrs_n(const RealBatch &a, const int *ipiv, const RealBatch &b, int nrhs, int trans, int *info,
                     cudaStream_t stream)
@@ -566,7 +751,7 @@ cudaError_t launch_getrf_small(const RealBatch &a, int m, int *ipiv, int *info, 
     if (big <= 8) return getrf_n<8>(a, m, ipiv, info, stream);
     if (big <= 16) return getrf_n<16>(a, m, ipiv, info, stream);
     if (big <= 32) return getrf_n<32>(a, m, ipiv, info, stream);
-    return getrf_n<64>(a, m, ipiv, info, stream);
+    return getrf_rot<GETRF_ROT_KB>(a, m, ipiv, info, stream);
 }
 
 cudaError_t launch_getrs_small(const RealBatch &a, const int *ipiv, const RealBatch &b, int nrhs, int trans,
