@@ -13,6 +13,8 @@
 // success path and the factor kernels then write every batch entry.
 #include <stdio.h>
 
+#include <vector>
+
 #include "handle.h"
 #include "launch.h"
 #include "launch_complex.h"
@@ -55,6 +57,31 @@ aclsolverStatus_t info_span(const int *info, int64_t count)
     if (!is_device_pointer(info)) return ACLSOLVER_STATUS_INVALID_VALUE;
     if (!device_span(info, (size_t)count * sizeof(int))) return ACLSOLVER_STATUS_INVALID_VALUE;
     return ACLSOLVER_STATUS_SUCCESS;
+}
+
+// Orders above CPOTRF_PACKED_MAX: one matrix at a time over the whole GPU, the backup for
+// the failure contract in handle scratch.  A batch's pointer table is read back first, so
+// that call synchronises; a null slot sets its info to -3.
+aclsolverStatus_t factor_large(Handle *h, float2 *single, float2 *const *table, int n, int lda, int upper, int count,
+                               int *info)
+{
+    ScratchBlock *blk = acquire_scratch(h, cpotrf_large_scratch_bytes(n));
+    if (!blk) return ACLSOLVER_STATUS_ALLOC_FAILED;
+    cudaError_t e = cudaSuccess;
+    if (!table)
+        e = launch_cpotrf_large(single, lda, upper, n, info, blk->ptr, h->stream);
+    else
+    {
+        std::vector<float2 *> ptrs((size_t)count);
+        e = cudaMemcpyAsync(ptrs.data(), table, (size_t)count * sizeof(float2 *), cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        for (int q = 0; q < count && e == cudaSuccess; ++q)
+            e = ptrs[q] ? launch_cpotrf_large(ptrs[q], lda, upper, n, info + q, blk->ptr, h->stream)
+                        : launch_fill_info(info + q, -3, 1, h->stream);
+    }
+    aclsolverStatus_t launched = launch_status(e);
+    aclsolverStatus_t fin = finish_scratch(h, blk);
+    return launched != ACLSOLVER_STATUS_SUCCESS ? launched : fin;
 }
 
 // Finish: pre-writes info[0] = -argument (0 when the arguments are valid).
@@ -122,6 +149,7 @@ extern "C"
         aclsolverStatus_t st = finish(handle, devInfo, arg);
         if (st != ACLSOLVER_STATUS_SUCCESS || n == 0) return st;
         Handle *h = to_handle(handle);
+        if (n > CPOTRF_PACKED_MAX) return factor_large(h, reinterpret_cast<float2 *>(A), nullptr, n, lda, uplo, 1, devInfo);
         return launch_status(launch_cpotrf(reinterpret_cast<float2 *>(A), nullptr, n, lda, uplo, 1, devInfo, h->stream));
     }
 
@@ -192,6 +220,9 @@ extern "C"
         if (st != ACLSOLVER_STATUS_SUCCESS || batchSize == 0) return st;
         Handle *h = to_handle(handle);
         if (n == 0) return launch_status(launch_fill_info(infoArray, 0, batchSize, h->stream));
+        if (n > CPOTRF_PACKED_MAX)
+            return factor_large(h, nullptr, reinterpret_cast<float2 *const *>(Aarray), n, lda, uplo, batchSize,
+                                infoArray);
         return launch_status(launch_cpotrf(nullptr, reinterpret_cast<float2 *const *>(Aarray), n, lda, uplo, batchSize,
                                            infoArray, h->stream));
     }

@@ -14,10 +14,11 @@
 // held to the 1e-5 relative tolerance and the reference's complex128 residual gate.
 //
 // Layouts: n <= 16 -- a width-N sub-warp per matrix, lane i holds row i (re[], im[]) and the
-// finished column is broadcast through shared memory; 17..128 -- one block per matrix, the
-// lower triangle packed in shared memory, a thread per row, factored left-looking in blocks
-// of 16 columns and solved in blocks of 16 rows (complex_block.cuh); above 128 -- one block
-// per matrix working in global memory.
+// finished column is broadcast through shared memory; 17..240 -- one block per matrix (64, 128
+// or 256 threads), the lower triangle packed in shared memory (n = 240: 226 KB), factored
+// left-looking in blocks of 16 columns and solved a warp per right-hand side
+// (complex_block.cuh); above 240 the factor runs one matrix at a time over the whole GPU
+// (cpotrf_large.cu) and the solve one block per matrix from global memory.
 // (A 32-lane register version needs more than 255 registers per lane for the complex rows.)
 #include "common.cuh"
 #include "complex_block.cuh"
@@ -272,62 +273,6 @@ __global__ void __launch_bounds__(T) cpotrs_cb_kernel(const float2 *a_single, co
 }
 
 // ---------------------------------------------------------------------------------------
-// n > 128: left-looking in global memory (same per-element order)
-// ---------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) cpotrf_left_kernel(float2 *single, float2 *const *table, int n, int lda,
-                                                          int upper, int count, int *info)
-{
-    extern __shared__ float2 colbuf[];
-    __shared__ int failed;
-    for (int64_t q = blockIdx.x; q < count; q += gridDim.x)
-    {
-        float2 *p = table ? slot(table, q) : single;
-        if (!p)
-        {
-            if (threadIdx.x == 0) info[q] = -3;
-            continue;
-        }
-        if (threadIdx.x == 0) failed = 0;
-        __syncthreads();
-        for (int j = 0; j < n; ++j)
-        {
-            for (int i = j + threadIdx.x; i < n; i += 256)
-            {
-                float2 z = load_tri(p, lda, upper, i, j);
-                for (int k = 0; k < j; ++k)
-                {
-                    const float2 l = load_tri(p, lda, upper, i, k);
-                    const float2 c = load_tri(p, lda, upper, j, k);
-                    sub_lconj(z.x, z.y, l.x, l.y, c.x, c.y);
-                }
-                colbuf[i] = z;
-            }
-            __syncthreads();
-            const float d = colbuf[j].x;
-            if (!(d > 0.0f && d <= FLT_MAX_VALUE))
-            {
-                if (threadIdx.x == 0) failed = j + 1;
-                __syncthreads();
-                break;
-            }
-            const float s = sqrt_rn(d);
-            for (int i = j + threadIdx.x; i < n; i += 256)
-            {
-                const float2 z = colbuf[i];
-                if (i == j)
-                    store_tri(p, lda, upper, i, j, s, 0.0f);
-                else
-                    store_tri(p, lda, upper, i, j, div_rn(z.x, s), div_rn(z.y, s));
-            }
-            __syncthreads();
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) info[q] = failed;
-        __syncthreads();
-    }
-}
-
-// ---------------------------------------------------------------------------------------
 // solve (any n): one block per matrix, L staged in shared memory when it fits, rows over
 // threads, right-looking sweeps; right-hand sides one after another.
 // ---------------------------------------------------------------------------------------
@@ -428,14 +373,15 @@ cudaError_t launch_cpotrf(float2 *single, float2 *const *table, int n, int lda, 
         cpotrf_cb_kernel<128><<<grid_of(count, 1, 148 * 8), 128, smem, stream>>>(single, table, n, lda, upper,
                                                                                 count, info);
     }
-    else
+    else if (n <= CPOTRF_PACKED_MAX)
     {
-        size_t smem = (size_t)n * sizeof(float2);
-        if (smem > 48 * 1024)
-            cudaFuncSetAttribute(cpotrf_left_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cpotrf_left_kernel<<<grid_of(count, 1, 148 * 4), 256, smem, stream>>>(single, table, n, lda, upper, count,
-                                                                             info);
+        const size_t smem = cb_smem_bytes(n);
+        cudaFuncSetAttribute(cpotrf_cb_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cpotrf_cb_kernel<256><<<grid_of(count, 1, 148 * 2), 256, smem, stream>>>(single, table, n, lda, upper,
+                                                                                count, info);
     }
+    else
+        return cudaErrorInvalidValue;  // one matrix at a time over the whole GPU: launch_cpotrf_large
     return cudaGetLastError();
 }
 
@@ -443,7 +389,7 @@ cudaError_t launch_cpotrs(const float2 *a_single, const float2 *const *a_table, 
                           float2 *const *b_table, int n, int lda, int ldb, int nrhs, int upper, int count,
                           const int *info, cudaStream_t stream)
 {
-    if (n > 16 && n <= 128)
+    if (n > 16 && n <= CPOTRF_PACKED_MAX)
     {
         const size_t smem = cb_smem_bytes(n);
         if (n <= 64)
@@ -452,10 +398,16 @@ cudaError_t launch_cpotrs(const float2 *a_single, const float2 *const *a_table, 
             cpotrs_cb_kernel<64><<<grid_of(count, 1, 148 * 16), 64, smem, stream>>>(
                 a_single, a_table, b_single, b_table, n, lda, ldb, nrhs, upper, count, info);
         }
-        else
+        else if (n <= 128)
         {
             cudaFuncSetAttribute(cpotrs_cb_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             cpotrs_cb_kernel<128><<<grid_of(count, 1, 148 * 8), 128, smem, stream>>>(
+                a_single, a_table, b_single, b_table, n, lda, ldb, nrhs, upper, count, info);
+        }
+        else
+        {
+            cudaFuncSetAttribute(cpotrs_cb_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cpotrs_cb_kernel<256><<<grid_of(count, 1, 148 * 2), 256, smem, stream>>>(
                 a_single, a_table, b_single, b_table, n, lda, ldb, nrhs, upper, count, info);
         }
         return cudaGetLastError();

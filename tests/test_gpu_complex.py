@@ -15,7 +15,7 @@ from helpers import info_buffer, same_bits
 
 pytestmark = pytest.mark.gpu
 SENTINEL = np.complex64(93 - 47j)  # the reference fixtures' padding value
-SIZES = [1, 2, 7, 8, 9, 16, 17, 31, 32, 33, 48, 64, 65, 100, 128, 129, 160]
+SIZES = [1, 2, 7, 8, 9, 16, 17, 31, 32, 33, 48, 64, 65, 100, 128, 129, 160, 200, 240]
 
 
 def hpd(count, n, seed):
@@ -123,7 +123,7 @@ def test_complex_null_handle_is_not_initialized(handle):
 
 
 @pytest.mark.parametrize("upper", [False, True])
-@pytest.mark.parametrize("n", [1, 8, 17, 32, 33, 64, 100, 128, 150])
+@pytest.mark.parametrize("n", [1, 8, 17, 32, 33, 64, 100, 128, 150, 240, 241])
 def test_cpotrs_batched(handle, n, upper):
     lib = aclsolver.library()
     a = hpd(4, n, seed=100 + n)
@@ -239,3 +239,47 @@ def test_cpotri_invalid_diagonal(handle):
     handle.stream.synchronize()
     assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 7
     assert dm.unchanged()
+
+
+@pytest.mark.parametrize("upper", [False, True])
+@pytest.mark.parametrize("n", [241, 300, 521])
+def test_cpotrf_large_over_the_whole_gpu(handle, n, upper):
+    """Orders above the shared-memory block path: one matrix over the whole GPU (64-column
+    panels, diagonal block / rows / trailing Hermitian update kernels), bit for bit the
+    oracle's order, padding untouched, within 1e-5 of FP64 LAPACK."""
+    lib = aclsolver.library()
+    a = hpd(1, n, seed=n + int(upper))
+    da = CMatrices(a, n + 3)
+    info = info_buffer(1)
+    st = lib.aclsolverCpotrf(handle.value, int(upper), n, da.tensor.data_ptr(), da.ld, None, 0, info.data_ptr())
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 0
+    got = da.read()
+    want, winfo = oracle.cpotrf_batched(a, upper=upper)
+    assert winfo[0] == 0
+    assert cbits(got, want), "large complex factor differs from the oracle"
+    tri = np.triu(got[0]) if upper else np.tril(got[0])
+    gold = la.cholesky(a[0].astype(np.complex128), lower=not upper)
+    assert np.abs(tri - gold).max() <= 1e-5 * max(1.0, np.abs(gold).max())
+
+
+def test_cpotrf_large_batched_failures_keep_the_input_from_the_failed_column(handle):
+    """CpotrfBatched above the block orders, one matrix at a time: a pivot failing in the
+    first panel and one failing in a later panel (NaN) report their column; the completed
+    columns hold the factor and the failed column onward the caller's input, as the
+    oracle; a null slot gives -3."""
+    lib = aclsolver.library()
+    n = 260
+    a = hpd(4, n, seed=21)
+    a[1, 70, 70] = -1.0
+    a[2, 255, 255] = np.nan
+    dm = CMatrices(a, n)
+    dm.table[3] = 0
+    info = info_buffer(4)
+    st = lib.aclsolverCpotrfBatched(handle.value, 0, n, dm.table.data_ptr(), n, info.data_ptr(), 4)
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS
+    want, winfo = oracle.cpotrf_batched(a[:3])
+    assert winfo.tolist() == [0, 71, 256]
+    assert info.cpu().tolist() == [0, 71, 256, -3]
+    assert cbits(dm.read()[:3], want)
