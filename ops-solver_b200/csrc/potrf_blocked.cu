@@ -10,10 +10,11 @@
 //
 // 33 <= n <= 256, any batch: one block per matrix, the lower triangle packed by columns in
 // shared memory (n = 256: 132 KB, one block per SM; n = 128: 33 KB), factored left-looking in
-// blocks of 16 columns: thread t owns row J0 + t of block column J0 in registers, applies
-// every earlier column to it (sixteen broadcast loads of the block's L(J0 + j, k) per k),
-// then the sixteen panel steps run with one barrier each; every thread keeps the block's
-// diagonal so the square roots need no second exchange.  Untouched columns stay untouched,
+// blocks of 16 columns: every earlier column is first applied to block column J0 in shared
+// memory, 16 / C threads per remaining row with C adjacent columns each (broadcast loads of
+// the block's L(J0 + j, k)); then thread t takes row J0 + t into registers and the sixteen
+// panel steps run with one barrier each, dividing only rows that exist; every thread keeps
+// the block's diagonal so the square roots need no second exchange.  Untouched columns stay untouched,
 // which keeps the failure contract for free.
 //
 // n > 256 (one matrix over the whole GPU, 64-column panels): the matrix is first copied to
@@ -56,6 +57,42 @@ __device__ __forceinline__ int64_t tri_at(int lda, int upper, int i, int j)
     return upper ? (int64_t)i * lda + j : (int64_t)j * lda + i;
 }
 
+// The left-looking update of block column J0 (rows J0..n-1, its w columns) by every earlier
+// column k < J0, in shared memory: G = RB / C threads share a row, each taking C adjacent
+// columns of it, so that the whole block works however few rows remain below J0.  Every
+// element still takes its updates one after another in ascending k, from one thread.
+template <int C>
+__device__ __forceinline__ void rb_left(float *tri, int n, int J0, int w)
+{
+    constexpr int G = RB / C;
+    const int t = threadIdx.x;
+    const int i = J0 + t / G;    // row
+    const int j0 = (t % G) * C;  // first column of this thread within the block
+    if (i >= n) return;
+    float z[C];
+#pragma unroll
+    for (int u = 0; u < C; ++u)
+    {
+        const int j = j0 + u;
+        z[u] = (j < w && J0 + j <= i) ? tri[rb_col(J0 + j, n) + i - (J0 + j)] : 0.0f;
+    }
+    int ok = 0;  // packed offset of column k
+    for (int k = 0; k < J0; ++k)
+    {
+        const float a = tri[ok + i - k];
+        const float *c = tri + ok + J0 - k + j0;  // c[u] = L(J0 + j0 + u, k)
+#pragma unroll
+        for (int u = 0; u < C; ++u) z[u] = fma_rn(-a, c[u], z[u]);
+        ok += n - k;
+    }
+#pragma unroll
+    for (int u = 0; u < C; ++u)
+    {
+        const int j = j0 + u;
+        if (j < w && J0 + j <= i) tri[rb_col(J0 + j, n) + i - (J0 + j)] = z[u];
+    }
+}
+
 template <int T>
 __global__ void __launch_bounds__(T) potrf_packed_kernel(float *single, float *const *table, int first, int n,
                                                          int lda, int upper, int count, int *info)
@@ -89,24 +126,28 @@ __global__ void __launch_bounds__(T) potrf_packed_kernel(float *single, float *c
         for (int J0 = 0; J0 < n && !failure; J0 += RB)
         {
             const int w = min(RB, n - J0);
+            if (J0 > 0)
+            {
+                // threads per row: the most that fit the rows left (uniform over the block)
+                const int rows = n - J0;
+                if (rows > T / 2)
+                    rb_left<16>(tri, n, J0, w);
+                else if (rows > T / 4)
+                    rb_left<8>(tri, n, J0, w);
+                else if (rows > T / 8)
+                    rb_left<4>(tri, n, J0, w);
+                else if (rows > T / 16)
+                    rb_left<2>(tri, n, J0, w);
+                else
+                    rb_left<1>(tri, n, J0, w);
+                __syncthreads();
+            }
             const int i = J0 + t;
             const bool own = i < n;
             float z[RB];
 #pragma unroll
             for (int j = 0; j < RB; ++j)
                 z[j] = (own && j < w && J0 + j <= i) ? tri[rb_col(J0 + j, n) + i - (J0 + j)] : 0.0f;
-            if (own)
-            {
-                int ok = 0;
-                for (int k = 0; k < J0; ++k)
-                {
-                    const float a = tri[ok + i - k];
-                    const float *c = tri + ok + J0 - k;
-#pragma unroll
-                    for (int j = 0; j < RB; ++j) z[j] = fma_rn(-a, c[j], z[j]);
-                    ok += n - k;
-                }
-            }
             if (t < w)
             {
                 float dv = 0.0f;
@@ -136,7 +177,7 @@ __global__ void __launch_bounds__(T) potrf_packed_kernel(float *single, float *c
                         float l = z[kk];
                         if (i == k)
                             l = sq;
-                        else if (i > k)
+                        else if (i > k && own)  // rows past n would take the slow division on zeros
                             l = div_by(l, sq, y, okd);
                         z[kk] = l;
                         float *sl = xch + (kk & 1) * RB;
