@@ -114,6 +114,48 @@ def test_sgetrf_single(handle, m, n):
     assert judges.lu_reconstruction_ok(a[0], dm.read()[0], wpiv[0])
 
 
+@pytest.mark.parametrize("name", ["2x2 subnormal pivot", "2x2 normal-scale control", "513x1 subnormal pivot"])
+def test_sgetrf_subnormal_pivot_cases(handle, name):
+    """The reference's subnormal-pivot cases (test/sgetrf/sgetrf_subnormal_pivot_test.cpp:
+    157-167): a 2 x 2 matrix of subnormal entries, its normal-scale control, and a 513 x 1
+    column of subnormals (the tall, single-column case, here on the whole-GPU path); the
+    factors equal the oracle's bit for bit and P A = L U holds to 1e-5 relative, as the
+    reference's check asks."""
+    import torch
+
+    tiny = np.float32(1.0e-39)
+    cases = {
+        "2x2 subnormal pivot": (2, 2, [2 * tiny, tiny, tiny, 2 * tiny]),
+        "2x2 normal-scale control": (2, 2, [4.0e-38, 2.0e-38, 2.0e-38, 4.0e-38]),
+        "513x1 subnormal pivot": (513, 1, [tiny] * 513),
+    }
+    m, n, values = cases[name]
+    a = np.asarray(values, dtype=np.float32).reshape(1, m, n)  # row-major values, as the reference lists them
+    lib = aclsolver.library()
+    dm = DeviceMatrices(a, ld=m)
+    lw = C.c_int(-1)
+    assert lib.aclsolverSgetrf_bufferSize(handle.value, m, n, dm.ptr, m, C.byref(lw)) == aclsolver.SUCCESS
+    work = torch.empty(max(1, lw.value), dtype=torch.float32, device="cuda")
+    piv = device_ints(np.zeros(min(m, n)))
+    info = info_buffer(1)
+    st = lib.aclsolverSgetrf(handle.value, m, n, dm.ptr, m, work.data_ptr(), piv.data_ptr(), info.data_ptr())
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 0
+    lu, wpiv, winfo = oracle.sgetrf_batched(a)
+    assert winfo[0] == 0 and piv.cpu().tolist() == wpiv[0].tolist()
+    got = dm.read()[0]
+    assert same_bits(got, lu[0])
+    # P A = L U in FP64, relative to max |A|
+    k = min(m, n)
+    low = np.tril(got.astype(np.float64), -1)[:, :k] + np.eye(m, k)
+    up = np.triu(got.astype(np.float64))[:k, :]
+    pa = a[0].astype(np.float64).copy()
+    for i, p in enumerate(wpiv[0]):
+        pa[[i, p - 1]] = pa[[p - 1, i]]
+    resid = np.abs(pa - low @ up).max() / np.abs(a[0]).max()
+    assert np.isfinite(resid) and resid <= 1e-5, resid
+
+
 def test_sgetrf_known_answer(handle):
     lib = aclsolver.library()
     case = KA["sgetrf_4x4"]
