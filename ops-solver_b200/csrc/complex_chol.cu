@@ -8,7 +8,9 @@
 //       re = fma(-ar, cr, re); re = fma(-ai, ci, re); im = fma(-ai, cr, im); im = fma(ar, ci, im)
 //   with l_ik = (ar, ai), l_jk = (cr, ci).  A failed matrix keeps its completed columns.
 //   solve: forward z_i -= l_ik * y_k (y_k = z_k / l_kk) and backward z_i -= conj(l_ki) * x_k,
-//   both right-looking, the complex products again as two FMAs per component.
+//   both right-looking, the complex products again as two FMAs per component; above order
+//   240 in blocks of 64 rows, the rows outside a block taking it as one partial sum from
+//   zero and one subtraction (orc_cpotrs_blocked).
 // The reference's own kernels (src/cpotrf/arch35) keep a compensated double-float first
 // column and diagonal and hand n > 64 to a CATLASS complex GEMM, so parity with them is
 // held to the 1e-5 relative tolerance and the reference's complex128 residual gate.
@@ -39,6 +41,17 @@ __device__ __forceinline__ void sub_lconj(float &re, float &im, float ar, float 
     im = fma_rn(-ai, cr, im);
     im = fma_rn(ar, ci, im);
 }
+// t += l * y, a block's partial sum in the large-order solve:
+//   tr = fma(lr, yr, tr); tr = fma(-li, yi, tr); ti = fma(lr, yi, ti); ti = fma(li, yr, ti)
+__device__ __forceinline__ void add_prod(float2 &t, float2 l, float2 y)
+{
+    t.x = fma_rn(l.x, y.x, t.x);
+    t.x = fma_rn(-l.y, y.y, t.x);
+    t.y = fma_rn(l.x, y.y, t.y);
+    t.y = fma_rn(l.y, y.x, t.y);
+}
+constexpr int SOLVE_BLOCK = 64;  // rows per block of the large-order solve's partial sums
+
 // z -= l * y
 __device__ __forceinline__ void sub_prod(float &re, float &im, float ar, float ai, float yr, float yi)
 {
@@ -304,36 +317,66 @@ __global__ void __launch_bounds__(128) cpotrs_block_kernel(const float2 *a_singl
             float2 *xb = pb + (int64_t)r * ldb;
             for (int i = threadIdx.x; i < n; i += 128) x[i] = xb[i];
             __syncthreads();
-            for (int k = 0; k < n; ++k)
+            // forward in blocks of SOLVE_BLOCK rows: inside a block y_k = z_k / l_kk and the
+            // block's later rows take z_i -= l_ik y_k; the rows below take the block as one
+            // partial sum t = sum_k l_ik y_k from zero (ascending k), then z_i - t
+            for (int K0 = 0; K0 < n; K0 += SOLVE_BLOCK)
             {
-                const float dk = L(k, k).x;
-                const float2 zk = x[k];
-                const float yr = div_rn(zk.x, dk), yi = div_rn(zk.y, dk);
-                for (int i = k + 1 + threadIdx.x; i < n; i += 128)
+                const int kend = min(K0 + SOLVE_BLOCK, n);
+                for (int k = K0; k < kend; ++k)
                 {
-                    const float2 l = L(i, k);
-                    float2 z = x[i];
-                    sub_prod(z.x, z.y, l.x, l.y, yr, yi);
-                    x[i] = z;
+                    const float dk = L(k, k).x;
+                    const float2 zk = x[k];
+                    const float yr = div_rn(zk.x, dk), yi = div_rn(zk.y, dk);
+                    for (int i = k + 1 + threadIdx.x; i < kend; i += 128)
+                    {
+                        const float2 l = L(i, k);
+                        float2 z = x[i];
+                        sub_prod(z.x, z.y, l.x, l.y, yr, yi);
+                        x[i] = z;
+                    }
+                    __syncthreads();
+                    if (threadIdx.x == 0) x[k] = make_float2(yr, yi);
+                    __syncthreads();
                 }
-                __syncthreads();
-                if (threadIdx.x == 0) x[k] = make_float2(yr, yi);
+                for (int i = kend + threadIdx.x; i < n; i += 128)
+                {
+                    float2 t = make_float2(0.0f, 0.0f);
+                    for (int k = K0; k < kend; ++k) add_prod(t, L(i, k), x[k]);
+                    x[i] = make_float2(sub_rn(x[i].x, t.x), sub_rn(x[i].y, t.y));
+                }
                 __syncthreads();
             }
-            for (int k = n - 1; k >= 0; --k)
+            // backward, blocks in descending order, with conj(l_ki)
+            for (int K0 = ((n - 1) / SOLVE_BLOCK) * SOLVE_BLOCK; n > 0 && K0 >= 0; K0 -= SOLVE_BLOCK)
             {
-                const float dk = L(k, k).x;
-                const float2 zk = x[k];
-                const float yr = div_rn(zk.x, dk), yi = div_rn(zk.y, dk);
-                for (int i = threadIdx.x; i < k; i += 128)
+                const int kend = min(K0 + SOLVE_BLOCK, n);
+                for (int k = kend - 1; k >= K0; --k)
                 {
-                    const float2 l = L(k, i);
-                    float2 z = x[i];
-                    sub_prod(z.x, z.y, l.x, -l.y, yr, yi);
-                    x[i] = z;
+                    const float dk = L(k, k).x;
+                    const float2 zk = x[k];
+                    const float yr = div_rn(zk.x, dk), yi = div_rn(zk.y, dk);
+                    for (int i = K0 + threadIdx.x; i < k; i += 128)
+                    {
+                        const float2 l = L(k, i);
+                        float2 z = x[i];
+                        sub_prod(z.x, z.y, l.x, -l.y, yr, yi);
+                        x[i] = z;
+                    }
+                    __syncthreads();
+                    if (threadIdx.x == 0) x[k] = make_float2(yr, yi);
+                    __syncthreads();
                 }
-                __syncthreads();
-                if (threadIdx.x == 0) x[k] = make_float2(yr, yi);
+                for (int i = threadIdx.x; i < K0; i += 128)
+                {
+                    float2 t = make_float2(0.0f, 0.0f);
+                    for (int k = K0; k < kend; ++k)
+                    {
+                        const float2 l = L(k, i);
+                        add_prod(t, make_float2(l.x, -l.y), x[k]);
+                    }
+                    x[i] = make_float2(sub_rn(x[i].x, t.x), sub_rn(x[i].y, t.y));
+                }
                 __syncthreads();
             }
             for (int i = threadIdx.x; i < n; i += 128) xb[i] = x[i];

@@ -1,13 +1,15 @@
 // cpotrf_large.cu -- complex64 Cholesky of one matrix above the packed-triangle orders, over
 // the whole GPU (aclsolverCpotrf; aclsolverCpotrfBatched takes it one matrix at a time).
 //
-// Arithmetic: the per-element order of orc_cpotrf (oracle/oracle.c) and of the other complex
-// kernels -- every a_ij, j <= i, takes its updates a_ij -= l_ik conj(l_jk) as four FMAs in
-// ascending k (re = fma(-ar, cr, re); re = fma(-ai, ci, re); im = fma(-ai, cr, im);
-// im = fma(ar, ci, im) with l_ik = (ar, ai), l_jk = (cr, ci)); then the pivot check on
-// d = Re a_jj (d > 0 and d <= FLT_MAX), s = sqrt(d) (IEEE), l_jj = (s, 0), and the IEEE
-// division of both components of the column below by s.  Only the schedule differs from the
-// oracle's loop, so the factor is the oracle's bit for bit.
+// Arithmetic (orc_cpotrf_blocked in oracle/oracle.c): inside a 64-column panel every a_ij,
+// j <= i, takes the panel's updates a_ij -= l_ik conj(l_jk) as four FMAs in ascending k
+// (re = fma(-ar, cr, re); re = fma(-ai, ci, re); im = fma(-ai, cr, im); im = fma(ar, ci, im)
+// with l_ik = (ar, ai), l_jk = (cr, ci)); an element right of the panel takes the panel's
+// products as one partial sum from zero and one subtraction (see herk below), which keeps
+// the rounding at a blocked LAPACK's size, as the reference's residual gate asks.  Then the
+// pivot check on d = Re a_jj (d > 0 and d <= FLT_MAX), s = sqrt(d) (IEEE), l_jj = (s, 0),
+// and the IEEE division of both components of the column below by s.  The factor is the
+// oracle's bit for bit.
 //
 // Right-looking with 64-column panels; per panel
 //   diag:  one block factors the 64 x 64 diagonal block in shared memory;
@@ -15,7 +17,8 @@
 //          128 rows per block;
 //   herk:  the trailing lower triangle takes A22 -= L21 L21^H over 64 x 64 tiles (lower tiles
 //          only), both operand panels staged in shared memory, a 4 x 4 tile of complex
-//          accumulators per thread.
+//          accumulators per thread: per element the panel's 64 products form one partial
+//          sum t from zero (ascending k), then a_ij - t (orc_cpotrf_blocked).
 // Failure contract (the reference's): the columns before the failed one keep their factor,
 // the failed column and all after it keep the caller's input.  The lower triangle is backed
 // up first; every kernel reads info and stops once a pivot has failed, and a restore pass
@@ -60,6 +63,16 @@ __device__ __forceinline__ void sub_lconj(float2 &z, float2 l, float2 c)
     z.x = fma_rn(-l.y, c.y, z.x);
     z.y = fma_rn(-l.y, c.x, z.y);
     z.y = fma_rn(l.x, c.y, z.y);
+}
+
+// t += l * conj(c), the partial sum of a panel:
+//   tr = fma(ar, cr, tr); tr = fma(ai, ci, tr); ti = fma(ai, cr, ti); ti = fma(-ar, ci, ti)
+__device__ __forceinline__ void add_lconj(float2 &t, float2 l, float2 c)
+{
+    t.x = fma_rn(l.x, c.x, t.x);
+    t.x = fma_rn(l.y, c.y, t.x);
+    t.y = fma_rn(l.y, c.x, t.y);
+    t.y = fma_rn(-l.x, c.y, t.y);
 }
 
 __device__ __forceinline__ float2 div2(float2 v, float s, float y, bool ok)
@@ -207,6 +220,13 @@ __global__ void __launch_bounds__(256) cherk_kernel(float2 *A, int lda, int uppe
             const int i = i0 + u, j = j0 + v;
             c[u][v] = (i < n && j <= i) ? ld(A, lda, upper, i, j) : zero;
         }
+    // the panel's products as one partial sum per element, t = sum_k l_ik conj(l_jk), then one
+    // subtraction per component
+    float2 acc[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = zero;
 #pragma unroll 4
     for (int k = 0; k < CPB; ++k)
     {
@@ -221,8 +241,16 @@ __global__ void __launch_bounds__(256) cherk_kernel(float2 *A, int lda, int uppe
 #pragma unroll
         for (int u = 0; u < 4; ++u)
 #pragma unroll
-            for (int v = 0; v < 4; ++v) sub_lconj(c[u][v], l[u], m[v]);
+            for (int v = 0; v < 4; ++v) add_lconj(acc[u][v], l[u], m[v]);
     }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+        {
+            c[u][v].x = sub_rn(c[u][v].x, acc[u][v].x);
+            c[u][v].y = sub_rn(c[u][v].y, acc[u][v].y);
+        }
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll

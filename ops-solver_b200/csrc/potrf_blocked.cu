@@ -1,12 +1,16 @@
 // potrf_blocked.cu -- real Cholesky factorisation above order 32 (sm_100a).
 //
-// Arithmetic (the oracle's orc_spotrf_fma, this build's order for n > 32, where the
-// reference hands its updates to a CATLASS Gram product): every a_ij, j <= i, takes its
-// updates a_ij = fma(-l_ik, l_jk, a_ij) in ascending k, then the pivot check
-// (d > 0 and d <= FLT_MAX), the IEEE square root of the diagonal and the IEEE division of the
-// column below it.  A failed matrix keeps its completed columns; the columns from the failed
-// one on keep the caller's input.  Both paths below keep every element's operation sequence,
-// so their factors equal the oracle's bit for bit.
+// Arithmetic (this build's orders for n > 32, where the reference hands its updates to a
+// CATLASS Gram product; restated in the oracle): up to order 256 (orc_spotrf_fma) every
+// a_ij, j <= i, takes its updates a_ij = fma(-l_ik, l_jk, a_ij) in ascending k; above 256
+// (orc_spotrf_blocked) the same inside each 64-column panel, while an element right of the
+// panel takes the panel's products as one partial sum t = fma(l_ik, l_jk, t) from zero,
+// then a_ij - t (a chain of n / 64 subtractions instead of n: the rounding of a blocked
+// LAPACK, which the reference's residual gate asks for at orders in the thousands).  Then
+// the pivot check (d > 0 and d <= FLT_MAX), the IEEE square root of the diagonal and the IEEE
+// division of the column below it.  A failed matrix keeps its completed columns; the columns
+// from the failed one on keep the caller's input.  The factors equal the oracle's bit for
+// bit.
 //
 // 33 <= n <= 256, any batch: one block per matrix, the lower triangle packed by columns in
 // shared memory (n = 256: 132 KB, one block per SM; n = 128: 33 KB), factored left-looking in
@@ -26,7 +30,7 @@
 //          only), each tile's two 64 x 64 operand panels loaded by TMA (a 2-D tensor map of
 //          the matrix, completion on an mbarrier with a bounded wait) when the matrix is
 //          16-byte aligned with lda % 4 == 0, by plain loads otherwise; FP32 FMAs in ascending
-//          k into a 4 x 4 register tile per thread.
+//          k into a 4 x 4 tile of partial sums per thread, subtracted once.
 // Every kernel reads the info word first and stops once a pivot has failed; after the last
 // panel a restore pass copies the backup back into the columns from the failed one on.
 #include <cuda.h>
@@ -366,8 +370,9 @@ __device__ __forceinline__ void lower_tile(int idx, int &ti, int &tj)
     tj = idx - r * (r + 1) / 2;
 }
 
-// A22 -= L21 L21^T on the lower tiles; per element the 32 updates in ascending k.  tma: the
-// operand panels come by TMA through `map` (lower storage, aligned); else by plain loads.
+// A22 -= L21 L21^T on the lower tiles: per element the panel's 64 products as one partial sum
+// t = fma(l_ik, l_jk, t) from zero in ascending k, then a_ij - t.  tma: the operand panels
+// come by TMA through `map` (lower storage, aligned); else by plain loads.
 __global__ void __launch_bounds__(256) potrf_syrk_kernel(const __grid_constant__ CUtensorMap map, bool tma, float *A,
                                                          int lda, int upper, int k0, int n, int *info)
 {
@@ -435,6 +440,12 @@ __global__ void __launch_bounds__(256) potrf_syrk_kernel(const __grid_constant__
             }
         }
     }
+    // the panel's 64 products as one partial sum per element, then one subtraction
+    float ps[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) ps[u][v] = 0.0f;
 #pragma unroll 8
     for (int k = 0; k < PB; ++k)
     {
@@ -445,8 +456,12 @@ __global__ void __launch_bounds__(256) potrf_syrk_kernel(const __grid_constant__
 #pragma unroll
         for (int u = 0; u < 4; ++u)
 #pragma unroll
-            for (int v = 0; v < 4; ++v) c[u][v] = fma_rn(-ar[u], bc[v], c[u][v]);
+            for (int v = 0; v < 4; ++v) ps[u][v] = fma_rn(ar[u], bc[v], ps[u][v]);
     }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) c[u][v] = sub_rn(c[u][v], ps[u][v]);
 #pragma unroll
     for (int v = 0; v < 4; ++v)
     {

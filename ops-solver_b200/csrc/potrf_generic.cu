@@ -3,7 +3,8 @@
 //
 // Solve orders (the parity contract, oracle orc_spotrs):
 //   DOT   (33..128): dot accumulators, x_k = (b_k - dot_k) / l_kk   (cholesky_vector.cpp:30-122)
-//   RIGHT (> 128):   right-looking x_i = fma(-l, x_k, x_i) in both sweeps (this build's order)
+//   RIGHT (> 128):   right-looking sweeps in 64-row blocks, fma inside a block and one
+//                    partial sum per block for the rows outside it (this build's order)
 #include "common.cuh"
 #include "launch.h"
 
@@ -20,6 +21,56 @@ __device__ __forceinline__ int64_t tri(int lda, int upper, int i, int j)
 
 constexpr int ORDER_DOT = 1;
 constexpr int ORDER_RIGHT = 2;
+
+// The right-looking sweeps of one right-hand side in blocks of SB rows (orc_spotrs_right):
+// inside a block the unknowns are finished one at a time and taken into the block's other
+// rows by fma; the rows outside the block take the whole block as one partial sum
+// t = fma(l, x_k, t) from zero (ascending k), then x_i - t -- the rounding of a blocked
+// solve, which the reference's residual gate asks for at large orders.  x in shared memory.
+constexpr int SB = 64;
+__device__ __forceinline__ void blocked_sweeps(const float *pa, int lda, int upper, int n, float *x)
+{
+    // forward: L y = b
+    for (int K0 = 0; K0 < n; K0 += SB)
+    {
+        const int kend = min(K0 + SB, n);
+        for (int k = K0; k < kend; ++k)
+        {
+            const float xk = div_rn(x[k], pa[(int64_t)k * (lda + 1)]);
+            for (int i = k + 1 + threadIdx.x; i < kend; i += GT) x[i] = fma_rn(-pa[tri(lda, upper, i, k)], xk, x[i]);
+            __syncthreads();
+            if (threadIdx.x == 0) x[k] = xk;
+            __syncthreads();
+        }
+        for (int i = kend + threadIdx.x; i < n; i += GT)
+        {
+            float t = 0.0f;
+            for (int k = K0; k < kend; ++k) t = fma_rn(pa[tri(lda, upper, i, k)], x[k], t);
+            x[i] = sub_rn(x[i], t);
+        }
+        __syncthreads();
+    }
+    // backward: L^T x = y, blocks in descending order
+    for (int K0 = ((n - 1) / SB) * SB; n > 0 && K0 >= 0; K0 -= SB)
+    {
+        const int kend = min(K0 + SB, n);
+        for (int k = kend - 1; k >= K0; --k)
+        {
+            const float xk = div_rn(x[k], pa[(int64_t)k * (lda + 1)]);
+            for (int i = K0 + threadIdx.x; i < k; i += GT) x[i] = fma_rn(-pa[tri(lda, upper, k, i)], xk, x[i]);
+            __syncthreads();
+            if (threadIdx.x == 0) x[k] = xk;
+            __syncthreads();
+        }
+        for (int i = threadIdx.x; i < K0; i += GT)
+        {
+            float t = 0.0f;
+            for (int k = K0; k < kend; ++k) t = fma_rn(pa[tri(lda, upper, k, i)], x[k], t);
+            x[i] = sub_rn(x[i], t);
+        }
+        __syncthreads();
+    }
+}
 
 // One block per (matrix); right-hand sides one after another; x and the accumulators in
 // shared memory, rows spread over the threads.
@@ -47,6 +98,15 @@ __global__ void __launch_bounds__(GT) potrs_generic_kernel(float *a_single, floa
                 dot[i] = 0.0f;
             }
             __syncthreads();
+            if constexpr (ORDER == ORDER_RIGHT)
+            {
+                blocked_sweeps(pa, lda, upper, n, x);
+                for (int i = threadIdx.x; i < n; i += GT) xb[i] = x[i];
+                __syncthreads();
+                continue;
+            }
+            else
+            {
             // forward: L x = b
             for (int k = 0; k < n; ++k)
             {
@@ -90,6 +150,7 @@ __global__ void __launch_bounds__(GT) potrs_generic_kernel(float *a_single, floa
             }
             for (int i = threadIdx.x; i < n; i += GT) xb[i] = x[i];
             __syncthreads();
+            }
         }
     }
 }

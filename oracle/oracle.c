@@ -17,10 +17,12 @@
  *   orc_sgetri_vector   src/sgetri/real_lu_blocked_inverse_kernel.cpp:676-830,1040-1044
  * Routines for sizes where the reference hands its arithmetic to a third-party Cube GEMM
  * (CATLASS / CANN MatmulImpl) restate this build's own order instead, and say so:
- *   orc_spotrf_fma      right-looking Cholesky with FMA updates in ascending k (n > 32)
- *   orc_spotrs_right    right-looking Cholesky solve (n > 128)
+ *   orc_spotrf_fma      right-looking Cholesky with FMA updates in ascending k (33..256)
+ *   orc_spotrf_blocked  the same in 64-column panels with panel partial sums (n > 256)
+ *   orc_spotrs_right    right-looking Cholesky solve in 64-row blocks (n > 128)
  *   orc_sgetrs          column-oriented LU solve (math of test/utils/lu_verify_utils.py:67-192)
- *   orc_cpotrf/cpotrs   complex64 Cholesky factor and solve, FMA order (see their comment)
+ *   orc_cpotrf/cpotrs   complex64 Cholesky factor and solve, FMA order (see their comment);
+ *                       above order 240 in 64-column panels with panel partial sums
  *
  * Compiled with -ffp-contract=off: every fused multiply-add is an explicit fmaf().
  */
@@ -169,12 +171,64 @@ int orc_spotrf_fma(int n, float *a, int lda, int upper)
     return failure;
 }
 
+/* Above order 256 (this build's order for the whole-GPU factorisation; the reference hands
+ * these orders to a blocked Gram product): right-looking in panels of ORC_NB = 64 columns.
+ * Inside a panel every element takes the panel's updates one by one, fmaf(-l_ik, l_jk, a_ij)
+ * in ascending k, and each column is divided as it is finished; an element right of the
+ * panel takes the panel's products as one partial sum t = fmaf(l_ik, l_jk, t) from zero in
+ * ascending k, then a_ij - t.  The partial sums keep each element's chain of roundings at
+ * n / 64 subtractions plus 64-term sums (the size of a blocked LAPACK's) instead of n, which
+ * the reference's residual gate needs at orders in the thousands. */
+#define ORC_NB 64
+int orc_spotrf_blocked(int n, float *a, int lda, int upper)
+{
+    float *w = (float *)malloc(sizeof(float) * (size_t)n * (size_t)n + 4);
+    for (int j = 0; j < n; ++j)
+        for (int i = j; i < n; ++i) w[(size_t)j * n + i] = a[tri_at(lda, upper, i, j)];
+    int failure = 0;
+    for (int k0 = 0; k0 < n && !failure; k0 += ORC_NB)
+    {
+        const int kend = k0 + ORC_NB < n ? k0 + ORC_NB : n;
+        for (int k = k0; k < kend; ++k)
+        {
+            float d = w[(size_t)k * n + k];
+            if (!(d > 0.0f && d <= FLT_MAX_VALUE))
+            {
+                failure = k + 1;
+                break;
+            }
+            float s = sqrtf(d);
+            w[(size_t)k * n + k] = s;
+            for (int i = k + 1; i < n; ++i) w[(size_t)k * n + i] = w[(size_t)k * n + i] / s;
+            for (int j = k + 1; j < kend; ++j)
+            {
+                float ljk = w[(size_t)k * n + j];
+                for (int i = j; i < n; ++i) w[(size_t)j * n + i] = fmaf(-w[(size_t)k * n + i], ljk, w[(size_t)j * n + i]);
+            }
+        }
+        if (failure) break;
+        for (int j = kend; j < n; ++j)
+            for (int i = j; i < n; ++i)
+            {
+                float t = 0.0f;
+                for (int k = k0; k < kend; ++k) t = fmaf(w[(size_t)k * n + i], w[(size_t)k * n + j], t);
+                w[(size_t)j * n + i] = w[(size_t)j * n + i] - t;
+            }
+    }
+    int done = failure ? failure - 1 : n;
+    for (int j = 0; j < done; ++j)
+        for (int i = j; i < n; ++i) a[tri_at(lda, upper, i, j)] = w[(size_t)j * n + i];
+    free(w);
+    return failure;
+}
+
 /* The size dispatch of SpotrfBatched / Spotrf in this build. */
 int orc_spotrf(int n, float *a, int lda, int upper)
 {
     if (n <= 8) return orc_spotrf_simt(n, a, lda, upper);
     if (n <= 32) return orc_spotrf_group(n, a, lda, upper);
-    return orc_spotrf_fma(n, a, lda, upper);
+    if (n <= 256) return orc_spotrf_fma(n, a, lda, upper);
+    return orc_spotrf_blocked(n, a, lda, upper);
 }
 
 /* SolveKernel (cholesky_simt.cpp:93-117): per right-hand side a forward then a backward
@@ -228,22 +282,47 @@ void orc_spotrs_dot(int n, int nrhs, const float *a, int lda, float *b, int ldb,
 }
 
 /* n > 128 (this build's order; the reference solves panels with a Cube product here):
- * right-looking sweeps, x_k = x_k / l_kk then x_i = fmaf(-l_ik, x_k, x_i) for i > k (k
- * ascending), and the same with l_ki for i < k (k descending). */
+ * right-looking sweeps in blocks of ORC_NB rows.  Forward, per block [K0, K0 + w): the
+ * block's unknowns x_k = x_k / l_kk in ascending k, each taken into the block's later rows
+ * by fmaf(-l_ik, x_k, x_i); then every row below takes the block as one partial sum
+ * t = fmaf(l_ik, x_k, t) from zero in ascending k, x_i = x_i - t.  Backward, blocks in
+ * descending order: x_k = x_k / l_kk in descending k, taken into the block's earlier rows by
+ * fmaf(-l_ki, x_k, x_i); every row above takes t = fmaf(l_ki, x_k, t) over the block in
+ * ascending k, x_i = x_i - t. */
 void orc_spotrs_right(int n, int nrhs, const float *a, int lda, float *b, int ldb, int upper)
 {
     for (int r = 0; r < nrhs; ++r)
     {
         float *x = b + (int64_t)r * ldb;
-        for (int k = 0; k < n; ++k)
+        for (int K0 = 0; K0 < n; K0 += ORC_NB)
         {
-            x[k] = x[k] / a[(int64_t)k * (lda + 1)];
-            for (int i = k + 1; i < n; ++i) x[i] = fmaf(-a[tri_at(lda, upper, i, k)], x[k], x[i]);
+            const int kend = K0 + ORC_NB < n ? K0 + ORC_NB : n;
+            for (int k = K0; k < kend; ++k)
+            {
+                x[k] = x[k] / a[(int64_t)k * (lda + 1)];
+                for (int i = k + 1; i < kend; ++i) x[i] = fmaf(-a[tri_at(lda, upper, i, k)], x[k], x[i]);
+            }
+            for (int i = kend; i < n; ++i)
+            {
+                float t = 0.0f;
+                for (int k = K0; k < kend; ++k) t = fmaf(a[tri_at(lda, upper, i, k)], x[k], t);
+                x[i] = x[i] - t;
+            }
         }
-        for (int k = n - 1; k >= 0; --k)
+        for (int K0 = ((n - 1) / ORC_NB) * ORC_NB; n > 0 && K0 >= 0; K0 -= ORC_NB)
         {
-            x[k] = x[k] / a[(int64_t)k * (lda + 1)];
-            for (int i = 0; i < k; ++i) x[i] = fmaf(-a[tri_at(lda, upper, k, i)], x[k], x[i]);
+            const int kend = K0 + ORC_NB < n ? K0 + ORC_NB : n;
+            for (int k = kend - 1; k >= K0; --k)
+            {
+                x[k] = x[k] / a[(int64_t)k * (lda + 1)];
+                for (int i = K0; i < k; ++i) x[i] = fmaf(-a[tri_at(lda, upper, k, i)], x[k], x[i]);
+            }
+            for (int i = 0; i < K0; ++i)
+            {
+                float t = 0.0f;
+                for (int k = K0; k < kend; ++k) t = fmaf(a[tri_at(lda, upper, k, i)], x[k], t);
+                x[i] = x[i] - t;
+            }
         }
     }
 }
@@ -467,7 +546,7 @@ static inline void ctri_set(float *a, int lda, int upper, int i, int j, float re
 /* Right-looking: d = Re(a_kk) (d > 0 and finite), s = sqrtf(d), l_kk = (s, 0),
  * l_ik = a_ik / s per component; a_ij -= l_ik conj(l_jk) as
  * re = fmaf(-ar, cr, re); re = fmaf(-ai, ci, re); im = fmaf(-ai, cr, im); im = fmaf(ar, ci, im). */
-int orc_cpotrf(int n, float *a, int lda, int upper)
+static int orc_cpotrf_seq(int n, float *a, int lda, int upper)
 {
     float *w = (float *)malloc(sizeof(float) * 2 * (size_t)n * (size_t)n + 8);
     for (int j = 0; j < n; ++j)
@@ -517,7 +596,7 @@ int orc_cpotrf(int n, float *a, int lda, int upper)
 /* Right-looking sweeps: y_k = z_k / l_kk, z_i -= l_ik y_k (i > k); then x_k = z_k / l_kk,
  * z_i -= conj(l_ki) x_k (i < k, k descending); z -= l y as re = fmaf(-lr, yr, re);
  * re = fmaf(li, yi, re); im = fmaf(-lr, yi, im); im = fmaf(-li, yr, im). */
-void orc_cpotrs(int n, int nrhs, const float *a, int lda, float *b, int ldb, int upper)
+static void orc_cpotrs_seq(int n, int nrhs, const float *a, int lda, float *b, int ldb, int upper)
 {
     for (int r = 0; r < nrhs; ++r)
     {
@@ -564,6 +643,187 @@ void orc_cpotrs(int n, int nrhs, const float *a, int lda, float *b, int ldb, int
             x[2 * k + 1] = yi;
         }
     }
+}
+
+/* Above order 240 (the whole-GPU complex factorisation and the solve that goes with it):
+ * the same arithmetic in 64-column panels with panel partial sums, as orc_spotrf_blocked.
+ * Inside a panel: l_ik = a_ik / s, a_ij -= l_ik conj(l_jk) as the four FMAs above in
+ * ascending k.  Right of the panel: t = sum_k l_ik conj(l_jk) from zero in ascending k,
+ *   tr = fmaf(ar, cr, tr); tr = fmaf(ai, ci, tr); ti = fmaf(ai, cr, ti); ti = fmaf(-ar, ci, ti)
+ * then a_ij = (re - tr, im - ti). */
+static int orc_cpotrf_blocked(int n, float *a, int lda, int upper)
+{
+    float *w = (float *)malloc(sizeof(float) * 2 * (size_t)n * (size_t)n + 8);
+#define W(i, j) (w + 2 * ((size_t)(j) * n + (i)))
+    for (int j = 0; j < n; ++j)
+        for (int i = j; i < n; ++i) ctri_get(a, lda, upper, i, j, W(i, j), W(i, j) + 1);
+    int failure = 0;
+    for (int k0 = 0; k0 < n && !failure; k0 += ORC_NB)
+    {
+        const int kend = k0 + ORC_NB < n ? k0 + ORC_NB : n;
+        for (int k = k0; k < kend; ++k)
+        {
+            float d = W(k, k)[0];
+            if (!(d > 0.0f && d <= FLT_MAX_VALUE))
+            {
+                failure = k + 1;
+                break;
+            }
+            float s = sqrtf(d);
+            W(k, k)[0] = s;
+            W(k, k)[1] = 0.0f;
+            for (int i = k + 1; i < n; ++i)
+            {
+                W(i, k)[0] = W(i, k)[0] / s;
+                W(i, k)[1] = W(i, k)[1] / s;
+            }
+            for (int j = k + 1; j < kend; ++j)
+            {
+                const float cr = W(j, k)[0], ci = W(j, k)[1];
+                for (int i = j; i < n; ++i)
+                {
+                    const float ar = W(i, k)[0], ai = W(i, k)[1];
+                    float re = W(i, j)[0], im = W(i, j)[1];
+                    re = fmaf(-ar, cr, re);
+                    re = fmaf(-ai, ci, re);
+                    im = fmaf(-ai, cr, im);
+                    im = fmaf(ar, ci, im);
+                    W(i, j)[0] = re;
+                    W(i, j)[1] = im;
+                }
+            }
+        }
+        if (failure) break;
+        for (int j = kend; j < n; ++j)
+            for (int i = j; i < n; ++i)
+            {
+                float tr = 0.0f, ti = 0.0f;
+                for (int k = k0; k < kend; ++k)
+                {
+                    const float ar = W(i, k)[0], ai = W(i, k)[1], cr = W(j, k)[0], ci = W(j, k)[1];
+                    tr = fmaf(ar, cr, tr);
+                    tr = fmaf(ai, ci, tr);
+                    ti = fmaf(ai, cr, ti);
+                    ti = fmaf(-ar, ci, ti);
+                }
+                W(i, j)[0] = W(i, j)[0] - tr;
+                W(i, j)[1] = W(i, j)[1] - ti;
+            }
+    }
+    int done = failure ? failure - 1 : n;
+    for (int j = 0; j < done; ++j)
+        for (int i = j; i < n; ++i) ctri_set(a, lda, upper, i, j, W(i, j)[0], W(i, j)[1]);
+#undef W
+    free(w);
+    return failure;
+}
+
+/* The blocked solve above order 240, as orc_spotrs_right with complex products: inside a
+ * block z_i -= l_ik y_k (the four FMAs of orc_cpotrs_seq), below it one partial sum
+ *   tr = fmaf(lr, yr, tr); tr = fmaf(-li, yi, tr); ti = fmaf(lr, yi, ti); ti = fmaf(li, yr, ti)
+ * from zero in ascending k, then z_i = (re - tr, im - ti); backward the same with conj(l_ki). */
+static void orc_cpotrs_blocked(int n, int nrhs, const float *a, int lda, float *b, int ldb, int upper)
+{
+    for (int r = 0; r < nrhs; ++r)
+    {
+        float *x = b + 2 * (int64_t)r * ldb;
+        for (int K0 = 0; K0 < n; K0 += ORC_NB)
+        {
+            const int kend = K0 + ORC_NB < n ? K0 + ORC_NB : n;
+            for (int k = K0; k < kend; ++k)
+            {
+                float dr, di;
+                ctri_get(a, lda, upper, k, k, &dr, &di);
+                const float yr = x[2 * k] / dr, yi = x[2 * k + 1] / dr;
+                for (int i = k + 1; i < kend; ++i)
+                {
+                    float lr, li;
+                    ctri_get(a, lda, upper, i, k, &lr, &li);
+                    float re = x[2 * i], im = x[2 * i + 1];
+                    re = fmaf(-lr, yr, re);
+                    re = fmaf(li, yi, re);
+                    im = fmaf(-lr, yi, im);
+                    im = fmaf(-li, yr, im);
+                    x[2 * i] = re;
+                    x[2 * i + 1] = im;
+                }
+                x[2 * k] = yr;
+                x[2 * k + 1] = yi;
+            }
+            for (int i = kend; i < n; ++i)
+            {
+                float tr = 0.0f, ti = 0.0f;
+                for (int k = K0; k < kend; ++k)
+                {
+                    float lr, li;
+                    ctri_get(a, lda, upper, i, k, &lr, &li);
+                    const float yr = x[2 * k], yi = x[2 * k + 1];
+                    tr = fmaf(lr, yr, tr);
+                    tr = fmaf(-li, yi, tr);
+                    ti = fmaf(lr, yi, ti);
+                    ti = fmaf(li, yr, ti);
+                }
+                x[2 * i] = x[2 * i] - tr;
+                x[2 * i + 1] = x[2 * i + 1] - ti;
+            }
+        }
+        for (int K0 = ((n - 1) / ORC_NB) * ORC_NB; n > 0 && K0 >= 0; K0 -= ORC_NB)
+        {
+            const int kend = K0 + ORC_NB < n ? K0 + ORC_NB : n;
+            for (int k = kend - 1; k >= K0; --k)
+            {
+                float dr, di;
+                ctri_get(a, lda, upper, k, k, &dr, &di);
+                const float yr = x[2 * k] / dr, yi = x[2 * k + 1] / dr;
+                for (int i = K0; i < k; ++i)
+                {
+                    float lr, li;
+                    ctri_get(a, lda, upper, k, i, &lr, &li);
+                    li = -li; /* conj(l_ki) */
+                    float re = x[2 * i], im = x[2 * i + 1];
+                    re = fmaf(-lr, yr, re);
+                    re = fmaf(li, yi, re);
+                    im = fmaf(-lr, yi, im);
+                    im = fmaf(-li, yr, im);
+                    x[2 * i] = re;
+                    x[2 * i + 1] = im;
+                }
+                x[2 * k] = yr;
+                x[2 * k + 1] = yi;
+            }
+            for (int i = 0; i < K0; ++i)
+            {
+                float tr = 0.0f, ti = 0.0f;
+                for (int k = K0; k < kend; ++k)
+                {
+                    float lr, li;
+                    ctri_get(a, lda, upper, k, i, &lr, &li);
+                    li = -li; /* conj(l_ki) */
+                    const float yr = x[2 * k], yi = x[2 * k + 1];
+                    tr = fmaf(lr, yr, tr);
+                    tr = fmaf(-li, yi, tr);
+                    ti = fmaf(lr, yi, ti);
+                    ti = fmaf(li, yr, ti);
+                }
+                x[2 * i] = x[2 * i] - tr;
+                x[2 * i + 1] = x[2 * i + 1] - ti;
+            }
+        }
+    }
+}
+
+/* The complex dispatch of this build: the block and register paths up to order 240, the
+ * whole-GPU blocked order above. */
+int orc_cpotrf(int n, float *a, int lda, int upper)
+{
+    return n > 240 ? orc_cpotrf_blocked(n, a, lda, upper) : orc_cpotrf_seq(n, a, lda, upper);
+}
+void orc_cpotrs(int n, int nrhs, const float *a, int lda, float *b, int ldb, int upper)
+{
+    if (n > 240)
+        orc_cpotrs_blocked(n, nrhs, a, lda, b, ldb, upper);
+    else
+        orc_cpotrs_seq(n, nrhs, a, lda, b, ldb, upper);
 }
 
 /* ---------------------------------------------------------------------------------------

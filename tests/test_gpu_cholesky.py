@@ -301,3 +301,34 @@ def test_spotrf_batched_above_packed_orders(handle):
     want, winfo = oracle.spotrf_batched(a)
     assert st == aclsolver.SUCCESS and info.tolist() == winfo.tolist()
     assert same_bits(np.tril(dm.read()), np.tril(want))
+
+
+@pytest.mark.parametrize("n", [1024, 2048, 4096])
+def test_large_spotrf_spotrs_pass_the_reference_residual_gate(handle, n):
+    """The reference's residual judge (test/cholesky/lapack_residual.py: ratio <= 5 x FP32
+    LAPACK's) at the orders where a plain ascending-k chain of n roundings per element fails
+    it: the whole-GPU factor and the blocked solve take each 64-column panel as one partial
+    sum, which keeps them near LAPACK's ratio.  Bit for bit the oracle's order where the
+    oracle finishes in seconds (n <= 2048)."""
+    lib = aclsolver.library()
+    a = spd_batch(1, n, seed=n + 5)
+    da = DeviceMatrices(a, ld=n)
+    info = info_buffer(1)
+    st = lib.aclsolverSpotrf(handle.value, 0, n, da.ptr, n, None, 0, info.data_ptr())
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 0
+    f = da.read()
+    b = np.random.default_rng(n).standard_normal((1, n, 1)).astype(np.float32)
+    db = DeviceMatrices(b, ld=n)
+    st = lib.aclsolverSpotrs(handle.value, 0, n, 1, da.ptr, n, db.ptr, n, info.data_ptr())
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 0
+    x = db.read()
+    if n <= 2048:
+        wf, _ = oracle.spotrf_batched(a)
+        assert same_bits(np.tril(f[0]), np.tril(wf[0]))
+        assert same_bits(x, oracle.spotrs_batched(wf, b, single=True))
+    r, c = judges.paired_cholesky("potrf", a[0], f[0])
+    assert r <= 5 * c, (r, c)
+    rs, cs = judges.paired_cholesky("potrs", a[0], x[0], b32=b[0])
+    assert rs <= 5 * cs, (rs, cs)
