@@ -129,6 +129,49 @@ extern "C"
     aclError aclsolverSgetrs(aclsolverHandle_t handle, const uint64_t trans, const int64_t n, const int64_t nrhs,
                              float *A, const int64_t lda, int32_t *ipiv, float *B, const int64_t ldb, int32_t *info);
 
+    /* ---- complex LU family; reference include/cann_ops_solver.h:882-921 and :1042 ---------- */
+
+    /* Lwork (complex elements) for Cgetrf: 0, the panels factor in shared memory.
+     * m <= 4096, n <= 8192, lda >= max(1, m); an invalid shape or a null Lwork returns
+     * INVALID_VALUE and writes nothing; replaces cann_ops_solver.h:882 (cgetrf_host.cpp:34). */
+    aclsolverStatus_t aclsolverCgetrf_bufferSize(aclsolverHandle_t handle, int m, int n, aclFloatComplex *A, int lda,
+                                                 int *Lwork);
+    /* In-place complex LU with partial pivoting by the L1 magnitude (earliest row on ties);
+     * devIpiv null selects no pivoting; Workspace may be null.  devInfo = 0, the first exactly
+     * zero pivot (1-based), or -i for invalid argument i (1 m, 2 n, 3 A, 4 lda, 5 Workspace,
+     * 6 devIpiv); replaces cann_ops_solver.h:890 (cgetrf_host.cpp:54). */
+    aclsolverStatus_t aclsolverCgetrf(aclsolverHandle_t handle, int m, int n, aclFloatComplex *A, int lda,
+                                      aclFloatComplex *Workspace, int *devIpiv, int *devInfo);
+    /* Lwork = n * n for Cgetri (n <= 4096); A may be null; replaces cann_ops_solver.h:896
+     * (cgetri_host.cpp:78). */
+    aclsolverStatus_t aclsolverCgetri_bufferSize(aclsolverHandle_t handle, int n, aclFloatComplex *A, int lda,
+                                                 int *Lwork);
+    /* In-place inverse from Cgetrf's LU and pivots (null = no pivoting).  devInfo = -4 for a
+     * pivot outside [row+1, n] (the call then returns INVALID_VALUE), else the first zero
+     * diagonal with A unchanged, else 0.  Workspace (n*n) must not overlap A, devIpiv or
+     * devInfo; replaces cann_ops_solver.h:903 (cgetri_host.cpp:95). */
+    aclsolverStatus_t aclsolverCgetri(aclsolverHandle_t handle, int n, aclFloatComplex *A, int lda, int *devIpiv,
+                                      aclFloatComplex *Workspace, int Lwork, int *devInfo);
+    /* Out-of-place inverses from LU factors: Aarray / Carray device tables, PivotArray n per
+     * matrix or null; per-matrix infoArray as for Cgetri, failed outputs left unwritten;
+     * batchSize <= 1,000,000; replaces cann_ops_solver.h:911 (cgetri_batched_host.cpp:33). */
+    aclsolverStatus_t aclsolverCgetriBatched(aclsolverHandle_t handle, int n, const aclFloatComplex *const Aarray[],
+                                             int lda, const int *PivotArray, aclFloatComplex *const Carray[], int ldc,
+                                             int *infoArray, int batchSize);
+    /* Direct out-of-place inverses (Gauss-Jordan, partial pivoting) of n <= 32 matrices;
+     * info per matrix = the first zero pivot (output unwritten) or 0; batchSize <=
+     * 10,000,000; replaces cann_ops_solver.h:919 (cmatinv_batched_host.cpp:33). */
+    aclsolverStatus_t aclsolverCmatinvBatched(aclsolverHandle_t handle, int n, const aclFloatComplex *const A[],
+                                              int lda, aclFloatComplex *const Ainv[], int lda_inv, int *info,
+                                              int batchSize);
+    /* Host-buffer complex LU solve, ROW-major like aclsolverSgetrs: trans 0 A X = B, 1 A^T X = B,
+     * 2 A^H X = B; n, nrhs in [1, 8192]; an ipiv entry outside [1, n] sets *info = -4.
+     * Synchronous; returns ACL_SUCCESS or ACL_ERROR_INVALID_PARAM; replaces
+     * cann_ops_solver.h:1042 (src/cgetrs/cgetrs_host.cpp:172). */
+    aclError aclsolverCgetrs(aclsolverHandle_t handle, const uint64_t trans, const int64_t n, const int64_t nrhs,
+                             aclFloatComplex *A, const int64_t lda, int32_t *ipiv, aclFloatComplex *B,
+                             const int64_t ldb, int32_t *info);
+
 #ifdef __cplusplus
 }
 #endif

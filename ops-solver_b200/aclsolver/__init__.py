@@ -70,6 +70,13 @@ ARGTYPES = {
     "aclsolverSgetriBatched": [VP, I32, VP, I32, VP, VP, I32, VP, I32],
     "aclsolverSmatinvBatched": [VP, I32, VP, I32, VP, I32, VP, I32],
     "aclsolverSgetrs": [VP, U64, I64, I64, VP, I64, VP, VP, I64, VP],
+    "aclsolverCgetrf_bufferSize": [VP, I32, I32, VP, I32, C.POINTER(I32)],
+    "aclsolverCgetrf": [VP, I32, I32, VP, I32, VP, VP, VP],
+    "aclsolverCgetri_bufferSize": [VP, I32, VP, I32, C.POINTER(I32)],
+    "aclsolverCgetri": [VP, I32, VP, I32, VP, VP, I32, VP],
+    "aclsolverCgetriBatched": [VP, I32, VP, I32, VP, VP, I32, VP, I32],
+    "aclsolverCmatinvBatched": [VP, I32, VP, I32, VP, I32, VP, I32],
+    "aclsolverCgetrs": [VP, U64, I64, I64, VP, I64, VP, VP, I64, VP],
     # additions of this build
     "aclsolverSetDeviceChecks": [VP, I32],
     "aclsolverGetDeviceChecks": [VP, C.POINTER(I32)],

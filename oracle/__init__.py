@@ -39,6 +39,11 @@ def lib():
         _lib.orc_sgetri_batched.argtypes = [_i, _F, _i, _l, _VP, _F, _i, _l, _i, _I, _i]
         _lib.orc_cpotrf_batched.argtypes = [_i, _F, _i, _l, _i, _i, _I, _i]
         _lib.orc_cpotrs_batched.argtypes = [_i, _i, _F, _i, _l, _F, _i, _l, _i, _i, _i]
+        _lib.orc_cgetrf_batched.argtypes = [_i, _i, _F, _i, _l, _i, _i, _I, _I, _i]
+        _lib.orc_cgetri_batched.argtypes = [_i, _F, _i, _l, _VP, _F, _i, _l, _i, _I, _i]
+        _lib.orc_cmatinv_batched.argtypes = [_i, _F, _i, _l, _F, _i, _l, _i, _I, _i]
+        _lib.orc_cgetrs_batched.argtypes = [_i, _i, _i, _F, _i, _l, _VP, _F, _i, _l, _i, _i]
+        _lib.orc_cdivide_many.argtypes = [_F, _F, _F, _l]
         _lib.orc_max_threads.restype = _i
     return _lib
 
@@ -143,3 +148,57 @@ def cpotrs_batched(factors, b, upper=False, threads=0):
     count, n, nrhs = fshape[0], fshape[1], bshape[1]
     lib().orc_cpotrs_batched(n, nrhs, fa, n, n * n, fb, n, n * nrhs, count, int(upper), threads)
     return _uncslab(fb, bshape)
+
+
+def cgetrf_batched(a, pivoting=True, threads=0):
+    """Complex LU of each (m, n) matrix; returns (lu, ipiv (count, min(m, n)) 1-based, info)."""
+    flat, shape = _cslab(a)
+    count, n, m = shape
+    steps = min(m, n)
+    ipiv = np.zeros((count, max(steps, 1)), dtype=np.int32)
+    info = np.zeros(count, dtype=np.int32)
+    lib().orc_cgetrf_batched(m, n, flat, m, m * n, count, int(pivoting), ipiv, info, threads)
+    return _uncslab(flat, shape), ipiv[:, :steps], info
+
+
+def cgetri_batched(lu, ipiv, threads=0):
+    """Inverse from complex LU factors (compensated column solves); returns (inverse, info).
+    A matrix whose info is nonzero keeps a zero output here (the library leaves it unwritten)."""
+    flat, shape = _cslab(lu)
+    count, n = shape[0], shape[1]
+    piv = None if ipiv is None else np.ascontiguousarray(ipiv, dtype=np.int32)
+    out = np.zeros_like(flat)
+    info = np.zeros(count, dtype=np.int32)
+    lib().orc_cgetri_batched(n, flat, n, n * n, None if piv is None else piv.ctypes.data, out, n, n * n, count,
+                             info, threads)
+    return _uncslab(out, shape), info
+
+
+def cmatinv_batched(a, threads=0):
+    """Gauss-Jordan inverse of each (n, n) matrix; returns (inverse, info)."""
+    flat, shape = _cslab(a)
+    count, n = shape[0], shape[1]
+    out = np.zeros_like(flat)
+    info = np.zeros(count, dtype=np.int32)
+    lib().orc_cmatinv_batched(n, flat, n, n * n, out, n, n * n, count, info, threads)
+    return _uncslab(out, shape), info
+
+
+def cgetrs_batched(lu, ipiv, b, trans=0, threads=0):
+    """Solve op(A) x = b from complex LU factors; b (count, n, nrhs)."""
+    fa, fshape = _cslab(lu)
+    fb, bshape = _cslab(b)
+    count, n, nrhs = fshape[0], fshape[1], bshape[1]
+    piv = None if ipiv is None else np.ascontiguousarray(ipiv, dtype=np.int32)
+    lib().orc_cgetrs_batched(int(trans), n, nrhs, fa, n, n * n, None if piv is None else piv.ctypes.data, fb, n,
+                             n * nrhs, count, threads)
+    return _uncslab(fb, bshape)
+
+
+def cdivide(a, b):
+    """Elementwise complex64 a / b in the reference's compensated division."""
+    a = np.ascontiguousarray(a, dtype=np.complex64).reshape(-1)
+    b = np.ascontiguousarray(b, dtype=np.complex64).reshape(-1)
+    out = np.zeros_like(a)
+    lib().orc_cdivide_many(a.view(np.float32), b.view(np.float32), out.view(np.float32), a.size)
+    return out

@@ -10,6 +10,11 @@
       |err| <= 1e-3 or |err| / |x| <= 1e-3 on at least 99.99 % of entries.
   solve_lu                           test/utils/lu_verify_utils.py:67-192 (numpy LU solve)
   backward_error / forward_error     normwise errors against an FP64 LAPACK solve.
+  cgetrf_gate                        test/cgetrf/data/verify_result.py:60-110
+      |(P A)_ij - (L U)_ij| / |(P A)_ij| <= 1e-3 on all but 1e-4 of the entries, all finite.
+  complex_solve_compare_ok           test/utils/lu_verify_utils.py:262-290 on complex values.
+  inverse_golden_ok                  test/cgetri_batched/data/verify_result.py:28-79
+      isclose(out, numpy inverse, rtol = atol = 5e-3) on all but 1e-4 of the entries.
 """
 
 import numpy as np
@@ -196,3 +201,39 @@ def inverse_judge(a, x):
     miss = ~np.isclose(out, golden, rtol=5e-3, atol=5e-3, equal_nan=True)
     ratio = float(miss.sum()) / golden.size
     return ratio <= 1e-4, ratio
+
+
+def cgetrf_gate(a, lu, ipiv):
+    """The reference's complex LU acceptance: rows of A swapped by the pivots, compared
+    elementwise with L U in complex64 arithmetic as numpy evaluates it there."""
+    a = np.array(a, dtype=np.complex64)
+    lu = np.asarray(lu, dtype=np.complex64)
+    m, n = a.shape
+    for i, p in enumerate(np.asarray(ipiv) - 1):
+        if p != i:
+            a[[i, p], :] = a[[p, i], :]
+    k = min(m, n)
+    lower = np.tril(lu[:, :k], -1)
+    lower[np.arange(k), np.arange(k)] = 1
+    prod = lower @ np.triu(lu[:k, :])
+    if not np.isfinite(prod).all():
+        return False
+    ratio = np.abs(a - prod) / np.abs(a)
+    bad = (ratio > 1e-3) | ~np.isfinite(ratio)
+    return bool(bad.sum() / a.size <= 1e-4)
+
+
+def complex_solve_compare_ok(actual, expected):
+    actual = np.asarray(actual, dtype=np.complex128)
+    expected = np.asarray(expected, dtype=np.complex128)
+    err = np.abs(actual - expected)
+    den = np.where(np.abs(expected) > 1e-12, np.abs(expected), 1.0)
+    bad = (err > 1e-3) & (err / den > 1e-3)
+    return bool(np.isfinite(actual).all() and bad.sum() / bad.size <= 1e-4)
+
+
+def inverse_golden_ok(out, golden):
+    out = np.asarray(out).reshape(-1)
+    golden = np.asarray(golden).reshape(-1)
+    miss = ~np.isclose(out, golden, rtol=5e-3, atol=5e-3, equal_nan=True)
+    return bool(miss.sum() / golden.size <= 1e-4)

@@ -911,3 +911,442 @@ void orc_cpotrs_batched(int n, int nrhs, const float *a, int lda, int64_t astrid
     for (int q = 0; q < count; ++q)
         orc_cpotrs(n, nrhs, a + 2 * (int64_t)q * astride, lda, b + 2 * (int64_t)q * bstride, ldb, upper);
 }
+
+/* ---------------------------------------------------------------------------------------
+ * Complex LU family (complex64 stored as interleaved float pairs, column-major)
+ *
+ * Restated from the reference's SIMT helpers (paths relative to the reference root):
+ *   c_score            src/utils/complex_solver_kernel.hpp:48-67   (PivotScore)
+ *   c_submul           :69-72                                     (SubMul)
+ *   c_quotient         :74-86                                     (Quotient)
+ *   c_scaled_quotient  :88-106                                    (ScaledQuotient)
+ *   c_needs_scaled     :108-117                                   (NeedsScaledNumerator)
+ *   c_divide           :119-143                                   (Divide)
+ *   orc_cgetrf         :161-250 (FindPivot, SwapRows, DivideColumn, UpdatePanel,
+ *                      FactorColumn): every element receives its SubMul updates one
+ *                      pivot at a time in ascending order, so the reference's panel,
+ *                      cached-panel and vector trailing-update schedules all give these bits
+ *   orc_cgetri         src/utils/complex_solver_resident.hpp:21-170 (CompensatedSubtract,
+ *                      CompensatedSubMul, WarpResidentStep / WarpResidentSolve) with
+ *                      ParallelCheckLu (complex_solver_kernel.hpp:262-292)
+ *   orc_cmatinv        src/utils/complex_solver_register.hpp:271-326 (InvertSmallInPlace,
+ *                      SolveDirectInPlace: Gauss-Jordan in place, then the column permutation)
+ *   orc_cgetrs         this build's own order (the reference hands its solve to Cube
+ *                      matrix multiplies, src/cgetrs/kernel/trsm_custom.hpp): pivots, then
+ *                      per-element SubMul chains in pivot order, Divide by the diagonal
+ * ------------------------------------------------------------------------------------- */
+
+typedef struct
+{
+    float re, im;
+} cfl;
+
+static inline uint32_t c_bits(float x)
+{
+    uint32_t u;
+    memcpy(&u, &x, sizeof u);
+    return u;
+}
+
+static inline float c_float(uint32_t u)
+{
+    float x;
+    memcpy(&x, &u, sizeof x);
+    return x;
+}
+
+/* Abs keeps the sign of a negative zero (x < 0 is false for -0). */
+static inline float c_abs(float x) { return x < 0.0f ? -x : x; }
+
+static inline int c_zero(cfl v) { return v.re == 0.0f && v.im == 0.0f; }
+
+/* L1 magnitude as an ordered key: NaN 0, zero 1, an overflowing sum re-scaled by 1/2 with
+ * its exponent extended by one. */
+static inline uint32_t c_score(cfl v)
+{
+    float re = c_abs(v.re), im = c_abs(v.im);
+    float s = re + im;
+    if (!(s >= 0.0f)) return 0u;
+    if (s == 0.0f) return 1u;
+    if (s > FLT_MAX_VALUE) return c_bits(re * 0.5f + im * 0.5f) + 0x00800001u;
+    return c_bits(s) + 1u;
+}
+
+/* x - a*b with the reference's two-FMA order per component. */
+static inline cfl c_submul(cfl x, cfl a, cfl b)
+{
+    cfl r;
+    r.re = fmaf(a.im, b.im, fmaf(-a.re, b.re, x.re));
+    r.im = fmaf(-a.im, b.re, fmaf(-a.re, b.im, x.im));
+    return r;
+}
+
+static inline float c_quotient(float ar, float br, float ai, float bi, float den, float den_err)
+{
+    float product = ar * br;
+    float other = ai * bi;
+    float numerator = product + other;
+    float part = numerator - product;
+    float error = (product - (numerator - part)) + (other - part) + fmaf(ar, br, -product) + fmaf(ai, bi, -other);
+    float reciprocal = 1.0f / den;
+    float result = numerator * reciprocal;
+    float remainder = fmaf(-result, den, numerator) + error - result * den_err;
+    return fmaf(remainder, reciprocal, result);
+}
+
+static inline float c_scaled_quotient(float a, float b, float c, float d, float scale, float den, float den_err)
+{
+    int ae, be, ce, de, se;
+    float am = frexpf(a, &ae), bm = frexpf(b, &be);
+    float cm = frexpf(c, &ce), dm = frexpf(d, &de);
+    float sm = frexpf(scale, &se);
+    int ab = ae + be, cd = ce + de;
+    int zab = a == 0.0f || b == 0.0f, zcd = c == 0.0f || d == 0.0f;
+    int e = zab ? cd : zcd ? ab : (ab > cd ? ab : cd);
+    am = zab ? 0.0f : ldexpf(am, ab - e);
+    cm = zcd ? 0.0f : ldexpf(cm, cd - e);
+    float q = c_quotient(am, bm, cm, dm, den, den_err);
+    return ldexpf(q / (sm * sm), e - 2 * se);
+}
+
+static inline int c_needs_scaled(cfl a, cfl b, float scale, float ar, float ai)
+{
+    return c_abs(a.re) <= FLT_MAX_VALUE && c_abs(a.im) <= FLT_MAX_VALUE && scale > 0.0f && scale <= FLT_MAX_VALUE &&
+           (c_abs(ar) > 0x1p120f || c_abs(ai) > 0x1p120f || (a.re != 0.0f && c_abs(ar) < 0x1p-100f) ||
+            (a.im != 0.0f && c_abs(ai) < 0x1p-100f) || (b.re != 0.0f && c_abs(b.re / scale) < 0x1p-100f) ||
+            (b.im != 0.0f && c_abs(b.im / scale) < 0x1p-100f));
+}
+
+/* a / b: both scaled by the exponent of max(|b.re|, |b.im|), the compensated quotient, and
+ * exponent-aligned products when the scaled operands would lose bits. */
+static cfl c_divide(cfl a, cfl b)
+{
+    float s = c_abs(b.re) > c_abs(b.im) ? c_abs(b.re) : c_abs(b.im);
+    uint32_t ex = c_bits(s) & 0x7f800000u;
+    if (ex != 0) s = c_float(ex);
+    float br = b.re / s, bi = b.im / s, ar = a.re / s, ai = a.im / s;
+    float first = c_abs(br) > c_abs(bi) ? br : bi;
+    float second = c_abs(br) > c_abs(bi) ? bi : br;
+    float square = first * first;
+    float den = fmaf(second, second, square);
+    float err = fmaf(first, first, -square) + fmaf(second, second, square - den);
+    cfl r;
+    if (c_needs_scaled(a, b, s, ar, ai))
+    {
+        r.re = c_scaled_quotient(a.re, b.re, a.im, b.im, s, den, err);
+        r.im = c_scaled_quotient(a.im, b.re, -a.re, b.im, s, den, err);
+        return r;
+    }
+    r.re = c_quotient(ar, br, ai, bi, den, err);
+    r.im = c_quotient(ai, br, -ar, bi, den, err);
+    return r;
+}
+
+#define CAT(a, lda, r, c) ((a)[(int64_t)(c) * (lda) + (r)])
+
+/* In-place LU of the m x n matrix; ipiv NULL selects no pivoting.  Returns info: the first
+ * column whose pivot is exactly zero, 1-based, or 0. */
+int orc_cgetrf(int m, int n, float *af, int lda, int *ipiv)
+{
+    cfl *a = (cfl *)af;
+    int info = 0, lim = m < n ? m : n;
+    for (int k = 0; k < lim; ++k)
+    {
+        int p = k;
+        if (ipiv)
+        {
+            uint32_t best = 0;
+            p = m;
+            for (int r = k; r < m; ++r)
+            {
+                uint32_t s = c_score(CAT(a, lda, r, k));
+                if (s > best || (s == best && r < p))
+                {
+                    best = s;
+                    p = r;
+                }
+            }
+            ipiv[k] = p + 1;
+        }
+        if (info == 0 && c_zero(CAT(a, lda, p, k))) info = k + 1;
+        if (p != k)
+            for (int j = 0; j < n; ++j)
+            {
+                cfl t = CAT(a, lda, k, j);
+                CAT(a, lda, k, j) = CAT(a, lda, p, j);
+                CAT(a, lda, p, j) = t;
+            }
+        cfl d = CAT(a, lda, k, k);
+        if (!c_zero(d))
+            for (int r = k + 1; r < m; ++r) CAT(a, lda, r, k) = c_divide(CAT(a, lda, r, k), d);
+        for (int j = k + 1; j < n; ++j)
+        {
+            cfl u = CAT(a, lda, k, j);
+            for (int r = k + 1; r < m; ++r) CAT(a, lda, r, j) = c_submul(CAT(a, lda, r, j), CAT(a, lda, r, k), u);
+        }
+    }
+    return info;
+}
+
+/* Status of an LU ahead of its inverse: -4 for a pivot outside [row+1, n], else the first
+ * exactly-zero diagonal (1-based), else 0. */
+int orc_ccheck_lu(int n, const float *lu, int lda, const int *ipiv)
+{
+    const cfl *a = (const cfl *)lu;
+    if (ipiv)
+        for (int r = 0; r < n; ++r)
+            if (ipiv[r] < r + 1 || ipiv[r] > n) return -4;
+    for (int r = 0; r < n; ++r)
+        if (c_zero(CAT(a, lda, r, r))) return r + 1;
+    return 0;
+}
+
+/* value - left*right, its rounding error carried into *corr. */
+static inline float c_comp_sub(float value, float *corr, float left, float right)
+{
+    float product = left * right;
+    float product_err = fmaf(left, right, -product);
+    float result = value - product;
+    float virt = result - value;
+    float sum_err = (value - (result - virt)) - (product + virt);
+    *corr += sum_err - product_err;
+    return result;
+}
+
+static inline void c_comp_submul(cfl *v, cfl *corr, cfl f, cfl s)
+{
+    v->re = c_comp_sub(v->re, &corr->re, f.re, s.re);
+    v->re = c_comp_sub(v->re, &corr->re, -f.im, s.im);
+    v->im = c_comp_sub(v->im, &corr->im, f.im, s.re);
+    v->im = c_comp_sub(v->im, &corr->im, f.re, s.im);
+}
+
+/* Inverse from an LU: column j solves L U x = P e_j with compensated updates.  C is written
+ * only when the LU check passes.  Returns the check status. */
+int orc_cgetri(int n, const float *lu, int lda, const int *ipiv, float *cf_, int ldc)
+{
+    const cfl *a = (const cfl *)lu;
+    cfl *c = (cfl *)cf_;
+    int status = orc_ccheck_lu(n, lu, lda, ipiv);
+    if (status != 0) return status;
+    int *perm = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    cfl *x = (cfl *)malloc(sizeof(cfl) * 2 * (size_t)(n > 0 ? n : 1));
+    cfl *e = x + n;
+    for (int r = 0; r < n; ++r) perm[r] = r;
+    if (ipiv)
+        for (int r = 0; r < n; ++r)
+        {
+            int t = ipiv[r] - 1, v = perm[r];
+            perm[r] = perm[t];
+            perm[t] = v;
+        }
+    for (int j = 0; j < n; ++j)
+    {
+        for (int r = 0; r < n; ++r)
+        {
+            x[r].re = perm[r] == j ? 1.0f : 0.0f;
+            x[r].im = 0.0f;
+            e[r].re = e[r].im = 0.0f;
+        }
+        for (int p = 0; p < n; ++p)
+        {
+            cfl v = {x[p].re + e[p].re, x[p].im + e[p].im};
+            for (int r = p + 1; r < n; ++r) c_comp_submul(&x[r], &e[r], CAT(a, lda, r, p), v);
+        }
+        for (int p = n - 1; p >= 0; --p)
+        {
+            cfl v = {x[p].re + e[p].re, x[p].im + e[p].im};
+            v = c_divide(v, CAT(a, lda, p, p));
+            x[p] = v;
+            e[p].re = e[p].im = 0.0f;
+            for (int r = 0; r < p; ++r) c_comp_submul(&x[r], &e[r], CAT(a, lda, r, p), v);
+        }
+        for (int r = 0; r < n; ++r) CAT(c, ldc, r, j) = x[r];
+    }
+    free(x);
+    free(perm);
+    return 0;
+}
+
+/* Gauss-Jordan inverse in place with partial pivoting (n <= 32 in the API).  An exactly
+ * zero pivot stops the sweep and returns its column, 1-based, with C unwritten. */
+int orc_cmatinv(int n, const float *af, int lda, float *cf_, int ldc)
+{
+    const cfl *a = (const cfl *)af;
+    cfl *c = (cfl *)cf_;
+    size_t nn = (size_t)(n > 0 ? n : 1);
+    cfl *w = (cfl *)malloc(sizeof(cfl) * nn * nn);
+    cfl *upper = (cfl *)malloc(sizeof(cfl) * nn);
+    int *piv = (int *)malloc(sizeof(int) * nn);
+    int status = 0;
+    for (int j = 0; j < n; ++j)
+        for (int r = 0; r < n; ++r) CAT(w, n, r, j) = CAT(a, lda, r, j);
+    for (int col = 0; col < n && status == 0; ++col)
+    {
+        uint32_t best = 0;
+        int p = col;
+        for (int r = col; r < n; ++r)
+        {
+            uint32_t s = c_score(CAT(w, n, r, col));
+            if (s > best)
+            {
+                best = s;
+                p = r;
+            }
+        }
+        piv[col] = p;
+        for (int j = 0; j < n; ++j)
+        {
+            cfl t = CAT(w, n, col, j);
+            CAT(w, n, col, j) = CAT(w, n, p, j);
+            CAT(w, n, p, j) = t;
+        }
+        cfl d = CAT(w, n, col, col);
+        if (c_zero(d))
+        {
+            status = col + 1;
+            break;
+        }
+        cfl one = {1.0f, 0.0f};
+        cfl inv = c_divide(one, d);
+        for (int j = 0; j < n; ++j) upper[j] = j == col ? inv : c_divide(CAT(w, n, col, j), d);
+        for (int j = 0; j < n; ++j) CAT(w, n, col, j) = upper[j];
+        for (int r = 0; r < n; ++r)
+        {
+            if (r == col) continue;
+            cfl f = CAT(w, n, r, col);
+            for (int j = 0; j < n; ++j)
+            {
+                if (j == col)
+                {
+                    cfl v;
+                    v.re = fmaf(f.im, inv.im, -f.re * inv.re);
+                    v.im = fmaf(-f.re, inv.im, -f.im * inv.re);
+                    CAT(w, n, r, j) = v;
+                }
+                else
+                    CAT(w, n, r, j) = c_submul(CAT(w, n, r, j), f, upper[j]);
+            }
+        }
+    }
+    if (status == 0)
+        for (int col = 0; col < n; ++col)
+        {
+            int t = col;
+            for (int r = n - 1; r >= 0; --r)
+            {
+                int q = piv[r];
+                t = t == r ? q : t == q ? r : t;
+            }
+            for (int r = 0; r < n; ++r) CAT(c, ldc, r, t) = CAT(w, n, r, col);
+        }
+    free(piv);
+    free(upper);
+    free(w);
+    return status;
+}
+
+/* Solve with an LU: trans 0 A X = B, 1 A^T X = B, 2 A^H X = B.  The working triangle is
+ * M = A (trans 0) or op(A) (trans 1, 2); every element of B receives its SubMul updates in
+ * pivot order and is divided by the diagonal of the non-unit factor after them. */
+void orc_cgetrs(int trans, int n, int nrhs, const float *lu, int lda, const int *ipiv, float *bf, int ldb)
+{
+    const cfl *a = (const cfl *)lu;
+    cfl *b = (cfl *)bf;
+    const float cj = trans == 2 ? -1.0f : 1.0f;
+#define CM(r, c)                                                                                     \
+    (trans == 0 ? CAT(a, lda, r, c)                                                                  \
+                : (cfl){CAT(a, lda, c, r).re, cj * CAT(a, lda, c, r).im})
+    for (int j = 0; j < nrhs; ++j)
+    {
+        cfl *x = b + (int64_t)j * ldb;
+        if (trans == 0)
+        {
+            if (ipiv)
+                for (int k = 0; k < n; ++k)
+                {
+                    int t = ipiv[k] - 1;
+                    cfl v = x[k];
+                    x[k] = x[t];
+                    x[t] = v;
+                }
+            for (int k = 0; k < n; ++k)
+                for (int i = k + 1; i < n; ++i) x[i] = c_submul(x[i], CM(i, k), x[k]);
+            for (int k = n - 1; k >= 0; --k)
+            {
+                x[k] = c_divide(x[k], CM(k, k));
+                for (int i = 0; i < k; ++i) x[i] = c_submul(x[i], CM(i, k), x[k]);
+            }
+        }
+        else
+        {
+            for (int k = 0; k < n; ++k)
+            {
+                x[k] = c_divide(x[k], CM(k, k));
+                for (int i = k + 1; i < n; ++i) x[i] = c_submul(x[i], CM(i, k), x[k]);
+            }
+            for (int k = n - 1; k >= 0; --k)
+                for (int i = 0; i < k; ++i) x[i] = c_submul(x[i], CM(i, k), x[k]);
+            if (ipiv)
+                for (int k = n - 1; k >= 0; --k)
+                {
+                    int t = ipiv[k] - 1;
+                    cfl v = x[k];
+                    x[k] = x[t];
+                    x[t] = v;
+                }
+        }
+    }
+#undef CM
+}
+
+/* Complex divide and pivot score exposed for the element-level parity tests. */
+void orc_cdivide_many(const float *a, const float *b, float *out, int64_t count)
+{
+    for (int64_t i = 0; i < count; ++i)
+    {
+        cfl x = {a[2 * i], a[2 * i + 1]}, y = {b[2 * i], b[2 * i + 1]};
+        cfl r = c_divide(x, y);
+        out[2 * i] = r.re;
+        out[2 * i + 1] = r.im;
+    }
+}
+
+void orc_cgetrf_batched(int m, int n, float *a, int lda, int64_t stride, int count, int pivoting, int *ipiv,
+                        int *info, int threads)
+{
+    int lim = m < n ? m : n;
+    set_threads(threads);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int q = 0; q < count; ++q)
+        info[q] = orc_cgetrf(m, n, a + 2 * (int64_t)q * stride, lda, pivoting ? ipiv + (int64_t)q * lim : NULL);
+}
+
+void orc_cgetri_batched(int n, const float *lu, int lda, int64_t astride, const int *ipiv, float *c, int ldc,
+                        int64_t cstride, int count, int *info, int threads)
+{
+    set_threads(threads);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int q = 0; q < count; ++q)
+        info[q] = orc_cgetri(n, lu + 2 * (int64_t)q * astride, lda, ipiv ? ipiv + (int64_t)q * n : NULL,
+                             c + 2 * (int64_t)q * cstride, ldc);
+}
+
+void orc_cmatinv_batched(int n, const float *a, int lda, int64_t astride, float *c, int ldc, int64_t cstride,
+                         int count, int *info, int threads)
+{
+    set_threads(threads);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int q = 0; q < count; ++q)
+        info[q] = orc_cmatinv(n, a + 2 * (int64_t)q * astride, lda, c + 2 * (int64_t)q * cstride, ldc);
+}
+
+void orc_cgetrs_batched(int trans, int n, int nrhs, const float *lu, int lda, int64_t astride, const int *ipiv,
+                        float *b, int ldb, int64_t bstride, int count, int threads)
+{
+    set_threads(threads);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int q = 0; q < count; ++q)
+        orc_cgetrs(trans, n, nrhs, lu + 2 * (int64_t)q * astride, lda, ipiv ? ipiv + (int64_t)q * n : NULL,
+                   b + 2 * (int64_t)q * bstride, ldb);
+}

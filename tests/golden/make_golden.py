@@ -16,6 +16,8 @@ Outputs (committed; the tests read only these files, never the reference tree):
   solve_lu.npz         seeded LU factors (LAPACK sgetrf), right-hand sides and the solution
                        the reference's own numpy solver computes
                        (test/utils/lu_verify_utils.py:172-192, solve_lu), for trans 0 and 1
+  complex_lu.npz       the reference's complex LU data recipes with LAPACK's pivots, the
+                       solutions of its numpy LU solver (trans 0, 1, 2) and numpy inverses
   cholesky_cpu_ratios.npz  seeded SPD matrices (the reference runner's recipe,
                        test/cholesky/runner.py:265-272) with the FP32-LAPACK residual
                        ratios of the reference judge (test/cholesky/lapack_residual.py:64-86)
@@ -82,6 +84,15 @@ def known_answers(ref):
         "layout": "row-major (re, im) pairs",
         "source": "docs/zh/cpotrf_batched.md",
     }
+    b = example_blocks(docs / "cgetrs.md")
+    out["cgetrs_4x4"] = {
+        "lu": b[0],
+        "ipiv": [int(v) for v in b[1]],
+        "b": b[2],
+        "x": b[3],
+        "layout": "row-major (re, im) pairs",
+        "source": "docs/zh/cgetrs.md",
+    }
     return out
 
 
@@ -131,6 +142,53 @@ def solve_lu_vectors(ref):
     return out
 
 
+def complex_lu_vectors(ref):
+    """The reference's complex LU data recipes (test/cgetrf/data/gen_data.py: integer parts
+    1..10; test/cgetrs/data/gen_data.py: a dominant shuffled diagonal, seed 149;
+    test/cgetri_batched/data/gen_data.py: N(0,1) parts with a raised diagonal, seed 42) with
+    LAPACK's complex64 pivots and the solutions of the reference's own numpy LU solver
+    (test/utils/lu_verify_utils.py:174-191, solve_lu, trans 0 / 1 / 2)."""
+    sys.path.insert(0, str(Path(ref) / "test" / "utils"))
+    from lu_verify_utils import solve_lu  # the reference's own numpy solver
+
+    out = {}
+    for m, n in [(32, 32), (48, 64), (64, 48), (128, 128)]:
+        rng = np.random.RandomState(149)
+        a = rng.randint(1, 11, size=(m, n * 2)).astype(np.float32).view(np.complex64)
+        lu, piv, info = lapack.cgetrf(a)
+        assert info == 0
+        out[f"getrf_m{m}_n{n}_a"] = a
+        out[f"getrf_m{m}_n{n}_lapack_ipiv"] = (piv + 1).astype(np.int32)
+    for n, nrhs in [(4, 1), (32, 32), (65, 3)]:
+        rng = np.random.RandomState(149)
+        a = (rng.randint(1, 11, size=(n, n)) + 1j * rng.randint(1, 11, size=(n, n))).astype(np.complex64)
+        for i in range(n):
+            row = np.sum(np.abs(a[i, :])) - np.abs(a[i, i])
+            a[i, i] = row + rng.rand() * 10 + 1j * rng.rand() * 10
+        rng.shuffle(a)
+        b = (rng.randn(n, nrhs) + 1j * rng.randn(n, nrhs)).astype(np.complex64)
+        lu, piv, info = lapack.cgetrf(a)
+        assert info == 0
+        key = f"getrs_n{n}_r{nrhs}"
+        out[key + "_lu"] = lu.astype(np.complex64)
+        out[key + "_ipiv"] = (piv + 1).astype(np.int32)
+        out[key + "_b"] = b
+        for trans in (0, 1, 2):
+            x = solve_lu(lu.astype(np.complex128), b.astype(np.complex128), piv.astype(np.int64), trans)
+            out[f"{key}_x{trans}"] = np.asarray(x, dtype=np.complex128)
+    for n, count in [(48, 2), (3, 2), (32, 4)]:
+        np.random.seed(42)
+        a = np.random.randn(count, n, n).astype(np.float32) + 1j * np.random.randn(count, n, n).astype(np.float32)
+        for q in range(count):
+            for i in range(n):
+                row = np.sum(np.abs(a[q, i, :])) - np.abs(a[q, i, i])
+                a[q, i, i] = (row + np.random.rand() * 10) * (1 + 1j)
+        a = a.astype(np.complex64)
+        out[f"inverse_n{n}_a"] = a
+        out[f"inverse_n{n}_golden"] = np.stack([np.linalg.inv(a[q]).astype(np.complex64) for q in range(count)])
+    return out
+
+
 def cholesky_ratios(ref):
     sys.path.insert(0, str(Path(ref) / "test" / "cholesky"))
     from lapack_residual import paired  # the reference judge
@@ -159,6 +217,7 @@ def main(ref):
     (OUT / "basic_lu_cases.json").write_text(json.dumps(basic_lu_cases()))
     np.savez_compressed(OUT / "solve_lu.npz", **solve_lu_vectors(ref))
     np.savez_compressed(OUT / "cholesky_cpu_ratios.npz", **cholesky_ratios(ref))
+    np.savez_compressed(OUT / "complex_lu.npz", **complex_lu_vectors(ref))
     print("golden fixtures written to", OUT)
 
 
