@@ -448,6 +448,7 @@ def run_b200(args, rank, world):
         roof_ms = max(FACTOR_BYTES * COUNT / (hbm * 1e9), FACTOR_FLOPS * COUNT / (bf16 * 1e12)) * 1e3
         cpu = cpu_baseline_headline(args, a_cm, b_cm, x64)
         large = measure_large(handle, args) if args.large else None
+        complex_lu = measure_complex_lu(handle, args) if args.complex_lu else None
         by_kappa = {}
         for k, kappa in enumerate(KAPPAS):
             idx = list(range(k, COUNT, len(KAPPAS)))
@@ -535,6 +536,7 @@ def run_b200(args, rank, world):
             "cpu_baseline": cpu,
             "configs": configs,
             "large": large,
+            "complex_lu": complex_lu,
         }
         print(json.dumps(line), flush=True)
     handle.close()
@@ -990,6 +992,195 @@ def measure_spotrf_large(handle, args, n=4096, steps=3):
     return out
 
 
+def measure_complex_lu(handle, args, steps=3):
+    """The complex LU family on its own workloads, device time per call (median of `steps`
+    after one warm-up, inputs restored before each call):
+      cgetrf   one 4096 x 4096 matrix of the reference's recipe (test/cgetrf/data/gen_data.py:
+               integer real and imaginary parts 1..10), aclsolverCgetrf with pivots;
+      cgetri   its inverse from the LU (aclsolverCgetri, the compensated column solves);
+      cgetri_batched  10,000 LU factors of order 64 (aclsolverCgetriBatched);
+      cmatinv  100,000 matrices of order 32 (aclsolverCmatinvBatched, Gauss-Jordan);
+      cgetrs   one 4096 system with 64 right-hand sides through the host-buffer
+               aclsolverCgetrs (row-major host A and B, copies inside the timed call)."""
+    import numpy as np
+    import torch
+
+    import aclsolver
+
+    lib = aclsolver.library()
+    stream = handle.stream
+    fp32 = fp32_peak_tflops()
+    hbm, _, _ = peaks()
+
+    def timed(call, restore=None):
+        times = []
+        for _ in range(steps + 1):
+            if restore:
+                restore()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            call()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        return sorted(times[1:])[len(times[1:]) // 2]
+
+    out = {}
+    n = 4096
+    rng = np.random.RandomState(149)
+    a_host = rng.randint(1, 11, size=(n, 2 * n)).astype(np.float32).view(np.complex64)
+    a0 = torch.from_numpy(np.ascontiguousarray(a_host.T).view(np.float32).reshape(-1)).cuda()  # column-major
+    a = torch.empty_like(a0)
+    ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ms = timed(lambda: aclsolver.check(lib.aclsolverCgetrf(handle.value, n, n, a.data_ptr(), n, None,
+                                                            ipiv.data_ptr(), info.data_ptr())),
+               lambda: a.copy_(a0))
+    assert int(info.item()) == 0
+    flops = 8.0 * n ** 3 / 3
+    out["cgetrf"] = {"workload": f"one {n} x {n} complex64 matrix (integer parts 1..10), partial pivoting",
+                     "ms": round(ms, 3), "gflops": round(flops / (ms * 1e-3) / 1e9, 1),
+                     "roofline": {"bound": "fp32 FMA (CUDA cores)", "achieved_tflops": round(flops / ms / 1e9, 2),
+                                  "peak_tflops": fp32, "frac": round(flops / ms / 1e9 / fp32, 4)}}
+    lu = a.clone()
+    work = torch.empty(2 * n * n, dtype=torch.float32, device="cuda")
+    inv = torch.empty_like(lu)
+    ms = timed(lambda: aclsolver.check(lib.aclsolverCgetri(handle.value, n, inv.data_ptr(), n, ipiv.data_ptr(),
+                                                            work.data_ptr(), n * n, info.data_ptr())),
+               lambda: inv.copy_(lu))
+    assert int(info.item()) == 0
+    cflops = 36.0 * n ** 3  # n^3 compensated complex updates of 36 flops each
+    out["cgetri"] = {"workload": f"inverse of that {n} x {n} LU in place (compensated column solves)",
+                     "ms": round(ms, 3),
+                     "roofline": {"bound": "fp32 (CUDA cores)", "achieved_tflops": round(cflops / ms / 1e9, 2),
+                                  "peak_tflops": fp32, "frac": round(cflops / ms / 1e9 / fp32, 4)}}
+    del work, inv
+
+    # batched inverse from LU factors, order 64
+    count, m = 10_000, 64
+    g = torch.Generator(device="cuda").manual_seed(3)
+    lus = torch.randn(count, m, m, 2, device="cuda", generator=g)
+    lus[:, torch.arange(m), torch.arange(m), 0] += 2.0 * m  # a dominant diagonal keeps every factor regular
+    lus = lus.reshape(-1).contiguous()
+    piv = torch.arange(1, m + 1, dtype=torch.int32, device="cuda").repeat(count)
+    outs = torch.empty_like(lus)
+    tab_a = aclsolver.pointer_table(lus, count, m * m * 8)
+    tab_c = aclsolver.pointer_table(outs, count, m * m * 8)
+    infos = torch.zeros(count, dtype=torch.int32, device="cuda")
+    ms = timed(lambda: aclsolver.check(lib.aclsolverCgetriBatched(handle.value, m, tab_a.data_ptr(), m, piv.data_ptr(),
+                                                                   tab_c.data_ptr(), m, infos.data_ptr(), count)))
+    assert int((infos != 0).sum().item()) == 0
+    bytes_ = 2.0 * count * m * m * 8
+    out["cgetri_batched"] = {"workload": f"{count:,} LU factors of order {m} (complex64), identity pivots",
+                             "ms": round(ms, 3), "matrices_per_s": round(count / (ms * 1e-3), 1),
+                             "roofline": {"bound": "fp32 (CUDA cores)",
+                                          "achieved_tflops": round(36.0 * m ** 3 * count / ms / 1e9, 2),
+                                          "peak_tflops": fp32, "hbm_gbs": round(bytes_ / ms / 1e6, 1),
+                                          "hbm_frac": round(bytes_ / ms / 1e6 / hbm, 4)}}
+    del lus, outs
+
+    # direct inverse, order 32, the reference's inverse recipe
+    count, m = 100_000, 32
+    g = torch.Generator(device="cuda").manual_seed(4)
+    mats = torch.randn(count, m, m, 2, device="cuda", generator=g)
+    mats[:, torch.arange(m), torch.arange(m), :] += 4.0 * m ** 0.5
+    mats = mats.reshape(-1).contiguous()
+    outs = torch.empty_like(mats)
+    tab_a = aclsolver.pointer_table(mats, count, m * m * 8)
+    tab_c = aclsolver.pointer_table(outs, count, m * m * 8)
+    infos = torch.zeros(count, dtype=torch.int32, device="cuda")
+    ms = timed(lambda: aclsolver.check(lib.aclsolverCmatinvBatched(handle.value, m, tab_a.data_ptr(), m,
+                                                                    tab_c.data_ptr(), m, infos.data_ptr(), count)))
+    assert int((infos != 0).sum().item()) == 0
+    bytes_ = 2.0 * count * m * m * 8
+    gj = 8.0 * m ** 3 * count  # n^3 complex multiply-adds per Gauss-Jordan
+    out["cmatinv"] = {"workload": f"{count:,} matrices of order {m} (complex64), Gauss-Jordan",
+                      "ms": round(ms, 3), "matrices_per_s": round(count / (ms * 1e-3), 1),
+                      "roofline": {"bound": "fp32 FMA (CUDA cores)", "achieved_tflops": round(gj / ms / 1e9, 2),
+                                   "peak_tflops": fp32, "frac": round(gj / ms / 1e9 / fp32, 4),
+                                   "hbm_gbs": round(bytes_ / ms / 1e6, 1), "hbm_frac": round(bytes_ / ms / 1e6 / hbm, 4)}}
+    del mats, outs
+
+    # host-buffer solve
+    nrhs = 64
+    lu_host = np.ascontiguousarray(lu.cpu().numpy().view(np.complex64).reshape(n, n).T)  # row-major LU
+    piv_host = ipiv.cpu().numpy().astype(np.int32)
+    b_host = (rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))).astype(np.complex64)
+    hinfo = np.zeros(1, dtype=np.int32)
+    times = []
+    for _ in range(steps + 1):
+        b = b_host.copy()
+        t0 = time.perf_counter()
+        st = lib.aclsolverCgetrs(handle.value, 0, n, nrhs, lu_host.ctypes.data, n, piv_host.ctypes.data,
+                                 b.ctypes.data, nrhs, hinfo.ctypes.data)
+        times.append((time.perf_counter() - t0) * 1e3)
+        assert st == 0 and hinfo[0] == 0
+    ms = sorted(times[1:])[len(times[1:]) // 2]
+    out["cgetrs_host"] = {"workload": f"one {n} system, {nrhs} right-hand sides, host row-major buffers "
+                                      "(H2D, layout, solve, D2H inside the call)",
+                          "ms_wall": round(ms, 3), "h2d_bytes": n * n * 8 + n * nrhs * 8 + n * 4,
+                          "d2h_bytes": n * nrhs * 8}
+    if args is not None and args.cpu_seconds > 0:
+        from scipy.linalg import lapack
+
+        t0 = time.perf_counter()
+        _, _, st = lapack.cgetrf(a_host)
+        dt = time.perf_counter() - t0
+        out["cgetrf"]["cpu_baseline"] = {"ms": round(dt * 1e3, 1), "kind": "scipy LAPACK cgetrf (OpenBLAS threads)",
+                                         "info": int(st)}
+    return out
+
+
+def run_profile_complex():
+    """Each complex LU workload once, for an ncu capture: Cgetrf of one 2048 x 2048 matrix
+    (the reference recipe), CgetriBatched of 10,000 order-64 LU factors, CmatinvBatched of
+    100,000 order-32 matrices, Cgetri of one 512 x 512 LU."""
+    import numpy as np
+    import torch
+
+    import aclsolver
+
+    lib = aclsolver.library()
+    handle = aclsolver.Handle()
+    n = 2048
+    rng = np.random.RandomState(149)
+    a_host = rng.randint(1, 11, size=(n, 2 * n)).astype(np.float32).view(np.complex64)
+    a = torch.from_numpy(np.ascontiguousarray(a_host.T).view(np.float32).reshape(-1)).cuda()
+    ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    aclsolver.check(lib.aclsolverCgetrf(handle.value, n, n, a.data_ptr(), n, None, ipiv.data_ptr(), info.data_ptr()))
+    count, m = 10_000, 64
+    g = torch.Generator(device="cuda").manual_seed(3)
+    lus = torch.randn(count, m, m, 2, device="cuda", generator=g)
+    lus[:, torch.arange(m), torch.arange(m), 0] += 2.0 * m
+    lus = lus.reshape(-1).contiguous()
+    piv = torch.arange(1, m + 1, dtype=torch.int32, device="cuda").repeat(count)
+    outs = torch.empty_like(lus)
+    infos = torch.zeros(count, dtype=torch.int32, device="cuda")
+    tab_a, tab_c = aclsolver.pointer_table(lus, count, m * m * 8), aclsolver.pointer_table(outs, count, m * m * 8)
+    aclsolver.check(lib.aclsolverCgetriBatched(handle.value, m, tab_a.data_ptr(), m, piv.data_ptr(), tab_c.data_ptr(),
+                                               m, infos.data_ptr(), count))
+    count, m = 100_000, 32
+    mats = torch.randn(count, m, m, 2, device="cuda", generator=g)
+    mats[:, torch.arange(m), torch.arange(m), :] += 4.0 * m ** 0.5
+    mats = mats.reshape(-1).contiguous()
+    outs = torch.empty_like(mats)
+    infos = torch.zeros(count, dtype=torch.int32, device="cuda")
+    tab_a, tab_c = aclsolver.pointer_table(mats, count, m * m * 8), aclsolver.pointer_table(outs, count, m * m * 8)
+    aclsolver.check(lib.aclsolverCmatinvBatched(handle.value, m, tab_a.data_ptr(), m, tab_c.data_ptr(), m,
+                                                infos.data_ptr(), count))
+    m = 512
+    sub = a.view(n, n, 2)[:m, :m].contiguous()  # a leading block of the LU: regular, identity pivots
+    pv = torch.arange(1, m + 1, dtype=torch.int32, device="cuda")
+    work = torch.empty(2 * m * m, dtype=torch.float32, device="cuda")
+    aclsolver.check(lib.aclsolverCgetri(handle.value, m, sub.data_ptr(), m, pv.data_ptr(), work.data_ptr(), m * m,
+                                        info.data_ptr()))
+    torch.cuda.synchronize()
+    handle.close()
+    print("profile-complex done", flush=True)
+
+
 # ---------------------------------------------------------------------------------------
 # CPU baselines
 # ---------------------------------------------------------------------------------------
@@ -1163,6 +1354,10 @@ def main():
                     help="skip the single 8192 x 8192 system reported under the 'large' key")
     ap.add_argument("--no-configs", dest="configs", action="store_false",
                     help="skip the plain batched workloads reported under the 'configs' key")
+    ap.add_argument("--no-complex-lu", dest="complex_lu", action="store_false",
+                    help="skip the complex LU family workloads reported under the 'complex_lu' key")
+    ap.add_argument("--profile-complex", action="store_true",
+                    help="run each complex LU workload once (for an ncu capture) and exit")
     ap.add_argument("--profile-large", action="store_true",
                     help="one large plain factorisation + solve and one large refinement call, for ncu")
     ap.add_argument("--profile", action="store_true",
@@ -1186,6 +1381,8 @@ def main():
             run_profile()
         elif args.profile_small:
             run_profile_small(args)
+        elif args.profile_complex:
+            run_profile_complex()
         elif args.profile_large:
             run_profile_large()
         elif args.impl == "reference":

@@ -109,25 +109,28 @@ aclsolverStatus_t check_matrices(Handle *h, const void *a_table, const void *c_t
     const uintptr_t *in = reinterpret_cast<const uintptr_t *>(host);
     const uintptr_t *out = reinterpret_cast<const uintptr_t *>(host + ptr_bytes);
     const size_t a_bytes = (size_t)lda * n * sizeof(float2), c_bytes = (size_t)ldc * n * sizeof(float2);
-    std::vector<Span> spans;
+    std::vector<Span> ins, outs, spans;
     try
     {
-        spans.reserve((size_t)batch * 2 + n_extra);
+        ins.reserve((size_t)batch);
+        outs.reserve((size_t)batch);
+        spans.resize((size_t)batch * 2);
     }
     catch (...)
     {
         return ACLSOLVER_STATUS_ALLOC_FAILED;
     }
+    SpanCache in_cache, out_cache;
     for (int q = 0; q < batch; ++q)
     {
         const void *ib = reinterpret_cast<const void *>(in[q]);
         const void *ob = reinterpret_cast<const void *>(out[q]);
-        if (!span_ok(ib, a_bytes, alignof(float2)))
+        if (!in_cache.ok(ib, a_bytes, alignof(float2)))
         {
             *bad = in_arg;
             return ACLSOLVER_STATUS_INVALID_VALUE;
         }
-        if (!span_ok(ob, c_bytes, alignof(float2)))
+        if (!out_cache.ok(ob, c_bytes, alignof(float2)))
         {
             *bad = out_arg;
             return ACLSOLVER_STATUS_INVALID_VALUE;
@@ -139,8 +142,8 @@ aclsolverStatus_t check_matrices(Handle *h, const void *a_table, const void *c_t
                 *bad = extra_arg[x];
                 return ACLSOLVER_STATUS_INVALID_VALUE;
             }
-        spans.push_back({in[q], in[q] + a_bytes, 0});
-        spans.push_back({out[q], out[q] + c_bytes, 1});
+        ins.push_back({in[q], in[q] + a_bytes, 0});
+        outs.push_back({out[q], out[q] + c_bytes, 1});
     }
     for (int x = 0; x < n_extra; ++x)
         for (int y = x + 1; y < n_extra; ++y)
@@ -149,8 +152,11 @@ aclsolverStatus_t check_matrices(Handle *h, const void *a_table, const void *c_t
                 *bad = extra_arg[y];
                 return ACLSOLVER_STATUS_INVALID_VALUE;
             }
-    std::sort(spans.begin(), spans.end(), [](const Span &x, const Span &y)
-              { return x.begin < y.begin || (x.begin == y.begin && x.role < y.role); });
+    // tables over a slab arrive in ascending order: sort only when they do not, then merge
+    auto before = [](const Span &x, const Span &y) { return x.begin < y.begin || (x.begin == y.begin && x.role < y.role); };
+    if (!std::is_sorted(ins.begin(), ins.end(), before)) std::sort(ins.begin(), ins.end(), before);
+    if (!std::is_sorted(outs.begin(), outs.end(), before)) std::sort(outs.begin(), outs.end(), before);
+    std::merge(ins.begin(), ins.end(), outs.begin(), outs.end(), spans.begin(), before);
     uintptr_t read_end = 0, write_end = 0;
     for (const Span &s : spans)
     {

@@ -184,13 +184,14 @@ aclsolverStatus_t check_arrays(Handle *h, int n, const float *const *a, int lda,
     {
         return ACLSOLVER_STATUS_ALLOC_FAILED;
     }
+    SpanCache in_cache, out_cache;
     for (int b = 0; b < batch; ++b)
     {
         if (in[b] != in[0] + (size_t)b * a_bytes || out[b] != out[0] + (size_t)b * c_bytes) layout.contiguous = false;
         const void *ib = reinterpret_cast<const void *>(in[b]);
         const void *ob = reinterpret_cast<const void *>(out[b]);
-        if (!device_fits(ib, a_bytes, alignof(float))) return invalid(h, info, batch, 2);
-        if (!device_fits(ob, c_bytes, alignof(float))) return invalid(h, info, batch, out_arg);
+        if (!in_cache.ok(ib, a_bytes, alignof(float))) return invalid(h, info, batch, 2);
+        if (!out_cache.ok(ob, c_bytes, alignof(float))) return invalid(h, info, batch, out_arg);
         if (overlap(ib, a_bytes, info, info_bytes) || overlap(ob, c_bytes, info, info_bytes))
             return ACLSOLVER_STATUS_INVALID_VALUE;
         for (int i = 0; i < 3; ++i)

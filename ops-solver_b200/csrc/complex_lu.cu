@@ -10,8 +10,10 @@
 //   cgetrf_panel_kernel   one block factors a panel held in shared memory: pivot search
 //                         (PivotScore, earliest row on ties), row swap, Divide of the column
 //                         below the diagonal, rank-1 SubMul update of the panel's columns
-//   claswp_kernel         the panel's interchanges applied to the columns outside it
-//   ctrsm_block_kernel    a <= 32-row block of a triangular solve, one thread per column,
+//   claswp_kernel         a whole interchange sequence on a solve's right-hand sides
+//   claswp_panel_kernel   a panel's interchanges applied to the columns outside it as one
+//                         composed row move per (column, row)
+//   ctrsm_block_kernel    a <= 32-row block of a triangular solve, one warp per column,
 //                         the diagonal tile in shared memory (unit or Divide diagonal)
 //   cchain_update_kernel  C -= A B over k <= 32 as a per-element SubMul chain in pivot
 //                         order (ascending, or descending for backward solves), 64 x 64 tiles
@@ -37,7 +39,7 @@ namespace
 constexpr int PANEL = 32;               // columns per factor panel and per update step
 constexpr int PANEL_THREADS = 1024;     // one block factors a panel
 constexpr int CAPACITY = 24 * 1024;     // complex elements of a panel held in shared memory
-constexpr int TRSM_THREADS = 128;
+constexpr int TRSM_THREADS = 256;  // 8 columns per block, one warp each
 constexpr int UPD_TILE = 64;
 constexpr int INV_BLOCK = 64;           // rows per compensated block step (order > 256)
 constexpr int INV_TILE_COLS = 32;
@@ -172,8 +174,9 @@ __global__ void claswp_kernel(float2 *A, int64_t lda, int ncols, int k0, int k1,
 }
 
 // One block of a triangular solve: rows [0, w) of X's columns [0, ncols) against the w x w
-// diagonal tile T.  FWD: x_i -= T_ip x_p for p < i in ascending order; BWD: for p > i in
-// descending order; a non-unit diagonal divides x_p (Divide) when its turn comes.
+// diagonal tile T, one warp per column with lane i holding row i.  FWD: x_i -= T_ip x_p for
+// p < i in ascending order; BWD: for p > i in descending order; a non-unit diagonal divides
+// x_p (Divide) when its turn comes.
 template <bool FWD, bool UNIT>
 __global__ void __launch_bounds__(TRSM_THREADS) ctrsm_block_kernel(const float2 *T, int64_t ldt, float2 *X,
                                                                    int64_t ldx, int w, int ncols)
@@ -191,38 +194,62 @@ __global__ void __launch_bounds__(TRSM_THREADS) ctrsm_block_kernel(const float2 
         if (threadIdx.x < w) dv[threadIdx.x] = cprepare(tile[threadIdx.x][threadIdx.x]);
         __syncthreads();
     }
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int j = blockIdx.x * (TRSM_THREADS / 32) + (threadIdx.x >> 5);
     if (j >= ncols) return;
     float2 *xc = X + (int64_t)j * ldx;
-    float2 x[PANEL];
-#pragma unroll
-    for (int i = 0; i < PANEL; ++i) x[i] = i < w ? xc[i] : make_float2(0.0f, 0.0f);
-    if (FWD)
+    float2 x = lane < w ? xc[lane] : make_float2(0.0f, 0.0f);
+    for (int t = 0; t < w; ++t)
     {
-#pragma unroll
-        for (int p = 0; p < PANEL; ++p)
-            if (p < w)
-            {
-                if (!UNIT) x[p] = cdivide(x[p], dv[p]);
-#pragma unroll
-                for (int i = p + 1; i < PANEL; ++i)
-                    if (i < w) x[i] = csubmul(x[i], tile[p][i], x[p]);
-            }
+        const int p = FWD ? t : w - 1 - t;
+        if (!UNIT && lane == p) x = cdivide(x, dv[p]);
+        const float2 v = make_float2(__shfl_sync(0xffffffffu, x.x, p), __shfl_sync(0xffffffffu, x.y, p));
+        if (FWD ? (lane > p && lane < w) : (lane < p)) x = csubmul(x, tile[p][lane], v);
     }
-    else
+    if (lane < w) xc[lane] = x;
+}
+
+// The interchanges ipiv[k0..k0+w) (global 1-based rows, w <= 32) applied in order to columns
+// [0, ncols) of A except [skip0, skip1).  Their composition moves at most 2w rows; thread 0
+// derives it (row_of[i] receives the original row src_of[i]), then each thread moves one
+// row of one column: every value is read before any is written.
+__global__ void __launch_bounds__(256) claswp_panel_kernel(float2 *A, int64_t lda, int ncols, int k0, int w,
+                                                           const int *ipiv, int skip0, int skip1)
+{
+    __shared__ int row_of[2 * PANEL], src_of[2 * PANEL], count;
+    if (threadIdx.x == 0)
     {
-#pragma unroll
-        for (int p = PANEL - 1; p >= 0; --p)
-            if (p < w)
+        int cnt = w;
+        for (int i = 0; i < w; ++i) row_of[i] = src_of[i] = k0 + i;
+        for (int k = 0; k < w; ++k)
+        {
+            const int p = __ldg(ipiv + k0 + k) - 1;
+            int ip = -1;
+            if (p >= k0 && p < k0 + w)
+                ip = p - k0;
+            else
             {
-                if (!UNIT) x[p] = cdivide(x[p], dv[p]);
-#pragma unroll
-                for (int i = 0; i < p; ++i) x[i] = csubmul(x[i], tile[p][i], x[p]);
+                for (int e = w; e < cnt; ++e)
+                    if (row_of[e] == p) ip = e;
+                if (ip < 0)
+                {
+                    ip = cnt++;
+                    row_of[ip] = src_of[ip] = p;
+                }
             }
+            const int t = src_of[k];
+            src_of[k] = src_of[ip];
+            src_of[ip] = t;
+        }
+        count = cnt;
     }
-#pragma unroll
-    for (int i = 0; i < PANEL; ++i)
-        if (i < w) xc[i] = x[i];
+    __syncthreads();
+    const int j = blockIdx.x * 4 + (threadIdx.x >> 6), idx = threadIdx.x & 63;
+    const bool act = j < ncols && (j < skip0 || j >= skip1) && idx < count && src_of[idx] != row_of[idx];
+    float2 v = make_float2(0.0f, 0.0f);
+    if (act) v = A[(int64_t)j * lda + src_of[idx]];
+    __syncthreads();
+    if (act) A[(int64_t)j * lda + row_of[idx]] = v;
 }
 
 // C[r][j] (r < rows, j < cols) -= sum over p < k of A[r][p] B[p][j] as a SubMul chain per
@@ -720,7 +747,8 @@ cudaError_t trsm_block(bool fwd, bool unit, const float2 *T, int64_t ldt, float2
                        cudaStream_t stream)
 {
     if (ncols <= 0 || w <= 0) return cudaSuccess;
-    const int grid = (ncols + TRSM_THREADS - 1) / TRSM_THREADS;
+    const int per_block = TRSM_THREADS / 32;
+    const int grid = (ncols + per_block - 1) / per_block;
     if (fwd && unit)
         ctrsm_block_kernel<true, true><<<grid, TRSM_THREADS, 0, stream>>>(T, ldt, X, ldx, w, ncols);
     else if (fwd)
@@ -768,7 +796,11 @@ cudaError_t launch_cgetrf(float2 *A, int lda, int m, int n, int *ipiv, int *info
             const size_t smem = (size_t)(m - c) * w * sizeof(float2);
             cgetrf_panel_kernel<<<1, PANEL_THREADS, smem, stream>>>(A, lda, m, c, c + w, c + w, ipiv, info);
             e = cudaGetLastError();
-            if (e == cudaSuccess && ipiv) e = laswp(A, lda, n, c, c + w, ipiv, c, c + w, false, stream);
+            if (e == cudaSuccess && ipiv && n > w)
+            {
+                claswp_panel_kernel<<<(n + 3) / 4, 256, 0, stream>>>(A, lda, n, c, w, ipiv, c, c + w);
+                e = cudaGetLastError();
+            }
             if (e == cudaSuccess && c + w < k + kb)
             {
                 const int right = k + kb - (c + w);

@@ -43,7 +43,10 @@ __device__ __forceinline__ float2 csubmul(float2 x, float2 a, float2 b)
     return make_float2(fma_rn(a.y, b.y, fma_rn(-a.x, b.x, x.x)), fma_rn(-a.y, b.x, fma_rn(-a.x, b.y, x.y)));
 }
 
-__device__ __forceinline__ float cquotient(float ar, float br, float ai, float bi, float den, float den_err)
+// Quotient with the divisor's reciprocal 1/den supplied (the same IEEE value the reference
+// computes inline; PreparedQuotient, complex_solver_register.hpp:203-214, passes it in too).
+__device__ __forceinline__ float cquotient(float ar, float br, float ai, float bi, float den, float den_err,
+                                           float reciprocal)
 {
     float product = mul_rn(ar, br);
     float other = mul_rn(ai, bi);
@@ -52,7 +55,6 @@ __device__ __forceinline__ float cquotient(float ar, float br, float ai, float b
     float error = add_rn(add_rn(add_rn(sub_rn(product, sub_rn(numerator, part)), sub_rn(other, part)),
                                 fma_rn(ar, br, -product)),
                          fma_rn(ai, bi, -other));
-    float reciprocal = div_rn(1.0f, den);
     float result = mul_rn(numerator, reciprocal);
     float remainder = sub_rn(add_rn(fma_rn(-result, den, numerator), error), mul_rn(result, den_err));
     return fma_rn(remainder, reciprocal, result);
@@ -69,25 +71,28 @@ static __device__ __noinline__ float cscaled_quot(float a, float b, float c, flo
     int e = zab ? cd : zcd ? ab : (ab > cd ? ab : cd);
     am = zab ? 0.0f : ldexpf(am, ab - e);
     cm = zcd ? 0.0f : ldexpf(cm, cd - e);
-    float q = cquotient(am, bm, cm, dm, den, den_err);
+    float q = cquotient(am, bm, cm, dm, den, den_err, div_rn(1.0f, den));
     return ldexpf(div_rn(q, mul_rn(sm, sm)), e - 2 * se);
-}
-
-__device__ __forceinline__ bool cneeds_scaled(float2 a, float2 b, float scale, float ar, float ai)
-{
-    return cabs1(a.x) <= FMAX && cabs1(a.y) <= FMAX && scale > 0.0f && scale <= FMAX &&
-           (cabs1(ar) > 0x1p120f || cabs1(ai) > 0x1p120f || (a.x != 0.0f && cabs1(ar) < 0x1p-100f) ||
-            (a.y != 0.0f && cabs1(ai) < 0x1p-100f) || (b.x != 0.0f && cabs1(div_rn(b.x, scale)) < 0x1p-100f) ||
-            (b.y != 0.0f && cabs1(div_rn(b.y, scale)) < 0x1p-100f));
 }
 
 // The divisor's half of Divide, shared by every numerator divided by the same value
 // (the reference's PrepareDivisor computes exactly these terms, complex_solver_register.hpp:183-201).
+// inv_s = 1/s when s is a normal power of two, so x * inv_s is the correctly rounded x / s
+// (both round the same exact value once); 0 when s must be divided by.  divisor_tiny and
+// divisor_ok fold the numerator-independent terms of NeedsScaledNumerator.
 struct Divisor
 {
     float2 b;
-    float s, br, bi, den, err;
+    float s, br, bi, den, err, rcp, inv_s;
+    bool divisor_ok, divisor_tiny;
 };
+
+__device__ __forceinline__ bool cneeds_scaled(float2 a, const Divisor &d, float ar, float ai)
+{
+    return cabs1(a.x) <= FMAX && cabs1(a.y) <= FMAX && d.divisor_ok &&
+           (cabs1(ar) > 0x1p120f || cabs1(ai) > 0x1p120f || (a.x != 0.0f && cabs1(ar) < 0x1p-100f) ||
+            (a.y != 0.0f && cabs1(ai) < 0x1p-100f) || d.divisor_tiny);
+}
 
 __device__ __forceinline__ Divisor cprepare(float2 b)
 {
@@ -104,16 +109,31 @@ __device__ __forceinline__ Divisor cprepare(float2 b)
     float square = mul_rn(first, first);
     d.den = fma_rn(second, second, square);
     d.err = add_rn(fma_rn(first, first, -square), fma_rn(second, second, sub_rn(square, d.den)));
+    d.rcp = div_rn(1.0f, d.den);
+    d.inv_s = ex != 0 && ex <= 0x7e800000u ? __uint_as_float(0x7f000000u - ex) : 0.0f;  // 2^-e for s = 2^e <= 2^126
+    d.divisor_ok = s > 0.0f && s <= FMAX;
+    d.divisor_tiny = (b.x != 0.0f && cabs1(d.br) < 0x1p-100f) || (b.y != 0.0f && cabs1(d.bi) < 0x1p-100f);
     return d;
 }
 
 __device__ __forceinline__ float2 cdivide(float2 a, const Divisor &d)
 {
-    float ar = div_rn(a.x, d.s), ai = div_rn(a.y, d.s);
-    if (cneeds_scaled(a, d.b, d.s, ar, ai))
+    float ar, ai;
+    if (d.inv_s != 0.0f)
+    {
+        ar = mul_rn(a.x, d.inv_s);
+        ai = mul_rn(a.y, d.inv_s);
+    }
+    else
+    {
+        ar = div_rn(a.x, d.s);
+        ai = div_rn(a.y, d.s);
+    }
+    if (cneeds_scaled(a, d, ar, ai))
         return make_float2(cscaled_quot(a.x, d.b.x, a.y, d.b.y, d.s, d.den, d.err),
                            cscaled_quot(a.y, d.b.x, -a.x, d.b.y, d.s, d.den, d.err));
-    return make_float2(cquotient(ar, d.br, ai, d.bi, d.den, d.err), cquotient(ai, d.br, -ar, d.bi, d.den, d.err));
+    return make_float2(cquotient(ar, d.br, ai, d.bi, d.den, d.err, d.rcp),
+                       cquotient(ai, d.br, -ar, d.bi, d.den, d.err, d.rcp));
 }
 
 __device__ __forceinline__ float2 cdivide(float2 a, float2 b) { return cdivide(a, cprepare(b)); }

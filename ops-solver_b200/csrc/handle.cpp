@@ -75,6 +75,22 @@ bool device_span(const void *p, size_t bytes)
     return a >= b0 && bytes <= size - (a - b0);
 }
 
+bool SpanCache::ok(const void *p, size_t bytes, size_t align)
+{
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    if (!p || a % align != 0) return false;
+    if (a >= begin && a < end && bytes <= end - a) return true;
+    if (!is_device_pointer(p)) return false;
+    MemGetAddressRangeFn fn = address_range_fn();
+    if (!fn) return true;
+    CUdeviceptr base = 0;
+    size_t size = 0;
+    if (fn(&base, &size, (CUdeviceptr)a) != CUDA_SUCCESS) return false;
+    begin = (uintptr_t)base;
+    end = begin + size;
+    return a >= begin && bytes <= end - a;
+}
+
 aclsolverStatus_t launch_status(cudaError_t launch)
 {
     cudaError_t last = cudaGetLastError();

@@ -63,6 +63,15 @@ bool is_device_pointer(const void *p);
 // the driver query is unavailable the span is accepted.
 bool device_span(const void *p, size_t bytes);
 
+// Per-call memo of verified device allocations for pointer tables: a slot that lies inside
+// an allocation already queried needs no driver call (tables of 10^6 slots over one slab
+// cost one query instead of two per slot).
+struct SpanCache
+{
+    uintptr_t begin = 0, end = 0;
+    bool ok(const void *p, size_t bytes, size_t align);
+};
+
 // Status of the launches just enqueued (consumes this library's last CUDA error).
 aclsolverStatus_t launch_status(cudaError_t launch);
 
