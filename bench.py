@@ -1133,7 +1133,7 @@ def measure_complex_lu(handle, args, steps=3):
 
 
 def run_profile_complex():
-    """Each complex LU workload once, for an ncu capture: Cgetrf of one 2048 x 2048 matrix
+    """Each complex LU workload once, for an ncu capture: Cgetrf of one 4096 x 4096 matrix
     (the reference recipe), CgetriBatched of 10,000 order-64 LU factors, CmatinvBatched of
     100,000 order-32 matrices, Cgetri of one 512 x 512 LU."""
     import numpy as np
@@ -1143,7 +1143,7 @@ def run_profile_complex():
 
     lib = aclsolver.library()
     handle = aclsolver.Handle()
-    n = 2048
+    n = 4096
     rng = np.random.RandomState(149)
     a_host = rng.randint(1, 11, size=(n, 2 * n)).astype(np.float32).view(np.complex64)
     a = torch.from_numpy(np.ascontiguousarray(a_host.T).view(np.float32).reshape(-1)).cuda()

@@ -7,9 +7,12 @@
 // src/utils/complex_solver_kernel.hpp:161-250, complex_solver_update.hpp:60-82), so the
 // factor is the same bits whether it runs in one block's shared memory or blocked over
 // the whole GPU:
-//   cgetrf_panel_kernel   one block factors a panel held in shared memory: pivot search
+//   cgetrf_panel_kernel   one block factors a whole small matrix in shared memory: pivot search
 //                         (PivotScore, earliest row on ties), row swap, Divide of the column
 //                         below the diagonal, rank-1 SubMul update of the panel's columns
+//   cgetrf_row_panel_kernel  a 32-column panel of a larger matrix, one row per thread over a
+//                         thread-block cluster of up to 8 blocks (distributed shared memory
+//                         for the pivot candidates and rows, cluster barriers)
 //   claswp_kernel         a whole interchange sequence on a solve's right-hand sides
 //   claswp_panel_kernel   a panel's interchanges applied to the columns outside it as one
 //                         composed row move per (column, row)
@@ -23,6 +26,8 @@
 // two planes and sweep 64-row blocks (cinv_block_kernel + cinv_update_kernel), same order.
 // The direct inverse restates InvertSmallInPlace (src/utils/complex_solver_register.hpp:
 // 271-326): Gauss-Jordan with one lane per column, the matrix in registers.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <atomic>
 
@@ -150,6 +155,140 @@ __global__ void __launch_bounds__(PANEL_THREADS) cgetrf_panel_kernel(float2 *A, 
         int r = idx % H, j = idx / H;
         A[(int64_t)(c0 + j) * lda + c0 + r] = sp[idx];
     }
+}
+
+// Row-per-thread panel: rows [c0, m) x columns [c0, c0 + w) (w <= 32), each thread of a
+// cluster of `cl` blocks owning one panel row (block r: panel rows [rR, rR + R), R <= ROW_MAX,
+// so the diagonal rows live in block 0), kept in the thread's own shared-memory row (pitch 33:
+// a warp's rows fall in distinct banks).  Per column: the block's pivot candidate (warp
+// shuffles, one barrier); cluster barrier; all candidates read through distributed shared
+// memory; the pivot row's owner publishes it and block 0's row-lc thread publishes row lc;
+// cluster barrier; every block copies the pivot row locally, the two owners take each other's
+// row, and every thread below the diagonal divides its l and updates its row.  The column loop
+// stays rolled (an unrolled one overflows the instruction cache).  Same per-element
+// arithmetic as the single-block kernel.
+constexpr int ROW_MAX = 512;
+constexpr int ROW_PITCH = PANEL + 1;
+
+__global__ void __launch_bounds__(ROW_MAX, 1) cgetrf_row_panel_kernel(float2 *A, int lda, int m, int c0, int w,
+                                                                      int R, int *ipiv, int *info)
+{
+    namespace cg = cooperative_groups;
+    extern __shared__ float2 rows_sm[];  // blockDim.x rows x ROW_PITCH
+    __shared__ uint32_t red_score[ROW_MAX / 32];
+    __shared__ int red_row[ROW_MAX / 32];
+    __shared__ uint32_t cand_score;
+    __shared__ int cand_row, pivot_row;
+    __shared__ float2 pub[PANEL], kpub[PANEL], prow[PANEL];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank(), cl = (int)cluster.num_blocks();
+    const int H = m - c0, r0 = rank * R, tid = threadIdx.x;
+    const int g = r0 + tid;  // this thread's panel row
+    const bool valid = tid < R && g < H;
+    float2 *a = rows_sm + (int64_t)tid * ROW_PITCH;
+    for (int j = 0; j < w; ++j) a[j] = valid ? A[(int64_t)(c0 + j) * lda + c0 + g] : make_float2(0.0f, 0.0f);
+#pragma unroll 1
+    for (int lc = 0; lc < w; ++lc)
+    {
+        uint32_t best = 0;
+        int row = H;
+        if (ipiv && valid && g >= lc)
+        {
+            best = cscore(a[lc]);
+            row = g;
+        }
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            uint32_t os = __shfl_down_sync(0xffffffffu, best, off);
+            int orow = __shfl_down_sync(0xffffffffu, row, off);
+            if (os > best || (os == best && orow < row))
+            {
+                best = os;
+                row = orow;
+            }
+        }
+        if ((tid & 31) == 0)
+        {
+            red_score[tid >> 5] = best;
+            red_row[tid >> 5] = row;
+        }
+        __syncthreads();
+        if (tid < 32)
+        {
+            const int warps = blockDim.x >> 5;
+            best = tid < warps ? red_score[tid] : 0u;
+            row = tid < warps ? red_row[tid] : H;
+            for (int off = 16; off > 0; off >>= 1)
+            {
+                uint32_t os = __shfl_down_sync(0xffffffffu, best, off);
+                int orow = __shfl_down_sync(0xffffffffu, row, off);
+                if (os > best || (os == best && orow < row))
+                {
+                    best = os;
+                    row = orow;
+                }
+            }
+            if (tid == 0)
+            {
+                cand_score = best;
+                cand_row = row;
+            }
+        }
+        cluster.sync();
+        if (tid < 32)
+        {
+            uint32_t b = 0;
+            int p = H;
+            if (tid < cl)
+            {
+                b = *cluster.map_shared_rank(&cand_score, tid);
+                p = *cluster.map_shared_rank(&cand_row, tid);
+            }
+            for (int off = 16; off > 0; off >>= 1)
+            {
+                uint32_t os = __shfl_down_sync(0xffffffffu, b, off);
+                int orow = __shfl_down_sync(0xffffffffu, p, off);
+                if (os > b || (os == b && orow < p))
+                {
+                    b = os;
+                    p = orow;
+                }
+            }
+            if (tid == 0) pivot_row = ipiv ? p : lc;
+        }
+        __syncthreads();
+        const int p = pivot_row, owner = p / R;
+        if (valid && g == p)
+            for (int j = 0; j < w; ++j) pub[j] = a[j];
+        if (valid && g == lc)
+            for (int j = 0; j < w; ++j) kpub[j] = a[j];
+        cluster.sync();
+        if (tid < w) prow[tid] = cluster.map_shared_rank(pub, owner)[tid];
+        if (valid && g == p && p != lc)
+        {
+            const float2 *kr = cluster.map_shared_rank(kpub, 0);
+            for (int j = 0; j < w; ++j) a[j] = kr[j];
+        }
+        __syncthreads();
+        if (valid && g == lc)
+            for (int j = 0; j < w; ++j) a[j] = prow[j];
+        if (rank == 0 && tid == 0)
+        {
+            if (ipiv) ipiv[c0 + lc] = c0 + p + 1;
+            if (*info == 0 && czero(prow[lc])) *info = c0 + lc + 1;
+        }
+        if (valid && g > lc)
+        {
+            const float2 d = prow[lc];
+            float2 l = a[lc];
+            if (!czero(d)) l = cdivide(l, cprepare(d));
+            a[lc] = l;
+            for (int j = lc + 1; j < w; ++j) a[j] = csubmul(a[j], l, prow[j]);
+        }
+    }
+    if (valid)
+        for (int j = 0; j < w; ++j) A[(int64_t)(c0 + j) * lda + c0 + g] = a[j];
+    cluster.sync();  // no block leaves while another may still read its shared memory
 }
 
 // Interchanges ipiv[k0..k1) (global 1-based rows), in order, on columns [0, ncols) of A
@@ -710,10 +849,38 @@ cudaError_t panel_attr()
     return once_per_device(g_panel_attr,
                            []
                            {
-                               return cudaFuncSetAttribute(cgetrf_panel_kernel,
-                                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                           (int)(CAPACITY * sizeof(float2)));
+                               cudaError_t e = cudaFuncSetAttribute(cgetrf_panel_kernel,
+                                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                                    (int)(CAPACITY * sizeof(float2)));
+                               if (e == cudaSuccess)
+                                   e = cudaFuncSetAttribute(cgetrf_row_panel_kernel,
+                                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                            (int)(ROW_MAX * ROW_PITCH * sizeof(float2)));
+                               return e;
                            });
+}
+
+// Factor panel columns [k, k + w) (w <= 32) of rows [k, m): each row owned by one thread,
+// over a cluster of ceil((m - k) / 512) blocks (at most 8 for m <= 4096).
+cudaError_t factor_panel(float2 *A, int lda, int m, int k, int w, int *ipiv, int *info, cudaStream_t stream)
+{
+    const int H = m - k;
+    const int cl = (H + ROW_MAX - 1) / ROW_MAX;
+    if (cl > 8) return cudaErrorInvalidValue;
+    const int R = (H + cl - 1) / cl;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cl);
+    cfg.blockDim = dim3((R + 31) / 32 * 32);
+    cfg.dynamicSmemBytes = (size_t)cfg.blockDim.x * ROW_PITCH * sizeof(float2);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, cgetrf_row_panel_kernel, A, lda, m, k, w, R, ipiv, info);
 }
 
 cudaError_t resident_attr()
@@ -788,29 +955,11 @@ cudaError_t launch_cgetrf(float2 *A, int lda, int m, int n, int *ipiv, int *info
     for (int k = 0; k < lim && e == cudaSuccess; k += PANEL)
     {
         const int kb = std::min(PANEL, lim - k);
-        for (int c = k; c < k + kb && e == cudaSuccess;)
+        e = factor_panel(A, lda, m, k, kb, ipiv, info, stream);
+        if (e == cudaSuccess && ipiv && n > kb)
         {
-            int w = PANEL;
-            while (w > 1 && (int64_t)(m - c) * w > CAPACITY) w >>= 1;
-            w = std::min(w, k + kb - c);
-            const size_t smem = (size_t)(m - c) * w * sizeof(float2);
-            cgetrf_panel_kernel<<<1, PANEL_THREADS, smem, stream>>>(A, lda, m, c, c + w, c + w, ipiv, info);
+            claswp_panel_kernel<<<(n + 3) / 4, 256, 0, stream>>>(A, lda, n, k, kb, ipiv, k, k + kb);
             e = cudaGetLastError();
-            if (e == cudaSuccess && ipiv && n > w)
-            {
-                claswp_panel_kernel<<<(n + 3) / 4, 256, 0, stream>>>(A, lda, n, c, w, ipiv, c, c + w);
-                e = cudaGetLastError();
-            }
-            if (e == cudaSuccess && c + w < k + kb)
-            {
-                const int right = k + kb - (c + w);
-                float2 *diag = A + (int64_t)c * lda + c;
-                e = trsm_block(true, true, diag, lda, A + (int64_t)(c + w) * lda + c, lda, w, right, stream);
-                if (e == cudaSuccess)
-                    e = chain_update(A + (int64_t)(c + w) * lda + c + w, lda, A + (int64_t)c * lda + c + w, lda,
-                                     A + (int64_t)(c + w) * lda + c, lda, m - c - w, right, w, false, stream);
-            }
-            c += w;
         }
         if (e == cudaSuccess && k + kb < n)
         {

@@ -58,7 +58,7 @@ def check_getrf(handle, a, pad=1, pivoting=True):
 
 @pytest.mark.parametrize("m,n", [(1, 1), (2, 1), (1, 3), (5, 5), (32, 32), (33, 17), (17, 70), (100, 100),
                                  (150, 150), (200, 200), (300, 257), (257, 300), (800, 40), (20, 2000),
-                                 (1000, 1000)])
+                                 (1000, 1000), (4096, 64), (2500, 700)])
 def test_cgetrf_matches_oracle(handle, m, n):
     a = crandn(np.random.default_rng(m * 7 + n), m, n)
     check_getrf(handle, a, pad=3)
