@@ -61,6 +61,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) cgetrf_panel_kernel(float2 *A, 
     __shared__ uint32_t red_score[PANEL_THREADS / 32];
     __shared__ int red_row[PANEL_THREADS / 32];
     const int H = m - c0, W = c_end - c0, tid = threadIdx.x, T = blockDim.x;
+    int info_now = tid == 0 ? *info : 0;  // read once: this kernel alone writes it meanwhile
     for (int idx = tid; idx < H * W; idx += T)
     {
         int r = idx % H, j = idx / H;
@@ -130,7 +131,11 @@ __global__ void __launch_bounds__(PANEL_THREADS) cgetrf_panel_kernel(float2 *A, 
             }
         __syncthreads();
         const float2 d = col[lc];
-        if (tid == 0 && *info == 0 && czero(d)) *info = c0 + lc + 1;
+        if (tid == 0 && info_now == 0 && czero(d))
+        {
+            info_now = c0 + lc + 1;
+            *info = info_now;
+        }
         if (!czero(d))
         {
             const Divisor dv = cprepare(d);
@@ -187,6 +192,7 @@ __global__ void __launch_bounds__(ROW_MAX, 1) cgetrf_row_panel_kernel(float2 *A,
     const bool valid = tid < R && g < H;
     float2 *a = rows_sm + (int64_t)tid * ROW_PITCH;
     for (int j = 0; j < w; ++j) a[j] = valid ? A[(int64_t)(c0 + j) * lda + c0 + g] : make_float2(0.0f, 0.0f);
+    int info_now = rank == 0 && tid == 0 ? *info : 0;  // read once: this kernel alone writes it meanwhile
 #pragma unroll 1
     for (int lc = 0; lc < w; ++lc)
     {
@@ -258,25 +264,31 @@ __global__ void __launch_bounds__(ROW_MAX, 1) cgetrf_row_panel_kernel(float2 *A,
         }
         __syncthreads();
         const int p = pivot_row, owner = p / R;
-        if (valid && g == p)
-            for (int j = 0; j < w; ++j) pub[j] = a[j];
-        if (valid && g == lc)
-            for (int j = 0; j < w; ++j) kpub[j] = a[j];
-        cluster.sync();
-        if (tid < w) prow[tid] = cluster.map_shared_rank(pub, owner)[tid];
-        if (valid && g == p && p != lc)
+        // the first warp copies whole rows, one column per lane
+        if (tid < w)
         {
-            const float2 *kr = cluster.map_shared_rank(kpub, 0);
-            for (int j = 0; j < w; ++j) a[j] = kr[j];
+            if (rank == owner) pub[tid] = rows_sm[(int64_t)(p - r0) * ROW_PITCH + tid];
+            if (rank == 0) kpub[tid] = rows_sm[(int64_t)lc * ROW_PITCH + tid];
         }
-        __syncthreads();
-        if (valid && g == lc)
-            for (int j = 0; j < w; ++j) a[j] = prow[j];
+        cluster.sync();
+        if (tid < w)
+        {
+            const float2 v = cluster.map_shared_rank(pub, owner)[tid];
+            prow[tid] = v;
+            if (rank == owner && p != lc)
+                rows_sm[(int64_t)(p - r0) * ROW_PITCH + tid] = cluster.map_shared_rank(kpub, 0)[tid];
+            if (rank == 0) rows_sm[(int64_t)lc * ROW_PITCH + tid] = v;
+        }
         if (rank == 0 && tid == 0)
         {
             if (ipiv) ipiv[c0 + lc] = c0 + p + 1;
-            if (*info == 0 && czero(prow[lc])) *info = c0 + lc + 1;
+            if (info_now == 0 && czero(prow[lc]))
+            {
+                info_now = c0 + lc + 1;
+                *info = info_now;
+            }
         }
+        __syncthreads();
         if (valid && g > lc)
         {
             const float2 d = prow[lc];
