@@ -165,11 +165,11 @@ __global__ void __launch_bounds__(PANEL_THREADS) cgetrf_panel_kernel(float2 *A, 
 // Row-per-thread panel: rows [c0, m) x columns [c0, c0 + w) (w <= 32), each thread of a
 // cluster of `cl` blocks owning one panel row (block r: panel rows [rR, rR + R), R <= ROW_MAX,
 // so the diagonal rows live in block 0), kept in the thread's own shared-memory row (pitch 33:
-// a warp's rows fall in distinct banks).  Per column: the block's pivot candidate (warp
-// shuffles, one barrier); cluster barrier; all candidates read through distributed shared
-// memory; the pivot row's owner publishes it and block 0's row-lc thread publishes row lc;
-// cluster barrier; every block copies the pivot row locally, the two owners take each other's
-// row, and every thread below the diagonal divides its l and updates its row.  The column loop
+// a warp's rows fall in distinct banks).  Per column: each block's pivot candidate (warp
+// shuffles, one barrier) published with its row, block 0 also publishing row lc; one cluster
+// barrier; every block reads all candidates and the winner's row through distributed shared
+// memory, the two owners take each other's row, and every thread below the diagonal divides
+// its l and updates its row.  The column loop
 // stays rolled (an unrolled one overflows the instruction cache).  Same per-element
 // arithmetic as the single-block kernel.
 constexpr int ROW_MAX = 512;
@@ -182,9 +182,11 @@ __global__ void __launch_bounds__(ROW_MAX, 1) cgetrf_row_panel_kernel(float2 *A,
     extern __shared__ float2 rows_sm[];  // blockDim.x rows x ROW_PITCH
     __shared__ uint32_t red_score[ROW_MAX / 32];
     __shared__ int red_row[ROW_MAX / 32];
-    __shared__ uint32_t cand_score;
-    __shared__ int cand_row, pivot_row;
-    __shared__ float2 pub[PANEL], kpub[PANEL], prow[PANEL];
+    // published per column, double-buffered by column parity: a block rewrites a buffer only
+    // after every block has passed the next column's cluster barrier, i.e. finished reading it
+    __shared__ uint32_t cand_score[2];
+    __shared__ int cand_row[2];
+    __shared__ float2 pub[2][PANEL], kpub[2][PANEL], prow[PANEL];
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank(), cl = (int)cluster.num_blocks();
     const int H = m - c0, r0 = rank * R, tid = threadIdx.x;
@@ -196,6 +198,7 @@ __global__ void __launch_bounds__(ROW_MAX, 1) cgetrf_row_panel_kernel(float2 *A,
 #pragma unroll 1
     for (int lc = 0; lc < w; ++lc)
     {
+        const int buf = lc & 1;
         uint32_t best = 0;
         int row = H;
         if (ipiv && valid && g >= lc)
@@ -221,6 +224,7 @@ __global__ void __launch_bounds__(ROW_MAX, 1) cgetrf_row_panel_kernel(float2 *A,
         __syncthreads();
         if (tid < 32)
         {
+            // the block's candidate, then its row (and block 0's row lc) published by this warp
             const int warps = blockDim.x >> 5;
             best = tid < warps ? red_score[tid] : 0u;
             row = tid < warps ? red_row[tid] : H;
@@ -234,10 +238,17 @@ __global__ void __launch_bounds__(ROW_MAX, 1) cgetrf_row_panel_kernel(float2 *A,
                     row = orow;
                 }
             }
+            best = __shfl_sync(0xffffffffu, best, 0);
+            row = __shfl_sync(0xffffffffu, row, 0);
             if (tid == 0)
             {
-                cand_score = best;
-                cand_row = row;
+                cand_score[buf] = best;
+                cand_row[buf] = row;
+            }
+            if (tid < w)
+            {
+                if (row < H) pub[buf][tid] = rows_sm[(int64_t)(row - r0) * ROW_PITCH + tid];
+                if (rank == 0) kpub[buf][tid] = rows_sm[(int64_t)lc * ROW_PITCH + tid];
             }
         }
         cluster.sync();
@@ -247,8 +258,8 @@ __global__ void __launch_bounds__(ROW_MAX, 1) cgetrf_row_panel_kernel(float2 *A,
             int p = H;
             if (tid < cl)
             {
-                b = *cluster.map_shared_rank(&cand_score, tid);
-                p = *cluster.map_shared_rank(&cand_row, tid);
+                b = cluster.map_shared_rank(cand_score, tid)[buf];
+                p = cluster.map_shared_rank(cand_row, tid)[buf];
             }
             for (int off = 16; off > 0; off >>= 1)
             {
@@ -260,32 +271,27 @@ __global__ void __launch_bounds__(ROW_MAX, 1) cgetrf_row_panel_kernel(float2 *A,
                     p = orow;
                 }
             }
-            if (tid == 0) pivot_row = ipiv ? p : lc;
-        }
-        __syncthreads();
-        const int p = pivot_row, owner = p / R;
-        // the first warp copies whole rows, one column per lane
-        if (tid < w)
-        {
-            if (rank == owner) pub[tid] = rows_sm[(int64_t)(p - r0) * ROW_PITCH + tid];
-            if (rank == 0) kpub[tid] = rows_sm[(int64_t)lc * ROW_PITCH + tid];
-        }
-        cluster.sync();
-        if (tid < w)
-        {
-            const float2 v = cluster.map_shared_rank(pub, owner)[tid];
-            prow[tid] = v;
-            if (rank == owner && p != lc)
-                rows_sm[(int64_t)(p - r0) * ROW_PITCH + tid] = cluster.map_shared_rank(kpub, 0)[tid];
-            if (rank == 0) rows_sm[(int64_t)lc * ROW_PITCH + tid] = v;
-        }
-        if (rank == 0 && tid == 0)
-        {
-            if (ipiv) ipiv[c0 + lc] = c0 + p + 1;
-            if (info_now == 0 && czero(prow[lc]))
+            p = ipiv ? __shfl_sync(0xffffffffu, p, 0) : lc;
+            const int owner = p / R;
+            if (tid < w)
             {
-                info_now = c0 + lc + 1;
-                *info = info_now;
+                // without pivoting the pivot row is row lc, which block 0 published as kpub
+                const float2 v = ipiv ? cluster.map_shared_rank(&pub[0][0], owner)[buf * PANEL + tid]
+                                      : cluster.map_shared_rank(&kpub[0][0], 0)[buf * PANEL + tid];
+                prow[tid] = v;
+                if (rank == owner && p != lc)
+                    rows_sm[(int64_t)(p - r0) * ROW_PITCH + tid] = cluster.map_shared_rank(&kpub[0][0], 0)[buf * PANEL + tid];
+                if (rank == 0) rows_sm[(int64_t)lc * ROW_PITCH + tid] = v;
+            }
+            __syncwarp();
+            if (rank == 0 && tid == 0)
+            {
+                if (ipiv) ipiv[c0 + lc] = c0 + p + 1;
+                if (info_now == 0 && czero(prow[lc]))
+                {
+                    info_now = c0 + lc + 1;
+                    *info = info_now;
+                }
             }
         }
         __syncthreads();
@@ -367,14 +373,16 @@ __global__ void __launch_bounds__(TRSM_THREADS) ctrsm_block_kernel(const float2 
 __global__ void __launch_bounds__(256) claswp_panel_kernel(float2 *A, int64_t lda, int ncols, int k0, int w,
                                                            const int *ipiv, int skip0, int skip1)
 {
-    __shared__ int row_of[2 * PANEL], src_of[2 * PANEL], count;
+    __shared__ int row_of[2 * PANEL], src_of[2 * PANEL], piv_sm[PANEL], count;
+    if (threadIdx.x < w) piv_sm[threadIdx.x] = __ldg(ipiv + k0 + threadIdx.x) - 1;  // one parallel load
+    __syncthreads();
     if (threadIdx.x == 0)
     {
         int cnt = w;
         for (int i = 0; i < w; ++i) row_of[i] = src_of[i] = k0 + i;
         for (int k = 0; k < w; ++k)
         {
-            const int p = __ldg(ipiv + k0 + k) - 1;
+            const int p = piv_sm[k];
             int ip = -1;
             if (p >= k0 && p < k0 + w)
                 ip = p - k0;
