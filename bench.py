@@ -449,6 +449,7 @@ def run_b200(args, rank, world):
         cpu = cpu_baseline_headline(args, a_cm, b_cm, x64)
         large = measure_large(handle, args) if args.large else None
         complex_lu = measure_complex_lu(handle, args) if args.complex_lu else None
+        qr = measure_qr(handle, args) if args.complex_lu else None
         by_kappa = {}
         for k, kappa in enumerate(KAPPAS):
             idx = list(range(k, COUNT, len(KAPPAS)))
@@ -537,6 +538,7 @@ def run_b200(args, rank, world):
             "configs": configs,
             "large": large,
             "complex_lu": complex_lu,
+            "qr": qr,
         }
         print(json.dumps(line), flush=True)
     handle.close()
@@ -1132,6 +1134,80 @@ def measure_complex_lu(handle, args, steps=3):
     return out
 
 
+def measure_qr(handle, args, steps=3):
+    """The real QR family: aclsolverSgeqrf of one 4096 x 4096 and one 2048 x 2048 N(0,1)
+    matrix, and aclsolverSSgels of a 4096 x 4096 system with one right-hand side (device time
+    per call, inputs restored before each).  `case_list_us` is the time the reference's own
+    case lists carry for the same shape (test/sgeqrf/data/sgeqrf_cases.txt,
+    test/sgels/data/sgels_cases.txt, a cuSOLVER run on the hardware those lists were made on)."""
+    import ctypes as C
+
+    import torch
+
+    import aclsolver
+
+    lib = aclsolver.library()
+    stream = handle.stream
+    fp32 = fp32_peak_tflops()
+
+    def timed(call, restore):
+        times = []
+        for _ in range(steps + 1):
+            restore()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            call()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        return sorted(times[1:])[len(times[1:]) // 2]
+
+    out = {}
+    g = torch.Generator(device="cuda").manual_seed(11)
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    for n, listed in ((4096, 25449.6), (2048, 8781.9)):
+        a0 = torch.randn(n * n, device="cuda", generator=g)
+        a = torch.empty_like(a0)
+        tau = torch.empty(n, device="cuda")
+        work = torch.empty(1024, device="cuda")
+        ms = timed(lambda: aclsolver.check(lib.aclsolverSgeqrf(handle.value, n, n, a.data_ptr(), n, tau.data_ptr(),
+                                                                work.data_ptr(), 1024, info.data_ptr())),
+                   lambda: a.copy_(a0))
+        assert int(info.item()) == 0
+        flops = 4.0 * n ** 3 / 3
+        out[f"sgeqrf_{n}"] = {"workload": f"one {n} x {n} N(0,1) matrix: aclsolverSgeqrf", "ms": round(ms, 3),
+                              "gflops": round(flops / (ms * 1e-3) / 1e9, 1),
+                              "roofline": {"bound": "fp32 FMA (CUDA cores)", "frac": round(flops / ms / 1e9 / fp32, 4),
+                                           "peak_tflops": fp32},
+                              "case_list_us": listed}
+        if n == 4096 and args is not None and args.cpu_seconds > 0:
+            from scipy.linalg import lapack
+
+            a_h = a0.cpu().numpy().reshape(n, n)
+            t0 = time.perf_counter()
+            lapack.sgeqrf(a_h)
+            out[f"sgeqrf_{n}"]["cpu_baseline"] = {"ms": round((time.perf_counter() - t0) * 1e3, 1),
+                                                  "kind": "scipy LAPACK sgeqrf (OpenBLAS threads)"}
+    n = 4096
+    a0 = torch.randn(n * n, device="cuda", generator=g)
+    a = torch.empty_like(a0)
+    b = torch.randn(n, device="cuda", generator=g)
+    x = torch.empty(n, device="cuda")
+    lw = C.c_size_t(0)
+    aclsolver.check(lib.aclsolverSSgels_bufferSize(handle.value, n, n, 1, a.data_ptr(), n, b.data_ptr(), n,
+                                                   x.data_ptr(), n, None, C.byref(lw)))
+    work = torch.empty(lw.value // 4 + 1, device="cuda")
+    niter = C.c_int(0)
+    ms = timed(lambda: aclsolver.check(lib.aclsolverSSgels(handle.value, n, n, 1, a.data_ptr(), n, b.data_ptr(), n,
+                                                           x.data_ptr(), n, work.data_ptr(), lw.value,
+                                                           C.byref(niter), info.data_ptr())),
+               lambda: a.copy_(a0))
+    out["sgels_4096"] = {"workload": "4096 x 4096 system, 1 right-hand side: aclsolverSSgels", "ms": round(ms, 3),
+                         "case_list_us": 30675.3}
+    return out
+
+
 def run_profile_complex():
     """Each complex LU workload once, for an ncu capture: Cgetrf of one 4096 x 4096 matrix
     (the reference recipe), CgetriBatched of 10,000 order-64 LU factors, CmatinvBatched of
@@ -1355,7 +1431,7 @@ def main():
     ap.add_argument("--no-configs", dest="configs", action="store_false",
                     help="skip the plain batched workloads reported under the 'configs' key")
     ap.add_argument("--no-complex-lu", dest="complex_lu", action="store_false",
-                    help="skip the complex LU family workloads reported under the 'complex_lu' key")
+                    help="skip the complex LU and QR workloads reported under the 'complex_lu' and 'qr' keys")
     ap.add_argument("--profile-complex", action="store_true",
                     help="run each complex LU workload once (for an ncu capture) and exit")
     ap.add_argument("--profile-large", action="store_true",

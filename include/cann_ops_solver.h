@@ -172,6 +172,46 @@ extern "C"
                              aclFloatComplex *A, const int64_t lda, int32_t *ipiv, aclFloatComplex *B,
                              const int64_t ldb, int32_t *info);
 
+    /* ---- real QR family; reference include/cann_ops_solver.h:566-861 --------------------- */
+
+    /* Lwork (floats) for Sgeqrf: 0 for an empty problem, else one 32 x 32 block factor;
+     * m <= 8192 (NOT_SUPPORTED above); replaces cann_ops_solver.h:566 (sgeqrf_host.cpp:173). */
+    aclsolverStatus_t aclsolverSgeqrf_bufferSize(aclsolverHandle_t handle, int m, int n, float *A, int lda, int *Lwork);
+    /* Householder QR in place (LAPACK sign convention): R on and above the diagonal, the
+     * reflectors below it, TAU[min(m, n)]; devInfo 0 or -i (1 m, 2 n, 3 A, 4 lda, 5 TAU,
+     * 6 Workspace, 7 Lwork); replaces cann_ops_solver.h:598 (sgeqrf_host.cpp:204). */
+    aclsolverStatus_t aclsolverSgeqrf(aclsolverHandle_t handle, int m, int n, float *A, int lda, float *TAU,
+                                      float *Workspace, int Lwork, int *devInfo);
+    /* lwork (floats) for Sorgqr: m * k + 1024; m <= 4096; replaces cann_ops_solver.h:619
+     * (sorgqr_host.cpp:142). */
+    aclsolverStatus_t aclsolverSorgqr_bufferSize(aclsolverHandle_t handle, int m, int n, int k, const float *A,
+                                                 int lda, const float *tau, int *lwork);
+    /* The first n columns of Q = H(1) ... H(k), overwriting A; replaces cann_ops_solver.h:645
+     * (sorgqr_host.cpp:181). */
+    aclsolverStatus_t aclsolverSorgqr(aclsolverHandle_t handle, int m, int n, int k, float *A, int lda,
+                                      const float *tau, float *work, int lwork, int *devInfo);
+    /* lwork (floats) for Sormqr: one 32 x 32 block factor; nq <= 4096; replaces
+     * cann_ops_solver.h:675 (sormqr_host.cpp:149). */
+    aclsolverStatus_t aclsolverSormqr_bufferSize(aclsolverHandle_t handle, aclsolverSideMode_t side,
+                                                 aclsolverOperation_t trans, int m, int n, int k, const float *A,
+                                                 int lda, const float *tau, const float *C, int ldc, int *lwork);
+    /* op(Q) C (LEFT) or C op(Q) (RIGHT), OP_T / OP_C apply Q^T; replaces cann_ops_solver.h:708
+     * (sormqr_host.cpp:254). */
+    aclsolverStatus_t aclsolverSormqr(aclsolverHandle_t handle, aclsolverSideMode_t side, aclsolverOperation_t trans,
+                                      int m, int n, int k, const float *A, int lda, const float *tau, float *C,
+                                      int ldc, float *work, int lwork, int *devInfo);
+    /* Bytes for SSgels: tau, Q^T B and one block factor; m >= n, m, n <= 4096, nrhs <= 128;
+     * replaces cann_ops_solver.h:815 (sgels_host.cpp:149). */
+    aclsolverStatus_t aclsolverSSgels_bufferSize(aclsolverHandle_t handle, int m, int n, int nrhs, float *dA, int ldda,
+                                                 float *dB, int lddb, float *dX, int lddx, void *dwork,
+                                                 size_t *lwork_bytes);
+    /* Least squares by QR: X = R^-1 (Q^T B)(1:n, :); dA overwritten, dB read only, dX must
+     * overlap neither; *niter = 0; a zero diagonal of R propagates Inf/NaN (not reported);
+     * replaces cann_ops_solver.h:859 (sgels_host.cpp:285). */
+    aclsolverStatus_t aclsolverSSgels(aclsolverHandle_t handle, int m, int n, int nrhs, float *dA, int ldda, float *dB,
+                                      int lddb, float *dX, int lddx, void *dWorkspace, size_t lwork_bytes, int *niter,
+                                      int *dinfo);
+
 #ifdef __cplusplus
 }
 #endif

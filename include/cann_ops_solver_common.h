@@ -79,6 +79,13 @@ extern "C"
         ACLSOLVER_OP_C = 2
     } aclsolverOperation_t;
 
+    /* Side from which an orthogonal factor is applied (reference cann_ops_solver_common.h:93-98). */
+    typedef enum
+    {
+        ACLSOLVER_SIDE_LEFT = 0,
+        ACLSOLVER_SIDE_RIGHT = 1
+    } aclsolverSideMode_t;
+
 #ifdef __cplusplus
 }
 #endif

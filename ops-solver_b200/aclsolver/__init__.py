@@ -77,6 +77,14 @@ ARGTYPES = {
     "aclsolverCgetriBatched": [VP, I32, VP, I32, VP, VP, I32, VP, I32],
     "aclsolverCmatinvBatched": [VP, I32, VP, I32, VP, I32, VP, I32],
     "aclsolverCgetrs": [VP, U64, I64, I64, VP, I64, VP, VP, I64, VP],
+    "aclsolverSgeqrf_bufferSize": [VP, I32, I32, VP, I32, C.POINTER(I32)],
+    "aclsolverSgeqrf": [VP, I32, I32, VP, I32, VP, VP, I32, VP],
+    "aclsolverSorgqr_bufferSize": [VP, I32, I32, I32, VP, I32, VP, C.POINTER(I32)],
+    "aclsolverSorgqr": [VP, I32, I32, I32, VP, I32, VP, VP, I32, VP],
+    "aclsolverSormqr_bufferSize": [VP, I32, I32, I32, I32, I32, VP, I32, VP, VP, I32, C.POINTER(I32)],
+    "aclsolverSormqr": [VP, I32, I32, I32, I32, I32, VP, I32, VP, VP, I32, VP, I32, VP],
+    "aclsolverSSgels_bufferSize": [VP, I32, I32, I32, VP, I32, VP, I32, VP, I32, VP, C.POINTER(C.c_size_t)],
+    "aclsolverSSgels": [VP, I32, I32, I32, VP, I32, VP, I32, VP, I32, VP, C.c_size_t, C.POINTER(I32), VP],
     # additions of this build
     "aclsolverSetDeviceChecks": [VP, I32],
     "aclsolverGetDeviceChecks": [VP, C.POINTER(I32)],

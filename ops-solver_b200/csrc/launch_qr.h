@@ -1,0 +1,24 @@
+// launch_qr.h -- launchers of the real QR family (qr.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace ops_solver
+{
+constexpr int QR_BLOCK = 32;                    // reflectors per panel / block factor
+constexpr int QR_T_FLOATS = QR_BLOCK * QR_BLOCK;  // one block factor T
+// In-place Householder QR of one m x n matrix; tau gets min(m, n) scalars; T holds one
+// 32 x 32 block factor (QR_T_FLOATS floats of workspace).
+cudaError_t launch_sgeqrf(float *A, int lda, int m, int n, float *tau, float *T, cudaStream_t stream);
+// op(Q) C (side 0) or C op(Q) (side 1), trans 0 = Q, else Q^T; Q from k reflectors of A.
+cudaError_t launch_sormqr(int side, int trans, int m, int n, int k, const float *A, int lda, const float *tau,
+                          float *C, int ldc, float *T, cudaStream_t stream);
+// The first n columns of Q from k reflectors, overwriting A; work holds m * k + QR_T_FLOATS floats.
+cudaError_t launch_sorgqr(int m, int n, int k, float *A, int lda, const float *tau, float *work, cudaStream_t stream);
+// Least squares (m >= n): A overwritten by its QR, B read only, X = n x nrhs solution;
+// work holds sgels_work_floats(m, n, nrhs) floats.
+size_t sgels_work_floats(int m, int n, int nrhs);
+cudaError_t launch_sgels(int m, int n, int nrhs, float *A, int lda, const float *B, int ldb, float *X, int ldx,
+                         float *work, cudaStream_t stream);
+}  // namespace ops_solver

@@ -1,0 +1,367 @@
+// qr.cu -- the real QR family: Householder factorisation (Sgeqrf), application of Q or Q^T
+// from either side (Sormqr), explicit Q (Sorgqr) and least squares (SSgels).
+//
+// Reflectors follow LAPACK's convention, as the reference's CPU golden does
+// (src/sgeqrf/kernel/householder.hpp:55-141, Larfg): beta = -sign(alpha) ||x||,
+// tau = (beta - alpha) / beta, v = x2 / (alpha - beta), tau = 0 for an all-zero x2.  The
+// schedule is this build's: 32-column panels, the slarft block factor T, and block
+// application C -= V op(T) (V^T C).  Every reduction over rows is a "lane sum": row r feeds
+// lane r mod 32 (an FMA chain in ascending row order), and a warp butterfly
+// (v += shfl_xor(v, off), off = 16 .. 1) combines the lanes, so the results do not depend
+// on the grid and the CPU oracle restates them exactly:
+//   qr_panel_kernel      one block factors a panel: warp 0 forms the reflector, the other
+//                        warps apply it to one panel column each
+//   qr_larft_kernel      T of the panel (forward, columnwise)
+//   qr_apply_kernel      one warp per column (left) or row (right) of C: W = V^T c by lane
+//                        sums over 32-row chunks of V staged in shared memory, W2 = op(T) W,
+//                        then c -= V W2 with an FMA chain over the reflectors
+//   qr_trsv_kernel       R X = Y, one block per right-hand side, backward sweep
+#include <algorithm>
+
+#include "common.cuh"
+#include "launch_qr.h"
+
+namespace ops_solver
+{
+namespace
+{
+constexpr int NB = 32;
+constexpr int PANEL_THREADS = 1024;
+constexpr int APPLY_WARPS = 8;
+
+__device__ __forceinline__ float lane_fold(float p)
+{
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) p = add_rn(p, __shfl_xor_sync(0xffffffffu, p, off));
+    return p;
+}
+
+// Panel columns [k, k + kb) of rows [k, m), in place in A (L2-resident).
+__global__ void __launch_bounds__(PANEL_THREADS) qr_panel_kernel(float *A, int lda, int m, int k, int kb, float *tau)
+{
+    __shared__ float s_tau, s_scale;
+    __shared__ int s_apply;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int c = k; c < k + kb; ++c)
+    {
+        float *col = A + (int64_t)c * lda;
+        if (warp == 0)
+        {
+            float p = 0.0f;
+            for (int base = (c + 1) & ~31; base < m; base += 32)
+            {
+                const int row = base + lane;
+                if (row > c && row < m)
+                {
+                    const float x = col[row];
+                    p = fma_rn(x, x, p);
+                }
+            }
+            const float sumsq = lane_fold(p);
+            if (lane == 0)
+            {
+                float t = 0.0f, scale = 0.0f;
+                int apply = 0;
+                if (m - c > 1 && sumsq != 0.0f)
+                {
+                    const float alpha = col[c];
+                    const float norm = sqrt_rn(add_rn(mul_rn(alpha, alpha), sumsq));
+                    const float beta = alpha >= 0.0f ? -norm : norm;
+                    t = div_rn(sub_rn(beta, alpha), beta);
+                    scale = div_rn(1.0f, sub_rn(alpha, beta));
+                    col[c] = beta;
+                    apply = 1;
+                }
+                tau[c] = t;
+                s_tau = t;
+                s_scale = scale;
+                s_apply = apply;
+            }
+        }
+        __syncthreads();
+        const bool apply = s_apply != 0;
+        const float t = s_tau;
+        if (apply)
+        {
+            const float scale = s_scale;
+            for (int row = c + 1 + tid; row < m; row += PANEL_THREADS) col[row] = mul_rn(col[row], scale);
+        }
+        __syncthreads();
+        const int j = c + warp;
+        if (apply && warp >= 1 && j < k + kb)
+        {
+            float *cj = A + (int64_t)j * lda;
+            float p = 0.0f;
+            for (int base = c & ~31; base < m; base += 32)
+            {
+                const int row = base + lane;
+                if (row >= c && row < m) p = fma_rn(row == c ? 1.0f : col[row], cj[row], p);
+            }
+            const float w = mul_rn(t, lane_fold(p));
+            for (int base = c & ~31; base < m; base += 32)
+            {
+                const int row = base + lane;
+                if (row >= c && row < m) cj[row] = fma_rn(-w, row == c ? 1.0f : col[row], cj[row]);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// T (kb x kb upper, column-major, ld NB) of the reflectors at columns [k, k + kb), length nq.
+__global__ void __launch_bounds__(PANEL_THREADS) qr_larft_kernel(const float *A, int lda, int nq, int k, int kb,
+                                                                 const float *tau, float *T)
+{
+    __shared__ float d[NB][NB];   // d[i][r] = -tau_i (v_r . v_i)
+    __shared__ float ts[NB][NB];  // ts[i][r] = T(r, i)
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int pairs = kb * (kb - 1) / 2;
+    for (int pr = warp; pr < pairs; pr += PANEL_THREADS / 32)
+    {
+        int i = 1, rem = pr;
+        while (rem >= i)
+        {
+            rem -= i;
+            ++i;
+        }
+        const int r = rem;
+        const float *vr = A + (int64_t)(k + r) * lda, *vi = A + (int64_t)(k + i) * lda;
+        float p = 0.0f;
+        for (int base = (k + i) & ~31; base < nq; base += 32)
+        {
+            const int row = base + lane;
+            if (row >= k + i && row < nq) p = fma_rn(vr[row], row == k + i ? 1.0f : vi[row], p);
+        }
+        const float dot = lane_fold(p);
+        if (lane == 0) d[i][r] = mul_rn(-tau[k + i], dot);
+    }
+    __syncthreads();
+    for (int i = 0; i < kb; ++i)
+    {
+        const float ti = tau[k + i];
+        if (tid <= i)
+        {
+            if (ti == 0.0f)
+                ts[i][tid] = 0.0f;
+            else if (tid == i)
+                ts[i][i] = ti;
+            else
+            {
+                float acc = 0.0f;
+                for (int q = tid; q < i; ++q) acc = fma_rn(ts[q][tid], d[i][q], acc);
+                ts[i][tid] = acc;
+            }
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < kb * kb; idx += PANEL_THREADS)
+    {
+        const int r = idx % kb, i = idx / kb;
+        if (r <= i) T[i * NB + r] = ts[i][r];
+    }
+}
+
+// C = C - V op(T) (V^T C) (LEFT: one warp per column of C, reflector index = C's row) or
+// C = C - (C V) op(T) V^T (RIGHT: one warp per row of C, reflector index = C's column).
+// LOWER_CHAIN: W2[i] = sum_{q <= i} T(q, i) W[q] (op(T) = T^T for LEFT, T for RIGHT);
+// otherwise W2[i] = sum_{q >= i} T(i, q) W[q].
+template <bool RIGHT, bool LOWER_CHAIN>
+__global__ void __launch_bounds__(APPLY_WARPS * 32) qr_apply_kernel(const float *V, int ldv, int nq, int k, int kb,
+                                                                    const float *T, float *C, int64_t ldc, int count)
+{
+    __shared__ float vs[32][NB + 1];
+    __shared__ float ts[NB * NB];
+    __shared__ float w2s[APPLY_WARPS][NB];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int j = blockIdx.x * APPLY_WARPS + warp;  // column (LEFT) or row (RIGHT) of C
+    const bool live = j < count;
+    for (int idx = tid; idx < NB * NB; idx += APPLY_WARPS * 32) ts[idx] = T[idx];
+    float p[NB];
+#pragma unroll
+    for (int i = 0; i < NB; ++i) p[i] = 0.0f;
+    const int first = k & ~31;
+    for (int base = first; base < nq; base += 32)
+    {
+        __syncthreads();
+        for (int idx = tid; idx < 32 * kb; idx += APPLY_WARPS * 32)
+        {
+            const int rr = idx & 31, i = idx >> 5, row = base + rr;
+            vs[rr][i] = row < nq && row > k + i ? V[(int64_t)(k + i) * ldv + row] : (row == k + i ? 1.0f : 0.0f);
+        }
+        __syncthreads();
+        const int row = base + lane;
+        if (live && row >= k && row < nq)
+        {
+            const float c = RIGHT ? C[(int64_t)row * ldc + j] : C[(int64_t)j * ldc + row];
+#pragma unroll
+            for (int i = 0; i < NB; ++i)
+                if (i < kb && row >= k + i) p[i] = fma_rn(vs[lane][i], c, p[i]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NB; ++i) p[i] = lane_fold(p[i]);
+    {
+        float acc = 0.0f;
+#pragma unroll
+        for (int q = 0; q < NB; ++q)
+        {
+            if (LOWER_CHAIN)
+            {
+                if (q <= lane && lane < kb) acc = fma_rn(ts[lane * NB + q], p[q], acc);
+            }
+            else
+            {
+                if (q >= lane && q < kb) acc = fma_rn(ts[q * NB + lane], p[q], acc);
+            }
+        }
+        w2s[warp][lane] = acc;
+    }
+    __syncwarp();
+    for (int base = first; base < nq; base += 32)
+    {
+        __syncthreads();
+        for (int idx = tid; idx < 32 * kb; idx += APPLY_WARPS * 32)
+        {
+            const int rr = idx & 31, i = idx >> 5, row = base + rr;
+            vs[rr][i] = row < nq && row > k + i ? V[(int64_t)(k + i) * ldv + row] : (row == k + i ? 1.0f : 0.0f);
+        }
+        __syncthreads();
+        const int row = base + lane;
+        if (live && row >= k && row < nq)
+        {
+            float *cp = RIGHT ? C + (int64_t)row * ldc + j : C + (int64_t)j * ldc + row;
+            float c = *cp;
+#pragma unroll
+            for (int i = 0; i < NB; ++i)
+                if (i < kb && i <= row - k) c = fma_rn(-vs[lane][i], w2s[warp][i], c);
+            *cp = c;
+        }
+    }
+}
+
+// R X = Y for one right-hand side per block: x_p = x_p / R_pp, then x_i -= R_ip x_p, p descending.
+__global__ void __launch_bounds__(1024) qr_trsv_kernel(const float *R, int ldr, int n, const float *Y, int ldy,
+                                                       float *X, int ldx)
+{
+    extern __shared__ float xs[];
+    const int j = blockIdx.x, tid = threadIdx.x;
+    for (int i = tid; i < n; i += blockDim.x) xs[i] = Y[(int64_t)j * ldy + i];
+    __syncthreads();
+    for (int p = n - 1; p >= 0; --p)
+    {
+        const float *rp = R + (int64_t)p * ldr;
+        if (tid == 0) xs[p] = div_rn(xs[p], rp[p]);
+        __syncthreads();
+        const float xp = xs[p];
+        for (int i = tid; i < p; i += blockDim.x) xs[i] = fma_rn(-rp[i], xp, xs[i]);
+        __syncthreads();
+    }
+    for (int i = tid; i < n; i += blockDim.x) X[(int64_t)j * ldx + i] = xs[i];
+}
+
+__global__ void qr_identity_kernel(float *A, int lda, int m, int n)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)m * n) return;
+    const int r = (int)(idx % m), c = (int)(idx / m);
+    A[(int64_t)c * lda + r] = r == c ? 1.0f : 0.0f;
+}
+
+cudaError_t apply_block(bool right, bool lower_chain, const float *V, int ldv, int nq, int k, int kb, const float *T,
+                        float *C, int64_t ldc, int count, cudaStream_t stream)
+{
+    if (count <= 0) return cudaSuccess;
+    const unsigned grid = (unsigned)((count + APPLY_WARPS - 1) / APPLY_WARPS);
+    if (right && lower_chain)
+        qr_apply_kernel<true, true><<<grid, APPLY_WARPS * 32, 0, stream>>>(V, ldv, nq, k, kb, T, C, ldc, count);
+    else if (right)
+        qr_apply_kernel<true, false><<<grid, APPLY_WARPS * 32, 0, stream>>>(V, ldv, nq, k, kb, T, C, ldc, count);
+    else if (lower_chain)
+        qr_apply_kernel<false, true><<<grid, APPLY_WARPS * 32, 0, stream>>>(V, ldv, nq, k, kb, T, C, ldc, count);
+    else
+        qr_apply_kernel<false, false><<<grid, APPLY_WARPS * 32, 0, stream>>>(V, ldv, nq, k, kb, T, C, ldc, count);
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_sgeqrf(float *A, int lda, int m, int n, float *tau, float *T, cudaStream_t stream)
+{
+    const int lim = std::min(m, n);
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < lim && e == cudaSuccess; k += NB)
+    {
+        const int kb = std::min(NB, lim - k);
+        qr_panel_kernel<<<1, PANEL_THREADS, 0, stream>>>(A, lda, m, k, kb, tau);
+        e = cudaGetLastError();
+        if (e == cudaSuccess && k + kb < n)
+        {
+            qr_larft_kernel<<<1, PANEL_THREADS, 0, stream>>>(A, lda, m, k, kb, tau, T);
+            e = cudaGetLastError();
+            if (e == cudaSuccess)
+                e = apply_block(false, true, A, lda, m, k, kb, T, A + (int64_t)(k + kb) * lda, lda, n - k - kb,
+                                stream);
+        }
+    }
+    return e;
+}
+
+cudaError_t launch_sormqr(int side, int trans, int m, int n, int k, const float *A, int lda, const float *tau,
+                          float *C, int ldc, float *T, cudaStream_t stream)
+{
+    const bool right = side != 0, tr = trans != 0;
+    const int nq = right ? n : m, count = right ? m : n;
+    const int npan = (k + NB - 1) / NB;
+    const bool forward = !right == tr;  // Q^T from the left and Q from the right take H(1) first
+    cudaError_t e = cudaSuccess;
+    for (int s = 0; s < npan && e == cudaSuccess; ++s)
+    {
+        const int pi = forward ? s : npan - 1 - s;
+        const int k0 = pi * NB, kb = std::min(NB, k - k0);
+        qr_larft_kernel<<<1, PANEL_THREADS, 0, stream>>>(A, lda, nq, k0, kb, tau, T);
+        e = cudaGetLastError();
+        // op(T) = T^T (lower chain) for Q^T from the left and for Q from the right
+        if (e == cudaSuccess) e = apply_block(right, right ? !tr : tr, A, lda, nq, k0, kb, T, C, ldc, count, stream);
+    }
+    return e;
+}
+
+cudaError_t launch_sorgqr(int m, int n, int k, float *A, int lda, const float *tau, float *work, cudaStream_t stream)
+{
+    float *v = work, *T = work + (size_t)m * k;
+    cudaError_t e = cudaSuccess;
+    if (k > 0)
+        e = cudaMemcpy2DAsync(v, (size_t)m * sizeof(float), A, (size_t)lda * sizeof(float), (size_t)m * sizeof(float),
+                              k, cudaMemcpyDeviceToDevice, stream);
+    if (e == cudaSuccess)
+    {
+        const int64_t total = (int64_t)m * n;
+        qr_identity_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(A, lda, m, n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && k > 0) e = launch_sormqr(0, 0, m, n, k, v, m, tau, A, lda, T, stream);
+    return e;
+}
+
+size_t sgels_work_floats(int m, int n, int nrhs)
+{
+    auto up = [](size_t x) { return (x + 63) & ~size_t(63); };
+    return up((size_t)std::max(n, 1)) + up((size_t)m * nrhs) + up(NB * NB);
+}
+
+cudaError_t launch_sgels(int m, int n, int nrhs, float *A, int lda, const float *B, int ldb, float *X, int ldx,
+                         float *work, cudaStream_t stream)
+{
+    auto up = [](size_t x) { return (x + 63) & ~size_t(63); };
+    float *tau = work, *Y = tau + up((size_t)std::max(n, 1)), *T = Y + up((size_t)m * nrhs);
+    cudaError_t e = cudaMemcpy2DAsync(Y, (size_t)m * sizeof(float), B, (size_t)ldb * sizeof(float),
+                                      (size_t)m * sizeof(float), nrhs, cudaMemcpyDeviceToDevice, stream);
+    if (e == cudaSuccess) e = launch_sgeqrf(A, lda, m, n, tau, T, stream);
+    if (e == cudaSuccess) e = launch_sormqr(0, 1, m, nrhs, n, A, lda, tau, Y, m, T, stream);
+    if (e == cudaSuccess)
+    {
+        qr_trsv_kernel<<<nrhs, 1024, (size_t)n * sizeof(float), stream>>>(A, lda, n, Y, m, X, ldx);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+}  // namespace ops_solver

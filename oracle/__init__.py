@@ -44,6 +44,11 @@ def lib():
         _lib.orc_cmatinv_batched.argtypes = [_i, _F, _i, _l, _F, _i, _l, _i, _I, _i]
         _lib.orc_cgetrs_batched.argtypes = [_i, _i, _i, _F, _i, _l, _VP, _F, _i, _l, _i, _i]
         _lib.orc_cdivide_many.argtypes = [_F, _F, _F, _l]
+        _lib.orc_sgeqrf.argtypes = [_i, _i, _F, _i, _F]
+        _lib.orc_sgeqr2_golden.argtypes = [_i, _i, _F, _i, _F]
+        _lib.orc_sormqr.argtypes = [_i, _i, _i, _i, _i, _F, _i, _F, _F, _i]
+        _lib.orc_sorgqr.argtypes = [_i, _i, _i, _F, _i, _F]
+        _lib.orc_sgels.argtypes = [_i, _i, _i, _F, _i, _F, _i, _F, _i, _F]
         _lib.orc_max_threads.restype = _i
     return _lib
 
@@ -202,3 +207,69 @@ def cdivide(a, b):
     out = np.zeros_like(a)
     lib().orc_cdivide_many(a.view(np.float32), b.view(np.float32), out.view(np.float32), a.size)
     return out
+
+
+def _cm(a):
+    """2-D column-major float32 copy (as a flat C-contiguous array of the transpose)."""
+    a = np.asarray(a, dtype=np.float32)
+    return np.array(a.T, dtype=np.float32, order="C", copy=True).reshape(-1)
+
+
+def _uncm(flat, rows, cols):
+    return np.ascontiguousarray(flat.reshape(cols, rows).T)
+
+
+def sgeqrf(a):
+    """Blocked Householder QR of one (m, n) matrix; returns (R and V packed, tau)."""
+    m, n = a.shape
+    f = _cm(a)
+    tau = np.zeros(max(1, min(m, n)), dtype=np.float32)
+    lib().orc_sgeqrf(m, n, f, max(1, m), tau)
+    return _uncm(f, m, n), tau[: min(m, n)]
+
+
+def sgeqr2_golden(a):
+    """The reference's unblocked CPU golden QR (sequential sums)."""
+    m, n = a.shape
+    f = _cm(a)
+    tau = np.zeros(max(1, min(m, n)), dtype=np.float32)
+    lib().orc_sgeqr2_golden(m, n, f, max(1, m), tau)
+    return _uncm(f, m, n), tau[: min(m, n)]
+
+
+def sormqr(side, trans, qr, tau, c):
+    """op(Q) C (side 0) or C op(Q) (side 1) from packed reflectors; trans 0 = Q."""
+    m, n = c.shape
+    nq = qr.shape[0]
+    k = len(tau)
+    fa = _cm(qr)
+    fc = _cm(c)
+    t = np.ascontiguousarray(tau, dtype=np.float32)
+    if t.size == 0:
+        t = np.zeros(1, dtype=np.float32)
+    lib().orc_sormqr(int(side), int(trans), m, n, k, fa, max(1, nq), t, fc, max(1, m))
+    return _uncm(fc, m, n)
+
+
+def sorgqr(qr, tau, n):
+    """The first n columns of Q from packed reflectors (k = len(tau))."""
+    m = qr.shape[0]
+    k = len(tau)
+    f = _cm(qr[:, :n] if qr.shape[1] >= n else np.pad(qr, ((0, 0), (0, n - qr.shape[1]))))
+    t = np.ascontiguousarray(tau, dtype=np.float32)
+    if t.size == 0:
+        t = np.zeros(1, dtype=np.float32)
+    lib().orc_sorgqr(m, n, k, f, max(1, m), t)
+    return _uncm(f, m, n)
+
+
+def sgels(a, b):
+    """Least squares min ||A X - B|| (m >= n); returns (X, packed QR, tau)."""
+    m, n = a.shape
+    nrhs = b.shape[1]
+    fa = _cm(a)
+    fb = _cm(b)
+    x = np.zeros(max(1, n) * max(1, nrhs), dtype=np.float32)
+    tau = np.zeros(max(1, n), dtype=np.float32)
+    lib().orc_sgels(m, n, nrhs, fa, max(1, m), fb, max(1, m), x, max(1, n), tau)
+    return _uncm(x, max(1, n), max(1, nrhs))[:n, :nrhs], _uncm(fa, m, n), tau[:n]

@@ -13,6 +13,9 @@
   cgetrf_gate                        test/cgetrf/data/verify_result.py:60-110
       |(P A)_ij - (L U)_ij| / |(P A)_ij| <= 1e-3 on all but 1e-4 of the entries, all finite.
   complex_solve_compare_ok           test/utils/lu_verify_utils.py:262-290 on complex values.
+  qr_ratio                           test/sgeqrf/sgeqrf_test.cpp:16,44-97 (SQRT01 residual)
+      ||R - Q^T A||_1 / (m ||A||_1 eps), Q formed in FP64 from the reflectors.
+  gels_ok                            test/sgels/sgels_test.cpp:16-24 (SQRT16 / SQRT17)
   inverse_golden_ok                  test/cgetri_batched/data/verify_result.py:28-79
       isclose(out, numpy inverse, rtol = atol = 5e-3) on all but 1e-4 of the entries.
 """
@@ -237,3 +240,53 @@ def inverse_golden_ok(out, golden):
     golden = np.asarray(golden).reshape(-1)
     miss = ~np.isclose(out, golden, rtol=5e-3, atol=5e-3, equal_nan=True)
     return bool(miss.sum() / golden.size <= 1e-4)
+
+
+def q_from_reflectors(qr, tau):
+    """Q (m x m, FP64) = H(1) ... H(k) from LAPACK-style packed reflectors."""
+    qr = np.asarray(qr, dtype=np.float64)
+    m = qr.shape[0]
+    q = np.eye(m)
+    for i in reversed(range(len(tau))):
+        v = np.zeros(m)
+        v[i] = 1.0
+        v[i + 1:] = qr[i + 1:, i]
+        q -= float(tau[i]) * np.outer(v, v @ q)
+    return q
+
+
+def qr_ratio(a, qr, tau):
+    """SQRT01: ||R - Q^T A||_1 / (m ||A||_1 eps), the reference's Sgeqrf residual."""
+    a = np.asarray(a, dtype=np.float64)
+    m, n = a.shape
+    r = np.triu(np.asarray(qr, dtype=np.float64))
+    q = q_from_reflectors(qr, tau)
+    diff = np.abs(r - q.T @ a).sum(axis=0).max()
+    anorm = np.abs(a).sum(axis=0).max()
+    return float(diff / (m * anorm * EPS)) if anorm > 0 else 0.0
+
+
+def gels_ratio(a, b, x):
+    """SQRT16 for square systems (max_j ||b_j - A x_j||_1 / (max(m,n) ||A||_1 ||x_j||_1 eps)),
+    SQRT17 for overdetermined ones (||R^T A||_1 / (||A||_1 ||B||_1 max(m, n, nrhs) eps))."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    x = np.asarray(x, dtype=np.float64)
+    m, n = a.shape
+    anorm = np.abs(a).sum(axis=0).max()
+    res = b - a @ x
+    if m == n:
+        num = np.abs(res).sum(axis=0)
+        den = max(m, n) * anorm * np.abs(x).sum(axis=0) * EPS
+        return float(np.max(num / den))
+    rta = res.T @ a
+    return float(np.abs(rta).sum(axis=0).max() / (anorm * np.abs(b).sum(axis=0).max() * max(m, n, b.shape[1]) * EPS))
+
+
+def gels_ok(a, b, x, x_cpu):
+    """The reference's SSgels acceptance: square <= max(5 cpu, 0.015), overdetermined <= 10 cpu."""
+    m, n = np.asarray(a).shape
+    r, c = gels_ratio(a, b, x), gels_ratio(a, b, x_cpu)
+    if not np.isfinite(r):
+        return False
+    return r <= (max(5 * c, 0.015) if m == n else 10 * c)

@@ -1350,3 +1350,298 @@ void orc_cgetrs_batched(int trans, int n, int nrhs, const float *lu, int lda, in
         orc_cgetrs(trans, n, nrhs, lu + 2 * (int64_t)q * astride, lda, ipiv ? ipiv + (int64_t)q * n : NULL,
                    b + 2 * (int64_t)q * bstride, ldb);
 }
+
+/* ---------------------------------------------------------------------------------------
+ * Real QR family (Householder, column-major)
+ *
+ * The reference's CPU golden for its QR tests is QrCore::Larfg / Geqr2 / Larft
+ * (src/sgeqrf/kernel/householder.hpp:55-200): LAPACK's sign convention (beta = -sign(alpha)
+ * ||x||, tau = (beta - alpha) / beta, v = x2 / (alpha - beta), tau = 0 when x2 is zero).
+ * Its device kernels hand the trailing products to the Cube unit, whose summation order is
+ * not in its sources, so these routines state this build's blocked order, which the CUDA
+ * kernels follow bit for bit:
+ *   - every reduction over rows is a "lane sum": row r feeds partial r mod 32 (an FMA
+ *     chain in ascending row order per partial), then the 32 partials are combined by a
+ *     butterfly, p[l] = p[l] + p[l ^ off] for off = 16, 8, 4, 2, 1;
+ *   - panels of 32 columns: Larfg per column, the reflector applied to the rest of the
+ *     panel (w = tau * (v . a), a -= w v by FMA), the block factor T of slarft (forward,
+ *     columnwise), then the trailing columns C -= V (T^T (V^T C)) with each W2 entry an FMA
+ *     chain over T in ascending order and each C entry an FMA chain over the reflectors in
+ *     ascending order;
+ *   - orc_sgels: geqrf, Q^T B by the same block application, then R X = (Q^T B)(1:n) by a
+ *     backward sweep (IEEE division, FMA updates in descending pivot order).
+ * Outside the magnitude window 5e-20 < max|A| < 1.8e19 the squares overflow or underflow, as
+ * in the reference kernels (no rescaling pass).
+ * ------------------------------------------------------------------------------------- */
+
+#define QR_NB 32
+#define RAT(a, lda, r, c) ((a)[(int64_t)(c) * (lda) + (r)])
+
+static float qr_lane_fold(float *p)
+{
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        float q[32];
+        for (int l = 0; l < 32; ++l) q[l] = p[l] + p[l ^ off];
+        memcpy(p, q, sizeof q);
+    }
+    return p[0];
+}
+
+/* Reflector i of a panel starting at column k: v(row) = 1 at row k+i, A(row, k+i) below. */
+static inline float qr_v(const float *a, int lda, int k, int i, int row)
+{
+    return row == k + i ? 1.0f : RAT(a, lda, row, k + i);
+}
+
+static void qr_larfg(int m, float *a, int lda, int c, float *tau)
+{
+    *tau = 0.0f;
+    if (m - c <= 1) return;
+    float p[32] = {0};
+    for (int row = c + 1; row < m; ++row)
+    {
+        float x = RAT(a, lda, row, c);
+        p[row & 31] = fmaf(x, x, p[row & 31]);
+    }
+    float sumsq = qr_lane_fold(p);
+    if (sumsq == 0.0f) return;
+    float alpha = RAT(a, lda, c, c);
+    float norm = sqrtf(alpha * alpha + sumsq);
+    float beta = alpha >= 0.0f ? -norm : norm;
+    *tau = (beta - alpha) / beta;
+    float scale = 1.0f / (alpha - beta);
+    for (int row = c + 1; row < m; ++row) RAT(a, lda, row, c) = RAT(a, lda, row, c) * scale;
+    RAT(a, lda, c, c) = beta;
+}
+
+/* Factor panel columns [k, k+kb) of rows [k, m). */
+static void qr_panel(int m, int k, int kb, float *a, int lda, float *tau)
+{
+    for (int c = k; c < k + kb; ++c)
+    {
+        qr_larfg(m, a, lda, c, &tau[c]);
+        const float t = tau[c];
+        if (t == 0.0f) continue;
+        for (int j = c + 1; j < k + kb; ++j)
+        {
+            float p[32] = {0};
+            for (int row = c; row < m; ++row)
+            {
+                float v = row == c ? 1.0f : RAT(a, lda, row, c);
+                p[row & 31] = fmaf(v, RAT(a, lda, row, j), p[row & 31]);
+            }
+            float w = t * qr_lane_fold(p);
+            for (int row = c; row < m; ++row)
+            {
+                float v = row == c ? 1.0f : RAT(a, lda, row, c);
+                RAT(a, lda, row, j) = fmaf(-w, v, RAT(a, lda, row, j));
+            }
+        }
+    }
+}
+
+/* T (kb x kb, upper, ld 32) of the panel's reflectors (slarft, forward, columnwise). */
+static void qr_larft(int m, int k, int kb, const float *a, int lda, const float *tau, float *T)
+{
+    float d[QR_NB];
+    for (int i = 0; i < kb; ++i)
+    {
+        const float ti = tau[k + i];
+        if (ti == 0.0f)
+        {
+            for (int r = 0; r <= i; ++r) T[i * QR_NB + r] = 0.0f;
+            continue;
+        }
+        for (int r = 0; r < i; ++r)
+        {
+            float p[32] = {0};
+            for (int row = k + i; row < m; ++row)
+                p[row & 31] = fmaf(RAT(a, lda, row, k + r), qr_v(a, lda, k, i, row), p[row & 31]);
+            d[r] = (-ti) * qr_lane_fold(p);
+        }
+        for (int r = 0; r < i; ++r)
+        {
+            float acc = 0.0f;
+            for (int q = r; q < i; ++q) acc = fmaf(T[q * QR_NB + r], d[q], acc);
+            T[i * QR_NB + r] = acc;
+        }
+        T[i * QR_NB + i] = ti;
+    }
+}
+
+/* Columns [0, ncols) of C (rows [k, m), ld ldc): C = (I - V op(T) V^T) C with op(T) = T^T when
+ * tr, else T.  V = the panel at columns [k, k+kb) of a. */
+static void qr_apply_left(int m, int k, int kb, const float *a, int lda, const float *T, int tr, float *c,
+                          int ldc, int ncols)
+{
+    for (int j = 0; j < ncols; ++j)
+    {
+        float w[QR_NB], w2[QR_NB];
+        for (int i = 0; i < kb; ++i)
+        {
+            float p[32] = {0};
+            for (int row = k + i; row < m; ++row)
+                p[row & 31] = fmaf(qr_v(a, lda, k, i, row), RAT(c, ldc, row, j), p[row & 31]);
+            w[i] = qr_lane_fold(p);
+        }
+        for (int i = 0; i < kb; ++i)
+        {
+            float acc = 0.0f;
+            if (tr)
+                for (int q = 0; q <= i; ++q) acc = fmaf(T[i * QR_NB + q], w[q], acc);
+            else
+                for (int q = i; q < kb; ++q) acc = fmaf(T[q * QR_NB + i], w[q], acc);
+            w2[i] = acc;
+        }
+        for (int row = k; row < m; ++row)
+        {
+            float x = RAT(c, ldc, row, j);
+            for (int i = 0; i < kb && i <= row - k; ++i) x = fmaf(-qr_v(a, lda, k, i, row), w2[i], x);
+            RAT(c, ldc, row, j) = x;
+        }
+    }
+}
+
+/* Rows [0, nrows) of C (columns [k, nq), ld ldc): C = C (I - V op(T) V^T), op(T) = T when
+ * !tr (C Q), T^T when tr (C Q^T). */
+static void qr_apply_right(int nq, int k, int kb, const float *a, int lda, const float *T, int tr, float *c,
+                           int ldc, int nrows)
+{
+    for (int r = 0; r < nrows; ++r)
+    {
+        float y[QR_NB], y2[QR_NB];
+        for (int i = 0; i < kb; ++i)
+        {
+            float p[32] = {0};
+            for (int col = k + i; col < nq; ++col)
+                p[col & 31] = fmaf(qr_v(a, lda, k, i, col), RAT(c, ldc, r, col), p[col & 31]);
+            y[i] = qr_lane_fold(p);
+        }
+        for (int i = 0; i < kb; ++i)
+        {
+            float acc = 0.0f;
+            if (!tr)
+                for (int q = 0; q <= i; ++q) acc = fmaf(T[i * QR_NB + q], y[q], acc);
+            else
+                for (int q = i; q < kb; ++q) acc = fmaf(T[q * QR_NB + i], y[q], acc);
+            y2[i] = acc;
+        }
+        for (int col = k; col < nq; ++col)
+        {
+            float x = RAT(c, ldc, r, col);
+            for (int i = 0; i < kb && i <= col - k; ++i) x = fmaf(-qr_v(a, lda, k, i, col), y2[i], x);
+            RAT(c, ldc, r, col) = x;
+        }
+    }
+}
+
+void orc_sgeqrf(int m, int n, float *a, int lda, float *tau)
+{
+    const int lim = m < n ? m : n;
+    float T[QR_NB * QR_NB];
+    for (int k = 0; k < lim; k += QR_NB)
+    {
+        const int kb = lim - k < QR_NB ? lim - k : QR_NB;
+        qr_panel(m, k, kb, a, lda, tau);
+        if (k + kb < n)
+        {
+            qr_larft(m, k, kb, a, lda, tau, T);
+            qr_apply_left(m, k, kb, a, lda, T, 1, a + (int64_t)(k + kb) * lda, lda, n - k - kb);
+        }
+    }
+}
+
+/* side 0 left (C is m x n, nq = m), 1 right (nq = n); trans 0 applies Q, else Q^T. */
+void orc_sormqr(int side, int trans, int m, int n, int k, const float *a, int lda, const float *tau, float *c,
+                int ldc)
+{
+    const int nq = side == 0 ? m : n;
+    float T[QR_NB * QR_NB];
+    const int npan = (k + QR_NB - 1) / QR_NB;
+    /* forward panel order for Q^T from the left and Q from the right */
+    const int forward = (side == 0) == (trans != 0);
+    for (int s = 0; s < npan; ++s)
+    {
+        const int pi = forward ? s : npan - 1 - s;
+        const int k0 = pi * QR_NB, kb = k - k0 < QR_NB ? k - k0 : QR_NB;
+        qr_larft(nq, k0, kb, a, lda, tau, T);
+        if (side == 0)
+            qr_apply_left(m, k0, kb, a, lda, T, trans != 0, c, ldc, n);
+        else
+            qr_apply_right(n, k0, kb, a, lda, T, trans != 0, c, ldc, m);
+    }
+}
+
+/* Q (m x n) from k reflectors in a, overwriting a (the reflectors are copied first). */
+void orc_sorgqr(int m, int n, int k, float *a, int lda, const float *tau)
+{
+    float *v = (float *)malloc(sizeof(float) * (size_t)(m > 0 ? m : 1) * (size_t)(k > 0 ? k : 1));
+    for (int j = 0; j < k; ++j)
+        for (int r = 0; r < m; ++r) v[(int64_t)j * m + r] = RAT(a, lda, r, j);
+    for (int j = 0; j < n; ++j)
+        for (int r = 0; r < m; ++r) RAT(a, lda, r, j) = r == j ? 1.0f : 0.0f;
+    orc_sormqr(0, 0, m, n, k, v, m, tau, a, lda);
+    free(v);
+}
+
+/* Least squares, m >= n: X (n x nrhs) from the QR of a (overwritten) and B (read only). */
+void orc_sgels(int m, int n, int nrhs, float *a, int lda, const float *b, int ldb, float *x, int ldx, float *tau)
+{
+    float *y = (float *)malloc(sizeof(float) * (size_t)(m > 0 ? m : 1) * (size_t)(nrhs > 0 ? nrhs : 1));
+    for (int j = 0; j < nrhs; ++j)
+        for (int r = 0; r < m; ++r) y[(int64_t)j * m + r] = RAT(b, ldb, r, j);
+    orc_sgeqrf(m, n, a, lda, tau);
+    orc_sormqr(0, 1, m, nrhs, n, a, lda, tau, y, m);
+    for (int j = 0; j < nrhs; ++j)
+    {
+        float *yj = y + (int64_t)j * m;
+        for (int p = n - 1; p >= 0; --p)
+        {
+            yj[p] = yj[p] / RAT(a, lda, p, p);
+            for (int i = 0; i < p; ++i) yj[i] = fmaf(-RAT(a, lda, i, p), yj[p], yj[i]);
+        }
+        for (int r = 0; r < n; ++r) RAT(x, ldx, r, j) = yj[r];
+    }
+    free(y);
+}
+
+/* The reference's CPU golden (QrCore::Geqr2, householder.hpp:144-170, with Larfg :55-141 on
+ * its normal path): unblocked, sequential sums.  Used to pin the judges' CPU ratios. */
+void orc_sgeqr2_golden(int m, int n, float *a, int lda, float *tau)
+{
+    const int kmax = m < n ? m : n;
+    for (int j = 0; j < kmax; ++j)
+    {
+        const int len = m - j;
+        tau[j] = 0.0f;
+        if (len > 1)
+        {
+            float sumsq = 0.0f;
+            for (int i = j + 1; i < m; ++i) sumsq += RAT(a, lda, i, j) * RAT(a, lda, i, j);
+            if (sumsq != 0.0f)
+            {
+                const float al = RAT(a, lda, j, j);
+                const float norm = sqrtf(al * al + sumsq);
+                const float beta = al >= 0.0f ? -norm : norm;
+                tau[j] = (beta - al) / beta;
+                const float scale = 1.0f / (al - beta);
+                for (int i = j + 1; i < m; ++i) RAT(a, lda, i, j) *= scale;
+                RAT(a, lda, j, j) = beta;
+            }
+        }
+        if (tau[j] != 0.0f && j + 1 < n)
+        {
+            const float beta = RAT(a, lda, j, j);
+            RAT(a, lda, j, j) = 1.0f;
+            for (int c = j + 1; c < n; ++c)
+            {
+                float dot = 0.0f;
+                for (int r = j; r < m; ++r) dot += RAT(a, lda, r, j) * RAT(a, lda, r, c);
+                const float w = tau[j] * dot;
+                for (int r = j; r < m; ++r) RAT(a, lda, r, c) -= w * RAT(a, lda, r, j);
+            }
+            RAT(a, lda, j, j) = beta;
+        }
+    }
+}

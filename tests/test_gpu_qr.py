@@ -1,0 +1,169 @@
+"""The real QR family on the GPU through the C ABI: Sgeqrf, Sormqr (both sides, all
+operations), Sorgqr and SSgels, each bit for bit the oracle's blocked restatement
+(orc_sgeqrf / orc_sormqr / orc_sorgqr / orc_sgels), with the reference's acceptance gates
+(test/sgeqrf/sgeqrf_test.cpp:16, test/sgels/sgels_test.cpp:16-24) on top."""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+import aclsolver
+import oracle
+from oracle import judges
+from helpers import DeviceMatrices, info_buffer, same_bits
+
+pytestmark = pytest.mark.gpu
+
+LEFT, RIGHT = 0, 1
+OP_N, OP_T, OP_C = 0, 1, 2
+
+
+def rand(m, n, seed):
+    return np.random.default_rng(seed).standard_normal((m, n)).astype(np.float32)
+
+
+def work(floats):
+    return torch.full((max(1, floats),), float("nan"), dtype=torch.float32, device="cuda")
+
+
+def geqrf(handle, a, pad=0):
+    lib = aclsolver.library()
+    m, n = a.shape
+    dm = DeviceMatrices(a, m + pad)
+    tau = torch.full((max(1, min(m, n)),), float("nan"), dtype=torch.float32, device="cuda")
+    lw = C.c_int(-1)
+    assert lib.aclsolverSgeqrf_bufferSize(handle.value, m, n, dm.ptr, dm.ld, C.byref(lw)) == aclsolver.SUCCESS
+    w = work(lw.value)
+    info = info_buffer(1)
+    st = lib.aclsolverSgeqrf(handle.value, m, n, dm.ptr, dm.ld, tau.data_ptr(), w.data_ptr(), lw.value,
+                             info.data_ptr())
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 0
+    return dm.read()[0], tau.cpu().numpy()[: min(m, n)]
+
+
+@pytest.mark.parametrize("m,n", [(1, 1), (2, 2), (18, 8), (32, 4), (57, 57), (66, 8), (100, 33), (33, 100),
+                                 (300, 257), (257, 300), (1000, 200), (4096, 64), (1024, 1024)])
+def test_sgeqrf_matches_oracle(handle, m, n):
+    a = rand(m, n, m * 13 + n)
+    got, tau = geqrf(handle, a, pad=3)
+    want, wtau = oracle.sgeqrf(a)
+    assert same_bits(tau, wtau)
+    assert same_bits(got, want)
+
+
+def test_sgeqrf_zero_columns_and_the_reference_gate(handle):
+    a = rand(200, 150, 5)
+    a[:, 7] = 0.0
+    a[120:, 40] = 0.0
+    got, tau = geqrf(handle, a)
+    want, wtau = oracle.sgeqrf(a)
+    assert same_bits(got, want) and same_bits(tau, wtau)
+    g, gtau = oracle.sgeqr2_golden(a)
+    assert judges.qr_ratio(a, got, tau) <= max(5 * judges.qr_ratio(a, g, gtau), 0.1)
+
+
+def sormqr(handle, side, trans, qr, tau, c, pad=2):
+    lib = aclsolver.library()
+    m, n = c.shape
+    k = len(tau)
+    nq = qr.shape[0]
+    da = DeviceMatrices(qr, nq + 1)
+    dc = DeviceMatrices(c, m + pad)
+    dt = torch.tensor(np.ascontiguousarray(tau), device="cuda")
+    lw = C.c_int(-1)
+    assert lib.aclsolverSormqr_bufferSize(handle.value, side, trans, m, n, k, da.ptr, da.ld, dt.data_ptr(), dc.ptr,
+                                          dc.ld, C.byref(lw)) == aclsolver.SUCCESS
+    w = work(lw.value)
+    info = info_buffer(1)
+    st = lib.aclsolverSormqr(handle.value, side, trans, m, n, k, da.ptr, da.ld, dt.data_ptr(), dc.ptr, dc.ld,
+                             w.data_ptr(), lw.value, info.data_ptr())
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 0
+    return dc.read()[0]
+
+
+@pytest.mark.parametrize("side", [LEFT, RIGHT])
+@pytest.mark.parametrize("trans", [OP_N, OP_T, OP_C])
+@pytest.mark.parametrize("nq,k,other", [(70, 70, 9), (300, 100, 33), (64, 40, 1)])
+def test_sormqr_matches_oracle(handle, side, trans, nq, k, other):
+    a = rand(nq, k, nq + k)
+    qr, tau = oracle.sgeqrf(a)
+    c = rand(nq, other, 3) if side == LEFT else rand(other, nq, 3)
+    got = sormqr(handle, side, trans, qr, tau, c)
+    assert same_bits(got, oracle.sormqr(side, int(trans != OP_N), qr, tau, c))
+
+
+@pytest.mark.parametrize("m,n,k", [(100, 80, 60), (64, 64, 64), (50, 20, 0), (300, 300, 257)])
+def test_sorgqr_matches_oracle(handle, m, n, k):
+    lib = aclsolver.library()
+    a = rand(m, max(k, 1), m + n + k)
+    qr, tau = oracle.sgeqrf(a)
+    tau = tau[:k]
+    src = np.zeros((m, n), dtype=np.float32)
+    src[:, :k] = qr[:, :k]
+    dm = DeviceMatrices(src, m + 2)
+    dt = torch.tensor(np.ascontiguousarray(tau) if k else np.zeros(1, np.float32), device="cuda")
+    lw = C.c_int(-1)
+    assert lib.aclsolverSorgqr_bufferSize(handle.value, m, n, k, dm.ptr, dm.ld, dt.data_ptr(),
+                                          C.byref(lw)) == aclsolver.SUCCESS
+    w = work(lw.value)
+    info = info_buffer(1)
+    st = lib.aclsolverSorgqr(handle.value, m, n, k, dm.ptr, dm.ld, dt.data_ptr(), w.data_ptr(), lw.value,
+                             info.data_ptr())
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 0
+    got = dm.read()[0]
+    assert same_bits(got, oracle.sorgqr(src, tau, n))
+    assert np.abs(got.T.astype(np.float64) @ got - np.eye(n)).max() < 1e-4
+
+
+@pytest.mark.parametrize("m,n,nrhs", [(20, 20, 3), (64, 64, 1), (300, 70, 8), (1000, 500, 16), (257, 256, 128)])
+def test_sgels_matches_oracle_and_passes_the_gate(handle, m, n, nrhs):
+    lib = aclsolver.library()
+    a = rand(m, n, m * 3 + n)
+    b = rand(m, nrhs, nrhs + 1)
+    da = DeviceMatrices(a, m + 1)
+    db = DeviceMatrices(b, m + 2)
+    dx = DeviceMatrices(np.zeros((n, nrhs), np.float32), n + 3)
+    lw = C.c_size_t(0)
+    assert lib.aclsolverSSgels_bufferSize(handle.value, m, n, nrhs, da.ptr, da.ld, db.ptr, db.ld, dx.ptr, dx.ld,
+                                          None, C.byref(lw)) == aclsolver.SUCCESS
+    w = torch.zeros(lw.value // 4 + 1, dtype=torch.float32, device="cuda")
+    niter = C.c_int(-5)
+    info = info_buffer(1)
+    st = lib.aclsolverSSgels(handle.value, m, n, nrhs, da.ptr, da.ld, db.ptr, db.ld, dx.ptr, dx.ld, w.data_ptr(),
+                             lw.value, C.byref(niter), info.data_ptr())
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 0 and niter.value == 0
+    assert db.unchanged(), "B is read only"
+    x = dx.read()[0]
+    wx, wqr, _ = oracle.sgels(a.copy(), b)
+    assert same_bits(x, wx)
+    assert same_bits(da.read()[0], wqr)
+    g, gtau = oracle.sgeqr2_golden(a)
+    y = oracle.sormqr(0, 1, g, gtau, b)
+    xc = np.linalg.solve(np.triu(g[:n, :n]).astype(np.float64), y[:n].astype(np.float64)).astype(np.float32)
+    assert judges.gels_ok(a, b, x, xc)
+
+
+def test_argument_errors_write_info(handle):
+    lib = aclsolver.library()
+    info = info_buffer(1)
+    st = lib.aclsolverSgeqrf(handle.value, 10, 4, None, 9, None, None, 0, info.data_ptr())
+    handle.stream.synchronize()
+    assert st == 3 and int(info.cpu()[0]) == -4
+    st = lib.aclsolverSgeqrf(handle.value, 0, 4, None, 1, None, None, 0, info.data_ptr())
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS and int(info.cpu()[0]) == 0
+    a = DeviceMatrices(rand(8, 8, 1), 8)
+    st = lib.aclsolverSormqr(handle.value, 0, 1, 8, 8, 9, a.ptr, 8, a.ptr, a.ptr, 8, a.ptr, 1024, info.data_ptr())
+    handle.stream.synchronize()
+    assert st == 3 and int(info.cpu()[0]) == -5
+    niter = C.c_int(7)
+    st = lib.aclsolverSSgels(handle.value, 4, 5, 1, a.ptr, 8, a.ptr, 8, a.ptr, 8, a.ptr, 4096, C.byref(niter),
+                             info.data_ptr())
+    handle.stream.synchronize()
+    assert st == 3 and int(info.cpu()[0]) == -1 and niter.value == 0
