@@ -1208,6 +1208,41 @@ def measure_qr(handle, args, steps=3):
     return out
 
 
+def run_profile_qr():
+    """aclsolverSgeqrf of one 4096 x 4096 N(0,1) matrix and aclsolverSSgels of a 2048 x 2048
+    system with 4 right-hand sides, once each, for an ncu capture."""
+    import ctypes as C
+
+    import torch
+
+    import aclsolver
+
+    lib = aclsolver.library()
+    handle = aclsolver.Handle()
+    g = torch.Generator(device="cuda").manual_seed(11)
+    n = 4096
+    a = torch.randn(n * n, device="cuda", generator=g)
+    tau = torch.empty(n, device="cuda")
+    work = torch.empty(1024, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    aclsolver.check(lib.aclsolverSgeqrf(handle.value, n, n, a.data_ptr(), n, tau.data_ptr(), work.data_ptr(), 1024,
+                                        info.data_ptr()))
+    n, r = 2048, 4
+    a = torch.randn(n * n, device="cuda", generator=g)
+    b = torch.randn(n * r, device="cuda", generator=g)
+    x = torch.empty(n * r, device="cuda")
+    lw = C.c_size_t(0)
+    aclsolver.check(lib.aclsolverSSgels_bufferSize(handle.value, n, n, r, a.data_ptr(), n, b.data_ptr(), n,
+                                                   x.data_ptr(), n, None, C.byref(lw)))
+    ws = torch.empty(lw.value // 4 + 1, device="cuda")
+    niter = C.c_int(0)
+    aclsolver.check(lib.aclsolverSSgels(handle.value, n, n, r, a.data_ptr(), n, b.data_ptr(), n, x.data_ptr(), n,
+                                        ws.data_ptr(), lw.value, C.byref(niter), info.data_ptr()))
+    torch.cuda.synchronize()
+    handle.close()
+    print("profile-qr done", flush=True)
+
+
 def run_profile_complex():
     """Each complex LU workload once, for an ncu capture: Cgetrf of one 4096 x 4096 matrix
     (the reference recipe), CgetriBatched of 10,000 order-64 LU factors, CmatinvBatched of
@@ -1432,6 +1467,8 @@ def main():
                     help="skip the plain batched workloads reported under the 'configs' key")
     ap.add_argument("--no-complex-lu", dest="complex_lu", action="store_false",
                     help="skip the complex LU and QR workloads reported under the 'complex_lu' and 'qr' keys")
+    ap.add_argument("--profile-qr", action="store_true",
+                    help="run Sgeqrf 4096 and SSgels 2048 once (for an ncu capture) and exit")
     ap.add_argument("--profile-complex", action="store_true",
                     help="run each complex LU workload once (for an ncu capture) and exit")
     ap.add_argument("--profile-large", action="store_true",
@@ -1457,6 +1494,8 @@ def main():
             run_profile()
         elif args.profile_small:
             run_profile_small(args)
+        elif args.profile_qr:
+            run_profile_qr()
         elif args.profile_complex:
             run_profile_complex()
         elif args.profile_large:

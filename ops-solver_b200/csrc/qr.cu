@@ -9,16 +9,18 @@
 // lane r mod 32 (an FMA chain in ascending row order), and a warp butterfly
 // (v += shfl_xor(v, off), off = 16 .. 1) combines the lanes, so the results do not depend
 // on the grid and the CPU oracle restates them exactly:
-//   qr_panel_kernel      one block factors a panel: warp 0 forms the reflector, the other
-//                        warps apply it to one panel column each
+//   qr_panel_kernel      one block factors a panel (in shared memory when it fits): warp 0
+//                        forms the reflector, the other warps apply it to one column each
 //   qr_larft_kernel      T of the panel (forward, columnwise)
 //   qr_apply_kernel      one warp per column (left) or row (right) of C: W = V^T c by lane
 //                        sums over 32-row chunks of V staged in shared memory, W2 = op(T) W,
 //                        then c -= V W2 with an FMA chain over the reflectors
 //   qr_trsv_kernel       R X = Y, one block per right-hand side, backward sweep
 #include <algorithm>
+#include <atomic>
 
 #include "common.cuh"
+#include "device_once.h"
 #include "launch_qr.h"
 
 namespace ops_solver
@@ -27,7 +29,7 @@ namespace
 {
 constexpr int NB = 32;
 constexpr int PANEL_THREADS = 1024;
-constexpr int APPLY_WARPS = 8;
+constexpr int APPLY_WARPS = 16;
 
 __device__ __forceinline__ float lane_fold(float p)
 {
@@ -36,25 +38,47 @@ __device__ __forceinline__ float lane_fold(float p)
     return p;
 }
 
-// Panel columns [k, k + kb) of rows [k, m), in place in A (L2-resident).
+// Panel columns [k, k + kb) of rows [k, m).  SMEM: the panel is staged in shared memory
+// (pitch m - k); otherwise it stays in A (L2-resident) and each lane batches four loads
+// ahead of its FMA chain.  Same arithmetic either way.
+constexpr int PANEL_SMEM_FLOATS = 50 * 1024;
+
+template <bool SMEM>
 __global__ void __launch_bounds__(PANEL_THREADS) qr_panel_kernel(float *A, int lda, int m, int k, int kb, float *tau)
 {
+    extern __shared__ float sp[];
     __shared__ float s_tau, s_scale;
     __shared__ int s_apply;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int H = m - k;
+    auto at = [&](int j, int row) -> float & {
+        return SMEM ? sp[(int64_t)(j - k) * H + (row - k)] : A[(int64_t)j * lda + row];
+    };
+    if (SMEM)
+    {
+        for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) sp[idx] = A[(int64_t)(k + idx / H) * lda + k + idx % H];
+        __syncthreads();
+    }
+    constexpr int U = 8;
     for (int c = k; c < k + kb; ++c)
     {
-        float *col = A + (int64_t)c * lda;
         if (warp == 0)
         {
             float p = 0.0f;
-            for (int base = (c + 1) & ~31; base < m; base += 32)
+            for (int base = (c + 1) & ~31; base < m; base += 32 * U)
             {
-                const int row = base + lane;
-                if (row > c && row < m)
+                float x[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u)
                 {
-                    const float x = col[row];
-                    p = fma_rn(x, x, p);
+                    const int row = base + 32 * u + lane;
+                    x[u] = row > c && row < m ? at(c, row) : 0.0f;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                {
+                    const int row = base + 32 * u + lane;
+                    if (row > c && row < m) p = fma_rn(x[u], x[u], p);
                 }
             }
             const float sumsq = lane_fold(p);
@@ -64,12 +88,12 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_panel_kernel(float *A, int l
                 int apply = 0;
                 if (m - c > 1 && sumsq != 0.0f)
                 {
-                    const float alpha = col[c];
+                    const float alpha = at(c, c);
                     const float norm = sqrt_rn(add_rn(mul_rn(alpha, alpha), sumsq));
                     const float beta = alpha >= 0.0f ? -norm : norm;
                     t = div_rn(sub_rn(beta, alpha), beta);
                     scale = div_rn(1.0f, sub_rn(alpha, beta));
-                    col[c] = beta;
+                    at(c, c) = beta;
                     apply = 1;
                 }
                 tau[c] = t;
@@ -84,56 +108,112 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_panel_kernel(float *A, int l
         if (apply)
         {
             const float scale = s_scale;
-            for (int row = c + 1 + tid; row < m; row += PANEL_THREADS) col[row] = mul_rn(col[row], scale);
+            for (int row = c + 1 + tid; row < m; row += PANEL_THREADS) at(c, row) = mul_rn(at(c, row), scale);
         }
         __syncthreads();
         const int j = c + warp;
         if (apply && warp >= 1 && j < k + kb)
         {
-            float *cj = A + (int64_t)j * lda;
             float p = 0.0f;
-            for (int base = c & ~31; base < m; base += 32)
+            for (int base = c & ~31; base < m; base += 32 * U)
             {
-                const int row = base + lane;
-                if (row >= c && row < m) p = fma_rn(row == c ? 1.0f : col[row], cj[row], p);
+                float v[U], x[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                {
+                    const int row = base + 32 * u + lane;
+                    const bool ok = row >= c && row < m;
+                    v[u] = ok ? (row == c ? 1.0f : at(c, row)) : 0.0f;
+                    x[u] = ok ? at(j, row) : 0.0f;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                {
+                    const int row = base + 32 * u + lane;
+                    if (row >= c && row < m) p = fma_rn(v[u], x[u], p);
+                }
             }
             const float w = mul_rn(t, lane_fold(p));
-            for (int base = c & ~31; base < m; base += 32)
+            for (int base = c & ~31; base < m; base += 32 * U)
             {
-                const int row = base + lane;
-                if (row >= c && row < m) cj[row] = fma_rn(-w, row == c ? 1.0f : col[row], cj[row]);
+                float v[U], x[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                {
+                    const int row = base + 32 * u + lane;
+                    const bool ok = row >= c && row < m;
+                    v[u] = ok ? (row == c ? 1.0f : at(c, row)) : 0.0f;
+                    x[u] = ok ? at(j, row) : 0.0f;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                {
+                    const int row = base + 32 * u + lane;
+                    if (row >= c && row < m) at(j, row) = fma_rn(-w, v[u], x[u]);
+                }
             }
         }
         __syncthreads();
     }
+    if (SMEM)
+        for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) A[(int64_t)(k + idx / H) * lda + k + idx % H] = sp[idx];
 }
 
 // T (kb x kb upper, column-major, ld NB) of the reflectors at columns [k, k + kb), length nq.
+// The reflector Gram products are lane sums over 32-row chunks of V staged in shared
+// memory; warp w owns the pairs w, w + 32, ... of the (r < i) list.
 __global__ void __launch_bounds__(PANEL_THREADS) qr_larft_kernel(const float *A, int lda, int nq, int k, int kb,
                                                                  const float *tau, float *T)
 {
+    constexpr int ROWS = 128;  // four 32-row chunks staged per pass
+    __shared__ float vs[ROWS][NB + 1];
     __shared__ float d[NB][NB];   // d[i][r] = -tau_i (v_r . v_i)
     __shared__ float ts[NB][NB];  // ts[i][r] = T(r, i)
+    constexpr int PER_WARP = (NB * (NB - 1) / 2 + 31) / 32;  // 16 pairs per warp
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int pairs = kb * (kb - 1) / 2;
-    for (int pr = warp; pr < pairs; pr += PANEL_THREADS / 32)
+    int pr_r[PER_WARP], pr_i[PER_WARP];
+    float p[PER_WARP];
+#pragma unroll
+    for (int u = 0; u < PER_WARP; ++u)
     {
+        const int pr = warp + 32 * u;
         int i = 1, rem = pr;
         while (rem >= i)
         {
             rem -= i;
             ++i;
         }
-        const int r = rem;
-        const float *vr = A + (int64_t)(k + r) * lda, *vi = A + (int64_t)(k + i) * lda;
-        float p = 0.0f;
-        for (int base = (k + i) & ~31; base < nq; base += 32)
+        pr_r[u] = pr < pairs ? rem : 0;
+        pr_i[u] = pr < pairs ? i : NB;  // NB marks an unused slot
+        p[u] = 0.0f;
+    }
+    for (int base0 = (k + 1) & ~31; base0 < nq; base0 += ROWS)
+    {
+        __syncthreads();
+        for (int idx = tid; idx < ROWS * kb; idx += PANEL_THREADS)
         {
-            const int row = base + lane;
-            if (row >= k + i && row < nq) p = fma_rn(vr[row], row == k + i ? 1.0f : vi[row], p);
+            const int rr = idx % ROWS, i = idx / ROWS, row = base0 + rr;
+            vs[rr][i] = row < nq && row > k + i ? A[(int64_t)(k + i) * lda + row] : (row == k + i ? 1.0f : 0.0f);
         }
-        const float dot = lane_fold(p);
-        if (lane == 0) d[i][r] = mul_rn(-tau[k + i], dot);
+        __syncthreads();
+        for (int cc = 0; cc < ROWS; cc += 32)  // chunks in ascending row order
+        {
+            const int row = base0 + cc + lane;
+            if (row < nq)
+            {
+#pragma unroll
+                for (int u = 0; u < PER_WARP; ++u)
+                    if (pr_i[u] < kb && row >= k + pr_i[u])
+                        p[u] = fma_rn(vs[cc + lane][pr_r[u]], vs[cc + lane][pr_i[u]], p[u]);
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < PER_WARP; ++u)
+    {
+        const float dot = lane_fold(p[u]);
+        if (lane == 0 && pr_i[u] < kb) d[pr_i[u]][pr_r[u]] = mul_rn(-tau[k + pr_i[u]], dot);
     }
     __syncthreads();
     for (int i = 0; i < kb; ++i)
@@ -169,33 +249,45 @@ template <bool RIGHT, bool LOWER_CHAIN>
 __global__ void __launch_bounds__(APPLY_WARPS * 32) qr_apply_kernel(const float *V, int ldv, int nq, int k, int kb,
                                                                     const float *T, float *C, int64_t ldc, int count)
 {
-    __shared__ float vs[32][NB + 1];
+    constexpr int ROWS = 128;  // four 32-row chunks of V staged per pass
+    __shared__ float vs[ROWS][NB + 1];
     __shared__ float ts[NB * NB];
     __shared__ float w2s[APPLY_WARPS][NB];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int j = blockIdx.x * APPLY_WARPS + warp;  // column (LEFT) or row (RIGHT) of C
     const bool live = j < count;
     for (int idx = tid; idx < NB * NB; idx += APPLY_WARPS * 32) ts[idx] = T[idx];
+    auto cat = [&](int row) -> float * { return RIGHT ? C + (int64_t)row * ldc + j : C + (int64_t)j * ldc + row; };
     float p[NB];
 #pragma unroll
     for (int i = 0; i < NB; ++i) p[i] = 0.0f;
     const int first = k & ~31;
-    for (int base = first; base < nq; base += 32)
+    for (int base0 = first; base0 < nq; base0 += ROWS)
     {
-        __syncthreads();
-        for (int idx = tid; idx < 32 * kb; idx += APPLY_WARPS * 32)
+        float c[ROWS / 32];
+#pragma unroll
+        for (int u = 0; u < ROWS / 32; ++u)  // this warp's values, loaded before the staging barrier
         {
-            const int rr = idx & 31, i = idx >> 5, row = base + rr;
+            const int row = base0 + 32 * u + lane;
+            c[u] = live && row >= k && row < nq ? *cat(row) : 0.0f;
+        }
+        __syncthreads();
+        for (int idx = tid; idx < ROWS * kb; idx += APPLY_WARPS * 32)
+        {
+            const int rr = idx % ROWS, i = idx / ROWS, row = base0 + rr;
             vs[rr][i] = row < nq && row > k + i ? V[(int64_t)(k + i) * ldv + row] : (row == k + i ? 1.0f : 0.0f);
         }
         __syncthreads();
-        const int row = base + lane;
-        if (live && row >= k && row < nq)
-        {
-            const float c = RIGHT ? C[(int64_t)row * ldc + j] : C[(int64_t)j * ldc + row];
 #pragma unroll
-            for (int i = 0; i < NB; ++i)
-                if (i < kb && row >= k + i) p[i] = fma_rn(vs[lane][i], c, p[i]);
+        for (int u = 0; u < ROWS / 32; ++u)  // chunks in ascending row order
+        {
+            const int row = base0 + 32 * u + lane;
+            if (live && row >= k && row < nq)
+            {
+#pragma unroll
+                for (int i = 0; i < NB; ++i)
+                    if (i < kb && row >= k + i) p[i] = fma_rn(vs[32 * u + lane][i], c[u], p[i]);
+            }
         }
     }
 #pragma unroll
@@ -217,24 +309,34 @@ __global__ void __launch_bounds__(APPLY_WARPS * 32) qr_apply_kernel(const float 
         w2s[warp][lane] = acc;
     }
     __syncwarp();
-    for (int base = first; base < nq; base += 32)
+    for (int base0 = first; base0 < nq; base0 += ROWS)
     {
-        __syncthreads();
-        for (int idx = tid; idx < 32 * kb; idx += APPLY_WARPS * 32)
+        float c[ROWS / 32];
+#pragma unroll
+        for (int u = 0; u < ROWS / 32; ++u)
         {
-            const int rr = idx & 31, i = idx >> 5, row = base + rr;
+            const int row = base0 + 32 * u + lane;
+            c[u] = live && row >= k && row < nq ? *cat(row) : 0.0f;
+        }
+        __syncthreads();
+        for (int idx = tid; idx < ROWS * kb; idx += APPLY_WARPS * 32)
+        {
+            const int rr = idx % ROWS, i = idx / ROWS, row = base0 + rr;
             vs[rr][i] = row < nq && row > k + i ? V[(int64_t)(k + i) * ldv + row] : (row == k + i ? 1.0f : 0.0f);
         }
         __syncthreads();
-        const int row = base + lane;
-        if (live && row >= k && row < nq)
-        {
-            float *cp = RIGHT ? C + (int64_t)row * ldc + j : C + (int64_t)j * ldc + row;
-            float c = *cp;
 #pragma unroll
-            for (int i = 0; i < NB; ++i)
-                if (i < kb && i <= row - k) c = fma_rn(-vs[lane][i], w2s[warp][i], c);
-            *cp = c;
+        for (int u = 0; u < ROWS / 32; ++u)
+        {
+            const int row = base0 + 32 * u + lane;
+            if (live && row >= k && row < nq)
+            {
+                float x = c[u];
+#pragma unroll
+                for (int i = 0; i < NB; ++i)
+                    if (i < kb && i <= row - k) x = fma_rn(-vs[32 * u + lane][i], w2s[warp][i], x);
+                *cat(row) = x;
+            }
         }
     }
 }
@@ -284,14 +386,27 @@ cudaError_t apply_block(bool right, bool lower_chain, const float *V, int ldv, i
 }
 }  // namespace
 
+static std::atomic<unsigned long long> g_qr_attr{0};
+
 cudaError_t launch_sgeqrf(float *A, int lda, int m, int n, float *tau, float *T, cudaStream_t stream)
 {
     const int lim = std::min(m, n);
-    cudaError_t e = cudaSuccess;
+    cudaError_t e = once_per_device(g_qr_attr,
+                                    []
+                                    {
+                                        return cudaFuncSetAttribute(qr_panel_kernel<true>,
+                                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                                    PANEL_SMEM_FLOATS * (int)sizeof(float));
+                                    });
     for (int k = 0; k < lim && e == cudaSuccess; k += NB)
     {
         const int kb = std::min(NB, lim - k);
-        qr_panel_kernel<<<1, PANEL_THREADS, 0, stream>>>(A, lda, m, k, kb, tau);
+        const int64_t panel_floats = (int64_t)(m - k) * kb;
+        if (panel_floats <= PANEL_SMEM_FLOATS)
+            qr_panel_kernel<true><<<1, PANEL_THREADS, (size_t)panel_floats * sizeof(float), stream>>>(A, lda, m, k, kb,
+                                                                                                       tau);
+        else
+            qr_panel_kernel<false><<<1, PANEL_THREADS, 0, stream>>>(A, lda, m, k, kb, tau);
         e = cudaGetLastError();
         if (e == cudaSuccess && k + kb < n)
         {
