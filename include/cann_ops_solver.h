@@ -200,6 +200,26 @@ extern "C"
     aclsolverStatus_t aclsolverSormqr(aclsolverHandle_t handle, aclsolverSideMode_t side, aclsolverOperation_t trans,
                                       int m, int n, int k, const float *A, int lda, const float *tau, float *C,
                                       int ldc, float *work, int lwork, int *devInfo);
+    /* Workspace bytes for Xlarft: k * k floats on the device, 0 on the host; params must be
+     * NULL, storev COLUMNWISE, all types ACLSOLVER_R_32F (else NOT_SUPPORTED), n <= 4096 and
+     * k <= 256 (else NOT_SUPPORTED); replaces cann_ops_solver.h:742 (xlarft_host.cpp:117). */
+    aclsolverStatus_t aclsolverXlarft_bufferSize(aclsolverHandle_t handle, aclsolverParams_t params,
+                                                 aclsolverDirectMode_t direct, aclsolverStorevMode_t storev, int64_t n,
+                                                 int64_t k, aclsolverDataType_t dataTypeV, const void *V, int64_t ldv,
+                                                 aclsolverDataType_t dataTypeTau, const void *tau,
+                                                 aclsolverDataType_t dataTypeT, void *T, int64_t ldt,
+                                                 aclsolverDataType_t computeType, size_t *workspaceInBytesOnDevice,
+                                                 size_t *workspaceInBytesOnHost);
+    /* The triangular factor T of the block reflector (slarft, columnwise): FORWARD T upper for
+     * H(1)...H(k), BACKWARD T lower for H(k)...H(1); only that triangle is written; no devInfo;
+     * replaces cann_ops_solver.h:784 (xlarft_host.cpp:190). */
+    aclsolverStatus_t aclsolverXlarft(aclsolverHandle_t handle, aclsolverParams_t params, aclsolverDirectMode_t direct,
+                                      aclsolverStorevMode_t storev, int64_t n, int64_t k, aclsolverDataType_t dataTypeV,
+                                      const void *V, int64_t ldv, aclsolverDataType_t dataTypeTau, const void *tau,
+                                      aclsolverDataType_t dataTypeT, void *T, int64_t ldt,
+                                      aclsolverDataType_t computeType, void *bufferOnDevice,
+                                      size_t workspaceInBytesOnDevice, void *bufferOnHost,
+                                      size_t workspaceInBytesOnHost);
     /* Bytes for SSgels: tau, Q^T B and one block factor; m >= n, m, n <= 4096, nrhs <= 128;
      * replaces cann_ops_solver.h:815 (sgels_host.cpp:149). */
     aclsolverStatus_t aclsolverSSgels_bufferSize(aclsolverHandle_t handle, int m, int n, int nrhs, float *dA, int ldda,

@@ -79,6 +79,30 @@ extern "C"
         ACLSOLVER_OP_C = 2
     } aclsolverOperation_t;
 
+    /* Parameter object of the generic (X-prefixed) entries; this build ships none, so it must
+     * be NULL (reference cann_ops_solver_common.h:83). */
+    typedef void *aclsolverParams_t;
+
+    /* Order of the elementary reflectors of a block reflector (reference :101-105). */
+    typedef enum
+    {
+        ACLSOLVER_DIRECT_FORWARD = 0,
+        ACLSOLVER_DIRECT_BACKWARD = 1
+    } aclsolverDirectMode_t;
+
+    /* Storage of the reflector vectors (reference :108-111). */
+    typedef enum
+    {
+        ACLSOLVER_STOREV_COLUMNWISE = 0
+    } aclsolverStorevMode_t;
+
+    /* Element type of a generic entry (reference :114-118). */
+    typedef enum
+    {
+        ACLSOLVER_R_32F = 0,
+        ACLSOLVER_C_32F = 1
+    } aclsolverDataType_t;
+
     /* Side from which an orthogonal factor is applied (reference cann_ops_solver_common.h:93-98). */
     typedef enum
     {

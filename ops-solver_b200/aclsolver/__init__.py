@@ -83,6 +83,10 @@ ARGTYPES = {
     "aclsolverSorgqr": [VP, I32, I32, I32, VP, I32, VP, VP, I32, VP],
     "aclsolverSormqr_bufferSize": [VP, I32, I32, I32, I32, I32, VP, I32, VP, VP, I32, C.POINTER(I32)],
     "aclsolverSormqr": [VP, I32, I32, I32, I32, I32, VP, I32, VP, VP, I32, VP, I32, VP],
+    "aclsolverXlarft_bufferSize": [VP, VP, I32, I32, I64, I64, I32, VP, I64, I32, VP, I32, VP, I64, I32,
+                                   C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)],
+    "aclsolverXlarft": [VP, VP, I32, I32, I64, I64, I32, VP, I64, I32, VP, I32, VP, I64, I32, VP, C.c_size_t, VP,
+                        C.c_size_t],
     "aclsolverSSgels_bufferSize": [VP, I32, I32, I32, VP, I32, VP, I32, VP, I32, VP, C.POINTER(C.c_size_t)],
     "aclsolverSSgels": [VP, I32, I32, I32, VP, I32, VP, I32, VP, I32, VP, C.c_size_t, C.POINTER(I32), VP],
     # additions of this build

@@ -7,6 +7,8 @@
 //   Sormqr    src/sormqr/arch35/sormqr_host.cpp:100-316 (nq <= 4096, k <= nq)
 //   SSgels    src/sgels/arch35/sgels_host.cpp:110-352 (m >= n, m, n <= 4096, nrhs <= 128,
 //             niter set to 0, dX may overlap neither dB nor dA)
+//   Xlarft    src/xlarft/arch35/xlarft_host.cpp:84-247 (params NULL, COLUMNWISE, FP32 only,
+//             n <= 4096, k <= 256, no devInfo)
 // An argument error writes -i (i counted without the handle) to the info buffer when that
 // buffer is usable and returns INVALID_VALUE; shapes over the kernel limits return
 // NOT_SUPPORTED (SSgels: INVALID_VALUE with -1 / -3, as the reference).  Workspace sizes are
@@ -88,6 +90,23 @@ int ormqr_shape(int side, int trans, int m, int n, int k, int lda, int ldc)
     if (lda < std::max(1, nq)) return 7;
     if (ldc < std::max(1, m)) return 10;
     return 0;
+}
+
+constexpr int64_t XLARFT_MAX_N = 4096;
+constexpr int64_t XLARFT_MAX_K = 256;
+
+aclsolverStatus_t xlarft_args(aclsolverParams_t params, int direct, int storev, int64_t n, int64_t k, int64_t ldv,
+                              int64_t ldt, int dv, int dtau, int dt, int dc)
+{
+    if (params != nullptr) return ACLSOLVER_STATUS_INVALID_VALUE;
+    if (direct != ACLSOLVER_DIRECT_FORWARD && direct != ACLSOLVER_DIRECT_BACKWARD) return ACLSOLVER_STATUS_INVALID_VALUE;
+    if (storev != ACLSOLVER_STOREV_COLUMNWISE) return ACLSOLVER_STATUS_INVALID_VALUE;
+    if (n < 0 || k < 0 || n < k) return ACLSOLVER_STATUS_INVALID_VALUE;
+    if (ldv < std::max<int64_t>(1, n) || ldt < std::max<int64_t>(1, k)) return ACLSOLVER_STATUS_INVALID_VALUE;
+    if (ldv > INT32_MAX || ldt > INT32_MAX) return ACLSOLVER_STATUS_INVALID_VALUE;
+    if (dv != ACLSOLVER_R_32F || dtau != ACLSOLVER_R_32F || dt != ACLSOLVER_R_32F || dc != ACLSOLVER_R_32F)
+        return ACLSOLVER_STATUS_NOT_SUPPORTED;
+    return ACLSOLVER_STATUS_SUCCESS;
 }
 
 int gels_shape(int m, int n, int nrhs, int lda, int ldb, int ldx)
@@ -225,6 +244,63 @@ extern "C"
         if (st != ACLSOLVER_STATUS_SUCCESS) return st;
         return finish(launch_sormqr(side == ACLSOLVER_SIDE_RIGHT, trans != ACLSOLVER_OP_N, m, n, k, A, lda, tau, C,
                                     ldc, work, h->stream));
+    }
+
+    aclsolverStatus_t aclsolverXlarft_bufferSize(aclsolverHandle_t handle, aclsolverParams_t params,
+                                                 aclsolverDirectMode_t direct, aclsolverStorevMode_t storev, int64_t n,
+                                                 int64_t k, aclsolverDataType_t dataTypeV, const void *V, int64_t ldv,
+                                                 aclsolverDataType_t dataTypeTau, const void *tau,
+                                                 aclsolverDataType_t dataTypeT, void *T, int64_t ldt,
+                                                 aclsolverDataType_t computeType, size_t *workspaceInBytesOnDevice,
+                                                 size_t *workspaceInBytesOnHost)
+    {
+        (void)handle;
+        (void)V;
+        (void)tau;
+        (void)T;
+        if (!workspaceInBytesOnDevice || !workspaceInBytesOnHost) return ACLSOLVER_STATUS_INVALID_VALUE;
+        aclsolverStatus_t st = xlarft_args(params, direct, storev, n, k, ldv, ldt, dataTypeV, dataTypeTau, dataTypeT,
+                                           computeType);
+        if (st != ACLSOLVER_STATUS_SUCCESS) return st;
+        *workspaceInBytesOnHost = 0;
+        if (n == 0 || k == 0)
+        {
+            *workspaceInBytesOnDevice = 0;
+            return ACLSOLVER_STATUS_SUCCESS;
+        }
+        if (n > XLARFT_MAX_N || k > XLARFT_MAX_K) return ACLSOLVER_STATUS_NOT_SUPPORTED;
+        *workspaceInBytesOnDevice = xlarft_work_bytes((int)k);
+        return ACLSOLVER_STATUS_SUCCESS;
+    }
+
+    aclsolverStatus_t aclsolverXlarft(aclsolverHandle_t handle, aclsolverParams_t params, aclsolverDirectMode_t direct,
+                                      aclsolverStorevMode_t storev, int64_t n, int64_t k, aclsolverDataType_t dataTypeV,
+                                      const void *V, int64_t ldv, aclsolverDataType_t dataTypeTau, const void *tau,
+                                      aclsolverDataType_t dataTypeT, void *T, int64_t ldt,
+                                      aclsolverDataType_t computeType, void *bufferOnDevice,
+                                      size_t workspaceInBytesOnDevice, void *bufferOnHost,
+                                      size_t workspaceInBytesOnHost)
+    {
+        (void)bufferOnHost;
+        (void)workspaceInBytesOnHost;
+        if (!handle) return ACLSOLVER_STATUS_HANDLE_IS_NULLPTR;
+        Handle *h = to_handle(handle);
+        aclsolverStatus_t st = xlarft_args(params, direct, storev, n, k, ldv, ldt, dataTypeV, dataTypeTau, dataTypeT,
+                                           computeType);
+        if (st != ACLSOLVER_STATUS_SUCCESS) return st;
+        if (n == 0 || k == 0) return ACLSOLVER_STATUS_SUCCESS;
+        if (n > XLARFT_MAX_N || k > XLARFT_MAX_K) return ACLSOLVER_STATUS_NOT_SUPPORTED;
+        if (!V || !tau || !T || !bufferOnDevice) return ACLSOLVER_STATUS_INVALID_VALUE;
+        const size_t need = xlarft_work_bytes((int)k);
+        if (workspaceInBytesOnDevice < need) return ACLSOLVER_STATUS_INVALID_VALUE;
+        if (!span_ok(V, (size_t)ldv * k * sizeof(float), alignof(float)) ||
+            !span_ok(tau, (size_t)k * sizeof(float), alignof(float)) ||
+            !span_ok(T, (size_t)ldt * k * sizeof(float), alignof(float)) ||
+            !span_ok(bufferOnDevice, need, alignof(float)))
+            return ACLSOLVER_STATUS_INVALID_VALUE;
+        return finish(launch_xlarft(direct == ACLSOLVER_DIRECT_BACKWARD, (int)n, (int)k, static_cast<const float *>(V),
+                                    (int)ldv, static_cast<const float *>(tau), static_cast<float *>(T), (int)ldt,
+                                    static_cast<float *>(bufferOnDevice), h->stream));
     }
 
     aclsolverStatus_t aclsolverSSgels_bufferSize(aclsolverHandle_t handle, int m, int n, int nrhs, float *dA, int ldda,

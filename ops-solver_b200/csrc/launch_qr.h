@@ -21,4 +21,9 @@ cudaError_t launch_sorgqr(int m, int n, int k, float *A, int lda, const float *t
 size_t sgels_work_floats(int m, int n, int nrhs);
 cudaError_t launch_sgels(int m, int n, int nrhs, float *A, int lda, const float *B, int ldb, float *X, int ldx,
                          float *work, cudaStream_t stream);
+// T (k x k, ld ldt) of k <= 256 reflectors (backward: units at rows n-k+i), columnwise; G
+// holds xlarft_work_bytes(k) of workspace.  Only the referenced triangle of T is written.
+size_t xlarft_work_bytes(int k);
+cudaError_t launch_xlarft(int backward, int n, int k, const float *V, int ldv, const float *tau, float *T, int ldt,
+                          float *G, cudaStream_t stream);
 }  // namespace ops_solver

@@ -16,6 +16,8 @@
 //                        sums over 32-row chunks of V staged in shared memory, W2 = op(T) W,
 //                        then c -= V W2 with an FMA chain over the reflectors
 //   qr_trsv_kernel       R X = Y, one block per right-hand side, backward sweep
+//   xlarft_gram_kernel / xlarft_tri_kernel   Xlarft: the reflector products over 32 x 32
+//                        blocks, then slarft's recurrence on a packed triangle (k <= 256)
 #include <algorithm>
 #include <atomic>
 
@@ -361,6 +363,119 @@ __global__ void __launch_bounds__(1024) qr_trsv_kernel(const float *R, int ldr, 
     for (int i = tid; i < n; i += blockDim.x) X[(int64_t)j * ldx + i] = xs[i];
 }
 
+// Reflector products for Xlarft: G(r, i) = lane sum over the rows both reflectors share of
+// v_r . v_i, for the pairs r < i (forward: v_i's unit at row i, rows [i, n)) or r > i
+// (backward: unit at row n-k+i, rows [0, n-k+i]).  Block (rb, ib) covers r in [32 rb, +32),
+// i in [32 ib, +32); warp w owns i = 32 ib + w, lane t's accumulator t owns r = 32 rb + t;
+// 32-row chunks of both column blocks are staged in shared memory.
+template <bool BACKWARD>
+__global__ void __launch_bounds__(1024) xlarft_gram_kernel(const float *V, int ldv, int n, int k, float *G)
+{
+    __shared__ float vr[32][33], vi[32][33];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int r0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+    if (BACKWARD ? r0 + 31 <= i0 : r0 >= i0 + 31) return;  // no pair of this block is referenced
+    const int i = i0 + warp;
+    const int unit_i = BACKWARD ? n - k + i : i;
+    int lo, hi;  // rows any pair of the block reads
+    if (BACKWARD)
+    {
+        lo = 0;
+        hi = min(n - 1, n - k + min(i0 + 31, k - 1));
+    }
+    else
+    {
+        lo = i0 & ~31;
+        hi = n - 1;
+    }
+    float p[32];
+#pragma unroll
+    for (int t = 0; t < 32; ++t) p[t] = 0.0f;
+    for (int base = lo & ~31; base <= hi; base += 32)
+    {
+        __syncthreads();
+        {
+            const int rr = tid & 31, cc = tid >> 5, row = base + rr;
+            const int cr = r0 + cc, ci = i0 + cc;
+            vr[rr][cc] = row < n && cr < k ? V[(int64_t)cr * ldv + row] : 0.0f;
+            float x = 0.0f;
+            if (row < n && ci < k)
+            {
+                const int u = BACKWARD ? n - k + ci : ci;
+                x = row == u ? 1.0f : V[(int64_t)ci * ldv + row];
+            }
+            vi[rr][cc] = x;
+        }
+        __syncthreads();
+        const int row = base + lane;
+        const bool in_rows = i < k && row < n && (BACKWARD ? row <= unit_i : row >= unit_i);
+        if (in_rows)
+        {
+            const float x = vi[lane][warp];
+#pragma unroll
+            for (int t = 0; t < 32; ++t)
+            {
+                const int r = r0 + t;
+                if (r < k && (BACKWARD ? r > i : r < i)) p[t] = fma_rn(vr[lane][t], x, p[t]);
+            }
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < 32; ++t)
+    {
+        const float dot = lane_fold(p[t]);
+        const int r = r0 + t;
+        if (lane == 0 && i < k && r < k && (BACKWARD ? r > i : r < i)) G[(int64_t)i * k + r] = dot;
+    }
+}
+
+// slarft's recurrence, one block: forward, for i ascending, T(r, i) = sum_{q=r}^{i-1} T(r, q)
+// d_q (r < i); backward, for i descending, T(r, i) = sum_{q=i+1}^{r} T(r, q) d_q (r > i); d_q =
+// -tau_i G(q, i), every sum an FMA chain in ascending q.  The referenced triangle of T is kept
+// packed in shared memory and written out at the end.
+template <bool BACKWARD>
+__global__ void __launch_bounds__(256) xlarft_tri_kernel(const float *G, int k, const float *tau, float *T, int ldt)
+{
+    extern __shared__ float tp[];  // packed triangle, column by column
+    __shared__ float d[256];
+    const int tid = threadIdx.x;
+    // forward: column i holds rows 0..i at i(i+1)/2; backward: rows i..k-1 at i k - i(i-1)/2
+    auto at = [&](int r, int c) -> float & {
+        return BACKWARD ? tp[c * k - c * (c - 1) / 2 + (r - c)] : tp[c * (c + 1) / 2 + r];
+    };
+    for (int s = 0; s < k; ++s)
+    {
+        const int i = BACKWARD ? k - 1 - s : s;
+        const float ti = tau[i];
+        for (int q = tid; q < k; q += blockDim.x)
+            d[q] = (BACKWARD ? q > i : q < i) ? mul_rn(-ti, G[(int64_t)i * k + q]) : 0.0f;
+        __syncthreads();
+        for (int r = tid; r < k; r += blockDim.x)
+        {
+            if (BACKWARD ? r < i : r > i) continue;
+            float val;
+            if (ti == 0.0f)
+                val = 0.0f;
+            else if (r == i)
+                val = ti;
+            else
+            {
+                float acc = 0.0f;
+                if (BACKWARD)
+                    for (int q = i + 1; q <= r; ++q) acc = fma_rn(at(r, q), d[q], acc);
+                else
+                    for (int q = r; q < i; ++q) acc = fma_rn(at(r, q), d[q], acc);
+                val = acc;
+            }
+            at(r, i) = val;
+        }
+        __syncthreads();
+    }
+    for (int c = 0; c < k; ++c)
+        for (int r = tid; r < k; r += blockDim.x)
+            if (BACKWARD ? r >= c : r <= c) T[(int64_t)c * ldt + r] = at(r, c);
+}
+
 __global__ void qr_identity_kernel(float *A, int lda, int m, int n)
 {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -478,5 +593,36 @@ cudaError_t launch_sgels(int m, int n, int nrhs, float *A, int lda, const float 
         e = cudaGetLastError();
     }
     return e;
+}
+}  // namespace ops_solver
+
+namespace ops_solver
+{
+size_t xlarft_work_bytes(int k) { return (size_t)k * k * sizeof(float); }
+
+cudaError_t launch_xlarft(int backward, int n, int k, const float *V, int ldv, const float *tau, float *T, int ldt,
+                          float *G, cudaStream_t stream)
+{
+    if (n <= 0 || k <= 0) return cudaSuccess;
+    if (k > 256) return cudaErrorInvalidValue;
+    const int kb = (k + 31) / 32;
+    dim3 grid(kb, kb);
+    const size_t tri = (size_t)k * (k + 1) / 2 * sizeof(float);
+    cudaError_t e;
+    if (backward)
+    {
+        e = cudaFuncSetAttribute(xlarft_tri_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri);
+        if (e != cudaSuccess) return e;
+        xlarft_gram_kernel<true><<<grid, 1024, 0, stream>>>(V, ldv, n, k, G);
+        xlarft_tri_kernel<true><<<1, 256, tri, stream>>>(G, k, tau, T, ldt);
+    }
+    else
+    {
+        e = cudaFuncSetAttribute(xlarft_tri_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri);
+        if (e != cudaSuccess) return e;
+        xlarft_gram_kernel<false><<<grid, 1024, 0, stream>>>(V, ldv, n, k, G);
+        xlarft_tri_kernel<false><<<1, 256, tri, stream>>>(G, k, tau, T, ldt);
+    }
+    return cudaGetLastError();
 }
 }  // namespace ops_solver

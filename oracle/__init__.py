@@ -49,6 +49,7 @@ def lib():
         _lib.orc_sormqr.argtypes = [_i, _i, _i, _i, _i, _F, _i, _F, _F, _i]
         _lib.orc_sorgqr.argtypes = [_i, _i, _i, _F, _i, _F]
         _lib.orc_sgels.argtypes = [_i, _i, _i, _F, _i, _F, _i, _F, _i, _F]
+        _lib.orc_slarft.argtypes = [_i, _i, _i, _F, _i, _F, _F, _i]
         _lib.orc_max_threads.restype = _i
     return _lib
 
@@ -273,3 +274,14 @@ def sgels(a, b):
     tau = np.zeros(max(1, n), dtype=np.float32)
     lib().orc_sgels(m, n, nrhs, fa, max(1, m), fb, max(1, m), x, max(1, n), tau)
     return _uncm(x, max(1, n), max(1, nrhs))[:n, :nrhs], _uncm(fa, m, n), tau[:n]
+
+
+def slarft(direct, v, tau, t_init=None):
+    """T (k x k) of the block reflector of V (n x k) and tau; direct 0 forward, 1 backward.
+    Entries outside the referenced triangle keep t_init (zeros by default)."""
+    n, k = v.shape
+    fv = _cm(v)
+    t = _cm(np.zeros((k, k), np.float32) if t_init is None else t_init)
+    tt = np.ascontiguousarray(tau, dtype=np.float32)
+    lib().orc_slarft(int(direct), n, k, fv, max(1, n), tt if tt.size else np.zeros(1, np.float32), t, max(1, k))
+    return _uncm(t, k, k)

@@ -1645,3 +1645,68 @@ void orc_sgeqr2_golden(int m, int n, float *a, int lda, float *tau)
         }
     }
 }
+
+/* Block reflector factor T (k x k, ld ldt) of k reflectors in V (n x k, ld ldv), columnwise
+ * (slarft).  direct 0 (forward): v_i has its unit at row i and entries below, T upper;
+ * direct 1 (backward): the unit at row n-k+i and entries above, T lower.  Each reflector
+ * product is a lane sum over its rows; T's column i is -tau_i times the products, carried
+ * through the finished part of T by FMA chains (ascending q).  Only the referenced triangle
+ * of T is written. */
+void orc_slarft(int direct, int n, int k, const float *v, int ldv, const float *tau, float *t, int ldt)
+{
+    float *g = (float *)malloc(sizeof(float) * (size_t)(k > 0 ? k : 1));
+    if (direct == 0)
+    {
+        for (int i = 0; i < k; ++i)
+        {
+            const float ti = tau[i];
+            if (ti == 0.0f)
+            {
+                for (int r = 0; r <= i; ++r) RAT(t, ldt, r, i) = 0.0f;
+                continue;
+            }
+            for (int r = 0; r < i; ++r)
+            {
+                float p[32] = {0};
+                for (int row = i; row < n; ++row)
+                    p[row & 31] = fmaf(RAT(v, ldv, row, r), row == i ? 1.0f : RAT(v, ldv, row, i), p[row & 31]);
+                g[r] = (-ti) * qr_lane_fold(p);
+            }
+            for (int r = 0; r < i; ++r)
+            {
+                float acc = 0.0f;
+                for (int q = r; q < i; ++q) acc = fmaf(RAT(t, ldt, r, q), g[q], acc);
+                RAT(t, ldt, r, i) = acc;
+            }
+            RAT(t, ldt, i, i) = ti;
+        }
+    }
+    else
+    {
+        for (int i = k - 1; i >= 0; --i)
+        {
+            const float ti = tau[i];
+            const int unit = n - k + i;
+            if (ti == 0.0f)
+            {
+                for (int r = i; r < k; ++r) RAT(t, ldt, r, i) = 0.0f;
+                continue;
+            }
+            for (int r = i + 1; r < k; ++r)
+            {
+                float p[32] = {0};
+                for (int row = 0; row <= unit; ++row)
+                    p[row & 31] = fmaf(RAT(v, ldv, row, r), row == unit ? 1.0f : RAT(v, ldv, row, i), p[row & 31]);
+                g[r] = (-ti) * qr_lane_fold(p);
+            }
+            for (int r = i + 1; r < k; ++r)
+            {
+                float acc = 0.0f;
+                for (int q = i + 1; q <= r; ++q) acc = fmaf(RAT(t, ldt, r, q), g[q], acc);
+                RAT(t, ldt, r, i) = acc;
+            }
+            RAT(t, ldt, i, i) = ti;
+        }
+    }
+    free(g);
+}

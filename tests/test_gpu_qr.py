@@ -167,3 +167,48 @@ def test_argument_errors_write_info(handle):
                              info.data_ptr())
     handle.stream.synchronize()
     assert st == 3 and int(info.cpu()[0]) == -1 and niter.value == 0
+
+
+def xlarft(handle, direct, v, tau, ldt_pad=1):
+    lib = aclsolver.library()
+    n, k = v.shape
+    dv = DeviceMatrices(v, n + 2)
+    dtau = torch.tensor(np.ascontiguousarray(tau), device="cuda")
+    t0 = np.full((k, k), 9.0, dtype=np.float32)  # the unreferenced triangle must survive
+    dt = DeviceMatrices(t0, k + ldt_pad)
+    dev, host = C.c_size_t(0), C.c_size_t(1)
+    assert lib.aclsolverXlarft_bufferSize(handle.value, None, direct, 0, n, k, 0, dv.ptr, dv.ld, 0, dtau.data_ptr(), 0,
+                                          dt.ptr, dt.ld, 0, C.byref(dev), C.byref(host)) == aclsolver.SUCCESS
+    assert host.value == 0
+    w = torch.empty(dev.value // 4 + 1, dtype=torch.float32, device="cuda")
+    st = lib.aclsolverXlarft(handle.value, None, direct, 0, n, k, 0, dv.ptr, dv.ld, 0, dtau.data_ptr(), 0, dt.ptr,
+                             dt.ld, 0, w.data_ptr(), dev.value, None, 0)
+    handle.stream.synchronize()
+    assert st == aclsolver.SUCCESS
+    return dt.read()[0], t0
+
+
+@pytest.mark.parametrize("direct", [0, 1])
+@pytest.mark.parametrize("n,k", [(1, 1), (40, 7), (100, 32), (300, 33), (1000, 256), (256, 256)])
+def test_xlarft_matches_oracle(handle, direct, n, k):
+    rng = np.random.default_rng(n + k + direct)
+    v = (rng.standard_normal((n, k)) / np.sqrt(n)).astype(np.float32)
+    tau = rng.uniform(0.5, 1.5, k).astype(np.float32)
+    if k > 3:
+        tau[2] = 0.0
+    got, t0 = xlarft(handle, direct, v, tau)
+    want = oracle.slarft(direct, v, tau, t0)
+    assert same_bits(got, want)
+
+
+def test_xlarft_argument_checks(handle):
+    lib = aclsolver.library()
+    dev, host = C.c_size_t(0), C.c_size_t(0)
+    q = lambda *a: lib.aclsolverXlarft_bufferSize(handle.value, *a, C.byref(dev), C.byref(host))
+    assert q(None, 0, 0, 10, 4, 0, None, 10, 0, None, 0, None, 4, 0) == aclsolver.SUCCESS and dev.value == 64
+    assert q(C.c_void_p(8), 0, 0, 10, 4, 0, None, 10, 0, None, 0, None, 4, 0) == 3
+    assert q(None, 2, 0, 10, 4, 0, None, 10, 0, None, 0, None, 4, 0) == 3
+    assert q(None, 0, 0, 3, 4, 0, None, 10, 0, None, 0, None, 4, 0) == 3
+    assert q(None, 0, 0, 10, 4, 1, None, 10, 0, None, 0, None, 4, 0) == 7
+    assert q(None, 0, 0, 5000, 4, 0, None, 5000, 0, None, 0, None, 4, 0) == 7
+    assert q(None, 0, 0, 300, 257, 0, None, 300, 0, None, 0, None, 257, 0) == 7

@@ -93,3 +93,28 @@ def test_host_argument_ladders_without_a_gpu():
     assert lib.aclsolverSgeqrf(None, 4, 4, None, 4, None, None, 0, C.byref(info)) == NULL_HANDLE
     assert lib.aclsolverSgeqrf(None, 4, 4, None, 4, None, None, 0, None) == INVALID
     assert lib.aclsolverSSgels(None, 4, 4, 1, None, 4, None, 4, None, 4, None, 0, None, None) == INVALID
+
+
+@pytest.mark.parametrize("direct", [0, 1])
+def test_slarft_forms_the_block_reflector(direct):
+    """I - V T V^T equals H(1)...H(k) (forward) or H(k)...H(1) (backward), the reference's
+    Larft contract (householder.hpp:172-200 for the forward case)."""
+    rng = np.random.default_rng(direct)
+    n, k = 50, 9
+    v = rng.standard_normal((n, k)).astype(np.float32)
+    tau = rng.uniform(0.2, 1.8, k).astype(np.float32)
+    tau[4] = 0.0
+    full = np.zeros((n, k))
+    for i in range(k):
+        u = i if direct == 0 else n - k + i
+        full[u, i] = 1.0
+        if direct == 0:
+            full[u + 1:, i] = v[u + 1:, i]
+        else:
+            full[:u, i] = v[:u, i]
+    h = np.eye(n)
+    for i in (range(k) if direct == 0 else reversed(range(k))):
+        h = h @ (np.eye(n) - float(tau[i]) * np.outer(full[:, i], full[:, i]))
+    t = oracle.slarft(direct, v, tau).astype(np.float64)
+    assert np.abs(h - (np.eye(n) - full @ t @ full.T)).max() < 1e-4 * np.abs(h).max()
+    assert np.all((np.tril(t, -1) if direct == 0 else np.triu(t, 1)) == 0)
