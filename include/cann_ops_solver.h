@@ -232,6 +232,57 @@ extern "C"
                                       int lddb, float *dX, int lddx, void *dWorkspace, size_t lwork_bytes, int *niter,
                                       int *dinfo);
 
+    /* ---- complex QR family; reference include/cann_ops_solver.h:259-424 ------------------- *
+     * complex64, column-major; reflectors in the clarfg convention (H = I - tau v v^H, beta
+     * real); padding rows are preserved.  Each execute call screens its inputs for NaN / Inf
+     * first (one stream synchronisation and a four-byte read-back, as the reference does):
+     * INVALID_VALUE with info -i for the first such argument. */
+
+    /* Lwork (complex elements) for Cgeqrf: 0 for an empty problem, else one 32 x 32 block
+     * factor; replaces cann_ops_solver.h:259 (cgeqrf_host.cpp:45). */
+    aclsolverStatus_t aclsolverCgeqrf_bufferSize(aclsolverHandle_t handle, int m, int n, aclsolverFloatComplex *A,
+                                                 int lda, int *Lwork);
+    /* A = Q R in place, TAU[min(m, n)]; devInfo 0 or -i (1 m, 2 n, 3 A, 4 lda, 5 TAU,
+     * 6 Workspace, 7 Lwork); replaces cann_ops_solver.h:277 (cgeqrf_host.cpp:51). */
+    aclsolverStatus_t aclsolverCgeqrf(aclsolverHandle_t handle, int m, int n, aclsolverFloatComplex *A, int lda,
+                                      aclsolverFloatComplex *TAU, aclsolverFloatComplex *Workspace, int Lwork,
+                                      int *devInfo);
+    /* lwork (complex elements) for Cungqr: m * k + 1024 (0 when empty); replaces
+     * cann_ops_solver.h:292 (cungqr_host.cpp:47). */
+    aclsolverStatus_t aclsolverCungqr_bufferSize(aclsolverHandle_t handle, int m, int n, int k,
+                                                 const aclsolverFloatComplex *A, int lda,
+                                                 const aclsolverFloatComplex *tau, int *lwork);
+    /* The first n columns of Q = H(1) ... H(k) (k = 0: identity columns), overwriting A;
+     * replaces cann_ops_solver.h:310 (cungqr_host.cpp:54). */
+    aclsolverStatus_t aclsolverCungqr(aclsolverHandle_t handle, int m, int n, int k, aclsolverFloatComplex *A, int lda,
+                                      const aclsolverFloatComplex *tau, aclsolverFloatComplex *work, int lwork,
+                                      int *devInfo);
+    /* lwork (complex elements) for Cunmqr: one 32 x 32 block factor (0 when empty); trans N or
+     * C; replaces cann_ops_solver.h:329 (cunmqr_host.cpp:55). */
+    aclsolverStatus_t aclsolverCunmqr_bufferSize(aclsolverHandle_t handle, aclsolverSideMode_t side,
+                                                 aclsolverOperation_t trans, int m, int n, int k,
+                                                 const aclsolverFloatComplex *A, int lda,
+                                                 const aclsolverFloatComplex *tau, const aclsolverFloatComplex *C,
+                                                 int ldc, int *lwork);
+    /* op(Q) C (LEFT) or C op(Q) (RIGHT), op(Q) = Q (OP_N) or Q^H (OP_C; OP_T is rejected as
+     * argument 2); replaces cann_ops_solver.h:353 (cunmqr_host.cpp:65). */
+    aclsolverStatus_t aclsolverCunmqr(aclsolverHandle_t handle, aclsolverSideMode_t side, aclsolverOperation_t trans,
+                                      int m, int n, int k, const aclsolverFloatComplex *A, int lda,
+                                      const aclsolverFloatComplex *tau, aclsolverFloatComplex *C, int ldc,
+                                      aclsolverFloatComplex *work, int lwork, int *devInfo);
+    /* Bytes for CCgels: tau, Q^H B and one block factor; m >= n, m, n <= 4096, nrhs <= 128;
+     * replaces cann_ops_solver.h:376 (ccgels_host.cpp:68). */
+    aclsolverStatus_t aclsolverCCgels_bufferSize(aclsolverHandle_t handle, int m, int n, int nrhs,
+                                                 aclsolverFloatComplex *dA, int ldda, aclsolverFloatComplex *dB,
+                                                 int lddb, aclsolverFloatComplex *dX, int lddx, void *dwork,
+                                                 size_t *lwork_bytes);
+    /* Least squares by QR: X = R^-1 (Q^H B)(1:n, :); dA overwritten, dB read only, dX must
+     * overlap neither; *niter = 0; a zero diagonal entry of R sets dinfo to its one-based
+     * position and leaves dX untouched; replaces cann_ops_solver.h:408 (ccgels_host.cpp:77). */
+    aclsolverStatus_t aclsolverCCgels(aclsolverHandle_t handle, int m, int n, int nrhs, aclsolverFloatComplex *dA,
+                                      int ldda, aclsolverFloatComplex *dB, int lddb, aclsolverFloatComplex *dX,
+                                      int lddx, void *dWorkspace, size_t lwork_bytes, int *niter, int *dinfo);
+
 #ifdef __cplusplus
 }
 #endif

@@ -89,6 +89,14 @@ ARGTYPES = {
                         C.c_size_t],
     "aclsolverSSgels_bufferSize": [VP, I32, I32, I32, VP, I32, VP, I32, VP, I32, VP, C.POINTER(C.c_size_t)],
     "aclsolverSSgels": [VP, I32, I32, I32, VP, I32, VP, I32, VP, I32, VP, C.c_size_t, C.POINTER(I32), VP],
+    "aclsolverCgeqrf_bufferSize": [VP, I32, I32, VP, I32, C.POINTER(I32)],
+    "aclsolverCgeqrf": [VP, I32, I32, VP, I32, VP, VP, I32, VP],
+    "aclsolverCungqr_bufferSize": [VP, I32, I32, I32, VP, I32, VP, C.POINTER(I32)],
+    "aclsolverCungqr": [VP, I32, I32, I32, VP, I32, VP, VP, I32, VP],
+    "aclsolverCunmqr_bufferSize": [VP, I32, I32, I32, I32, I32, VP, I32, VP, VP, I32, C.POINTER(I32)],
+    "aclsolverCunmqr": [VP, I32, I32, I32, I32, I32, VP, I32, VP, VP, I32, VP, I32, VP],
+    "aclsolverCCgels_bufferSize": [VP, I32, I32, I32, VP, I32, VP, I32, VP, I32, VP, C.POINTER(C.c_size_t)],
+    "aclsolverCCgels": [VP, I32, I32, I32, VP, I32, VP, I32, VP, I32, VP, C.c_size_t, C.POINTER(I32), VP],
     # additions of this build
     "aclsolverSetDeviceChecks": [VP, I32],
     "aclsolverGetDeviceChecks": [VP, C.POINTER(I32)],

@@ -1,0 +1,593 @@
+// cqr.cu -- the complex QR family: Cgeqrf, Cunmqr, Cungqr and CCgels (complex64).
+//
+// Reflectors follow LAPACK clarfg, as the reference's kernel does
+// (src/cgeqrf/arch35/cgeqrf_reflector_simd.h:89-170): beta = -copysign(||(alpha; x)||, Re alpha),
+// tau = ((beta - Re alpha) / beta, -(Im alpha / beta)), v = x / (alpha - beta), tau = 0 when
+// x is zero and alpha real; Q = H(1)...H(k), H = I - tau v v^H.  The schedule is the real
+// family's (qr.cu): 32-column panels, lane sums over rows (row r into lane r mod 32, a warp
+// butterfly per component), slarft's T, block application.  The complex products are fixed
+// FMA sequences (cq_* below) that the CPU oracle restates.
+#include <limits.h>
+
+#include <algorithm>
+#include <atomic>
+
+#include "complex_lu.cuh"
+#include "device_once.h"
+#include "launch_qr.h"
+
+namespace ops_solver
+{
+namespace
+{
+constexpr int NB = 32;
+constexpr int PANEL_THREADS = 1024;
+constexpr int APPLY_WARPS = 16;
+constexpr int PANEL_SMEM_ELEMS = 25 * 1024;  // complex elements of a panel kept in shared memory
+
+// acc += conj(v) a
+__device__ __forceinline__ float2 cq_conjdot(float2 acc, float2 v, float2 a)
+{
+    return make_float2(fma_rn(v.y, a.y, fma_rn(v.x, a.x, acc.x)), fma_rn(-v.y, a.x, fma_rn(v.x, a.y, acc.y)));
+}
+// acc += c v
+__device__ __forceinline__ float2 cq_dot(float2 acc, float2 c, float2 v)
+{
+    return make_float2(fma_rn(-c.y, v.y, fma_rn(c.x, v.x, acc.x)), fma_rn(c.y, v.x, fma_rn(c.x, v.y, acc.y)));
+}
+// x - y conj(v)
+__device__ __forceinline__ float2 cq_submulc(float2 x, float2 y, float2 v)
+{
+    return make_float2(fma_rn(-y.y, v.y, fma_rn(-y.x, v.x, x.x)), fma_rn(y.x, v.y, fma_rn(-y.y, v.x, x.y)));
+}
+__device__ __forceinline__ float2 cq_mul(float2 a, float2 b)
+{
+    return make_float2(fma_rn(-a.y, b.y, mul_rn(a.x, b.x)), fma_rn(a.y, b.x, mul_rn(a.x, b.y)));
+}
+__device__ __forceinline__ float2 cq_mulc(float2 a, float2 b)
+{
+    return make_float2(fma_rn(a.y, b.y, mul_rn(a.x, b.x)), fma_rn(-a.y, b.x, mul_rn(a.x, b.y)));
+}
+// acc + a b
+__device__ __forceinline__ float2 cq_fma(float2 a, float2 b, float2 acc)
+{
+    return make_float2(fma_rn(-a.y, b.y, fma_rn(a.x, b.x, acc.x)), fma_rn(a.y, b.x, fma_rn(a.x, b.y, acc.y)));
+}
+// acc + conj(a) b
+__device__ __forceinline__ float2 cq_fmac(float2 a, float2 b, float2 acc)
+{
+    return make_float2(fma_rn(a.y, b.y, fma_rn(a.x, b.x, acc.x)), fma_rn(-a.y, b.x, fma_rn(a.x, b.y, acc.y)));
+}
+
+__device__ __forceinline__ float fold1(float p)
+{
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) p = add_rn(p, __shfl_xor_sync(0xffffffffu, p, off));
+    return p;
+}
+__device__ __forceinline__ float2 fold2(float2 p) { return make_float2(fold1(p.x), fold1(p.y)); }
+
+__device__ __forceinline__ bool czero2(float2 v) { return v.x == 0.0f && v.y == 0.0f; }
+
+// Panel columns [k, k + kb) of rows [k, m); SMEM keeps the panel in shared memory.
+template <bool SMEM>
+__global__ void __launch_bounds__(PANEL_THREADS) cq_panel_kernel(float2 *A, int lda, int m, int k, int kb, float2 *tau)
+{
+    extern __shared__ float2 sp[];
+    __shared__ float2 s_tau;
+    __shared__ float s_dr, s_di, s_den;
+    __shared__ int s_apply;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int H = m - k;
+    auto at = [&](int j, int row) -> float2 & {
+        return SMEM ? sp[(int64_t)(j - k) * H + (row - k)] : A[(int64_t)j * lda + row];
+    };
+    if (SMEM)
+    {
+        for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) sp[idx] = A[(int64_t)(k + idx / H) * lda + k + idx % H];
+        __syncthreads();
+    }
+    constexpr int U = 8;
+    for (int c = k; c < k + kb; ++c)
+    {
+        if (warp == 0)
+        {
+            float p = 0.0f;
+            for (int base = (c + 1) & ~31; base < m; base += 32 * U)
+            {
+                float2 x[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                {
+                    const int row = base + 32 * u + lane;
+                    x[u] = row > c && row < m ? at(c, row) : make_float2(0.0f, 0.0f);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                {
+                    const int row = base + 32 * u + lane;
+                    if (row > c && row < m) p = fma_rn(x[u].y, x[u].y, fma_rn(x[u].x, x[u].x, p));
+                }
+            }
+            const float sumsq = fold1(p);
+            if (lane == 0)
+            {
+                const float2 al = at(c, c);
+                float2 t = make_float2(0.0f, 0.0f);
+                int apply = 0;
+                if (!(sumsq == 0.0f && al.y == 0.0f))
+                {
+                    const float norm = sqrt_rn(add_rn(add_rn(mul_rn(al.x, al.x), mul_rn(al.y, al.y)), sumsq));
+                    const float beta = -copysignf(norm, al.x);
+                    t = make_float2(div_rn(sub_rn(beta, al.x), beta), -div_rn(al.y, beta));
+                    const float dr = sub_rn(al.x, beta), di = al.y;
+                    s_dr = dr;
+                    s_di = di;
+                    s_den = add_rn(mul_rn(dr, dr), mul_rn(di, di));
+                    at(c, c) = make_float2(beta, 0.0f);
+                    apply = 1;
+                }
+                tau[c] = t;
+                s_tau = t;
+                s_apply = apply;
+            }
+        }
+        __syncthreads();
+        const bool apply = s_apply != 0;
+        const float2 t = s_tau;
+        if (apply)
+        {
+            const float dr = s_dr, di = s_di, den = s_den;
+            for (int row = c + 1 + tid; row < m; row += PANEL_THREADS)
+            {
+                const float2 x = at(c, row);
+                at(c, row) = make_float2(div_rn(add_rn(mul_rn(x.x, dr), mul_rn(x.y, di)), den),
+                                         div_rn(sub_rn(mul_rn(x.y, dr), mul_rn(x.x, di)), den));
+            }
+        }
+        __syncthreads();
+        const int j = c + warp;
+        if (apply && warp >= 1 && j < k + kb)
+        {
+            float2 p = make_float2(0.0f, 0.0f);
+            for (int base = c & ~31; base < m; base += 32 * U)
+            {
+                float2 v[U], x[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                {
+                    const int row = base + 32 * u + lane;
+                    const bool ok = row >= c && row < m;
+                    v[u] = ok ? (row == c ? make_float2(1.0f, 0.0f) : at(c, row)) : make_float2(0.0f, 0.0f);
+                    x[u] = ok ? at(j, row) : make_float2(0.0f, 0.0f);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                {
+                    const int row = base + 32 * u + lane;
+                    if (row >= c && row < m) p = cq_conjdot(p, v[u], x[u]);
+                }
+            }
+            const float2 w = cq_mulc(t, fold2(p));
+            for (int base = c & ~31; base < m; base += 32 * U)
+            {
+                float2 v[U], x[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                {
+                    const int row = base + 32 * u + lane;
+                    const bool ok = row >= c && row < m;
+                    v[u] = ok ? (row == c ? make_float2(1.0f, 0.0f) : at(c, row)) : make_float2(0.0f, 0.0f);
+                    x[u] = ok ? at(j, row) : make_float2(0.0f, 0.0f);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                {
+                    const int row = base + 32 * u + lane;
+                    if (row >= c && row < m) at(j, row) = clu::csubmul(x[u], v[u], w);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (SMEM)
+        for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) A[(int64_t)(k + idx / H) * lda + k + idx % H] = sp[idx];
+}
+
+// T (kb x kb upper, ld NB) of the reflectors at columns [k, k + kb), length nq.
+__global__ void __launch_bounds__(PANEL_THREADS) cq_larft_kernel(const float2 *A, int lda, int nq, int k, int kb,
+                                                                 const float2 *tau, float2 *T)
+{
+    constexpr int ROWS = 64;
+    __shared__ float2 vs[ROWS][NB + 1];
+    __shared__ float2 d[NB][NB];   // d[i][r] = -tau_i (v_r^H v_i)
+    __shared__ float2 ts[NB][NB];  // ts[i][r] = T(r, i)
+    constexpr int PER_WARP = (NB * (NB - 1) / 2 + 31) / 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int pairs = kb * (kb - 1) / 2;
+    int pr_r[PER_WARP], pr_i[PER_WARP];
+    float2 p[PER_WARP];
+#pragma unroll
+    for (int u = 0; u < PER_WARP; ++u)
+    {
+        const int pr = warp + 32 * u;
+        int i = 1, rem = pr;
+        while (rem >= i)
+        {
+            rem -= i;
+            ++i;
+        }
+        pr_r[u] = pr < pairs ? rem : 0;
+        pr_i[u] = pr < pairs ? i : NB;
+        p[u] = make_float2(0.0f, 0.0f);
+    }
+    for (int base0 = (k + 1) & ~31; base0 < nq; base0 += ROWS)
+    {
+        __syncthreads();
+        for (int idx = tid; idx < ROWS * kb; idx += PANEL_THREADS)
+        {
+            const int rr = idx % ROWS, i = idx / ROWS, row = base0 + rr;
+            vs[rr][i] = row < nq && row > k + i ? A[(int64_t)(k + i) * lda + row]
+                                                : make_float2(row == k + i ? 1.0f : 0.0f, 0.0f);
+        }
+        __syncthreads();
+        for (int cc = 0; cc < ROWS; cc += 32)
+        {
+            const int row = base0 + cc + lane;
+            if (row < nq)
+            {
+#pragma unroll
+                for (int u = 0; u < PER_WARP; ++u)
+                    if (pr_i[u] < kb && row >= k + pr_i[u])
+                        p[u] = cq_conjdot(p[u], vs[cc + lane][pr_r[u]], vs[cc + lane][pr_i[u]]);
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < PER_WARP; ++u)
+    {
+        const float2 dot = fold2(p[u]);
+        if (lane == 0 && pr_i[u] < kb)
+        {
+            const float2 ti = tau[k + pr_i[u]];
+            d[pr_i[u]][pr_r[u]] = cq_mul(make_float2(-ti.x, -ti.y), dot);
+        }
+    }
+    __syncthreads();
+    for (int i = 0; i < kb; ++i)
+    {
+        const float2 ti = tau[k + i];
+        if (tid <= i)
+        {
+            if (czero2(ti))
+                ts[i][tid] = make_float2(0.0f, 0.0f);
+            else if (tid == i)
+                ts[i][i] = ti;
+            else
+            {
+                float2 acc = make_float2(0.0f, 0.0f);
+                for (int q = tid; q < i; ++q) acc = cq_fma(ts[q][tid], d[i][q], acc);
+                ts[i][tid] = acc;
+            }
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < kb * kb; idx += PANEL_THREADS)
+    {
+        const int r = idx % kb, i = idx / kb;
+        if (r <= i) T[i * NB + r] = ts[i][r];
+    }
+}
+
+// LEFT: C = (I - V op(T) V^H) C, one warp per column of C; RIGHT: C = C (I - V op(T) V^H), one
+// warp per row.  HERM selects op(T) = T^H (LEFT: Q^H C; RIGHT: C Q^H), else T.
+template <bool RIGHT, bool HERM>
+__global__ void __launch_bounds__(APPLY_WARPS * 32) cq_apply_kernel(const float2 *V, int ldv, int nq, int k, int kb,
+                                                                    const float2 *T, float2 *C, int64_t ldc, int count)
+{
+    constexpr int ROWS = 64;
+    __shared__ float2 vs[ROWS][NB + 1];
+    __shared__ float2 ts[NB * NB];
+    __shared__ float2 w2s[APPLY_WARPS][NB];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int j = blockIdx.x * APPLY_WARPS + warp;
+    const bool live = j < count;
+    for (int idx = tid; idx < NB * NB; idx += APPLY_WARPS * 32) ts[idx] = T[idx];
+    auto cat = [&](int row) -> float2 * { return RIGHT ? C + (int64_t)row * ldc + j : C + (int64_t)j * ldc + row; };
+    float2 p[NB];
+#pragma unroll
+    for (int i = 0; i < NB; ++i) p[i] = make_float2(0.0f, 0.0f);
+    const int first = k & ~31;
+    for (int base0 = first; base0 < nq; base0 += ROWS)
+    {
+        float2 c[ROWS / 32];
+#pragma unroll
+        for (int u = 0; u < ROWS / 32; ++u)
+        {
+            const int row = base0 + 32 * u + lane;
+            c[u] = live && row >= k && row < nq ? *cat(row) : make_float2(0.0f, 0.0f);
+        }
+        __syncthreads();
+        for (int idx = tid; idx < ROWS * kb; idx += APPLY_WARPS * 32)
+        {
+            const int rr = idx % ROWS, i = idx / ROWS, row = base0 + rr;
+            vs[rr][i] = row < nq && row > k + i ? V[(int64_t)(k + i) * ldv + row]
+                                                : make_float2(row == k + i ? 1.0f : 0.0f, 0.0f);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < ROWS / 32; ++u)
+        {
+            const int row = base0 + 32 * u + lane;
+            if (live && row >= k && row < nq)
+            {
+#pragma unroll
+                for (int i = 0; i < NB; ++i)
+                    if (i < kb && row >= k + i)
+                        p[i] = RIGHT ? cq_dot(p[i], c[u], vs[32 * u + lane][i])
+                                     : cq_conjdot(p[i], vs[32 * u + lane][i], c[u]);
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NB; ++i) p[i] = fold2(p[i]);
+    {
+        // lower chain (sum over q <= i of T(q, i)): LEFT with T^H, RIGHT with T
+        constexpr bool LOWER = RIGHT ? !HERM : HERM;
+        float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll
+        for (int q = 0; q < NB; ++q)
+        {
+            if (LOWER)
+            {
+                if (q <= lane && lane < kb)
+                    acc = HERM ? cq_fmac(ts[lane * NB + q], p[q], acc) : cq_fma(ts[lane * NB + q], p[q], acc);
+            }
+            else
+            {
+                if (q >= lane && q < kb)
+                    acc = HERM ? cq_fmac(ts[q * NB + lane], p[q], acc) : cq_fma(ts[q * NB + lane], p[q], acc);
+            }
+        }
+        w2s[warp][lane] = acc;
+    }
+    __syncwarp();
+    for (int base0 = first; base0 < nq; base0 += ROWS)
+    {
+        float2 c[ROWS / 32];
+#pragma unroll
+        for (int u = 0; u < ROWS / 32; ++u)
+        {
+            const int row = base0 + 32 * u + lane;
+            c[u] = live && row >= k && row < nq ? *cat(row) : make_float2(0.0f, 0.0f);
+        }
+        __syncthreads();
+        for (int idx = tid; idx < ROWS * kb; idx += APPLY_WARPS * 32)
+        {
+            const int rr = idx % ROWS, i = idx / ROWS, row = base0 + rr;
+            vs[rr][i] = row < nq && row > k + i ? V[(int64_t)(k + i) * ldv + row]
+                                                : make_float2(row == k + i ? 1.0f : 0.0f, 0.0f);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < ROWS / 32; ++u)
+        {
+            const int row = base0 + 32 * u + lane;
+            if (live && row >= k && row < nq)
+            {
+                float2 x = c[u];
+#pragma unroll
+                for (int i = 0; i < NB; ++i)
+                    if (i < kb && i <= row - k)
+                        x = RIGHT ? cq_submulc(x, w2s[warp][i], vs[32 * u + lane][i])
+                                  : clu::csubmul(x, vs[32 * u + lane][i], w2s[warp][i]);
+                *cat(row) = x;
+            }
+        }
+    }
+}
+
+// R X = Y for one right-hand side per block; R's diagonal is real.  Every block first looks
+// for a zero diagonal entry: the first one (one-based) goes to info and X is left untouched.
+__global__ void __launch_bounds__(1024) cq_trsv_kernel(const float2 *R, int ldr, int n, const float2 *Y, int ldy,
+                                                       float2 *X, int ldx, int *info)
+{
+    extern __shared__ float2 xs[];
+    __shared__ int s_zero;
+    const int j = blockIdx.x, tid = threadIdx.x;
+    if (tid == 0) s_zero = n;
+    __syncthreads();
+    for (int i = tid; i < n; i += blockDim.x)
+        if (czero2(R[(int64_t)i * ldr + i])) atomicMin(&s_zero, i);
+    __syncthreads();
+    const int zero = s_zero;
+    if (zero < n)
+    {
+        if (j == 0 && tid == 0) *info = zero + 1;
+        return;
+    }
+    for (int i = tid; i < n; i += blockDim.x) xs[i] = Y[(int64_t)j * ldy + i];
+    __syncthreads();
+    for (int p = n - 1; p >= 0; --p)
+    {
+        const float2 *rp = R + (int64_t)p * ldr;
+        if (tid == 0)
+        {
+            const float d = rp[p].x;
+            xs[p] = make_float2(div_rn(xs[p].x, d), div_rn(xs[p].y, d));
+        }
+        __syncthreads();
+        const float2 xp = xs[p];
+        for (int i = tid; i < p; i += blockDim.x) xs[i] = clu::csubmul(xs[i], rp[i], xp);
+        __syncthreads();
+    }
+    for (int i = tid; i < n; i += blockDim.x) X[(int64_t)j * ldx + i] = xs[i];
+}
+
+// Input screening: the smallest code among the regions holding a NaN or an infinity goes to
+// *flag (atomicMin over an initial INT_MAX).  A region with strict set is a reflector store:
+// only the entries below its diagonal are inputs.
+struct FiniteRegion
+{
+    const float2 *p;
+    int rows, cols;
+    int64_t ld;
+    int strict, code;
+};
+
+__global__ void cq_finite_kernel(FiniteRegion r0, FiniteRegion r1, FiniteRegion r2, int *flag)
+{
+    const FiniteRegion rs[3] = {r0, r1, r2};
+    int found = INT_MAX;
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+    {
+        const FiniteRegion r = rs[q];
+        if (!r.p || r.rows <= 0 || r.cols <= 0) continue;
+        const int64_t total = (int64_t)r.rows * r.cols;
+        for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+             idx += (int64_t)gridDim.x * blockDim.x)
+        {
+            const int row = (int)(idx % r.rows), col = (int)(idx / r.rows);
+            if (r.strict && row <= col) continue;
+            const float2 v = r.p[(int64_t)col * r.ld + row];
+            if (!isfinite(v.x) || !isfinite(v.y)) found = min(found, r.code);
+        }
+    }
+    // the warp's smallest code, one atomic per warp
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) found = min(found, __shfl_xor_sync(0xffffffffu, found, off));
+    if ((threadIdx.x & 31) == 0 && found != INT_MAX) atomicMin(flag, found);
+}
+
+__global__ void cq_identity_kernel(float2 *A, int lda, int m, int n)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)m * n) return;
+    const int r = (int)(idx % m), c = (int)(idx / m);
+    A[(int64_t)c * lda + r] = make_float2(r == c ? 1.0f : 0.0f, 0.0f);
+}
+
+cudaError_t cq_apply(bool right, bool herm, const float2 *V, int ldv, int nq, int k, int kb, const float2 *T,
+                     float2 *C, int64_t ldc, int count, cudaStream_t stream)
+{
+    if (count <= 0) return cudaSuccess;
+    const unsigned grid = (unsigned)((count + APPLY_WARPS - 1) / APPLY_WARPS);
+    if (right && herm)
+        cq_apply_kernel<true, true><<<grid, APPLY_WARPS * 32, 0, stream>>>(V, ldv, nq, k, kb, T, C, ldc, count);
+    else if (right)
+        cq_apply_kernel<true, false><<<grid, APPLY_WARPS * 32, 0, stream>>>(V, ldv, nq, k, kb, T, C, ldc, count);
+    else if (herm)
+        cq_apply_kernel<false, true><<<grid, APPLY_WARPS * 32, 0, stream>>>(V, ldv, nq, k, kb, T, C, ldc, count);
+    else
+        cq_apply_kernel<false, false><<<grid, APPLY_WARPS * 32, 0, stream>>>(V, ldv, nq, k, kb, T, C, ldc, count);
+    return cudaGetLastError();
+}
+
+std::atomic<unsigned long long> g_cq_attr{0};
+}  // namespace
+
+cudaError_t launch_cgeqrf(float2 *A, int lda, int m, int n, float2 *tau, float2 *T, cudaStream_t stream)
+{
+    cudaError_t e = once_per_device(g_cq_attr,
+                                    []
+                                    {
+                                        return cudaFuncSetAttribute(cq_panel_kernel<true>,
+                                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                                    PANEL_SMEM_ELEMS * (int)sizeof(float2));
+                                    });
+    const int lim = std::min(m, n);
+    for (int k = 0; k < lim && e == cudaSuccess; k += NB)
+    {
+        const int kb = std::min(NB, lim - k);
+        const int64_t elems = (int64_t)(m - k) * kb;
+        if (elems <= PANEL_SMEM_ELEMS)
+            cq_panel_kernel<true><<<1, PANEL_THREADS, (size_t)elems * sizeof(float2), stream>>>(A, lda, m, k, kb, tau);
+        else
+            cq_panel_kernel<false><<<1, PANEL_THREADS, 0, stream>>>(A, lda, m, k, kb, tau);
+        e = cudaGetLastError();
+        if (e == cudaSuccess && k + kb < n)
+        {
+            cq_larft_kernel<<<1, PANEL_THREADS, 0, stream>>>(A, lda, m, k, kb, tau, T);
+            e = cudaGetLastError();
+            if (e == cudaSuccess)
+                e = cq_apply(false, true, A, lda, m, k, kb, T, A + (int64_t)(k + kb) * lda, lda, n - k - kb, stream);
+        }
+    }
+    return e;
+}
+
+cudaError_t launch_cunmqr(int side, int herm, int m, int n, int k, const float2 *A, int lda, const float2 *tau,
+                          float2 *C, int ldc, float2 *T, cudaStream_t stream)
+{
+    const bool right = side != 0, h = herm != 0;
+    const int nq = right ? n : m, count = right ? m : n;
+    const int npan = (k + NB - 1) / NB;
+    const bool forward = !right == h;
+    cudaError_t e = cudaSuccess;
+    for (int s = 0; s < npan && e == cudaSuccess; ++s)
+    {
+        const int pi = forward ? s : npan - 1 - s;
+        const int k0 = pi * NB, kb = std::min(NB, k - k0);
+        cq_larft_kernel<<<1, PANEL_THREADS, 0, stream>>>(A, lda, nq, k0, kb, tau, T);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cq_apply(right, h, A, lda, nq, k0, kb, T, C, ldc, count, stream);
+    }
+    return e;
+}
+
+cudaError_t launch_cungqr(int m, int n, int k, float2 *A, int lda, const float2 *tau, float2 *work, cudaStream_t stream)
+{
+    float2 *v = work, *T = work + (size_t)m * k;
+    cudaError_t e = cudaSuccess;
+    if (k > 0)
+        e = cudaMemcpy2DAsync(v, (size_t)m * sizeof(float2), A, (size_t)lda * sizeof(float2),
+                              (size_t)m * sizeof(float2), k, cudaMemcpyDeviceToDevice, stream);
+    if (e == cudaSuccess)
+    {
+        const int64_t total = (int64_t)m * n;
+        cq_identity_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(A, lda, m, n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && k > 0) e = launch_cunmqr(0, 0, m, n, k, v, m, tau, A, lda, T, stream);
+    return e;
+}
+
+size_t cgels_work_elems(int m, int n, int nrhs)
+{
+    auto up = [](size_t x) { return (x + 31) & ~size_t(31); };
+    return up((size_t)std::max(n, 1)) + up((size_t)m * nrhs) + up(NB * NB);
+}
+
+cudaError_t launch_cgels(int m, int n, int nrhs, float2 *A, int lda, const float2 *B, int ldb, float2 *X, int ldx,
+                         float2 *work, int *info, cudaStream_t stream)
+{
+    auto up = [](size_t x) { return (x + 31) & ~size_t(31); };
+    float2 *tau = work, *Y = tau + up((size_t)std::max(n, 1)), *T = Y + up((size_t)m * nrhs);
+    cudaError_t e = cudaMemcpy2DAsync(Y, (size_t)m * sizeof(float2), B, (size_t)ldb * sizeof(float2),
+                                      (size_t)m * sizeof(float2), nrhs, cudaMemcpyDeviceToDevice, stream);
+    if (e == cudaSuccess) e = launch_cgeqrf(A, lda, m, n, tau, T, stream);
+    if (e == cudaSuccess) e = launch_cunmqr(0, 1, m, nrhs, n, A, lda, tau, Y, m, T, stream);
+    if (e == cudaSuccess)
+    {
+        cq_trsv_kernel<<<nrhs, 1024, (size_t)n * sizeof(float2), stream>>>(A, lda, n, Y, m, X, ldx, info);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+cudaError_t launch_cq_finite(const CqRegion *regions, int count, int *flag, cudaStream_t stream)
+{
+    FiniteRegion r[3] = {};
+    int64_t most = 0;
+    for (int q = 0; q < count && q < 3; ++q)
+    {
+        r[q] = {static_cast<const float2 *>(regions[q].p), regions[q].rows, regions[q].cols, regions[q].ld,
+                regions[q].strict, regions[q].code};
+        most = std::max<int64_t>(most, (int64_t)regions[q].rows * regions[q].cols);
+    }
+    const int64_t blocks = std::min<int64_t>(std::max<int64_t>((most + 255) / 256, 1), 148 * 8);
+    cq_finite_kernel<<<(unsigned)blocks, 256, 0, stream>>>(r[0], r[1], r[2], flag);
+    return cudaGetLastError();
+}
+}  // namespace ops_solver

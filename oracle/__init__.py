@@ -50,6 +50,10 @@ def lib():
         _lib.orc_sorgqr.argtypes = [_i, _i, _i, _F, _i, _F]
         _lib.orc_sgels.argtypes = [_i, _i, _i, _F, _i, _F, _i, _F, _i, _F]
         _lib.orc_slarft.argtypes = [_i, _i, _i, _F, _i, _F, _F, _i]
+        _lib.orc_cgeqrf.argtypes = [_i, _i, _F, _i, _F]
+        _lib.orc_cunmqr.argtypes = [_i, _i, _i, _i, _i, _F, _i, _F, _F, _i]
+        _lib.orc_cungqr.argtypes = [_i, _i, _i, _F, _i, _F]
+        _lib.orc_cgels.argtypes = [_i, _i, _i, _F, _i, _F, _i, _F, _i, _F]
         _lib.orc_max_threads.restype = _i
     return _lib
 
@@ -285,3 +289,60 @@ def slarft(direct, v, tau, t_init=None):
     tt = np.ascontiguousarray(tau, dtype=np.float32)
     lib().orc_slarft(int(direct), n, k, fv, max(1, n), tt if tt.size else np.zeros(1, np.float32), t, max(1, k))
     return _uncm(t, k, k)
+
+
+def _ccm(a):
+    """2-D complex64 column-major, as a flat float32 array."""
+    a = np.asarray(a, dtype=np.complex64)
+    return np.array(a.T, dtype=np.complex64, order="C", copy=True).reshape(-1).view(np.float32).copy()
+
+
+def _unccm(flat, rows, cols):
+    return np.ascontiguousarray(flat.view(np.complex64).reshape(cols, rows).T)
+
+
+def _ctau(tau):
+    t = np.ascontiguousarray(tau, dtype=np.complex64)
+    return (t if t.size else np.zeros(1, np.complex64)).view(np.float32).copy()
+
+
+def cgeqrf(a):
+    """Complex Householder QR of one (m, n) matrix; returns (R and V packed, tau)."""
+    m, n = a.shape
+    f = _ccm(a)
+    tau = np.zeros(2 * max(1, min(m, n)), dtype=np.float32)
+    lib().orc_cgeqrf(m, n, f, max(1, m), tau)
+    return _unccm(f, m, n), tau.view(np.complex64)[: min(m, n)].copy()
+
+
+def cunmqr(side, herm, qr, tau, c):
+    """op(Q) C (side 0) or C op(Q) (side 1); herm 1 applies Q^H."""
+    m, n = c.shape
+    nq = qr.shape[0]
+    fc = _ccm(c)
+    lib().orc_cunmqr(int(side), int(herm), m, n, len(tau), _ccm(qr), max(1, nq), _ctau(tau), fc, max(1, m))
+    return _unccm(fc, m, n)
+
+
+def cungqr(qr, tau, n):
+    """The first n columns of Q (k = len(tau) reflectors in the leading columns of qr)."""
+    m = qr.shape[0]
+    src = np.zeros((m, n), dtype=np.complex64)
+    kk = min(qr.shape[1], n)
+    src[:, :kk] = qr[:, :kk]
+    f = _ccm(src)
+    lib().orc_cungqr(m, n, len(tau), f, max(1, m), _ctau(tau))
+    return _unccm(f, m, n)
+
+
+def cgels(a, b):
+    """Complex least squares (m >= n); returns (X, packed QR, tau, info), info the one-based
+    position of the first zero diagonal entry of R (X then zero) or 0."""
+    m, n = a.shape
+    nrhs = b.shape[1]
+    fa = _ccm(a)
+    x = np.zeros(2 * max(1, n) * max(1, nrhs), dtype=np.float32)
+    tau = np.zeros(2 * max(1, n), dtype=np.float32)
+    info = lib().orc_cgels(m, n, nrhs, fa, max(1, m), _ccm(b), max(1, m), x, max(1, n), tau)
+    return (_unccm(x, max(1, n), max(1, nrhs))[:n, :nrhs], _unccm(fa, m, n), tau.view(np.complex64)[:n].copy(),
+            int(info))

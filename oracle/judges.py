@@ -290,3 +290,76 @@ def gels_ok(a, b, x, x_cpu):
     if not np.isfinite(r):
         return False
     return r <= (max(5 * c, 0.015) if m == n else 10 * c)
+
+
+# ---- complex QR (test/cgeqrf/data/verify_result.py and test/{cgeqrf,cungqr,cunmqr,ccgels}) ----
+
+EPS32 = 2.0 ** -24
+
+
+def _one_norm(x):
+    x = np.abs(np.asarray(x))
+    return float(x.astype(np.float64).sum(axis=0).max()) if x.size else 0.0
+
+
+def cq_from_reflectors(qr, tau):
+    """Q (m x m, complex128) = H(1) ... H(k), H = I - tau v v^H, from packed reflectors."""
+    qr = np.asarray(qr, dtype=np.complex128)
+    m = qr.shape[0]
+    q = np.eye(m, dtype=np.complex128)
+    for i in reversed(range(len(tau))):
+        v = np.zeros(m, dtype=np.complex128)
+        v[i] = 1.0
+        v[i + 1:] = qr[i + 1:, i]
+        q -= complex(tau[i]) * np.outer(v, v.conj() @ q)
+    return q
+
+
+def cqr_ratio(a, q, r):
+    """DQRT01: ||R - Q^H A||_1 / (m ||A||_1 eps32), Q m x k, R k x n (verify_result.py:209-229)."""
+    a = np.asarray(a, dtype=np.complex128)
+    q = np.asarray(q, dtype=np.complex128)
+    den = a.shape[0] * _one_norm(a) * EPS32
+    return _one_norm(np.asarray(r, dtype=np.complex128) - q.conj().T @ a) / den if den > 0 else 0.0
+
+
+def cgeqrf_gate(a, qr, tau):
+    """The reference's three Cgeqrf criteria (verify_result.py:88-100, 232-450), each on Q built
+    by f32 LAPACK cungqr from the packed result: DQRT01 ratio <= min(30, max(10 ratio_cpu, 10))
+    with ratio_cpu from f32 LAPACK cgeqrf + cungqr; A = Q R within 2^-13 + 2^-13 |A| on >= 99 %
+    of entries (or in Frobenius norm) and under the ULP-anchored hard limit; max|Q^H Q - I| <= 1e-4.
+    Returns (passed, ratio, ratio_cpu)."""
+    from scipy.linalg import lapack
+
+    a = np.asarray(a, dtype=np.complex64)
+    m, n = a.shape
+    k = min(m, n)
+
+    def build_q(packed, t):
+        q, _, info = lapack.cungqr(np.asfortranarray(packed[:, :k], dtype=np.complex64), np.asarray(t[:k], np.complex64))
+        assert info == 0
+        return q
+
+    q = build_q(qr, tau)
+    r = np.triu(np.asarray(qr)[:k])
+    ratio = cqr_ratio(a, q, r)
+    cq, ctau, _, info = lapack.cgeqrf(np.asfortranarray(a.copy()))
+    assert info == 0
+    cpu = cqr_ratio(a, build_q(cq, ctau), np.triu(cq[:k]))
+    ok = ratio <= min(30.0, max(10.0 * cpu, 10.0))
+    recon = q.astype(np.complex128) @ r.astype(np.complex128)
+    err = np.abs(a.astype(np.complex128) - recon)
+    tol = 2.0 ** -13 + 2.0 ** -13 * np.abs(a)
+    anchor = np.float32(np.abs(a.reshape(-1)[int(np.argmax(err))]))
+    limit = max(1e-2, 32 * float(np.spacing(np.float32(1.0))),
+                32 * float(np.spacing(anchor)) if np.isfinite(anchor) else 0.0)
+    ok &= err.max() <= limit
+    ok &= (np.count_nonzero(err <= tol) / a.size >= 0.99) or (np.linalg.norm(err) <= np.sqrt((tol ** 2).sum()))
+    ok &= np.abs(q.conj().T.astype(np.complex128) @ q - np.eye(k)).max() <= 1e-4
+    return bool(ok), ratio, cpu
+
+
+def close_2e4(got, want):
+    """The operator tests' tolerance (test/cungqr/test_cungqr.py:39 and its siblings):
+    assert_allclose(rtol=2e-4, atol=3e-5)."""
+    return bool(np.allclose(np.asarray(got, np.complex128), np.asarray(want, np.complex128), rtol=2e-4, atol=3e-5))

@@ -1710,3 +1710,319 @@ void orc_slarft(int direct, int n, int k, const float *v, int ldv, const float *
     }
     free(g);
 }
+
+/* ---------------------------------------------------------------------------------------
+ * Complex QR family (complex64 interleaved, column-major)
+ *
+ * Reflectors follow LAPACK clarfg, as the reference's kernel does
+ * (src/cgeqrf/arch35/cgeqrf_reflector_simd.h:89-170): beta = -copysign(||(alpha; x)||, Re alpha),
+ * tau = ((beta - Re alpha) / beta, -(Im alpha / beta)), v = x / (alpha - beta), tau = 0 when
+ * x is zero and alpha real; Q = H(1)...H(k), H = I - tau v v^H, R = Q^H A.  The schedule and
+ * reductions are the real family's (lane sums over rows, 32-column panels, slarft's T, block
+ * application), with these complex forms, each an explicit FMA sequence:
+ *   conj-dot   acc += conj(v) a : re = fma(v.im, a.im, fma(v.re, a.re, re)),
+ *                                 im = fma(-v.im, a.re, fma(v.re, a.im, im))
+ *   dot        acc += c v       : re = fma(-c.im, v.im, fma(c.re, v.re, re)),
+ *                                 im = fma(c.im, v.re, fma(c.re, v.im, im))
+ *   submul     x - a b          (the LU family's SubMul)
+ *   submulc    x - y conj(v)    : re = fma(-y.im, v.im, fma(-y.re, v.re, x.re)),
+ *                                 im = fma(y.re, v.im, fma(-y.im, v.re, x.im))
+ *   mul        a b              : (fma(-a.im, b.im, a.re b.re), fma(a.im, b.re, a.re b.im))
+ *   mulc       conj(a) b        : (fma(a.im, b.im, a.re b.re), fma(-a.im, b.re, a.re b.im))
+ * The least-squares triangle has a real diagonal, so x_p is divided componentwise by R_pp.
+ * ------------------------------------------------------------------------------------- */
+
+static inline cfl q_conjdot(cfl acc, cfl v, cfl a)
+{
+    cfl r = {fmaf(v.im, a.im, fmaf(v.re, a.re, acc.re)), fmaf(-v.im, a.re, fmaf(v.re, a.im, acc.im))};
+    return r;
+}
+static inline cfl q_dot(cfl acc, cfl c, cfl v)
+{
+    cfl r = {fmaf(-c.im, v.im, fmaf(c.re, v.re, acc.re)), fmaf(c.im, v.re, fmaf(c.re, v.im, acc.im))};
+    return r;
+}
+static inline cfl q_submulc(cfl x, cfl y, cfl v)
+{
+    cfl r = {fmaf(-y.im, v.im, fmaf(-y.re, v.re, x.re)), fmaf(y.re, v.im, fmaf(-y.im, v.re, x.im))};
+    return r;
+}
+static inline cfl q_mul(cfl a, cfl b)
+{
+    cfl r = {fmaf(-a.im, b.im, a.re * b.re), fmaf(a.im, b.re, a.re * b.im)};
+    return r;
+}
+static inline cfl q_mulc(cfl a, cfl b)
+{
+    cfl r = {fmaf(a.im, b.im, a.re * b.re), fmaf(-a.im, b.re, a.re * b.im)};
+    return r;
+}
+static inline cfl q_fma(cfl a, cfl b, cfl acc) /* acc + a b */
+{
+    cfl r = {fmaf(-a.im, b.im, fmaf(a.re, b.re, acc.re)), fmaf(a.im, b.re, fmaf(a.re, b.im, acc.im))};
+    return r;
+}
+static inline cfl q_fmac(cfl a, cfl b, cfl acc) /* acc + conj(a) b */
+{
+    cfl r = {fmaf(a.im, b.im, fmaf(a.re, b.re, acc.re)), fmaf(-a.im, b.re, fmaf(a.re, b.im, acc.im))};
+    return r;
+}
+
+static cfl q_fold(cfl *p)
+{
+    float re[32], im[32];
+    for (int l = 0; l < 32; ++l)
+    {
+        re[l] = p[l].re;
+        im[l] = p[l].im;
+    }
+    cfl r = {qr_lane_fold(re), qr_lane_fold(im)};
+    return r;
+}
+
+static inline cfl cq_v(const cfl *a, int lda, int k, int i, int row)
+{
+    if (row == k + i)
+    {
+        cfl one = {1.0f, 0.0f};
+        return one;
+    }
+    return CAT(a, lda, row, k + i);
+}
+
+static void cq_larfg(int m, cfl *a, int lda, int c, cfl *tau)
+{
+    tau->re = tau->im = 0.0f;
+    float p[32] = {0};
+    for (int row = c + 1; row < m; ++row)
+    {
+        cfl x = CAT(a, lda, row, c);
+        p[row & 31] = fmaf(x.im, x.im, fmaf(x.re, x.re, p[row & 31]));
+    }
+    const float sumsq = qr_lane_fold(p);
+    const cfl al = CAT(a, lda, c, c);
+    if (sumsq == 0.0f && al.im == 0.0f) return;
+    const float norm = sqrtf(al.re * al.re + al.im * al.im + sumsq);
+    const float beta = copysignf(norm, al.re) * -1.0f;
+    tau->re = (beta - al.re) / beta;
+    tau->im = -(al.im / beta);
+    const float dr = al.re - beta, di = al.im;
+    const float den = dr * dr + di * di;
+    for (int row = c + 1; row < m; ++row)
+    {
+        cfl x = CAT(a, lda, row, c);
+        cfl v = {(x.re * dr + x.im * di) / den, (x.im * dr - x.re * di) / den};
+        CAT(a, lda, row, c) = v;
+    }
+    cfl b = {beta, 0.0f};
+    CAT(a, lda, c, c) = b;
+}
+
+static void cq_panel(int m, int k, int kb, cfl *a, int lda, cfl *tau)
+{
+    for (int c = k; c < k + kb; ++c)
+    {
+        cq_larfg(m, a, lda, c, &tau[c]);
+        const cfl t = tau[c];
+        if (t.re == 0.0f && t.im == 0.0f) continue;
+        for (int j = c + 1; j < k + kb; ++j)
+        {
+            cfl p[32];
+            memset(p, 0, sizeof p);
+            for (int row = c; row < m; ++row)
+            {
+                cfl v = row == c ? (cfl){1.0f, 0.0f} : CAT(a, lda, row, c);
+                p[row & 31] = q_conjdot(p[row & 31], v, CAT(a, lda, row, j));
+            }
+            const cfl w = q_mulc(t, q_fold(p));
+            for (int row = c; row < m; ++row)
+            {
+                cfl v = row == c ? (cfl){1.0f, 0.0f} : CAT(a, lda, row, c);
+                CAT(a, lda, row, j) = c_submul(CAT(a, lda, row, j), v, w);
+            }
+        }
+    }
+}
+
+/* T (kb x kb upper, ld 32) of the panel's reflectors: T(i,i) = tau_i, T(0:i, i) = T(0:i, 0:i) d,
+ * d_r = -tau_i (v_r^H v_i). */
+static void cq_larft(int nq, int k, int kb, const cfl *a, int lda, const cfl *tau, cfl *T)
+{
+    cfl d[QR_NB];
+    for (int i = 0; i < kb; ++i)
+    {
+        const cfl ti = tau[k + i];
+        if (ti.re == 0.0f && ti.im == 0.0f)
+        {
+            for (int r = 0; r <= i; ++r) T[i * QR_NB + r] = (cfl){0.0f, 0.0f};
+            continue;
+        }
+        const cfl nt = {-ti.re, -ti.im};
+        for (int r = 0; r < i; ++r)
+        {
+            cfl p[32];
+            memset(p, 0, sizeof p);
+            for (int row = k + i; row < nq; ++row)
+                p[row & 31] = q_conjdot(p[row & 31], CAT(a, lda, row, k + r), cq_v(a, lda, k, i, row));
+            d[r] = q_mul(nt, q_fold(p));
+        }
+        for (int r = 0; r < i; ++r)
+        {
+            cfl acc = {0.0f, 0.0f};
+            for (int q = r; q < i; ++q) acc = q_fma(T[q * QR_NB + r], d[q], acc);
+            T[i * QR_NB + r] = acc;
+        }
+        T[i * QR_NB + i] = ti;
+    }
+}
+
+/* Left: C = (I - V op(T) V^H) C, op(T) = T^H when herm (Q^H C), T otherwise (Q C). */
+static void cq_apply_left(int m, int k, int kb, const cfl *a, int lda, const cfl *T, int herm, cfl *c, int ldc,
+                          int ncols)
+{
+    for (int j = 0; j < ncols; ++j)
+    {
+        cfl w[QR_NB], w2[QR_NB];
+        for (int i = 0; i < kb; ++i)
+        {
+            cfl p[32];
+            memset(p, 0, sizeof p);
+            for (int row = k + i; row < m; ++row)
+                p[row & 31] = q_conjdot(p[row & 31], cq_v(a, lda, k, i, row), CAT(c, ldc, row, j));
+            w[i] = q_fold(p);
+        }
+        for (int i = 0; i < kb; ++i)
+        {
+            cfl acc = {0.0f, 0.0f};
+            if (herm)
+                for (int q = 0; q <= i; ++q) acc = q_fmac(T[i * QR_NB + q], w[q], acc);
+            else
+                for (int q = i; q < kb; ++q) acc = q_fma(T[q * QR_NB + i], w[q], acc);
+            w2[i] = acc;
+        }
+        for (int row = k; row < m; ++row)
+        {
+            cfl x = CAT(c, ldc, row, j);
+            for (int i = 0; i < kb && i <= row - k; ++i) x = c_submul(x, cq_v(a, lda, k, i, row), w2[i]);
+            CAT(c, ldc, row, j) = x;
+        }
+    }
+}
+
+/* Right: C = C (I - V op(T) V^H), op(T) = T (C Q) or T^H when herm (C Q^H). */
+static void cq_apply_right(int nq, int k, int kb, const cfl *a, int lda, const cfl *T, int herm, cfl *c, int ldc,
+                           int nrows)
+{
+    for (int r = 0; r < nrows; ++r)
+    {
+        cfl y[QR_NB], y2[QR_NB];
+        for (int i = 0; i < kb; ++i)
+        {
+            cfl p[32];
+            memset(p, 0, sizeof p);
+            for (int col = k + i; col < nq; ++col)
+                p[col & 31] = q_dot(p[col & 31], CAT(c, ldc, r, col), cq_v(a, lda, k, i, col));
+            y[i] = q_fold(p);
+        }
+        for (int i = 0; i < kb; ++i)
+        {
+            cfl acc = {0.0f, 0.0f};
+            if (!herm)
+                for (int q = 0; q <= i; ++q) acc = q_fma(T[i * QR_NB + q], y[q], acc);
+            else
+                for (int q = i; q < kb; ++q) acc = q_fmac(T[q * QR_NB + i], y[q], acc);
+            y2[i] = acc;
+        }
+        for (int col = k; col < nq; ++col)
+        {
+            cfl x = CAT(c, ldc, r, col);
+            for (int i = 0; i < kb && i <= col - k; ++i) x = q_submulc(x, y2[i], cq_v(a, lda, k, i, col));
+            CAT(c, ldc, r, col) = x;
+        }
+    }
+}
+
+void orc_cgeqrf(int m, int n, float *af, int lda, float *tauf)
+{
+    cfl *a = (cfl *)af, *tau = (cfl *)tauf;
+    const int lim = m < n ? m : n;
+    cfl T[QR_NB * QR_NB];
+    for (int k = 0; k < lim; k += QR_NB)
+    {
+        const int kb = lim - k < QR_NB ? lim - k : QR_NB;
+        cq_panel(m, k, kb, a, lda, tau);
+        if (k + kb < n)
+        {
+            cq_larft(m, k, kb, a, lda, tau, T);
+            cq_apply_left(m, k, kb, a, lda, T, 1, a + (int64_t)(k + kb) * lda, lda, n - k - kb);
+        }
+    }
+}
+
+/* side 0 left (nq = m), 1 right (nq = n); herm 0 applies Q, 1 applies Q^H. */
+void orc_cunmqr(int side, int herm, int m, int n, int k, const float *af, int lda, const float *tauf, float *cf,
+                int ldc)
+{
+    const cfl *a = (const cfl *)af, *tau = (const cfl *)tauf;
+    cfl *c = (cfl *)cf;
+    const int nq = side == 0 ? m : n;
+    cfl T[QR_NB * QR_NB];
+    const int npan = (k + QR_NB - 1) / QR_NB;
+    const int forward = (side == 0) == (herm != 0);
+    for (int s = 0; s < npan; ++s)
+    {
+        const int pi = forward ? s : npan - 1 - s;
+        const int k0 = pi * QR_NB, kb = k - k0 < QR_NB ? k - k0 : QR_NB;
+        cq_larft(nq, k0, kb, a, lda, tau, T);
+        if (side == 0)
+            cq_apply_left(m, k0, kb, a, lda, T, herm, c, ldc, n);
+        else
+            cq_apply_right(n, k0, kb, a, lda, T, herm, c, ldc, m);
+    }
+}
+
+void orc_cungqr(int m, int n, int k, float *af, int lda, const float *tauf)
+{
+    cfl *a = (cfl *)af;
+    cfl *v = (cfl *)malloc(sizeof(cfl) * (size_t)(m > 0 ? m : 1) * (size_t)(k > 0 ? k : 1));
+    for (int j = 0; j < k; ++j)
+        for (int r = 0; r < m; ++r) v[(int64_t)j * m + r] = CAT(a, lda, r, j);
+    for (int j = 0; j < n; ++j)
+        for (int r = 0; r < m; ++r) CAT(a, lda, r, j) = (cfl){r == j ? 1.0f : 0.0f, 0.0f};
+    orc_cunmqr(0, 0, m, n, k, (const float *)v, m, tauf, af, lda);
+    free(v);
+}
+
+/* Returns the one-based position of the first zero diagonal entry of R (X then untouched),
+ * as the reference's back substitution reports it (src/ccgels/arch35/ccgels_kernel.cpp:150-176,
+ * FindZeroDiagonal), else 0. */
+int orc_cgels(int m, int n, int nrhs, float *af, int lda, const float *bf, int ldb, float *xf, int ldx, float *tauf)
+{
+    cfl *a = (cfl *)af, *x = (cfl *)xf;
+    const cfl *b = (const cfl *)bf;
+    cfl *y = (cfl *)malloc(sizeof(cfl) * (size_t)(m > 0 ? m : 1) * (size_t)(nrhs > 0 ? nrhs : 1));
+    for (int j = 0; j < nrhs; ++j)
+        for (int r = 0; r < m; ++r) y[(int64_t)j * m + r] = CAT(b, ldb, r, j);
+    orc_cgeqrf(m, n, af, lda, tauf);
+    orc_cunmqr(0, 1, m, nrhs, n, af, lda, tauf, (float *)y, m);
+    for (int p = 0; p < n; ++p)
+        if (CAT(a, lda, p, p).re == 0.0f && CAT(a, lda, p, p).im == 0.0f)
+        {
+            free(y);
+            return p + 1;
+        }
+    for (int j = 0; j < nrhs; ++j)
+    {
+        cfl *yj = y + (int64_t)j * m;
+        for (int p = n - 1; p >= 0; --p)
+        {
+            const float d = CAT(a, lda, p, p).re;
+            yj[p].re = yj[p].re / d;
+            yj[p].im = yj[p].im / d;
+            for (int i = 0; i < p; ++i) yj[i] = c_submul(yj[i], CAT(a, lda, i, p), yj[p]);
+        }
+        for (int r = 0; r < n; ++r) CAT(x, ldx, r, j) = yj[r];
+    }
+    free(y);
+    return 0;
+}
