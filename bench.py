@@ -1135,13 +1135,15 @@ def measure_complex_lu(handle, args, steps=3):
 
 
 def measure_qr(handle, args, steps=3):
-    """The real QR family: aclsolverSgeqrf of one 4096 x 4096 and one 2048 x 2048 N(0,1)
-    matrix, and aclsolverSSgels of a 4096 x 4096 system with one right-hand side (device time
-    per call, inputs restored before each).  `case_list_us` is the time the reference's own
+    """The QR families: aclsolverSgeqrf of one 4096 x 4096 and one 2048 x 2048 N(0,1)
+    matrix, aclsolverSSgels of a 4096 x 4096 system with one right-hand side, and their complex
+    counterparts aclsolverCgeqrf / aclsolverCCgels at 4096 (device time per call, inputs
+    restored before each).  `case_list_us` is the time the reference's own
     case lists carry for the same shape (test/sgeqrf/data/sgeqrf_cases.txt,
     test/sgels/data/sgels_cases.txt, a cuSOLVER run on the hardware those lists were made on)."""
     import ctypes as C
 
+    import numpy as np
     import torch
 
     import aclsolver
@@ -1205,12 +1207,48 @@ def measure_qr(handle, args, steps=3):
                lambda: a.copy_(a0))
     out["sgels_4096"] = {"workload": "4096 x 4096 system, 1 right-hand side: aclsolverSSgels", "ms": round(ms, 3),
                          "case_list_us": 30675.3}
+    # complex family: Cgeqrf of one 4096 x 4096 matrix, CCgels of a 4096 x 4096 system (complex64,
+    # real and imaginary parts N(0,1)); each call includes the reference's non-finite input screen
+    a0 = torch.randn(2 * n * n, device="cuda", generator=g)
+    a = torch.empty_like(a0)
+    tau = torch.empty(2 * n, device="cuda")
+    work = torch.empty(2 * 1024, device="cuda")
+    ms = timed(lambda: aclsolver.check(lib.aclsolverCgeqrf(handle.value, n, n, a.data_ptr(), n, tau.data_ptr(),
+                                                           work.data_ptr(), 1024, info.data_ptr())),
+               lambda: a.copy_(a0))
+    assert int(info.item()) == 0
+    flops = 16.0 * n ** 3 / 3  # 4 n^3 / 3 complex multiply-adds, 4 real each
+    out["cgeqrf_4096"] = {"workload": f"one {n} x {n} complex64 N(0,1) matrix: aclsolverCgeqrf", "ms": round(ms, 3),
+                          "gflops": round(flops / (ms * 1e-3) / 1e9, 1),
+                          "roofline": {"bound": "fp32 FMA (CUDA cores)", "frac": round(flops / ms / 1e9 / fp32, 4),
+                                       "peak_tflops": fp32}}
+    if args is not None and args.cpu_seconds > 0:
+        from scipy.linalg import lapack
+
+        a_h = a0.cpu().numpy().view(np.complex64).reshape(n, n)
+        t0 = time.perf_counter()
+        lapack.cgeqrf(a_h)
+        out["cgeqrf_4096"]["cpu_baseline"] = {"ms": round((time.perf_counter() - t0) * 1e3, 1),
+                                              "kind": "scipy LAPACK cgeqrf (OpenBLAS threads)"}
+    b = torch.randn(2 * n, device="cuda", generator=g)
+    x = torch.empty(2 * n, device="cuda")
+    aclsolver.check(lib.aclsolverCCgels_bufferSize(handle.value, n, n, 1, a.data_ptr(), n, b.data_ptr(), n,
+                                                   x.data_ptr(), n, None, C.byref(lw)))
+    work = torch.empty(lw.value // 4 + 1, device="cuda")
+    ms = timed(lambda: aclsolver.check(lib.aclsolverCCgels(handle.value, n, n, 1, a.data_ptr(), n, b.data_ptr(), n,
+                                                           x.data_ptr(), n, work.data_ptr(), lw.value,
+                                                           C.byref(niter), info.data_ptr())),
+               lambda: a.copy_(a0))
+    assert int(info.item()) == 0
+    out["ccgels_4096"] = {"workload": "4096 x 4096 complex64 system, 1 right-hand side: aclsolverCCgels",
+                          "ms": round(ms, 3)}
     return out
 
 
 def run_profile_qr():
-    """aclsolverSgeqrf of one 4096 x 4096 N(0,1) matrix and aclsolverSSgels of a 2048 x 2048
-    system with 4 right-hand sides, once each, for an ncu capture."""
+    """aclsolverSgeqrf of one 4096 x 4096 N(0,1) matrix, aclsolverSSgels of a 2048 x 2048
+    system with 4 right-hand sides and aclsolverCgeqrf of one 2048 x 2048 complex64 matrix,
+    once each, for an ncu capture."""
     import ctypes as C
 
     import torch
@@ -1238,6 +1276,12 @@ def run_profile_qr():
     niter = C.c_int(0)
     aclsolver.check(lib.aclsolverSSgels(handle.value, n, n, r, a.data_ptr(), n, b.data_ptr(), n, x.data_ptr(), n,
                                         ws.data_ptr(), lw.value, C.byref(niter), info.data_ptr()))
+    n = 2048
+    a = torch.randn(2 * n * n, device="cuda", generator=g)
+    tau = torch.empty(2 * n, device="cuda")
+    work = torch.empty(2 * 1024, device="cuda")
+    aclsolver.check(lib.aclsolverCgeqrf(handle.value, n, n, a.data_ptr(), n, tau.data_ptr(), work.data_ptr(), 1024,
+                                        info.data_ptr()))
     torch.cuda.synchronize()
     handle.close()
     print("profile-qr done", flush=True)

@@ -69,8 +69,12 @@ __device__ __forceinline__ float2 fold2(float2 p) { return make_float2(fold1(p.x
 
 __device__ __forceinline__ bool czero2(float2 v) { return v.x == 0.0f && v.y == 0.0f; }
 
-// Panel columns [k, k + kb) of rows [k, m); SMEM keeps the panel in shared memory.
-template <bool SMEM>
+// Panel columns [k, k + kb) of rows [k, m).  MODE 1: the panel is staged in shared memory.
+// MODE 2: the panel stays in A and two column buffers in shared memory mirror the reflector
+// column c and the next column c + 1 (written by the warp that updates it), so only the
+// target columns are read from A.  MODE 0 (more rows than the buffers hold): everything is
+// read from A.  Same arithmetic in every mode.
+template <int MODE>
 __global__ void __launch_bounds__(PANEL_THREADS) cq_panel_kernel(float2 *A, int lda, int m, int k, int kb, float2 *tau)
 {
     extern __shared__ float2 sp[];
@@ -80,13 +84,14 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_panel_kernel(float2 *A, int 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int H = m - k;
     auto at = [&](int j, int row) -> float2 & {
-        return SMEM ? sp[(int64_t)(j - k) * H + (row - k)] : A[(int64_t)j * lda + row];
+        return MODE == 1 ? sp[(int64_t)(j - k) * H + (row - k)] : A[(int64_t)j * lda + row];
     };
-    if (SMEM)
-    {
+    auto col = [&](int j, int row) -> float2 & { return MODE == 2 ? sp[(j & 1) * H + (row - k)] : at(j, row); };
+    if (MODE == 1)
         for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) sp[idx] = A[(int64_t)(k + idx / H) * lda + k + idx % H];
-        __syncthreads();
-    }
+    if (MODE == 2)
+        for (int row = k + tid; row < m; row += PANEL_THREADS) col(k, row) = A[(int64_t)k * lda + row];
+    __syncthreads();
     constexpr int U = 8;
     for (int c = k; c < k + kb; ++c)
     {
@@ -100,7 +105,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_panel_kernel(float2 *A, int 
                 for (int u = 0; u < U; ++u)
                 {
                     const int row = base + 32 * u + lane;
-                    x[u] = row > c && row < m ? at(c, row) : make_float2(0.0f, 0.0f);
+                    x[u] = row > c && row < m ? col(c, row) : make_float2(0.0f, 0.0f);
                 }
 #pragma unroll
                 for (int u = 0; u < U; ++u)
@@ -112,7 +117,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_panel_kernel(float2 *A, int 
             const float sumsq = fold1(p);
             if (lane == 0)
             {
-                const float2 al = at(c, c);
+                const float2 al = col(c, c);
                 float2 t = make_float2(0.0f, 0.0f);
                 int apply = 0;
                 if (!(sumsq == 0.0f && al.y == 0.0f))
@@ -140,9 +145,11 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_panel_kernel(float2 *A, int 
             const float dr = s_dr, di = s_di, den = s_den;
             for (int row = c + 1 + tid; row < m; row += PANEL_THREADS)
             {
-                const float2 x = at(c, row);
-                at(c, row) = make_float2(div_rn(add_rn(mul_rn(x.x, dr), mul_rn(x.y, di)), den),
-                                         div_rn(sub_rn(mul_rn(x.y, dr), mul_rn(x.x, di)), den));
+                const float2 x = col(c, row);
+                const float2 v = make_float2(div_rn(add_rn(mul_rn(x.x, dr), mul_rn(x.y, di)), den),
+                                             div_rn(sub_rn(mul_rn(x.y, dr), mul_rn(x.x, di)), den));
+                at(c, row) = v;
+                if (MODE == 2) col(c, row) = v;
             }
         }
         __syncthreads();
@@ -152,108 +159,109 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_panel_kernel(float2 *A, int 
             float2 p = make_float2(0.0f, 0.0f);
             for (int base = c & ~31; base < m; base += 32 * U)
             {
-                float2 v[U], x[U];
+                float2 x[U];
 #pragma unroll
                 for (int u = 0; u < U; ++u)
                 {
                     const int row = base + 32 * u + lane;
-                    const bool ok = row >= c && row < m;
-                    v[u] = ok ? (row == c ? make_float2(1.0f, 0.0f) : at(c, row)) : make_float2(0.0f, 0.0f);
-                    x[u] = ok ? at(j, row) : make_float2(0.0f, 0.0f);
+                    x[u] = row >= c && row < m ? at(j, row) : make_float2(0.0f, 0.0f);
                 }
 #pragma unroll
                 for (int u = 0; u < U; ++u)
                 {
                     const int row = base + 32 * u + lane;
-                    if (row >= c && row < m) p = cq_conjdot(p, v[u], x[u]);
+                    if (row >= c && row < m)
+                        p = cq_conjdot(p, row == c ? make_float2(1.0f, 0.0f) : col(c, row), x[u]);
                 }
             }
             const float2 w = cq_mulc(t, fold2(p));
             for (int base = c & ~31; base < m; base += 32 * U)
             {
-                float2 v[U], x[U];
+                float2 x[U];
 #pragma unroll
                 for (int u = 0; u < U; ++u)
                 {
                     const int row = base + 32 * u + lane;
-                    const bool ok = row >= c && row < m;
-                    v[u] = ok ? (row == c ? make_float2(1.0f, 0.0f) : at(c, row)) : make_float2(0.0f, 0.0f);
-                    x[u] = ok ? at(j, row) : make_float2(0.0f, 0.0f);
+                    x[u] = row >= c && row < m ? at(j, row) : make_float2(0.0f, 0.0f);
                 }
 #pragma unroll
                 for (int u = 0; u < U; ++u)
                 {
                     const int row = base + 32 * u + lane;
-                    if (row >= c && row < m) at(j, row) = clu::csubmul(x[u], v[u], w);
+                    if (row >= c && row < m)
+                    {
+                        const float2 y = clu::csubmul(x[u], row == c ? make_float2(1.0f, 0.0f) : col(c, row), w);
+                        at(j, row) = y;
+                        if (MODE == 2 && j == c + 1) col(j, row) = y;
+                    }
                 }
             }
         }
+        else if (MODE == 2 && !apply && warp == 1 && j < k + kb)
+            for (int row = c + 1 + lane; row < m; row += 32) col(j, row) = at(j, row);
         __syncthreads();
     }
-    if (SMEM)
+    if (MODE == 1)
         for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) A[(int64_t)(k + idx / H) * lda + k + idx % H] = sp[idx];
 }
 
-// T (kb x kb upper, ld NB) of the reflectors at columns [k, k + kb), length nq.
-__global__ void __launch_bounds__(PANEL_THREADS) cq_larft_kernel(const float2 *A, int lda, int nq, int k, int kb,
-                                                                 const float2 *tau, float2 *T)
+// The reflector products of a panel for T: d(i, r) = -tau_i (v_r^H v_i) for r < i, one warp
+// per pair, each a lane sum in ascending rows, stored below T's diagonal (T[r * NB + i]);
+// cq_tri_kernel then forms T's upper triangle from them.
+constexpr int GRAM_WARPS = 8;
+
+__global__ void __launch_bounds__(GRAM_WARPS * 32) cq_gram_kernel(const float2 *A, int lda, int nq, int k, int kb,
+                                                                  const float2 *tau, float2 *T)
 {
-    constexpr int ROWS = 64;
-    __shared__ float2 vs[ROWS][NB + 1];
-    __shared__ float2 d[NB][NB];   // d[i][r] = -tau_i (v_r^H v_i)
+    const int lane = threadIdx.x & 31;
+    const int pr = blockIdx.x * GRAM_WARPS + (threadIdx.x >> 5);
+    if (pr >= kb * (kb - 1) / 2) return;
+    int i = 1, r = pr;
+    while (r >= i)
+    {
+        r -= i;
+        ++i;
+    }
+    const float2 *vr = A + (int64_t)(k + r) * lda, *vi = A + (int64_t)(k + i) * lda;
+    const int first = k + i;
+    constexpr int U = 8;
+    float2 p = make_float2(0.0f, 0.0f);
+    for (int base = first & ~31; base < nq; base += 32 * U)
+    {
+        float2 a[U], b[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const int row = base + 32 * u + lane;
+            const bool ok = row >= first && row < nq;
+            a[u] = ok ? vr[row] : make_float2(0.0f, 0.0f);
+            b[u] = ok ? (row == first ? make_float2(1.0f, 0.0f) : vi[row]) : make_float2(0.0f, 0.0f);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const int row = base + 32 * u + lane;
+            if (row >= first && row < nq) p = cq_conjdot(p, a[u], b[u]);
+        }
+    }
+    const float2 dot = fold2(p);
+    if (lane == 0)
+    {
+        const float2 ti = tau[k + i];
+        T[r * NB + i] = cq_mul(make_float2(-ti.x, -ti.y), dot);
+    }
+}
+
+// T (kb x kb upper, ld NB): T(i, i) = tau_i, T(0:i, i) = T(0:i, 0:i) d(i, 0:i) (a chain in
+// ascending q), a zero column where tau_i = 0.
+__global__ void __launch_bounds__(32) cq_tri_kernel(int k, int kb, const float2 *tau, float2 *T)
+{
+    __shared__ float2 d[NB][NB];   // d[i][q] = d(i, q)
     __shared__ float2 ts[NB][NB];  // ts[i][r] = T(r, i)
-    constexpr int PER_WARP = (NB * (NB - 1) / 2 + 31) / 32;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int pairs = kb * (kb - 1) / 2;
-    int pr_r[PER_WARP], pr_i[PER_WARP];
-    float2 p[PER_WARP];
-#pragma unroll
-    for (int u = 0; u < PER_WARP; ++u)
-    {
-        const int pr = warp + 32 * u;
-        int i = 1, rem = pr;
-        while (rem >= i)
-        {
-            rem -= i;
-            ++i;
-        }
-        pr_r[u] = pr < pairs ? rem : 0;
-        pr_i[u] = pr < pairs ? i : NB;
-        p[u] = make_float2(0.0f, 0.0f);
-    }
-    for (int base0 = (k + 1) & ~31; base0 < nq; base0 += ROWS)
-    {
-        __syncthreads();
-        for (int idx = tid; idx < ROWS * kb; idx += PANEL_THREADS)
-        {
-            const int rr = idx % ROWS, i = idx / ROWS, row = base0 + rr;
-            vs[rr][i] = row < nq && row > k + i ? A[(int64_t)(k + i) * lda + row]
-                                                : make_float2(row == k + i ? 1.0f : 0.0f, 0.0f);
-        }
-        __syncthreads();
-        for (int cc = 0; cc < ROWS; cc += 32)
-        {
-            const int row = base0 + cc + lane;
-            if (row < nq)
-            {
-#pragma unroll
-                for (int u = 0; u < PER_WARP; ++u)
-                    if (pr_i[u] < kb && row >= k + pr_i[u])
-                        p[u] = cq_conjdot(p[u], vs[cc + lane][pr_r[u]], vs[cc + lane][pr_i[u]]);
-            }
-        }
-    }
-#pragma unroll
-    for (int u = 0; u < PER_WARP; ++u)
-    {
-        const float2 dot = fold2(p[u]);
-        if (lane == 0 && pr_i[u] < kb)
-        {
-            const float2 ti = tau[k + pr_i[u]];
-            d[pr_i[u]][pr_r[u]] = cq_mul(make_float2(-ti.x, -ti.y), dot);
-        }
-    }
-    __syncthreads();
+    const int tid = threadIdx.x;
+    for (int i = 0; i < kb; ++i)
+        if (tid < i) d[i][tid] = T[tid * NB + i];
+    __syncwarp();
     for (int i = 0; i < kb; ++i)
     {
         const float2 ti = tau[k + i];
@@ -270,13 +278,10 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_larft_kernel(const float2 *A
                 ts[i][tid] = acc;
             }
         }
-        __syncthreads();
+        __syncwarp();
     }
-    for (int idx = tid; idx < kb * kb; idx += PANEL_THREADS)
-    {
-        const int r = idx % kb, i = idx / kb;
-        if (r <= i) T[i * NB + r] = ts[i][r];
-    }
+    for (int i = 0; i < kb; ++i)
+        if (tid <= i) T[i * NB + tid] = ts[i][tid];
 }
 
 // LEFT: C = (I - V op(T) V^H) C, one warp per column of C; RIGHT: C = C (I - V op(T) V^H), one
@@ -468,6 +473,21 @@ __global__ void cq_identity_kernel(float2 *A, int lda, int m, int n)
     A[(int64_t)c * lda + r] = make_float2(r == c ? 1.0f : 0.0f, 0.0f);
 }
 
+cudaError_t cq_larft(const float2 *A, int lda, int nq, int k, int kb, const float2 *tau, float2 *T,
+                     cudaStream_t stream)
+{
+    const int pairs = kb * (kb - 1) / 2;
+    if (pairs > 0)
+    {
+        cq_gram_kernel<<<(pairs + GRAM_WARPS - 1) / GRAM_WARPS, GRAM_WARPS * 32, 0, stream>>>(A, lda, nq, k, kb, tau,
+                                                                                             T);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    cq_tri_kernel<<<1, 32, 0, stream>>>(k, kb, tau, T);
+    return cudaGetLastError();
+}
+
 cudaError_t cq_apply(bool right, bool herm, const float2 *V, int ldv, int nq, int k, int kb, const float2 *T,
                      float2 *C, int64_t ldc, int count, cudaStream_t stream)
 {
@@ -492,9 +512,14 @@ cudaError_t launch_cgeqrf(float2 *A, int lda, int m, int n, float2 *tau, float2 
     cudaError_t e = once_per_device(g_cq_attr,
                                     []
                                     {
-                                        return cudaFuncSetAttribute(cq_panel_kernel<true>,
-                                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                                    PANEL_SMEM_ELEMS * (int)sizeof(float2));
+                                        cudaError_t r = cudaFuncSetAttribute(
+                                            cq_panel_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            PANEL_SMEM_ELEMS * (int)sizeof(float2));
+                                        if (r == cudaSuccess)
+                                            r = cudaFuncSetAttribute(cq_panel_kernel<2>,
+                                                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                                     PANEL_SMEM_ELEMS * (int)sizeof(float2));
+                                        return r;
                                     });
     const int lim = std::min(m, n);
     for (int k = 0; k < lim && e == cudaSuccess; k += NB)
@@ -502,14 +527,16 @@ cudaError_t launch_cgeqrf(float2 *A, int lda, int m, int n, float2 *tau, float2 
         const int kb = std::min(NB, lim - k);
         const int64_t elems = (int64_t)(m - k) * kb;
         if (elems <= PANEL_SMEM_ELEMS)
-            cq_panel_kernel<true><<<1, PANEL_THREADS, (size_t)elems * sizeof(float2), stream>>>(A, lda, m, k, kb, tau);
+            cq_panel_kernel<1><<<1, PANEL_THREADS, (size_t)elems * sizeof(float2), stream>>>(A, lda, m, k, kb, tau);
+        else if (2 * (int64_t)(m - k) <= PANEL_SMEM_ELEMS)
+            cq_panel_kernel<2><<<1, PANEL_THREADS, (size_t)2 * (m - k) * sizeof(float2), stream>>>(A, lda, m, k, kb,
+                                                                                                     tau);
         else
-            cq_panel_kernel<false><<<1, PANEL_THREADS, 0, stream>>>(A, lda, m, k, kb, tau);
+            cq_panel_kernel<0><<<1, PANEL_THREADS, 0, stream>>>(A, lda, m, k, kb, tau);
         e = cudaGetLastError();
         if (e == cudaSuccess && k + kb < n)
         {
-            cq_larft_kernel<<<1, PANEL_THREADS, 0, stream>>>(A, lda, m, k, kb, tau, T);
-            e = cudaGetLastError();
+            e = cq_larft(A, lda, m, k, kb, tau, T, stream);
             if (e == cudaSuccess)
                 e = cq_apply(false, true, A, lda, m, k, kb, T, A + (int64_t)(k + kb) * lda, lda, n - k - kb, stream);
         }
@@ -529,8 +556,7 @@ cudaError_t launch_cunmqr(int side, int herm, int m, int n, int k, const float2 
     {
         const int pi = forward ? s : npan - 1 - s;
         const int k0 = pi * NB, kb = std::min(NB, k - k0);
-        cq_larft_kernel<<<1, PANEL_THREADS, 0, stream>>>(A, lda, nq, k0, kb, tau, T);
-        e = cudaGetLastError();
+        e = cq_larft(A, lda, nq, k0, kb, tau, T, stream);
         if (e == cudaSuccess) e = cq_apply(right, h, A, lda, nq, k0, kb, T, C, ldc, count, stream);
     }
     return e;

@@ -9,9 +9,11 @@
 // lane r mod 32 (an FMA chain in ascending row order), and a warp butterfly
 // (v += shfl_xor(v, off), off = 16 .. 1) combines the lanes, so the results do not depend
 // on the grid and the CPU oracle restates them exactly:
-//   qr_panel_kernel      one block factors a panel (in shared memory when it fits): warp 0
-//                        forms the reflector, the other warps apply it to one column each
-//   qr_larft_kernel      T of the panel (forward, columnwise)
+//   qr_panel_kernel      one block factors a panel (in shared memory when it fits, else with
+//                        the current and next columns mirrored there): warp 0 forms the
+//                        reflector, the other warps apply it to one column each
+//   qr_gram_kernel /     T of the panel (forward, columnwise): the reflector products one warp
+//   qr_tri_kernel        per pair across the grid, then slarft's recurrence in one warp
 //   qr_apply_kernel      one warp per column (left) or row (right) of C: W = V^T c by lane
 //                        sums over 32-row chunks of V staged in shared memory, W2 = op(T) W,
 //                        then c -= V W2 with an FMA chain over the reflectors
@@ -41,8 +43,11 @@ __device__ __forceinline__ float lane_fold(float p)
 }
 
 // Panel columns [k, k + kb) of rows [k, m).  SMEM: the panel is staged in shared memory
-// (pitch m - k); otherwise it stays in A (L2-resident) and each lane batches four loads
-// ahead of its FMA chain.  Same arithmetic either way.
+// (pitch m - k).  Otherwise it stays in A (L2-resident) and two column buffers in shared
+// memory mirror the reflector column c and the next column c + 1 (written by the warp that
+// updates it), so the norm and the reflector reads come from shared memory and only the
+// target columns are read from A, twelve loads ahead of each lane's FMA chain.  Same
+// arithmetic either way.
 constexpr int PANEL_SMEM_FLOATS = 50 * 1024;
 
 template <bool SMEM>
@@ -53,15 +58,17 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_panel_kernel(float *A, int l
     __shared__ int s_apply;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int H = m - k;
+    // the panel (SMEM) or the column buffers: column c lives in sp + (c & 1) * H
     auto at = [&](int j, int row) -> float & {
         return SMEM ? sp[(int64_t)(j - k) * H + (row - k)] : A[(int64_t)j * lda + row];
     };
+    auto col = [&](int j, int row) -> float & { return SMEM ? at(j, row) : sp[(j & 1) * H + (row - k)]; };
     if (SMEM)
-    {
         for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) sp[idx] = A[(int64_t)(k + idx / H) * lda + k + idx % H];
-        __syncthreads();
-    }
-    constexpr int U = 8;
+    else
+        for (int row = k + tid; row < m; row += PANEL_THREADS) col(k, row) = A[(int64_t)k * lda + row];
+    __syncthreads();
+    constexpr int U = 8, UX = SMEM ? 8 : 12;
     for (int c = k; c < k + kb; ++c)
     {
         if (warp == 0)
@@ -74,7 +81,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_panel_kernel(float *A, int l
                 for (int u = 0; u < U; ++u)
                 {
                     const int row = base + 32 * u + lane;
-                    x[u] = row > c && row < m ? at(c, row) : 0.0f;
+                    x[u] = row > c && row < m ? col(c, row) : 0.0f;
                 }
 #pragma unroll
                 for (int u = 0; u < U; ++u)
@@ -90,7 +97,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_panel_kernel(float *A, int l
                 int apply = 0;
                 if (m - c > 1 && sumsq != 0.0f)
                 {
-                    const float alpha = at(c, c);
+                    const float alpha = col(c, c);
                     const float norm = sqrt_rn(add_rn(mul_rn(alpha, alpha), sumsq));
                     const float beta = alpha >= 0.0f ? -norm : norm;
                     t = div_rn(sub_rn(beta, alpha), beta);
@@ -110,114 +117,118 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_panel_kernel(float *A, int l
         if (apply)
         {
             const float scale = s_scale;
-            for (int row = c + 1 + tid; row < m; row += PANEL_THREADS) at(c, row) = mul_rn(at(c, row), scale);
+            for (int row = c + 1 + tid; row < m; row += PANEL_THREADS)
+            {
+                const float v = mul_rn(col(c, row), scale);
+                at(c, row) = v;
+                if (!SMEM) col(c, row) = v;
+            }
         }
         __syncthreads();
         const int j = c + warp;
         if (apply && warp >= 1 && j < k + kb)
         {
             float p = 0.0f;
-            for (int base = c & ~31; base < m; base += 32 * U)
+            for (int base = c & ~31; base < m; base += 32 * UX)
             {
-                float v[U], x[U];
+                float x[UX];
 #pragma unroll
-                for (int u = 0; u < U; ++u)
+                for (int u = 0; u < UX; ++u)
                 {
                     const int row = base + 32 * u + lane;
-                    const bool ok = row >= c && row < m;
-                    v[u] = ok ? (row == c ? 1.0f : at(c, row)) : 0.0f;
-                    x[u] = ok ? at(j, row) : 0.0f;
+                    x[u] = row >= c && row < m ? at(j, row) : 0.0f;
                 }
 #pragma unroll
-                for (int u = 0; u < U; ++u)
+                for (int u = 0; u < UX; ++u)
                 {
                     const int row = base + 32 * u + lane;
-                    if (row >= c && row < m) p = fma_rn(v[u], x[u], p);
+                    if (row >= c && row < m) p = fma_rn(row == c ? 1.0f : col(c, row), x[u], p);
                 }
             }
             const float w = mul_rn(t, lane_fold(p));
-            for (int base = c & ~31; base < m; base += 32 * U)
+            for (int base = c & ~31; base < m; base += 32 * UX)
             {
-                float v[U], x[U];
+                float x[UX];
 #pragma unroll
-                for (int u = 0; u < U; ++u)
+                for (int u = 0; u < UX; ++u)
                 {
                     const int row = base + 32 * u + lane;
-                    const bool ok = row >= c && row < m;
-                    v[u] = ok ? (row == c ? 1.0f : at(c, row)) : 0.0f;
-                    x[u] = ok ? at(j, row) : 0.0f;
+                    x[u] = row >= c && row < m ? at(j, row) : 0.0f;
                 }
 #pragma unroll
-                for (int u = 0; u < U; ++u)
+                for (int u = 0; u < UX; ++u)
                 {
                     const int row = base + 32 * u + lane;
-                    if (row >= c && row < m) at(j, row) = fma_rn(-w, v[u], x[u]);
+                    if (row >= c && row < m)
+                    {
+                        const float y = fma_rn(-w, row == c ? 1.0f : col(c, row), x[u]);
+                        at(j, row) = y;
+                        if (!SMEM && j == c + 1) col(j, row) = y;
+                    }
                 }
             }
         }
+        else if (!SMEM && !apply && warp == 1 && j < k + kb)
+            for (int row = c + 1 + lane; row < m; row += 32) col(j, row) = at(j, row);
         __syncthreads();
     }
     if (SMEM)
         for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) A[(int64_t)(k + idx / H) * lda + k + idx % H] = sp[idx];
 }
 
-// T (kb x kb upper, column-major, ld NB) of the reflectors at columns [k, k + kb), length nq.
-// The reflector Gram products are lane sums over 32-row chunks of V staged in shared
-// memory; warp w owns the pairs w, w + 32, ... of the (r < i) list.
-__global__ void __launch_bounds__(PANEL_THREADS) qr_larft_kernel(const float *A, int lda, int nq, int k, int kb,
-                                                                 const float *tau, float *T)
+// The reflector Gram products of a panel for slarft: d(i, r) = -tau_i (v_r . v_i) for r < i,
+// one warp per pair, each a lane sum in ascending rows, stored below T's diagonal
+// (T[r * NB + i]); qr_tri_kernel then forms T's upper triangle from them.
+constexpr int GRAM_WARPS = 8;
+
+__global__ void __launch_bounds__(GRAM_WARPS * 32) qr_gram_kernel(const float *A, int lda, int nq, int k, int kb,
+                                                                  const float *tau, float *T)
 {
-    constexpr int ROWS = 128;  // four 32-row chunks staged per pass
-    __shared__ float vs[ROWS][NB + 1];
-    __shared__ float d[NB][NB];   // d[i][r] = -tau_i (v_r . v_i)
+    const int lane = threadIdx.x & 31;
+    const int pr = blockIdx.x * GRAM_WARPS + (threadIdx.x >> 5);
+    if (pr >= kb * (kb - 1) / 2) return;
+    int i = 1, r = pr;
+    while (r >= i)
+    {
+        r -= i;
+        ++i;
+    }
+    const float *vr = A + (int64_t)(k + r) * lda, *vi = A + (int64_t)(k + i) * lda;
+    const int first = k + i;
+    constexpr int U = 16;
+    float p = 0.0f;
+    for (int base = first & ~31; base < nq; base += 32 * U)
+    {
+        float a[U], b[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const int row = base + 32 * u + lane;
+            const bool ok = row >= first && row < nq;
+            a[u] = ok ? vr[row] : 0.0f;
+            b[u] = ok ? (row == first ? 1.0f : vi[row]) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const int row = base + 32 * u + lane;
+            if (row >= first && row < nq) p = fma_rn(a[u], b[u], p);
+        }
+    }
+    const float dot = lane_fold(p);
+    if (lane == 0) T[r * NB + i] = mul_rn(-tau[k + i], dot);
+}
+
+// T (kb x kb upper, column-major, ld NB): T(i, i) = tau_i, T(0:i, i) = T(0:i, 0:i) d(i, 0:i)
+// (an FMA chain in ascending q), a zero column where tau_i = 0.
+__global__ void __launch_bounds__(32) qr_tri_kernel(int k, int kb, const float *tau, float *T)
+{
+    __shared__ float d[NB][NB];   // d[i][q] = d(i, q)
     __shared__ float ts[NB][NB];  // ts[i][r] = T(r, i)
-    constexpr int PER_WARP = (NB * (NB - 1) / 2 + 31) / 32;  // 16 pairs per warp
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int pairs = kb * (kb - 1) / 2;
-    int pr_r[PER_WARP], pr_i[PER_WARP];
-    float p[PER_WARP];
-#pragma unroll
-    for (int u = 0; u < PER_WARP; ++u)
-    {
-        const int pr = warp + 32 * u;
-        int i = 1, rem = pr;
-        while (rem >= i)
-        {
-            rem -= i;
-            ++i;
-        }
-        pr_r[u] = pr < pairs ? rem : 0;
-        pr_i[u] = pr < pairs ? i : NB;  // NB marks an unused slot
-        p[u] = 0.0f;
-    }
-    for (int base0 = (k + 1) & ~31; base0 < nq; base0 += ROWS)
-    {
-        __syncthreads();
-        for (int idx = tid; idx < ROWS * kb; idx += PANEL_THREADS)
-        {
-            const int rr = idx % ROWS, i = idx / ROWS, row = base0 + rr;
-            vs[rr][i] = row < nq && row > k + i ? A[(int64_t)(k + i) * lda + row] : (row == k + i ? 1.0f : 0.0f);
-        }
-        __syncthreads();
-        for (int cc = 0; cc < ROWS; cc += 32)  // chunks in ascending row order
-        {
-            const int row = base0 + cc + lane;
-            if (row < nq)
-            {
-#pragma unroll
-                for (int u = 0; u < PER_WARP; ++u)
-                    if (pr_i[u] < kb && row >= k + pr_i[u])
-                        p[u] = fma_rn(vs[cc + lane][pr_r[u]], vs[cc + lane][pr_i[u]], p[u]);
-            }
-        }
-    }
-#pragma unroll
-    for (int u = 0; u < PER_WARP; ++u)
-    {
-        const float dot = lane_fold(p[u]);
-        if (lane == 0 && pr_i[u] < kb) d[pr_i[u]][pr_r[u]] = mul_rn(-tau[k + pr_i[u]], dot);
-    }
-    __syncthreads();
+    const int tid = threadIdx.x;
+    for (int i = 0; i < kb; ++i)
+        if (tid < i) d[i][tid] = T[tid * NB + i];
+    __syncwarp();
     for (int i = 0; i < kb; ++i)
     {
         const float ti = tau[k + i];
@@ -234,13 +245,10 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_larft_kernel(const float *A,
                 ts[i][tid] = acc;
             }
         }
-        __syncthreads();
+        __syncwarp();
     }
-    for (int idx = tid; idx < kb * kb; idx += PANEL_THREADS)
-    {
-        const int r = idx % kb, i = idx / kb;
-        if (r <= i) T[i * NB + r] = ts[i][r];
-    }
+    for (int i = 0; i < kb; ++i)
+        if (tid <= i) T[i * NB + tid] = ts[i][tid];
 }
 
 // C = C - V op(T) (V^T C) (LEFT: one warp per column of C, reflector index = C's row) or
@@ -499,6 +507,20 @@ cudaError_t apply_block(bool right, bool lower_chain, const float *V, int ldv, i
         qr_apply_kernel<false, false><<<grid, APPLY_WARPS * 32, 0, stream>>>(V, ldv, nq, k, kb, T, C, ldc, count);
     return cudaGetLastError();
 }
+// T of the panel's kb reflectors: the Gram products over the grid, then the recurrence.
+cudaError_t larft(const float *A, int lda, int nq, int k, int kb, const float *tau, float *T, cudaStream_t stream)
+{
+    const int pairs = kb * (kb - 1) / 2;
+    if (pairs > 0)
+    {
+        qr_gram_kernel<<<(pairs + GRAM_WARPS - 1) / GRAM_WARPS, GRAM_WARPS * 32, 0, stream>>>(A, lda, nq, k, kb, tau,
+                                                                                             T);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    qr_tri_kernel<<<1, 32, 0, stream>>>(k, kb, tau, T);
+    return cudaGetLastError();
+}
 }  // namespace
 
 static std::atomic<unsigned long long> g_qr_attr{0};
@@ -509,9 +531,14 @@ cudaError_t launch_sgeqrf(float *A, int lda, int m, int n, float *tau, float *T,
     cudaError_t e = once_per_device(g_qr_attr,
                                     []
                                     {
-                                        return cudaFuncSetAttribute(qr_panel_kernel<true>,
-                                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                                    PANEL_SMEM_FLOATS * (int)sizeof(float));
+                                        cudaError_t r = cudaFuncSetAttribute(
+                                            qr_panel_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            PANEL_SMEM_FLOATS * (int)sizeof(float));
+                                        if (r == cudaSuccess)
+                                            r = cudaFuncSetAttribute(qr_panel_kernel<false>,
+                                                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                                     PANEL_SMEM_FLOATS * (int)sizeof(float));
+                                        return r;
                                     });
     for (int k = 0; k < lim && e == cudaSuccess; k += NB)
     {
@@ -520,13 +547,13 @@ cudaError_t launch_sgeqrf(float *A, int lda, int m, int n, float *tau, float *T,
         if (panel_floats <= PANEL_SMEM_FLOATS)
             qr_panel_kernel<true><<<1, PANEL_THREADS, (size_t)panel_floats * sizeof(float), stream>>>(A, lda, m, k, kb,
                                                                                                        tau);
-        else
-            qr_panel_kernel<false><<<1, PANEL_THREADS, 0, stream>>>(A, lda, m, k, kb, tau);
+        else  // two column buffers: 2 (m - k) floats, within PANEL_SMEM_FLOATS for m <= 25,600
+            qr_panel_kernel<false><<<1, PANEL_THREADS, (size_t)2 * (m - k) * sizeof(float), stream>>>(A, lda, m, k,
+                                                                                                        kb, tau);
         e = cudaGetLastError();
         if (e == cudaSuccess && k + kb < n)
         {
-            qr_larft_kernel<<<1, PANEL_THREADS, 0, stream>>>(A, lda, m, k, kb, tau, T);
-            e = cudaGetLastError();
+            e = larft(A, lda, m, k, kb, tau, T, stream);
             if (e == cudaSuccess)
                 e = apply_block(false, true, A, lda, m, k, kb, T, A + (int64_t)(k + kb) * lda, lda, n - k - kb,
                                 stream);
@@ -547,8 +574,7 @@ cudaError_t launch_sormqr(int side, int trans, int m, int n, int k, const float 
     {
         const int pi = forward ? s : npan - 1 - s;
         const int k0 = pi * NB, kb = std::min(NB, k - k0);
-        qr_larft_kernel<<<1, PANEL_THREADS, 0, stream>>>(A, lda, nq, k0, kb, tau, T);
-        e = cudaGetLastError();
+        e = larft(A, lda, nq, k0, kb, tau, T, stream);
         // op(T) = T^T (lower chain) for Q^T from the left and for Q from the right
         if (e == cudaSuccess) e = apply_block(right, right ? !tr : tr, A, lda, nq, k0, kb, T, C, ldc, count, stream);
     }
