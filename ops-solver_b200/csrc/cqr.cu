@@ -7,6 +7,7 @@
 // family's (qr.cu): 32-column panels, lane sums over rows (row r into lane r mod 32, a warp
 // butterfly per component), slarft's T, block application.  The complex products are fixed
 // FMA sequences (cq_* below) that the CPU oracle restates.
+#include <cooperative_groups.h>
 #include <limits.h>
 
 #include <algorithm>
@@ -203,6 +204,124 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_panel_kernel(float2 *A, int 
     }
     if (MODE == 1)
         for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) A[(int64_t)(k + idx / H) * lda + k + idx % H] = sp[idx];
+}
+
+// Rows per block of a panel spread over a cluster (0: the panel fits one block, or is too
+// tall for eight), as in the real family; the CPU oracle reduces with the same segments.
+__host__ __device__ inline int panel_seg(int H, int kb, int budget)
+{
+    if ((int64_t)H * kb <= budget) return 0;
+    const int seg = ((H + 7) / 8 + 31) & ~31;
+    return (int64_t)seg * kb <= budget ? seg : 0;
+}
+
+// A tall panel over a cluster of ceil((m - k) / seg) blocks, block g holding rows
+// [k + g seg, k + (g + 1) seg) in shared memory; per-block lane sums, folded, published and
+// added in ascending block order by every block through distributed shared memory.
+__global__ void __launch_bounds__(PANEL_THREADS) cq_cluster_panel_kernel(float2 *A, int lda, int m, int k, int kb,
+                                                                         int seg, float2 *tau)
+{
+    namespace cg = cooperative_groups;
+    extern __shared__ float2 sp[];  // sp[(j - k) * seg + (row - r0)]
+    __shared__ float2 s_alpha, s_dot[NB];
+    __shared__ float s_norm;
+    __shared__ float2 s_tau;
+    __shared__ float s_dr, s_di, s_den;
+    __shared__ int s_apply;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int g = (int)cluster.block_rank(), G = (int)cluster.num_blocks();
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int r0 = k + g * seg, r1 = min(m, r0 + seg);
+    const int rows = max(0, r1 - r0);
+    auto at = [&](int j, int row) -> float2 & { return sp[(j - k) * seg + (row - r0)]; };
+    for (int idx = tid; idx < rows * kb; idx += PANEL_THREADS)
+        sp[(idx / rows) * seg + idx % rows] = A[(int64_t)(k + idx / rows) * lda + r0 + idx % rows];
+    __syncthreads();
+    for (int c = k; c < k + kb; ++c)
+    {
+        if (warp == 0)
+        {
+            float p = 0.0f;
+            for (int row = r0 + lane; row < r1; row += 32)
+                if (row > c)
+                {
+                    const float2 x = at(c, row);
+                    p = fma_rn(x.y, x.y, fma_rn(x.x, x.x, p));
+                }
+            const float part = fold1(p);
+            if (lane == 0)
+            {
+                s_norm = part;
+                if (c >= r0 && c < r1) s_alpha = at(c, c);
+            }
+        }
+        cluster.sync();
+        if (tid == 0)
+        {
+            float parts[8];
+            for (int q = 0; q < G; ++q) parts[q] = *cluster.map_shared_rank(&s_norm, q);
+            float sumsq = parts[0];
+            for (int q = 1; q < G; ++q) sumsq = add_rn(sumsq, parts[q]);
+            const int owner = (c - k) / seg;
+            const float2 al = *cluster.map_shared_rank(&s_alpha, owner);
+            float2 t = make_float2(0.0f, 0.0f);
+            int apply = 0;
+            if (!(sumsq == 0.0f && al.y == 0.0f))
+            {
+                const float norm = sqrt_rn(add_rn(add_rn(mul_rn(al.x, al.x), mul_rn(al.y, al.y)), sumsq));
+                const float beta = -copysignf(norm, al.x);
+                t = make_float2(div_rn(sub_rn(beta, al.x), beta), -div_rn(al.y, beta));
+                const float dr = sub_rn(al.x, beta), di = al.y;
+                s_dr = dr;
+                s_di = di;
+                s_den = add_rn(mul_rn(dr, dr), mul_rn(di, di));
+                if (owner == g) at(c, c) = make_float2(beta, 0.0f);
+                apply = 1;
+            }
+            if (g == 0) tau[c] = t;
+            s_tau = t;
+            s_apply = apply;
+        }
+        __syncthreads();
+        const bool apply = s_apply != 0;
+        const float2 t = s_tau;
+        if (apply)
+        {
+            const float dr = s_dr, di = s_di, den = s_den;
+            for (int row = max(r0, c + 1) + tid; row < r1; row += PANEL_THREADS)
+            {
+                const float2 x = at(c, row);
+                at(c, row) = make_float2(div_rn(add_rn(mul_rn(x.x, dr), mul_rn(x.y, di)), den),
+                                         div_rn(sub_rn(mul_rn(x.y, dr), mul_rn(x.x, di)), den));
+            }
+        }
+        __syncthreads();
+        const int j = c + warp;
+        const bool mine = apply && warp >= 1 && j < k + kb;
+        if (mine)
+        {
+            float2 p = make_float2(0.0f, 0.0f);
+            for (int row = r0 + lane; row < r1; row += 32)
+                if (row >= c) p = cq_conjdot(p, row == c ? make_float2(1.0f, 0.0f) : at(c, row), at(j, row));
+            const float2 part = fold2(p);
+            if (lane == 0) s_dot[warp] = part;
+        }
+        cluster.sync();
+        if (mine)
+        {
+            float2 parts[8];
+            for (int q = 0; q < G; ++q) parts[q] = *cluster.map_shared_rank(&s_dot[warp], q);
+            float2 dot = parts[0];
+            for (int q = 1; q < G; ++q) dot = make_float2(add_rn(dot.x, parts[q].x), add_rn(dot.y, parts[q].y));
+            const float2 w = cq_mulc(t, dot);
+            for (int row = r0 + lane; row < r1; row += 32)
+                if (row >= c) at(j, row) = clu::csubmul(at(j, row), row == c ? make_float2(1.0f, 0.0f) : at(c, row), w);
+        }
+        __syncthreads();
+    }
+    cluster.sync();  // no block leaves while another may still read its partials
+    for (int idx = tid; idx < rows * kb; idx += PANEL_THREADS)
+        A[(int64_t)(k + idx / rows) * lda + r0 + idx % rows] = sp[(idx / rows) * seg + idx % rows];
 }
 
 // The reflector products of a panel for T: d(i, r) = -tau_i (v_r^H v_i) for r < i, one warp
@@ -519,6 +638,10 @@ cudaError_t launch_cgeqrf(float2 *A, int lda, int m, int n, float2 *tau, float2 
                                             r = cudaFuncSetAttribute(cq_panel_kernel<2>,
                                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                                      PANEL_SMEM_ELEMS * (int)sizeof(float2));
+                                        if (r == cudaSuccess)
+                                            r = cudaFuncSetAttribute(cq_cluster_panel_kernel,
+                                                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                                     PANEL_SMEM_ELEMS * (int)sizeof(float2));
                                         return r;
                                     });
     const int lim = std::min(m, n);
@@ -526,14 +649,31 @@ cudaError_t launch_cgeqrf(float2 *A, int lda, int m, int n, float2 *tau, float2 
     {
         const int kb = std::min(NB, lim - k);
         const int64_t elems = (int64_t)(m - k) * kb;
+        const int seg = panel_seg(m - k, kb, PANEL_SMEM_ELEMS);
         if (elems <= PANEL_SMEM_ELEMS)
             cq_panel_kernel<1><<<1, PANEL_THREADS, (size_t)elems * sizeof(float2), stream>>>(A, lda, m, k, kb, tau);
+        else if (seg > 0)
+        {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)((m - k + seg - 1) / seg));
+            cfg.blockDim = dim3(PANEL_THREADS);
+            cfg.dynamicSmemBytes = (size_t)seg * kb * sizeof(float2);
+            cfg.stream = stream;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = cfg.gridDim.x;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            e = cudaLaunchKernelEx(&cfg, cq_cluster_panel_kernel, A, lda, m, k, kb, seg, tau);
+        }
         else if (2 * (int64_t)(m - k) <= PANEL_SMEM_ELEMS)
             cq_panel_kernel<2><<<1, PANEL_THREADS, (size_t)2 * (m - k) * sizeof(float2), stream>>>(A, lda, m, k, kb,
                                                                                                      tau);
         else
             cq_panel_kernel<0><<<1, PANEL_THREADS, 0, stream>>>(A, lda, m, k, kb, tau);
-        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaGetLastError();
         if (e == cudaSuccess && k + kb < n)
         {
             e = cq_larft(A, lda, m, k, kb, tau, T, stream);

@@ -20,6 +20,8 @@
 //   qr_trsv_kernel       R X = Y, one block per right-hand side, backward sweep
 //   xlarft_gram_kernel / xlarft_tri_kernel   Xlarft: the reflector products over 32 x 32
 //                        blocks, then slarft's recurrence on a packed triangle (k <= 256)
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <atomic>
 
@@ -174,6 +176,114 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_panel_kernel(float *A, int l
     }
     if (SMEM)
         for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) A[(int64_t)(k + idx / H) * lda + k + idx % H] = sp[idx];
+}
+
+// Rows per block of a panel spread over a cluster (0: the panel fits one block, or is too
+// tall for eight): ceil((m - k) / 8) rounded up to a multiple of 32.  The CPU oracle reduces
+// with the same segments.
+__host__ __device__ inline int panel_seg(int H, int kb, int budget)
+{
+    if ((int64_t)H * kb <= budget) return 0;
+    const int seg = ((H + 7) / 8 + 31) & ~31;
+    return (int64_t)seg * kb <= budget ? seg : 0;
+}
+
+// A tall panel over a cluster of ceil((m - k) / seg) blocks: block g holds rows
+// [k + g seg, k + (g + 1) seg) of the kb columns in shared memory.  Each reduction over rows is
+// a lane sum per block, folded; the blocks' totals are published in shared memory and every
+// block adds them in ascending block order through distributed shared memory, so all blocks
+// derive the same reflector and the same column weights.  Two cluster barriers per column.
+__global__ void __launch_bounds__(PANEL_THREADS) qr_cluster_panel_kernel(float *A, int lda, int m, int k, int kb,
+                                                                         int seg, float *tau)
+{
+    namespace cg = cooperative_groups;
+    extern __shared__ float sp[];  // sp[(j - k) * seg + (row - r0)]
+    __shared__ float s_norm, s_alpha, s_dot[NB];
+    __shared__ float s_tau, s_scale;
+    __shared__ int s_apply;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int g = (int)cluster.block_rank(), G = (int)cluster.num_blocks();
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int r0 = k + g * seg, r1 = min(m, r0 + seg);
+    const int rows = max(0, r1 - r0);
+    auto at = [&](int j, int row) -> float & { return sp[(j - k) * seg + (row - r0)]; };
+    for (int idx = tid; idx < rows * kb; idx += PANEL_THREADS)
+        sp[(idx / rows) * seg + idx % rows] = A[(int64_t)(k + idx / rows) * lda + r0 + idx % rows];
+    __syncthreads();
+    for (int c = k; c < k + kb; ++c)
+    {
+        if (warp == 0)
+        {
+            float p = 0.0f;
+            for (int row = r0 + lane; row < r1; row += 32)
+                if (row > c) p = fma_rn(at(c, row), at(c, row), p);
+            const float part = lane_fold(p);
+            if (lane == 0)
+            {
+                s_norm = part;
+                if (c >= r0 && c < r1) s_alpha = at(c, c);
+            }
+        }
+        cluster.sync();
+        if (tid == 0)
+        {
+            float parts[8];
+            for (int q = 0; q < G; ++q) parts[q] = *cluster.map_shared_rank(&s_norm, q);
+            float sumsq = parts[0];
+            for (int q = 1; q < G; ++q) sumsq = add_rn(sumsq, parts[q]);
+            const int owner = (c - k) / seg;
+            float t = 0.0f, scale = 0.0f;
+            int apply = 0;
+            if (m - c > 1 && sumsq != 0.0f)
+            {
+                const float alpha = *cluster.map_shared_rank(&s_alpha, owner);
+                const float norm = sqrt_rn(add_rn(mul_rn(alpha, alpha), sumsq));
+                const float beta = alpha >= 0.0f ? -norm : norm;
+                t = div_rn(sub_rn(beta, alpha), beta);
+                scale = div_rn(1.0f, sub_rn(alpha, beta));
+                if (owner == g) at(c, c) = beta;
+                apply = 1;
+            }
+            if (g == 0) tau[c] = t;
+            s_tau = t;
+            s_scale = scale;
+            s_apply = apply;
+        }
+        __syncthreads();
+        const bool apply = s_apply != 0;
+        const float t = s_tau;
+        if (apply)
+        {
+            const float scale = s_scale;
+            for (int row = max(r0, c + 1) + tid; row < r1; row += PANEL_THREADS) at(c, row) = mul_rn(at(c, row), scale);
+        }
+        __syncthreads();
+        const int j = c + warp;
+        const bool mine = apply && warp >= 1 && j < k + kb;
+        if (mine)
+        {
+            float p = 0.0f;
+            for (int row = r0 + lane; row < r1; row += 32)
+                if (row >= c) p = fma_rn(row == c ? 1.0f : at(c, row), at(j, row), p);
+            const float part = lane_fold(p);
+            if (lane == 0) s_dot[warp] = part;
+        }
+        cluster.sync();
+        if (mine)
+        {
+            float parts[8];
+            for (int q = 0; q < G; ++q) parts[q] = *cluster.map_shared_rank(&s_dot[warp], q);
+            float dot = parts[0];
+            for (int q = 1; q < G; ++q) dot = add_rn(dot, parts[q]);
+            const float w = mul_rn(t, dot);
+            for (int row = r0 + lane; row < r1; row += 32)
+                if (row >= c) at(j, row) = fma_rn(-w, row == c ? 1.0f : at(c, row), at(j, row));
+        }
+        __syncthreads();
+    }
+    cluster.sync();  // no block leaves while another may still read its partials
+    for (int idx = tid; idx < rows * kb; idx += PANEL_THREADS)
+        A[(int64_t)(k + idx / rows) * lda + r0 + idx % rows] = sp[(idx / rows) * seg + idx % rows];
 }
 
 // The reflector Gram products of a panel for slarft: d(i, r) = -tau_i (v_r . v_i) for r < i,
@@ -538,19 +648,45 @@ cudaError_t launch_sgeqrf(float *A, int lda, int m, int n, float *tau, float *T,
                                             r = cudaFuncSetAttribute(qr_panel_kernel<false>,
                                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                                      PANEL_SMEM_FLOATS * (int)sizeof(float));
+                                        if (r == cudaSuccess)
+                                            r = cudaFuncSetAttribute(qr_cluster_panel_kernel,
+                                                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                                     PANEL_SMEM_FLOATS * (int)sizeof(float));
                                         return r;
                                     });
     for (int k = 0; k < lim && e == cudaSuccess; k += NB)
     {
         const int kb = std::min(NB, lim - k);
         const int64_t panel_floats = (int64_t)(m - k) * kb;
+        const int seg = panel_seg(m - k, kb, PANEL_SMEM_FLOATS);
         if (panel_floats <= PANEL_SMEM_FLOATS)
+        {
             qr_panel_kernel<true><<<1, PANEL_THREADS, (size_t)panel_floats * sizeof(float), stream>>>(A, lda, m, k, kb,
                                                                                                        tau);
+            e = cudaGetLastError();
+        }
+        else if (seg > 0)
+        {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)((m - k + seg - 1) / seg));
+            cfg.blockDim = dim3(PANEL_THREADS);
+            cfg.dynamicSmemBytes = (size_t)seg * kb * sizeof(float);
+            cfg.stream = stream;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = cfg.gridDim.x;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            e = cudaLaunchKernelEx(&cfg, qr_cluster_panel_kernel, A, lda, m, k, kb, seg, tau);
+        }
         else  // two column buffers: 2 (m - k) floats, within PANEL_SMEM_FLOATS for m <= 25,600
+        {
             qr_panel_kernel<false><<<1, PANEL_THREADS, (size_t)2 * (m - k) * sizeof(float), stream>>>(A, lda, m, k,
                                                                                                         kb, tau);
-        e = cudaGetLastError();
+            e = cudaGetLastError();
+        }
         if (e == cudaSuccess && k + kb < n)
         {
             e = larft(A, lda, m, k, kb, tau, T, stream);

@@ -1394,17 +1394,44 @@ static inline float qr_v(const float *a, int lda, int k, int i, int row)
     return row == k + i ? 1.0f : RAT(a, lda, row, k + i);
 }
 
-static void qr_larfg(int m, float *a, int lda, int c, float *tau)
+/* Rows per segment of a panel's reductions.  A panel (rows [k, m) of kb columns) that fits
+ * one block's shared memory (budget elements) is reduced as one segment (0).  A larger one is
+ * spread over an eight-block cluster: block s holds rows [k + s seg, k + (s + 1) seg), seg =
+ * ceil((m - k) / 8) rounded up to a multiple of 32, and each reduction over rows becomes one
+ * lane sum per segment, folded, with the segment totals added in ascending order.  A panel
+ * too tall even for that is again one segment. */
+static int qr_panel_seg(int H, int kb, int budget)
+{
+    if ((int64_t)H * kb <= budget) return 0;
+    const int seg = ((H + 7) / 8 + 31) & ~31;
+    return (int64_t)seg * kb <= budget ? seg : 0;
+}
+
+/* Folds the lane partials p of one segment into *total (segment totals in ascending order). */
+static void qr_seg_flush(float *p, float *total, int *started)
+{
+    const float part = qr_lane_fold(p);
+    *total = *started ? *total + part : part;
+    *started = 1;
+    memset(p, 0, 32 * sizeof(float));
+}
+
+/* Starts a new segment at `row` (rows counted from the panel start k). */
+#define QR_SEG_EDGE(row, first, k, seg) ((seg) && (row) > (first) && ((row) - (k)) % (seg) == 0)
+
+static void qr_larfg(int m, int k, int seg, float *a, int lda, int c, float *tau)
 {
     *tau = 0.0f;
     if (m - c <= 1) return;
-    float p[32] = {0};
+    float p[32] = {0}, sumsq = 0.0f;
+    int started = 0;
     for (int row = c + 1; row < m; ++row)
     {
+        if (QR_SEG_EDGE(row, c + 1, k, seg)) qr_seg_flush(p, &sumsq, &started);
         float x = RAT(a, lda, row, c);
         p[row & 31] = fmaf(x, x, p[row & 31]);
     }
-    float sumsq = qr_lane_fold(p);
+    qr_seg_flush(p, &sumsq, &started);
     if (sumsq == 0.0f) return;
     float alpha = RAT(a, lda, c, c);
     float norm = sqrtf(alpha * alpha + sumsq);
@@ -1418,20 +1445,24 @@ static void qr_larfg(int m, float *a, int lda, int c, float *tau)
 /* Factor panel columns [k, k+kb) of rows [k, m). */
 static void qr_panel(int m, int k, int kb, float *a, int lda, float *tau)
 {
+    const int seg = qr_panel_seg(m - k, kb, 50 * 1024);
     for (int c = k; c < k + kb; ++c)
     {
-        qr_larfg(m, a, lda, c, &tau[c]);
+        qr_larfg(m, k, seg, a, lda, c, &tau[c]);
         const float t = tau[c];
         if (t == 0.0f) continue;
         for (int j = c + 1; j < k + kb; ++j)
         {
-            float p[32] = {0};
+            float p[32] = {0}, dot = 0.0f;
+            int started = 0;
             for (int row = c; row < m; ++row)
             {
+                if (QR_SEG_EDGE(row, c, k, seg)) qr_seg_flush(p, &dot, &started);
                 float v = row == c ? 1.0f : RAT(a, lda, row, c);
                 p[row & 31] = fmaf(v, RAT(a, lda, row, j), p[row & 31]);
             }
-            float w = t * qr_lane_fold(p);
+            qr_seg_flush(p, &dot, &started);
+            float w = t * dot;
             for (int row = c; row < m; ++row)
             {
                 float v = row == c ? 1.0f : RAT(a, lda, row, c);
@@ -1790,16 +1821,34 @@ static inline cfl cq_v(const cfl *a, int lda, int k, int i, int row)
     return CAT(a, lda, row, k + i);
 }
 
-static void cq_larfg(int m, cfl *a, int lda, int c, cfl *tau)
+static void cq_seg_flush(cfl *p, cfl *total, int *started)
+{
+    const cfl part = q_fold(p);
+    if (*started)
+    {
+        total->re = total->re + part.re;
+        total->im = total->im + part.im;
+    }
+    else
+        *total = part;
+    *started = 1;
+    memset(p, 0, 32 * sizeof(cfl));
+}
+
+/* Panels are reduced in segments as in the real family (qr_panel_seg), with a budget of
+ * 25,600 complex elements per block. */
+static void cq_larfg(int m, int k, int seg, cfl *a, int lda, int c, cfl *tau)
 {
     tau->re = tau->im = 0.0f;
-    float p[32] = {0};
+    float p[32] = {0}, sumsq = 0.0f;
+    int started = 0;
     for (int row = c + 1; row < m; ++row)
     {
+        if (QR_SEG_EDGE(row, c + 1, k, seg)) qr_seg_flush(p, &sumsq, &started);
         cfl x = CAT(a, lda, row, c);
         p[row & 31] = fmaf(x.im, x.im, fmaf(x.re, x.re, p[row & 31]));
     }
-    const float sumsq = qr_lane_fold(p);
+    qr_seg_flush(p, &sumsq, &started);
     const cfl al = CAT(a, lda, c, c);
     if (sumsq == 0.0f && al.im == 0.0f) return;
     const float norm = sqrtf(al.re * al.re + al.im * al.im + sumsq);
@@ -1820,21 +1869,25 @@ static void cq_larfg(int m, cfl *a, int lda, int c, cfl *tau)
 
 static void cq_panel(int m, int k, int kb, cfl *a, int lda, cfl *tau)
 {
+    const int seg = qr_panel_seg(m - k, kb, 25 * 1024);
     for (int c = k; c < k + kb; ++c)
     {
-        cq_larfg(m, a, lda, c, &tau[c]);
+        cq_larfg(m, k, seg, a, lda, c, &tau[c]);
         const cfl t = tau[c];
         if (t.re == 0.0f && t.im == 0.0f) continue;
         for (int j = c + 1; j < k + kb; ++j)
         {
-            cfl p[32];
+            cfl p[32], dot = {0.0f, 0.0f};
+            int started = 0;
             memset(p, 0, sizeof p);
             for (int row = c; row < m; ++row)
             {
+                if (QR_SEG_EDGE(row, c, k, seg)) cq_seg_flush(p, &dot, &started);
                 cfl v = row == c ? (cfl){1.0f, 0.0f} : CAT(a, lda, row, c);
                 p[row & 31] = q_conjdot(p[row & 31], v, CAT(a, lda, row, j));
             }
-            const cfl w = q_mulc(t, q_fold(p));
+            cq_seg_flush(p, &dot, &started);
+            const cfl w = q_mulc(t, dot);
             for (int row = c; row < m; ++row)
             {
                 cfl v = row == c ? (cfl){1.0f, 0.0f} : CAT(a, lda, row, c);

@@ -55,7 +55,8 @@ def geqrf(handle, a, pad=3):
 
 
 @pytest.mark.parametrize("m,n", [(1, 1), (7, 3), (3, 7), (65, 33), (257, 131), (2, 2), (32, 32), (33, 33),
-                                 (100, 64), (300, 257), (257, 300), (1000, 200), (4096, 40), (1024, 1024)])
+                                 (100, 64), (300, 257), (257, 300), (1000, 200), (4096, 40), (1024, 1024),
+                                 (801, 64), (7000, 33)])
 def test_cgeqrf_matches_oracle(handle, m, n):
     a = crand(m, n, m * 29 + n)
     got, tau = geqrf(handle, a)

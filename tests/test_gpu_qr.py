@@ -45,7 +45,8 @@ def geqrf(handle, a, pad=0):
 
 
 @pytest.mark.parametrize("m,n", [(1, 1), (2, 2), (18, 8), (32, 4), (57, 57), (66, 8), (100, 33), (33, 100),
-                                 (300, 257), (257, 300), (1000, 200), (4096, 64), (1024, 1024)])
+                                 (300, 257), (257, 300), (1000, 200), (4096, 64), (1024, 1024), (2500, 100),
+                                 (1700, 33)])
 def test_sgeqrf_matches_oracle(handle, m, n):
     a = rand(m, n, m * 13 + n)
     got, tau = geqrf(handle, a, pad=3)

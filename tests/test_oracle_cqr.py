@@ -25,7 +25,8 @@ def crand(m, n, seed):
     return (rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))).astype(np.complex64)
 
 
-@pytest.mark.parametrize("m,n", [(1, 1), (7, 3), (3, 7), (65, 33), (257, 131), (40, 40), (100, 64), (33, 100)])
+@pytest.mark.parametrize("m,n", [(1, 1), (7, 3), (3, 7), (65, 33), (257, 131), (40, 40), (100, 64), (33, 100),
+                                 (1000, 40), (801, 64)])  # the last two: panels reduced in row segments
 def test_cgeqrf_matches_lapack_and_passes_the_reference_criteria(m, n):
     from scipy.linalg import lapack
 

@@ -18,7 +18,8 @@ import pytest
 import oracle
 from oracle import judges
 
-SHAPES = [(2, 2), (18, 8), (32, 4), (57, 57), (66, 8), (100, 33), (33, 100), (128, 128), (300, 70)]
+SHAPES = [(2, 2), (18, 8), (32, 4), (57, 57), (66, 8), (100, 33), (33, 100), (128, 128), (300, 70),
+          (2000, 40)]  # the last: panels reduced in eight row segments
 
 
 def rand(m, n, seed):
