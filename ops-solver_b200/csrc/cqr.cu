@@ -405,56 +405,97 @@ __global__ void __launch_bounds__(32) cq_tri_kernel(int k, int kb, const float2 
 
 // LEFT: C = (I - V op(T) V^H) C, one warp per column of C; RIGHT: C = C (I - V op(T) V^H), one
 // warp per row.  HERM selects op(T) = T^H (LEFT: Q^H C; RIGHT: C Q^H), else T.
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
 template <bool RIGHT, bool HERM>
 __global__ void __launch_bounds__(APPLY_WARPS * 32) cq_apply_kernel(const float2 *V, int ldv, int nq, int k, int kb,
                                                                     const float2 *T, float2 *C, int64_t ldc, int count)
 {
     constexpr int ROWS = 64;
-    __shared__ float2 vs[ROWS][NB + 1];
+    constexpr int CU = ROWS / 32;
+    // V double-buffered (the next pass copied by cp.async while this one computes), raw: the
+    // unit diagonal and the zeros above it are applied when the first 32 rows are read.
+    __shared__ __align__(16) float2 vs[2][ROWS][NB + 2];  // even pitch: 128-bit reads of two entries
     __shared__ float2 ts[NB * NB];
-    __shared__ float2 w2s[APPLY_WARPS][NB];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int j = blockIdx.x * APPLY_WARPS + warp;
     const bool live = j < count;
     for (int idx = tid; idx < NB * NB; idx += APPLY_WARPS * 32) ts[idx] = T[idx];
     auto cat = [&](int row) -> float2 * { return RIGHT ? C + (int64_t)row * ldc + j : C + (int64_t)j * ldc + row; };
-    float2 p[NB];
-#pragma unroll
-    for (int i = 0; i < NB; ++i) p[i] = make_float2(0.0f, 0.0f);
-    const int first = k & ~31;
-    for (int base0 = first; base0 < nq; base0 += ROWS)
+    auto stage = [&](int base0, int b)
     {
-        float2 c[ROWS / 32];
+        if (base0 < nq)
+            for (int idx = tid; idx < ROWS * kb; idx += APPLY_WARPS * 32)
+            {
+                const int rr = idx % ROWS, i = idx / ROWS, row = base0 + rr;
+                if (row < nq) cp_async8(&vs[b][rr][i], V + (int64_t)(k + i) * ldv + row);
+            }
+        cp_async_commit();
+    };
+    auto load_c = [&](int base0, float2 *c)
+    {
 #pragma unroll
-        for (int u = 0; u < ROWS / 32; ++u)
+        for (int u = 0; u < CU; ++u)
         {
             const int row = base0 + 32 * u + lane;
             c[u] = live && row >= k && row < nq ? *cat(row) : make_float2(0.0f, 0.0f);
         }
-        __syncthreads();
-        for (int idx = tid; idx < ROWS * kb; idx += APPLY_WARPS * 32)
-        {
-            const int rr = idx % ROWS, i = idx / ROWS, row = base0 + rr;
-            vs[rr][i] = row < nq && row > k + i ? V[(int64_t)(k + i) * ldv + row]
-                                                : make_float2(row == k + i ? 1.0f : 0.0f, 0.0f);
-        }
+    };
+    const float2 one = make_float2(1.0f, 0.0f);
+    float2 p[NB];
+#pragma unroll
+    for (int i = 0; i < NB; ++i) p[i] = make_float2(0.0f, 0.0f);
+    const int first = k & ~31;
+    float2 c[CU];
+    stage(first, 0);
+    load_c(first, c);
+    int b = 0;
+    for (int base0 = first; base0 < nq; base0 += ROWS, b ^= 1)
+    {
+        stage(base0 + ROWS, b ^ 1);
+        float2 cn[CU];
+        load_c(base0 + ROWS, cn);
+        cp_async_wait_prior();
         __syncthreads();
 #pragma unroll
-        for (int u = 0; u < ROWS / 32; ++u)
+        for (int u = 0; u < CU; ++u)
         {
             const int row = base0 + 32 * u + lane;
-            if (live && row >= k && row < nq)
+            if (live && kb == NB && row >= k + NB && row < nq)  // below every reflector's unit entry
+            {
+#pragma unroll
+                for (int i = 0; i < NB; i += 2)
+                {
+                    const float4 v2 = *reinterpret_cast<const float4 *>(&vs[b][32 * u + lane][i]);
+                    const float2 va = make_float2(v2.x, v2.y), vb = make_float2(v2.z, v2.w);
+                    p[i] = RIGHT ? cq_dot(p[i], c[u], va) : cq_conjdot(p[i], va, c[u]);
+                    p[i + 1] = RIGHT ? cq_dot(p[i + 1], c[u], vb) : cq_conjdot(p[i + 1], vb, c[u]);
+                }
+            }
+            else if (live && row >= k && row < nq)
             {
 #pragma unroll
                 for (int i = 0; i < NB; ++i)
                     if (i < kb && row >= k + i)
-                        p[i] = RIGHT ? cq_dot(p[i], c[u], vs[32 * u + lane][i])
-                                     : cq_conjdot(p[i], vs[32 * u + lane][i], c[u]);
+                    {
+                        const float2 v = row == k + i ? one : vs[b][32 * u + lane][i];
+                        p[i] = RIGHT ? cq_dot(p[i], c[u], v) : cq_conjdot(p[i], v, c[u]);
+                    }
             }
         }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < CU; ++u) c[u] = cn[u];
     }
 #pragma unroll
     for (int i = 0; i < NB; ++i) p[i] = fold2(p[i]);
+    float2 w2[NB];  // W2 = op(T) W, lane i forming entry i, then shared across the warp
     {
         // lower chain (sum over q <= i of T(q, i)): LEFT with T^H, RIGHT with T
         constexpr bool LOWER = RIGHT ? !HERM : HERM;
@@ -473,41 +514,53 @@ __global__ void __launch_bounds__(APPLY_WARPS * 32) cq_apply_kernel(const float2
                     acc = HERM ? cq_fmac(ts[q * NB + lane], p[q], acc) : cq_fma(ts[q * NB + lane], p[q], acc);
             }
         }
-        w2s[warp][lane] = acc;
+#pragma unroll
+        for (int i = 0; i < NB; ++i)
+            w2[i] = make_float2(__shfl_sync(0xffffffffu, acc.x, i), __shfl_sync(0xffffffffu, acc.y, i));
     }
-    __syncwarp();
-    for (int base0 = first; base0 < nq; base0 += ROWS)
+    stage(first, 0);
+    load_c(first, c);
+    b = 0;
+    for (int base0 = first; base0 < nq; base0 += ROWS, b ^= 1)
     {
-        float2 c[ROWS / 32];
-#pragma unroll
-        for (int u = 0; u < ROWS / 32; ++u)
-        {
-            const int row = base0 + 32 * u + lane;
-            c[u] = live && row >= k && row < nq ? *cat(row) : make_float2(0.0f, 0.0f);
-        }
-        __syncthreads();
-        for (int idx = tid; idx < ROWS * kb; idx += APPLY_WARPS * 32)
-        {
-            const int rr = idx % ROWS, i = idx / ROWS, row = base0 + rr;
-            vs[rr][i] = row < nq && row > k + i ? V[(int64_t)(k + i) * ldv + row]
-                                                : make_float2(row == k + i ? 1.0f : 0.0f, 0.0f);
-        }
+        stage(base0 + ROWS, b ^ 1);
+        float2 cn[CU];
+        load_c(base0 + ROWS, cn);
+        cp_async_wait_prior();
         __syncthreads();
 #pragma unroll
-        for (int u = 0; u < ROWS / 32; ++u)
+        for (int u = 0; u < CU; ++u)
         {
             const int row = base0 + 32 * u + lane;
-            if (live && row >= k && row < nq)
+            if (live && kb == NB && row >= k + NB && row < nq)
+            {
+                float2 x = c[u];
+#pragma unroll
+                for (int i = 0; i < NB; i += 2)
+                {
+                    const float4 v2 = *reinterpret_cast<const float4 *>(&vs[b][32 * u + lane][i]);
+                    const float2 va = make_float2(v2.x, v2.y), vb = make_float2(v2.z, v2.w);
+                    x = RIGHT ? cq_submulc(x, w2[i], va) : clu::csubmul(x, va, w2[i]);
+                    x = RIGHT ? cq_submulc(x, w2[i + 1], vb) : clu::csubmul(x, vb, w2[i + 1]);
+                }
+                *cat(row) = x;
+            }
+            else if (live && row >= k && row < nq)
             {
                 float2 x = c[u];
 #pragma unroll
                 for (int i = 0; i < NB; ++i)
                     if (i < kb && i <= row - k)
-                        x = RIGHT ? cq_submulc(x, w2s[warp][i], vs[32 * u + lane][i])
-                                  : clu::csubmul(x, vs[32 * u + lane][i], w2s[warp][i]);
+                    {
+                        const float2 v = row == k + i ? one : vs[b][32 * u + lane][i];
+                        x = RIGHT ? cq_submulc(x, w2[i], v) : clu::csubmul(x, v, w2[i]);
+                    }
                 *cat(row) = x;
             }
         }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < CU; ++u) c[u] = cn[u];
     }
 }
 

@@ -35,7 +35,7 @@ namespace
 {
 constexpr int NB = 32;
 constexpr int PANEL_THREADS = 1024;
-constexpr int APPLY_WARPS = 16;
+constexpr int APPLY_WARPS = 8;
 
 __device__ __forceinline__ float lane_fold(float p)
 {
@@ -365,53 +365,97 @@ __global__ void __launch_bounds__(32) qr_tri_kernel(int k, int kb, const float *
 // C = C - (C V) op(T) V^T (RIGHT: one warp per row of C, reflector index = C's column).
 // LOWER_CHAIN: W2[i] = sum_{q <= i} T(q, i) W[q] (op(T) = T^T for LEFT, T for RIGHT);
 // otherwise W2[i] = sum_{q >= i} T(i, q) W[q].
-template <bool RIGHT, bool LOWER_CHAIN>
-__global__ void __launch_bounds__(APPLY_WARPS * 32) qr_apply_kernel(const float *V, int ldv, int nq, int k, int kb,
-                                                                    const float *T, float *C, int64_t ldc, int count)
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
 {
-    constexpr int ROWS = 128;  // four 32-row chunks of V staged per pass
-    __shared__ float vs[ROWS][NB + 1];
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+template <bool RIGHT, bool LOWER_CHAIN>
+__global__ void __launch_bounds__(APPLY_WARPS * 32, 3) qr_apply_kernel(const float *V, int ldv, int nq, int k, int kb,
+                                                                       const float *T, float *C, int64_t ldc,
+                                                                       int count)
+{
+    constexpr int ROWS = 128;   // four 32-row chunks of V per pass
+    constexpr int VP = NB + 4;  // row pitch: 16-byte aligned rows, conflict-free 128-bit reads
+    constexpr int CU = ROWS / 32;
+    // V is double-buffered: the next pass's rows are copied (cp.async) while this pass computes.
+    // The raw reflector store is staged; the unit diagonal and the zeros above it are applied
+    // when the first 32 rows are read.
+    __shared__ __align__(16) float vs[2][ROWS][VP];
     __shared__ float ts[NB * NB];
-    __shared__ float w2s[APPLY_WARPS][NB];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int j = blockIdx.x * APPLY_WARPS + warp;  // column (LEFT) or row (RIGHT) of C
     const bool live = j < count;
     for (int idx = tid; idx < NB * NB; idx += APPLY_WARPS * 32) ts[idx] = T[idx];
     auto cat = [&](int row) -> float * { return RIGHT ? C + (int64_t)row * ldc + j : C + (int64_t)j * ldc + row; };
-    float p[NB];
-#pragma unroll
-    for (int i = 0; i < NB; ++i) p[i] = 0.0f;
-    const int first = k & ~31;
-    for (int base0 = first; base0 < nq; base0 += ROWS)
+    auto stage = [&](int base0, int b)
     {
-        float c[ROWS / 32];
+        if (base0 < nq)
+            for (int idx = tid; idx < ROWS * kb; idx += APPLY_WARPS * 32)
+            {
+                const int rr = idx % ROWS, i = idx / ROWS, row = base0 + rr;
+                if (row < nq) cp_async4(&vs[b][rr][i], V + (int64_t)(k + i) * ldv + row);
+            }
+        cp_async_commit();
+    };
+    auto load_c = [&](int base0, float *c)
+    {
 #pragma unroll
-        for (int u = 0; u < ROWS / 32; ++u)  // this warp's values, loaded before the staging barrier
+        for (int u = 0; u < CU; ++u)
         {
             const int row = base0 + 32 * u + lane;
             c[u] = live && row >= k && row < nq ? *cat(row) : 0.0f;
         }
-        __syncthreads();
-        for (int idx = tid; idx < ROWS * kb; idx += APPLY_WARPS * 32)
-        {
-            const int rr = idx % ROWS, i = idx / ROWS, row = base0 + rr;
-            vs[rr][i] = row < nq && row > k + i ? V[(int64_t)(k + i) * ldv + row] : (row == k + i ? 1.0f : 0.0f);
-        }
+    };
+    const int first = k & ~31;
+    float p[NB];
+#pragma unroll
+    for (int i = 0; i < NB; ++i) p[i] = 0.0f;
+    float c[CU];
+    stage(first, 0);
+    load_c(first, c);
+    int b = 0;
+    for (int base0 = first; base0 < nq; base0 += ROWS, b ^= 1)
+    {
+        stage(base0 + ROWS, b ^ 1);
+        float cn[CU];
+        load_c(base0 + ROWS, cn);
+        cp_async_wait_prior();
         __syncthreads();
 #pragma unroll
-        for (int u = 0; u < ROWS / 32; ++u)  // chunks in ascending row order
+        for (int u = 0; u < CU; ++u)  // chunks in ascending row order
         {
             const int row = base0 + 32 * u + lane;
-            if (live && row >= k && row < nq)
+            if (live && kb == NB && row >= k + NB && row < nq)  // below every reflector's unit entry
+            {
+#pragma unroll
+                for (int i = 0; i < NB; i += 4)
+                {
+                    const float4 v = *reinterpret_cast<const float4 *>(&vs[b][32 * u + lane][i]);
+                    p[i] = fma_rn(v.x, c[u], p[i]);
+                    p[i + 1] = fma_rn(v.y, c[u], p[i + 1]);
+                    p[i + 2] = fma_rn(v.z, c[u], p[i + 2]);
+                    p[i + 3] = fma_rn(v.w, c[u], p[i + 3]);
+                }
+            }
+            else if (live && row >= k && row < nq)
             {
 #pragma unroll
                 for (int i = 0; i < NB; ++i)
-                    if (i < kb && row >= k + i) p[i] = fma_rn(vs[32 * u + lane][i], c[u], p[i]);
+                    if (i < kb && row >= k + i)
+                        p[i] = fma_rn(row == k + i ? 1.0f : vs[b][32 * u + lane][i], c[u], p[i]);
             }
         }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < CU; ++u) c[u] = cn[u];
     }
 #pragma unroll
     for (int i = 0; i < NB; ++i) p[i] = lane_fold(p[i]);
+    float w2[NB];  // W2 = op(T) W, lane i forming entry i, then shared across the warp
     {
         float acc = 0.0f;
 #pragma unroll
@@ -426,38 +470,49 @@ __global__ void __launch_bounds__(APPLY_WARPS * 32) qr_apply_kernel(const float 
                 if (q >= lane && q < kb) acc = fma_rn(ts[q * NB + lane], p[q], acc);
             }
         }
-        w2s[warp][lane] = acc;
+#pragma unroll
+        for (int i = 0; i < NB; ++i) w2[i] = __shfl_sync(0xffffffffu, acc, i);
     }
-    __syncwarp();
-    for (int base0 = first; base0 < nq; base0 += ROWS)
+    stage(first, 0);
+    load_c(first, c);
+    b = 0;
+    for (int base0 = first; base0 < nq; base0 += ROWS, b ^= 1)
     {
-        float c[ROWS / 32];
-#pragma unroll
-        for (int u = 0; u < ROWS / 32; ++u)
-        {
-            const int row = base0 + 32 * u + lane;
-            c[u] = live && row >= k && row < nq ? *cat(row) : 0.0f;
-        }
-        __syncthreads();
-        for (int idx = tid; idx < ROWS * kb; idx += APPLY_WARPS * 32)
-        {
-            const int rr = idx % ROWS, i = idx / ROWS, row = base0 + rr;
-            vs[rr][i] = row < nq && row > k + i ? V[(int64_t)(k + i) * ldv + row] : (row == k + i ? 1.0f : 0.0f);
-        }
+        stage(base0 + ROWS, b ^ 1);
+        float cn[CU];
+        load_c(base0 + ROWS, cn);
+        cp_async_wait_prior();
         __syncthreads();
 #pragma unroll
-        for (int u = 0; u < ROWS / 32; ++u)
+        for (int u = 0; u < CU; ++u)
         {
             const int row = base0 + 32 * u + lane;
-            if (live && row >= k && row < nq)
+            if (live && kb == NB && row >= k + NB && row < nq)
+            {
+                float x = c[u];
+#pragma unroll
+                for (int i = 0; i < NB; i += 4)
+                {
+                    const float4 v = *reinterpret_cast<const float4 *>(&vs[b][32 * u + lane][i]);
+                    x = fma_rn(-v.x, w2[i], x);
+                    x = fma_rn(-v.y, w2[i + 1], x);
+                    x = fma_rn(-v.z, w2[i + 2], x);
+                    x = fma_rn(-v.w, w2[i + 3], x);
+                }
+                *cat(row) = x;
+            }
+            else if (live && row >= k && row < nq)
             {
                 float x = c[u];
 #pragma unroll
                 for (int i = 0; i < NB; ++i)
-                    if (i < kb && i <= row - k) x = fma_rn(-vs[32 * u + lane][i], w2s[warp][i], x);
+                    if (i < kb && i <= row - k) x = fma_rn(-(row == k + i ? 1.0f : vs[b][32 * u + lane][i]), w2[i], x);
                 *cat(row) = x;
             }
         }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < CU; ++u) c[u] = cn[u];
     }
 }
 
