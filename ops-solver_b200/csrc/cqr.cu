@@ -372,35 +372,40 @@ __global__ void __launch_bounds__(GRAM_WARPS * 32) cq_gram_kernel(const float2 *
 }
 
 // T (kb x kb upper, ld NB): T(i, i) = tau_i, T(0:i, i) = T(0:i, 0:i) d(i, 0:i) (a chain in
-// ascending q), a zero column where tau_i = 0.
+// ascending q), a zero column where tau_i = 0.  Lane r keeps row r of T in registers.
 __global__ void __launch_bounds__(32) cq_tri_kernel(int k, int kb, const float2 *tau, float2 *T)
 {
-    __shared__ float2 d[NB][NB];   // d[i][q] = d(i, q)
-    __shared__ float2 ts[NB][NB];  // ts[i][r] = T(r, i)
-    const int tid = threadIdx.x;
+    __shared__ float2 d[NB][NB];  // d[i][q] = d(i, q)
+    const int r = threadIdx.x;
     for (int i = 0; i < kb; ++i)
-        if (tid < i) d[i][tid] = T[tid * NB + i];
+        if (r < i) d[i][r] = T[r * NB + i];
     __syncwarp();
-    for (int i = 0; i < kb; ++i)
+    float2 tr[NB];  // tr[q] = T(r, q)
+#pragma unroll
+    for (int i = 0; i < NB; ++i)
     {
-        const float2 ti = tau[k + i];
-        if (tid <= i)
+        tr[i] = make_float2(0.0f, 0.0f);
+        if (i < kb)
         {
-            if (czero2(ti))
-                ts[i][tid] = make_float2(0.0f, 0.0f);
-            else if (tid == i)
-                ts[i][i] = ti;
-            else
+            const float2 ti = tau[k + i];
+            if (!czero2(ti))
             {
-                float2 acc = make_float2(0.0f, 0.0f);
-                for (int q = tid; q < i; ++q) acc = cq_fma(ts[q][tid], d[i][q], acc);
-                ts[i][tid] = acc;
+                if (r == i)
+                    tr[i] = ti;
+                else if (r < i)
+                {
+                    float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll
+                    for (int q = 0; q < i; ++q)
+                        if (q >= r) acc = cq_fma(tr[q], d[i][q], acc);
+                    tr[i] = acc;
+                }
             }
         }
-        __syncwarp();
     }
-    for (int i = 0; i < kb; ++i)
-        if (tid <= i) T[i * NB + tid] = ts[i][tid];
+#pragma unroll
+    for (int i = 0; i < NB; ++i)
+        if (i < kb && r <= i) T[i * NB + r] = tr[i];
 }
 
 // LEFT: C = (I - V op(T) V^H) C, one warp per column of C; RIGHT: C = C (I - V op(T) V^H), one
@@ -566,12 +571,16 @@ __global__ void __launch_bounds__(APPLY_WARPS * 32) cq_apply_kernel(const float2
 
 // R X = Y for one right-hand side per block; R's diagonal is real.  Every block first looks
 // for a zero diagonal entry: the first one (one-based) goes to info and X is left untouched.
-__global__ void __launch_bounds__(1024) cq_trsv_kernel(const float2 *R, int ldr, int n, const float2 *Y, int ldy,
+// Then 32-column blocks from the bottom: warp 0 solves the diagonal block with the
+// right-hand side in its lanes (x_p = x_p / R_pp componentwise, then x_i -= R_ip x_p, p
+// descending), and every thread applies the block's columns to the rows above it, p
+// descending, so each x_i receives its updates in descending p.
+__global__ void __launch_bounds__(512) cq_trsv_kernel(const float2 *R, int ldr, int n, const float2 *Y, int ldy,
                                                        float2 *X, int ldx, int *info)
 {
     extern __shared__ float2 xs[];
     __shared__ int s_zero;
-    const int j = blockIdx.x, tid = threadIdx.x;
+    const int j = blockIdx.x, tid = threadIdx.x, lane = tid & 31;
     if (tid == 0) s_zero = n;
     __syncthreads();
     for (int i = tid; i < n; i += blockDim.x)
@@ -585,17 +594,32 @@ __global__ void __launch_bounds__(1024) cq_trsv_kernel(const float2 *R, int ldr,
     }
     for (int i = tid; i < n; i += blockDim.x) xs[i] = Y[(int64_t)j * ldy + i];
     __syncthreads();
-    for (int p = n - 1; p >= 0; --p)
+    for (int c0 = (n - 1) & ~31; c0 >= 0; c0 -= 32)
     {
-        const float2 *rp = R + (int64_t)p * ldr;
-        if (tid == 0)
+        const int cw = min(32, n - c0);
+        if (tid < 32)
         {
-            const float d = rp[p].x;
-            xs[p] = make_float2(div_rn(xs[p].x, d), div_rn(xs[p].y, d));
+            float2 r[32];
+#pragma unroll
+            for (int q = 0; q < 32; ++q)
+                r[q] = lane < cw && q < cw ? R[(int64_t)(c0 + q) * ldr + c0 + lane] : make_float2(1.0f, 0.0f);
+            float2 x = lane < cw ? xs[c0 + lane] : make_float2(0.0f, 0.0f);
+#pragma unroll
+            for (int q = 31; q >= 0; --q)
+            {
+                if (q < cw && lane == q) x = make_float2(div_rn(x.x, r[q].x), div_rn(x.y, r[q].x));
+                const float2 xp = make_float2(__shfl_sync(0xffffffffu, x.x, q), __shfl_sync(0xffffffffu, x.y, q));
+                if (q < cw && lane < q) x = clu::csubmul(x, r[q], xp);
+            }
+            if (lane < cw) xs[c0 + lane] = x;
         }
         __syncthreads();
-        const float2 xp = xs[p];
-        for (int i = tid; i < p; i += blockDim.x) xs[i] = clu::csubmul(xs[i], rp[i], xp);
+        for (int i = tid; i < c0; i += blockDim.x)
+        {
+            float2 x = xs[i];
+            for (int q = cw - 1; q >= 0; --q) x = clu::csubmul(x, R[(int64_t)(c0 + q) * ldr + i], xs[c0 + q]);
+            xs[i] = x;
+        }
         __syncthreads();
     }
     for (int i = tid; i < n; i += blockDim.x) X[(int64_t)j * ldx + i] = xs[i];
@@ -789,7 +813,7 @@ cudaError_t launch_cgels(int m, int n, int nrhs, float2 *A, int lda, const float
     if (e == cudaSuccess) e = launch_cunmqr(0, 1, m, nrhs, n, A, lda, tau, Y, m, T, stream);
     if (e == cudaSuccess)
     {
-        cq_trsv_kernel<<<nrhs, 1024, (size_t)n * sizeof(float2), stream>>>(A, lda, n, Y, m, X, ldx, info);
+        cq_trsv_kernel<<<nrhs, 512, (size_t)n * sizeof(float2), stream>>>(A, lda, n, Y, m, X, ldx, info);
         e = cudaGetLastError();
     }
     return e;

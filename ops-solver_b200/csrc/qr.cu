@@ -17,7 +17,7 @@
 //   qr_apply_kernel      one warp per column (left) or row (right) of C: W = V^T c by lane
 //                        sums over 32-row chunks of V staged in shared memory, W2 = op(T) W,
 //                        then c -= V W2 with an FMA chain over the reflectors
-//   qr_trsv_kernel       R X = Y, one block per right-hand side, backward sweep
+//   qr_trsv_kernel       R X = Y, one block per right-hand side, 32-column blocks from the bottom
 //   xlarft_gram_kernel / xlarft_tri_kernel   Xlarft: the reflector products over 32 x 32
 //                        blocks, then slarft's recurrence on a packed triangle (k <= 256)
 #include <cooperative_groups.h>
@@ -330,35 +330,41 @@ __global__ void __launch_bounds__(GRAM_WARPS * 32) qr_gram_kernel(const float *A
 }
 
 // T (kb x kb upper, column-major, ld NB): T(i, i) = tau_i, T(0:i, i) = T(0:i, 0:i) d(i, 0:i)
-// (an FMA chain in ascending q), a zero column where tau_i = 0.
+// (an FMA chain in ascending q), a zero column where tau_i = 0.  Lane r keeps row r of T in
+// registers.
 __global__ void __launch_bounds__(32) qr_tri_kernel(int k, int kb, const float *tau, float *T)
 {
-    __shared__ float d[NB][NB];   // d[i][q] = d(i, q)
-    __shared__ float ts[NB][NB];  // ts[i][r] = T(r, i)
-    const int tid = threadIdx.x;
+    __shared__ float d[NB][NB];  // d[i][q] = d(i, q)
+    const int r = threadIdx.x;
     for (int i = 0; i < kb; ++i)
-        if (tid < i) d[i][tid] = T[tid * NB + i];
+        if (r < i) d[i][r] = T[r * NB + i];
     __syncwarp();
-    for (int i = 0; i < kb; ++i)
+    float tr[NB];  // tr[q] = T(r, q)
+#pragma unroll
+    for (int i = 0; i < NB; ++i)
     {
-        const float ti = tau[k + i];
-        if (tid <= i)
+        tr[i] = 0.0f;
+        if (i < kb)
         {
-            if (ti == 0.0f)
-                ts[i][tid] = 0.0f;
-            else if (tid == i)
-                ts[i][i] = ti;
-            else
+            const float ti = tau[k + i];
+            if (ti != 0.0f)
             {
-                float acc = 0.0f;
-                for (int q = tid; q < i; ++q) acc = fma_rn(ts[q][tid], d[i][q], acc);
-                ts[i][tid] = acc;
+                if (r == i)
+                    tr[i] = ti;
+                else if (r < i)
+                {
+                    float acc = 0.0f;
+#pragma unroll
+                    for (int q = 0; q < i; ++q)
+                        if (q >= r) acc = fma_rn(tr[q], d[i][q], acc);
+                    tr[i] = acc;
+                }
             }
         }
-        __syncwarp();
     }
-    for (int i = 0; i < kb; ++i)
-        if (tid <= i) T[i * NB + tid] = ts[i][tid];
+#pragma unroll
+    for (int i = 0; i < NB; ++i)
+        if (i < kb && r <= i) T[i * NB + r] = tr[i];
 }
 
 // C = C - V op(T) (V^T C) (LEFT: one warp per column of C, reflector index = C's row) or
@@ -516,21 +522,44 @@ __global__ void __launch_bounds__(APPLY_WARPS * 32, 3) qr_apply_kernel(const flo
     }
 }
 
-// R X = Y for one right-hand side per block: x_p = x_p / R_pp, then x_i -= R_ip x_p, p descending.
+// R X = Y for one right-hand side per block, in 32-column blocks from the bottom: warp 0
+// solves the diagonal block with the right-hand side in its lanes (x_p = x_p / R_pp, then
+// x_i -= R_ip x_p, p descending, R's block columns preloaded in registers), then every
+// thread applies the block's columns to the rows above it, p descending.  Each x_i receives
+// its updates in descending p, as a column sweep would.
 __global__ void __launch_bounds__(1024) qr_trsv_kernel(const float *R, int ldr, int n, const float *Y, int ldy,
                                                        float *X, int ldx)
 {
     extern __shared__ float xs[];
-    const int j = blockIdx.x, tid = threadIdx.x;
+    const int j = blockIdx.x, tid = threadIdx.x, lane = tid & 31;
     for (int i = tid; i < n; i += blockDim.x) xs[i] = Y[(int64_t)j * ldy + i];
     __syncthreads();
-    for (int p = n - 1; p >= 0; --p)
+    for (int c0 = (n - 1) & ~31; c0 >= 0; c0 -= 32)
     {
-        const float *rp = R + (int64_t)p * ldr;
-        if (tid == 0) xs[p] = div_rn(xs[p], rp[p]);
+        const int cw = min(32, n - c0);
+        if (tid < 32)
+        {
+            float r[32];
+#pragma unroll
+            for (int q = 0; q < 32; ++q)
+                r[q] = lane < cw && q < cw ? R[(int64_t)(c0 + q) * ldr + c0 + lane] : 1.0f;
+            float x = lane < cw ? xs[c0 + lane] : 0.0f;
+#pragma unroll
+            for (int q = 31; q >= 0; --q)
+            {
+                if (q < cw && lane == q) x = div_rn(x, r[q]);
+                const float xp = __shfl_sync(0xffffffffu, x, q);
+                if (q < cw && lane < q) x = fma_rn(-r[q], xp, x);
+            }
+            if (lane < cw) xs[c0 + lane] = x;
+        }
         __syncthreads();
-        const float xp = xs[p];
-        for (int i = tid; i < p; i += blockDim.x) xs[i] = fma_rn(-rp[i], xp, xs[i]);
+        for (int i = tid; i < c0; i += blockDim.x)
+        {
+            float x = xs[i];
+            for (int q = cw - 1; q >= 0; --q) x = fma_rn(-R[(int64_t)(c0 + q) * ldr + i], xs[c0 + q], x);
+            xs[i] = x;
+        }
         __syncthreads();
     }
     for (int i = tid; i < n; i += blockDim.x) X[(int64_t)j * ldx + i] = xs[i];
