@@ -1172,9 +1172,9 @@ def measure_qr(handle, args, steps=3):
         a0 = torch.randn(n * n, device="cuda", generator=g)
         a = torch.empty_like(a0)
         tau = torch.empty(n, device="cuda")
-        work = torch.empty(1024, device="cuda")
+        work = torch.empty(2048, device="cuda")
         ms = timed(lambda: aclsolver.check(lib.aclsolverSgeqrf(handle.value, n, n, a.data_ptr(), n, tau.data_ptr(),
-                                                                work.data_ptr(), 1024, info.data_ptr())),
+                                                                work.data_ptr(), 2048, info.data_ptr())),
                    lambda: a.copy_(a0))
         assert int(info.item()) == 0
         flops = 4.0 * n ** 3 / 3
@@ -1212,9 +1212,9 @@ def measure_qr(handle, args, steps=3):
     a0 = torch.randn(2 * n * n, device="cuda", generator=g)
     a = torch.empty_like(a0)
     tau = torch.empty(2 * n, device="cuda")
-    work = torch.empty(2 * 1024, device="cuda")
+    work = torch.empty(2 * 2048, device="cuda")
     ms = timed(lambda: aclsolver.check(lib.aclsolverCgeqrf(handle.value, n, n, a.data_ptr(), n, tau.data_ptr(),
-                                                           work.data_ptr(), 1024, info.data_ptr())),
+                                                           work.data_ptr(), 2048, info.data_ptr())),
                lambda: a.copy_(a0))
     assert int(info.item()) == 0
     flops = 16.0 * n ** 3 / 3  # 4 n^3 / 3 complex multiply-adds, 4 real each
@@ -1261,9 +1261,9 @@ def run_profile_qr():
     n = 4096
     a = torch.randn(n * n, device="cuda", generator=g)
     tau = torch.empty(n, device="cuda")
-    work = torch.empty(1024, device="cuda")
+    work = torch.empty(2048, device="cuda")
     info = torch.zeros(1, dtype=torch.int32, device="cuda")
-    aclsolver.check(lib.aclsolverSgeqrf(handle.value, n, n, a.data_ptr(), n, tau.data_ptr(), work.data_ptr(), 1024,
+    aclsolver.check(lib.aclsolverSgeqrf(handle.value, n, n, a.data_ptr(), n, tau.data_ptr(), work.data_ptr(), 2048,
                                         info.data_ptr()))
     n, r = 2048, 4
     a = torch.randn(n * n, device="cuda", generator=g)
@@ -1279,8 +1279,8 @@ def run_profile_qr():
     n = 2048
     a = torch.randn(2 * n * n, device="cuda", generator=g)
     tau = torch.empty(2 * n, device="cuda")
-    work = torch.empty(2 * 1024, device="cuda")
-    aclsolver.check(lib.aclsolverCgeqrf(handle.value, n, n, a.data_ptr(), n, tau.data_ptr(), work.data_ptr(), 1024,
+    work = torch.empty(2 * 2048, device="cuda")
+    aclsolver.check(lib.aclsolverCgeqrf(handle.value, n, n, a.data_ptr(), n, tau.data_ptr(), work.data_ptr(), 2048,
                                         info.data_ptr()))
     torch.cuda.synchronize()
     handle.close()

@@ -17,8 +17,9 @@
 //   CCgels      src/ccgels/arch35/ccgels_host.cpp:22-150 (1 m (m < n), 2 n, 3 nrhs, 4 dA, 5 lda,
 //               6 dB, 7 ldb, 8 dX, 9 ldx, then dX overlapping dA or dB -> 8, nrhs > 128 -> 3,
 //               m or n > 4096 -> 1; 10 workspace, 11 bytes, 12 niter; screens dA -> 4, dB -> 6)
-// Workspace sizes are this build's: one 32 x 32 complex block factor, plus the reflector copy
-// (Cungqr) or tau and Q^H B (CCgels).
+// Workspace sizes are this build's: one 32 x 32 complex block factor (two for Cgeqrf and CCgels,
+// whose look-ahead keeps consecutive panels' factors), plus the reflector copy (Cungqr) or tau
+// and Q^H B (CCgels).
 #include <limits.h>
 
 #include <algorithm>
@@ -160,7 +161,7 @@ extern "C"
     {
         if (!handle) return ACLSOLVER_STATUS_HANDLE_IS_NULLPTR;
         if (!Lwork || geqrf_shape(m, n, A, lda)) return ACLSOLVER_STATUS_INVALID_VALUE;
-        *Lwork = m == 0 || n == 0 ? 0 : QR_T_FLOATS;
+        *Lwork = m == 0 || n == 0 ? 0 : QR_GEQRF_T_FLOATS;
         return ACLSOLVER_STATUS_SUCCESS;
     }
 
@@ -173,7 +174,7 @@ extern "C"
         const bool empty = m == 0 || n == 0;
         int b = geqrf_shape(m, n, A, lda);
         if (!b && !empty && !TAU) b = 5;
-        const int need = empty ? 0 : QR_T_FLOATS;
+        const int need = empty ? 0 : QR_GEQRF_T_FLOATS;
         if (!b && Lwork < need) b = 7;
         if (!b && need && !Workspace) b = 6;
         if (!devInfo) return ACLSOLVER_STATUS_INVALID_VALUE;

@@ -12,8 +12,8 @@
 // An argument error writes -i (i counted without the handle) to the info buffer when that
 // buffer is usable and returns INVALID_VALUE; shapes over the kernel limits return
 // NOT_SUPPORTED (SSgels: INVALID_VALUE with -1 / -3, as the reference).  Workspace sizes are
-// this build's: one 32 x 32 block factor, plus the reflector copy (Sorgqr) or tau and Q^T B
-// (SSgels).
+// this build's: one 32 x 32 block factor (two for Sgeqrf and SSgels, whose look-ahead keeps
+// consecutive panels' factors), plus the reflector copy (Sorgqr) or tau and Q^T B (SSgels).
 #include <stdio.h>
 
 #include <algorithm>
@@ -134,7 +134,7 @@ extern "C"
             return ACLSOLVER_STATUS_SUCCESS;
         }
         if (m > GEQRF_MAX_ROWS) return ACLSOLVER_STATUS_NOT_SUPPORTED;
-        *Lwork = QR_T_FLOATS;
+        *Lwork = QR_GEQRF_T_FLOATS;
         return ACLSOLVER_STATUS_SUCCESS;
     }
 
@@ -150,10 +150,11 @@ extern "C"
         if (!TAU) return bad(h, devInfo, 5);
         if (m > GEQRF_MAX_ROWS) return bad(h, devInfo, 1, ACLSOLVER_STATUS_NOT_SUPPORTED);
         if (!Workspace) return bad(h, devInfo, 6);
-        if (Lwork < QR_T_FLOATS) return bad(h, devInfo, 7);
+        if (Lwork < QR_GEQRF_T_FLOATS) return bad(h, devInfo, 7);
         if (!span_ok(A, (size_t)lda * n * sizeof(float), alignof(float))) return bad(h, devInfo, 3);
         if (!span_ok(TAU, (size_t)std::min(m, n) * sizeof(float), alignof(float))) return bad(h, devInfo, 5);
-        if (!span_ok(Workspace, (size_t)QR_T_FLOATS * sizeof(float), alignof(float))) return bad(h, devInfo, 6);
+        if (!span_ok(Workspace, (size_t)QR_GEQRF_T_FLOATS * sizeof(float), alignof(float)))
+            return bad(h, devInfo, 6);
         if (!span_ok(devInfo, sizeof(int), alignof(int))) return ACLSOLVER_STATUS_INVALID_VALUE;
         aclsolverStatus_t st = info_zero(h, devInfo);
         if (st != ACLSOLVER_STATUS_SUCCESS) return st;

@@ -16,6 +16,7 @@
 #include "complex_lu.cuh"
 #include "device_once.h"
 #include "launch_qr.h"
+#include "lookahead.h"
 
 namespace ops_solver
 {
@@ -722,20 +723,25 @@ cudaError_t launch_cgeqrf(float2 *A, int lda, int m, int n, float2 *tau, float2 
                                         return r;
                                     });
     const int lim = std::min(m, n);
+    // Look-ahead (panels on a high-priority stream beside the wide update), as the real family.
+    Lookahead la;
+    const bool ahead = e == cudaSuccess && m >= 512 && n > 3 * NB;
+    if (ahead) e = la.open(stream);
+    cudaStream_t ps = ahead ? la.panel : stream;
     for (int k = 0; k < lim && e == cudaSuccess; k += NB)
     {
         const int kb = std::min(NB, lim - k);
         const int64_t elems = (int64_t)(m - k) * kb;
         const int seg = panel_seg(m - k, kb, PANEL_SMEM_ELEMS);
         if (elems <= PANEL_SMEM_ELEMS)
-            cq_panel_kernel<1><<<1, PANEL_THREADS, (size_t)elems * sizeof(float2), stream>>>(A, lda, m, k, kb, tau);
+            cq_panel_kernel<1><<<1, PANEL_THREADS, (size_t)elems * sizeof(float2), ps>>>(A, lda, m, k, kb, tau);
         else if (seg > 0)
         {
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3((unsigned)((m - k + seg - 1) / seg));
             cfg.blockDim = dim3(PANEL_THREADS);
             cfg.dynamicSmemBytes = (size_t)seg * kb * sizeof(float2);
-            cfg.stream = stream;
+            cfg.stream = ps;
             cudaLaunchAttribute attr[1];
             attr[0].id = cudaLaunchAttributeClusterDimension;
             attr[0].val.clusterDim.x = cfg.gridDim.x;
@@ -746,17 +752,34 @@ cudaError_t launch_cgeqrf(float2 *A, int lda, int m, int n, float2 *tau, float2 
             e = cudaLaunchKernelEx(&cfg, cq_cluster_panel_kernel, A, lda, m, k, kb, seg, tau);
         }
         else if (2 * (int64_t)(m - k) <= PANEL_SMEM_ELEMS)
-            cq_panel_kernel<2><<<1, PANEL_THREADS, (size_t)2 * (m - k) * sizeof(float2), stream>>>(A, lda, m, k, kb,
+            cq_panel_kernel<2><<<1, PANEL_THREADS, (size_t)2 * (m - k) * sizeof(float2), ps>>>(A, lda, m, k, kb,
                                                                                                      tau);
         else
-            cq_panel_kernel<0><<<1, PANEL_THREADS, 0, stream>>>(A, lda, m, k, kb, tau);
+            cq_panel_kernel<0><<<1, PANEL_THREADS, 0, ps>>>(A, lda, m, k, kb, tau);
         if (e == cudaSuccess) e = cudaGetLastError();
         if (e == cudaSuccess && k + kb < n)
         {
-            e = cq_larft(A, lda, m, k, kb, tau, T, stream);
+            float2 *Tk = T + (size_t)((k / NB) & 1) * QR_T_FLOATS;  // panel p's T, read by its wide update
+            e = cq_larft(A, lda, m, k, kb, tau, Tk, ps);
+            const int next = ahead ? std::min(NB, n - k - kb) : n - k - kb;
+            // the previous wide update has reached the next panel's columns
+            if (e == cudaSuccess && ahead && k > 0) e = la.to_panel(stream);
             if (e == cudaSuccess)
-                e = cq_apply(false, true, A, lda, m, k, kb, T, A + (int64_t)(k + kb) * lda, lda, n - k - kb, stream);
+                e = cq_apply(false, true, A, lda, m, k, kb, Tk, A + (int64_t)(k + kb) * lda, lda, next, ps);
+            const int rest = n - k - kb - next;
+            if (e == cudaSuccess && rest > 0)
+            {
+                e = la.to_main(stream);  // T and the reflectors are ready
+                if (e == cudaSuccess)
+                    e = cq_apply(false, true, A, lda, m, k, kb, Tk, A + (int64_t)(k + kb + next) * lda, lda, rest,
+                                 stream);
+            }
         }
+    }
+    if (ahead)
+    {
+        const cudaError_t c = la.close(stream);
+        if (e == cudaSuccess) e = c;
     }
     return e;
 }
@@ -799,7 +822,7 @@ cudaError_t launch_cungqr(int m, int n, int k, float2 *A, int lda, const float2 
 size_t cgels_work_elems(int m, int n, int nrhs)
 {
     auto up = [](size_t x) { return (x + 31) & ~size_t(31); };
-    return up((size_t)std::max(n, 1)) + up((size_t)m * nrhs) + up(NB * NB);
+    return up((size_t)std::max(n, 1)) + up((size_t)m * nrhs) + up(QR_GEQRF_T_FLOATS);
 }
 
 cudaError_t launch_cgels(int m, int n, int nrhs, float2 *A, int lda, const float2 *B, int ldb, float2 *X, int ldx,

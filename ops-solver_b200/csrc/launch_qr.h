@@ -8,8 +8,10 @@ namespace ops_solver
 {
 constexpr int QR_BLOCK = 32;                    // reflectors per panel / block factor
 constexpr int QR_T_FLOATS = QR_BLOCK * QR_BLOCK;  // one block factor T
-// In-place Householder QR of one m x n matrix; tau gets min(m, n) scalars; T holds one
-// 32 x 32 block factor (QR_T_FLOATS floats of workspace).
+// The factorisations keep two block factors: with look-ahead, consecutive panels' T overlap.
+constexpr int QR_GEQRF_T_FLOATS = 2 * QR_T_FLOATS;
+// In-place Householder QR of one m x n matrix; tau gets min(m, n) scalars; T holds two
+// 32 x 32 block factors (QR_GEQRF_T_FLOATS floats of workspace).
 cudaError_t launch_sgeqrf(float *A, int lda, int m, int n, float *tau, float *T, cudaStream_t stream);
 // op(Q) C (side 0) or C op(Q) (side 1), trans 0 = Q, else Q^T; Q from k reflectors of A.
 cudaError_t launch_sormqr(int side, int trans, int m, int n, int k, const float *A, int lda, const float *tau,
@@ -29,7 +31,7 @@ cudaError_t launch_xlarft(int backward, int n, int k, const float *V, int ldv, c
 
 // ---- complex QR family (cqr.cu), complex64 as float2, column-major -------------------------
 // In-place Householder QR (clarfg convention); tau gets min(m, n) scalars; T holds
-// QR_T_FLOATS complex elements of workspace.
+// QR_GEQRF_T_FLOATS complex elements of workspace.
 cudaError_t launch_cgeqrf(float2 *A, int lda, int m, int n, float2 *tau, float2 *T, cudaStream_t stream);
 // op(Q) C (side 0) or C op(Q) (side 1), herm 0 = Q, else Q^H; Q from k reflectors of A.
 cudaError_t launch_cunmqr(int side, int herm, int m, int n, int k, const float2 *A, int lda, const float2 *tau,

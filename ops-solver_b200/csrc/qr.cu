@@ -28,6 +28,7 @@
 #include "common.cuh"
 #include "device_once.h"
 #include "launch_qr.h"
+#include "lookahead.h"
 
 namespace ops_solver
 {
@@ -738,6 +739,12 @@ cudaError_t launch_sgeqrf(float *A, int lda, int m, int n, float *tau, float *T,
                                                                      PANEL_SMEM_FLOATS * (int)sizeof(float));
                                         return r;
                                     });
+    // Look-ahead (panels on a high-priority stream beside the wide update) once the trailing
+    // matrix is wide and tall enough to keep the rest of the GPU busy.
+    Lookahead la;
+    const bool ahead = e == cudaSuccess && m >= 512 && n > 3 * NB;
+    if (ahead) e = la.open(stream);
+    cudaStream_t ps = ahead ? la.panel : stream;
     for (int k = 0; k < lim && e == cudaSuccess; k += NB)
     {
         const int kb = std::min(NB, lim - k);
@@ -745,8 +752,8 @@ cudaError_t launch_sgeqrf(float *A, int lda, int m, int n, float *tau, float *T,
         const int seg = panel_seg(m - k, kb, PANEL_SMEM_FLOATS);
         if (panel_floats <= PANEL_SMEM_FLOATS)
         {
-            qr_panel_kernel<true><<<1, PANEL_THREADS, (size_t)panel_floats * sizeof(float), stream>>>(A, lda, m, k, kb,
-                                                                                                       tau);
+            qr_panel_kernel<true><<<1, PANEL_THREADS, (size_t)panel_floats * sizeof(float), ps>>>(A, lda, m, k, kb,
+                                                                                                   tau);
             e = cudaGetLastError();
         }
         else if (seg > 0)
@@ -755,7 +762,7 @@ cudaError_t launch_sgeqrf(float *A, int lda, int m, int n, float *tau, float *T,
             cfg.gridDim = dim3((unsigned)((m - k + seg - 1) / seg));
             cfg.blockDim = dim3(PANEL_THREADS);
             cfg.dynamicSmemBytes = (size_t)seg * kb * sizeof(float);
-            cfg.stream = stream;
+            cfg.stream = ps;
             cudaLaunchAttribute attr[1];
             attr[0].id = cudaLaunchAttributeClusterDimension;
             attr[0].val.clusterDim.x = cfg.gridDim.x;
@@ -767,17 +774,33 @@ cudaError_t launch_sgeqrf(float *A, int lda, int m, int n, float *tau, float *T,
         }
         else  // two column buffers: 2 (m - k) floats, within PANEL_SMEM_FLOATS for m <= 25,600
         {
-            qr_panel_kernel<false><<<1, PANEL_THREADS, (size_t)2 * (m - k) * sizeof(float), stream>>>(A, lda, m, k,
-                                                                                                        kb, tau);
+            qr_panel_kernel<false><<<1, PANEL_THREADS, (size_t)2 * (m - k) * sizeof(float), ps>>>(A, lda, m, k, kb,
+                                                                                                    tau);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess && k + kb < n)
         {
-            e = larft(A, lda, m, k, kb, tau, T, stream);
+            float *Tk = T + (size_t)((k / NB) & 1) * QR_T_FLOATS;  // panel p's T, read by its wide update
+            e = larft(A, lda, m, k, kb, tau, Tk, ps);
+            const int next = ahead ? std::min(NB, n - k - kb) : n - k - kb;
+            // the previous wide update has reached the next panel's columns
+            if (e == cudaSuccess && ahead && k > 0) e = la.to_panel(stream);
             if (e == cudaSuccess)
-                e = apply_block(false, true, A, lda, m, k, kb, T, A + (int64_t)(k + kb) * lda, lda, n - k - kb,
-                                stream);
+                e = apply_block(false, true, A, lda, m, k, kb, Tk, A + (int64_t)(k + kb) * lda, lda, next, ps);
+            const int rest = n - k - kb - next;
+            if (e == cudaSuccess && rest > 0)
+            {
+                e = la.to_main(stream);  // T and the reflectors are ready
+                if (e == cudaSuccess)
+                    e = apply_block(false, true, A, lda, m, k, kb, Tk, A + (int64_t)(k + kb + next) * lda, lda, rest,
+                                    stream);
+            }
         }
+    }
+    if (ahead)
+    {
+        const cudaError_t c = la.close(stream);
+        if (e == cudaSuccess) e = c;
     }
     return e;
 }
@@ -821,7 +844,7 @@ cudaError_t launch_sorgqr(int m, int n, int k, float *A, int lda, const float *t
 size_t sgels_work_floats(int m, int n, int nrhs)
 {
     auto up = [](size_t x) { return (x + 63) & ~size_t(63); };
-    return up((size_t)std::max(n, 1)) + up((size_t)m * nrhs) + up(NB * NB);
+    return up((size_t)std::max(n, 1)) + up((size_t)m * nrhs) + up(QR_GEQRF_T_FLOATS);
 }
 
 cudaError_t launch_sgels(int m, int n, int nrhs, float *A, int lda, const float *B, int ldb, float *X, int ldx,

@@ -211,8 +211,8 @@ def test_nonfinite_inputs_are_rejected_after_a_screen(handle):
     a = crand(40, 20, 1)
     a[33, 5] = np.complex64(complex(0, np.inf))
     dm = CMatrices(a[None], 41)
-    tau, w, info = cwork(20), cwork(1024), info_buffer(1)
-    st = lib.aclsolverCgeqrf(handle.value, 40, 20, dm.tensor.data_ptr(), 41, tau.data_ptr(), w.data_ptr(), 1024,
+    tau, w, info = cwork(20), cwork(2048), info_buffer(1)
+    st = lib.aclsolverCgeqrf(handle.value, 40, 20, dm.tensor.data_ptr(), 41, tau.data_ptr(), w.data_ptr(), 2048,
                              info.data_ptr())
     handle.stream.synchronize()
     assert st == aclsolver.INVALID_VALUE and int(info.cpu()[0]) == -3 and dm.unchanged()
@@ -247,11 +247,11 @@ def test_argument_ladders_write_minus_the_index(handle):
         handle.stream.synchronize()
         return int(info.cpu()[0])
 
-    assert lib.aclsolverCgeqrf(handle.value, 16, 16, p, 16, None, w.data_ptr(), 1024, info.data_ptr()) == 3
+    assert lib.aclsolverCgeqrf(handle.value, 16, 16, p, 16, None, w.data_ptr(), 2048, info.data_ptr()) == 3
     assert code() == -5
-    assert lib.aclsolverCgeqrf(handle.value, 16, 16, p, 16, tau.data_ptr(), w.data_ptr(), 1023, info.data_ptr()) == 3
+    assert lib.aclsolverCgeqrf(handle.value, 16, 16, p, 16, tau.data_ptr(), w.data_ptr(), 2047, info.data_ptr()) == 3
     assert code() == -7
-    assert lib.aclsolverCgeqrf(handle.value, 16, 16, p, 16, tau.data_ptr(), None, 1024, info.data_ptr()) == 3
+    assert lib.aclsolverCgeqrf(handle.value, 16, 16, p, 16, tau.data_ptr(), None, 2048, info.data_ptr()) == 3
     assert code() == -6
     assert lib.aclsolverCgeqrf(handle.value, 0, 16, None, 1, None, None, 0, info.data_ptr()) == 0 and code() == 0
     assert lib.aclsolverCungqr(handle.value, 16, 17, 4, p, 16, tau.data_ptr(), w.data_ptr(), 2048,

@@ -121,7 +121,7 @@ def test_host_argument_ladders_without_a_gpu():
     fake = C.c_void_p(16)  # never dereferenced by a query or an argument rejection
     lw = C.c_int(-1)
     assert lib.aclsolverCgeqrf_bufferSize(None, 4, 4, None, 4, C.byref(lw)) == NULL_HANDLE
-    assert lib.aclsolverCgeqrf_bufferSize(fake, 10, 4, C.c_void_p(64), 10, C.byref(lw)) == 0 and lw.value == 1024
+    assert lib.aclsolverCgeqrf_bufferSize(fake, 10, 4, C.c_void_p(64), 10, C.byref(lw)) == 0 and lw.value == 2048
     assert lib.aclsolverCgeqrf_bufferSize(fake, 0, 4, None, 1, C.byref(lw)) == 0 and lw.value == 0
     assert lib.aclsolverCgeqrf_bufferSize(fake, 10, 4, None, 10, C.byref(lw)) == INVALID  # A null
     assert lib.aclsolverCgeqrf_bufferSize(fake, 10, 4, C.c_void_p(64), 9, C.byref(lw)) == INVALID

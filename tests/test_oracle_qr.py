@@ -78,7 +78,7 @@ def test_host_argument_ladders_without_a_gpu():
     lib = aclsolver.library()
     INVALID, NOT_SUPPORTED, NULL_HANDLE = 3, 7, 9
     lw = C.c_int(-1)
-    assert lib.aclsolverSgeqrf_bufferSize(None, 10, 4, None, 10, C.byref(lw)) == 0 and lw.value == 1024
+    assert lib.aclsolverSgeqrf_bufferSize(None, 10, 4, None, 10, C.byref(lw)) == 0 and lw.value == 2048
     assert lib.aclsolverSgeqrf_bufferSize(None, 0, 4, None, 1, C.byref(lw)) == 0 and lw.value == 0
     assert lib.aclsolverSgeqrf_bufferSize(None, 10, 4, None, 9, C.byref(lw)) == INVALID
     assert lib.aclsolverSgeqrf_bufferSize(None, 8193, 4, None, 8193, C.byref(lw)) == NOT_SUPPORTED
