@@ -71,140 +71,111 @@ __device__ __forceinline__ float2 fold2(float2 p) { return make_float2(fold1(p.x
 
 __device__ __forceinline__ bool czero2(float2 v) { return v.x == 0.0f && v.y == 0.0f; }
 
-// Panel columns [k, k + kb) of rows [k, m).  MODE 1: the panel is staged in shared memory.
-// MODE 2: the panel stays in A and two column buffers in shared memory mirror the reflector
-// column c and the next column c + 1 (written by the warp that updates it), so only the
-// target columns are read from A.  MODE 0 (more rows than the buffers hold): everything is
-// read from A.  Same arithmetic in every mode.
-template <int MODE>
+// Panel columns [k, k + kb) of rows [k, m), in shared memory (SMEM) or, for panels taller
+// than eight blocks hold, in A.  Per column c, every reduction over the rows below c is taken
+// at once from the column as it stands: warp 0 forms sumsq = sum |x_i|^2 and warp w >= 1
+// forms S_j = sum conj(x_i) A(i, j) for column j = c + w, in parallel.  Thread 0 then forms
+// beta, tau, d = alpha - beta, den = |d|^2 and g = d / den; warp w applies
+// w_j = conj(tau) (A(c, j) + g S_j) with v_i = x_i / d formed on the fly; column c itself is
+// divided during the next column's reductions.
+__device__ __forceinline__ float2 cq_reflect(float2 x, float dr, float di, float den)
+{
+    return make_float2(div_rn(add_rn(mul_rn(x.x, dr), mul_rn(x.y, di)), den),
+                       div_rn(sub_rn(mul_rn(x.y, dr), mul_rn(x.x, di)), den));
+}
+
+template <bool SMEM>
 __global__ void __launch_bounds__(PANEL_THREADS) cq_panel_kernel(float2 *A, int lda, int m, int k, int kb, float2 *tau)
 {
     extern __shared__ float2 sp[];
-    __shared__ float2 s_tau;
-    __shared__ float s_dr, s_di, s_den;
+    __shared__ float2 s_S[NB], s_tau, s_g;
+    __shared__ float s_sumsq, s_dr, s_di, s_den;
     __shared__ int s_apply;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int H = m - k;
     auto at = [&](int j, int row) -> float2 & {
-        return MODE == 1 ? sp[(int64_t)(j - k) * H + (row - k)] : A[(int64_t)j * lda + row];
+        return SMEM ? sp[(int64_t)(j - k) * H + (row - k)] : A[(int64_t)j * lda + row];
     };
-    auto col = [&](int j, int row) -> float2 & { return MODE == 2 ? sp[(j & 1) * H + (row - k)] : at(j, row); };
-    if (MODE == 1)
+    if (SMEM)
+    {
         for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) sp[idx] = A[(int64_t)(k + idx / H) * lda + k + idx % H];
-    if (MODE == 2)
-        for (int row = k + tid; row < m; row += PANEL_THREADS) col(k, row) = A[(int64_t)k * lda + row];
-    __syncthreads();
-    constexpr int U = 8;
+        __syncthreads();
+    }
+    bool prev_apply = false;
+    float pdr = 0.0f, pdi = 0.0f, pden = 1.0f;
     for (int c = k; c < k + kb; ++c)
     {
+        if (prev_apply)  // column c - 1 becomes its reflector
+            for (int row = c + tid; row < m; row += PANEL_THREADS) at(c - 1, row) = cq_reflect(at(c - 1, row), pdr, pdi, pden);
+        const int j = c + warp;
         if (warp == 0)
         {
             float p = 0.0f;
-            for (int base = (c + 1) & ~31; base < m; base += 32 * U)
+            for (int row = c + 1 + lane; row < m; row += 32)
             {
-                float2 x[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                {
-                    const int row = base + 32 * u + lane;
-                    x[u] = row > c && row < m ? col(c, row) : make_float2(0.0f, 0.0f);
-                }
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                {
-                    const int row = base + 32 * u + lane;
-                    if (row > c && row < m) p = fma_rn(x[u].y, x[u].y, fma_rn(x[u].x, x[u].x, p));
-                }
+                const float2 x = at(c, row);
+                p = fma_rn(x.y, x.y, fma_rn(x.x, x.x, p));
             }
-            const float sumsq = fold1(p);
-            if (lane == 0)
-            {
-                const float2 al = col(c, c);
-                float2 t = make_float2(0.0f, 0.0f);
-                int apply = 0;
-                if (!(sumsq == 0.0f && al.y == 0.0f))
-                {
-                    const float norm = sqrt_rn(add_rn(add_rn(mul_rn(al.x, al.x), mul_rn(al.y, al.y)), sumsq));
-                    const float beta = -copysignf(norm, al.x);
-                    t = make_float2(div_rn(sub_rn(beta, al.x), beta), -div_rn(al.y, beta));
-                    const float dr = sub_rn(al.x, beta), di = al.y;
-                    s_dr = dr;
-                    s_di = di;
-                    s_den = add_rn(mul_rn(dr, dr), mul_rn(di, di));
-                    at(c, c) = make_float2(beta, 0.0f);
-                    apply = 1;
-                }
-                tau[c] = t;
-                s_tau = t;
-                s_apply = apply;
-            }
+            const float part = fold1(p);
+            if (lane == 0) s_sumsq = part;
         }
-        __syncthreads();
-        const bool apply = s_apply != 0;
-        const float2 t = s_tau;
-        if (apply)
-        {
-            const float dr = s_dr, di = s_di, den = s_den;
-            for (int row = c + 1 + tid; row < m; row += PANEL_THREADS)
-            {
-                const float2 x = col(c, row);
-                const float2 v = make_float2(div_rn(add_rn(mul_rn(x.x, dr), mul_rn(x.y, di)), den),
-                                             div_rn(sub_rn(mul_rn(x.y, dr), mul_rn(x.x, di)), den));
-                at(c, row) = v;
-                if (MODE == 2) col(c, row) = v;
-            }
-        }
-        __syncthreads();
-        const int j = c + warp;
-        if (apply && warp >= 1 && j < k + kb)
+        else if (j < k + kb)
         {
             float2 p = make_float2(0.0f, 0.0f);
-            for (int base = c & ~31; base < m; base += 32 * U)
-            {
-                float2 x[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                {
-                    const int row = base + 32 * u + lane;
-                    x[u] = row >= c && row < m ? at(j, row) : make_float2(0.0f, 0.0f);
-                }
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                {
-                    const int row = base + 32 * u + lane;
-                    if (row >= c && row < m)
-                        p = cq_conjdot(p, row == c ? make_float2(1.0f, 0.0f) : col(c, row), x[u]);
-                }
-            }
-            const float2 w = cq_mulc(t, fold2(p));
-            for (int base = c & ~31; base < m; base += 32 * U)
-            {
-                float2 x[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                {
-                    const int row = base + 32 * u + lane;
-                    x[u] = row >= c && row < m ? at(j, row) : make_float2(0.0f, 0.0f);
-                }
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                {
-                    const int row = base + 32 * u + lane;
-                    if (row >= c && row < m)
-                    {
-                        const float2 y = clu::csubmul(x[u], row == c ? make_float2(1.0f, 0.0f) : col(c, row), w);
-                        at(j, row) = y;
-                        if (MODE == 2 && j == c + 1) col(j, row) = y;
-                    }
-                }
-            }
+            for (int row = c + 1 + lane; row < m; row += 32) p = cq_conjdot(p, at(c, row), at(j, row));
+            const float2 part = fold2(p);
+            if (lane == 0) s_S[warp] = part;
         }
-        else if (MODE == 2 && !apply && warp == 1 && j < k + kb)
-            for (int row = c + 1 + lane; row < m; row += 32) col(j, row) = at(j, row);
+        __syncthreads();
+        if (tid == 0)
+        {
+            const float2 al = at(c, c);
+            float2 t = make_float2(0.0f, 0.0f);
+            int apply = 0;
+            if (!(s_sumsq == 0.0f && al.y == 0.0f))
+            {
+                const float norm = sqrt_rn(add_rn(add_rn(mul_rn(al.x, al.x), mul_rn(al.y, al.y)), s_sumsq));
+                const float beta = -copysignf(norm, al.x);
+                t = make_float2(div_rn(sub_rn(beta, al.x), beta), -div_rn(al.y, beta));
+                const float dr = sub_rn(al.x, beta), di = al.y;
+                const float den = add_rn(mul_rn(dr, dr), mul_rn(di, di));
+                s_dr = dr;
+                s_di = di;
+                s_den = den;
+                s_g = make_float2(div_rn(dr, den), div_rn(di, den));
+                at(c, c) = make_float2(beta, 0.0f);
+                apply = 1;
+            }
+            tau[c] = t;
+            s_tau = t;
+            s_apply = apply;
+        }
+        __syncthreads();
+        prev_apply = s_apply != 0;
+        if (prev_apply)
+        {
+            pdr = s_dr;
+            pdi = s_di;
+            pden = s_den;
+        }
+        if (prev_apply && warp >= 1 && j < k + kb)
+        {
+            const float2 w = cq_mulc(s_tau, cq_fma(s_g, s_S[warp], at(j, c)));
+            __syncwarp();
+            if (lane == 0) at(j, c) = clu::csubmul(at(j, c), make_float2(1.0f, 0.0f), w);
+            for (int row = c + 1 + lane; row < m; row += 32)
+                at(j, row) = clu::csubmul(at(j, row), cq_reflect(at(c, row), pdr, pdi, pden), w);
+        }
         __syncthreads();
     }
-    if (MODE == 1)
+    if (prev_apply)
+        for (int row = k + kb + tid; row < m; row += PANEL_THREADS)
+            at(k + kb - 1, row) = cq_reflect(at(k + kb - 1, row), pdr, pdi, pden);
+    if (SMEM)
+    {
+        __syncthreads();
         for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) A[(int64_t)(k + idx / H) * lda + k + idx % H] = sp[idx];
+    }
 }
 
 // Rows per block of a panel spread over a cluster (0: the panel fits one block, or is too
@@ -217,16 +188,18 @@ __host__ __device__ inline int panel_seg(int H, int kb, int budget)
 }
 
 // A tall panel over a cluster of ceil((m - k) / seg) blocks, block g holding rows
-// [k + g seg, k + (g + 1) seg) in shared memory; per-block lane sums, folded, published and
-// added in ascending block order by every block through distributed shared memory.
+// [k + g seg, k + (g + 1) seg) in shared memory and running the one-block schedule on them;
+// the per-block lane sums (and block 0's row of diagonal entries) are published in shared
+// memory double-buffered by column parity and, after one cluster barrier per column, added
+// in ascending block order by every block through distributed shared memory.
 __global__ void __launch_bounds__(PANEL_THREADS) cq_cluster_panel_kernel(float2 *A, int lda, int m, int k, int kb,
                                                                          int seg, float2 *tau)
 {
     namespace cg = cooperative_groups;
     extern __shared__ float2 sp[];  // sp[(j - k) * seg + (row - r0)]
-    __shared__ float2 s_alpha, s_dot[NB];
-    __shared__ float s_norm;
-    __shared__ float2 s_tau;
+    __shared__ float pub_sumsq[2];
+    __shared__ float2 pub_S[2][NB], pub_row[2][NB];
+    __shared__ float2 s_tau, s_g;
     __shared__ float s_dr, s_di, s_den;
     __shared__ int s_apply;
     cg::cluster_group cluster = cg::this_cluster();
@@ -238,8 +211,15 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_cluster_panel_kernel(float2 
     for (int idx = tid; idx < rows * kb; idx += PANEL_THREADS)
         sp[(idx / rows) * seg + idx % rows] = A[(int64_t)(k + idx / rows) * lda + r0 + idx % rows];
     __syncthreads();
+    bool prev_apply = false;
+    float pdr = 0.0f, pdi = 0.0f, pden = 1.0f;
     for (int c = k; c < k + kb; ++c)
     {
+        const int par = c & 1, owner = (c - k) / seg;
+        if (prev_apply)
+            for (int row = max(r0, c) + tid; row < r1; row += PANEL_THREADS)
+                at(c - 1, row) = cq_reflect(at(c - 1, row), pdr, pdi, pden);
+        const int j = c + warp;
         if (warp == 0)
         {
             float p = 0.0f;
@@ -250,21 +230,25 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_cluster_panel_kernel(float2 
                     p = fma_rn(x.y, x.y, fma_rn(x.x, x.x, p));
                 }
             const float part = fold1(p);
-            if (lane == 0)
-            {
-                s_norm = part;
-                if (c >= r0 && c < r1) s_alpha = at(c, c);
-            }
+            if (lane == 0) pub_sumsq[par] = part;
         }
+        else if (j < k + kb)
+        {
+            float2 p = make_float2(0.0f, 0.0f);
+            for (int row = r0 + lane; row < r1; row += 32)
+                if (row > c) p = cq_conjdot(p, at(c, row), at(j, row));
+            const float2 part = fold2(p);
+            if (lane == 0) pub_S[par][warp] = part;
+        }
+        if (j < k + kb && lane == 0 && g == owner) pub_row[par][warp] = at(j, c);
         cluster.sync();
         if (tid == 0)
         {
             float parts[8];
-            for (int q = 0; q < G; ++q) parts[q] = *cluster.map_shared_rank(&s_norm, q);
+            for (int q = 0; q < G; ++q) parts[q] = *cluster.map_shared_rank(&pub_sumsq[par], q);
             float sumsq = parts[0];
             for (int q = 1; q < G; ++q) sumsq = add_rn(sumsq, parts[q]);
-            const int owner = (c - k) / seg;
-            const float2 al = *cluster.map_shared_rank(&s_alpha, owner);
+            const float2 al = *cluster.map_shared_rank(&pub_row[par][0], owner);
             float2 t = make_float2(0.0f, 0.0f);
             int apply = 0;
             if (!(sumsq == 0.0f && al.y == 0.0f))
@@ -273,9 +257,11 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_cluster_panel_kernel(float2 
                 const float beta = -copysignf(norm, al.x);
                 t = make_float2(div_rn(sub_rn(beta, al.x), beta), -div_rn(al.y, beta));
                 const float dr = sub_rn(al.x, beta), di = al.y;
+                const float den = add_rn(mul_rn(dr, dr), mul_rn(di, di));
                 s_dr = dr;
                 s_di = di;
-                s_den = add_rn(mul_rn(dr, dr), mul_rn(di, di));
+                s_den = den;
+                s_g = make_float2(div_rn(dr, den), div_rn(di, den));
                 if (owner == g) at(c, c) = make_float2(beta, 0.0f);
                 apply = 1;
             }
@@ -284,43 +270,31 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_cluster_panel_kernel(float2 
             s_apply = apply;
         }
         __syncthreads();
-        const bool apply = s_apply != 0;
-        const float2 t = s_tau;
-        if (apply)
+        prev_apply = s_apply != 0;
+        if (prev_apply)
         {
-            const float dr = s_dr, di = s_di, den = s_den;
-            for (int row = max(r0, c + 1) + tid; row < r1; row += PANEL_THREADS)
-            {
-                const float2 x = at(c, row);
-                at(c, row) = make_float2(div_rn(add_rn(mul_rn(x.x, dr), mul_rn(x.y, di)), den),
-                                         div_rn(sub_rn(mul_rn(x.y, dr), mul_rn(x.x, di)), den));
-            }
+            pdr = s_dr;
+            pdi = s_di;
+            pden = s_den;
         }
-        __syncthreads();
-        const int j = c + warp;
-        const bool mine = apply && warp >= 1 && j < k + kb;
-        if (mine)
-        {
-            float2 p = make_float2(0.0f, 0.0f);
-            for (int row = r0 + lane; row < r1; row += 32)
-                if (row >= c) p = cq_conjdot(p, row == c ? make_float2(1.0f, 0.0f) : at(c, row), at(j, row));
-            const float2 part = fold2(p);
-            if (lane == 0) s_dot[warp] = part;
-        }
-        cluster.sync();
-        if (mine)
+        if (prev_apply && warp >= 1 && j < k + kb)
         {
             float2 parts[8];
-            for (int q = 0; q < G; ++q) parts[q] = *cluster.map_shared_rank(&s_dot[warp], q);
-            float2 dot = parts[0];
-            for (int q = 1; q < G; ++q) dot = make_float2(add_rn(dot.x, parts[q].x), add_rn(dot.y, parts[q].y));
-            const float2 w = cq_mulc(t, dot);
+            for (int q = 0; q < G; ++q) parts[q] = *cluster.map_shared_rank(&pub_S[par][warp], q);
+            float2 S = parts[0];
+            for (int q = 1; q < G; ++q) S = make_float2(add_rn(S.x, parts[q].x), add_rn(S.y, parts[q].y));
+            const float2 acj = *cluster.map_shared_rank(&pub_row[par][warp], owner);
+            const float2 w = cq_mulc(s_tau, cq_fma(s_g, S, acj));
+            if (lane == 0 && g == owner) at(j, c) = clu::csubmul(acj, make_float2(1.0f, 0.0f), w);
             for (int row = r0 + lane; row < r1; row += 32)
-                if (row >= c) at(j, row) = clu::csubmul(at(j, row), row == c ? make_float2(1.0f, 0.0f) : at(c, row), w);
+                if (row > c) at(j, row) = clu::csubmul(at(j, row), cq_reflect(at(c, row), pdr, pdi, pden), w);
         }
         __syncthreads();
     }
-    cluster.sync();  // no block leaves while another may still read its partials
+    if (prev_apply)
+        for (int row = max(r0, k + kb) + tid; row < r1; row += PANEL_THREADS)
+            at(k + kb - 1, row) = cq_reflect(at(k + kb - 1, row), pdr, pdi, pden);
+    cluster.sync();  // no block leaves while another may still read what it published
     for (int idx = tid; idx < rows * kb; idx += PANEL_THREADS)
         A[(int64_t)(k + idx / rows) * lda + r0 + idx % rows] = sp[(idx / rows) * seg + idx % rows];
 }
@@ -710,12 +684,8 @@ cudaError_t launch_cgeqrf(float2 *A, int lda, int m, int n, float2 *tau, float2 
                                     []
                                     {
                                         cudaError_t r = cudaFuncSetAttribute(
-                                            cq_panel_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            cq_panel_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             PANEL_SMEM_ELEMS * (int)sizeof(float2));
-                                        if (r == cudaSuccess)
-                                            r = cudaFuncSetAttribute(cq_panel_kernel<2>,
-                                                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                                     PANEL_SMEM_ELEMS * (int)sizeof(float2));
                                         if (r == cudaSuccess)
                                             r = cudaFuncSetAttribute(cq_cluster_panel_kernel,
                                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -734,7 +704,7 @@ cudaError_t launch_cgeqrf(float2 *A, int lda, int m, int n, float2 *tau, float2 
         const int64_t elems = (int64_t)(m - k) * kb;
         const int seg = panel_seg(m - k, kb, PANEL_SMEM_ELEMS);
         if (elems <= PANEL_SMEM_ELEMS)
-            cq_panel_kernel<1><<<1, PANEL_THREADS, (size_t)elems * sizeof(float2), ps>>>(A, lda, m, k, kb, tau);
+            cq_panel_kernel<true><<<1, PANEL_THREADS, (size_t)elems * sizeof(float2), ps>>>(A, lda, m, k, kb, tau);
         else if (seg > 0)
         {
             cudaLaunchConfig_t cfg = {};
@@ -751,11 +721,8 @@ cudaError_t launch_cgeqrf(float2 *A, int lda, int m, int n, float2 *tau, float2 
             cfg.numAttrs = 1;
             e = cudaLaunchKernelEx(&cfg, cq_cluster_panel_kernel, A, lda, m, k, kb, seg, tau);
         }
-        else if (2 * (int64_t)(m - k) <= PANEL_SMEM_ELEMS)
-            cq_panel_kernel<2><<<1, PANEL_THREADS, (size_t)2 * (m - k) * sizeof(float2), ps>>>(A, lda, m, k, kb,
-                                                                                                     tau);
         else
-            cq_panel_kernel<0><<<1, PANEL_THREADS, 0, ps>>>(A, lda, m, k, kb, tau);
+            cq_panel_kernel<false><<<1, PANEL_THREADS, 0, ps>>>(A, lda, m, k, kb, tau);
         if (e == cudaSuccess) e = cudaGetLastError();
         if (e == cudaSuccess && k + kb < n)
         {

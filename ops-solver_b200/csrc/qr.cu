@@ -9,14 +9,14 @@
 // lane r mod 32 (an FMA chain in ascending row order), and a warp butterfly
 // (v += shfl_xor(v, off), off = 16 .. 1) combines the lanes, so the results do not depend
 // on the grid and the CPU oracle restates them exactly:
-//   qr_panel_kernel      one block factors a panel (in shared memory when it fits, else with
-//                        the current and next columns mirrored there): warp 0 forms the
-//                        reflector, the other warps apply it to one column each
+//   qr_panel_kernel /    one block factors a panel in shared memory, or an eight-block cluster
+//   qr_cluster_panel_kernel   a taller one: per column, warp 0 sums the squares and the other
+//                        warps the products with their columns at once, then the reflector
 //   qr_gram_kernel /     T of the panel (forward, columnwise): the reflector products one warp
 //   qr_tri_kernel        per pair across the grid, then slarft's recurrence in one warp
 //   qr_apply_kernel      one warp per column (left) or row (right) of C: W = V^T c by lane
-//                        sums over 32-row chunks of V staged in shared memory, W2 = op(T) W,
-//                        then c -= V W2 with an FMA chain over the reflectors
+//                        sums over 128-row chunks of V double-buffered in shared memory,
+//                        W2 = op(T) W, then c -= V W2 with an FMA chain over the reflectors
 //   qr_trsv_kernel       R X = Y, one block per right-hand side, 32-column blocks from the bottom
 //   xlarft_gram_kernel / xlarft_tri_kernel   Xlarft: the reflector products over 32 x 32
 //                        blocks, then slarft's recurrence on a packed triangle (k <= 256)
@@ -45,138 +45,82 @@ __device__ __forceinline__ float lane_fold(float p)
     return p;
 }
 
-// Panel columns [k, k + kb) of rows [k, m).  SMEM: the panel is staged in shared memory
-// (pitch m - k).  Otherwise it stays in A (L2-resident) and two column buffers in shared
-// memory mirror the reflector column c and the next column c + 1 (written by the warp that
-// updates it), so the norm and the reflector reads come from shared memory and only the
-// target columns are read from A, twelve loads ahead of each lane's FMA chain.  Same
-// arithmetic either way.
+// Panel columns [k, k + kb) of rows [k, m), staged in shared memory (pitch m - k).  Per column
+// c, every reduction over the rows below c is taken at once from the column as it stands:
+// warp 0 forms sumsq = sum x_i^2 and warp w >= 1 forms S_j = sum x_i A(i, j) for column
+// j = c + w (lane sums), in parallel.  Thread 0 then forms beta, tau and scale =
+// 1 / (alpha - beta); warp w applies w_j = tau fma(scale, S_j, A(c, j)) with v_i = x_i scale
+// (v_c = 1) formed on the fly; column c itself is scaled during the next column's reductions.
 constexpr int PANEL_SMEM_FLOATS = 50 * 1024;
 
-template <bool SMEM>
 __global__ void __launch_bounds__(PANEL_THREADS) qr_panel_kernel(float *A, int lda, int m, int k, int kb, float *tau)
 {
     extern __shared__ float sp[];
-    __shared__ float s_tau, s_scale;
+    __shared__ float s_sumsq, s_S[NB], s_tau, s_scale;
     __shared__ int s_apply;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int H = m - k;
-    // the panel (SMEM) or the column buffers: column c lives in sp + (c & 1) * H
-    auto at = [&](int j, int row) -> float & {
-        return SMEM ? sp[(int64_t)(j - k) * H + (row - k)] : A[(int64_t)j * lda + row];
-    };
-    auto col = [&](int j, int row) -> float & { return SMEM ? at(j, row) : sp[(j & 1) * H + (row - k)]; };
-    if (SMEM)
-        for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) sp[idx] = A[(int64_t)(k + idx / H) * lda + k + idx % H];
-    else
-        for (int row = k + tid; row < m; row += PANEL_THREADS) col(k, row) = A[(int64_t)k * lda + row];
+    auto at = [&](int j, int row) -> float & { return sp[(j - k) * H + (row - k)]; };
+    for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) sp[idx] = A[(int64_t)(k + idx / H) * lda + k + idx % H];
     __syncthreads();
-    constexpr int U = 8, UX = SMEM ? 8 : 12;
+    bool prev_apply = false;
+    float prev_scale = 0.0f;
     for (int c = k; c < k + kb; ++c)
     {
-        if (warp == 0)
+        if (prev_apply)  // column c - 1 becomes its reflector
+            for (int row = c + tid; row < m; row += PANEL_THREADS) at(c - 1, row) = mul_rn(at(c - 1, row), prev_scale);
+        const int j = c + warp;
+        if (m - c > 1 && j < k + kb)
         {
             float p = 0.0f;
-            for (int base = (c + 1) & ~31; base < m; base += 32 * U)
-            {
-                float x[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                {
-                    const int row = base + 32 * u + lane;
-                    x[u] = row > c && row < m ? col(c, row) : 0.0f;
-                }
-#pragma unroll
-                for (int u = 0; u < U; ++u)
-                {
-                    const int row = base + 32 * u + lane;
-                    if (row > c && row < m) p = fma_rn(x[u], x[u], p);
-                }
-            }
-            const float sumsq = lane_fold(p);
+            for (int row = c + 1 + lane; row < m; row += 32) p = fma_rn(at(c, row), at(j, row), p);
+            const float part = lane_fold(p);
             if (lane == 0)
             {
-                float t = 0.0f, scale = 0.0f;
-                int apply = 0;
-                if (m - c > 1 && sumsq != 0.0f)
-                {
-                    const float alpha = col(c, c);
-                    const float norm = sqrt_rn(add_rn(mul_rn(alpha, alpha), sumsq));
-                    const float beta = alpha >= 0.0f ? -norm : norm;
-                    t = div_rn(sub_rn(beta, alpha), beta);
-                    scale = div_rn(1.0f, sub_rn(alpha, beta));
-                    at(c, c) = beta;
-                    apply = 1;
-                }
-                tau[c] = t;
-                s_tau = t;
-                s_scale = scale;
-                s_apply = apply;
+                if (warp == 0)
+                    s_sumsq = part;
+                else
+                    s_S[warp] = part;
             }
         }
         __syncthreads();
-        const bool apply = s_apply != 0;
-        const float t = s_tau;
-        if (apply)
+        if (tid == 0)
         {
-            const float scale = s_scale;
-            for (int row = c + 1 + tid; row < m; row += PANEL_THREADS)
+            float t = 0.0f, scale = 0.0f;
+            int apply = 0;
+            if (m - c > 1 && s_sumsq != 0.0f)
             {
-                const float v = mul_rn(col(c, row), scale);
-                at(c, row) = v;
-                if (!SMEM) col(c, row) = v;
+                const float alpha = at(c, c);
+                const float norm = sqrt_rn(add_rn(mul_rn(alpha, alpha), s_sumsq));
+                const float beta = alpha >= 0.0f ? -norm : norm;
+                t = div_rn(sub_rn(beta, alpha), beta);
+                scale = div_rn(1.0f, sub_rn(alpha, beta));
+                at(c, c) = beta;
+                apply = 1;
             }
+            tau[c] = t;
+            s_tau = t;
+            s_scale = scale;
+            s_apply = apply;
         }
         __syncthreads();
-        const int j = c + warp;
-        if (apply && warp >= 1 && j < k + kb)
+        prev_apply = s_apply != 0;
+        prev_scale = s_scale;
+        if (prev_apply && warp >= 1 && j < k + kb)
         {
-            float p = 0.0f;
-            for (int base = c & ~31; base < m; base += 32 * UX)
-            {
-                float x[UX];
-#pragma unroll
-                for (int u = 0; u < UX; ++u)
-                {
-                    const int row = base + 32 * u + lane;
-                    x[u] = row >= c && row < m ? at(j, row) : 0.0f;
-                }
-#pragma unroll
-                for (int u = 0; u < UX; ++u)
-                {
-                    const int row = base + 32 * u + lane;
-                    if (row >= c && row < m) p = fma_rn(row == c ? 1.0f : col(c, row), x[u], p);
-                }
-            }
-            const float w = mul_rn(t, lane_fold(p));
-            for (int base = c & ~31; base < m; base += 32 * UX)
-            {
-                float x[UX];
-#pragma unroll
-                for (int u = 0; u < UX; ++u)
-                {
-                    const int row = base + 32 * u + lane;
-                    x[u] = row >= c && row < m ? at(j, row) : 0.0f;
-                }
-#pragma unroll
-                for (int u = 0; u < UX; ++u)
-                {
-                    const int row = base + 32 * u + lane;
-                    if (row >= c && row < m)
-                    {
-                        const float y = fma_rn(-w, row == c ? 1.0f : col(c, row), x[u]);
-                        at(j, row) = y;
-                        if (!SMEM && j == c + 1) col(j, row) = y;
-                    }
-                }
-            }
+            const float w = mul_rn(s_tau, fma_rn(prev_scale, s_S[warp], at(j, c)));
+            __syncwarp();
+            if (lane == 0) at(j, c) = fma_rn(-w, 1.0f, at(j, c));
+            for (int row = c + 1 + lane; row < m; row += 32)
+                at(j, row) = fma_rn(-w, mul_rn(at(c, row), prev_scale), at(j, row));
         }
-        else if (!SMEM && !apply && warp == 1 && j < k + kb)
-            for (int row = c + 1 + lane; row < m; row += 32) col(j, row) = at(j, row);
         __syncthreads();
     }
-    if (SMEM)
-        for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) A[(int64_t)(k + idx / H) * lda + k + idx % H] = sp[idx];
+    if (prev_apply)
+        for (int row = k + kb + tid; row < m; row += PANEL_THREADS)
+            at(k + kb - 1, row) = mul_rn(at(k + kb - 1, row), prev_scale);
+    __syncthreads();
+    for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) A[(int64_t)(k + idx / H) * lda + k + idx % H] = sp[idx];
 }
 
 // Rows per block of a panel spread over a cluster (0: the panel fits one block, or is too
@@ -190,16 +134,18 @@ __host__ __device__ inline int panel_seg(int H, int kb, int budget)
 }
 
 // A tall panel over a cluster of ceil((m - k) / seg) blocks: block g holds rows
-// [k + g seg, k + (g + 1) seg) of the kb columns in shared memory.  Each reduction over rows is
-// a lane sum per block, folded; the blocks' totals are published in shared memory and every
-// block adds them in ascending block order through distributed shared memory, so all blocks
-// derive the same reflector and the same column weights.  Two cluster barriers per column.
+// [k + g seg, k + (g + 1) seg) of the kb columns in shared memory and runs the one-block
+// schedule on them.  The reductions are lane sums per block, folded and published (with the
+// rows of column c's diagonal entry, which block 0 holds) in shared memory double-buffered
+// by column parity; after one cluster barrier per column every block adds the published
+// totals in ascending block order through distributed shared memory, so all blocks derive
+// the same reflector and the same column weights.
 __global__ void __launch_bounds__(PANEL_THREADS) qr_cluster_panel_kernel(float *A, int lda, int m, int k, int kb,
                                                                          int seg, float *tau)
 {
     namespace cg = cooperative_groups;
     extern __shared__ float sp[];  // sp[(j - k) * seg + (row - r0)]
-    __shared__ float s_norm, s_alpha, s_dot[NB];
+    __shared__ float pub_sumsq[2], pub_S[2][NB], pub_row[2][NB];
     __shared__ float s_tau, s_scale;
     __shared__ int s_apply;
     cg::cluster_group cluster = cg::this_cluster();
@@ -211,33 +157,42 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_cluster_panel_kernel(float *
     for (int idx = tid; idx < rows * kb; idx += PANEL_THREADS)
         sp[(idx / rows) * seg + idx % rows] = A[(int64_t)(k + idx / rows) * lda + r0 + idx % rows];
     __syncthreads();
+    bool prev_apply = false;
+    float prev_scale = 0.0f;
     for (int c = k; c < k + kb; ++c)
     {
-        if (warp == 0)
+        const int par = c & 1, owner = (c - k) / seg;
+        if (prev_apply)
+            for (int row = max(r0, c) + tid; row < r1; row += PANEL_THREADS)
+                at(c - 1, row) = mul_rn(at(c - 1, row), prev_scale);
+        const int j = c + warp;
+        if (j < k + kb)
         {
             float p = 0.0f;
             for (int row = r0 + lane; row < r1; row += 32)
-                if (row > c) p = fma_rn(at(c, row), at(c, row), p);
+                if (row > c) p = fma_rn(at(c, row), at(j, row), p);
             const float part = lane_fold(p);
             if (lane == 0)
             {
-                s_norm = part;
-                if (c >= r0 && c < r1) s_alpha = at(c, c);
+                if (warp == 0)
+                    pub_sumsq[par] = part;
+                else
+                    pub_S[par][warp] = part;
+                if (g == owner) pub_row[par][warp] = at(j, c);
             }
         }
         cluster.sync();
         if (tid == 0)
         {
             float parts[8];
-            for (int q = 0; q < G; ++q) parts[q] = *cluster.map_shared_rank(&s_norm, q);
+            for (int q = 0; q < G; ++q) parts[q] = *cluster.map_shared_rank(&pub_sumsq[par], q);
             float sumsq = parts[0];
             for (int q = 1; q < G; ++q) sumsq = add_rn(sumsq, parts[q]);
-            const int owner = (c - k) / seg;
             float t = 0.0f, scale = 0.0f;
             int apply = 0;
             if (m - c > 1 && sumsq != 0.0f)
             {
-                const float alpha = *cluster.map_shared_rank(&s_alpha, owner);
+                const float alpha = *cluster.map_shared_rank(&pub_row[par][0], owner);
                 const float norm = sqrt_rn(add_rn(mul_rn(alpha, alpha), sumsq));
                 const float beta = alpha >= 0.0f ? -norm : norm;
                 t = div_rn(sub_rn(beta, alpha), beta);
@@ -251,38 +206,26 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_cluster_panel_kernel(float *
             s_apply = apply;
         }
         __syncthreads();
-        const bool apply = s_apply != 0;
-        const float t = s_tau;
-        if (apply)
-        {
-            const float scale = s_scale;
-            for (int row = max(r0, c + 1) + tid; row < r1; row += PANEL_THREADS) at(c, row) = mul_rn(at(c, row), scale);
-        }
-        __syncthreads();
-        const int j = c + warp;
-        const bool mine = apply && warp >= 1 && j < k + kb;
-        if (mine)
-        {
-            float p = 0.0f;
-            for (int row = r0 + lane; row < r1; row += 32)
-                if (row >= c) p = fma_rn(row == c ? 1.0f : at(c, row), at(j, row), p);
-            const float part = lane_fold(p);
-            if (lane == 0) s_dot[warp] = part;
-        }
-        cluster.sync();
-        if (mine)
+        prev_apply = s_apply != 0;
+        prev_scale = s_scale;
+        if (prev_apply && warp >= 1 && j < k + kb)
         {
             float parts[8];
-            for (int q = 0; q < G; ++q) parts[q] = *cluster.map_shared_rank(&s_dot[warp], q);
-            float dot = parts[0];
-            for (int q = 1; q < G; ++q) dot = add_rn(dot, parts[q]);
-            const float w = mul_rn(t, dot);
+            for (int q = 0; q < G; ++q) parts[q] = *cluster.map_shared_rank(&pub_S[par][warp], q);
+            float S = parts[0];
+            for (int q = 1; q < G; ++q) S = add_rn(S, parts[q]);
+            const float acj = *cluster.map_shared_rank(&pub_row[par][warp], owner);
+            const float w = mul_rn(s_tau, fma_rn(prev_scale, S, acj));
+            if (lane == 0 && g == owner) at(j, c) = fma_rn(-w, 1.0f, acj);
             for (int row = r0 + lane; row < r1; row += 32)
-                if (row >= c) at(j, row) = fma_rn(-w, row == c ? 1.0f : at(c, row), at(j, row));
+                if (row > c) at(j, row) = fma_rn(-w, mul_rn(at(c, row), prev_scale), at(j, row));
         }
         __syncthreads();
     }
-    cluster.sync();  // no block leaves while another may still read its partials
+    if (prev_apply)
+        for (int row = max(r0, k + kb) + tid; row < r1; row += PANEL_THREADS)
+            at(k + kb - 1, row) = mul_rn(at(k + kb - 1, row), prev_scale);
+    cluster.sync();  // no block leaves while another may still read what it published
     for (int idx = tid; idx < rows * kb; idx += PANEL_THREADS)
         A[(int64_t)(k + idx / rows) * lda + r0 + idx % rows] = sp[(idx / rows) * seg + idx % rows];
 }
@@ -727,12 +670,8 @@ cudaError_t launch_sgeqrf(float *A, int lda, int m, int n, float *tau, float *T,
                                     []
                                     {
                                         cudaError_t r = cudaFuncSetAttribute(
-                                            qr_panel_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            qr_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             PANEL_SMEM_FLOATS * (int)sizeof(float));
-                                        if (r == cudaSuccess)
-                                            r = cudaFuncSetAttribute(qr_panel_kernel<false>,
-                                                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                                     PANEL_SMEM_FLOATS * (int)sizeof(float));
                                         if (r == cudaSuccess)
                                             r = cudaFuncSetAttribute(qr_cluster_panel_kernel,
                                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -752,8 +691,7 @@ cudaError_t launch_sgeqrf(float *A, int lda, int m, int n, float *tau, float *T,
         const int seg = panel_seg(m - k, kb, PANEL_SMEM_FLOATS);
         if (panel_floats <= PANEL_SMEM_FLOATS)
         {
-            qr_panel_kernel<true><<<1, PANEL_THREADS, (size_t)panel_floats * sizeof(float), ps>>>(A, lda, m, k, kb,
-                                                                                                   tau);
+            qr_panel_kernel<<<1, PANEL_THREADS, (size_t)panel_floats * sizeof(float), ps>>>(A, lda, m, k, kb, tau);
             e = cudaGetLastError();
         }
         else if (seg > 0)
@@ -772,12 +710,8 @@ cudaError_t launch_sgeqrf(float *A, int lda, int m, int n, float *tau, float *T,
             cfg.numAttrs = 1;
             e = cudaLaunchKernelEx(&cfg, qr_cluster_panel_kernel, A, lda, m, k, kb, seg, tau);
         }
-        else  // two column buffers: 2 (m - k) floats, within PANEL_SMEM_FLOATS for m <= 25,600
-        {
-            qr_panel_kernel<false><<<1, PANEL_THREADS, (size_t)2 * (m - k) * sizeof(float), ps>>>(A, lda, m, k, kb,
-                                                                                                    tau);
-            e = cudaGetLastError();
-        }
+        else  // taller than eight blocks hold (m > 12,800): not reached, the entries cap m at 8,192
+            e = cudaErrorInvalidValue;
         if (e == cudaSuccess && k + kb < n)
         {
             float *Tk = T + (size_t)((k / NB) & 1) * QR_T_FLOATS;  // panel p's T, read by its wide update

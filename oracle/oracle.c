@@ -1419,56 +1419,52 @@ static void qr_seg_flush(float *p, float *total, int *started)
 /* Starts a new segment at `row` (rows counted from the panel start k). */
 #define QR_SEG_EDGE(row, first, k, seg) ((seg) && (row) > (first) && ((row) - (k)) % (seg) == 0)
 
-static void qr_larfg(int m, int k, int seg, float *a, int lda, int c, float *tau)
+/* Segmented lane sum over rows [first, m) of x[row] * y[row]. */
+static float qr_seg_dot(int m, int k, int seg, int first, const float *x, const float *y)
 {
-    *tau = 0.0f;
-    if (m - c <= 1) return;
-    float p[32] = {0}, sumsq = 0.0f;
+    float p[32] = {0}, total = 0.0f;
     int started = 0;
-    for (int row = c + 1; row < m; ++row)
+    for (int row = first; row < m; ++row)
     {
-        if (QR_SEG_EDGE(row, c + 1, k, seg)) qr_seg_flush(p, &sumsq, &started);
-        float x = RAT(a, lda, row, c);
-        p[row & 31] = fmaf(x, x, p[row & 31]);
+        if (QR_SEG_EDGE(row, first, k, seg)) qr_seg_flush(p, &total, &started);
+        p[row & 31] = fmaf(x[row], y[row], p[row & 31]);
     }
-    qr_seg_flush(p, &sumsq, &started);
-    if (sumsq == 0.0f) return;
-    float alpha = RAT(a, lda, c, c);
-    float norm = sqrtf(alpha * alpha + sumsq);
-    float beta = alpha >= 0.0f ? -norm : norm;
-    *tau = (beta - alpha) / beta;
-    float scale = 1.0f / (alpha - beta);
-    for (int row = c + 1; row < m; ++row) RAT(a, lda, row, c) = RAT(a, lda, row, c) * scale;
-    RAT(a, lda, c, c) = beta;
+    qr_seg_flush(p, &total, &started);
+    return total;
 }
 
-/* Factor panel columns [k, k+kb) of rows [k, m). */
+/* Factor panel columns [k, k+kb) of rows [k, m).  Per column c every reduction over the rows
+ * below c is taken at once from the column as it stands (x = A(c+1:m, c)): sumsq = sum x_i^2
+ * and, for each later panel column j, S_j = sum x_i A(i, j).  Then LAPACK's beta, tau and
+ * scale = 1 / (alpha - beta); v_i = x_i * scale; w_j = tau * fma(scale, S_j, A(c, j)), which is
+ * tau v^T a_j with v_c = 1; A(c, j) = fma(-w_j, 1, A(c, j)) and A(i, j) = fma(-w_j, v_i, A(i, j)). */
 static void qr_panel(int m, int k, int kb, float *a, int lda, float *tau)
 {
     const int seg = qr_panel_seg(m - k, kb, 50 * 1024);
+    float S[QR_NB];
     for (int c = k; c < k + kb; ++c)
     {
-        qr_larfg(m, k, seg, a, lda, c, &tau[c]);
-        const float t = tau[c];
-        if (t == 0.0f) continue;
+        float *x = a + (int64_t)c * lda;
+        tau[c] = 0.0f;
+        if (m - c <= 1) continue;
+        const float sumsq = qr_seg_dot(m, k, seg, c + 1, x, x);
+        for (int j = c + 1; j < k + kb; ++j) S[j - c] = qr_seg_dot(m, k, seg, c + 1, x, a + (int64_t)j * lda);
+        if (sumsq == 0.0f) continue;
+        const float alpha = x[c];
+        const float norm = sqrtf(alpha * alpha + sumsq);
+        const float beta = alpha >= 0.0f ? -norm : norm;
+        const float t = (beta - alpha) / beta;
+        const float scale = 1.0f / (alpha - beta);
+        tau[c] = t;
         for (int j = c + 1; j < k + kb; ++j)
         {
-            float p[32] = {0}, dot = 0.0f;
-            int started = 0;
-            for (int row = c; row < m; ++row)
-            {
-                if (QR_SEG_EDGE(row, c, k, seg)) qr_seg_flush(p, &dot, &started);
-                float v = row == c ? 1.0f : RAT(a, lda, row, c);
-                p[row & 31] = fmaf(v, RAT(a, lda, row, j), p[row & 31]);
-            }
-            qr_seg_flush(p, &dot, &started);
-            float w = t * dot;
-            for (int row = c; row < m; ++row)
-            {
-                float v = row == c ? 1.0f : RAT(a, lda, row, c);
-                RAT(a, lda, row, j) = fmaf(-w, v, RAT(a, lda, row, j));
-            }
+            float *y = a + (int64_t)j * lda;
+            const float w = t * fmaf(scale, S[j - c], y[c]);
+            y[c] = fmaf(-w, 1.0f, y[c]);
+            for (int row = c + 1; row < m; ++row) y[row] = fmaf(-w, x[row] * scale, y[row]);
         }
+        for (int row = c + 1; row < m; ++row) x[row] = x[row] * scale;
+        x[c] = beta;
     }
 }
 
@@ -1835,65 +1831,78 @@ static void cq_seg_flush(cfl *p, cfl *total, int *started)
     memset(p, 0, 32 * sizeof(cfl));
 }
 
-/* Panels are reduced in segments as in the real family (qr_panel_seg), with a budget of
- * 25,600 complex elements per block. */
-static void cq_larfg(int m, int k, int seg, cfl *a, int lda, int c, cfl *tau)
+/* Segmented lane sums over rows [first, m): of |x_i|^2, and of conj(x_i) y_i. */
+static float cq_seg_sumsq(int m, int k, int seg, int first, const cfl *x)
 {
-    tau->re = tau->im = 0.0f;
-    float p[32] = {0}, sumsq = 0.0f;
+    float p[32] = {0}, total = 0.0f;
     int started = 0;
-    for (int row = c + 1; row < m; ++row)
+    for (int row = first; row < m; ++row)
     {
-        if (QR_SEG_EDGE(row, c + 1, k, seg)) qr_seg_flush(p, &sumsq, &started);
-        cfl x = CAT(a, lda, row, c);
-        p[row & 31] = fmaf(x.im, x.im, fmaf(x.re, x.re, p[row & 31]));
+        if (QR_SEG_EDGE(row, first, k, seg)) qr_seg_flush(p, &total, &started);
+        p[row & 31] = fmaf(x[row].im, x[row].im, fmaf(x[row].re, x[row].re, p[row & 31]));
     }
-    qr_seg_flush(p, &sumsq, &started);
-    const cfl al = CAT(a, lda, c, c);
-    if (sumsq == 0.0f && al.im == 0.0f) return;
-    const float norm = sqrtf(al.re * al.re + al.im * al.im + sumsq);
-    const float beta = copysignf(norm, al.re) * -1.0f;
-    tau->re = (beta - al.re) / beta;
-    tau->im = -(al.im / beta);
-    const float dr = al.re - beta, di = al.im;
-    const float den = dr * dr + di * di;
-    for (int row = c + 1; row < m; ++row)
-    {
-        cfl x = CAT(a, lda, row, c);
-        cfl v = {(x.re * dr + x.im * di) / den, (x.im * dr - x.re * di) / den};
-        CAT(a, lda, row, c) = v;
-    }
-    cfl b = {beta, 0.0f};
-    CAT(a, lda, c, c) = b;
+    qr_seg_flush(p, &total, &started);
+    return total;
 }
 
+static cfl cq_seg_conjdot(int m, int k, int seg, int first, const cfl *x, const cfl *y)
+{
+    cfl p[32], total = {0.0f, 0.0f};
+    int started = 0;
+    memset(p, 0, sizeof p);
+    for (int row = first; row < m; ++row)
+    {
+        if (QR_SEG_EDGE(row, first, k, seg)) cq_seg_flush(p, &total, &started);
+        p[row & 31] = q_conjdot(p[row & 31], x[row], y[row]);
+    }
+    cq_seg_flush(p, &total, &started);
+    return total;
+}
+
+/* Panels are reduced in segments as in the real family (qr_panel_seg, a budget of 25,600
+ * complex elements per block) and, as there, every reduction of column c's step is taken at
+ * once from the column as it stands (x = A(c+1:m, c)): sumsq = sum |x_i|^2 and, per later panel
+ * column j, S_j = sum conj(x_i) A(i, j).  With d = alpha - beta = (dr, di), den = |d|^2 and
+ * g = (dr / den, di / den): v_i = x_i / d (two real divisions per part), v^H a_j =
+ * A(c, j) + g S_j (one complex FMA sequence), w_j = conj(tau) v^H a_j. */
 static void cq_panel(int m, int k, int kb, cfl *a, int lda, cfl *tau)
 {
     const int seg = qr_panel_seg(m - k, kb, 25 * 1024);
+    cfl S[QR_NB];
+    const cfl one = {1.0f, 0.0f};
     for (int c = k; c < k + kb; ++c)
     {
-        cq_larfg(m, k, seg, a, lda, c, &tau[c]);
-        const cfl t = tau[c];
-        if (t.re == 0.0f && t.im == 0.0f) continue;
+        cfl *x = a + (int64_t)c * lda;
+        tau[c].re = tau[c].im = 0.0f;
+        const float sumsq = cq_seg_sumsq(m, k, seg, c + 1, x);
+        for (int j = c + 1; j < k + kb; ++j) S[j - c] = cq_seg_conjdot(m, k, seg, c + 1, x, a + (int64_t)j * lda);
+        const cfl al = x[c];
+        if (sumsq == 0.0f && al.im == 0.0f) continue;
+        const float norm = sqrtf(al.re * al.re + al.im * al.im + sumsq);
+        const float beta = copysignf(norm, al.re) * -1.0f;
+        const cfl t = {(beta - al.re) / beta, -(al.im / beta)};
+        const float dr = al.re - beta, di = al.im;
+        const float den = dr * dr + di * di;
+        const cfl g = {dr / den, di / den};
+        tau[c] = t;
         for (int j = c + 1; j < k + kb; ++j)
         {
-            cfl p[32], dot = {0.0f, 0.0f};
-            int started = 0;
-            memset(p, 0, sizeof p);
-            for (int row = c; row < m; ++row)
+            cfl *y = a + (int64_t)j * lda;
+            const cfl w = q_mulc(t, q_fma(g, S[j - c], y[c]));
+            y[c] = c_submul(y[c], one, w);
+            for (int row = c + 1; row < m; ++row)
             {
-                if (QR_SEG_EDGE(row, c, k, seg)) cq_seg_flush(p, &dot, &started);
-                cfl v = row == c ? (cfl){1.0f, 0.0f} : CAT(a, lda, row, c);
-                p[row & 31] = q_conjdot(p[row & 31], v, CAT(a, lda, row, j));
-            }
-            cq_seg_flush(p, &dot, &started);
-            const cfl w = q_mulc(t, dot);
-            for (int row = c; row < m; ++row)
-            {
-                cfl v = row == c ? (cfl){1.0f, 0.0f} : CAT(a, lda, row, c);
-                CAT(a, lda, row, j) = c_submul(CAT(a, lda, row, j), v, w);
+                const cfl v = {(x[row].re * dr + x[row].im * di) / den, (x[row].im * dr - x[row].re * di) / den};
+                y[row] = c_submul(y[row], v, w);
             }
         }
+        for (int row = c + 1; row < m; ++row)
+        {
+            const cfl v = {(x[row].re * dr + x[row].im * di) / den, (x[row].im * dr - x[row].re * di) / den};
+            x[row] = v;
+        }
+        x[c].re = beta;
+        x[c].im = 0.0f;
     }
 }
 
