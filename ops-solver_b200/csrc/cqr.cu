@@ -24,7 +24,7 @@ namespace
 {
 constexpr int NB = 32;
 constexpr int PANEL_THREADS = 1024;
-constexpr int APPLY_WARPS = 16;
+constexpr int APPLY_WARPS = 8;
 constexpr int PANEL_SMEM_ELEMS = 25 * 1024;  // complex elements of a panel kept in shared memory
 
 // acc += conj(v) a
@@ -111,6 +111,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_panel_kernel(float2 *A, int 
         if (warp == 0)
         {
             float p = 0.0f;
+#pragma unroll 4
             for (int row = c + 1 + lane; row < m; row += 32)
             {
                 const float2 x = at(c, row);
@@ -122,6 +123,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_panel_kernel(float2 *A, int 
         else if (j < k + kb)
         {
             float2 p = make_float2(0.0f, 0.0f);
+#pragma unroll 4
             for (int row = c + 1 + lane; row < m; row += 32) p = cq_conjdot(p, at(c, row), at(j, row));
             const float2 part = fold2(p);
             if (lane == 0) s_S[warp] = part;
@@ -163,6 +165,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_panel_kernel(float2 *A, int 
             const float2 w = cq_mulc(s_tau, cq_fma(s_g, s_S[warp], at(j, c)));
             __syncwarp();
             if (lane == 0) at(j, c) = clu::csubmul(at(j, c), make_float2(1.0f, 0.0f), w);
+#pragma unroll 4
             for (int row = c + 1 + lane; row < m; row += 32)
                 at(j, row) = clu::csubmul(at(j, row), cq_reflect(at(c, row), pdr, pdi, pden), w);
         }
@@ -223,6 +226,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_cluster_panel_kernel(float2 
         if (warp == 0)
         {
             float p = 0.0f;
+#pragma unroll 4
             for (int row = r0 + lane; row < r1; row += 32)
                 if (row > c)
                 {
@@ -235,6 +239,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_cluster_panel_kernel(float2 
         else if (j < k + kb)
         {
             float2 p = make_float2(0.0f, 0.0f);
+#pragma unroll 4
             for (int row = r0 + lane; row < r1; row += 32)
                 if (row > c) p = cq_conjdot(p, at(c, row), at(j, row));
             const float2 part = fold2(p);
@@ -286,6 +291,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_cluster_panel_kernel(float2 
             const float2 acj = *cluster.map_shared_rank(&pub_row[par][warp], owner);
             const float2 w = cq_mulc(s_tau, cq_fma(s_g, S, acj));
             if (lane == 0 && g == owner) at(j, c) = clu::csubmul(acj, make_float2(1.0f, 0.0f), w);
+#pragma unroll 4
             for (int row = r0 + lane; row < r1; row += 32)
                 if (row > c) at(j, row) = clu::csubmul(at(j, row), cq_reflect(at(c, row), pdr, pdi, pden), w);
         }

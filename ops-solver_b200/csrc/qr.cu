@@ -73,6 +73,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_panel_kernel(float *A, int l
         if (m - c > 1 && j < k + kb)
         {
             float p = 0.0f;
+#pragma unroll 4
             for (int row = c + 1 + lane; row < m; row += 32) p = fma_rn(at(c, row), at(j, row), p);
             const float part = lane_fold(p);
             if (lane == 0)
@@ -111,6 +112,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_panel_kernel(float *A, int l
             const float w = mul_rn(s_tau, fma_rn(prev_scale, s_S[warp], at(j, c)));
             __syncwarp();
             if (lane == 0) at(j, c) = fma_rn(-w, 1.0f, at(j, c));
+#pragma unroll 4
             for (int row = c + 1 + lane; row < m; row += 32)
                 at(j, row) = fma_rn(-w, mul_rn(at(c, row), prev_scale), at(j, row));
         }
@@ -169,6 +171,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_cluster_panel_kernel(float *
         if (j < k + kb)
         {
             float p = 0.0f;
+#pragma unroll 4
             for (int row = r0 + lane; row < r1; row += 32)
                 if (row > c) p = fma_rn(at(c, row), at(j, row), p);
             const float part = lane_fold(p);
@@ -217,6 +220,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_cluster_panel_kernel(float *
             const float acj = *cluster.map_shared_rank(&pub_row[par][warp], owner);
             const float w = mul_rn(s_tau, fma_rn(prev_scale, S, acj));
             if (lane == 0 && g == owner) at(j, c) = fma_rn(-w, 1.0f, acj);
+#pragma unroll 4
             for (int row = r0 + lane; row < r1; row += 32)
                 if (row > c) at(j, row) = fma_rn(-w, mul_rn(at(c, row), prev_scale), at(j, row));
         }
