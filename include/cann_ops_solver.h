@@ -174,7 +174,7 @@ extern "C"
 
     /* ---- real QR family; reference include/cann_ops_solver.h:566-861 --------------------- */
 
-    /* Lwork (floats) for Sgeqrf: 0 for an empty problem, else one 32 x 32 block factor;
+    /* Lwork (floats) for Sgeqrf: 0 for an empty problem, else two 32 x 32 block factors;
      * m <= 8192 (NOT_SUPPORTED above); replaces cann_ops_solver.h:566 (sgeqrf_host.cpp:173). */
     aclsolverStatus_t aclsolverSgeqrf_bufferSize(aclsolverHandle_t handle, int m, int n, float *A, int lda, int *Lwork);
     /* Householder QR in place (LAPACK sign convention): R on and above the diagonal, the
@@ -220,7 +220,7 @@ extern "C"
                                       aclsolverDataType_t computeType, void *bufferOnDevice,
                                       size_t workspaceInBytesOnDevice, void *bufferOnHost,
                                       size_t workspaceInBytesOnHost);
-    /* Bytes for SSgels: tau, Q^T B and one block factor; m >= n, m, n <= 4096, nrhs <= 128;
+    /* Bytes for SSgels: tau, Q^T B and two block factors; m >= n, m, n <= 4096, nrhs <= 128;
      * replaces cann_ops_solver.h:815 (sgels_host.cpp:149). */
     aclsolverStatus_t aclsolverSSgels_bufferSize(aclsolverHandle_t handle, int m, int n, int nrhs, float *dA, int ldda,
                                                  float *dB, int lddb, float *dX, int lddx, void *dwork,
@@ -238,8 +238,8 @@ extern "C"
      * first (one stream synchronisation and a four-byte read-back, as the reference does):
      * INVALID_VALUE with info -i for the first such argument. */
 
-    /* Lwork (complex elements) for Cgeqrf: 0 for an empty problem, else one 32 x 32 block
-     * factor; replaces cann_ops_solver.h:259 (cgeqrf_host.cpp:45). */
+    /* Lwork (complex elements) for Cgeqrf: 0 for an empty problem, else two 32 x 32 block
+     * factors; replaces cann_ops_solver.h:259 (cgeqrf_host.cpp:45). */
     aclsolverStatus_t aclsolverCgeqrf_bufferSize(aclsolverHandle_t handle, int m, int n, aclsolverFloatComplex *A,
                                                  int lda, int *Lwork);
     /* A = Q R in place, TAU[min(m, n)]; devInfo 0 or -i (1 m, 2 n, 3 A, 4 lda, 5 TAU,
@@ -270,7 +270,7 @@ extern "C"
                                       int m, int n, int k, const aclsolverFloatComplex *A, int lda,
                                       const aclsolverFloatComplex *tau, aclsolverFloatComplex *C, int ldc,
                                       aclsolverFloatComplex *work, int lwork, int *devInfo);
-    /* Bytes for CCgels: tau, Q^H B and one block factor; m >= n, m, n <= 4096, nrhs <= 128;
+    /* Bytes for CCgels: tau, Q^H B and two block factors; m >= n, m, n <= 4096, nrhs <= 128;
      * replaces cann_ops_solver.h:376 (ccgels_host.cpp:68). */
     aclsolverStatus_t aclsolverCCgels_bufferSize(aclsolverHandle_t handle, int m, int n, int nrhs,
                                                  aclsolverFloatComplex *dA, int ldda, aclsolverFloatComplex *dB,
