@@ -701,7 +701,14 @@ cudaError_t launch_cgeqrf(float2 *A, int lda, int m, int n, float2 *tau, float2 
     const int lim = std::min(m, n);
     // Look-ahead (panels on a high-priority stream beside the wide update), as the real family.
     Lookahead la;
-    const bool ahead = e == cudaSuccess && m >= 512 && n > 3 * NB;
+    // No look-ahead while the stream is being captured: it would create a stream and events.
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &capture) != cudaSuccess)
+    {
+        cudaGetLastError();
+        capture = cudaStreamCaptureStatusActive;
+    }
+    const bool ahead = e == cudaSuccess && capture == cudaStreamCaptureStatusNone && m >= 512 && n > 3 * NB;
     if (ahead) e = la.open(stream);
     cudaStream_t ps = ahead ? la.panel : stream;
     for (int k = 0; k < lim && e == cudaSuccess; k += NB)

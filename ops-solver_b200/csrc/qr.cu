@@ -56,19 +56,21 @@ constexpr int PANEL_SMEM_FLOATS = 50 * 1024;
 __global__ void __launch_bounds__(PANEL_THREADS) qr_panel_kernel(float *A, int lda, int m, int k, int kb, float *tau)
 {
     extern __shared__ float sp[];
-    __shared__ float s_sumsq, s_S[NB], s_tau, s_scale;
-    __shared__ int s_apply;
+    __shared__ float s_sumsq, s_alpha, s_S[NB];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int H = m - k;
     auto at = [&](int j, int row) -> float & { return sp[(j - k) * H + (row - k)]; };
     for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) sp[idx] = A[(int64_t)(k + idx / H) * lda + k + idx % H];
     __syncthreads();
     bool prev_apply = false;
-    float prev_scale = 0.0f;
+    float prev_scale = 0.0f, prev_beta = 0.0f;
     for (int c = k; c < k + kb; ++c)
     {
-        if (prev_apply)  // column c - 1 becomes its reflector
+        if (prev_apply)  // column c - 1 becomes its reflector, beta its diagonal entry
+        {
+            if (tid == 0) at(c - 1, c - 1) = prev_beta;
             for (int row = c + tid; row < m; row += PANEL_THREADS) at(c - 1, row) = mul_rn(at(c - 1, row), prev_scale);
+        }
         const int j = c + warp;
         if (m - c > 1 && j < k + kb)
         {
@@ -79,48 +81,47 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_panel_kernel(float *A, int l
             if (lane == 0)
             {
                 if (warp == 0)
+                {
                     s_sumsq = part;
+                    s_alpha = at(c, c);
+                }
                 else
                     s_S[warp] = part;
             }
         }
         __syncthreads();
-        if (tid == 0)
+        // every thread forms the reflector's scalars (the same operations on the same values)
+        float t = 0.0f, scale = 0.0f, beta = 0.0f;
+        const bool apply = m - c > 1 && s_sumsq != 0.0f;
+        if (apply)
         {
-            float t = 0.0f, scale = 0.0f;
-            int apply = 0;
-            if (m - c > 1 && s_sumsq != 0.0f)
-            {
-                const float alpha = at(c, c);
-                const float norm = sqrt_rn(add_rn(mul_rn(alpha, alpha), s_sumsq));
-                const float beta = alpha >= 0.0f ? -norm : norm;
-                t = div_rn(sub_rn(beta, alpha), beta);
-                scale = div_rn(1.0f, sub_rn(alpha, beta));
-                at(c, c) = beta;
-                apply = 1;
-            }
-            tau[c] = t;
-            s_tau = t;
-            s_scale = scale;
-            s_apply = apply;
+            const float alpha = s_alpha;
+            const float norm = sqrt_rn(add_rn(mul_rn(alpha, alpha), s_sumsq));
+            beta = alpha >= 0.0f ? -norm : norm;
+            t = div_rn(sub_rn(beta, alpha), beta);
+            scale = div_rn(1.0f, sub_rn(alpha, beta));
         }
-        __syncthreads();
-        prev_apply = s_apply != 0;
-        prev_scale = s_scale;
-        if (prev_apply && warp >= 1 && j < k + kb)
+        if (tid == 0) tau[c] = t;
+        if (apply && warp >= 1 && j < k + kb)
         {
-            const float w = mul_rn(s_tau, fma_rn(prev_scale, s_S[warp], at(j, c)));
+            const float w = mul_rn(t, fma_rn(scale, s_S[warp], at(j, c)));
             __syncwarp();
             if (lane == 0) at(j, c) = fma_rn(-w, 1.0f, at(j, c));
 #pragma unroll 4
             for (int row = c + 1 + lane; row < m; row += 32)
-                at(j, row) = fma_rn(-w, mul_rn(at(c, row), prev_scale), at(j, row));
+                at(j, row) = fma_rn(-w, mul_rn(at(c, row), scale), at(j, row));
         }
+        prev_apply = apply;
+        prev_scale = scale;
+        prev_beta = beta;
         __syncthreads();
     }
     if (prev_apply)
+    {
+        if (tid == 0) at(k + kb - 1, k + kb - 1) = prev_beta;
         for (int row = k + kb + tid; row < m; row += PANEL_THREADS)
             at(k + kb - 1, row) = mul_rn(at(k + kb - 1, row), prev_scale);
+    }
     __syncthreads();
     for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) A[(int64_t)(k + idx / H) * lda + k + idx % H] = sp[idx];
 }
@@ -148,32 +149,40 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_cluster_panel_kernel(float *
     namespace cg = cooperative_groups;
     extern __shared__ float sp[];  // sp[(j - k) * seg + (row - r0)]
     __shared__ float pub_sumsq[2], pub_S[2][NB], pub_row[2][NB];
-    __shared__ float s_tau, s_scale;
-    __shared__ int s_apply;
     cg::cluster_group cluster = cg::this_cluster();
     const int g = (int)cluster.block_rank(), G = (int)cluster.num_blocks();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int r0 = k + g * seg, r1 = min(m, r0 + seg);
     const int rows = max(0, r1 - r0);
     auto at = [&](int j, int row) -> float & { return sp[(j - k) * seg + (row - r0)]; };
+    // the blocks' totals in ascending block order: lane q fetches block q's, every lane adds
+    auto total = [&](float *mine) -> float
+    {
+        const float part = lane < G ? *cluster.map_shared_rank(mine, lane) : 0.0f;
+        float sum = __shfl_sync(0xffffffffu, part, 0);
+        for (int q = 1; q < G; ++q) sum = add_rn(sum, __shfl_sync(0xffffffffu, part, q));
+        return sum;
+    };
     for (int idx = tid; idx < rows * kb; idx += PANEL_THREADS)
         sp[(idx / rows) * seg + idx % rows] = A[(int64_t)(k + idx / rows) * lda + r0 + idx % rows];
     __syncthreads();
     bool prev_apply = false;
-    float prev_scale = 0.0f;
+    float prev_scale = 0.0f, prev_beta = 0.0f;
     for (int c = k; c < k + kb; ++c)
     {
         const int par = c & 1, owner = (c - k) / seg;
-        if (prev_apply)
+        if (prev_apply)  // column c - 1 becomes its reflector, beta its diagonal entry
+        {
+            if (tid == 0 && c - 1 >= r0 && c - 1 < r1) at(c - 1, c - 1) = prev_beta;
             for (int row = max(r0, c) + tid; row < r1; row += PANEL_THREADS)
                 at(c - 1, row) = mul_rn(at(c - 1, row), prev_scale);
+        }
         const int j = c + warp;
         if (j < k + kb)
         {
             float p = 0.0f;
 #pragma unroll 4
-            for (int row = r0 + lane; row < r1; row += 32)
-                if (row > c) p = fma_rn(at(c, row), at(j, row), p);
+            for (int row = max(r0, c + 1) + lane; row < r1; row += 32) p = fma_rn(at(c, row), at(j, row), p);
             const float part = lane_fold(p);
             if (lane == 0)
             {
@@ -185,50 +194,40 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_cluster_panel_kernel(float *
             }
         }
         cluster.sync();
-        if (tid == 0)
+        // every warp forms the reflector's scalars (the same operations on the same values)
+        const float sumsq = total(&pub_sumsq[par]);
+        const bool apply = m - c > 1 && sumsq != 0.0f;
+        float t = 0.0f, scale = 0.0f, beta = 0.0f;
+        if (apply)
         {
-            float parts[8];
-            for (int q = 0; q < G; ++q) parts[q] = *cluster.map_shared_rank(&pub_sumsq[par], q);
-            float sumsq = parts[0];
-            for (int q = 1; q < G; ++q) sumsq = add_rn(sumsq, parts[q]);
-            float t = 0.0f, scale = 0.0f;
-            int apply = 0;
-            if (m - c > 1 && sumsq != 0.0f)
-            {
-                const float alpha = *cluster.map_shared_rank(&pub_row[par][0], owner);
-                const float norm = sqrt_rn(add_rn(mul_rn(alpha, alpha), sumsq));
-                const float beta = alpha >= 0.0f ? -norm : norm;
-                t = div_rn(sub_rn(beta, alpha), beta);
-                scale = div_rn(1.0f, sub_rn(alpha, beta));
-                if (owner == g) at(c, c) = beta;
-                apply = 1;
-            }
-            if (g == 0) tau[c] = t;
-            s_tau = t;
-            s_scale = scale;
-            s_apply = apply;
+            const float alpha = *cluster.map_shared_rank(&pub_row[par][0], owner);
+            const float norm = sqrt_rn(add_rn(mul_rn(alpha, alpha), sumsq));
+            beta = alpha >= 0.0f ? -norm : norm;
+            t = div_rn(sub_rn(beta, alpha), beta);
+            scale = div_rn(1.0f, sub_rn(alpha, beta));
         }
-        __syncthreads();
-        prev_apply = s_apply != 0;
-        prev_scale = s_scale;
-        if (prev_apply && warp >= 1 && j < k + kb)
+        if (tid == 0 && g == 0) tau[c] = t;
+        if (apply && warp >= 1 && j < k + kb)
         {
-            float parts[8];
-            for (int q = 0; q < G; ++q) parts[q] = *cluster.map_shared_rank(&pub_S[par][warp], q);
-            float S = parts[0];
-            for (int q = 1; q < G; ++q) S = add_rn(S, parts[q]);
+            const float S = total(&pub_S[par][warp]);
             const float acj = *cluster.map_shared_rank(&pub_row[par][warp], owner);
-            const float w = mul_rn(s_tau, fma_rn(prev_scale, S, acj));
+            const float w = mul_rn(t, fma_rn(scale, S, acj));
             if (lane == 0 && g == owner) at(j, c) = fma_rn(-w, 1.0f, acj);
 #pragma unroll 4
-            for (int row = r0 + lane; row < r1; row += 32)
-                if (row > c) at(j, row) = fma_rn(-w, mul_rn(at(c, row), prev_scale), at(j, row));
+            for (int row = max(r0, c + 1) + lane; row < r1; row += 32)
+                at(j, row) = fma_rn(-w, mul_rn(at(c, row), scale), at(j, row));
         }
+        prev_apply = apply;
+        prev_scale = scale;
+        prev_beta = beta;
         __syncthreads();
     }
     if (prev_apply)
+    {
+        if (tid == 0 && k + kb - 1 >= r0 && k + kb - 1 < r1) at(k + kb - 1, k + kb - 1) = prev_beta;
         for (int row = max(r0, k + kb) + tid; row < r1; row += PANEL_THREADS)
             at(k + kb - 1, row) = mul_rn(at(k + kb - 1, row), prev_scale);
+    }
     cluster.sync();  // no block leaves while another may still read what it published
     for (int idx = tid; idx < rows * kb; idx += PANEL_THREADS)
         A[(int64_t)(k + idx / rows) * lda + r0 + idx % rows] = sp[(idx / rows) * seg + idx % rows];
@@ -685,7 +684,14 @@ cudaError_t launch_sgeqrf(float *A, int lda, int m, int n, float *tau, float *T,
     // Look-ahead (panels on a high-priority stream beside the wide update) once the trailing
     // matrix is wide and tall enough to keep the rest of the GPU busy.
     Lookahead la;
-    const bool ahead = e == cudaSuccess && m >= 512 && n > 3 * NB;
+    // No look-ahead while the stream is being captured: it would create a stream and events.
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &capture) != cudaSuccess)
+    {
+        cudaGetLastError();
+        capture = cudaStreamCaptureStatusActive;
+    }
+    const bool ahead = e == cudaSuccess && capture == cudaStreamCaptureStatusNone && m >= 512 && n > 3 * NB;
     if (ahead) e = la.open(stream);
     cudaStream_t ps = ahead ? la.panel : stream;
     for (int k = 0; k < lim && e == cudaSuccess; k += NB)

@@ -213,3 +213,39 @@ def test_xlarft_argument_checks(handle):
     assert q(None, 0, 0, 10, 4, 1, None, 10, 0, None, 0, None, 4, 0) == 7
     assert q(None, 0, 0, 5000, 4, 0, None, 5000, 0, None, 0, None, 4, 0) == 7
     assert q(None, 0, 0, 300, 257, 0, None, 300, 0, None, 0, None, 257, 0) == 7
+
+
+def test_sgeqrf_captured_in_a_cuda_graph(handle):
+    """A call captured on a stream (where the look-ahead's private stream stays off) replays
+    to the same bits as the oracle, twice."""
+    lib = aclsolver.library()
+    m = n = 1024
+    a = rand(m, n, 77)
+    stream = torch.cuda.Stream()
+    with aclsolver.Handle(stream=stream) as h:
+        dm = DeviceMatrices(a, m)
+        tau = torch.zeros(n, dtype=torch.float32, device="cuda")
+        lw = C.c_int(-1)
+        assert lib.aclsolverSgeqrf_bufferSize(h.value, m, n, dm.ptr, m, C.byref(lw)) == aclsolver.SUCCESS
+        w = work(lw.value)
+        info = info_buffer(1)
+        original = dm.tensor.clone()
+
+        def call():
+            return lib.aclsolverSgeqrf(h.value, m, n, dm.ptr, m, tau.data_ptr(), w.data_ptr(), lw.value,
+                                       info.data_ptr())
+
+        assert call() == aclsolver.SUCCESS  # warm-up outside the capture (kernel attributes)
+        stream.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream, capture_error_mode="relaxed"):
+            assert call() == aclsolver.SUCCESS
+        want, wtau = oracle.sgeqrf(a)
+        for _ in range(2):
+            dm.tensor.copy_(original)
+            torch.cuda.synchronize()
+            graph.replay()
+            torch.cuda.synchronize()
+            assert int(info.cpu()[0]) == 0
+            assert same_bits(dm.read()[0], want) and same_bits(tau.cpu().numpy(), wtau)
+        del graph
