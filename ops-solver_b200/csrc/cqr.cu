@@ -84,13 +84,38 @@ __device__ __forceinline__ float2 cq_reflect(float2 x, float dr, float di, float
                        div_rn(sub_rn(mul_rn(x.y, dr), mul_rn(x.x, di)), den));
 }
 
+// Scalars of column c's reflector from sumsq and alpha (every thread forms them identically).
+struct CqScalars
+{
+    bool apply;
+    float beta, dr, di, den;
+    float2 t, g;
+};
+
+__device__ __forceinline__ CqScalars cq_scalars(float sumsq, float2 al)
+{
+    CqScalars r{};
+    r.apply = !(sumsq == 0.0f && al.y == 0.0f);
+    r.t = make_float2(0.0f, 0.0f);
+    if (r.apply)
+    {
+        const float norm = sqrt_rn(add_rn(add_rn(mul_rn(al.x, al.x), mul_rn(al.y, al.y)), sumsq));
+        r.beta = -copysignf(norm, al.x);
+        r.t = make_float2(div_rn(sub_rn(r.beta, al.x), r.beta), -div_rn(al.y, r.beta));
+        r.dr = sub_rn(al.x, r.beta);
+        r.di = al.y;
+        r.den = add_rn(mul_rn(r.dr, r.dr), mul_rn(r.di, r.di));
+        r.g = make_float2(div_rn(r.dr, r.den), div_rn(r.di, r.den));
+    }
+    return r;
+}
+
 template <bool SMEM>
 __global__ void __launch_bounds__(PANEL_THREADS) cq_panel_kernel(float2 *A, int lda, int m, int k, int kb, float2 *tau)
 {
     extern __shared__ float2 sp[];
-    __shared__ float2 s_S[NB], s_tau, s_g;
-    __shared__ float s_sumsq, s_dr, s_di, s_den;
-    __shared__ int s_apply;
+    __shared__ float2 s_S[NB], s_alpha;
+    __shared__ float s_sumsq;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int H = m - k;
     auto at = [&](int j, int row) -> float2 & {
@@ -101,12 +126,16 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_panel_kernel(float2 *A, int 
         for (int idx = tid; idx < H * kb; idx += PANEL_THREADS) sp[idx] = A[(int64_t)(k + idx / H) * lda + k + idx % H];
         __syncthreads();
     }
-    bool prev_apply = false;
-    float pdr = 0.0f, pdi = 0.0f, pden = 1.0f;
+    CqScalars prev{};
+    prev.apply = false;
     for (int c = k; c < k + kb; ++c)
     {
-        if (prev_apply)  // column c - 1 becomes its reflector
-            for (int row = c + tid; row < m; row += PANEL_THREADS) at(c - 1, row) = cq_reflect(at(c - 1, row), pdr, pdi, pden);
+        if (prev.apply)  // column c - 1 becomes its reflector, beta its diagonal entry
+        {
+            if (tid == 0) at(c - 1, c - 1) = make_float2(prev.beta, 0.0f);
+            for (int row = c + tid; row < m; row += PANEL_THREADS)
+                at(c - 1, row) = cq_reflect(at(c - 1, row), prev.dr, prev.di, prev.den);
+        }
         const int j = c + warp;
         if (warp == 0)
         {
@@ -118,7 +147,11 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_panel_kernel(float2 *A, int 
                 p = fma_rn(x.y, x.y, fma_rn(x.x, x.x, p));
             }
             const float part = fold1(p);
-            if (lane == 0) s_sumsq = part;
+            if (lane == 0)
+            {
+                s_sumsq = part;
+                s_alpha = at(c, c);
+            }
         }
         else if (j < k + kb)
         {
@@ -129,51 +162,26 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_panel_kernel(float2 *A, int 
             if (lane == 0) s_S[warp] = part;
         }
         __syncthreads();
-        if (tid == 0)
+        const CqScalars r = cq_scalars(s_sumsq, s_alpha);
+        if (tid == 0) tau[c] = r.t;
+        if (r.apply && warp >= 1 && j < k + kb)
         {
-            const float2 al = at(c, c);
-            float2 t = make_float2(0.0f, 0.0f);
-            int apply = 0;
-            if (!(s_sumsq == 0.0f && al.y == 0.0f))
-            {
-                const float norm = sqrt_rn(add_rn(add_rn(mul_rn(al.x, al.x), mul_rn(al.y, al.y)), s_sumsq));
-                const float beta = -copysignf(norm, al.x);
-                t = make_float2(div_rn(sub_rn(beta, al.x), beta), -div_rn(al.y, beta));
-                const float dr = sub_rn(al.x, beta), di = al.y;
-                const float den = add_rn(mul_rn(dr, dr), mul_rn(di, di));
-                s_dr = dr;
-                s_di = di;
-                s_den = den;
-                s_g = make_float2(div_rn(dr, den), div_rn(di, den));
-                at(c, c) = make_float2(beta, 0.0f);
-                apply = 1;
-            }
-            tau[c] = t;
-            s_tau = t;
-            s_apply = apply;
-        }
-        __syncthreads();
-        prev_apply = s_apply != 0;
-        if (prev_apply)
-        {
-            pdr = s_dr;
-            pdi = s_di;
-            pden = s_den;
-        }
-        if (prev_apply && warp >= 1 && j < k + kb)
-        {
-            const float2 w = cq_mulc(s_tau, cq_fma(s_g, s_S[warp], at(j, c)));
+            const float2 w = cq_mulc(r.t, cq_fma(r.g, s_S[warp], at(j, c)));
             __syncwarp();
             if (lane == 0) at(j, c) = clu::csubmul(at(j, c), make_float2(1.0f, 0.0f), w);
 #pragma unroll 4
             for (int row = c + 1 + lane; row < m; row += 32)
-                at(j, row) = clu::csubmul(at(j, row), cq_reflect(at(c, row), pdr, pdi, pden), w);
+                at(j, row) = clu::csubmul(at(j, row), cq_reflect(at(c, row), r.dr, r.di, r.den), w);
         }
+        prev = r;
         __syncthreads();
     }
-    if (prev_apply)
+    if (prev.apply)
+    {
+        if (tid == 0) at(k + kb - 1, k + kb - 1) = make_float2(prev.beta, 0.0f);
         for (int row = k + kb + tid; row < m; row += PANEL_THREADS)
-            at(k + kb - 1, row) = cq_reflect(at(k + kb - 1, row), pdr, pdi, pden);
+            at(k + kb - 1, row) = cq_reflect(at(k + kb - 1, row), prev.dr, prev.di, prev.den);
+    }
     if (SMEM)
     {
         __syncthreads();
@@ -202,37 +210,53 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_cluster_panel_kernel(float2 
     extern __shared__ float2 sp[];  // sp[(j - k) * seg + (row - r0)]
     __shared__ float pub_sumsq[2];
     __shared__ float2 pub_S[2][NB], pub_row[2][NB];
-    __shared__ float2 s_tau, s_g;
-    __shared__ float s_dr, s_di, s_den;
-    __shared__ int s_apply;
     cg::cluster_group cluster = cg::this_cluster();
     const int g = (int)cluster.block_rank(), G = (int)cluster.num_blocks();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int r0 = k + g * seg, r1 = min(m, r0 + seg);
     const int rows = max(0, r1 - r0);
     auto at = [&](int j, int row) -> float2 & { return sp[(j - k) * seg + (row - r0)]; };
+    // the blocks' totals in ascending block order: lane q fetches block q's, every lane adds
+    auto total1 = [&](float *mine) -> float
+    {
+        const float part = lane < G ? *cluster.map_shared_rank(mine, lane) : 0.0f;
+        float sum = __shfl_sync(0xffffffffu, part, 0);
+        for (int q = 1; q < G; ++q) sum = add_rn(sum, __shfl_sync(0xffffffffu, part, q));
+        return sum;
+    };
+    auto total2 = [&](float2 *mine) -> float2
+    {
+        const float2 part = lane < G ? *cluster.map_shared_rank(mine, lane) : make_float2(0.0f, 0.0f);
+        float2 sum = make_float2(__shfl_sync(0xffffffffu, part.x, 0), __shfl_sync(0xffffffffu, part.y, 0));
+        for (int q = 1; q < G; ++q)
+            sum = make_float2(add_rn(sum.x, __shfl_sync(0xffffffffu, part.x, q)),
+                              add_rn(sum.y, __shfl_sync(0xffffffffu, part.y, q)));
+        return sum;
+    };
     for (int idx = tid; idx < rows * kb; idx += PANEL_THREADS)
         sp[(idx / rows) * seg + idx % rows] = A[(int64_t)(k + idx / rows) * lda + r0 + idx % rows];
     __syncthreads();
-    bool prev_apply = false;
-    float pdr = 0.0f, pdi = 0.0f, pden = 1.0f;
+    CqScalars prev{};
+    prev.apply = false;
     for (int c = k; c < k + kb; ++c)
     {
         const int par = c & 1, owner = (c - k) / seg;
-        if (prev_apply)
+        if (prev.apply)  // column c - 1 becomes its reflector, beta its diagonal entry
+        {
+            if (tid == 0 && c - 1 >= r0 && c - 1 < r1) at(c - 1, c - 1) = make_float2(prev.beta, 0.0f);
             for (int row = max(r0, c) + tid; row < r1; row += PANEL_THREADS)
-                at(c - 1, row) = cq_reflect(at(c - 1, row), pdr, pdi, pden);
+                at(c - 1, row) = cq_reflect(at(c - 1, row), prev.dr, prev.di, prev.den);
+        }
         const int j = c + warp;
         if (warp == 0)
         {
             float p = 0.0f;
 #pragma unroll 4
-            for (int row = r0 + lane; row < r1; row += 32)
-                if (row > c)
-                {
-                    const float2 x = at(c, row);
-                    p = fma_rn(x.y, x.y, fma_rn(x.x, x.x, p));
-                }
+            for (int row = max(r0, c + 1) + lane; row < r1; row += 32)
+            {
+                const float2 x = at(c, row);
+                p = fma_rn(x.y, x.y, fma_rn(x.x, x.x, p));
+            }
             const float part = fold1(p);
             if (lane == 0) pub_sumsq[par] = part;
         }
@@ -240,66 +264,33 @@ __global__ void __launch_bounds__(PANEL_THREADS) cq_cluster_panel_kernel(float2 
         {
             float2 p = make_float2(0.0f, 0.0f);
 #pragma unroll 4
-            for (int row = r0 + lane; row < r1; row += 32)
-                if (row > c) p = cq_conjdot(p, at(c, row), at(j, row));
+            for (int row = max(r0, c + 1) + lane; row < r1; row += 32) p = cq_conjdot(p, at(c, row), at(j, row));
             const float2 part = fold2(p);
             if (lane == 0) pub_S[par][warp] = part;
         }
         if (j < k + kb && lane == 0 && g == owner) pub_row[par][warp] = at(j, c);
         cluster.sync();
-        if (tid == 0)
+        const CqScalars r = cq_scalars(total1(&pub_sumsq[par]), *cluster.map_shared_rank(&pub_row[par][0], owner));
+        if (tid == 0 && g == 0) tau[c] = r.t;
+        if (r.apply && warp >= 1 && j < k + kb)
         {
-            float parts[8];
-            for (int q = 0; q < G; ++q) parts[q] = *cluster.map_shared_rank(&pub_sumsq[par], q);
-            float sumsq = parts[0];
-            for (int q = 1; q < G; ++q) sumsq = add_rn(sumsq, parts[q]);
-            const float2 al = *cluster.map_shared_rank(&pub_row[par][0], owner);
-            float2 t = make_float2(0.0f, 0.0f);
-            int apply = 0;
-            if (!(sumsq == 0.0f && al.y == 0.0f))
-            {
-                const float norm = sqrt_rn(add_rn(add_rn(mul_rn(al.x, al.x), mul_rn(al.y, al.y)), sumsq));
-                const float beta = -copysignf(norm, al.x);
-                t = make_float2(div_rn(sub_rn(beta, al.x), beta), -div_rn(al.y, beta));
-                const float dr = sub_rn(al.x, beta), di = al.y;
-                const float den = add_rn(mul_rn(dr, dr), mul_rn(di, di));
-                s_dr = dr;
-                s_di = di;
-                s_den = den;
-                s_g = make_float2(div_rn(dr, den), div_rn(di, den));
-                if (owner == g) at(c, c) = make_float2(beta, 0.0f);
-                apply = 1;
-            }
-            if (g == 0) tau[c] = t;
-            s_tau = t;
-            s_apply = apply;
-        }
-        __syncthreads();
-        prev_apply = s_apply != 0;
-        if (prev_apply)
-        {
-            pdr = s_dr;
-            pdi = s_di;
-            pden = s_den;
-        }
-        if (prev_apply && warp >= 1 && j < k + kb)
-        {
-            float2 parts[8];
-            for (int q = 0; q < G; ++q) parts[q] = *cluster.map_shared_rank(&pub_S[par][warp], q);
-            float2 S = parts[0];
-            for (int q = 1; q < G; ++q) S = make_float2(add_rn(S.x, parts[q].x), add_rn(S.y, parts[q].y));
+            const float2 S = total2(&pub_S[par][warp]);
             const float2 acj = *cluster.map_shared_rank(&pub_row[par][warp], owner);
-            const float2 w = cq_mulc(s_tau, cq_fma(s_g, S, acj));
+            const float2 w = cq_mulc(r.t, cq_fma(r.g, S, acj));
             if (lane == 0 && g == owner) at(j, c) = clu::csubmul(acj, make_float2(1.0f, 0.0f), w);
 #pragma unroll 4
-            for (int row = r0 + lane; row < r1; row += 32)
-                if (row > c) at(j, row) = clu::csubmul(at(j, row), cq_reflect(at(c, row), pdr, pdi, pden), w);
+            for (int row = max(r0, c + 1) + lane; row < r1; row += 32)
+                at(j, row) = clu::csubmul(at(j, row), cq_reflect(at(c, row), r.dr, r.di, r.den), w);
         }
+        prev = r;
         __syncthreads();
     }
-    if (prev_apply)
+    if (prev.apply)
+    {
+        if (tid == 0 && k + kb - 1 >= r0 && k + kb - 1 < r1) at(k + kb - 1, k + kb - 1) = make_float2(prev.beta, 0.0f);
         for (int row = max(r0, k + kb) + tid; row < r1; row += PANEL_THREADS)
-            at(k + kb - 1, row) = cq_reflect(at(k + kb - 1, row), pdr, pdi, pden);
+            at(k + kb - 1, row) = cq_reflect(at(k + kb - 1, row), prev.dr, prev.di, prev.den);
+    }
     cluster.sync();  // no block leaves while another may still read what it published
     for (int idx = tid; idx < rows * kb; idx += PANEL_THREADS)
         A[(int64_t)(k + idx / rows) * lda + r0 + idx % rows] = sp[(idx / rows) * seg + idx % rows];
