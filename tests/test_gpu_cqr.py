@@ -273,3 +273,30 @@ def test_argument_ladders_write_minus_the_index(handle):
                                C.byref(niter), info.data_ptr()) == 3 and code() == -11
     assert lib.aclsolverCCgels(handle.value, 16, 16, 1, p, 16, big.data_ptr(), 16, xb.data_ptr(), 16, w.data_ptr(),
                                1 << 20, None, info.data_ptr()) == 3 and code() == -12
+
+
+def test_cgeqrf_look_ahead_on_a_side_stream():
+    """On a non-default stream the look-ahead forks and joins its panel stream around the
+    caller's work: the result is the oracle's bits and later work on the stream sees it."""
+    lib = aclsolver.library()
+    m, n = 900, 700
+    a = crand(m, n, 123)
+    stream = torch.cuda.Stream()
+    with aclsolver.Handle(stream=stream) as h:
+        dm = CMatrices(a[None], m + 2)
+        tau = cwork(n)
+        lw = C.c_int(-1)
+        assert lib.aclsolverCgeqrf_bufferSize(h.value, m, n, dm.tensor.data_ptr(), dm.ld, C.byref(lw)) == 0
+        w = cwork(lw.value)
+        info = info_buffer(1)
+        copy = torch.empty_like(dm.tensor)
+        torch.cuda.synchronize()  # the buffers were filled on the default stream
+        with torch.cuda.stream(stream):
+            assert lib.aclsolverCgeqrf(h.value, m, n, dm.tensor.data_ptr(), dm.ld, tau.data_ptr(), w.data_ptr(),
+                                       lw.value, info.data_ptr()) == aclsolver.SUCCESS
+            copy.copy_(dm.tensor)  # ordered after the call on the same stream
+        stream.synchronize()
+        want, wtau = oracle.cgeqrf(a)
+        got = np.ascontiguousarray(copy.cpu().numpy().view(np.complex64).reshape(n, m + 2)[:, :m].T)
+        assert int(info.cpu()[0]) == 0
+        assert cbits(got, want) and cbits(tau.cpu().numpy().view(np.complex64)[:n], wtau)

@@ -249,3 +249,35 @@ def test_sgeqrf_captured_in_a_cuda_graph(handle):
             assert int(info.cpu()[0]) == 0
             assert same_bits(dm.read()[0], want) and same_bits(tau.cpu().numpy(), wtau)
         del graph
+
+
+def test_sgeqrf_look_ahead_on_two_streams_at_once():
+    """Two handles on two streams factor at the same time; each call forks its own panel
+    stream and joins it back, so both results are the oracle's bits."""
+    lib = aclsolver.library()
+    m, n = 1500, 1200  # tall enough for the look-ahead and the cluster panels
+    mats = [rand(m, n, 90 + q) for q in range(2)]
+    streams = [torch.cuda.Stream() for _ in range(2)]
+    handles = [aclsolver.Handle(stream=s) for s in streams]
+    try:
+        bufs = []
+        for q in range(2):
+            dm = DeviceMatrices(mats[q], m + 1)
+            tau = torch.zeros(n, dtype=torch.float32, device="cuda")
+            lw = C.c_int(-1)
+            assert lib.aclsolverSgeqrf_bufferSize(handles[q].value, m, n, dm.ptr, dm.ld, C.byref(lw)) == 0
+            bufs.append((dm, tau, work(lw.value), info_buffer(1), lw.value))
+        torch.cuda.synchronize()
+        for q in range(2):
+            dm, tau, w, info, lw = bufs[q]
+            assert lib.aclsolverSgeqrf(handles[q].value, m, n, dm.ptr, dm.ld, tau.data_ptr(), w.data_ptr(), lw,
+                                       info.data_ptr()) == aclsolver.SUCCESS
+        torch.cuda.synchronize()
+        for q in range(2):
+            dm, tau, _, info, _ = bufs[q]
+            want, wtau = oracle.sgeqrf(mats[q])
+            assert int(info.cpu()[0]) == 0
+            assert same_bits(dm.read()[0], want) and same_bits(tau.cpu().numpy(), wtau)
+    finally:
+        for h in handles:
+            h.close()
