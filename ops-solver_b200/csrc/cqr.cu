@@ -74,10 +74,10 @@ __device__ __forceinline__ bool czero2(float2 v) { return v.x == 0.0f && v.y == 
 // Panel columns [k, k + kb) of rows [k, m), in shared memory (SMEM) or, for panels taller
 // than eight blocks hold, in A.  Per column c, every reduction over the rows below c is taken
 // at once from the column as it stands: warp 0 forms sumsq = sum |x_i|^2 and warp w >= 1
-// forms S_j = sum conj(x_i) A(i, j) for column j = c + w, in parallel.  Thread 0 then forms
-// beta, tau, d = alpha - beta, den = |d|^2 and g = d / den; warp w applies
-// w_j = conj(tau) (A(c, j) + g S_j) with v_i = x_i / d formed on the fly; column c itself is
-// divided during the next column's reductions.
+// forms S_j = sum conj(x_i) A(i, j) for column j = c + w, in parallel.  After one barrier
+// every thread forms beta, tau, d = alpha - beta, den = |d|^2 and g = d / den (cq_scalars);
+// warp w applies w_j = conj(tau) (A(c, j) + g S_j) with v_i = x_i / d formed on the fly;
+// column c itself is divided, and beta stored, during the next column's reductions.
 __device__ __forceinline__ float2 cq_reflect(float2 x, float dr, float di, float den)
 {
     return make_float2(div_rn(add_rn(mul_rn(x.x, dr), mul_rn(x.y, di)), den),

@@ -48,9 +48,10 @@ __device__ __forceinline__ float lane_fold(float p)
 // Panel columns [k, k + kb) of rows [k, m), staged in shared memory (pitch m - k).  Per column
 // c, every reduction over the rows below c is taken at once from the column as it stands:
 // warp 0 forms sumsq = sum x_i^2 and warp w >= 1 forms S_j = sum x_i A(i, j) for column
-// j = c + w (lane sums), in parallel.  Thread 0 then forms beta, tau and scale =
-// 1 / (alpha - beta); warp w applies w_j = tau fma(scale, S_j, A(c, j)) with v_i = x_i scale
-// (v_c = 1) formed on the fly; column c itself is scaled during the next column's reductions.
+// j = c + w (lane sums), in parallel.  After one barrier every thread forms beta, tau and
+// scale = 1 / (alpha - beta) (the same operations on the same values, so no second barrier);
+// warp w applies w_j = tau fma(scale, S_j, A(c, j)) with v_i = x_i scale (v_c = 1) formed on
+// the fly; column c itself is scaled, and beta stored, during the next column's reductions.
 constexpr int PANEL_SMEM_FLOATS = 50 * 1024;
 
 __global__ void __launch_bounds__(PANEL_THREADS) qr_panel_kernel(float *A, int lda, int m, int k, int kb, float *tau)
