@@ -699,8 +699,12 @@ cudaError_t launch_cgeqrf(float2 *A, int lda, int m, int n, float2 *tau, float2 
         cudaGetLastError();
         capture = cudaStreamCaptureStatusActive;
     }
-    const bool ahead = e == cudaSuccess && capture == cudaStreamCaptureStatusNone && m >= 512 && n > 3 * NB;
-    if (ahead) e = la.open(stream);
+    bool ahead = e == cudaSuccess && capture == cudaStreamCaptureStatusNone && m >= 512 && n > 3 * NB;
+    if (ahead && la.open(stream) != cudaSuccess)
+    {
+        la.abandon();  // no private stream to be had: factor on the caller's stream alone
+        ahead = false;
+    }
     cudaStream_t ps = ahead ? la.panel : stream;
     for (int k = 0; k < lim && e == cudaSuccess; k += NB)
     {

@@ -48,6 +48,13 @@ class Lookahead
         release();
         return e;
     }
+    // Gives up after a failed open (nothing but the fork is queued on the panel stream); the
+    // caller then runs without look-ahead.
+    void abandon()
+    {
+        cudaGetLastError();
+        release();
+    }
 
   private:
     cudaEvent_t to_main_ = nullptr, to_panel_ = nullptr;
