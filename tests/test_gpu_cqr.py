@@ -300,3 +300,13 @@ def test_cgeqrf_look_ahead_on_a_side_stream():
         got = np.ascontiguousarray(copy.cpu().numpy().view(np.complex64).reshape(n, m + 2)[:, :m].T)
         assert int(info.cpu()[0]) == 0
         assert cbits(got, want) and cbits(tau.cpu().numpy().view(np.complex64)[:n], wtau)
+
+
+@pytest.mark.parametrize("m,n", [(4100, 70), (513, 200), (700, 1000), (801, 97), (6401, 40)])
+def test_cgeqrf_shape_sweep(handle, m, n):
+    """Shapes around the panel thresholds (one block up to 800 rows, an eight-block cluster up
+    to 6,400, then one block reading A), and the look-ahead's, against the oracle."""
+    a = crand(m, n, m + 3 * n)
+    got, tau = geqrf(handle, a, pad=1)
+    want, wtau = oracle.cgeqrf(a)
+    assert cbits(tau, wtau) and cbits(got, want)

@@ -281,3 +281,13 @@ def test_sgeqrf_look_ahead_on_two_streams_at_once():
     finally:
         for h in handles:
             h.close()
+
+
+@pytest.mark.parametrize("m,n", [(8192, 40), (513, 513), (2049, 97), (600, 1000), (1601, 130), (3000, 64)])
+def test_sgeqrf_shape_sweep(handle, m, n):
+    """Shapes around the panel thresholds (one block up to 1,600 rows, then an eight-block
+    cluster), the look-ahead's (m >= 512, n > 96) and the row limit, against the oracle."""
+    a = rand(m, n, m + 7 * n)
+    got, tau = geqrf(handle, a, pad=1)
+    want, wtau = oracle.sgeqrf(a)
+    assert same_bits(tau, wtau) and same_bits(got, want)
